@@ -1,0 +1,182 @@
+/*
+ * tfdtd.h - C ABI of the B200-native fused Yee/CPML engine (libtfdtd.so).
+ *
+ * This is the drop-in boundary for TorchFDTD's fused CUDA path. In the
+ * reference the path is reached from Python through
+ *   Simulation(project).run()                      torchfdtd/solver.py:662-908
+ *   configure_cuda_kernel(grid, 'fused')           torchfdtd/cuda_kernels.py:368-373
+ *   FusedYeeCUDA.update_E / update_H               torchfdtd/cuda_kernels.py:349-365
+ *   FusedFrequencyPlanes.update(counter)           torchfdtd/cuda_monitors.py:135-155
+ *   CudaStepGraphs(step, states, steps, width)     torchfdtd/cuda_graph.py:187-218
+ * Here the same work sits behind plain C entry points (pointers, sizes, int
+ * status codes, no exceptions, no torch types) that any host language can bind;
+ * the Python package binds them with ctypes.
+ *
+ * Memory: the caller allocates ONE device arena of tfd_plan_bytes() bytes
+ * (PyTorch does, mirroring the reference, where torch owns every array,
+ * torchfdtd/cuda_kernels.py:120-128) and the library lays out fields, CPML
+ * memories, material, tables and monitor accumulators inside it. The main
+ * entry points never call cudaMalloc.
+ *
+ * Streams: every call takes a cudaStream_t (as void*); work is enqueued on it.
+ * tfd_step is capturable in a CUDA graph (no allocation, no synchronisation,
+ * the time step is read from a device counter). Calls with TFD_HOST buffers
+ * synchronise the stream before returning.
+ *
+ * Every function returns TFD_OK (0) or an error code; tfd_last_error() gives a
+ * message for the calling thread's last failure.
+ */
+#ifndef TFDTD_H
+#define TFDTD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TFD_ABI_VERSION 1
+
+enum tfd_code {
+    TFD_OK = 0,
+    TFD_ERR_INVALID = 1,       /* bad argument or descriptor; reference: ValueError */
+    TFD_ERR_UNSUPPORTED = 2,   /* feature outside the fused path; reference: ValueError naming it */
+    TFD_ERR_CUDA = 3,          /* CUDA runtime error; reference: RuntimeError */
+    TFD_ERR_ARENA = 4,         /* arena too small or misaligned */
+    TFD_ERR_DEVICE = 5         /* a kernel reported a failure in the device status word */
+};
+
+enum tfd_face { TFD_FACE_PML = 0, TFD_FACE_PERIODIC = 1, TFD_FACE_PEC = 2 };
+enum tfd_where { TFD_DEVICE = 0, TFD_HOST = 1 };
+enum tfd_kernel { TFD_KERNEL_AUTO = 0, TFD_KERNEL_MARCH = 1, TFD_KERNEL_GATHER = 2 };
+
+/* One CPML slab of one field family on one axis (both curl terms of that axis share it).
+ * forward = 0: E family (backward differences), 1: H family (forward differences).
+ * Targets are cells [lo, hi) along axis; b, c, inv_kappa hold hi-lo float64 values.
+ * Reference: YeeGrid._prepare_boundaries, torchfdtd/boundaries.py:307-355. */
+typedef struct tfd_cpml_segment {
+    int32_t forward, axis, lo, hi;
+    const double *b, *c, *inv_kappa;
+} tfd_cpml_segment;
+
+/* A soft source term: values[n] is ADDED to component `component` of family
+ * `family` (0 E, 1 H) on cells [lo, hi) right after that family's update of
+ * step n. Reference: torchfdtd/injection.py:117-141, torchfdtd/solver.py:778-789. */
+typedef struct tfd_source_term {
+    int32_t family, component;
+    int32_t lo[3], hi[3];
+    const double *values;     /* steps samples, rounded to the field precision */
+} tfd_source_term;
+
+/* A point trace, recorded after the H update of each step.
+ * Reference: torchfdtd/solver.py:765,790-796. */
+typedef struct tfd_trace {
+    int32_t family, component;
+    int32_t index[3];
+} tfd_trace;
+
+/* An online DFT plane: per step n, sample = sum_k field[corner k] * weight k (field
+ * precision, in corner order) * window[n]; then for every frequency f
+ * acc[f][p][c] += exp(i*omega_f*(n+1)) * sample, times exp(i*pi*f*dt) for H samples.
+ * Accumulators are complex float64. E components come first.
+ * Reference: torchfdtd/field_monitors.py:121-164, torchfdtd/cuda_monitors.py:65-155. */
+typedef struct tfd_plane {
+    int32_t points, frequencies, components, corners;
+    const int32_t *component_ids;  /* components entries, 0..5 = Ex Ey Ez Hx Hy Hz */
+    const int64_t *corner_cells;   /* [components][corners][points] flat (x*ny+y)*nz+z */
+    const double *corner_weights;  /* same shape */
+    const double *frequency_hz;    /* frequencies */
+    const double *window_e;        /* steps: apodization * dt * downsample mask, E samples */
+    const double *window_h;        /* steps, H samples (half a step later) */
+} tfd_plane;
+
+typedef struct tfd_desc {
+    int32_t abi_version;           /* TFD_ABI_VERSION */
+    int32_t nx, ny, nz;            /* Yee cells; nz = 1 for 2D */
+    int32_t precision;             /* 4: float32 fields, 8: float64 fields */
+    int32_t material_samples;      /* 1 (one inverse permittivity per cell) or 3 (per E component) */
+    int32_t components;            /* bit c (0..5) set = component advanced; 0x3F in 3D */
+    int32_t steps;                 /* length of every per-step table (sources, windows, traces) */
+    int32_t kernel;                /* enum tfd_kernel */
+    int32_t face[3][2];            /* enum tfd_face per axis and side */
+    double courant;                /* rectangular Courant number c*dt/dx */
+    double time_step;              /* seconds */
+    double pec_upper[3];           /* H ghost factor on PEC upper faces (reference_step / last width) */
+    int32_t n_segments;
+    const tfd_cpml_segment *segments;
+    int32_t n_sources;
+    const tfd_source_term *sources;
+    int32_t n_traces;
+    const tfd_trace *traces;
+    int32_t n_planes;
+    const tfd_plane *planes;
+} tfd_desc;
+
+typedef struct tfd_plan tfd_plan;
+
+/* Arena size for a descriptor. Replaces the reference's per-array torch allocations
+ * (torchfdtd/boundaries.py:231-256, torchfdtd/solver.py:769-771, field_monitors.py:136). */
+int tfd_plan_bytes(const tfd_desc *desc, size_t *bytes);
+
+/* Lay out the arena, upload the tables and zero the state (fields, CPML memories,
+ * monitors, step counter). Replaces YeeGrid(...) + configure_cuda_kernel(grid, 'fused')
+ * + FrequencyUpdates(...) (torchfdtd/solver.py:741-776). The arena must be 256-byte
+ * aligned and stay allocated until tfd_plan_destroy. */
+int tfd_plan_create(const tfd_desc *desc, void *arena, size_t arena_bytes, void *stream, tfd_plan **plan);
+void tfd_plan_destroy(tfd_plan *plan);
+
+/* Inverse permittivity in the reference layout (nx, ny, nz[, 3]) C order, z fastest,
+ * field precision. Replaces g.inverse_permittivity[:] = 1/eps (torchfdtd/solver.py:742-745). */
+int tfd_set_material(tfd_plan *plan, const void *inv_eps, int where, void *stream);
+
+/* E and H in the reference layout (nx, ny, nz, 3), field precision (g.E, g.H). */
+int tfd_set_fields(tfd_plan *plan, const void *E, const void *H, int where, void *stream);
+int tfd_get_fields(tfd_plan *plan, void *E, void *H, int where, void *stream);
+
+/* Every CPML memory concatenated in the reference's YeeGrid.memory_states order and
+ * shapes (torchfdtd/boundaries.py:307-355); tfd_psi_count gives the element count. */
+int tfd_psi_count(const tfd_plan *plan, size_t *count);
+int tfd_set_psi(tfd_plan *plan, const void *psi, int where, void *stream);
+int tfd_get_psi(tfd_plan *plan, void *psi, int where, void *stream);
+
+/* Advance nsteps time steps: fused E update + E sources + H update + H sources, then
+ * the point traces, the DFT planes and the step counter. Replaces one replay of the
+ * reference's captured step (torchfdtd/solver.py:785-797, cuda_graph.py:62-63).
+ * Capturable in a CUDA graph. */
+int tfd_step(tfd_plan *plan, int32_t nsteps, void *stream);
+
+/* Zero fields, CPML memories, traces, DFT accumulators and the step counter. */
+int tfd_reset(tfd_plan *plan, void *stream);
+
+/* Point traces, (steps, n_traces) field precision (torchfdtd/solver.py:771,908). */
+int tfd_get_traces(tfd_plan *plan, void *dst, int where, void *stream);
+
+/* DFT plane k accumulators as complex float64 (frequencies, points, components). */
+int tfd_get_plane(tfd_plan *plan, int32_t k, void *dst, int where, void *stream);
+
+/* One plane of one component (0..5) at `index` on `axis`, reference order of the two
+ * remaining axes, field precision: the snapshot frame (torchfdtd/solver.py:821-863). */
+int tfd_get_slice(tfd_plan *plan, int32_t component, int32_t axis, int32_t index, void *dst, int where, void *stream);
+
+/* Divergence diagnostics of torchfdtd/run_control.py:127-159: out[0] = sum over cells and
+ * components of E^2/inv_eps + H^2 (float64), out[1] = max |E|, |H|, out[2] = 1 when every
+ * CPML memory is finite. Synchronises the stream. */
+int tfd_diagnose(tfd_plan *plan, double out[3], void *stream);
+
+/* The device step counter (synchronises the stream). */
+int tfd_counter(tfd_plan *plan, int64_t *value, void *stream);
+
+/* The device status word: 0, or the code a kernel recorded (synchronises the stream). */
+int tfd_device_status(tfd_plan *plan, int32_t *status, void *stream);
+
+/* Which step kernel the plan runs (enum tfd_kernel) after TFD_KERNEL_AUTO is resolved. */
+int tfd_kernel_in_use(const tfd_plan *plan, int32_t *kernel);
+
+const char *tfd_error_string(int code);
+const char *tfd_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TFDTD_H */

@@ -1,0 +1,860 @@
+// C ABI of libtfdtd: arena layout, table upload, step dispatch, layout conversion and
+// diagnostics. Declarations and the reference interfaces they replace: include/tfdtd.h.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "aux.cuh"
+#include "internal.cuh"
+#include "step_gather.cuh"
+
+using namespace tfd;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string &msg) {
+    g_error = msg;
+    return code;
+}
+
+#define TFD_CUDA(expr)                                                                                 \
+    do {                                                                                               \
+        cudaError_t e_ = (expr);                                                                       \
+        if (e_ != cudaSuccess) return fail(TFD_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int kMaskTM = 0x04 | 0x08 | 0x10;   // Ez, Hx, Hy
+constexpr int kMaskTE = 0x01 | 0x02 | 0x20;   // Ex, Ey, Hz
+constexpr int kMaskAll = 0x3F;
+constexpr int kDiagBlocks = 296;
+
+// Offsets start at 256: offset 0 means "not allocated" (a component 2D does not advance).
+struct Bump {
+    size_t off = 256;
+    size_t take(size_t bytes) {
+        const size_t o = (off + 255) & ~size_t(255);
+        off = o + bytes;
+        return o;
+    }
+};
+
+struct PlaneLayout {
+    size_t cell, weight, omega, half, window, acc;
+};
+
+struct Layout {
+    int elem = 4;
+    int pitch = 0;
+    long long count = 0;           // elements per component array (one parity)
+    size_t E[3], H[3];             // both parities, contiguous
+    size_t inv[3];
+    size_t cb[2][3], cc[2][3], ck[2][3], row[2][3];
+    int rows[2][3];
+    long long psi_len[2][3];
+    size_t psiE[3][2], psiH[3][2];
+    size_t src_values = 0, trace_tab = 0, trace_out = 0, plane_tab = 0;
+    std::vector<PlaneLayout> planes;
+    size_t counter = 0, done = 0, status = 0, diag = 0, stage = 0;
+    size_t stage_bytes = 0;
+    size_t psi_total = 0;          // elements of the reference psi vector
+    size_t total = 0;
+};
+
+bool active(int mask, int bit) { return (mask >> bit) & 1; }
+
+int validate(const tfd_desc *d) {
+    if (d == nullptr) return fail(TFD_ERR_INVALID, "descriptor is null");
+    if (d->abi_version != TFD_ABI_VERSION) return fail(TFD_ERR_INVALID, "descriptor ABI version mismatch");
+    if (d->nx < 1 || d->ny < 1 || d->nz < 1) return fail(TFD_ERR_INVALID, "grid extents must be positive");
+    if (d->nx > 1000000 || d->ny > 1000000 || d->nz > 1000000) return fail(TFD_ERR_INVALID, "a grid axis may hold at most one million cells");
+    if (d->precision != 4 && d->precision != 8) return fail(TFD_ERR_INVALID, "precision must be 4 (float32) or 8 (float64)");
+    if (d->material_samples != 1 && d->material_samples != 3) return fail(TFD_ERR_INVALID, "material_samples must be 1 or 3");
+    if (d->steps < 0) return fail(TFD_ERR_INVALID, "steps must be non-negative");
+    if (!(d->courant > 0) || !std::isfinite(d->courant)) return fail(TFD_ERR_INVALID, "courant must be positive and finite");
+    const int n[3] = {d->nx, d->ny, d->nz};
+    const bool two_d = d->nz == 1;
+    if (two_d) {
+        if (d->components != kMaskTM && d->components != kMaskTE && d->components != kMaskAll)
+            return fail(TFD_ERR_INVALID, "2D components must be TM (Ez,Hx,Hy), TE (Ex,Ey,Hz) or all six");
+    } else if (d->components != kMaskAll) {
+        return fail(TFD_ERR_INVALID, "3D grids advance all six components");
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int s = 0; s < 2; ++s)
+            if (d->face[a][s] < TFD_FACE_PML || d->face[a][s] > TFD_FACE_PEC) return fail(TFD_ERR_UNSUPPORTED, "unsupported boundary kind");
+    for (int a = 0; a < 3; ++a)
+        if (n[a] > 1 && ((d->face[a][0] == TFD_FACE_PERIODIC) != (d->face[a][1] == TFD_FACE_PERIODIC)))
+            return fail(TFD_ERR_INVALID, "periodic faces must be paired on an axis");
+    if (d->n_segments < 0 || d->n_segments > 12 || (d->n_segments && !d->segments)) return fail(TFD_ERR_INVALID, "bad CPML segment list");
+    for (int k = 0; k < d->n_segments; ++k) {
+        const tfd_cpml_segment &s = d->segments[k];
+        if (s.forward < 0 || s.forward > 1 || s.axis < 0 || s.axis > 2) return fail(TFD_ERR_INVALID, "bad CPML segment family/axis");
+        if (n[s.axis] == 1) return fail(TFD_ERR_INVALID, "CPML segment on an invariant axis");
+        const int lo_min = s.forward ? 0 : 1, hi_max = s.forward ? n[s.axis] - 1 : n[s.axis];
+        if (s.lo < lo_min || s.hi > hi_max || s.lo >= s.hi) return fail(TFD_ERR_INVALID, "CPML segment outside the active derivative range");
+        if (!s.b || !s.c || !s.inv_kappa) return fail(TFD_ERR_INVALID, "CPML segment coefficients missing");
+        for (int q = 0; q < k; ++q) {
+            const tfd_cpml_segment &o = d->segments[q];
+            if (o.forward == s.forward && o.axis == s.axis && s.lo < o.hi && o.lo < s.hi)
+                return fail(TFD_ERR_INVALID, "overlapping CPML segments");
+        }
+    }
+    if (d->n_sources < 0 || d->n_sources > kMaxSources || (d->n_sources && !d->sources))
+        return fail(TFD_ERR_INVALID, "at most 16 source terms are supported per plan");
+    for (int k = 0; k < d->n_sources; ++k) {
+        const tfd_source_term &s = d->sources[k];
+        if (s.family < 0 || s.family > 1 || s.component < 0 || s.component > 2) return fail(TFD_ERR_INVALID, "bad source component");
+        for (int a = 0; a < 3; ++a)
+            if (s.lo[a] < 0 || s.hi[a] > n[a] || s.lo[a] >= s.hi[a]) return fail(TFD_ERR_INVALID, "source box outside the grid");
+        if (d->steps > 0 && !s.values) return fail(TFD_ERR_INVALID, "source values missing");
+    }
+    if (d->n_traces < 0 || (d->n_traces && !d->traces)) return fail(TFD_ERR_INVALID, "bad trace list");
+    for (int k = 0; k < d->n_traces; ++k) {
+        const tfd_trace &t = d->traces[k];
+        if (t.family < 0 || t.family > 1 || t.component < 0 || t.component > 2) return fail(TFD_ERR_INVALID, "bad trace component");
+        for (int a = 0; a < 3; ++a)
+            if (t.index[a] < 0 || t.index[a] >= n[a]) return fail(TFD_ERR_INVALID, "trace index outside the grid");
+    }
+    if (d->n_planes < 0 || d->n_planes > 65535 || (d->n_planes && !d->planes)) return fail(TFD_ERR_INVALID, "bad plane list");
+    const long long cells = (long long)n[0] * n[1] * n[2];
+    for (int k = 0; k < d->n_planes; ++k) {
+        const tfd_plane &p = d->planes[k];
+        if (p.points < 0 || p.frequencies < 0 || p.components < 1 || p.components > 6 || p.corners < 1 || p.corners > 8)
+            return fail(TFD_ERR_INVALID, "bad plane sizes");
+        if ((long long)p.points * p.components > (1LL << 30)) return fail(TFD_ERR_INVALID, "plane too large");
+        if (!p.component_ids || (p.points && (!p.corner_cells || !p.corner_weights)) || (p.frequencies && !p.frequency_hz) ||
+            (d->steps && (!p.window_e || !p.window_h)))
+            return fail(TFD_ERR_INVALID, "plane tables missing");
+        int ne = 0;
+        for (int c = 0; c < p.components; ++c) {
+            const int id = p.component_ids[c];
+            if (id < 0 || id > 5) return fail(TFD_ERR_INVALID, "bad plane component id");
+            if (id < 3) {
+                if (ne != c) return fail(TFD_ERR_INVALID, "plane E components must come first");
+                ++ne;
+            }
+        }
+        const long long entries = (long long)p.components * p.corners * p.points;
+        for (long long e = 0; e < entries; ++e)
+            if (p.corner_cells[e] < 0 || p.corner_cells[e] >= cells) return fail(TFD_ERR_INVALID, "plane corner outside the grid");
+    }
+    return TFD_OK;
+}
+
+// The segment order of the reference's memory_states: family, then CURL_TERMS order
+// ((a, j) = (0,0),(0,1),(1,0),(1,1),(2,0),(2,1)), then side.
+std::vector<PsiSegment> psi_segments(const tfd_desc *d, size_t *total) {
+    const int n[3] = {d->nx, d->ny, d->nz};
+    std::vector<PsiSegment> out;
+    long long off = 0;
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 3; ++a)
+            for (int j = 0; j < 2; ++j) {
+                if (n[a] == 1) continue;
+                std::vector<const tfd_cpml_segment *> segs;
+                for (int k = 0; k < d->n_segments; ++k)
+                    if (d->segments[k].forward == f && d->segments[k].axis == a) segs.push_back(&d->segments[k]);
+                std::sort(segs.begin(), segs.end(), [](auto *x, auto *y) { return x->lo < y->lo; });
+                for (auto *s : segs) {
+                    long long ext[3] = {n[0], n[1], n[2]};
+                    ext[a] = s->hi - s->lo;
+                    out.push_back(PsiSegment{off, f, a, j, s->lo, s->hi});
+                    off += ext[0] * ext[1] * ext[2];
+                }
+            }
+    *total = (size_t)off;
+    return out;
+}
+
+void compute_layout(const tfd_desc *d, Layout &L) {
+    Bump b;
+    const int n[3] = {d->nx, d->ny, d->nz};
+    L.elem = d->precision;
+    L.pitch = (d->nx + kPitchAlign - 1) / kPitchAlign * kPitchAlign;
+    L.count = (long long)d->nz * d->ny * L.pitch;
+    L.count = (L.count + 63) / 64 * 64;          // parity-1 arrays stay 256-byte aligned
+    const size_t comp_bytes = (size_t)L.count * L.elem;
+    for (int c = 0; c < 3; ++c) {
+        L.E[c] = active(d->components, c) ? b.take(2 * comp_bytes) : 0;
+        L.H[c] = active(d->components, 3 + c) ? b.take(2 * comp_bytes) : 0;
+    }
+    for (int s = 0; s < 3; ++s) L.inv[s] = s < d->material_samples ? b.take(comp_bytes) : 0;
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 3; ++a) {
+            int rows = 0;
+            for (int k = 0; k < d->n_segments; ++k)
+                if (d->segments[k].forward == f && d->segments[k].axis == a) rows += d->segments[k].hi - d->segments[k].lo;
+            L.rows[f][a] = rows;
+            L.cb[f][a] = L.cc[f][a] = L.ck[f][a] = L.row[f][a] = 0;
+            L.psi_len[f][a] = 0;
+            if (rows == 0) continue;
+            L.cb[f][a] = b.take((size_t)n[a] * L.elem);
+            L.cc[f][a] = b.take((size_t)n[a] * L.elem);
+            L.ck[f][a] = b.take((size_t)n[a] * L.elem);
+            L.row[f][a] = b.take((size_t)n[a] * sizeof(int));
+            L.psi_len[f][a] = a == 0 ? (long long)n[2] * n[1] * rows
+                            : a == 1 ? (long long)n[2] * rows * L.pitch
+                                     : (long long)rows * n[1] * L.pitch;
+        }
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 2; ++j) {
+            L.psiE[a][j] = L.psi_len[0][a] && active(d->components, term_out(a, j))
+                               ? b.take(2 * (size_t)((L.psi_len[0][a] + 63) / 64 * 64) * L.elem) : 0;
+            L.psiH[a][j] = L.psi_len[1][a] && active(d->components, 3 + term_out(a, j))
+                               ? b.take((size_t)L.psi_len[1][a] * L.elem) : 0;
+        }
+    L.src_values = b.take((size_t)std::max(1, d->n_sources) * std::max(1, d->steps) * L.elem);
+    L.trace_tab = b.take((size_t)std::max(1, d->n_traces) * sizeof(TraceDev));
+    L.trace_out = b.take((size_t)std::max(1, d->n_traces) * std::max(1, d->steps) * L.elem);
+    L.plane_tab = b.take((size_t)std::max(1, d->n_planes) * sizeof(PlaneDev));
+    size_t largest_plane = 0;
+    L.planes.resize(d->n_planes);
+    for (int k = 0; k < d->n_planes; ++k) {
+        const tfd_plane &p = d->planes[k];
+        const size_t entries = (size_t)p.components * p.corners * p.points;
+        PlaneLayout &q = L.planes[k];
+        q.cell = b.take(std::max<size_t>(1, entries) * sizeof(long long));
+        q.weight = b.take(std::max<size_t>(1, entries) * L.elem);
+        q.omega = b.take(std::max<size_t>(1, p.frequencies) * sizeof(double));
+        q.half = b.take(std::max<size_t>(1, p.frequencies) * 2 * sizeof(double));
+        q.window = b.take(2 * (size_t)std::max(1, d->steps) * L.elem);
+        const size_t acc = (size_t)p.frequencies * p.points * p.components * 2 * sizeof(double);
+        q.acc = b.take(std::max<size_t>(1, acc));
+        largest_plane = std::max(largest_plane, acc);
+    }
+    L.counter = b.take(sizeof(long long));
+    L.done = b.take(sizeof(unsigned));
+    L.status = b.take(sizeof(int));
+    L.diag = b.take((size_t)kDiagBlocks * 4 * sizeof(double));
+    psi_segments(d, &L.psi_total);
+    const long long cells = (long long)n[0] * n[1] * n[2];
+    L.stage_bytes = std::max({(size_t)cells * 3 * L.elem, L.psi_total * L.elem, largest_plane,
+                              (size_t)std::max(1, d->n_traces) * std::max(1, d->steps) * L.elem, (size_t)256});
+    L.stage = b.take(L.stage_bytes);
+    L.total = b.off + 256;
+}
+
+}  // namespace
+
+struct tfd_plan {
+    tfd_desc desc;               // sizes and flags only; host pointers are not kept
+    Layout L;
+    char *arena = nullptr;
+    Grid<float> gf;
+    Grid<double> gd;
+    int kernel = TFD_KERNEL_GATHER;
+    std::vector<PsiSegment> psi_segs;
+    std::vector<int> planes_f, planes_p, planes_c;
+    int max_samples = 0;
+
+    template <typename T> Grid<T> &grid();
+    template <typename T> T *ptr(size_t off) const { return off ? (T *)(arena + off) : nullptr; }
+};
+template <> Grid<float> &tfd_plan::grid<float>() { return gf; }
+template <> Grid<double> &tfd_plan::grid<double>() { return gd; }
+
+namespace {
+
+template <typename T>
+__global__ void k_fill(T *p, long long n, T v) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) p[e] = v;
+}
+
+int launch_blocks(long long work, int threads = 256) {
+    long long b = (work + threads - 1) / threads;
+    return (int)std::max(1LL, std::min(b, 148LL * 32));
+}
+
+template <typename T>
+int upload(cudaStream_t s, tfd_plan *p, size_t off, const std::vector<T> &v) {
+    if (v.empty()) return TFD_OK;
+    TFD_CUDA(cudaMemcpyAsync(p->arena + off, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    return TFD_OK;
+}
+
+template <typename T>
+int create_typed(tfd_plan *p, const tfd_desc *d, cudaStream_t s) {
+    const Layout &L = p->L;
+    Grid<T> &g = p->grid<T>();
+    std::memset(&g, 0, sizeof(g));
+    const int n[3] = {d->nx, d->ny, d->nz};
+    for (int a = 0; a < 3; ++a) g.n[a] = n[a];
+    g.pitch = L.pitch;
+    g.plane = (long long)d->ny * L.pitch;
+    g.count = L.count;
+    g.steps = d->steps;
+    g.active = d->components;
+    g.cn = (T)d->courant;
+    for (int a = 0; a < 3; ++a) {
+        g.periodic[a] = n[a] > 1 && d->face[a][0] == TFD_FACE_PERIODIC;
+        g.pec_on[a] = n[a] > 1 && !g.periodic[a] && d->face[a][1] == TFD_FACE_PEC;
+        g.pec_neg[a] = (T)(-d->pec_upper[a]);
+    }
+    for (int par = 0; par < 2; ++par)
+        for (int c = 0; c < 3; ++c) {
+            g.E[par][c] = L.E[c] ? p->ptr<T>(L.E[c]) + par * L.count : nullptr;
+            g.H[par][c] = L.H[c] ? p->ptr<T>(L.H[c]) + par * L.count : nullptr;
+        }
+    for (int c = 0; c < 3; ++c) g.inv_eps[c] = p->ptr<T>(L.inv[d->material_samples == 3 ? c : 0]);
+    // CPML tables
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 3; ++a) {
+            g.rows[f][a] = L.rows[f][a];
+            if (!L.rows[f][a]) continue;
+            std::vector<T> vb(n[a], T(0)), vc(n[a], T(0)), vk(n[a], T(1));
+            std::vector<int> vr(n[a], -1);
+            std::vector<const tfd_cpml_segment *> segs;
+            for (int k = 0; k < d->n_segments; ++k)
+                if (d->segments[k].forward == f && d->segments[k].axis == a) segs.push_back(&d->segments[k]);
+            std::sort(segs.begin(), segs.end(), [](auto *x, auto *y) { return x->lo < y->lo; });
+            int r = 0;
+            for (auto *sg : segs)
+                for (int i = sg->lo; i < sg->hi; ++i) {
+                    vb[i] = (T)sg->b[i - sg->lo];
+                    vc[i] = (T)sg->c[i - sg->lo];
+                    vk[i] = (T)sg->inv_kappa[i - sg->lo];
+                    vr[i] = r++;
+                }
+            int rc;
+            if ((rc = upload(s, p, L.cb[f][a], vb)) || (rc = upload(s, p, L.cc[f][a], vc)) || (rc = upload(s, p, L.ck[f][a], vk)) ||
+                (rc = upload(s, p, L.row[f][a], vr)))
+                return rc;
+            g.cb[f][a] = p->ptr<T>(L.cb[f][a]);
+            g.cc[f][a] = p->ptr<T>(L.cc[f][a]);
+            g.ck[f][a] = p->ptr<T>(L.ck[f][a]);
+            g.row[f][a] = p->ptr<int>(L.row[f][a]);
+        }
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 2; ++j) {
+            const long long padded = (L.psi_len[0][a] + 63) / 64 * 64;
+            for (int par = 0; par < 2; ++par) g.psiE[par][a][j] = L.psiE[a][j] ? p->ptr<T>(L.psiE[a][j]) + par * padded : nullptr;
+            g.psiH[a][j] = p->ptr<T>(L.psiH[a][j]);
+        }
+    // sources
+    g.n_src = d->n_sources;
+    std::vector<T> values((size_t)std::max(1, d->n_sources) * std::max(1, d->steps), T(0));
+    for (int k = 0; k < d->n_sources; ++k) {
+        const tfd_source_term &t = d->sources[k];
+        g.src[k].family = t.family;
+        g.src[k].comp = t.component;
+        for (int a = 0; a < 3; ++a) { g.src[k].lo[a] = t.lo[a]; g.src[k].hi[a] = t.hi[a]; }
+        for (int q = 0; q < d->steps; ++q) values[(size_t)k * d->steps + q] = (T)t.values[q];
+        if (!active(d->components, 3 * t.family + t.component))
+            return fail(TFD_ERR_INVALID, "a source drives a component this plan does not advance");
+    }
+    int rc;
+    if ((rc = upload(s, p, L.src_values, values))) return rc;
+    g.src_values = p->ptr<T>(L.src_values);
+    g.counter = p->ptr<long long>(L.counter);
+    g.status = p->ptr<int>(L.status);
+    // traces
+    std::vector<TraceDev> traces(d->n_traces);
+    for (int k = 0; k < d->n_traces; ++k) {
+        const tfd_trace &t = d->traces[k];
+        traces[k] = TraceDev{t.family, t.component, ((long long)t.index[2] * d->ny + t.index[1]) * L.pitch + t.index[0]};
+    }
+    if ((rc = upload(s, p, L.trace_tab, traces))) return rc;
+    // planes
+    std::vector<PlaneDev> planes(d->n_planes);
+    p->max_samples = 0;
+    for (int k = 0; k < d->n_planes; ++k) {
+        const tfd_plane &src = d->planes[k];
+        const PlaneLayout &q = L.planes[k];
+        PlaneDev &pd = planes[k];
+        std::memset(&pd, 0, sizeof(pd));
+        pd.points = src.points;
+        pd.frequencies = src.frequencies;
+        pd.components = src.components;
+        pd.corners = src.corners;
+        pd.ne = 0;
+        for (int c = 0; c < src.components; ++c) {
+            pd.comp[c] = src.component_ids[c];
+            pd.ne += src.component_ids[c] < 3;
+        }
+        const size_t entries = (size_t)src.components * src.corners * src.points;
+        std::vector<long long> cells(entries);
+        std::vector<T> weights(entries);
+        for (size_t e = 0; e < entries; ++e) {
+            const long long cell = src.corner_cells[e];
+            const long long x = cell / ((long long)d->ny * d->nz), y = (cell / d->nz) % d->ny, z = cell % d->nz;
+            cells[e] = (z * d->ny + y) * L.pitch + x;
+            weights[e] = (T)src.corner_weights[e];
+        }
+        std::vector<double> omega(src.frequencies), half(2 * (size_t)src.frequencies);
+        for (int f = 0; f < src.frequencies; ++f) {
+            omega[f] = (2.0 * M_PI * src.frequency_hz[f]) * d->time_step;
+            const double ang = (M_PI * src.frequency_hz[f]) * d->time_step;
+            half[2 * f] = std::cos(ang);
+            half[2 * f + 1] = std::sin(ang);
+        }
+        std::vector<T> window(2 * (size_t)std::max(1, d->steps), T(0));
+        for (int q2 = 0; q2 < d->steps; ++q2) {
+            window[q2] = (T)src.window_e[q2];
+            window[d->steps + q2] = (T)src.window_h[q2];
+        }
+        if ((rc = upload(s, p, q.cell, cells)) || (rc = upload(s, p, q.weight, weights)) || (rc = upload(s, p, q.omega, omega)) ||
+            (rc = upload(s, p, q.half, half)) || (rc = upload(s, p, q.window, window)))
+            return rc;
+        pd.cell = p->ptr<long long>(q.cell);
+        pd.weight = p->ptr<T>(q.weight);
+        pd.omega = p->ptr<double>(q.omega);
+        pd.half = p->ptr<double>(q.half);
+        pd.window = p->ptr<T>(q.window);
+        pd.acc = p->ptr<double>(q.acc);
+        p->max_samples = std::max(p->max_samples, src.points * src.components);
+    }
+    if ((rc = upload(s, p, L.plane_tab, planes))) return rc;
+    // zero the state; the material starts as vacuum (inverse permittivity 1)
+    return TFD_OK;
+}
+
+template <typename T>
+int zero_state(tfd_plan *p, cudaStream_t s) {
+    const Layout &L = p->L;
+    const size_t comp_bytes = (size_t)L.count * L.elem;
+    for (int c = 0; c < 3; ++c) {
+        if (L.E[c]) TFD_CUDA(cudaMemsetAsync(p->arena + L.E[c], 0, 2 * comp_bytes, s));
+        if (L.H[c]) TFD_CUDA(cudaMemsetAsync(p->arena + L.H[c], 0, 2 * comp_bytes, s));
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 2; ++j) {
+            if (L.psiE[a][j]) TFD_CUDA(cudaMemsetAsync(p->arena + L.psiE[a][j], 0, 2 * (size_t)((L.psi_len[0][a] + 63) / 64 * 64) * L.elem, s));
+            if (L.psiH[a][j]) TFD_CUDA(cudaMemsetAsync(p->arena + L.psiH[a][j], 0, (size_t)L.psi_len[1][a] * L.elem, s));
+        }
+    TFD_CUDA(cudaMemsetAsync(p->arena + L.trace_out, 0, (size_t)std::max(1, p->desc.n_traces) * std::max(1, p->desc.steps) * L.elem, s));
+    for (size_t k = 0; k < L.planes.size(); ++k) {
+        const size_t acc = (size_t)p->planes_f[k] * p->planes_p[k] * p->planes_c[k] * 2 * sizeof(double);
+        if (acc) TFD_CUDA(cudaMemsetAsync(p->arena + L.planes[k].acc, 0, acc, s));
+    }
+    TFD_CUDA(cudaMemsetAsync(p->arena + L.counter, 0, sizeof(long long), s));
+    TFD_CUDA(cudaMemsetAsync(p->arena + L.done, 0, sizeof(unsigned), s));
+    TFD_CUDA(cudaMemsetAsync(p->arena + L.status, 0, sizeof(int), s));
+    return TFD_OK;
+}
+
+}  // namespace
+
+// ---- C ABI ---------------------------------------------------------------------------------------
+namespace {
+
+cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
+
+template <typename T>
+FieldSet<T> field_set(tfd_plan *p) {
+    FieldSet<T> fs;
+    Grid<T> &g = p->grid<T>();
+    for (int par = 0; par < 2; ++par)
+        for (int c = 0; c < 3; ++c) {
+            fs.f[par][c] = g.E[par][c];
+            fs.f[par][3 + c] = g.H[par][c];
+        }
+    return fs;
+}
+
+template <typename T>
+PsiArgs<T> psi_args(tfd_plan *p) {
+    PsiArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    Grid<T> &g = p->grid<T>();
+    a.n_seg = (int)p->psi_segs.size();
+    for (int k = 0; k < a.n_seg; ++k) a.seg[k] = p->psi_segs[k];
+    for (int q = 0; q < 3; ++q) a.n[q] = g.n[q];
+    a.pitch = g.pitch;
+    for (int f = 0; f < 2; ++f)
+        for (int q = 0; q < 3; ++q) {
+            a.row[f][q] = g.row[f][q];
+            a.rows[f][q] = g.rows[f][q];
+        }
+    std::memcpy(a.psiE, g.psiE, sizeof(a.psiE));
+    std::memcpy(a.psiH, g.psiH, sizeof(a.psiH));
+    a.counter = g.counter;
+    return a;
+}
+
+// Copy `bytes` between a caller buffer (host or device) and the plan's stage buffer.
+int stage_in(tfd_plan *p, const void *src, size_t bytes, int where, cudaStream_t s, const void **dev) {
+    if (where == TFD_DEVICE) { *dev = src; return TFD_OK; }
+    if (where != TFD_HOST) return fail(TFD_ERR_INVALID, "where must be TFD_DEVICE or TFD_HOST");
+    if (bytes > p->L.stage_bytes) return fail(TFD_ERR_INVALID, "transfer larger than the stage buffer");
+    TFD_CUDA(cudaMemcpyAsync(p->arena + p->L.stage, src, bytes, cudaMemcpyHostToDevice, s));
+    *dev = p->arena + p->L.stage;
+    return TFD_OK;
+}
+
+template <typename T>
+int set_material_t(tfd_plan *p, const void *src, int where, cudaStream_t s) {
+    const tfd_desc &d = p->desc;
+    const int S = d.material_samples;
+    const size_t bytes = (size_t)d.nx * d.ny * d.nz * S * sizeof(T);
+    const void *dev;
+    int rc = stage_in(p, src, bytes, where, s, &dev);
+    if (rc) return rc;
+    Grid<T> &g = p->grid<T>();
+    k_reference_to_internal<T><<<launch_blocks((long long)d.nx * d.ny * d.nz * S), 256, 0, s>>>(
+        (const T *)dev, S, d.nx, d.ny, d.nz, g.pitch, (T *)g.inv_eps[0], (T *)(S == 3 ? g.inv_eps[1] : nullptr),
+        (T *)(S == 3 ? g.inv_eps[2] : nullptr));
+    TFD_CUDA(cudaGetLastError());
+    if (where == TFD_HOST) TFD_CUDA(cudaStreamSynchronize(s));
+    return TFD_OK;
+}
+
+template <typename T>
+int set_fields_t(tfd_plan *p, const void *E, const void *H, int where, cudaStream_t s) {
+    const tfd_desc &d = p->desc;
+    const long long total = (long long)d.nx * d.ny * d.nz * 3;
+    const size_t bytes = total * sizeof(T);
+    const FieldSet<T> fs = field_set<T>(p);
+    for (int fam = 0; fam < 2; ++fam) {
+        const void *src = fam == 0 ? E : H;
+        if (!src) continue;
+        const void *dev;
+        int rc = stage_in(p, src, bytes, where, s, &dev);
+        if (rc) return rc;
+        k_reference_to_fields<T><<<launch_blocks(total), 256, 0, s>>>(fam == 0 ? (const T *)dev : nullptr,
+                                                                       fam == 1 ? (const T *)dev : nullptr, d.nx, d.ny, d.nz,
+                                                                       p->L.pitch, fs, p->grid<T>().counter);
+        TFD_CUDA(cudaGetLastError());
+        if (where == TFD_HOST) TFD_CUDA(cudaStreamSynchronize(s));
+    }
+    return TFD_OK;
+}
+
+template <typename T>
+int get_fields_t(tfd_plan *p, void *E, void *H, int where, cudaStream_t s) {
+    const tfd_desc &d = p->desc;
+    const long long total = (long long)d.nx * d.ny * d.nz * 3;
+    const size_t bytes = total * sizeof(T);
+    const FieldSet<T> fs = field_set<T>(p);
+    for (int fam = 0; fam < 2; ++fam) {
+        void *dst = fam == 0 ? E : H;
+        if (!dst) continue;
+        void *dev = where == TFD_DEVICE ? dst : p->arena + p->L.stage;
+        if (where == TFD_HOST && bytes > p->L.stage_bytes) return fail(TFD_ERR_INVALID, "transfer larger than the stage buffer");
+        k_fields_to_reference<T><<<launch_blocks(total), 256, 0, s>>>(fam == 0 ? (T *)dev : nullptr, fam == 1 ? (T *)dev : nullptr,
+                                                                       d.nx, d.ny, d.nz, p->L.pitch, fs, p->grid<T>().counter);
+        TFD_CUDA(cudaGetLastError());
+        if (where == TFD_HOST) {
+            TFD_CUDA(cudaMemcpyAsync(dst, dev, bytes, cudaMemcpyDeviceToHost, s));
+            TFD_CUDA(cudaStreamSynchronize(s));
+        }
+    }
+    return TFD_OK;
+}
+
+template <typename T>
+int psi_t(tfd_plan *p, void *vec, int where, cudaStream_t s, bool to_reference) {
+    const size_t bytes = p->L.psi_total * sizeof(T);
+    if (p->psi_segs.empty()) return TFD_OK;
+    void *dev = vec;
+    if (where == TFD_HOST) {
+        dev = p->arena + p->L.stage;
+        if (!to_reference) TFD_CUDA(cudaMemcpyAsync(dev, vec, bytes, cudaMemcpyHostToDevice, s));
+    }
+    const PsiArgs<T> a = psi_args<T>(p);
+    long long largest = 0;
+    for (auto &sg : p->psi_segs) {
+        long long ext[3] = {p->desc.nx, p->desc.ny, p->desc.nz};
+        ext[sg.a] = sg.hi - sg.lo;
+        largest = std::max(largest, ext[0] * ext[1] * ext[2]);
+    }
+    dim3 grid(launch_blocks(largest), (unsigned)p->psi_segs.size());
+    k_psi_copy<T><<<grid, 256, 0, s>>>((T *)dev, a, to_reference ? 1 : 0);
+    TFD_CUDA(cudaGetLastError());
+    if (where == TFD_HOST) {
+        if (to_reference) TFD_CUDA(cudaMemcpyAsync(vec, dev, bytes, cudaMemcpyDeviceToHost, s));
+        TFD_CUDA(cudaStreamSynchronize(s));
+    }
+    return TFD_OK;
+}
+
+template <typename T>
+MonitorArgs<T> monitor_args(tfd_plan *p) {
+    MonitorArgs<T> m;
+    std::memset(&m, 0, sizeof(m));
+    Grid<T> &g = p->grid<T>();
+    for (int c = 0; c < 3; ++c) {
+        m.field[c] = g.E[0][c];
+        m.field[3 + c] = g.H[0][c];
+    }
+    m.count = g.count;
+    m.steps = g.steps;
+    m.counter = g.counter;
+    m.done = p->ptr<unsigned>(p->L.done);
+    m.n_traces = p->desc.n_traces;
+    m.traces = p->ptr<TraceDev>(p->L.trace_tab);
+    m.trace_out = p->ptr<T>(p->L.trace_out);
+    m.n_planes = p->desc.n_planes;
+    m.planes = p->ptr<PlaneDev>(p->L.plane_tab);
+    m.max_samples = p->max_samples;
+    return m;
+}
+
+template <typename T>
+int launch_step_gather(tfd_plan *p, cudaStream_t s) {
+    const Grid<T> &g = p->grid<T>();
+    dim3 block(128), grid((unsigned)((long long)g.n[1] * g.n[2]), (unsigned)((g.n[0] + 127) / 128));
+    // rows on x (up to 2^31-1), x chunks on y
+    switch (g.active) {
+        case kMaskTM: k_step_gather_rows<T, kMaskTM><<<grid, block, 0, s>>>(g); break;
+        case kMaskTE: k_step_gather_rows<T, kMaskTE><<<grid, block, 0, s>>>(g); break;
+        default: k_step_gather_rows<T, kMaskAll><<<grid, block, 0, s>>>(g); break;
+    }
+    return TFD_OK;
+}
+
+template <typename T>
+int step_t(tfd_plan *p, int nsteps, cudaStream_t s) {
+    const MonitorArgs<T> m = monitor_args<T>(p);
+    dim3 mgrid((unsigned)std::max(1, (p->max_samples + kMonitorThreads - 1) / kMonitorThreads), (unsigned)std::max(1, p->desc.n_planes));
+    for (int k = 0; k < nsteps; ++k) {
+        int rc = launch_step_gather<T>(p, s);
+        if (rc) return rc;
+        k_monitor<T><<<mgrid, kMonitorThreads, 0, s>>>(m);
+    }
+    TFD_CUDA(cudaGetLastError());
+    return TFD_OK;
+}
+
+template <typename T>
+int diagnose_t(tfd_plan *p, double out[3], cudaStream_t s) {
+    long long counter = 0;
+    TFD_CUDA(cudaMemcpyAsync(&counter, p->arena + p->L.counter, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    TFD_CUDA(cudaStreamSynchronize(s));
+    const int par = (int)(counter & 1);
+    Grid<T> &g = p->grid<T>();
+    DiagArgs<T> d;
+    std::memset(&d, 0, sizeof(d));
+    d.fs = field_set<T>(p);
+    for (int c = 0; c < 3; ++c) d.inv_eps[c] = g.inv_eps[c];
+    d.nx = g.n[0];
+    d.ny = g.n[1];
+    d.nz = g.n[2];
+    d.pitch = g.pitch;
+    d.counter = g.counter;
+    const Layout &L = p->L;
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 2; ++j) {
+            if (g.psiE[par][a][j]) { d.psi[d.n_psi] = g.psiE[par][a][j]; d.psi_len[d.n_psi++] = L.psi_len[0][a]; }
+            if (g.psiH[a][j]) { d.psi[d.n_psi] = g.psiH[a][j]; d.psi_len[d.n_psi++] = L.psi_len[1][a]; }
+        }
+    d.partial = p->ptr<double>(L.diag);
+    k_diag<T><<<kDiagBlocks, kDiagThreads, 0, s>>>(d);
+    TFD_CUDA(cudaGetLastError());
+    std::vector<double> part((size_t)kDiagBlocks * 4);
+    TFD_CUDA(cudaMemcpyAsync(part.data(), d.partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    TFD_CUDA(cudaStreamSynchronize(s));
+    double energy = 0, peak = 0, finite = 1, nan_seen = 0;
+    for (int b = 0; b < kDiagBlocks; ++b) {
+        energy += part[4 * b];
+        peak = std::max(peak, part[4 * b + 1]);
+        finite = std::min(finite, part[4 * b + 2]);
+        nan_seen = std::max(nan_seen, part[4 * b + 3]);
+    }
+    out[0] = energy;
+    out[1] = nan_seen > 0 ? NAN : peak;
+    out[2] = finite;
+    return TFD_OK;
+}
+
+template <typename T>
+int slice_t(tfd_plan *p, int comp, int axis, int index, void *dst, int where, cudaStream_t s) {
+    const tfd_desc &d = p->desc;
+    const int n[3] = {d.nx, d.ny, d.nz};
+    if (comp < 0 || comp > 5 || axis < 0 || axis > 2 || index < 0 || index >= n[axis]) return fail(TFD_ERR_INVALID, "bad slice");
+    const int ua = axis == 0 ? 1 : 0, va = axis == 2 ? 1 : 2;
+    const long long total = (long long)n[ua] * n[va];
+    void *dev = where == TFD_DEVICE ? dst : p->arena + p->L.stage;
+    k_slice<T><<<launch_blocks(total), 256, 0, s>>>((T *)dev, field_set<T>(p), comp, axis, index, d.nx, d.ny, d.nz, p->L.pitch,
+                                                    p->grid<T>().counter);
+    TFD_CUDA(cudaGetLastError());
+    if (where == TFD_HOST) {
+        TFD_CUDA(cudaMemcpyAsync(dst, dev, total * sizeof(T), cudaMemcpyDeviceToHost, s));
+        TFD_CUDA(cudaStreamSynchronize(s));
+    }
+    return TFD_OK;
+}
+
+template <typename T>
+int reset_t(tfd_plan *p, cudaStream_t s) { return zero_state<T>(p, s); }
+
+#define TFD_DISPATCH(p, fn, ...) ((p)->desc.precision == 8 ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
+
+}  // namespace
+
+extern "C" {
+
+const char *tfd_error_string(int code) {
+    switch (code) {
+        case TFD_OK: return "ok";
+        case TFD_ERR_INVALID: return "invalid argument";
+        case TFD_ERR_UNSUPPORTED: return "unsupported feature";
+        case TFD_ERR_CUDA: return "CUDA error";
+        case TFD_ERR_ARENA: return "arena too small or misaligned";
+        case TFD_ERR_DEVICE: return "device status error";
+        default: return "unknown error";
+    }
+}
+
+const char *tfd_last_error(void) { return g_error.c_str(); }
+
+int tfd_plan_bytes(const tfd_desc *desc, size_t *bytes) {
+    int rc = validate(desc);
+    if (rc) return rc;
+    if (!bytes) return fail(TFD_ERR_INVALID, "bytes is null");
+    Layout L;
+    compute_layout(desc, L);
+    *bytes = L.total;
+    return TFD_OK;
+}
+
+int tfd_plan_create(const tfd_desc *desc, void *arena, size_t arena_bytes, void *stream, tfd_plan **out) {
+    int rc = validate(desc);
+    if (rc) return rc;
+    if (!out) return fail(TFD_ERR_INVALID, "plan output is null");
+    *out = nullptr;
+    tfd_plan *p = new tfd_plan();
+    p->desc = *desc;
+    p->desc.segments = nullptr;
+    p->desc.sources = nullptr;
+    p->desc.traces = nullptr;
+    p->desc.planes = nullptr;
+    compute_layout(desc, p->L);
+    if (!arena || ((uintptr_t)arena & 255) || arena_bytes < p->L.total) {
+        delete p;
+        return fail(TFD_ERR_ARENA, "arena must be 256-byte aligned and at least tfd_plan_bytes() long");
+    }
+    p->arena = (char *)arena;
+    size_t total;
+    p->psi_segs = psi_segments(desc, &total);
+    for (int k = 0; k < desc->n_planes; ++k) {
+        p->planes_f.push_back(desc->planes[k].frequencies);
+        p->planes_p.push_back(desc->planes[k].points);
+        p->planes_c.push_back(desc->planes[k].components);
+    }
+    p->kernel = TFD_KERNEL_GATHER;
+    cudaStream_t s = as_stream(stream);
+    rc = desc->precision == 8 ? create_typed<double>(p, desc, s) : create_typed<float>(p, desc, s);
+    if (!rc) rc = TFD_DISPATCH(p, zero_state, p, s);
+    if (!rc) {
+        const long long n = p->L.count;
+        for (int q = 0; q < desc->material_samples; ++q) {
+            if (desc->precision == 8) k_fill<double><<<launch_blocks(n), 256, 0, s>>>((double *)(p->arena + p->L.inv[q]), n, 1.0);
+            else k_fill<float><<<launch_blocks(n), 256, 0, s>>>((float *)(p->arena + p->L.inv[q]), n, 1.0f);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) rc = fail(TFD_ERR_CUDA, std::string("plan setup: ") + cudaGetErrorString(e));
+    }
+    if (rc) {
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return TFD_OK;
+}
+
+void tfd_plan_destroy(tfd_plan *plan) { delete plan; }
+
+int tfd_set_material(tfd_plan *p, const void *inv_eps, int where, void *stream) {
+    if (!p || !inv_eps) return fail(TFD_ERR_INVALID, "null argument");
+    return TFD_DISPATCH(p, set_material_t, p, inv_eps, where, as_stream(stream));
+}
+
+int tfd_set_fields(tfd_plan *p, const void *E, const void *H, int where, void *stream) {
+    if (!p) return fail(TFD_ERR_INVALID, "null plan");
+    return TFD_DISPATCH(p, set_fields_t, p, E, H, where, as_stream(stream));
+}
+
+int tfd_get_fields(tfd_plan *p, void *E, void *H, int where, void *stream) {
+    if (!p) return fail(TFD_ERR_INVALID, "null plan");
+    return TFD_DISPATCH(p, get_fields_t, p, E, H, where, as_stream(stream));
+}
+
+int tfd_psi_count(const tfd_plan *p, size_t *count) {
+    if (!p || !count) return fail(TFD_ERR_INVALID, "null argument");
+    *count = p->L.psi_total;
+    return TFD_OK;
+}
+
+int tfd_set_psi(tfd_plan *p, const void *psi, int where, void *stream) {
+    if (!p || !psi) return fail(TFD_ERR_INVALID, "null argument");
+    return TFD_DISPATCH(p, psi_t, p, (void *)psi, where, as_stream(stream), false);
+}
+
+int tfd_get_psi(tfd_plan *p, void *psi, int where, void *stream) {
+    if (!p || !psi) return fail(TFD_ERR_INVALID, "null argument");
+    return TFD_DISPATCH(p, psi_t, p, psi, where, as_stream(stream), true);
+}
+
+int tfd_step(tfd_plan *p, int32_t nsteps, void *stream) {
+    if (!p) return fail(TFD_ERR_INVALID, "null plan");
+    if (nsteps < 0) return fail(TFD_ERR_INVALID, "nsteps must be non-negative");
+    return TFD_DISPATCH(p, step_t, p, nsteps, as_stream(stream));
+}
+
+int tfd_reset(tfd_plan *p, void *stream) {
+    if (!p) return fail(TFD_ERR_INVALID, "null plan");
+    return TFD_DISPATCH(p, reset_t, p, as_stream(stream));
+}
+
+int tfd_get_traces(tfd_plan *p, void *dst, int where, void *stream) {
+    if (!p || !dst) return fail(TFD_ERR_INVALID, "null argument");
+    const size_t bytes = (size_t)p->desc.n_traces * p->desc.steps * p->L.elem;
+    if (!bytes) return TFD_OK;
+    cudaStream_t s = as_stream(stream);
+    TFD_CUDA(cudaMemcpyAsync(dst, p->arena + p->L.trace_out, bytes, where == TFD_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+    if (where == TFD_HOST) TFD_CUDA(cudaStreamSynchronize(s));
+    return TFD_OK;
+}
+
+int tfd_get_plane(tfd_plan *p, int32_t k, void *dst, int where, void *stream) {
+    if (!p || !dst || k < 0 || k >= p->desc.n_planes) return fail(TFD_ERR_INVALID, "bad plane request");
+    const size_t bytes = (size_t)p->planes_f[k] * p->planes_p[k] * p->planes_c[k] * 2 * sizeof(double);
+    if (!bytes) return TFD_OK;
+    cudaStream_t s = as_stream(stream);
+    TFD_CUDA(cudaMemcpyAsync(dst, p->arena + p->L.planes[k].acc, bytes, where == TFD_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
+    if (where == TFD_HOST) TFD_CUDA(cudaStreamSynchronize(s));
+    return TFD_OK;
+}
+
+int tfd_get_slice(tfd_plan *p, int32_t component, int32_t axis, int32_t index, void *dst, int where, void *stream) {
+    if (!p || !dst) return fail(TFD_ERR_INVALID, "null argument");
+    return TFD_DISPATCH(p, slice_t, p, component, axis, index, dst, where, as_stream(stream));
+}
+
+int tfd_diagnose(tfd_plan *p, double out[3], void *stream) {
+    if (!p || !out) return fail(TFD_ERR_INVALID, "null argument");
+    return TFD_DISPATCH(p, diagnose_t, p, out, as_stream(stream));
+}
+
+int tfd_counter(tfd_plan *p, int64_t *value, void *stream) {
+    if (!p || !value) return fail(TFD_ERR_INVALID, "null argument");
+    cudaStream_t s = as_stream(stream);
+    long long v = 0;
+    TFD_CUDA(cudaMemcpyAsync(&v, p->arena + p->L.counter, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    TFD_CUDA(cudaStreamSynchronize(s));
+    *value = v;
+    return TFD_OK;
+}
+
+int tfd_device_status(tfd_plan *p, int32_t *status, void *stream) {
+    if (!p || !status) return fail(TFD_ERR_INVALID, "null argument");
+    cudaStream_t s = as_stream(stream);
+    int v = 0;
+    TFD_CUDA(cudaMemcpyAsync(&v, p->arena + p->L.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TFD_CUDA(cudaStreamSynchronize(s));
+    *status = v;
+    return TFD_OK;
+}
+
+int tfd_kernel_in_use(const tfd_plan *p, int32_t *kernel) {
+    if (!p || !kernel) return fail(TFD_ERR_INVALID, "null argument");
+    *kernel = p->kernel;
+    return TFD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,138 @@
+// Fused E+H step, gather form: one thread per cell.
+//
+// Thread (x, y, z) computes E_new at its own cell (writing E and the E-family CPML
+// memory), then H_new at its own cell. The H update's forward differences need
+// E_new at (x+1), (y+1), (z+1); the thread recomputes those values from the old
+// buffers with the same arithmetic their owners use (bitwise identical, including
+// CPML and soft sources) instead of waiting for them, so a single launch advances a
+// whole step with no grid-wide synchronisation. Every arithmetic step follows the
+// reference operation order (torchfdtd/boundaries.py:363-438, torchfdtd/cuda_kernels.py:
+// 186-259,327-347): d = F[i] - F[i-1]; psi = psi*b + c*d; d = d*(1/kappa) + psi;
+// curl = (0 + s0*d0) + s1*d1; E += (cn*inv_eps)*curl; H -= cn*curl; soft sources are
+// added after the family update. The library is compiled with --fmad=false so no
+// multiply-add is contracted, as in the reference's NVRTC build.
+//
+// This kernel is the parity baseline and the fallback for shapes the marching
+// kernel does not tile; its extra work is three recomputed E components per H
+// component, served from L1/L2.
+#pragma once
+#include "internal.cuh"
+
+namespace tfd {
+
+template <typename T>
+__device__ __forceinline__ T inject(const Grid<T> &g, int family, int comp, long long n, int x, int y, int z, T v) {
+    if (n < g.steps) {
+        for (int s = 0; s < g.n_src; ++s) {
+            const SourceTerm &t = g.src[s];
+            if (t.family == family && t.comp == comp && x >= t.lo[0] && x < t.hi[0] && y >= t.lo[1] && y < t.hi[1] &&
+                z >= t.lo[2] && z < t.hi[2])
+                v = v + g.src_values[(long long)s * g.steps + n];
+        }
+    }
+    return v;
+}
+
+// One backward-difference curl term of E component C (k-th of its two terms).
+template <typename T, int C, int K>
+__device__ __forceinline__ void e_term(const Grid<T> &g, int par, int x, int y, int z, long long i, bool own, T &acc) {
+    constexpr Term t = term_of(C, K);
+    const int a = t.axis;
+    if (g.n[a] == 1) return;
+    const int coord = a == 0 ? x : (a == 1 ? y : z);
+    const T *h = g.H[par][t.in];
+    T d = T(0);
+    if (coord > 0) {
+        d = h[i] - h[i - g.stride(a)];
+        const int *rm = g.row[0][a];
+        if (rm != nullptr) {
+            const int r = rm[coord];
+            if (r >= 0) {
+                const long long p = g.psi_index(a, x, y, z, r, g.rows[0][a]);
+                const T mem = g.psiE[par][a][t.j][p] * g.cb[0][a][coord] + g.cc[0][a][coord] * d;
+                if (own) g.psiE[par ^ 1][a][t.j][p] = mem;
+                d = d * g.ck[0][a][coord] + mem;
+            }
+        }
+    } else if (g.periodic[a]) {
+        d = h[i] - h[i + (long long)(g.n[a] - 1) * g.stride(a)];
+    }
+    acc = acc + (t.sign > 0 ? d : -d);
+}
+
+template <typename T, int C>
+__device__ __forceinline__ T e_value(const Grid<T> &g, int par, long long n, int x, int y, int z, long long i, bool own) {
+    T acc = T(0);
+    e_term<T, C, 0>(g, par, x, y, z, i, own, acc);
+    e_term<T, C, 1>(g, par, x, y, z, i, own, acc);
+    const T e = g.E[par][C][i] + (g.cn * g.inv_eps[C][i]) * acc;
+    return inject(g, 0, C, n, x, y, z, e);
+}
+
+template <typename T, int IN>
+__device__ __forceinline__ T e_neighbour(const Grid<T> &g, int par, long long n, int a, int x, int y, int z, long long i, int coord_to) {
+    // E_new of component IN at the cell whose axis-a coordinate is coord_to (not owned).
+    long long j = i + (long long)(coord_to - (a == 0 ? x : a == 1 ? y : z)) * g.stride(a);
+    int xx = a == 0 ? coord_to : x, yy = a == 1 ? coord_to : y, zz = a == 2 ? coord_to : z;
+    return e_value<T, IN>(g, par, n, xx, yy, zz, j, false);
+}
+
+template <typename T, int C, int K>
+__device__ __forceinline__ void h_term(const Grid<T> &g, int par, long long n, int x, int y, int z, long long i, const T *e_own,
+                                       T &acc) {
+    constexpr Term t = term_of(C, K);
+    const int a = t.axis;
+    if (g.n[a] == 1) return;
+    const int coord = a == 0 ? x : (a == 1 ? y : z);
+    T d = T(0);
+    if (coord < g.n[a] - 1) {
+        d = e_neighbour<T, t.in>(g, par, n, a, x, y, z, i, coord + 1) - e_own[t.in];
+        const int *rm = g.row[1][a];
+        if (rm != nullptr) {
+            const int r = rm[coord];
+            if (r >= 0) {
+                const long long p = g.psi_index(a, x, y, z, r, g.rows[1][a]);
+                T *psi = g.psiH[a][t.j];
+                const T mem = psi[p] * g.cb[1][a][coord] + g.cc[1][a][coord] * d;
+                psi[p] = mem;
+                d = d * g.ck[1][a][coord] + mem;
+            }
+        }
+    } else if (g.periodic[a]) {
+        d = e_neighbour<T, t.in>(g, par, n, a, x, y, z, i, 0) - e_own[t.in];
+    } else if (g.pec_on[a]) {
+        d = g.pec_neg[a] * e_own[t.in];
+    }
+    acc = acc + (t.sign > 0 ? d : -d);
+}
+
+template <typename T, int C>
+__device__ __forceinline__ T h_value(const Grid<T> &g, int par, long long n, int x, int y, int z, long long i, const T *e_own) {
+    T acc = T(0);
+    h_term<T, C, 0>(g, par, n, x, y, z, i, e_own, acc);
+    h_term<T, C, 1>(g, par, n, x, y, z, i, e_own, acc);
+    const T h = g.H[par][C][i] - g.cn * acc;
+    return inject(g, 1, C, n, x, y, z, h);
+}
+
+// ACTIVE: bitmask of advanced components (bit c: E_c, bit 3+c: H_c).
+// Launch: blockIdx.x = row (z*ny + y), blockIdx.y = 128-cell chunk of the row.
+template <typename T, int ACTIVE>
+__global__ void __launch_bounds__(128) k_step_gather_rows(const __grid_constant__ Grid<T> g) {
+    const long long n = *g.counter;
+    const int par = (int)(n & 1);
+    const int x = blockIdx.y * blockDim.x + threadIdx.x;
+    const int y = blockIdx.x % g.n[1];
+    const int z = blockIdx.x / g.n[1];
+    if (x >= g.n[0]) return;
+    const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
+    T e[3] = {T(0), T(0), T(0)};
+    if (ACTIVE & 1) { e[0] = e_value<T, 0>(g, par, n, x, y, z, i, true); g.E[par ^ 1][0][i] = e[0]; }
+    if (ACTIVE & 2) { e[1] = e_value<T, 1>(g, par, n, x, y, z, i, true); g.E[par ^ 1][1][i] = e[1]; }
+    if (ACTIVE & 4) { e[2] = e_value<T, 2>(g, par, n, x, y, z, i, true); g.E[par ^ 1][2][i] = e[2]; }
+    if (ACTIVE & 8) g.H[par ^ 1][0][i] = h_value<T, 0>(g, par, n, x, y, z, i, e);
+    if (ACTIVE & 16) g.H[par ^ 1][1][i] = h_value<T, 1>(g, par, n, x, y, z, i, e);
+    if (ACTIVE & 32) g.H[par ^ 1][2][i] = h_value<T, 2>(g, par, n, x, y, z, i, e);
+}
+
+}  // namespace tfd

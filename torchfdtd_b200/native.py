@@ -1,0 +1,302 @@
+"""ctypes binding of the C ABI in include/tfdtd.h (libtfdtd.so, built in-tree).
+
+``NativeGrid`` turns a host ``GridPlan`` into a device plan: it fills ``tfd_desc``,
+lets PyTorch allocate the one device arena the library lays out (the reference
+also keeps every array in torch, ``torchfdtd/cuda_kernels.py:120-128``) and wraps
+the entry points. There is no CPU path: without the library or a GPU every entry
+point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIBRARY = HERE / 'libtfdtd.so'
+
+TFD_ABI_VERSION = 1
+TFD_DEVICE, TFD_HOST = 0, 1
+KERNELS = {'auto': 0, 'march': 1, 'gather': 2}
+FACE = {'pml': 0, 'periodic': 1, 'pec': 2, 'antisymmetric': 2}
+MASK = {'3d': 0x3F, 'both': 0x3F, 'TM': 0x04 | 0x08 | 0x10, 'TE': 0x01 | 0x02 | 0x20}
+
+c_i32, c_i64, c_dbl, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+P_dbl = ctypes.POINTER(ctypes.c_double)
+P_i32 = ctypes.POINTER(ctypes.c_int32)
+P_i64 = ctypes.POINTER(ctypes.c_int64)
+
+
+class CpmlSegment(ctypes.Structure):
+    _fields_ = [('forward', c_i32), ('axis', c_i32), ('lo', c_i32), ('hi', c_i32),
+                ('b', P_dbl), ('c', P_dbl), ('inv_kappa', P_dbl)]
+
+
+class SourceTermC(ctypes.Structure):
+    _fields_ = [('family', c_i32), ('component', c_i32), ('lo', c_i32 * 3), ('hi', c_i32 * 3), ('values', P_dbl)]
+
+
+class TraceC(ctypes.Structure):
+    _fields_ = [('family', c_i32), ('component', c_i32), ('index', c_i32 * 3)]
+
+
+class PlaneC(ctypes.Structure):
+    _fields_ = [('points', c_i32), ('frequencies', c_i32), ('components', c_i32), ('corners', c_i32),
+                ('component_ids', P_i32), ('corner_cells', P_i64), ('corner_weights', P_dbl),
+                ('frequency_hz', P_dbl), ('window_e', P_dbl), ('window_h', P_dbl)]
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [('abi_version', c_i32), ('nx', c_i32), ('ny', c_i32), ('nz', c_i32), ('precision', c_i32),
+                ('material_samples', c_i32), ('components', c_i32), ('steps', c_i32), ('kernel', c_i32),
+                ('face', (c_i32 * 2) * 3), ('courant', c_dbl), ('time_step', c_dbl), ('pec_upper', c_dbl * 3),
+                ('n_segments', c_i32), ('segments', ctypes.POINTER(CpmlSegment)),
+                ('n_sources', c_i32), ('sources', ctypes.POINTER(SourceTermC)),
+                ('n_traces', c_i32), ('traces', ctypes.POINTER(TraceC)),
+                ('n_planes', c_i32), ('planes', ctypes.POINTER(PlaneC))]
+
+
+# Every entry point of include/tfdtd.h with its ctypes signature.
+SIGNATURES = {
+    'tfd_plan_bytes': (ctypes.c_int, [ctypes.POINTER(Desc), ctypes.POINTER(ctypes.c_size_t)]),
+    'tfd_plan_create': (ctypes.c_int, [ctypes.POINTER(Desc), c_vp, ctypes.c_size_t, c_vp, ctypes.POINTER(c_vp)]),
+    'tfd_plan_destroy': (None, [c_vp]),
+    'tfd_set_material': (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, c_vp]),
+    'tfd_set_fields': (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int, c_vp]),
+    'tfd_get_fields': (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int, c_vp]),
+    'tfd_psi_count': (ctypes.c_int, [c_vp, ctypes.POINTER(ctypes.c_size_t)]),
+    'tfd_set_psi': (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, c_vp]),
+    'tfd_get_psi': (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, c_vp]),
+    'tfd_step': (ctypes.c_int, [c_vp, c_i32, c_vp]),
+    'tfd_reset': (ctypes.c_int, [c_vp, c_vp]),
+    'tfd_get_traces': (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, c_vp]),
+    'tfd_get_plane': (ctypes.c_int, [c_vp, c_i32, c_vp, ctypes.c_int, c_vp]),
+    'tfd_get_slice': (ctypes.c_int, [c_vp, c_i32, c_i32, c_i32, c_vp, ctypes.c_int, c_vp]),
+    'tfd_diagnose': (ctypes.c_int, [c_vp, P_dbl, c_vp]),
+    'tfd_counter': (ctypes.c_int, [c_vp, P_i64, c_vp]),
+    'tfd_device_status': (ctypes.c_int, [c_vp, P_i32, c_vp]),
+    'tfd_kernel_in_use': (ctypes.c_int, [c_vp, P_i32]),
+    'tfd_error_string': (ctypes.c_char_p, [ctypes.c_int]),
+    'tfd_last_error': (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def library():
+    """Load libtfdtd.so once; raise when it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not LIBRARY.exists():
+            raise RuntimeError(f'{LIBRARY.name} is not built. Build it with `python __graft_entry__.py` (build()) or '
+                               '`make -C torchfdtd_b200/csrc`; the fused B200 engine has no CPU fallback.')
+        lib = ctypes.CDLL(str(LIBRARY))
+        for name, (restype, argtypes) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = lib
+    return _lib
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+def check(code):
+    if code != 0:
+        lib = library()
+        message = lib.tfd_last_error().decode()
+        kind = lib.tfd_error_string(code).decode()
+        if code in (1, 2):
+            raise ValueError(f'{kind}: {message}')
+        raise NativeError(f'{kind}: {message}')
+
+
+def _ptr(array, ctype):
+    return array.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def _stream(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return c_vp(s.cuda_stream)
+
+
+class NativeGrid:
+    """A device plan built from a ``GridPlan`` (owns the arena tensor and the native handle)."""
+
+    def __init__(self, plan, kernel='auto', device=None):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError('CUDA requested but unavailable: the fused B200 engine runs on a CUDA GPU only.')
+        lib = library()
+        self.plan = plan
+        self.device = torch.device('cuda', torch.cuda.current_device() if device is None else device)
+        self.dtype = plan.dtype
+        self.torch_dtype = torch.float64 if plan.dtype == np.float64 else torch.float32
+        self._keep = []
+        desc = Desc()
+        desc.abi_version = TFD_ABI_VERSION
+        desc.nx, desc.ny, desc.nz = plan.shape
+        desc.precision = 8 if plan.dtype == np.float64 else 4
+        desc.material_samples = plan.material_samples
+        desc.components = MASK['3d' if plan.dimension == '3d' else plan.polarization]
+        desc.steps = plan.steps
+        desc.kernel = KERNELS[kernel]
+        for a in range(3):
+            for s in range(2):
+                desc.face[a][s] = FACE[plan.faces[a][s]]
+            desc.pec_upper[a] = plan.pec_upper.get(a, 0.0)
+        desc.courant = plan.courant
+        desc.time_step = plan.time_step
+        segs = (CpmlSegment * max(1, len(plan.segments)))()
+        for k, s in enumerate(plan.segments):
+            arrays = [np.ascontiguousarray(v, dtype=np.float64) for v in (s.b, s.c, s.inv_kappa)]
+            self._keep.extend(arrays)
+            segs[k] = CpmlSegment(int(s.forward), s.axis, s.lo, s.hi, *(_ptr(v, ctypes.c_double) for v in arrays))
+        desc.n_segments, desc.segments = len(plan.segments), segs
+        srcs = (SourceTermC * max(1, len(plan.sources)))()
+        for k, t in enumerate(plan.sources):
+            v = np.ascontiguousarray(t.values, dtype=np.float64)
+            self._keep.append(v)
+            srcs[k] = SourceTermC(t.family, t.comp, (c_i32 * 3)(*t.lo), (c_i32 * 3)(*t.hi), _ptr(v, ctypes.c_double))
+        desc.n_sources, desc.sources = len(plan.sources), srcs
+        traces = (TraceC * max(1, len(plan.traces)))()
+        for k, t in enumerate(plan.traces):
+            traces[k] = TraceC(t.family, t.comp, (c_i32 * 3)(*t.index))
+        desc.n_traces, desc.traces = len(plan.traces), traces
+        planes = (PlaneC * max(1, len(plan.planes)))()
+        for k, p in enumerate(plan.planes):
+            ids = np.array([['Ex', 'Ey', 'Ez', 'Hx', 'Hy', 'Hz'].index(c) for c in p.components], dtype=np.int32)
+            cells = np.ascontiguousarray(p.corner_cells, dtype=np.int64)
+            weights = np.ascontiguousarray(p.corner_weights, dtype=np.float64)
+            freq = np.ascontiguousarray(p.frequency, dtype=np.float64)
+            we = np.ascontiguousarray(p.windows[0], dtype=np.float64)
+            wh = np.ascontiguousarray(p.windows[1], dtype=np.float64)
+            self._keep.extend([ids, cells, weights, freq, we, wh])
+            planes[k] = PlaneC(cells.shape[2], len(freq), len(ids), cells.shape[1], _ptr(ids, c_i32), _ptr(cells, c_i64),
+                               _ptr(weights, ctypes.c_double), _ptr(freq, ctypes.c_double), _ptr(we, ctypes.c_double),
+                               _ptr(wh, ctypes.c_double))
+        desc.n_planes, desc.planes = len(plan.planes), planes
+        self._keep.extend([segs, srcs, traces, planes])
+        self.desc = desc
+        size = ctypes.c_size_t()
+        check(lib.tfd_plan_bytes(ctypes.byref(desc), ctypes.byref(size)))
+        self.arena_bytes = size.value
+        with torch.cuda.device(self.device):
+            self.arena = torch.empty(self.arena_bytes, dtype=torch.uint8, device=self.device)
+            handle = c_vp()
+            check(lib.tfd_plan_create(ctypes.byref(desc), c_vp(self.arena.data_ptr()), size, _stream(), ctypes.byref(handle)))
+        self.handle = handle
+        kernel_used = c_i32()
+        check(lib.tfd_kernel_in_use(self.handle, ctypes.byref(kernel_used)))
+        self.kernel = {v: k for k, v in KERNELS.items()}[kernel_used.value]
+        self.set_material(plan.inv_eps)
+
+    def close(self):
+        if getattr(self, 'handle', None):
+            library().tfd_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+    # ---- state transfer (reference layout, host numpy arrays) --------------------------------
+    def set_material(self, inv_eps):
+        a = np.ascontiguousarray(inv_eps, dtype=self.dtype)
+        check(library().tfd_set_material(self.handle, c_vp(a.ctypes.data), TFD_HOST, _stream()))
+
+    def set_fields(self, E=None, H=None):
+        e = None if E is None else np.ascontiguousarray(E, dtype=self.dtype)
+        h = None if H is None else np.ascontiguousarray(H, dtype=self.dtype)
+        check(library().tfd_set_fields(self.handle, c_vp(e.ctypes.data) if e is not None else None,
+                                       c_vp(h.ctypes.data) if h is not None else None, TFD_HOST, _stream()))
+
+    def get_fields(self):
+        shape = (*self.plan.shape, 3)
+        E, H = np.empty(shape, self.dtype), np.empty(shape, self.dtype)
+        check(library().tfd_get_fields(self.handle, c_vp(E.ctypes.data), c_vp(H.ctypes.data), TFD_HOST, _stream()))
+        return E, H
+
+    def fields_device(self):
+        """E and H as torch tensors in the reference layout, on the device (no host copy)."""
+        import torch
+        shape = (*self.plan.shape, 3)
+        E = torch.empty(shape, dtype=self.torch_dtype, device=self.device)
+        H = torch.empty(shape, dtype=self.torch_dtype, device=self.device)
+        check(library().tfd_get_fields(self.handle, c_vp(E.data_ptr()), c_vp(H.data_ptr()), TFD_DEVICE, _stream()))
+        return E, H
+
+    def psi_count(self):
+        n = ctypes.c_size_t()
+        check(library().tfd_psi_count(self.handle, ctypes.byref(n)))
+        return n.value
+
+    def get_psi(self):
+        """Every CPML memory, as a list in the reference's memory_states order and shapes."""
+        flat = np.empty(self.psi_count(), self.dtype)
+        if flat.size:
+            check(library().tfd_get_psi(self.handle, c_vp(flat.ctypes.data), TFD_HOST, _stream()))
+        out, off = [], 0
+        for _, shape in self.plan.psi_shapes():
+            size = int(np.prod(shape))
+            out.append(flat[off:off + size].reshape(shape))
+            off += size
+        return out
+
+    def set_psi(self, arrays):
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(a, dtype=self.dtype).ravel() for a in arrays]))
+        if flat.size != self.psi_count():
+            raise ValueError('CPML memory count differs from the plan.')
+        if flat.size:
+            check(library().tfd_set_psi(self.handle, c_vp(flat.ctypes.data), TFD_HOST, _stream()))
+
+    # ---- time stepping -------------------------------------------------------------------------
+    def step(self, n=1, stream=None):
+        check(library().tfd_step(self.handle, int(n), _stream(stream)))
+
+    def reset(self):
+        check(library().tfd_reset(self.handle, _stream()))
+
+    def counter(self):
+        v = c_i64()
+        check(library().tfd_counter(self.handle, ctypes.byref(v), _stream()))
+        return v.value
+
+    def device_status(self):
+        v = c_i32()
+        check(library().tfd_device_status(self.handle, ctypes.byref(v), _stream()))
+        return v.value
+
+    # ---- observations ----------------------------------------------------------------------------
+    def get_traces(self):
+        out = np.zeros((self.plan.steps, len(self.plan.traces)), self.dtype)
+        if out.size:
+            check(library().tfd_get_traces(self.handle, c_vp(out.ctypes.data), TFD_HOST, _stream()))
+        return out
+
+    def get_plane(self, k):
+        p = self.plan.planes[k]
+        out = np.zeros((len(p.frequency), p.corner_cells.shape[2], len(p.components)), np.complex128)
+        if out.size:
+            check(library().tfd_get_plane(self.handle, k, c_vp(out.ctypes.data), TFD_HOST, _stream()))
+        return out
+
+    def get_slice(self, component, axis, index):
+        n = list(self.plan.shape)
+        n.pop(axis)
+        out = np.empty(n, self.dtype)
+        c = ['Ex', 'Ey', 'Ez', 'Hx', 'Hy', 'Hz'].index(component) if isinstance(component, str) else int(component)
+        check(library().tfd_get_slice(self.handle, c, axis, int(index), c_vp(out.ctypes.data), TFD_HOST, _stream()))
+        return out
+
+    def diagnose(self):
+        out = (ctypes.c_double * 3)()
+        check(library().tfd_diagnose(self.handle, out, _stream()))
+        return float(out[0]), float(out[1]), bool(out[2] == 1.0)

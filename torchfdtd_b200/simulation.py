@@ -1,0 +1,319 @@
+"""``Simulation(project).run() -> Result`` on the fused B200 kernels.
+
+Mirrors reference ``torchfdtd/solver.py``: ``Simulation`` :642-908 (run loop,
+graph capture, observation barriers, diagnostics, frames, summary) and
+``Result`` :511-639 (fields, traces, spectra, DFT planes, NPZ layout that
+round-trips through ``Result.load``). The selector is
+``Region(backend="cuda", cuda_kernel="fused")``; 'auto' resolves to the same
+kernels. Any other choice, and every scene feature outside the fused
+nondispersive path, is refused with a ``ValueError`` that names it.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import math
+import threading
+import time
+from dataclasses import dataclass, field
+from functools import cached_property
+from pathlib import Path
+
+import numpy as np
+
+from .models import Project
+from .plan import index_at, plan_grid
+from .run_control import DecayDecision, observation_schedule, source_end_time, validate_graph_steps
+from .spectra import point_spectrum
+
+C0 = 299792458.0
+ENGINE_LOCK = threading.Lock()
+ENGINE = 'TorchFDTD-B200 fused Yee/CPML (sm_100a)'
+
+
+def algorithmic_bytes_per_step(plan):
+    """Compulsory HBM bytes of one step: each advanced field component read and written once,
+    each stored permittivity sample read once and each CPML memory read and written once."""
+    real = np.dtype(plan.dtype).itemsize
+    comps = len(plan.active_components())
+    samples = plan.material_samples if plan.dimension == '3d' else 1
+    psi = sum(int(np.prod(s)) for (f, a, c, side), s in plan.psi_shapes() if _psi_active(plan, f, a, c))
+    return plan.cells * (2 * real * comps + real * samples) + 2 * real * psi
+
+
+def _psi_active(plan, forward, axis, comp):
+    """Whether the curl term (axis, input comp) of a family writes an advanced component."""
+    out = {(0, 2): 1, (0, 1): 2, (1, 2): 0, (1, 0): 2, (2, 1): 0, (2, 0): 1}[(axis, comp)]
+    name = ('H' if forward else 'E') + 'xyz'[out]
+    return name in plan.active_components()
+
+
+def plane_result(monitor, plan, frequency, components, values, dimension):
+    """Plane record from accumulated (frequency, point, component) DFT values
+    (reference torchfdtd/field_monitors.py:167-183)."""
+    values = np.asarray(values).astype(np.complex128)
+    by_component = {c: values[..., i] for i, c in enumerate(components)}
+    density = {}
+    for axis in set(monitor.record_poynting) | ({monitor.normal} if monitor.record_flux else set()):
+        i = 'xyz'.index(axis)
+        b, c = 'xyz'[(i + 1) % 3], 'xyz'[(i + 2) % 3]
+        density[axis] = .5 * np.real(by_component['E' + b] * by_component['H' + c].conj()
+                                     - by_component['E' + c] * by_component['H' + b].conj())
+    flux = density[monitor.normal] @ plan['weights'] if monitor.record_flux else None
+    fields = values[..., [components.index(c) for c in monitor.record_fields]]
+    poynting = (np.stack([density[c] for c in monitor.record_poynting], axis=-1) if monitor.record_poynting
+                else np.empty((*values.shape[:2], 0)))
+    return dict(id=monitor.id, name=monitor.name, frequency_hz=frequency, fields=fields, poynting=poynting, flux=flux, **plan,
+                components=list(monitor.record_fields), poynting_components=list(monitor.record_poynting),
+                accumulated_components=list(components), time_downsample=monitor.time_downsample,
+                settings=monitor.model_dump(),
+                flux_units='reduced E*H * s^2 * ' + ('m per invariant length' if dimension == '2d' else 'm^2'),
+                field_units='reduced field * s', normal_axis=monitor.normal)
+
+
+def run_signature(project, steps):
+    r = project.region
+    config = dict(region=r.model_dump(exclude={'backend', 'cuda_kernel', 'cuda_monitor_kernel', 'execution_mode', 'tiling',
+                                               'resident_cell_limit', 'field', 'slice_axis', 'slice_position',
+                                               'complex_display', 'snapshot_interval'}),
+                  sources=[project.resolved_source(s).model_dump() for s in project.sources], steps=steps,
+                  nodes=[a.tolist() for a in r.mesh_nodes])
+    return hashlib.sha256(json.dumps(config, sort_keys=True).encode()).hexdigest()
+
+
+@dataclass
+class Result:
+    project: Project
+    summary: dict
+    frames: np.ndarray
+    frame_steps: np.ndarray
+    epsilon: np.ndarray
+    signals: np.ndarray
+    times: np.ndarray
+    electric: np.ndarray
+    magnetic: np.ndarray
+    frequency_fields: list = field(default_factory=list)
+    endpoint_fields: dict | None = None
+
+    @property
+    def point_monitors(self):
+        return [self.project.resolved_monitor(m) for m in self.project.monitors if m.enabled and m.kind == 'point']
+
+    @cached_property
+    def spectra(self):
+        # H is sampled half a step after E.
+        dt = self.times[1] - self.times[0] if len(self.times) > 1 else 0
+        return [point_spectrum((self.times + (dt / 2 if m.component.startswith('H') else 0))[::m.time_downsample],
+                               self.signals[::m.time_downsample, k], m.spectrum)
+                for k, m in enumerate(self.point_monitors)]
+
+    def save(self, path):
+        """NPZ layout of the reference ``Result.save`` (torchfdtd/solver.py:536-564)."""
+        path = Path(path)
+        path.parent.mkdir(parents=True, exist_ok=True)
+        spectral_arrays, metadata, plane_metadata = {}, [], []
+        for k, (m, spec) in enumerate(zip(self.point_monitors, self.spectra)):
+            spectral_arrays[f'monitor_{k}_frequency_hz'] = spec['frequency_hz']
+            spectral_arrays[f'monitor_{k}_spectrum'] = spec['value']
+            metadata.append({'id': m.id, 'name': m.name, 'component': m.component, 'settings': m.spectrum.model_dump(),
+                             'units': spec['units'], 'transform': spec['transform']})
+        for k, result in enumerate(self.frequency_fields):
+            plane_metadata.append({key: v for key, v in result.items() if not isinstance(v, np.ndarray)})
+            for key, v in result.items():
+                if isinstance(v, np.ndarray):
+                    spectral_arrays[f'field_monitor_{k}_{key}'] = v
+        np.savez_compressed(path, project=self.project.model_dump_json(), summary=json.dumps(self.summary, default=str),
+                            field_monitors=json.dumps(plane_metadata, default=str),
+                            **{f'mesh_{a}_um': nodes for a, nodes in zip('xyz', self.project.region.mesh_nodes)},
+                            frames=self.frames, frame_steps=self.frame_steps, epsilon=self.epsilon, signals=self.signals,
+                            times=self.times, E=self.electric, H=self.magnetic, monitor_spectra=json.dumps(metadata),
+                            **spectral_arrays)
+
+    @classmethod
+    def load(cls, path):
+        with np.load(path, allow_pickle=False) as data:
+            planes = json.loads(str(data['field_monitors'])) if 'field_monitors' in data else []
+            for k, plane in enumerate(planes):
+                prefix = f'field_monitor_{k}_'
+                plane.update({key[len(prefix):]: data[key].copy() for key in data.files if key.startswith(prefix)})
+            return cls(Project.model_validate_json(str(data['project'])), json.loads(str(data['summary'])),
+                       *(data[key].copy() for key in ('frames', 'frame_steps', 'epsilon', 'signals', 'times', 'E', 'H')),
+                       planes, None)
+
+    def field_monitor(self, name_or_id):
+        matches = [m for m in self.frequency_fields if name_or_id in (m['id'], m['name'])]
+        if len(matches) != 1:
+            raise ValueError('Expected one enabled frequency plane with this name or id.')
+        return matches[0]
+
+    def flux_data(self):
+        return [dict(id=m['id'], name=m['name'], normal=m['normal_axis'], frequency_thz=(m['frequency_hz'] * 1e-12).tolist(),
+                     wavelength_um=(C0 / m['frequency_hz'] * 1e6).tolist(), flux=m['flux'].tolist(), units=m['flux_units'],
+                     points=len(m['weights']), shape=m['shape'], settings=m['settings'])
+                for m in self.frequency_fields if m['flux'] is not None]
+
+
+def resolve_selector(region):
+    """Refuse every kernel/back-end choice other than the fused CUDA path (reference models.py:277,287-288)."""
+    if region.backend == 'cpu':
+        raise ValueError('The fused CUDA kernel requires backend="cuda" and a CUDA GPU; backend="cpu" is the reference '
+                         "NumPy path, which this engine does not provide.")
+    for name in ('cuda_kernel', 'cuda_monitor_kernel'):
+        if getattr(region, name) == 'torch':
+            raise ValueError(f'{name}="torch" selects the reference Torch kernels, which this engine does not provide; '
+                             'use "fused" or "auto".')
+    return 'fused'
+
+
+class Simulation:
+    """Run the fused Yee/CPML kernels on a B200 for a ``Project``.
+
+    Coordinates, spans, wavelength and mesh are micrometres; E/H are the reduced
+    fields of the reference, not calibrated V/m or A/m."""
+
+    def __init__(self, project: Project):
+        self.project = Project.model_validate(project.model_dump())
+        self.project.region.require_resident()
+
+    @cached_property
+    def plan(self):
+        return plan_grid(self.project)
+
+    def run(self, progress=None, cancel=None, cuda_graph=True, cuda_graph_steps=1, kernel='auto'):
+        with ENGINE_LOCK:
+            return self._run(progress, cancel, cuda_graph, cuda_graph_steps, kernel)
+
+    def _run(self, progress, cancel, cuda_graph, cuda_graph_steps, kernel):
+        import torch
+        from .native import NativeGrid
+        p, r = self.project, self.project.region
+        cuda_kernel = resolve_selector(r)
+        validate_graph_steps(cuda_graph_steps, cuda_graph)
+        if not torch.cuda.is_available():
+            raise RuntimeError('CUDA requested but unavailable. The fused B200 engine needs a CUDA GPU.')
+        started = time.perf_counter()
+        plan = self.plan
+        grid = NativeGrid(plan, kernel=kernel)
+        free, _ = torch.cuda.mem_get_info()
+        control = r.run_control
+        source_end = source_end_time(p)
+        decision = DecayDecision(control, source_end, r.time_step)
+        diagnose = control.auto_shutoff or control.divergence_check
+        warnings = list(plan.warnings)
+        if control.auto_shutoff and not math.isfinite(source_end):
+            warnings.append('Automatic decay shutoff is inactive while a continuous source is enabled.')
+        graphs = {}
+        width = 1
+        stream = torch.cuda.Stream()
+        stream.wait_stream(torch.cuda.current_stream())
+        if cuda_graph:
+            width = min(cuda_graph_steps, r.steps)
+            with torch.cuda.stream(stream):
+                # One eager step loads the kernels before capture; the state is then zeroed.
+                grid.step(1, stream)
+                grid.reset()
+                for count in sorted({1, width}):
+                    g = torch.cuda.CUDAGraph()
+                    g.capture_begin()
+                    grid.step(count, stream)
+                    g.capture_end()
+                    graphs[count] = g
+            torch.cuda.synchronize()
+        axis = 'xyz'.index(r.slice_axis)
+        plane_index = index_at(tuple(r.slice_position if i == axis else 0 for i in range(3)), r, r.field)[axis]
+        component = 'xyz'.index(r.field[1].lower())
+        eps = plan.epsilon
+
+        def decimate(a):
+            return a[::max(1, math.ceil(a.shape[0] / 256)), ::max(1, math.ceil(a.shape[1] / 256))]
+        sl = [slice(None)] * 3
+        sl[axis] = plane_index
+        eps_plane = np.array(decimate((eps[..., component] if eps.ndim == 4 else eps)[tuple(sl)]))
+        interval = max(r.snapshot_interval, math.ceil(r.steps / 100))
+        frames, frame_steps = [], []
+        torch.cuda.synchronize()
+        setup_seconds = time.perf_counter() - started
+        compute_start = time.perf_counter()
+        completed, termination_reason, diagnostic_seconds, replays = 0, 'max_steps', 0., 0
+        barriers = set(range(interval, r.steps + 1, interval))
+        if diagnose:
+            barriers.update(range(control.check_interval, r.steps + 1, control.check_interval))
+        with torch.cuda.stream(stream):
+            for target, advance in observation_schedule(r.steps, width, barriers):
+                if cancel is not None and cancel.is_set():
+                    termination_reason = 'cancelled'
+                    break
+                if graphs:
+                    graphs[advance].replay()
+                    replays += 1
+                else:
+                    grid.step(advance, stream)
+                completed = target
+                stop = False
+                if diagnose and (completed % control.check_interval == 0 or completed == r.steps):
+                    t0 = time.perf_counter()
+                    energy, peak, finite = grid.diagnose()
+                    if not finite:
+                        raise FloatingPointError(f'Non-finite CPML or incident-line memory detected. (diagnostic step {completed})')
+                    try:
+                        stop = decision.update(completed, energy, peak)
+                    except FloatingPointError as exc:
+                        raise FloatingPointError(f'{exc} (diagnostic step {completed})') from exc
+                    diagnostic_seconds += time.perf_counter() - t0
+                if stop:
+                    termination_reason = 'decayed'
+                if completed % interval == 0 or completed == r.steps or stop:
+                    frame = decimate(grid.get_slice(r.field, axis, plane_index))
+                    if not np.isfinite(frame).all():
+                        raise FloatingPointError('Fields diverged. Check mesh, sources and precision.')
+                    frame = {'real': np.real, 'imag': np.imag, 'magnitude': np.abs, 'phase': np.angle}[r.complex_display](frame)
+                    frames.append(frame)
+                    frame_steps.append(completed)
+                    if progress:
+                        progress({'step': completed, 'total': r.steps, 'frame': frame.tolist(),
+                                  'elapsed': time.perf_counter() - compute_start,
+                                  'termination_reason': termination_reason if stop else None,
+                                  'diagnostics': decision.history[-1] if decision.history else None})
+                if stop:
+                    break
+        torch.cuda.synchronize()
+        seconds = time.perf_counter() - compute_start
+        status = grid.device_status()
+        if status:
+            raise RuntimeError(f'A fused kernel reported device status {status}.')
+        e, h = grid.get_fields()
+        if not np.isfinite(e).all() or not np.isfinite(h).all():
+            raise FloatingPointError('Non-finite fields detected.')
+        traces = grid.get_traces()[:completed]
+        frequency_results = []
+        for k, pp in enumerate(plan.planes):
+            values = grid.get_plane(k)
+            frequency_results.append(plane_result(pp.monitor, pp.plan, pp.frequency, list(pp.components), values, r.dimension))
+        if frequency_results:
+            signature = run_signature(p, completed)
+            for m in frequency_results:
+                m['run_signature'] = signature
+        bytes_per_step = algorithmic_bytes_per_step(plan)
+        cells = math.prod(r.shape)
+        stats = dict(warnings=warnings, backend='cuda', precision=r.precision, gpu=torch.cuda.get_device_name(),
+                     cuda_graph=bool(graphs), cuda_graph_steps=width, cuda_graph_replays=replays,
+                     cuda_kernel=cuda_kernel, cuda_monitor_kernel='fused', kernel=grid.kernel,
+                     steps=completed, requested_steps=r.steps, cancelled=termination_reason == 'cancelled',
+                     termination_reason=termination_reason, auto_shutoff=termination_reason == 'decayed',
+                     diagnostics=decision.history, diagnostic_seconds=diagnostic_seconds,
+                     diagnostic_backend='fused_cuda' if diagnose else None,
+                     source_end_s=source_end if math.isfinite(source_end) else None,
+                     seconds=seconds, setup_seconds=setup_seconds,
+                     mcells_per_second=cells * completed / max(seconds, 1e-9) / 1e6,
+                     gcells_per_s=cells * completed / max(seconds, 1e-9) / 1e9,
+                     hbm_bytes_per_step=bytes_per_step, arena_bytes=grid.arena_bytes, free_device_bytes=free,
+                     field_peak=float(np.max(np.abs(e))), slice_index=plane_index,
+                     slice_position=(0 if r.dimension == '2d' and axis == 2 else (plane_index + .5) * r.mesh - r.actual_size[axis] / 2),
+                     complex_fields=False, complex_display=r.complex_display, material_update='nondispersive',
+                     dispersive_samples=0, material_sampling=r.material_sampling,
+                     epsilon_definition='instantaneous relative permittivity (epsilon-infinity for dispersive cells)',
+                     boundaries=r.boundaries.model_dump(), bloch_phase=r.bloch_phase,
+                     units='geometry: um; time: s; E/H: reduced fields; Bloch phase: rad', engine=ENGINE)
+        grid.close()
+        return Result(p, stats, np.array(frames), np.array(frame_steps), eps_plane, traces,
+                      np.arange(1, completed + 1) * r.time_step, e, h, frequency_results)
