@@ -1,0 +1,327 @@
+"""Benchmark of the fused Yee/CPML engine: Gcell-updates/s and HBM-roofline fraction.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload roofline|strip]
+
+Workload (default ``roofline``): 3D full-vector Yee + CPML, FP32, 512 x 512 x 256 cells
+at 0.05 um, CPML 12 cells per face (cubic grading, sigma_max = 0.8 (m+1)/(eta0 dx),
+kappa_max 1, alpha_max 0.05), seeded random piecewise-constant permittivity in [1, 12.1]
+on 8^3-cell blocks, Ey dipole at the centre, one Ey point trace. ``strip`` is the
+160 x 120 x 40 Si-strip scene with an x-normal DFT plane. All inputs are synthetic and
+seeded. A bench step is one FDTD time step over the whole grid (one fused step launch
+plus one observation launch).
+
+* ``value``: device-timed (CUDA events on the launching stream) whole-job throughput,
+  fields resident in HBM; inputs are larger than L2, so no flush is needed.
+* ``e2e``: the same metric through the public call ``Simulation(project, epsilon).run()``,
+  wall-clock from the call to its return (planning, host->device upload of the material,
+  graph capture, the K steps, device->host copies of fields, traces and frames).
+* ``roofline``: algorithmic bytes per step (each field component read and written once,
+  the permittivity read once, each CPML memory read and written once) per average step
+  time, against the measured HBM copy peak.
+* ``cpu_baseline``: the C oracle (oracle/yee_cpu.c, same arithmetic, all host threads) on
+  the same grid for a bounded number of steps.
+
+``--impl reference`` times the reference's CPU algorithm (the C port of its NumPy path)
+on the host cores. With torchrun (N>1) every rank runs its own replica (the benchmark
+configurations are single-GPU; the engine does not shard a grid): scaling "weak", time
+is the max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = 'Gcell-updates/s'
+C0 = 299792458.0
+# DRAM bytes per cell-update of the step kernel measured by ncu on this workload
+# (dram__bytes_read.sum + dram__bytes_write.sum per launch / cells); None until captured.
+MEASURED_TRAFFIC_PER_CELL = {}
+
+
+def baseline_face(layers):
+    from torchfdtd_b200 import BoundaryFace
+    return BoundaryFace(sigma_scale=3.2 * (layers + 1) / 40, kappa=1, alpha=0.05, polynomial=3, alpha_polynomial=1)
+
+
+def workload(name, steps, seed=2024):
+    """(project, epsilon or None, description) of a benchmark workload."""
+    from torchfdtd_b200 import Boundaries, FieldMonitor, Material, Monitor, Project, Region, Source, SpectrumSettings, Structure
+    from torchfdtd_b200.models import RunControl
+    lam = 1.55
+    control = RunControl(divergence_check=False)
+    src = dict(component='Ey', wavelength=lam, pulse='gaussian', time_definition='standard', pulse_length=20e-15, pulse_offset=40e-15)
+    if name in ('roofline', 'roofline256'):
+        # 'roofline256' is the same scene at 256^3 cells (about 1.3 GB on the device) for profiler captures.
+        n = (512, 512, 256) if name == 'roofline' else (256, 256, 256)
+        L = 12
+        b = Boundaries(**{f'{a}_{s}': baseline_face(L) for a in 'xyz' for s in ('min', 'max')})
+        region = Region(dimension='3d', size=tuple(v * .05 for v in n), mesh=.05, pml_cells=L, steps=steps, backend='cuda',
+                        cuda_kernel='fused', boundaries=b, run_control=control, snapshot_interval=10000)
+        project = Project(name=f'roofline {n[0]}x{n[1]}x{n[2]}', region=region, sources=[Source(id='dip', center=(0, 0, 0), **src)],
+                          monitors=[Monitor(id='probe', center=(1.0, 0, 0), component='Ey')])
+        rng = np.random.default_rng(seed)
+        blocks = rng.uniform(1, 12.1, tuple(v // 8 for v in n)).astype(np.float32)
+        eps = np.repeat(np.repeat(np.repeat(blocks, 8, 0), 8, 1), 8, 2)
+        return project, eps, (f'3D Yee+CPML {n[0]}x{n[1]}x{n[2]} (0.05 um), CPML 12, seeded random piecewise-constant eps in '
+                              '[1,12.1] on 8^3 blocks, Ey dipole at the centre, FP32')
+    if name == 'strip':
+        L = 12
+        b = Boundaries(**{f'{a}_{s}': baseline_face(L) for a in 'xyz' for s in ('min', 'max')})
+        region = Region(dimension='3d', size=(8, 6, 2), mesh=.05, pml_cells=L, background_index=2.085**.5, steps=steps,
+                        backend='cuda', cuda_kernel='fused', boundaries=b, run_control=control, snapshot_interval=10000)
+        custom = SpectrumSettings(sampling='custom', custom_frequencies_hz=[C0 / (lam * 1e-6)], apodization='none')
+        project = Project(name='Si strip 160x120x40', region=region, materials=[Material(name='Si', index=12.08**.5)],
+                          structures=[Structure(id='strip', size=(8, .65, .4), material='Si')],
+                          sources=[Source(id='dip', center=(-2.5, 0, 0), **src)],
+                          monitors=[FieldMonitor(id='plane', normal='x', center=(2, 0, 0), size=(0, 4.8, .8), dft_precision='float64',
+                                                 spectrum=custom)])
+        return project, None, ('3D Yee+CPML 160x120x40 (0.05 um), CPML 12, Si strip 0.65x0.4 um in SiO2, Ey dipole, '
+                               'x-normal DFT plane at 1.55 um, FP32')
+    raise ValueError(name)
+
+
+def measured_peaks():
+    path = ROOT / 'MEASURED_PEAKS.json'
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data['hbm_gbs']), 'measured'
+    return 6650.0, 'fallback'
+
+
+class ClockSampler:
+    """SM clock and throttle reasons through NVML every 20 ms while active."""
+    REASONS = {0x4: 'sw_power_cap', 0x8: 'hw_slowdown', 0x20: 'sw_thermal_slowdown', 0x40: 'hw_thermal_slowdown',
+               0x80: 'hw_power_brake_slowdown', 0x2: 'applications_clocks_setting', 0x1: 'gpu_idle'}
+
+    def __init__(self, index):
+        self.samples = []
+        self.window = None
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:  # noqa: BLE001 - no NVML: clocks are reported as unavailable
+            self.max_mhz = None
+        self.stop = threading.Event()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                mhz = self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM)
+                reasons = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                self.samples.append((time.time(), mhz, reasons))
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(0.02)
+
+    def start(self):
+        if self.ok:
+            self.thread.start()
+
+    def finish(self):
+        self.stop.set()
+        if self.ok:
+            self.thread.join()
+        if not self.samples:
+            return {'sm_mhz': None, 'sm_max_mhz': self.max_mhz, 'reasons': [], 'samples': 0}
+        lo, hi = self.window or (0, math.inf)
+        inside = [s for s in self.samples if lo <= s[0] <= hi] or self.samples
+        mask = 0
+        for _, _, r in inside:
+            mask |= r
+        names = sorted({name for bit, name in self.REASONS.items() if mask & bit and name != 'gpu_idle'})
+        return {'sm_mhz': float(np.median([s[1] for s in inside])), 'sm_max_mhz': self.max_mhz, 'reasons': names,
+                'samples': len(inside)}
+
+
+def cpu_rate(plan, budget_s=15.0, min_steps=2, max_steps=None, threads=None):
+    """Gcell-updates/s of the C oracle on the same plan; steps run until the time budget is spent."""
+    sys.path.insert(0, str(ROOT))
+    from oracle.cpu import CpuOracle
+    o = CpuOracle(plan, threads=threads)
+    o.run(1)  # warm-up (first touch of the state)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        o.run(1)
+        steps += 1
+        elapsed = time.perf_counter() - t0
+        if (steps >= min_steps and elapsed >= budget_s) or (max_steps and steps >= max_steps):
+            break
+    return plan.cells * steps / elapsed / 1e9, steps, elapsed, o.threads
+
+
+def dist_setup(args):
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=timedelta(seconds=600), device_id=torch.device('cuda', local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, world, rank):
+    from torchfdtd_b200.plan import plan_grid
+    if rank != 0:
+        return None
+    project, eps, desc = workload(args.workload, max(10, args.steps))
+    plan = plan_grid(project)
+    if eps is not None:
+        plan.epsilon, plan.inv_eps = eps, (1 / eps).astype(plan.dtype)
+    # Each bench step is one full time step over the whole grid; the run is bounded to ~2 minutes.
+    per_step_budget = 120.0 / max(1, args.steps + args.warmup)
+    rate, steps, elapsed, threads = cpu_rate(plan, budget_s=per_step_budget * args.steps, min_steps=min(args.steps, 2),
+                                             max_steps=args.steps)
+    sample = (f'{steps} full time steps of the {plan.shape[0]}x{plan.shape[1]}x{plan.shape[2]} grid on {threads} host threads '
+              f'(C port of the reference NumPy Yee/CPML update, bitwise equal to it), after 1 warm-up step')
+    line = dict(metric=METRIC, value=rate, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                ms_per_step=elapsed / steps * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
+                data='synthetic', impl='reference',
+                config=dict(workload=desc, cells=plan.cells, parallelism='host threads'),
+                cpu_baseline=dict(value=rate, unit=METRIC, cores=threads, kind='port', sample=sample),
+                e2e=dict(value=rate, unit=METRIC, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    return line
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from torchfdtd_b200 import Simulation
+    from torchfdtd_b200.native import NativeGrid
+    from torchfdtd_b200.plan import plan_grid
+    from torchfdtd_b200.simulation import algorithmic_bytes_per_step
+    device = torch.device('cuda', local)
+    torch.cuda.set_device(device)
+    total_steps = args.warmup + args.steps
+    project, eps, desc = workload(args.workload, max(10, total_steps))
+    plan = plan_grid(project)
+    if eps is not None:
+        plan.epsilon, plan.inv_eps = eps, (1 / eps).astype(plan.dtype)
+    grid = NativeGrid(plan, kernel=args.kernel)
+    stream = torch.cuda.Stream(device)
+    sampler = ClockSampler(local)
+    sampler.start()
+    with torch.cuda.stream(stream):
+        grid.step(args.warmup, stream)
+        stream.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_wall = time.time()
+        start.record(stream)
+        grid.step(args.steps, stream)
+        end.record(stream)
+        end.synchronize()
+        t_wall_end = time.time()
+    torch.cuda.synchronize()
+    barrier(world)
+    sampler.window = (t_wall, t_wall_end)
+    clocks = sampler.finish()
+    elapsed = max_over_ranks(start.elapsed_time(end) / 1e3, world)
+    status = grid.device_status()
+    kernel_used = grid.kernel
+    grid.close()
+    del grid
+    torch.cuda.empty_cache()
+    cells = plan.cells
+    value = world * cells * args.steps / elapsed / 1e9
+    bytes_step = algorithmic_bytes_per_step(plan)
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_step * args.steps / elapsed / 1e9
+    traffic = MEASURED_TRAFFIC_PER_CELL.get((args.workload, kernel_used))
+    roofline = dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak,
+                    traffic=None if traffic is None else traffic * cells, peak_source=peak_kind,
+                    algorithmic_bytes_per_step=bytes_step, kernel=f'k_step_{kernel_used}',
+                    note='achieved counts the whole step (fused step launch + observation launch)')
+    # ---- end to end through the public API --------------------------------------------------
+    e2e_steps = max(10, args.steps)
+    e2e_project, e2e_eps, _ = workload(args.workload, e2e_steps)
+    barrier(world)
+    t0 = time.perf_counter()
+    result = Simulation(e2e_project, epsilon=e2e_eps).run(cuda_graph=True, cuda_graph_steps=16, kernel=args.kernel)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    real = np.dtype(plan.dtype).itemsize
+    h2d = cells * plan.material_samples * real + sum(t.values.nbytes for t in plan.sources)
+    d2h = result.electric.nbytes + result.magnetic.nbytes + result.signals.nbytes + result.frames.nbytes
+    e2e = dict(value=world * cells * e2e_steps / e2e_s / 1e9, unit=METRIC, h2d_bytes_per_step=h2d / e2e_steps,
+               d2h_bytes_per_step=d2h / e2e_steps, seconds=e2e_s, steps=e2e_steps,
+               call='Simulation(project, epsilon).run(cuda_graph=True, cuda_graph_steps=16)')
+    line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                ms_per_step=elapsed / args.steps * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
+                data='synthetic (seeded)', config=dict(workload=desc, cells=cells, l2='inputs larger than L2 (no flush needed)',
+                                                       parallelism=f'replicas x{world}' if world > 1 else 'single GPU',
+                                                       kernel=kernel_used),
+                roofline=roofline, e2e=e2e, clocks=clocks, gpu_launches=2 * args.steps, device_status=status)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, steps, el, threads = cpu_rate(plan, budget_s=args.cpu_budget)
+        line['cpu_baseline'] = dict(value=rate, unit=METRIC, cores=threads, kind='port',
+                                    sample=f'{steps} full time steps of the same grid on {threads} host threads (C port of the '
+                                           f'reference NumPy update), {el:.1f} s')
+    return line if rank == 0 else None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=200)
+    ap.add_argument('--warmup', type=int, default=10)
+    ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
+    ap.add_argument('--workload', choices=['roofline', 'roofline256', 'strip'], default='roofline')
+    ap.add_argument('--kernel', choices=['auto', 'march', 'gather'], default='auto')
+    ap.add_argument('--cpu-budget', type=float, default=15.0)
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == 'reference':
+        # Rank 0 alone times the host-core reference; other ranks exit without work.
+        world, rank, local = int(os.environ.get('WORLD_SIZE', '1')), int(os.environ.get('RANK', '0')), 0
+        line = run_reference(args, world, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    world, rank, local = dist_setup(args)
+    try:
+        line = run_reference(args, world, rank) if args.impl == 'reference' else run_ours(args, world, rank, local)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

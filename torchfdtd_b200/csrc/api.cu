@@ -9,6 +9,8 @@
 #include "aux.cuh"
 #include "internal.cuh"
 #include "step_gather.cuh"
+#include "step_march.cuh"
+#include <cudaTypedefs.h>
 
 using namespace tfd;
 
@@ -250,12 +252,21 @@ struct tfd_plan {
     std::vector<PsiSegment> psi_segs;
     std::vector<int> planes_f, planes_p, planes_c;
     int max_samples = 0;
+    MarchArgs<float> mf;
+    MarchArgs<double> md;
+    dim3 march_grid;
+    size_t march_smem = 0;
+    void *march_launch = nullptr;
+    std::vector<int> seg_f, seg_a, seg_lo, seg_hi;
 
     template <typename T> Grid<T> &grid();
+    template <typename T> MarchArgs<T> &march();
     template <typename T> T *ptr(size_t off) const { return off ? (T *)(arena + off) : nullptr; }
 };
 template <> Grid<float> &tfd_plan::grid<float>() { return gf; }
 template <> Grid<double> &tfd_plan::grid<double>() { return gd; }
+template <> MarchArgs<float> &tfd_plan::march<float>() { return mf; }
+template <> MarchArgs<double> &tfd_plan::march<double>() { return md; }
 
 namespace {
 
@@ -438,6 +449,105 @@ int zero_state(tfd_plan *p, cudaStream_t s) {
 
 }  // namespace
 
+// ---- marching kernel set-up -------------------------------------------------------------------------
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+template <typename T>
+bool march_supported(const tfd_plan *p) {
+    const Grid<T> &g = const_cast<tfd_plan *>(p)->grid<T>();
+    return g.n[2] > 1 && !g.periodic[0] && !g.periodic[1] && g.active == 0x3F;
+}
+
+template <typename T, int SAMPLES>
+int setup_march_s(tfd_plan *p) {
+    using S = MarchShape<T, SAMPLES>;
+    Grid<T> &g = p->grid<T>();
+    MarchArgs<T> &a = p->march<T>();
+    std::memset(&a, 0, sizeof(a));
+    a.g = g;
+    if (g.count >= (1LL << 31)) return fail(TFD_ERR_UNSUPPORTED, "component arrays above 2^31 elements need the gather kernel");
+    for (int f = 0; f < 2; ++f)
+        for (int ax = 0; ax < 3; ++ax) {
+            if (p->L.psi_len[f][ax] >= (1LL << 31)) return fail(TFD_ERR_UNSUPPORTED, "CPML memory above 2^31 elements");
+            // slab bounds: segments of (family, axis) sorted by lo; empty slabs are [0, 0)
+            int k = 0;
+            int b[4] = {0, 0, 0, 0};
+            std::vector<std::pair<int, int>> segs;
+            for (int q = 0; q < p->desc.n_segments; ++q)
+                if (p->seg_f[q] == f && p->seg_a[q] == ax) segs.push_back({p->seg_lo[q], p->seg_hi[q]});
+            std::sort(segs.begin(), segs.end());
+            if (segs.size() > 2) return fail(TFD_ERR_INVALID, "more than two CPML slabs on one axis");
+            for (auto &sg : segs) { b[2 * k] = sg.first; b[2 * k + 1] = sg.second; ++k; }
+            for (int q = 0; q < 4; ++q) a.slab[f][ax][q] = b[q];
+        }
+    auto encode = tensor_map_encoder();
+    if (!encode) return fail(TFD_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable from the driver");
+    const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const cuuint64_t e = sizeof(T);
+    for (int c = 0; c < 6; ++c) {
+        T *base = c < 3 ? g.E[0][c] : g.H[0][c - 3];
+        const cuuint64_t dims[4] = {(cuuint64_t)g.n[0], (cuuint64_t)g.n[1], (cuuint64_t)g.n[2], 2};
+        const cuuint64_t strides[3] = {(cuuint64_t)g.pitch * e, (cuuint64_t)g.plane * e, (cuuint64_t)g.count * e};
+        const cuuint32_t box[4] = {(cuuint32_t)S::BXW, (cuuint32_t)S::BY, 1, 1};
+        const cuuint32_t elem[4] = {1, 1, 1, 1};
+        CUresult r = encode(&a.field[c], dt, 4, (void *)base, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(TFD_ERR_CUDA, "cuTensorMapEncodeTiled(field) failed: " + std::to_string((int)r));
+    }
+    for (int c = 0; c < SAMPLES; ++c) {
+        const cuuint64_t dims[3] = {(cuuint64_t)g.n[0], (cuuint64_t)g.n[1], (cuuint64_t)g.n[2]};
+        const cuuint64_t strides[2] = {(cuuint64_t)g.pitch * e, (cuuint64_t)g.plane * e};
+        const cuuint32_t box[3] = {(cuuint32_t)S::BXW, (cuuint32_t)S::BY, 1};
+        const cuuint32_t elem[3] = {1, 1, 1};
+        CUresult r = encode(&a.eps[c], dt, 3, (void *)g.inv_eps[c], dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return fail(TFD_ERR_CUDA, "cuTensorMapEncodeTiled(eps) failed: " + std::to_string((int)r));
+    }
+    p->march_smem = S::SMEM;
+    TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
+    int device = 0, sms = 148, per_sm = 1;
+    TFD_CUDA(cudaGetDevice(&device));
+    TFD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    TFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_march<T, SAMPLES>, kMarchThreads, p->march_smem));
+    const long long resident = (long long)sms * std::max(1, per_sm);
+    const int tx = (g.n[0] + kMarchOwnX - 1) / kMarchOwnX, ty = (g.n[1] + kMarchOwnY - 1) / kMarchOwnY;
+    const long long tiles = (long long)tx * ty;
+    // Planes per chunk: balance whole waves of resident CTAs against the two extra planes a chunk loads.
+    double best = -1;
+    int best_lz = g.n[2];
+    for (int chunks = 1; chunks <= std::max(1, g.n[2] / 4); ++chunks) {
+        const int lz = (g.n[2] + chunks - 1) / chunks;
+        const long long real_chunks = (g.n[2] + lz - 1) / lz;
+        const long long ctas = tiles * real_chunks;
+        const double waves = std::ceil((double)ctas / resident);
+        const double eff = (double)ctas / (waves * resident) * ((double)lz / (lz + 2));
+        if (eff > best + 1e-9) { best = eff; best_lz = lz; }
+    }
+    a.lz = best_lz;
+    p->march_grid = dim3(tx, ty, (g.n[2] + best_lz - 1) / best_lz);
+    p->march_launch = SAMPLES == 3 ? (void *)k_step_march<T, 3> : (void *)k_step_march<T, 1>;
+    return TFD_OK;
+}
+
+template <typename T>
+int setup_march(tfd_plan *p) {
+    return p->desc.material_samples == 3 ? setup_march_s<T, 3>(p) : setup_march_s<T, 1>(p);
+}
+
+}  // namespace
+
 // ---- C ABI ---------------------------------------------------------------------------------------
 namespace {
 
@@ -611,8 +721,15 @@ int step_t(tfd_plan *p, int nsteps, cudaStream_t s) {
     const MonitorArgs<T> m = monitor_args<T>(p);
     dim3 mgrid((unsigned)std::max(1, (p->max_samples + kMonitorThreads - 1) / kMonitorThreads), (unsigned)std::max(1, p->desc.n_planes));
     for (int k = 0; k < nsteps; ++k) {
-        int rc = launch_step_gather<T>(p, s);
-        if (rc) return rc;
+        if (p->kernel == TFD_KERNEL_MARCH) {
+            if (p->desc.material_samples == 3)
+                k_step_march<T, 3><<<p->march_grid, kMarchThreads, p->march_smem, s>>>(p->march<T>());
+            else
+                k_step_march<T, 1><<<p->march_grid, kMarchThreads, p->march_smem, s>>>(p->march<T>());
+        } else {
+            int rc = launch_step_gather<T>(p, s);
+            if (rc) return rc;
+        }
         k_monitor<T><<<mgrid, kMonitorThreads, 0, s>>>(m);
     }
     TFD_CUDA(cudaGetLastError());
@@ -730,14 +847,26 @@ int tfd_plan_create(const tfd_desc *desc, void *arena, size_t arena_bytes, void 
     p->arena = (char *)arena;
     size_t total;
     p->psi_segs = psi_segments(desc, &total);
+    for (int k = 0; k < desc->n_segments; ++k) {
+        p->seg_f.push_back(desc->segments[k].forward);
+        p->seg_a.push_back(desc->segments[k].axis);
+        p->seg_lo.push_back(desc->segments[k].lo);
+        p->seg_hi.push_back(desc->segments[k].hi);
+    }
     for (int k = 0; k < desc->n_planes; ++k) {
         p->planes_f.push_back(desc->planes[k].frequencies);
         p->planes_p.push_back(desc->planes[k].points);
         p->planes_c.push_back(desc->planes[k].components);
     }
-    p->kernel = TFD_KERNEL_GATHER;
     cudaStream_t s = as_stream(stream);
     rc = desc->precision == 8 ? create_typed<double>(p, desc, s) : create_typed<float>(p, desc, s);
+    if (!rc) {
+        const bool march_ok = desc->precision == 8 ? march_supported<double>(p) : march_supported<float>(p);
+        if (desc->kernel == TFD_KERNEL_MARCH && !march_ok)
+            rc = fail(TFD_ERR_UNSUPPORTED, "the marching kernel needs a 3D grid without periodic x/y faces");
+        p->kernel = (desc->kernel == TFD_KERNEL_GATHER || !march_ok) ? TFD_KERNEL_GATHER : TFD_KERNEL_MARCH;
+        if (!rc && p->kernel == TFD_KERNEL_MARCH) rc = TFD_DISPATCH(p, setup_march, p);
+    }
     if (!rc) rc = TFD_DISPATCH(p, zero_state, p, s);
     if (!rc) {
         const long long n = p->L.count;

@@ -171,13 +171,26 @@ class Simulation:
     Coordinates, spans, wavelength and mesh are micrometres; E/H are the reduced
     fields of the reference, not calibrated V/m or A/m."""
 
-    def __init__(self, project: Project):
+    def __init__(self, project: Project, epsilon=None):
+        """``epsilon`` (optional) replaces the voxelized relative permittivity with an array of the
+        grid shape, (nx, ny, nz) or (nx, ny, nz, 3): a material given at plan level instead of as
+        structures (the reference's differentiable path takes the same, torchfdtd/differentiable.py:100)."""
         self.project = Project.model_validate(project.model_dump())
         self.project.region.require_resident()
+        self.epsilon = epsilon
 
     @cached_property
     def plan(self):
-        return plan_grid(self.project)
+        plan = plan_grid(self.project)
+        if self.epsilon is not None:
+            eps = np.asarray(self.epsilon, dtype=plan.dtype)
+            if eps.shape not in (tuple(plan.shape), (*plan.shape, 3)):
+                raise ValueError(f'epsilon must have shape {tuple(plan.shape)} or {(*plan.shape, 3)}, not {eps.shape}.')
+            if not np.all(np.isfinite(eps)) or np.any(eps < 1):
+                raise ValueError('epsilon must be finite and at least 1.')
+            plan.epsilon = eps
+            plan.inv_eps = (1 / eps).astype(plan.dtype)
+        return plan
 
     def run(self, progress=None, cancel=None, cuda_graph=True, cuda_graph_steps=1, kernel='auto'):
         with ENGINE_LOCK:
