@@ -256,7 +256,7 @@ struct tfd_plan {
     MarchArgs<double> md;
     dim3 march_grid;
     size_t march_smem = 0;
-    void *march_launch = nullptr;
+    int march_variant = 42;
     std::vector<int> seg_f, seg_a, seg_lo, seg_hi;
 
     template <typename T> Grid<T> &grid();
@@ -470,13 +470,14 @@ bool march_supported(const tfd_plan *p) {
     return g.n[2] > 1 && !g.periodic[0] && !g.periodic[1] && g.active == 0x3F;
 }
 
-template <typename T, int SAMPLES>
+template <typename T, int SAMPLES, int D, int MINB>
 int setup_march_s(tfd_plan *p) {
-    using S = MarchShape<T, SAMPLES>;
+    using S = MarchShape<T, SAMPLES, D>;
     Grid<T> &g = p->grid<T>();
     MarchArgs<T> &a = p->march<T>();
     std::memset(&a, 0, sizeof(a));
     a.g = g;
+    for (int ax = 0; ax < 3; ++ax) a.psi_parity[ax] = (int)((p->L.psi_len[0][ax] + 63) / 64 * 64);
     if (g.count >= (1LL << 31)) return fail(TFD_ERR_UNSUPPORTED, "component arrays above 2^31 elements need the gather kernel");
     for (int f = 0; f < 2; ++f)
         for (int ax = 0; ax < 3; ++ax) {
@@ -500,7 +501,7 @@ int setup_march_s(tfd_plan *p) {
         T *base = c < 3 ? g.E[0][c] : g.H[0][c - 3];
         const cuuint64_t dims[4] = {(cuuint64_t)g.n[0], (cuuint64_t)g.n[1], (cuuint64_t)g.n[2], 2};
         const cuuint64_t strides[3] = {(cuuint64_t)g.pitch * e, (cuuint64_t)g.plane * e, (cuuint64_t)g.count * e};
-        const cuuint32_t box[4] = {(cuuint32_t)S::BXW, (cuuint32_t)S::BY, 1, 1};
+        const cuuint32_t box[4] = {(cuuint32_t)S::BXW, (cuuint32_t)(c < 3 ? S::BYE : S::BYH), 1, 1};
         const cuuint32_t elem[4] = {1, 1, 1, 1};
         CUresult r = encode(&a.field[c], dt, 4, (void *)base, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -509,18 +510,18 @@ int setup_march_s(tfd_plan *p) {
     for (int c = 0; c < SAMPLES; ++c) {
         const cuuint64_t dims[3] = {(cuuint64_t)g.n[0], (cuuint64_t)g.n[1], (cuuint64_t)g.n[2]};
         const cuuint64_t strides[2] = {(cuuint64_t)g.pitch * e, (cuuint64_t)g.plane * e};
-        const cuuint32_t box[3] = {(cuuint32_t)S::BXW, (cuuint32_t)S::BY, 1};
+        const cuuint32_t box[3] = {(cuuint32_t)S::BXW, (cuuint32_t)S::BYE, 1};
         const cuuint32_t elem[3] = {1, 1, 1};
         CUresult r = encode(&a.eps[c], dt, 3, (void *)g.inv_eps[c], dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return fail(TFD_ERR_CUDA, "cuTensorMapEncodeTiled(eps) failed: " + std::to_string((int)r));
     }
     p->march_smem = S::SMEM;
-    TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
+    TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
     int device = 0, sms = 148, per_sm = 1;
     TFD_CUDA(cudaGetDevice(&device));
     TFD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    TFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_march<T, SAMPLES>, kMarchThreads, p->march_smem));
+    TFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_march<T, SAMPLES, D, MINB>, kMarchThreads, p->march_smem));
     const long long resident = (long long)sms * std::max(1, per_sm);
     const int tx = (g.n[0] + kMarchOwnX - 1) / kMarchOwnX, ty = (g.n[1] + kMarchOwnY - 1) / kMarchOwnY;
     const long long tiles = (long long)tx * ty;
@@ -537,13 +538,37 @@ int setup_march_s(tfd_plan *p) {
     }
     a.lz = best_lz;
     p->march_grid = dim3(tx, ty, (g.n[2] + best_lz - 1) / best_lz);
-    p->march_launch = SAMPLES == 3 ? (void *)k_step_march<T, 3> : (void *)k_step_march<T, 1>;
+    p->march_variant = D * 10 + MINB;
     return TFD_OK;
 }
 
+// Prefetch depth D / CTAs per SM of the marching kernel, as the two digits of a variant:
+// 23 (FP32 default), 32, 14 and 22 (FP64 default). TFD_MARCH_VARIANT overrides it for launch-shape sweeps.
 template <typename T>
 int setup_march(tfd_plan *p) {
-    return p->desc.material_samples == 3 ? setup_march_s<T, 3>(p) : setup_march_s<T, 1>(p);
+    const char *env = getenv("TFD_MARCH_VARIANT");
+    const std::string v = env ? env : (sizeof(T) == 4 ? "23" : "22");
+    const bool three = p->desc.material_samples == 3;
+    if (sizeof(T) == 8 || v == "22") return three ? setup_march_s<T, 3, 2, 2>(p) : setup_march_s<T, 1, 2, 2>(p);
+    if (v == "32") return three ? setup_march_s<T, 3, 3, 2>(p) : setup_march_s<T, 1, 3, 2>(p);
+    if (v == "14") return three ? setup_march_s<T, 3, 1, 4>(p) : setup_march_s<T, 1, 1, 4>(p);
+    return three ? setup_march_s<T, 3, 2, 3>(p) : setup_march_s<T, 1, 2, 3>(p);
+}
+
+template <typename T, int SAMPLES, int D, int MINB>
+void launch_march(tfd_plan *p, cudaStream_t s) {
+    k_step_march<T, SAMPLES, D, MINB><<<p->march_grid, kMarchThreads, p->march_smem, s>>>(p->march<T>());
+}
+
+template <typename T>
+void launch_march_any(tfd_plan *p, cudaStream_t s) {
+    const bool three = p->desc.material_samples == 3;
+    switch (p->march_variant) {
+        case 23: three ? launch_march<T, 3, 2, 3>(p, s) : launch_march<T, 1, 2, 3>(p, s); break;
+        case 32: three ? launch_march<T, 3, 3, 2>(p, s) : launch_march<T, 1, 3, 2>(p, s); break;
+        case 14: three ? launch_march<T, 3, 1, 4>(p, s) : launch_march<T, 1, 1, 4>(p, s); break;
+        default: three ? launch_march<T, 3, 2, 2>(p, s) : launch_march<T, 1, 2, 2>(p, s); break;
+    }
 }
 
 }  // namespace
@@ -722,10 +747,7 @@ int step_t(tfd_plan *p, int nsteps, cudaStream_t s) {
     dim3 mgrid((unsigned)std::max(1, (p->max_samples + kMonitorThreads - 1) / kMonitorThreads), (unsigned)std::max(1, p->desc.n_planes));
     for (int k = 0; k < nsteps; ++k) {
         if (p->kernel == TFD_KERNEL_MARCH) {
-            if (p->desc.material_samples == 3)
-                k_step_march<T, 3><<<p->march_grid, kMarchThreads, p->march_smem, s>>>(p->march<T>());
-            else
-                k_step_march<T, 1><<<p->march_grid, kMarchThreads, p->march_smem, s>>>(p->march<T>());
+            launch_march_any<T>(p, s);
         } else {
             int rc = launch_step_gather<T>(p, s);
             if (rc) return rc;

@@ -38,8 +38,6 @@ constexpr int kMarchOwnX = 31;
 constexpr int kMarchRows = 16;      // computed E rows: 15 owned + the +y halo
 constexpr int kMarchOwnY = 15;
 constexpr int kMarchThreads = 256;
-constexpr int kMarchStages = 4;
-constexpr long long kWaitLimit = 1LL << 24;
 
 template <typename T>
 struct MarchArgs {
@@ -48,20 +46,27 @@ struct MarchArgs {
     Grid<T> g;
     int lz;                      // planes per chunk
     int slab[2][3][4];           // per family and axis: lo0, hi0, lo1, hi1 of the two CPML slabs
+    int psi_parity[3];           // elements between the two parities of an E-family CPML memory, per axis
 };
 
-template <typename T, int SAMPLES>
+// Shared-memory layout of the marching kernel. D = planes of TMA prefetch; the H ring holds
+// D + 2 planes (k-1 and k in use), the E ring (old E and inverse permittivity) D + 1 (k in use).
+template <typename T, int SAMPLES, int D>
 struct MarchShape {
     static constexpr int A = 16 / sizeof(T);                 // TMA x alignment in elements
     static constexpr int BXW = kMarchLanes + A;              // box columns from floor_A(x0-1)
-    static constexpr int BY = kMarchRows + 1;                // box rows y0-1 .. y0+15
-    static constexpr int BOX = BXW * BY;
-    static constexpr int BOX_BYTES = BOX * sizeof(T);
-    static constexpr int BOX_STRIDE = (BOX_BYTES + 127) / 128 * 128;
-    static constexpr int ARRAYS = 6 + SAMPLES;
-    static constexpr int STAGE_BYTES = ARRAYS * BOX_STRIDE;
+    static constexpr int BYH = kMarchRows + 1;               // H box rows y0-1 .. y0+15
+    static constexpr int BYE = kMarchRows;                   // E / eps box rows y0 .. y0+15
+    static constexpr int BOXH_BYTES = BXW * BYH * (int)sizeof(T);
+    static constexpr int BOXE_BYTES = BXW * BYE * (int)sizeof(T);
+    static constexpr int BOXH_STRIDE = (BOXH_BYTES + 127) / 128 * 128;
+    static constexpr int BOXE_STRIDE = (BOXE_BYTES + 127) / 128 * 128;
+    static constexpr int NH = D + 2, NE = D + 1;
+    static constexpr int EARR = 3 + SAMPLES;
+    static constexpr int HSLOT = 3 * BOXH_STRIDE, ESLOT = EARR * BOXE_STRIDE;
     static constexpr int EBUF = kMarchLanes * kMarchRows;    // one component of the E buffer
-    static constexpr size_t SMEM = (size_t)kMarchStages * STAGE_BYTES + 2 * 3 * EBUF * sizeof(T) + kMarchStages * 8 + 128;
+    static constexpr size_t HRING = (size_t)NH * HSLOT, ERING = (size_t)NE * ESLOT;
+    static constexpr size_t SMEM = HRING + ERING + 2 * 3 * EBUF * sizeof(T) + (NH + NE) * 8;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -74,14 +79,18 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
-// Bounded wait on phase `parity`; false when the limit is reached.
+// Bounded wait on phase `parity`; false when the limit is reached. Each try_wait suspends the
+// warp in hardware for up to kSuspendNs (it wakes when the phase completes), so waiting warps do
+// not take issue slots from the computing ones; the loop bounds the total wait to about 2 s.
+constexpr uint32_t kSuspendNs = 1000000;
+constexpr int kWaitTries = 2000;
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     const uint32_t addr = smem_u32(bar);
-    for (long long it = 0; it < kWaitLimit; ++it) {
+    for (int it = 0; it < kWaitTries; ++it) {
         uint32_t done;
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done) : "r"(addr), "r"(parity), "r"(kSuspendNs) : "memory");
         if (done) return true;
     }
     return false;
@@ -101,22 +110,54 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
-// Slab row of coordinate c, or -1: rows of the low slab first, then of the high slab.
-__device__ __forceinline__ int slab_row(const int *s, int c) {
-    return (c >= s[0] && c < s[1]) ? c - s[0] : (c >= s[2] && c < s[3]) ? (s[1] - s[0]) + (c - s[2]) : -1;
+// Slab row of coordinate c, or -1: rows of the low slab [l0, h0) first, then of the high slab [l1, h1).
+__device__ __forceinline__ int slab_row(int l0, int h0, int l1, int h1, int c) {
+    return (c >= l0 && c < h0) ? c - l0 : (c >= l1 && c < h1) ? (h0 - l0) + (c - l1) : -1;
 }
+#define TFD_SLAB_ROW(args, f, a, c) \
+    slab_row((args).slab[f][a][0], (args).slab[f][a][1], (args).slab[f][a][2], (args).slab[f][a][3], (c))
+// Whether [lo, hi) meets a slab of (family, axis).
+#define TFD_SLAB_MEETS(args, f, a, lo, hi) \
+    (((lo) < (args).slab[f][a][1] && (args).slab[f][a][0] < (hi)) || ((lo) < (args).slab[f][a][3] && (args).slab[f][a][2] < (hi)))
 
 // Index of a CPML memory element (32-bit; the plan bounds every array below 2^31 elements).
 __device__ __forceinline__ int psi_index32(int a, int x, int y, int z, int r, int R, int ny, int pitch) {
     return a == 0 ? (z * ny + y) * R + r : a == 1 ? (z * R + r) * pitch + x : (r * ny + y) * pitch + x;
 }
 
+// CPML coefficients of one slab row: decay b, coupling c, 1/kappa.
 template <typename T>
-__device__ __forceinline__ T cpml_e32(const Grid<T> &g, int par, int a, int j, int coord, int r, int x, int y, int z, bool own, T d) {
+struct Coef { T b, c, k; };
+
+template <typename T>
+__device__ __forceinline__ Coef<T> coef_at(const Grid<T> &g, int f, int a, int coord, int row) {
+    Coef<T> q{T(0), T(0), T(1)};
+    if (row >= 0) {
+        q.b = __ldg(&g.cb[f][a][coord]);
+        q.c = __ldg(&g.cc[f][a][coord]);
+        q.k = __ldg(&g.ck[f][a][coord]);
+    }
+    return q;
+}
+
+// E-family memories of both parities sit one psi_parity apart; `po`/`pn` are the old/new offsets.
+template <typename T>
+__device__ __forceinline__ T cpml_e32(const Grid<T> &g, int po, int pn, int a, int j, const Coef<T> &q, int r, int x, int y, int z,
+                                      bool own, T d) {
     const int p = psi_index32(a, x, y, z, r, g.rows[0][a], g.n[1], g.pitch);
-    const T mem = g.psiE[par][a][j][p] * __ldg(&g.cb[0][a][coord]) + __ldg(&g.cc[0][a][coord]) * d;
-    if (own) g.psiE[par ^ 1][a][j][p] = mem;
-    return d * __ldg(&g.ck[0][a][coord]) + mem;
+    T *base = g.psiE[0][a][j];
+    const T mem = base[po + p] * q.b + q.c * d;
+    if (own) base[pn + p] = mem;
+    return d * q.k + mem;
+}
+
+template <typename T>
+__device__ __forceinline__ T cpml_h32q(const Grid<T> &g, int a, int j, const Coef<T> &q, int r, int x, int y, int z, T d) {
+    const int p = psi_index32(a, x, y, z, r, g.rows[1][a], g.n[1], g.pitch);
+    T *psi = g.psiH[a][j];
+    const T mem = psi[p] * q.b + q.c * d;
+    psi[p] = mem;
+    return d * q.k + mem;
 }
 
 template <typename T>
@@ -154,50 +195,67 @@ __device__ __forceinline__ unsigned source_mask(const Grid<T> &g, int family, in
     return m;
 }
 
-// Per-cell slab rows (E family): x from the lane, y from the warp row, z from the plane.
-struct Rows { int x, y, z; };
+// Per-cell slab rows (E family): x from the lane, y from the warp row, z from the plane, with
+// their coefficients; po/pn: old/new parity offsets of the E-family memories of axis 0, 1, 2.
+template <typename T>
+struct Rows { int x, y, z; int po[3], pn[3]; Coef<T> qx, qy, qz; };
 
 // E_new of component C at stage index s. hk: plane k stage base, hm: plane k-1 stage base.
-template <typename T, int SAMPLES, int C>
-__device__ __forceinline__ T march_e(const Grid<T> &g, int par, const T *hk, const T *hm, int s, int x, int y, int z, bool zprev,
-                                     bool own, Rows rw) {
-    using S = MarchShape<T, SAMPLES>;
-    constexpr int ES = S::BOX_STRIDE / sizeof(T);          // element stride between stage arrays
+// hk / hm: H stage of plane k / k-1 (box row 0 = y0-1, stride HS); ek: E stage of plane k
+// (box row 0 = y0, stride ES); sh / se: the cell's element index in those boxes.
+// FAST: the warp row meets no CPML slab, no domain face and no source, and plane z has a previous
+// plane; the same arithmetic without the checks.
+template <typename T, int SAMPLES, int D, int C, bool FAST = false>
+__device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, int x, int y, int z,
+                                     bool zprev, bool own, const Rows<T> &rw) {
+    using S = MarchShape<T, SAMPLES, D>;
+    constexpr int HS = S::BOXH_STRIDE / sizeof(T);
+    constexpr int ES = S::BOXE_STRIDE / sizeof(T);
     T acc = T(0);
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const Term t = term_of(C, k);
-        const T *h = hk + (3 + t.in) * ES;
+        const T *h = hk + t.in * HS;
         T d;
-        if (t.axis == 0) {
+        if (FAST) {
+            d = t.axis == 0 ? h[s] - h[s - 1] : t.axis == 1 ? h[s] - h[s - S::BXW] : h[s] - hm[t.in * HS + s];
+        } else if (t.axis == 0) {
             const T diff = h[s] - h[s - 1];
             d = x > 0 ? diff : T(0);
-            if (rw.x >= 0) d = cpml_e32(g, par, 0, t.j, x, rw.x, x, y, z, own, d);
+            if (rw.x >= 0) d = cpml_e32(g, rw.po[0], rw.pn[0], 0, t.j, rw.qx, rw.x, x, y, z, own, d);
         } else if (t.axis == 1) {
             const T diff = h[s] - h[s - S::BXW];
             d = y > 0 ? diff : T(0);
-            if (rw.y >= 0) d = cpml_e32(g, par, 1, t.j, y, rw.y, x, y, z, own, d);
+            if (rw.y >= 0) d = cpml_e32(g, rw.po[1], rw.pn[1], 1, t.j, rw.qy, rw.y, x, y, z, own, d);
         } else {
             d = T(0);
             if (zprev) {
-                d = h[s] - hm[(3 + t.in) * ES + s];
-                if (rw.z >= 0) d = cpml_e32(g, par, 2, t.j, z, rw.z, x, y, z, own, d);
+                d = h[s] - hm[t.in * HS + s];
+                if (rw.z >= 0) d = cpml_e32(g, rw.po[2], rw.pn[2], 2, t.j, rw.qz, rw.z, x, y, z, own, d);
             }
         }
         acc = acc + (t.sign > 0 ? d : -d);
     }
-    return hk[C * ES + s] + (g.cn * hk[(6 + (SAMPLES == 3 ? C : 0)) * ES + s]) * acc;
+    return ek[C * ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? C : 0)) * ES + se]) * acc;
 }
 
-template <typename T, int SAMPLES>
-__global__ void __launch_bounds__(kMarchThreads, 2) k_step_march(const __grid_constant__ MarchArgs<T> args) {
-    using S = MarchShape<T, SAMPLES>;
-    constexpr int ES = S::BOX_STRIDE / sizeof(T);
+// D planes of TMA prefetch; MINB CTAs per SM requested from the register allocator.
+template <typename T, int SAMPLES, int D, int MINB>
+__global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid_constant__ MarchArgs<T> args) {
+    using S = MarchShape<T, SAMPLES, D>;
+    constexpr int HS = S::BOXH_STRIDE / sizeof(T);
+    constexpr int ES = S::BOXE_STRIDE / sizeof(T);
     const Grid<T> &g = args.g;
+    // Dynamic shared memory (16-byte aligned, enough for non-swizzled TMA boxes whose strides are
+    // multiples of 128 bytes), addressed as element offsets from the __shared__ array so every access
+    // stays a 32-bit shared-window load.
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
-    T *ebuf = (T *)(smem + (size_t)kMarchStages * S::STAGE_BYTES);
-    uint64_t *bars = (uint64_t *)(ebuf + 2 * 3 * S::EBUF);
+    T *const sm = reinterpret_cast<T *>(smem_raw);
+    constexpr int HSLOT_E = S::HSLOT / sizeof(T), ESLOT_E = S::ESLOT / sizeof(T);
+    constexpr int ERING_OFF = S::HRING / sizeof(T);
+    constexpr int EBUF_OFF = (S::HRING + S::ERING) / sizeof(T);
+    uint64_t *barh = reinterpret_cast<uint64_t *>(smem_raw + S::HRING + S::ERING + 2 * 3 * S::EBUF * sizeof(T));
+    uint64_t *bare = barh + S::NH;
 
     const long long n = *g.counter;
     const int par = (int)(n & 1);
@@ -209,87 +267,142 @@ __global__ void __launch_bounds__(kMarchThreads, 2) k_step_march(const __grid_co
     const bool zper = g.periodic[2] != 0;
     const bool has_prev = z0 > 0 || zper;                    // plane z0-1 exists (wrapped when periodic)
     const bool has_halo = z1 < nz || zper;                   // plane z1 exists (wrapped when periodic)
-    const int planes = (z1 - z0) + 1 + (has_halo ? 1 : 0);  // ring sequence q holds plane z0-1+q
+    const int nh = (z1 - z0) + 1 + (has_halo ? 1 : 0);      // H sequence i holds plane z0-1+i
+    const int ne = (z1 - z0) + (has_halo ? 1 : 0);          // E sequence i holds plane z0+i
     const int bx = (x0 - 1) & ~(S::A - 1);                   // TMA box origin: x0-1 rounded down to 16 bytes
     const int off = x0 - bx;                                 // smem column of x0
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    auto issue = [&](int q) {
-        uint64_t *bar = &bars[q % kMarchStages];
-        T *dst = (T *)(smem + (size_t)(q % kMarchStages) * S::STAGE_BYTES);
-        int z = z0 - 1 + q;
-        const bool exists = (q == 0) ? has_prev : (z < nz || zper);
-        if (z < 0) z += nz;
-        if (z >= nz) z -= nz;
-        if (!exists) {
+    auto wrap = [&](int z) { return z < 0 ? z + nz : (z >= nz ? z - nz : z); };
+    auto issue_h = [&](int i) {
+        uint64_t *bar = &barh[i % S::NH];
+        T *dst = sm + (i % S::NH) * HSLOT_E;
+        const int z = z0 - 1 + i;
+        if (i == 0 && !has_prev) {
             mbar_expect_tx(bar, 0);
             return;
         }
-        mbar_expect_tx(bar, (uint32_t)(S::ARRAYS * S::BOX_BYTES));
+        mbar_expect_tx(bar, (uint32_t)(3 * S::BOXH_BYTES));
 #pragma unroll
-        for (int c = 0; c < 6; ++c) tma_load_4d(dst + c * ES, &args.field[c], bar, bx, y0 - 1, z, par);
+        for (int c = 0; c < 3; ++c) tma_load_4d(dst + c * HS, &args.field[3 + c], bar, bx, y0 - 1, wrap(z), par);
+    };
+    auto issue_e = [&](int i) {
+        uint64_t *bar = &bare[i % S::NE];
+        T *dst = sm + ERING_OFF + (i % S::NE) * ESLOT_E;
+        const int z = wrap(z0 + i);
+        mbar_expect_tx(bar, (uint32_t)(S::EARR * S::BOXE_BYTES));
 #pragma unroll
-        for (int c = 0; c < SAMPLES; ++c) tma_load_3d(dst + (6 + c) * ES, &args.eps[c], bar, bx, y0 - 1, z);
+        for (int c = 0; c < 3; ++c) tma_load_4d(dst + c * ES, &args.field[c], bar, bx, y0, z, par);
+#pragma unroll
+        for (int c = 0; c < SAMPLES; ++c) tma_load_3d(dst + (3 + c) * ES, &args.eps[c], bar, bx, y0, z);
     };
 
     if (tid == 0) {
-        for (int s = 0; s < kMarchStages; ++s) mbar_init(&bars[s], 1);
+        for (int s = 0; s < S::NH + S::NE; ++s) mbar_init(&barh[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (tid == 0)
-        for (int q = 0; q < min(kMarchStages, planes); ++q) issue(q);
+    if (tid == 0) {
+        for (int i = 0; i < min(S::NH, nh); ++i) issue_h(i);
+        for (int i = 0; i < min(S::NE, ne); ++i) issue_e(i);
+    }
 
-    auto stage = [&](int q) { return (const T *)(smem + (size_t)(q % kMarchStages) * S::STAGE_BYTES); };
-    auto wait_stage = [&](int q) -> bool { return mbar_wait(&bars[q % kMarchStages], (uint32_t)((q / kMarchStages) & 1)); };
+    auto hstage = [&](int i) -> const T * { return sm + (i % S::NH) * HSLOT_E; };
+    auto estage = [&](int i) -> const T * { return sm + ERING_OFF + (i % S::NE) * ESLOT_E; };
+    auto wait_h = [&](int i) -> bool { return mbar_wait(&barh[i % S::NH], (uint32_t)((i / S::NH) & 1)); };
+    auto wait_e = [&](int i) -> bool { return mbar_wait(&bare[i % S::NE], (uint32_t)((i / S::NE) & 1)); };
 
-    // Per-thread invariants: column, rows of this warp, CPML slab rows, store offsets.
+    // Per-thread invariants: column, rows of this warp, CPML slab rows and coefficients.
     const int x = x0 + lane;
     const bool lane_own = lane < kMarchOwnX && x < nx;
     const bool lane_in = x < nx;
-    const int rxE = slab_row(args.slab[0][0], x), rxH = slab_row(args.slab[1][0], x);
+    const int rxE = TFD_SLAB_ROW(args, 0, 0, x), rxH = TFD_SLAB_ROW(args, 1, 0, x);
     int yrow[2], ryE[2], ryH[2];
+    Coef<T> qyE[2], qyH[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         yrow[h] = y0 + warp + 8 * h;
-        ryE[h] = slab_row(args.slab[0][1], yrow[h]);
-        ryH[h] = slab_row(args.slab[1][1], yrow[h]);
+        ryE[h] = TFD_SLAB_ROW(args, 0, 1, yrow[h]);
+        ryH[h] = TFD_SLAB_ROW(args, 1, 1, yrow[h]);
+        qyE[h] = coef_at(g, 0, 1, yrow[h], ryE[h]);
+        qyH[h] = coef_at(g, 1, 1, yrow[h], ryH[h]);
     }
-    const int smask_all = g.n_src;
+    const Coef<T> qxE = coef_at(g, 0, 0, x, rxE), qxH = coef_at(g, 1, 0, x, rxH);
+    // Warp-uniform fast-path conditions of this tile (x, y) and of each warp row.
+    const bool tile_in = x0 > 0 && x0 + kMarchLanes <= nx;            // all computed columns inside, x-1 exists
+    const bool fast_x_e = tile_in && !TFD_SLAB_MEETS(args, 0, 0, x0, x0 + kMarchLanes);
+    const bool fast_x_h = x0 + kMarchLanes < nx && !TFD_SLAB_MEETS(args, 1, 0, x0, x0 + kMarchOwnX);
+    bool fast_y_e[2], fast_y_h[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        fast_y_e[h] = yrow[h] > 0 && yrow[h] < ny && ryE[h] < 0;
+        fast_y_h[h] = yrow[h] < ny - 1 && ryH[h] < 0;
+    }
+    // Source terms whose x/y box meets this tile (E: with the halo), tested once per CTA.
+    unsigned tile_src_e = 0, tile_src_h = 0;
+    for (int t = 0; t < g.n_src; ++t) {
+        const SourceTerm &st = g.src[t];
+        const bool e_hit = st.lo[0] < x0 + kMarchLanes && x0 < st.hi[0] && st.lo[1] < y0 + kMarchRows && y0 < st.hi[1];
+        const bool h_hit = st.lo[0] < x0 + kMarchOwnX && x0 < st.hi[0] && st.lo[1] < y0 + kMarchOwnY && y0 < st.hi[1];
+        if (st.family == 0 && e_hit) tile_src_e |= 1u << t;
+        if (st.family == 1 && h_hit) tile_src_h |= 1u << t;
+    }
+    // New-parity offset of the fields; old/new offsets of the E-family CPML memories.
+    const size_t fn = par ? 0 : (size_t)g.count;
+    Rows<T> rw0;
+    for (int a = 0; a < 3; ++a) {
+        rw0.po[a] = par ? args.psi_parity[a] : 0;
+        rw0.pn[a] = par ? 0 : args.psi_parity[a];
+    }
 
-    if (!wait_stage(0)) {
+    if (!wait_h(0)) {
         if (tid == 0) atomicExch(g.status, kStatusPipelineTimeout);
         return;
     }
     for (int k = z0; k <= z1; ++k) {
-        const int q = k - z0 + 1;
+        const int t = k - z0;                                // E sequence index of plane k; H index is t + 1
         const bool halo_plane = k == z1;
         const bool compute_e = !halo_plane || has_halo;
-        if (compute_e && !wait_stage(q)) {
+        if (compute_e && !(wait_h(t + 1) && wait_e(t))) {
             if (tid == 0) atomicExch(g.status, kStatusPipelineTimeout);
             return;
         }
         const int kz = k >= nz ? k - nz : k;
-        T *ecur = ebuf + (k & 1) * 3 * S::EBUF;
-        const T *eprv = ebuf + ((k - 1) & 1) * 3 * S::EBUF;
+        T *ecur = sm + EBUF_OFF + (k & 1) * 3 * S::EBUF;
+        const T *eprv = sm + EBUF_OFF + ((k - 1) & 1) * 3 * S::EBUF;
         if (compute_e) {
-            const T *hk = stage(q), *hm = stage(q - 1);
+            const T *hk = hstage(t + 1), *hm = hstage(t), *ek = estage(t);
             const bool zprev = kz > 0 || zper;
-            const int rzE = slab_row(args.slab[0][2], kz);
-            const unsigned smask = smask_all ? source_mask(g, 0, x0, x0 + kMarchLanes, y0, y0 + kMarchRows, kz, n) : 0u;
-            T *gE0 = g.E[par ^ 1][0] + (size_t)kz * g.plane, *gE1 = g.E[par ^ 1][1] + (size_t)kz * g.plane,
-              *gE2 = g.E[par ^ 1][2] + (size_t)kz * g.plane;
+            const int rzE = TFD_SLAB_ROW(args, 0, 2, kz);
+            const Coef<T> qzE = coef_at(g, 0, 2, kz, rzE);
+            const unsigned smask = tile_src_e ? source_mask(g, 0, x0, x0 + kMarchLanes, y0, y0 + kMarchRows, kz, n) & tile_src_e : 0u;
+            T *gE0 = g.E[0][0] + fn + (size_t)kz * g.plane, *gE1 = g.E[0][1] + fn + (size_t)kz * g.plane,
+              *gE2 = g.E[0][2] + fn + (size_t)kz * g.plane;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int r = warp + 8 * h;
                 const int y = yrow[h];
                 if (!lane_in || y >= ny) continue;
                 const bool own = !halo_plane && lane_own && r < kMarchOwnY;
-                const int s = (r + 1) * S::BXW + off + lane;
-                const Rows rw{rxE, ryE[h], rzE};
-                T ex = march_e<T, SAMPLES, 0>(g, par, hk, hm, s, x, y, kz, zprev, own, rw);
-                T ey = march_e<T, SAMPLES, 1>(g, par, hk, hm, s, x, y, kz, zprev, own, rw);
-                T ez = march_e<T, SAMPLES, 2>(g, par, hk, hm, s, x, y, kz, zprev, own, rw);
+                const int sh = (r + 1) * S::BXW + off + lane;
+                const int se = r * S::BXW + off + lane;
+                Rows<T> rw = rw0;
+                rw.x = rxE;
+                rw.y = ryE[h];
+                rw.z = rzE;
+                rw.qx = qxE;
+                rw.qy = qyE[h];
+                rw.qz = qzE;
+                T ex, ey, ez;
+                if (fast_x_e && fast_y_e[h] && zprev && rzE < 0 && !smask) {
+                    ex = march_e<T, SAMPLES, D, 0, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
+                    ey = march_e<T, SAMPLES, D, 1, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
+                    ez = march_e<T, SAMPLES, D, 2, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
+                } else {
+                    ex = march_e<T, SAMPLES, D, 0>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
+                    ey = march_e<T, SAMPLES, D, 1>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
+                    ez = march_e<T, SAMPLES, D, 2>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
+                }
                 if (smask) {
                     ex = inject_masked(g, smask, 0, 0, n, x, y, kz, ex);
                     ey = inject_masked(g, smask, 0, 1, n, x, y, kz, ey);
@@ -308,66 +421,89 @@ __global__ void __launch_bounds__(kMarchThreads, 2) k_step_march(const __grid_co
             }
         }
         __syncthreads();
+        // The E slot of plane k is free: refill it D+1 planes ahead.
+        if (tid == 0 && compute_e && t + S::NE < ne) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue_e(t + S::NE);
+        }
         if (k > z0) {
             // H_new(k-1) on the owned tile.
             const int km = k - 1;
-            const T *hs = stage(q - 1);
+            const T *hs = hstage(t);
             const bool znext = compute_e;
-            const int rzH = slab_row(args.slab[1][2], km);
-            const unsigned hmask = smask_all ? source_mask(g, 1, x0, x0 + kMarchOwnX, y0, y0 + kMarchOwnY, km, n) : 0u;
-            T *gH[3] = {g.H[par ^ 1][0] + (size_t)km * g.plane, g.H[par ^ 1][1] + (size_t)km * g.plane,
-                        g.H[par ^ 1][2] + (size_t)km * g.plane};
+            const int rzH = TFD_SLAB_ROW(args, 1, 2, km);
+            const Coef<T> qzH = coef_at(g, 1, 2, km, rzH);
+            const unsigned hmask = tile_src_h ? source_mask(g, 1, x0, x0 + kMarchOwnX, y0, y0 + kMarchOwnY, km, n) & tile_src_h : 0u;
+            T *gH[3] = {g.H[0][0] + fn + (size_t)km * g.plane, g.H[0][1] + fn + (size_t)km * g.plane,
+                        g.H[0][2] + fn + (size_t)km * g.plane};
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int r = warp + 8 * h;
                 const int y = yrow[h];
                 if (!lane_own || r >= kMarchOwnY || y >= ny) continue;
-                const int s = (r + 1) * S::BXW + off + lane;
+                const int sh = (r + 1) * S::BXW + off + lane;
                 const int e = r * kMarchLanes + lane;
                 const int i = y * g.pitch + x;
+                if (fast_x_h && fast_y_h[h] && znext && rzH < 0 && !hmask) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const Term t0 = term_of(c, 0), t1 = term_of(c, 1);
+                        auto dif = [&](const Term &tm) -> T {
+                            const T *ep = eprv + tm.in * S::EBUF;
+                            return tm.axis == 0 ? ep[e + 1] - ep[e]
+                                 : tm.axis == 1 ? ep[e + kMarchLanes] - ep[e] : ecur[tm.in * S::EBUF + e] - ep[e];
+                        };
+                        const T d0 = dif(t0), d1 = dif(t1);
+                        T acc = T(0);
+                        acc = acc + (t0.sign > 0 ? d0 : -d0);
+                        acc = acc + (t1.sign > 0 ? d1 : -d1);
+                        gH[c][i] = hs[c * HS + sh] - g.cn * acc;
+                    }
+                    continue;
+                }
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     T acc = T(0);
 #pragma unroll
                     for (int kk = 0; kk < 2; ++kk) {
-                        const Term t = term_of(c, kk);
-                        const T *ep = eprv + t.in * S::EBUF;
+                        const Term tm = term_of(c, kk);
+                        const T *ep = eprv + tm.in * S::EBUF;
                         T d = T(0);
-                        if (t.axis == 0) {
+                        if (tm.axis == 0) {
                             if (x < nx - 1) {
                                 d = ep[e + 1] - ep[e];
-                                if (rxH >= 0) d = cpml_h32(g, 0, t.j, x, rxH, x, y, km, d);
+                                if (rxH >= 0) d = cpml_h32q(g, 0, tm.j, qxH, rxH, x, y, km, d);
                             } else if (g.pec_on[0]) {
                                 d = g.pec_neg[0] * ep[e];
                             }
-                        } else if (t.axis == 1) {
+                        } else if (tm.axis == 1) {
                             if (y < ny - 1) {
                                 d = ep[e + kMarchLanes] - ep[e];
-                                if (ryH[h] >= 0) d = cpml_h32(g, 1, t.j, y, ryH[h], x, y, km, d);
+                                if (ryH[h] >= 0) d = cpml_h32q(g, 1, tm.j, qyH[h], ryH[h], x, y, km, d);
                             } else if (g.pec_on[1]) {
                                 d = g.pec_neg[1] * ep[e];
                             }
                         } else {
                             if (znext) {
-                                d = ecur[t.in * S::EBUF + e] - ep[e];
-                                if (rzH >= 0) d = cpml_h32(g, 2, t.j, km, rzH, x, y, km, d);
+                                d = ecur[tm.in * S::EBUF + e] - ep[e];
+                                if (rzH >= 0) d = cpml_h32q(g, 2, tm.j, qzH, rzH, x, y, km, d);
                             } else if (g.pec_on[2]) {
                                 d = g.pec_neg[2] * ep[e];
                             }
                         }
-                        acc = acc + (t.sign > 0 ? d : -d);
+                        acc = acc + (tm.sign > 0 ? d : -d);
                     }
-                    T hv = hs[(3 + c) * ES + s] - g.cn * acc;
+                    T hv = hs[c * HS + sh] - g.cn * acc;
                     if (hmask) hv = inject_masked(g, hmask, 1, c, n, x, y, km, hv);
                     gH[c][i] = hv;
                 }
             }
         }
         __syncthreads();
-        // Stage q-1 is free: refill it with plane q-1+S.
-        if (tid == 0 && q - 1 + kMarchStages < planes) {
+        // The H slot of plane k-1 is free: refill it D+2 planes ahead.
+        if (tid == 0 && t + S::NH < nh) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(q - 1 + kMarchStages);
+            issue_h(t + S::NH);
         }
     }
 }
