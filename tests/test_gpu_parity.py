@@ -173,6 +173,34 @@ def test_z_faces_periodic_and_pec_match_oracle(kernel, zfaces):
 
 
 @pytest.mark.parametrize('kernel', KERNELS)
+@pytest.mark.parametrize('precision', ['float32', 'float64'])
+def test_interior_and_boundary_tiles_match_oracle(kernel, precision):
+    """A grid large enough for interior tiles (lean kernel, prefetched z-CPML memories) and boundary
+    strips (general kernel) in one step, with sources in the interior and a DFT plane."""
+    from torchfdtd_b200.models import FieldMonitor, Source, SpectrumSettings, Structure
+    region = Region(dimension='3d', size=(5.0, 3.0, 1.5), mesh=.05, pml_cells=6, steps=24, precision=precision, backend='cuda')
+    project = Project(region=region, structures=[Structure(kind='sphere', radius=.6, material='Si (constant n)')],
+                      sources=[Source(center=(-.4, .1, 0), component='Ez', pulse_cycles=1, wavelength=1.0),
+                               Source(center=(.6, -.2, .1), component='Hx', pulse_cycles=1, wavelength=1.0, amplitude=.2)],
+                      monitors=[FieldMonitor(center=(.9, 0, 0), size=(0, 1.2, .6),
+                                             spectrum=SpectrumSettings(sampling='frequency', frequency_points=2, apodization='none'))])
+    plan = plan_grid(project)
+    rng = np.random.default_rng(5)
+    oracle = YeeOracle(plan)
+    oracle.E[:] = rng.normal(size=oracle.E.shape).astype(plan.dtype) * .01
+    oracle.H[:] = rng.normal(size=oracle.H.shape).astype(plan.dtype) * .01
+    g = native(plan, kernel)
+    g.set_fields(oracle.E, oracle.H)
+    oracle.run()
+    g.step(plan.steps)
+    E, H = g.get_fields()
+    np.testing.assert_array_equal(E, oracle.E)
+    np.testing.assert_array_equal(H, oracle.H)
+    for got, want in zip(g.get_psi(), oracle.memory_states):
+        np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize('kernel', KERNELS)
 def test_graph_replay_equals_eager_steps(kernel):
     import torch
     project = random_project('3d', 'float32', steps=30)

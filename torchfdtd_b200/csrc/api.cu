@@ -256,6 +256,18 @@ struct tfd_plan {
     MarchArgs<double> md;
     dim3 march_grid;
     size_t march_smem = 0;
+    struct MarchLaunch { int mode; dim3 grid; int tx_off, ty_off, lz; };
+    std::vector<MarchLaunch> march_launches;
+    // Boundary strips run on auxiliary streams, forked from and joined back to the caller's stream
+    // (a CUDA graph capture records them as parallel branches).
+    std::vector<cudaStream_t> aux;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    ~tfd_plan() {
+        for (auto st : aux) cudaStreamDestroy(st);
+        for (auto ev : join) cudaEventDestroy(ev);
+        if (fork) cudaEventDestroy(fork);
+    }
     int march_variant = 42;
     std::vector<int> seg_f, seg_a, seg_lo, seg_hi;
 
@@ -517,37 +529,94 @@ int setup_march_s(tfd_plan *p) {
         if (r != CUDA_SUCCESS) return fail(TFD_ERR_CUDA, "cuTensorMapEncodeTiled(eps) failed: " + std::to_string((int)r));
     }
     p->march_smem = S::SMEM;
-    TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
+    TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
+    TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
     int device = 0, sms = 148, per_sm = 1;
     TFD_CUDA(cudaGetDevice(&device));
     TFD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    TFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_march<T, SAMPLES, D, MINB>, kMarchThreads, p->march_smem));
+    TFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_march<T, SAMPLES, D, MINB, 1>, kMarchThreads, p->march_smem));
     const long long resident = (long long)sms * std::max(1, per_sm);
     const int tx = (g.n[0] + kMarchOwnX - 1) / kMarchOwnX, ty = (g.n[1] + kMarchOwnY - 1) / kMarchOwnY;
-    const long long tiles = (long long)tx * ty;
-    // Planes per chunk: balance whole waves of resident CTAs against the two extra planes a chunk loads.
-    double best = -1;
-    int best_lz = g.n[2];
-    for (int chunks = 1; chunks <= std::max(1, g.n[2] / 4); ++chunks) {
-        const int lz = (g.n[2] + chunks - 1) / chunks;
-        const long long real_chunks = (g.n[2] + lz - 1) / lz;
-        const long long ctas = tiles * real_chunks;
-        const double waves = std::ceil((double)ctas / resident);
-        const double eff = (double)ctas / (waves * resident) * ((double)lz / (lz + 2));
-        if (eff > best + 1e-9) { best = eff; best_lz = lz; }
+    // Planes per chunk for a launch of `tiles` tiles sharing `share` of the resident CTA slots: balance
+    // whole waves against the two extra planes a chunk loads.
+    auto choose_lz = [&](long long tiles, double share) {
+        const double slots = std::max(1.0, share * resident);
+        double best = -1;
+        int best_lz = g.n[2];
+        for (int chunks = 1; chunks <= std::max(1, g.n[2] / 4); ++chunks) {
+            const int lz = (g.n[2] + chunks - 1) / chunks;
+            const long long ctas = tiles * ((g.n[2] + lz - 1) / lz);
+            const double waves = std::ceil(ctas / slots);
+            const double eff = ctas / (waves * slots) * ((double)lz / (lz + 2));
+            if (eff > best + 1e-9) { best = eff; best_lz = lz; }
+        }
+        return best_lz;
+    };
+    auto chunks_of = [&](int lz) { return (unsigned)((g.n[2] + lz - 1) / lz); };
+    const int lz_all = choose_lz((long long)tx * ty, 1.0);
+    p->march_grid = dim3(tx, ty, chunks_of(lz_all));
+    // Interior tiles: all 32 x 16 computed cells inside the domain, x-1 / y-1 present, H neighbours
+    // x+1 / y+1 present, and no E or H CPML slab on x or y. They form a contiguous tile range.
+    auto meets = [&](int f, int ax, int lo, int hi) {
+        const int *b = a.slab[f][ax];
+        return (lo < b[1] && b[0] < hi) || (lo < b[3] && b[2] < hi);
+    };
+    auto interior_x = [&](int t) {
+        const int x0 = t * kMarchOwnX;
+        return x0 > 0 && x0 + kMarchLanes < g.n[0] && !meets(0, 0, x0, x0 + kMarchLanes) && !meets(1, 0, x0, x0 + kMarchOwnX);
+    };
+    auto interior_y = [&](int t) {
+        const int y0 = t * kMarchOwnY;
+        return y0 > 0 && y0 + kMarchRows < g.n[1] && !meets(0, 1, y0, y0 + kMarchRows) && !meets(1, 1, y0, y0 + kMarchOwnY);
+    };
+    int ix0 = 0, ix1 = 0, iy0 = 0, iy1 = 0;
+    while (ix0 < tx && !interior_x(ix0)) ++ix0;
+    ix1 = ix0;
+    while (ix1 < tx && interior_x(ix1)) ++ix1;
+    while (iy0 < ty && !interior_y(iy0)) ++iy0;
+    iy1 = iy0;
+    while (iy1 < ty && interior_y(iy1)) ++iy1;
+    p->march_launches.clear();
+    // The interior/boundary split is off by default: measured on B200 at 512x512x256 it is slower
+    // (50.6 vs 54.8 Gcell/s) than one general launch; TFD_MARCH_SPLIT=1 enables it.
+    const char *split = getenv("TFD_MARCH_SPLIT");
+    if (ix1 > ix0 && iy1 > iy0 && split && std::string(split) == "1") {
+        const long long all = (long long)tx * ty, inner = (long long)(ix1 - ix0) * (iy1 - iy0);
+        const double inner_share = (double)inner / all, strip_share = 1.0 - inner_share;
+        const int lzi = choose_lz(inner, inner_share);
+        p->march_launches.push_back({1, dim3(ix1 - ix0, iy1 - iy0, chunks_of(lzi)), ix0, iy0, lzi});
+        auto strip = [&](int sx, int sy, int ox, int oy) {
+            const int lzs = choose_lz((long long)sx * sy, strip_share * sx * sy / std::max(1LL, all - inner));
+            p->march_launches.push_back({0, dim3(sx, sy, chunks_of(lzs)), ox, oy, lzs});
+        };
+        if (ix0 > 0) strip(ix0, ty, 0, 0);
+        if (ix1 < tx) strip(tx - ix1, ty, ix1, 0);
+        if (iy0 > 0) strip(ix1 - ix0, iy0, ix0, 0);
+        if (iy1 < ty) strip(ix1 - ix0, ty - iy1, ix0, iy1);
+    } else {
+        p->march_launches.push_back({0, dim3(tx, ty, chunks_of(lz_all)), 0, 0, lz_all});
     }
-    a.lz = best_lz;
-    p->march_grid = dim3(tx, ty, (g.n[2] + best_lz - 1) / best_lz);
+    if (p->aux.empty() && p->march_launches.size() > 1) {
+        TFD_CUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
+        for (size_t k = 1; k < p->march_launches.size(); ++k) {
+            cudaStream_t st;
+            cudaEvent_t ev;
+            TFD_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            TFD_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            p->aux.push_back(st);
+            p->join.push_back(ev);
+        }
+    }
     p->march_variant = D * 10 + MINB;
     return TFD_OK;
 }
 
 // Prefetch depth D / CTAs per SM of the marching kernel, as the two digits of a variant:
-// 23 (FP32 default), 32, 14 and 22 (FP64 default). TFD_MARCH_VARIANT overrides it for launch-shape sweeps.
+// 14 (FP32 default), 23, 32 and 22 (FP64 default). TFD_MARCH_VARIANT overrides it for launch-shape sweeps.
 template <typename T>
 int setup_march(tfd_plan *p) {
     const char *env = getenv("TFD_MARCH_VARIANT");
-    const std::string v = env ? env : (sizeof(T) == 4 ? "23" : "22");
+    const std::string v = env ? env : (sizeof(T) == 4 ? "14" : "22");
     const bool three = p->desc.material_samples == 3;
     if (sizeof(T) == 8 || v == "22") return three ? setup_march_s<T, 3, 2, 2>(p) : setup_march_s<T, 1, 2, 2>(p);
     if (v == "32") return three ? setup_march_s<T, 3, 3, 2>(p) : setup_march_s<T, 1, 3, 2>(p);
@@ -557,7 +626,19 @@ int setup_march(tfd_plan *p) {
 
 template <typename T, int SAMPLES, int D, int MINB>
 void launch_march(tfd_plan *p, cudaStream_t s) {
-    k_step_march<T, SAMPLES, D, MINB><<<p->march_grid, kMarchThreads, p->march_smem, s>>>(p->march<T>());
+    const size_t n = p->march_launches.size();
+    if (n > 1) cudaEventRecord(p->fork, s);
+    for (size_t k = 0; k < n; ++k) {
+        const auto &l = p->march_launches[k];
+        cudaStream_t st = k == 0 ? s : p->aux[k - 1];
+        if (k > 0) cudaStreamWaitEvent(st, p->fork, 0);
+        if (l.mode == 1)
+            k_step_march<T, SAMPLES, D, MINB, 1><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz);
+        else
+            k_step_march<T, SAMPLES, D, MINB, 0><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz);
+        if (k > 0) cudaEventRecord(p->join[k - 1], st);
+    }
+    for (size_t k = 1; k < n; ++k) cudaStreamWaitEvent(s, p->join[k - 1], 0);
 }
 
 template <typename T>
@@ -565,9 +646,9 @@ void launch_march_any(tfd_plan *p, cudaStream_t s) {
     const bool three = p->desc.material_samples == 3;
     switch (p->march_variant) {
         case 23: three ? launch_march<T, 3, 2, 3>(p, s) : launch_march<T, 1, 2, 3>(p, s); break;
+        case 22: three ? launch_march<T, 3, 2, 2>(p, s) : launch_march<T, 1, 2, 2>(p, s); break;
         case 32: three ? launch_march<T, 3, 3, 2>(p, s) : launch_march<T, 1, 3, 2>(p, s); break;
-        case 14: three ? launch_march<T, 3, 1, 4>(p, s) : launch_march<T, 1, 1, 4>(p, s); break;
-        default: three ? launch_march<T, 3, 2, 2>(p, s) : launch_march<T, 1, 2, 2>(p, s); break;
+        default: three ? launch_march<T, 3, 1, 4>(p, s) : launch_march<T, 1, 1, 4>(p, s); break;
     }
 }
 

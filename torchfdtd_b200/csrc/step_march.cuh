@@ -44,7 +44,6 @@ struct MarchArgs {
     CUtensorMap field[6];        // Ex Ey Ez Hx Hy Hz: dims (nx, ny, nz, parity), box (BXW, BY, 1, 1)
     CUtensorMap eps[3];          // inverse permittivity per stored sample: dims (nx, ny, nz), box (BXW, BY, 1)
     Grid<T> g;
-    int lz;                      // planes per chunk
     int slab[2][3][4];           // per family and axis: lo0, hi0, lo1, hi1 of the two CPML slabs
     int psi_parity[3];           // elements between the two parities of an E-family CPML memory, per axis
 };
@@ -205,9 +204,10 @@ struct Rows { int x, y, z; int po[3], pn[3]; Coef<T> qx, qy, qz; };
 // (box row 0 = y0, stride ES); sh / se: the cell's element index in those boxes.
 // FAST: the warp row meets no CPML slab, no domain face and no source, and plane z has a previous
 // plane; the same arithmetic without the checks.
-template <typename T, int SAMPLES, int D, int C, bool FAST = false>
+// PZ: the z-term's old CPML memory comes from pz[j] (prefetched by the caller) instead of a load.
+template <typename T, int SAMPLES, int D, int C, bool FAST = false, bool PZ = false>
 __device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, int x, int y, int z,
-                                     bool zprev, bool own, const Rows<T> &rw) {
+                                     bool zprev, bool own, const Rows<T> &rw, const T *pz = nullptr) {
     using S = MarchShape<T, SAMPLES, D>;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
@@ -219,6 +219,10 @@ __device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm,
         T d;
         if (FAST) {
             d = t.axis == 0 ? h[s] - h[s - 1] : t.axis == 1 ? h[s] - h[s - S::BXW] : h[s] - hm[t.in * HS + s];
+        } else if (PZ && t.axis == 0) {       // interior tile: x > 0, no x slab
+            d = h[s] - h[s - 1];
+        } else if (PZ && t.axis == 1) {       // interior tile: y > 0, no y slab
+            d = h[s] - h[s - S::BXW];
         } else if (t.axis == 0) {
             const T diff = h[s] - h[s - 1];
             d = x > 0 ? diff : T(0);
@@ -231,7 +235,16 @@ __device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm,
             d = T(0);
             if (zprev) {
                 d = h[s] - hm[t.in * HS + s];
-                if (rw.z >= 0) d = cpml_e32(g, rw.po[2], rw.pn[2], 2, t.j, rw.qz, rw.z, x, y, z, own, d);
+                if (rw.z >= 0) {
+                    if (PZ) {
+                        const T mem = pz[t.j] * rw.qz.b + rw.qz.c * d;
+                        if (own)
+                            g.psiE[0][2][t.j][rw.pn[2] + psi_index32(2, x, y, z, rw.z, g.rows[0][2], g.n[1], g.pitch)] = mem;
+                        d = d * rw.qz.k + mem;
+                    } else {
+                        d = cpml_e32(g, rw.po[2], rw.pn[2], 2, t.j, rw.qz, rw.z, x, y, z, own, d);
+                    }
+                }
             }
         }
         acc = acc + (t.sign > 0 ? d : -d);
@@ -240,9 +253,16 @@ __device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm,
 }
 
 // D planes of TMA prefetch; MINB CTAs per SM requested from the register allocator.
-template <typename T, int SAMPLES, int D, int MINB>
-__global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid_constant__ MarchArgs<T> args) {
+// MODE 0 (general) runs any tile; MODE 1 (interior) runs tiles whose computed 32 x 16 cells lie
+// inside the domain and outside every x/y CPML slab (the host launches it over that tile range and
+// the general kernel over the boundary strips), so only the z-CPML memories remain, and those are
+// loaded into registers at the top of each plane, ahead of the TMA wait. Tile (tx, ty) of a launch
+// is (blockIdx.x + tx_off, blockIdx.y + ty_off); lz planes per z chunk (blockIdx.z).
+template <typename T, int SAMPLES, int D, int MINB, int MODE>
+__global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid_constant__ MarchArgs<T> args, int tx_off, int ty_off,
+                                                                    int lz) {
     using S = MarchShape<T, SAMPLES, D>;
+    constexpr bool INTERIOR = MODE == 1;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
     const Grid<T> &g = args.g;
@@ -260,10 +280,10 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     const long long n = *g.counter;
     const int par = (int)(n & 1);
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
-    const int x0 = blockIdx.x * kMarchOwnX, y0 = blockIdx.y * kMarchOwnY;
-    const int z0 = blockIdx.z * args.lz;
+    const int x0 = (blockIdx.x + tx_off) * kMarchOwnX, y0 = (blockIdx.y + ty_off) * kMarchOwnY;
+    const int z0 = blockIdx.z * lz;
     if (z0 >= nz) return;
-    const int z1 = min(z0 + args.lz, nz);
+    const int z1 = min(z0 + lz, nz);
     const bool zper = g.periodic[2] != 0;
     const bool has_prev = z0 > 0 || zper;                    // plane z0-1 exists (wrapped when periodic)
     const bool has_halo = z1 < nz || zper;                   // plane z1 exists (wrapped when periodic)
@@ -330,13 +350,13 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     const Coef<T> qxE = coef_at(g, 0, 0, x, rxE), qxH = coef_at(g, 1, 0, x, rxH);
     // Warp-uniform fast-path conditions of this tile (x, y) and of each warp row.
     const bool tile_in = x0 > 0 && x0 + kMarchLanes <= nx;            // all computed columns inside, x-1 exists
-    const bool fast_x_e = tile_in && !TFD_SLAB_MEETS(args, 0, 0, x0, x0 + kMarchLanes);
-    const bool fast_x_h = x0 + kMarchLanes < nx && !TFD_SLAB_MEETS(args, 1, 0, x0, x0 + kMarchOwnX);
+    const bool fast_x_e = INTERIOR || (tile_in && !TFD_SLAB_MEETS(args, 0, 0, x0, x0 + kMarchLanes));
+    const bool fast_x_h = INTERIOR || (x0 + kMarchLanes < nx && !TFD_SLAB_MEETS(args, 1, 0, x0, x0 + kMarchOwnX));
     bool fast_y_e[2], fast_y_h[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-        fast_y_e[h] = yrow[h] > 0 && yrow[h] < ny && ryE[h] < 0;
-        fast_y_h[h] = yrow[h] < ny - 1 && ryH[h] < 0;
+        fast_y_e[h] = INTERIOR || (yrow[h] > 0 && yrow[h] < ny && ryE[h] < 0);
+        fast_y_h[h] = INTERIOR || (yrow[h] < ny - 1 && ryH[h] < 0);
     }
     // Source terms whose x/y box meets this tile (E: with the halo), tested once per CTA.
     unsigned tile_src_e = 0, tile_src_h = 0;
@@ -363,6 +383,30 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
         const int t = k - z0;                                // E sequence index of plane k; H index is t + 1
         const bool halo_plane = k == z1;
         const bool compute_e = !halo_plane || has_halo;
+        // Interior tiles: issue this plane's z-slab CPML memory loads before waiting for the TMA stages.
+        T pzE[2][2], pzH[2][2];
+        int rzE_pre = -1, rzH_pre = -1;
+        if (INTERIOR) {
+            const int kzp = k >= nz ? k - nz : k;
+            rzE_pre = compute_e && (kzp > 0 || zper) ? TFD_SLAB_ROW(args, 0, 2, kzp) : -1;
+            rzH_pre = k > z0 ? TFD_SLAB_ROW(args, 1, 2, k - 1) : -1;
+            if (rzE_pre >= 0) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    if (yrow[h] < ny)
+#pragma unroll
+                        for (int j = 0; j < 2; ++j)
+                            pzE[h][j] = g.psiE[0][2][j][rw0.po[2] + psi_index32(2, x, yrow[h], kzp, rzE_pre, g.rows[0][2], ny, g.pitch)];
+            }
+            if (rzH_pre >= 0) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    if (yrow[h] < ny && warp + 8 * h < kMarchOwnY && lane_own)
+#pragma unroll
+                        for (int j = 0; j < 2; ++j)
+                            pzH[h][j] = g.psiH[2][j][psi_index32(2, x, yrow[h], k - 1, rzH_pre, g.rows[1][2], ny, g.pitch)];
+            }
+        }
         if (compute_e && !(wait_h(t + 1) && wait_e(t))) {
             if (tid == 0) atomicExch(g.status, kStatusPipelineTimeout);
             return;
@@ -398,6 +442,11 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                     ex = march_e<T, SAMPLES, D, 0, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
                     ey = march_e<T, SAMPLES, D, 1, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
                     ez = march_e<T, SAMPLES, D, 2, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
+                } else if (INTERIOR) {
+                    // only the z-CPML memories and sources can apply here
+                    ex = march_e<T, SAMPLES, D, 0, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw, pzE[h]);
+                    ey = march_e<T, SAMPLES, D, 1, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw, pzE[h]);
+                    ez = march_e<T, SAMPLES, D, 2, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw, pzE[h]);
                 } else {
                     ex = march_e<T, SAMPLES, D, 0>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
                     ey = march_e<T, SAMPLES, D, 1>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
@@ -470,14 +519,18 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                         const T *ep = eprv + tm.in * S::EBUF;
                         T d = T(0);
                         if (tm.axis == 0) {
-                            if (x < nx - 1) {
+                            if (INTERIOR) {
+                                d = ep[e + 1] - ep[e];
+                            } else if (x < nx - 1) {
                                 d = ep[e + 1] - ep[e];
                                 if (rxH >= 0) d = cpml_h32q(g, 0, tm.j, qxH, rxH, x, y, km, d);
                             } else if (g.pec_on[0]) {
                                 d = g.pec_neg[0] * ep[e];
                             }
                         } else if (tm.axis == 1) {
-                            if (y < ny - 1) {
+                            if (INTERIOR) {
+                                d = ep[e + kMarchLanes] - ep[e];
+                            } else if (y < ny - 1) {
                                 d = ep[e + kMarchLanes] - ep[e];
                                 if (ryH[h] >= 0) d = cpml_h32q(g, 1, tm.j, qyH[h], ryH[h], x, y, km, d);
                             } else if (g.pec_on[1]) {
@@ -486,7 +539,15 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                         } else {
                             if (znext) {
                                 d = ecur[tm.in * S::EBUF + e] - ep[e];
-                                if (rzH >= 0) d = cpml_h32q(g, 2, tm.j, qzH, rzH, x, y, km, d);
+                                if (rzH >= 0) {
+                                    if (INTERIOR) {
+                                        const T mem = pzH[h][tm.j] * qzH.b + qzH.c * d;
+                                        g.psiH[2][tm.j][psi_index32(2, x, y, km, rzH, g.rows[1][2], ny, g.pitch)] = mem;
+                                        d = d * qzH.k + mem;
+                                    } else {
+                                        d = cpml_h32q(g, 2, tm.j, qzH, rzH, x, y, km, d);
+                                    }
+                                }
                             } else if (g.pec_on[2]) {
                                 d = g.pec_neg[2] * ep[e];
                             }
