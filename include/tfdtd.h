@@ -170,6 +170,18 @@ int tfd_counter(tfd_plan *plan, int64_t *value, void *stream);
 /* The device status word: 0, or the code a kernel recorded (synchronises the stream). */
 int tfd_device_status(tfd_plan *plan, int32_t *status, void *stream);
 
+/* Field energy and peak without any device allocation and without a plan. No counterpart in the
+ * reference. For callers that cannot allocate device memory: a health check that runs after an
+ * out-of-memory failure (when an allocation would fail again), or a host whose device memory belongs to
+ * a pool or budget it must not bypass. E, H: (cells, 3) and inv_eps: (cells, material_samples) device
+ * arrays in the field precision (4 or 8); out: 2 device doubles, set to the sum of E^2/inv_eps + H^2 and
+ * to max |E|, |H| (NaN if a field value is NaN) -- the first two values tfd_diagnose reports. Scratch is a
+ * static 32 KiB device array inside the library, so at most 67,108,864 cells are accepted (larger inputs
+ * return TFD_ERR_INVALID; use tfd_diagnose). The first call on a device looks the array up and should
+ * come before any stream capture; calls that overlap on the GPU share the array and race. */
+int tfd_field_norm_static(const void *E, const void *H, const void *inv_eps, int64_t cells, int32_t material_samples,
+                          int32_t precision, double *out, void *stream);
+
 /* Which step kernel the plan runs (enum tfd_kernel) after TFD_KERNEL_AUTO is resolved. */
 int tfd_kernel_in_use(const tfd_plan *plan, int32_t *kernel);
 

@@ -242,6 +242,10 @@ void compute_layout(const tfd_desc *d, Layout &L) {
 
 }  // namespace
 
+namespace tfd {
+void set_error(const std::string &msg) { g_error = msg; }
+}  // namespace tfd
+
 struct tfd_plan {
     tfd_desc desc;               // sizes and flags only; host pointers are not kept
     Layout L;

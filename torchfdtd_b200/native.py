@@ -78,6 +78,7 @@ SIGNATURES = {
     'tfd_counter': (ctypes.c_int, [c_vp, P_i64, c_vp]),
     'tfd_device_status': (ctypes.c_int, [c_vp, P_i32, c_vp]),
     'tfd_kernel_in_use': (ctypes.c_int, [c_vp, P_i32]),
+    'tfd_field_norm_static': (ctypes.c_int, [c_vp, c_vp, c_vp, c_i64, c_i32, c_i32, c_vp, c_vp]),
     'tfd_error_string': (ctypes.c_char_p, [ctypes.c_int]),
     'tfd_last_error': (ctypes.c_char_p, []),
 }
@@ -295,6 +296,15 @@ class NativeGrid:
         c = ['Ex', 'Ey', 'Ez', 'Hx', 'Hy', 'Hz'].index(component) if isinstance(component, str) else int(component)
         check(library().tfd_get_slice(self.handle, c, axis, int(index), c_vp(out.ctypes.data), TFD_HOST, _stream()))
         return out
+
+    def field_norm_static(self, E, H, inv_eps, out):
+        """Energy and peak of device tensors E, H (cells x 3) and inv_eps through the allocation-free entry
+        point; `out` is a 2-element float64 device tensor. For callers that must not allocate (see
+        include/tfdtd.h)."""
+        cells = E.numel() // 3
+        samples = inv_eps.numel() // max(cells, 1)
+        check(library().tfd_field_norm_static(c_vp(E.data_ptr()), c_vp(H.data_ptr()), c_vp(inv_eps.data_ptr()), cells, samples,
+                                              E.element_size(), c_vp(out.data_ptr()), _stream()))
 
     def diagnose(self):
         out = (ctypes.c_double * 3)()
