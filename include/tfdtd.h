@@ -49,7 +49,7 @@ enum tfd_code {
 
 enum tfd_face { TFD_FACE_PML = 0, TFD_FACE_PERIODIC = 1, TFD_FACE_PEC = 2 };
 enum tfd_where { TFD_DEVICE = 0, TFD_HOST = 1 };
-enum tfd_kernel { TFD_KERNEL_AUTO = 0, TFD_KERNEL_MARCH = 1, TFD_KERNEL_GATHER = 2 };
+enum tfd_kernel { TFD_KERNEL_AUTO = 0, TFD_KERNEL_MARCH = 1, TFD_KERNEL_GATHER = 2, TFD_KERNEL_TILE2D = 3 };
 
 /* One CPML slab of one field family on one axis (both curl terms of that axis share it).
  * forward = 0: E family (backward differences), 1: H family (forward differences).
@@ -99,6 +99,7 @@ typedef struct tfd_desc {
     int32_t components;            /* bit c (0..5) set = component advanced; 0x3F in 3D */
     int32_t steps;                 /* length of every per-step table (sources, windows, traces) */
     int32_t kernel;                /* enum tfd_kernel */
+    int32_t launch_variant;        /* 0: default launch shape; otherwise a kernel-specific variant (autotuner) */
     int32_t face[3][2];            /* enum tfd_face per axis and side */
     double courant;                /* rectangular Courant number c*dt/dx */
     double time_step;              /* seconds */
@@ -184,6 +185,24 @@ int tfd_field_norm_static(const void *E, const void *H, const void *inv_eps, int
 
 /* Which step kernel the plan runs (enum tfd_kernel) after TFD_KERNEL_AUTO is resolved. */
 int tfd_kernel_in_use(const tfd_plan *plan, int32_t *kernel);
+
+/* ---- batches: many independent 2D TMz grids of uneven size advanced by one launch per step ----
+ * Replaces run_tensor_batch / run_grouped_batch cohorts (torchfdtd/tensor_batch.py:45-337,
+ * torchfdtd/grouped_batch.py:38-146, torchfdtd/cuda_batch.py:19-169), which need identical shapes per
+ * cohort and launch one kernel per cohort. Members are ordinary plans (2D TMz, same precision, non-periodic,
+ * step counter 0); while batched they share the batch's step counter and must be advanced only through
+ * tfd_batch_step (tfd_step and tfd_reset refuse them). Members may have different step counts: a member
+ * whose run has ended is skipped by later batch steps. Its fields, traces, planes and diagnostics stay
+ * readable through the plan entry points while the batch's step is at most the member's own step count,
+ * and always after tfd_batch_destroy, which hands every member its step count (capped at its own). */
+typedef struct tfd_batch tfd_batch;
+int tfd_batch_bytes(int32_t n_plans, tfd_plan *const *plans, size_t *bytes);
+int tfd_batch_create(int32_t n_plans, tfd_plan *const *plans, void *arena, size_t arena_bytes, void *stream, tfd_batch **batch);
+/* Persistent CTA count of the batched step kernel (0: one wave of resident CTAs); the autotuner's knob. */
+int tfd_batch_set_ctas(tfd_batch *batch, int32_t ctas);
+int tfd_batch_step(tfd_batch *batch, int32_t nsteps, void *stream);
+int tfd_batch_tiles(const tfd_batch *batch, int32_t *tiles);
+void tfd_batch_destroy(tfd_batch *batch);
 
 const char *tfd_error_string(int code);
 const char *tfd_last_error(void);

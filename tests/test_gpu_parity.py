@@ -20,7 +20,7 @@ from torchfdtd_b200.plan import plan_grid
 
 pytestmark = pytest.mark.gpu
 
-KERNELS = ['gather', 'march']
+KERNELS = ['gather', 'march', 'tile2d']
 PLANE_TOL = {'float32': 1e-5, 'float64': 1e-12}
 
 
@@ -35,11 +35,16 @@ def native(plan, kernel):
 
 
 def skip_unmarchable(plan_or_project, kernel):
-    """The marching kernel tiles 3D grids without periodic x/y faces; other scenes run the gather kernel."""
+    """The marching kernel tiles 3D grids without periodic x/y faces, the 2D tile kernel 2D TMz grids without
+    periodic x/y faces; other scenes run the gather kernel."""
     region = getattr(plan_or_project, 'region', None) or plan_or_project.project.region
     periodic_xy = any(region.boundaries.pair(a)[0].kind == 'periodic' for a in (0, 1))
     if kernel == 'march' and (region.dimension == '2d' or periodic_xy):
         pytest.skip('scene runs the gather kernel')
+    if kernel == 'tile2d':
+        plan = plan_or_project if hasattr(plan_or_project, 'psi_shapes') else plan_grid(plan_or_project)
+        if region.dimension != '2d' or periodic_xy or plan.polarization != 'TM':
+            pytest.skip('scene is not a 2D TMz grid with PML/PEC x/y faces')
 
 
 def state_files(golden):
@@ -106,6 +111,7 @@ def test_planes_match_oracle_with_float64_accumulators(golden, kernel):
     project = Project.model_validate_json(str(d['project']))
     project.region.backend = 'cuda'
     plan = plan_grid(project)
+    skip_unmarchable(plan, kernel)
     oracle = YeeOracle(plan, dft_float64=True).run()
     g = native(plan, kernel)
     g.step(plan.steps)
@@ -131,8 +137,8 @@ def random_project(dimension, precision, sampling='cell', faces=None, steps=20):
 def test_odd_shapes_and_random_state_match_oracle(kernel, dimension, precision):
     """Ragged shapes (x not a multiple of the tile), kappa>1 CPML, sources on E and H, random start."""
     project = random_project(dimension, precision)
-    skip_unmarchable(project, kernel)
     plan = plan_grid(project, polarization='both')
+    skip_unmarchable(plan, kernel)
     rng = np.random.default_rng(7)
     oracle = YeeOracle(plan)
     oracle.E[:] = rng.normal(size=oracle.E.shape).astype(plan.dtype) * .01
@@ -157,6 +163,7 @@ def test_z_faces_periodic_and_pec_match_oracle(kernel, zfaces):
              'y_max': BoundaryFace(kind='pec')}
     project = random_project('3d', 'float32', faces=faces, steps=16)
     plan = plan_grid(project)
+    skip_unmarchable(plan, kernel)
     rng = np.random.default_rng(11)
     oracle = YeeOracle(plan)
     oracle.E[:] = rng.normal(size=oracle.E.shape).astype(plan.dtype) * .01
@@ -185,6 +192,7 @@ def test_interior_and_boundary_tiles_match_oracle(kernel, precision):
                       monitors=[FieldMonitor(center=(.9, 0, 0), size=(0, 1.2, .6),
                                              spectrum=SpectrumSettings(sampling='frequency', frequency_points=2, apodization='none'))])
     plan = plan_grid(project)
+    skip_unmarchable(plan, kernel)
     rng = np.random.default_rng(5)
     oracle = YeeOracle(plan)
     oracle.E[:] = rng.normal(size=oracle.E.shape).astype(plan.dtype) * .01
@@ -205,6 +213,7 @@ def test_graph_replay_equals_eager_steps(kernel):
     import torch
     project = random_project('3d', 'float32', steps=30)
     plan = plan_grid(project)
+    skip_unmarchable(plan, kernel)
     a, b = native(plan, kernel), native(plan, kernel)
     a.step(30)
     stream = torch.cuda.Stream()

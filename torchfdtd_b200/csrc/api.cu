@@ -10,6 +10,7 @@
 #include "internal.cuh"
 #include "step_gather.cuh"
 #include "step_march.cuh"
+#include "step2d.cuh"
 #include <cudaTypedefs.h>
 
 using namespace tfd;
@@ -61,6 +62,8 @@ struct Layout {
     size_t src_values = 0, trace_tab = 0, trace_out = 0, plane_tab = 0;
     std::vector<PlaneLayout> planes;
     size_t counter = 0, done = 0, status = 0, diag = 0, stage = 0;
+    size_t grid_tab = 0, tile_tab = 0;   // 2D tile kernel: this plan's Grid struct and its tile table
+    int tiles2d = 0;
     size_t stage_bytes = 0;
     size_t psi_total = 0;          // elements of the reference psi vector
     size_t total = 0;
@@ -172,6 +175,11 @@ std::vector<PsiSegment> psi_segments(const tfd_desc *d, size_t *total) {
     return out;
 }
 
+// The 2D tile kernel runs 2D TMz grids whose x and y faces are PML or PEC.
+bool tile2d_capable(const tfd_desc *d) {
+    return d->nz == 1 && d->components == kMaskTM && d->face[0][0] != TFD_FACE_PERIODIC && d->face[1][0] != TFD_FACE_PERIODIC;
+}
+
 void compute_layout(const tfd_desc *d, Layout &L) {
     Bump b;
     const int n[3] = {d->nx, d->ny, d->nz};
@@ -228,6 +236,11 @@ void compute_layout(const tfd_desc *d, Layout &L) {
         q.acc = b.take(std::max<size_t>(1, acc));
         largest_plane = std::max(largest_plane, acc);
     }
+    if (tile2d_capable(d)) {
+        L.tiles2d = ((d->nx + k2dOwnX - 1) / k2dOwnX) * ((d->ny + k2dOwnY - 1) / k2dOwnY);
+        L.grid_tab = b.take(std::max(sizeof(Grid<float>), sizeof(Grid<double>)));
+        L.tile_tab = b.take((size_t)L.tiles2d * sizeof(Tile2D));
+    }
     L.counter = b.take(sizeof(long long));
     L.done = b.take(sizeof(unsigned));
     L.status = b.take(sizeof(int));
@@ -273,6 +286,9 @@ struct tfd_plan {
         if (fork) cudaEventDestroy(fork);
     }
     int march_variant = 42;
+    int tile2d_ctas = 0;
+    bool in_batch = false;
+    long long *own_counter = nullptr;
     std::vector<int> seg_f, seg_a, seg_lo, seg_hi;
 
     template <typename T> Grid<T> &grid();
@@ -620,7 +636,8 @@ int setup_march_s(tfd_plan *p) {
 template <typename T>
 int setup_march(tfd_plan *p) {
     const char *env = getenv("TFD_MARCH_VARIANT");
-    const std::string v = env ? env : (sizeof(T) == 4 ? "14" : "22");
+    const std::string v = p->desc.launch_variant ? std::to_string(p->desc.launch_variant)
+                                                 : (env ? env : (sizeof(T) == 4 ? "14" : "22"));
     const bool three = p->desc.material_samples == 3;
     if (sizeof(T) == 8 || v == "22") return three ? setup_march_s<T, 3, 2, 2>(p) : setup_march_s<T, 1, 2, 2>(p);
     if (v == "32") return three ? setup_march_s<T, 3, 3, 2>(p) : setup_march_s<T, 1, 3, 2>(p);
@@ -654,6 +671,45 @@ void launch_march_any(tfd_plan *p, cudaStream_t s) {
         case 32: three ? launch_march<T, 3, 3, 2>(p, s) : launch_march<T, 1, 3, 2>(p, s); break;
         default: three ? launch_march<T, 3, 1, 4>(p, s) : launch_march<T, 1, 1, 4>(p, s); break;
     }
+}
+
+}  // namespace
+
+// ---- 2D tile kernel set-up ---------------------------------------------------------------------------
+namespace {
+
+int resident_ctas_2d(const void *kernel) {
+    int device = 0, sms = 148, per_sm = 1;
+    if (cudaGetDevice(&device) != cudaSuccess) return 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, k2dThreads, 0);
+    return sms * std::max(1, per_sm);
+}
+
+template <typename T>
+std::vector<Tile2D> tiles_of(const Grid<T> &g, int grid_index) {
+    std::vector<Tile2D> t;
+    for (int y0 = 0; y0 < g.n[1]; y0 += k2dOwnY)
+        for (int x0 = 0; x0 < g.n[0]; x0 += k2dOwnX) t.push_back(Tile2D{grid_index, x0, y0, 0});
+    return t;
+}
+
+template <typename T>
+int setup_tile2d(tfd_plan *p, cudaStream_t s) {
+    Grid<T> &g = p->grid<T>();
+    std::vector<Tile2D> tiles = tiles_of(g, 0);
+    TFD_CUDA(cudaMemcpyAsync(p->arena + p->L.grid_tab, &g, sizeof(Grid<T>), cudaMemcpyHostToDevice, s));
+    TFD_CUDA(cudaMemcpyAsync(p->arena + p->L.tile_tab, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice, s));
+    p->tile2d_ctas = std::min((int)tiles.size(), resident_ctas_2d((const void *)k_step2d_tm<T>));
+    if (p->desc.launch_variant > 0) p->tile2d_ctas = std::min((int)tiles.size(), p->desc.launch_variant);
+    return TFD_OK;
+}
+
+template <typename T>
+void launch_tile2d(tfd_plan *p, cudaStream_t s) {
+    k_step2d_tm<T><<<std::max(1, p->tile2d_ctas), k2dThreads, 0, s>>>((const Grid<T> *)(p->arena + p->L.grid_tab),
+                                                                     (const Tile2D *)(p->arena + p->L.tile_tab), p->L.tiles2d,
+                                                                     p->grid<T>().counter);
 }
 
 }  // namespace
@@ -833,6 +889,8 @@ int step_t(tfd_plan *p, int nsteps, cudaStream_t s) {
     for (int k = 0; k < nsteps; ++k) {
         if (p->kernel == TFD_KERNEL_MARCH) {
             launch_march_any<T>(p, s);
+        } else if (p->kernel == TFD_KERNEL_TILE2D) {
+            launch_tile2d<T>(p, s);
         } else {
             int rc = launch_step_gather<T>(p, s);
             if (rc) return rc;
@@ -969,10 +1027,17 @@ int tfd_plan_create(const tfd_desc *desc, void *arena, size_t arena_bytes, void 
     rc = desc->precision == 8 ? create_typed<double>(p, desc, s) : create_typed<float>(p, desc, s);
     if (!rc) {
         const bool march_ok = desc->precision == 8 ? march_supported<double>(p) : march_supported<float>(p);
+        const bool tile_ok = tile2d_capable(desc);
         if (desc->kernel == TFD_KERNEL_MARCH && !march_ok)
             rc = fail(TFD_ERR_UNSUPPORTED, "the marching kernel needs a 3D grid without periodic x/y faces");
-        p->kernel = (desc->kernel == TFD_KERNEL_GATHER || !march_ok) ? TFD_KERNEL_GATHER : TFD_KERNEL_MARCH;
+        else if (desc->kernel == TFD_KERNEL_TILE2D && !tile_ok)
+            rc = fail(TFD_ERR_UNSUPPORTED, "the 2D tile kernel needs a 2D TMz grid without periodic x/y faces");
+        if (desc->kernel == TFD_KERNEL_GATHER) p->kernel = TFD_KERNEL_GATHER;
+        else if (march_ok) p->kernel = TFD_KERNEL_MARCH;
+        else if (tile_ok) p->kernel = TFD_KERNEL_TILE2D;
+        else p->kernel = TFD_KERNEL_GATHER;
         if (!rc && p->kernel == TFD_KERNEL_MARCH) rc = TFD_DISPATCH(p, setup_march, p);
+        if (!rc && tile_ok) rc = TFD_DISPATCH(p, setup_tile2d, p, s);
     }
     if (!rc) rc = TFD_DISPATCH(p, zero_state, p, s);
     if (!rc) {
@@ -1028,12 +1093,14 @@ int tfd_get_psi(tfd_plan *p, void *psi, int where, void *stream) {
 
 int tfd_step(tfd_plan *p, int32_t nsteps, void *stream) {
     if (!p) return fail(TFD_ERR_INVALID, "null plan");
+    if (p->in_batch) return fail(TFD_ERR_INVALID, "this plan belongs to a batch: advance it with tfd_batch_step");
     if (nsteps < 0) return fail(TFD_ERR_INVALID, "nsteps must be non-negative");
     return TFD_DISPATCH(p, step_t, p, nsteps, as_stream(stream));
 }
 
 int tfd_reset(tfd_plan *p, void *stream) {
     if (!p) return fail(TFD_ERR_INVALID, "null plan");
+    if (p->in_batch) return fail(TFD_ERR_INVALID, "this plan belongs to a batch: destroy the batch before resetting it");
     return TFD_DISPATCH(p, reset_t, p, as_stream(stream));
 }
 
@@ -1091,6 +1158,178 @@ int tfd_kernel_in_use(const tfd_plan *p, int32_t *kernel) {
     if (!p || !kernel) return fail(TFD_ERR_INVALID, "null argument");
     *kernel = p->kernel;
     return TFD_OK;
+}
+
+}  // extern "C"
+
+// ---- batches ---------------------------------------------------------------------------------------------
+struct tfd_batch {
+    std::vector<tfd_plan *> plans;
+    int precision = 4;
+    char *arena = nullptr;
+    size_t counter = 0, done = 0, grids = 0, tiles = 0, mon = 0, total = 0;
+    int ntiles = 0, ctas = 0, resident = 0, max_planes = 0, max_chunks = 1;
+};
+
+namespace {
+
+int batch_layout(tfd_batch &b, int n, tfd_plan *const *plans) {
+    if (n < 1 || !plans) return fail(TFD_ERR_INVALID, "a batch needs at least one plan");
+    b.plans.assign(plans, plans + n);
+    b.precision = plans[0] ? plans[0]->desc.precision : 4;
+    b.ntiles = 0;
+    for (int i = 0; i < n; ++i) {
+        tfd_plan *p = plans[i];
+        if (!p) return fail(TFD_ERR_INVALID, "null plan in batch");
+        if (p->desc.precision != b.precision) return fail(TFD_ERR_INVALID, "batched plans must share one precision");
+        if (p->L.tiles2d == 0) return fail(TFD_ERR_UNSUPPORTED, "batches run 2D TMz grids without periodic x/y faces");
+        if (p->in_batch) return fail(TFD_ERR_INVALID, "a plan belongs to another batch");
+        for (int j = 0; j < i; ++j)
+            if (plans[j] == p) return fail(TFD_ERR_INVALID, "a plan appears twice in the batch");
+        b.ntiles += p->L.tiles2d;
+    }
+    const size_t grid_bytes = b.precision == 8 ? sizeof(Grid<double>) : sizeof(Grid<float>);
+    const size_t mon_bytes = b.precision == 8 ? sizeof(MonitorArgs<double>) : sizeof(MonitorArgs<float>);
+    Bump bump;
+    b.counter = bump.take(sizeof(long long));
+    b.done = bump.take(sizeof(unsigned));
+    b.grids = bump.take(n * grid_bytes);
+    b.tiles = bump.take((size_t)b.ntiles * sizeof(Tile2D));
+    b.mon = bump.take(n * mon_bytes);
+    b.total = bump.off + 256;
+    return TFD_OK;
+}
+
+template <typename T>
+int batch_create_t(tfd_batch *b, cudaStream_t s) {
+    const int n = (int)b->plans.size();
+    long long *counter = (long long *)(b->arena + b->counter);
+    std::vector<Grid<T>> grids;
+    std::vector<Tile2D> tiles;
+    std::vector<MonitorArgs<T>> mons;
+    for (int i = 0; i < n; ++i) {
+        tfd_plan *p = b->plans[i];
+        long long value = -1;
+        TFD_CUDA(cudaMemcpyAsync(&value, p->grid<T>().counter, sizeof(long long), cudaMemcpyDeviceToHost, s));
+        TFD_CUDA(cudaStreamSynchronize(s));
+        if (value != 0) return fail(TFD_ERR_INVALID, "batched plans must start at step 0 (tfd_reset them)");
+    }
+    for (int i = 0; i < n; ++i) {
+        tfd_plan *p = b->plans[i];
+        Grid<T> &g = p->grid<T>();
+        p->own_counter = g.counter;
+        g.counter = counter;                         // members read the batch's shared step counter
+        p->in_batch = true;
+        grids.push_back(g);
+        std::vector<Tile2D> t = tiles_of(g, i);
+        tiles.insert(tiles.end(), t.begin(), t.end());
+        MonitorArgs<T> m = monitor_args<T>(p);
+        mons.push_back(m);
+        b->max_planes = std::max(b->max_planes, p->desc.n_planes);
+        b->max_chunks = std::max(b->max_chunks, (p->max_samples + kMonitorThreads - 1) / kMonitorThreads);
+    }
+    TFD_CUDA(cudaMemsetAsync(b->arena + b->counter, 0, sizeof(long long), s));
+    TFD_CUDA(cudaMemsetAsync(b->arena + b->done, 0, sizeof(unsigned), s));
+    TFD_CUDA(cudaMemcpyAsync(b->arena + b->grids, grids.data(), grids.size() * sizeof(Grid<T>), cudaMemcpyHostToDevice, s));
+    TFD_CUDA(cudaMemcpyAsync(b->arena + b->tiles, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice, s));
+    TFD_CUDA(cudaMemcpyAsync(b->arena + b->mon, mons.data(), mons.size() * sizeof(MonitorArgs<T>), cudaMemcpyHostToDevice, s));
+    TFD_CUDA(cudaStreamSynchronize(s));
+    cudaFuncAttributes attr;                     // loads the monitor kernel now, before any graph capture
+    TFD_CUDA(cudaFuncGetAttributes(&attr, (const void *)k_monitor_batch<T>));
+    b->resident = resident_ctas_2d((const void *)k_step2d_tm<T>);
+    b->ctas = std::min(b->ntiles, b->resident);
+    return TFD_OK;
+}
+
+template <typename T>
+int batch_step_t(tfd_batch *b, int nsteps, cudaStream_t s) {
+    long long *counter = (long long *)(b->arena + b->counter);
+    const dim3 mgrid((unsigned)b->max_chunks, (unsigned)std::max(1, b->max_planes), (unsigned)b->plans.size());
+    for (int k = 0; k < nsteps; ++k) {
+        k_step2d_tm<T><<<std::max(1, b->ctas), k2dThreads, 0, s>>>((const Grid<T> *)(b->arena + b->grids),
+                                                                   (const Tile2D *)(b->arena + b->tiles), b->ntiles, counter);
+        k_monitor_batch<T><<<mgrid, kMonitorThreads, 0, s>>>((const MonitorArgs<T> *)(b->arena + b->mon), counter,
+                                                             (unsigned *)(b->arena + b->done));
+    }
+    TFD_CUDA(cudaGetLastError());
+    return TFD_OK;
+}
+
+template <typename T>
+void batch_release_t(tfd_batch *b) {
+    // Hand the step count back to every member (capped at its own run length: a finished grid was
+    // skipped from then on) and restore its own counter.
+    long long n = 0;
+    cudaMemcpy(&n, b->arena + b->counter, sizeof(long long), cudaMemcpyDeviceToHost);
+    for (tfd_plan *p : b->plans) {
+        Grid<T> &g = p->grid<T>();
+        if (p->own_counter) {
+            const long long mine = std::min<long long>(n, p->desc.steps);
+            cudaMemcpy(p->own_counter, &mine, sizeof(long long), cudaMemcpyHostToDevice);
+            g.counter = p->own_counter;
+            p->own_counter = nullptr;
+        }
+        p->in_batch = false;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int tfd_batch_bytes(int32_t n_plans, tfd_plan *const *plans, size_t *bytes) {
+    if (!bytes) return fail(TFD_ERR_INVALID, "bytes is null");
+    tfd_batch b;
+    int rc = batch_layout(b, n_plans, plans);
+    if (rc) return rc;
+    *bytes = b.total;
+    return TFD_OK;
+}
+
+int tfd_batch_create(int32_t n_plans, tfd_plan *const *plans, void *arena, size_t arena_bytes, void *stream, tfd_batch **out) {
+    if (!out) return fail(TFD_ERR_INVALID, "batch output is null");
+    *out = nullptr;
+    tfd_batch *b = new tfd_batch();
+    int rc = batch_layout(*b, n_plans, plans);
+    if (!rc && (!arena || ((uintptr_t)arena & 255) || arena_bytes < b->total))
+        rc = fail(TFD_ERR_ARENA, "batch arena must be 256-byte aligned and at least tfd_batch_bytes() long");
+    if (rc) {
+        delete b;
+        return rc;
+    }
+    b->arena = (char *)arena;
+    rc = b->precision == 8 ? batch_create_t<double>(b, as_stream(stream)) : batch_create_t<float>(b, as_stream(stream));
+    if (rc) {
+        if (b->precision == 8) batch_release_t<double>(b); else batch_release_t<float>(b);
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return TFD_OK;
+}
+
+int tfd_batch_set_ctas(tfd_batch *b, int32_t ctas) {
+    if (!b || ctas < 0) return fail(TFD_ERR_INVALID, "bad batch CTA count");
+    b->ctas = ctas == 0 ? std::min(b->ntiles, b->resident) : std::min(b->ntiles, (int)ctas);
+    return TFD_OK;
+}
+
+int tfd_batch_step(tfd_batch *b, int32_t nsteps, void *stream) {
+    if (!b || nsteps < 0) return fail(TFD_ERR_INVALID, "bad batch step");
+    return b->precision == 8 ? batch_step_t<double>(b, nsteps, as_stream(stream)) : batch_step_t<float>(b, nsteps, as_stream(stream));
+}
+
+int tfd_batch_tiles(const tfd_batch *b, int32_t *tiles) {
+    if (!b || !tiles) return fail(TFD_ERR_INVALID, "null argument");
+    *tiles = b->ntiles;
+    return TFD_OK;
+}
+
+void tfd_batch_destroy(tfd_batch *b) {
+    if (!b) return;
+    cudaDeviceSynchronize();
+    if (b->precision == 8) batch_release_t<double>(b); else batch_release_t<float>(b);
+    delete b;
 }
 
 }  // extern "C"

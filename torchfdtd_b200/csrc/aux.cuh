@@ -31,78 +31,97 @@ struct MonitorArgs {
 constexpr int kMonitorThreads = 256;
 constexpr int kPhaseChunk = 256;
 
+// Observations of step n for one plan: block (bx, by) handles sample chunk bx of plane by; block
+// (0, 0) also records the point traces.
 template <typename T>
-__global__ void __launch_bounds__(kMonitorThreads) k_monitor(const __grid_constant__ MonitorArgs<T> m) {
+__device__ __forceinline__ void monitor_work(const MonitorArgs<T> &m, int bx, int by, long long n) {
     __shared__ double2 phase_e[kPhaseChunk], phase_h[kPhaseChunk];
-    const long long n = *m.counter;
     const long long shift = ((n + 1) & 1) ? m.count : 0;   // current (new) parity
-    if (n < m.steps) {
-        if (blockIdx.x == 0 && blockIdx.y == 0) {
-            for (int k = threadIdx.x; k < m.n_traces; k += blockDim.x) {
-                const TraceDev t = m.traces[k];
-                const T *base = m.field[3 * t.family + t.comp];   // null: a component 2D does not advance (zero)
-                m.trace_out[n * m.n_traces + k] = base ? base[shift + t.offset] : T(0);
-            }
+    if (n >= m.steps) return;
+    if (bx == 0 && by == 0) {
+        for (int k = threadIdx.x; k < m.n_traces; k += blockDim.x) {
+            const TraceDev t = m.traces[k];
+            const T *base = m.field[3 * t.family + t.comp];   // null: a component 2D does not advance (zero)
+            m.trace_out[n * m.n_traces + k] = base ? base[shift + t.offset] : T(0);
         }
-        if (blockIdx.y < m.n_planes) {
-            const PlaneDev &pl = m.planes[blockIdx.y];
-            const int samples = pl.points * pl.components;
-            const int s = blockIdx.x * blockDim.x + threadIdx.x;
-            const T *win = (const T *)pl.window;
-            double value = 0.0;
-            int p = 0, c = 0;
-            const bool live = s < samples;
-            if (live) {
-                p = s / pl.components;
-                c = s % pl.components;
-                const int comp = pl.comp[c];
-                const T *f = m.field[comp];
-                const T *w = (const T *)pl.weight + (long long)c * pl.corners * pl.points;
-                const long long *cell = pl.cell + (long long)c * pl.corners * pl.points;
-                T sum = T(0);
-                if (f != nullptr) {
-                    f += shift;
-                    for (int k = 0; k < pl.corners; ++k)
-                        sum = sum + f[cell[(long long)k * pl.points + p]] * w[(long long)k * pl.points + p];
-                }
-                const T wv = win[(comp >= 3 ? m.steps : 0) + n];
-                value = (double)(sum * wv);
-            }
-            const bool magnetic = live && pl.comp[c] >= 3;
-            for (int f0 = 0; f0 < pl.frequencies; f0 += kPhaseChunk) {
-                const int nf = min(kPhaseChunk, pl.frequencies - f0);
-                __syncthreads();
-                for (int f = threadIdx.x; f < nf; f += blockDim.x) {
-                    double si, co;
-                    sincos(pl.omega[f0 + f] * (double)(n + 1), &si, &co);
-                    const double hr = pl.half[2 * (f0 + f)], hi = pl.half[2 * (f0 + f) + 1];
-                    phase_e[f] = make_double2(co, si);
-                    phase_h[f] = make_double2(co * hr - si * hi, co * hi + si * hr);
-                }
-                __syncthreads();
-                if (live) {
-                    for (int f = 0; f < nf; ++f) {
-                        const double2 ph = magnetic ? phase_h[f] : phase_e[f];
-                        double *acc = pl.acc + 2 * (((long long)(f0 + f) * pl.points + p) * pl.components + c);
-                        acc[0] += ph.x * value;
-                        acc[1] += ph.y * value;
-                    }
-                }
+    }
+    if (by >= m.n_planes) return;
+    const PlaneDev &pl = m.planes[by];
+    const int samples = pl.points * pl.components;
+    if (bx * (int)blockDim.x >= samples) return;          // uniform per block: no barrier below is skipped by part of it
+    const int s = bx * blockDim.x + threadIdx.x;
+    const T *win = (const T *)pl.window;
+    double value = 0.0;
+    int p = 0, c = 0;
+    const bool live = s < samples;
+    if (live) {
+        p = s / pl.components;
+        c = s % pl.components;
+        const int comp = pl.comp[c];
+        const T *f = m.field[comp];
+        const T *w = (const T *)pl.weight + (long long)c * pl.corners * pl.points;
+        const long long *cell = pl.cell + (long long)c * pl.corners * pl.points;
+        T sum = T(0);
+        if (f != nullptr) {
+            f += shift;
+            for (int k = 0; k < pl.corners; ++k)
+                sum = sum + f[cell[(long long)k * pl.points + p]] * w[(long long)k * pl.points + p];
+        }
+        const T wv = win[(comp >= 3 ? m.steps : 0) + n];
+        value = (double)(sum * wv);
+    }
+    const bool magnetic = live && pl.comp[c] >= 3;
+    for (int f0 = 0; f0 < pl.frequencies; f0 += kPhaseChunk) {
+        const int nf = min(kPhaseChunk, pl.frequencies - f0);
+        __syncthreads();
+        for (int f = threadIdx.x; f < nf; f += blockDim.x) {
+            double si, co;
+            sincos(pl.omega[f0 + f] * (double)(n + 1), &si, &co);
+            const double hr = pl.half[2 * (f0 + f)], hi = pl.half[2 * (f0 + f) + 1];
+            phase_e[f] = make_double2(co, si);
+            phase_h[f] = make_double2(co * hr - si * hi, co * hi + si * hr);
+        }
+        __syncthreads();
+        if (live) {
+            for (int f = 0; f < nf; ++f) {
+                const double2 ph = magnetic ? phase_h[f] : phase_e[f];
+                double *acc = pl.acc + 2 * (((long long)(f0 + f) * pl.points + p) * pl.components + c);
+                acc[0] += ph.x * value;
+                acc[1] += ph.y * value;
             }
         }
     }
-    // The last block to finish advances the step counter; every block read it above.
+}
+
+// The last block of a launch to finish advances the step counter; every block read it first.
+__device__ __forceinline__ void finish_step(long long *counter, unsigned *done, long long n) {
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        const unsigned total = gridDim.x * gridDim.y;
-        const unsigned prev = atomicAdd(m.done, 1u);
+        const unsigned total = gridDim.x * gridDim.y * gridDim.z;
+        const unsigned prev = atomicAdd(done, 1u);
         if (prev == total - 1) {
-            *m.done = 0;
+            *done = 0;
             __threadfence();
-            *m.counter = n + 1;
+            *counter = n + 1;
         }
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kMonitorThreads) k_monitor(const __grid_constant__ MonitorArgs<T> m) {
+    const long long n = *m.counter;
+    monitor_work(m, blockIdx.x, blockIdx.y, n);
+    finish_step(m.counter, m.done, n);
+}
+
+// Observations of every plan of a batch (plan = blockIdx.z), then the batch's shared step counter.
+template <typename T>
+__global__ void __launch_bounds__(kMonitorThreads) k_monitor_batch(const MonitorArgs<T> *__restrict__ args, long long *counter,
+                                                                  unsigned *done) {
+    const long long n = *counter;
+    monitor_work(args[blockIdx.z], blockIdx.x, blockIdx.y, n);
+    finish_step(counter, done, n);
 }
 
 // ---- layout conversion ----------------------------------------------------------------------

@@ -19,7 +19,7 @@ LIBRARY = HERE / 'libtfdtd.so'
 
 TFD_ABI_VERSION = 1
 TFD_DEVICE, TFD_HOST = 0, 1
-KERNELS = {'auto': 0, 'march': 1, 'gather': 2}
+KERNELS = {'auto': 0, 'march': 1, 'gather': 2, 'tile2d': 3}
 FACE = {'pml': 0, 'periodic': 1, 'pec': 2, 'antisymmetric': 2}
 MASK = {'3d': 0x3F, 'both': 0x3F, 'TM': 0x04 | 0x08 | 0x10, 'TE': 0x01 | 0x02 | 0x20}
 
@@ -51,6 +51,7 @@ class PlaneC(ctypes.Structure):
 class Desc(ctypes.Structure):
     _fields_ = [('abi_version', c_i32), ('nx', c_i32), ('ny', c_i32), ('nz', c_i32), ('precision', c_i32),
                 ('material_samples', c_i32), ('components', c_i32), ('steps', c_i32), ('kernel', c_i32),
+                ('launch_variant', c_i32),
                 ('face', (c_i32 * 2) * 3), ('courant', c_dbl), ('time_step', c_dbl), ('pec_upper', c_dbl * 3),
                 ('n_segments', c_i32), ('segments', ctypes.POINTER(CpmlSegment)),
                 ('n_sources', c_i32), ('sources', ctypes.POINTER(SourceTermC)),
@@ -79,6 +80,12 @@ SIGNATURES = {
     'tfd_device_status': (ctypes.c_int, [c_vp, P_i32, c_vp]),
     'tfd_kernel_in_use': (ctypes.c_int, [c_vp, P_i32]),
     'tfd_field_norm_static': (ctypes.c_int, [c_vp, c_vp, c_vp, c_i64, c_i32, c_i32, c_vp, c_vp]),
+    'tfd_batch_bytes': (ctypes.c_int, [c_i32, ctypes.POINTER(c_vp), ctypes.POINTER(ctypes.c_size_t)]),
+    'tfd_batch_create': (ctypes.c_int, [c_i32, ctypes.POINTER(c_vp), c_vp, ctypes.c_size_t, c_vp, ctypes.POINTER(c_vp)]),
+    'tfd_batch_set_ctas': (ctypes.c_int, [c_vp, c_i32]),
+    'tfd_batch_step': (ctypes.c_int, [c_vp, c_i32, c_vp]),
+    'tfd_batch_tiles': (ctypes.c_int, [c_vp, P_i32]),
+    'tfd_batch_destroy': (None, [c_vp]),
     'tfd_error_string': (ctypes.c_char_p, [ctypes.c_int]),
     'tfd_last_error': (ctypes.c_char_p, []),
 }
@@ -126,10 +133,69 @@ def _stream(stream=None):
     return c_vp(s.cuda_stream)
 
 
+def describe(plan, kernel='auto', variant=0):
+    """The C descriptor of a plan and the host arrays it points into (keep them alive while it is used)."""
+    keep = []
+    desc = Desc()
+    desc.abi_version = TFD_ABI_VERSION
+    desc.nx, desc.ny, desc.nz = plan.shape
+    desc.precision = 8 if plan.dtype == np.float64 else 4
+    desc.material_samples = plan.material_samples
+    desc.components = MASK['3d' if plan.dimension == '3d' else plan.polarization]
+    desc.steps = plan.steps
+    desc.kernel = KERNELS[kernel]
+    desc.launch_variant = int(variant)
+    for a in range(3):
+        for s in range(2):
+            desc.face[a][s] = FACE[plan.faces[a][s]]
+        desc.pec_upper[a] = plan.pec_upper.get(a, 0.0)
+    desc.courant = plan.courant
+    desc.time_step = plan.time_step
+    segs = (CpmlSegment * max(1, len(plan.segments)))()
+    for k, s in enumerate(plan.segments):
+        arrays = [np.ascontiguousarray(v, dtype=np.float64) for v in (s.b, s.c, s.inv_kappa)]
+        keep.extend(arrays)
+        segs[k] = CpmlSegment(int(s.forward), s.axis, s.lo, s.hi, *(_ptr(v, ctypes.c_double) for v in arrays))
+    desc.n_segments, desc.segments = len(plan.segments), segs
+    srcs = (SourceTermC * max(1, len(plan.sources)))()
+    for k, t in enumerate(plan.sources):
+        v = np.ascontiguousarray(t.values, dtype=np.float64)
+        keep.append(v)
+        srcs[k] = SourceTermC(t.family, t.comp, (c_i32 * 3)(*t.lo), (c_i32 * 3)(*t.hi), _ptr(v, ctypes.c_double))
+    desc.n_sources, desc.sources = len(plan.sources), srcs
+    traces = (TraceC * max(1, len(plan.traces)))()
+    for k, t in enumerate(plan.traces):
+        traces[k] = TraceC(t.family, t.comp, (c_i32 * 3)(*t.index))
+    desc.n_traces, desc.traces = len(plan.traces), traces
+    planes = (PlaneC * max(1, len(plan.planes)))()
+    for k, p in enumerate(plan.planes):
+        ids = np.array([['Ex', 'Ey', 'Ez', 'Hx', 'Hy', 'Hz'].index(c) for c in p.components], dtype=np.int32)
+        cells = np.ascontiguousarray(p.corner_cells, dtype=np.int64)
+        weights = np.ascontiguousarray(p.corner_weights, dtype=np.float64)
+        freq = np.ascontiguousarray(p.frequency, dtype=np.float64)
+        we = np.ascontiguousarray(p.windows[0], dtype=np.float64)
+        wh = np.ascontiguousarray(p.windows[1], dtype=np.float64)
+        keep.extend([ids, cells, weights, freq, we, wh])
+        planes[k] = PlaneC(cells.shape[2], len(freq), len(ids), cells.shape[1], _ptr(ids, c_i32), _ptr(cells, c_i64),
+                           _ptr(weights, ctypes.c_double), _ptr(freq, ctypes.c_double), _ptr(we, ctypes.c_double),
+                           _ptr(wh, ctypes.c_double))
+    desc.n_planes, desc.planes = len(plan.planes), planes
+    keep.extend([segs, srcs, traces, planes])
+    return desc, keep
+
+
 class NativeGrid:
     """A device plan built from a ``GridPlan`` (owns the arena tensor and the native handle)."""
 
-    def __init__(self, plan, kernel='auto', device=None):
+    @staticmethod
+    def plan_bytes(plan, kernel='auto'):
+        """Device bytes the plan's arena needs (no device work)."""
+        desc, keep = describe(plan, kernel)
+        size = ctypes.c_size_t()
+        check(library().tfd_plan_bytes(ctypes.byref(desc), ctypes.byref(size)))
+        return size.value
+
+    def __init__(self, plan, kernel='auto', device=None, variant=0):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError('CUDA requested but unavailable: the fused B200 engine runs on a CUDA GPU only.')
@@ -138,51 +204,7 @@ class NativeGrid:
         self.device = torch.device('cuda', torch.cuda.current_device() if device is None else device)
         self.dtype = plan.dtype
         self.torch_dtype = torch.float64 if plan.dtype == np.float64 else torch.float32
-        self._keep = []
-        desc = Desc()
-        desc.abi_version = TFD_ABI_VERSION
-        desc.nx, desc.ny, desc.nz = plan.shape
-        desc.precision = 8 if plan.dtype == np.float64 else 4
-        desc.material_samples = plan.material_samples
-        desc.components = MASK['3d' if plan.dimension == '3d' else plan.polarization]
-        desc.steps = plan.steps
-        desc.kernel = KERNELS[kernel]
-        for a in range(3):
-            for s in range(2):
-                desc.face[a][s] = FACE[plan.faces[a][s]]
-            desc.pec_upper[a] = plan.pec_upper.get(a, 0.0)
-        desc.courant = plan.courant
-        desc.time_step = plan.time_step
-        segs = (CpmlSegment * max(1, len(plan.segments)))()
-        for k, s in enumerate(plan.segments):
-            arrays = [np.ascontiguousarray(v, dtype=np.float64) for v in (s.b, s.c, s.inv_kappa)]
-            self._keep.extend(arrays)
-            segs[k] = CpmlSegment(int(s.forward), s.axis, s.lo, s.hi, *(_ptr(v, ctypes.c_double) for v in arrays))
-        desc.n_segments, desc.segments = len(plan.segments), segs
-        srcs = (SourceTermC * max(1, len(plan.sources)))()
-        for k, t in enumerate(plan.sources):
-            v = np.ascontiguousarray(t.values, dtype=np.float64)
-            self._keep.append(v)
-            srcs[k] = SourceTermC(t.family, t.comp, (c_i32 * 3)(*t.lo), (c_i32 * 3)(*t.hi), _ptr(v, ctypes.c_double))
-        desc.n_sources, desc.sources = len(plan.sources), srcs
-        traces = (TraceC * max(1, len(plan.traces)))()
-        for k, t in enumerate(plan.traces):
-            traces[k] = TraceC(t.family, t.comp, (c_i32 * 3)(*t.index))
-        desc.n_traces, desc.traces = len(plan.traces), traces
-        planes = (PlaneC * max(1, len(plan.planes)))()
-        for k, p in enumerate(plan.planes):
-            ids = np.array([['Ex', 'Ey', 'Ez', 'Hx', 'Hy', 'Hz'].index(c) for c in p.components], dtype=np.int32)
-            cells = np.ascontiguousarray(p.corner_cells, dtype=np.int64)
-            weights = np.ascontiguousarray(p.corner_weights, dtype=np.float64)
-            freq = np.ascontiguousarray(p.frequency, dtype=np.float64)
-            we = np.ascontiguousarray(p.windows[0], dtype=np.float64)
-            wh = np.ascontiguousarray(p.windows[1], dtype=np.float64)
-            self._keep.extend([ids, cells, weights, freq, we, wh])
-            planes[k] = PlaneC(cells.shape[2], len(freq), len(ids), cells.shape[1], _ptr(ids, c_i32), _ptr(cells, c_i64),
-                               _ptr(weights, ctypes.c_double), _ptr(freq, ctypes.c_double), _ptr(we, ctypes.c_double),
-                               _ptr(wh, ctypes.c_double))
-        desc.n_planes, desc.planes = len(plan.planes), planes
-        self._keep.extend([segs, srcs, traces, planes])
+        desc, self._keep = describe(plan, kernel, variant)
         self.desc = desc
         size = ctypes.c_size_t()
         check(lib.tfd_plan_bytes(ctypes.byref(desc), ctypes.byref(size)))
@@ -198,6 +220,8 @@ class NativeGrid:
         self.set_material(plan.inv_eps)
 
     def close(self):
+        if getattr(self, 'batch', None) is not None:
+            self.batch.close()
         if getattr(self, 'handle', None):
             library().tfd_plan_destroy(self.handle)
             self.handle = None
@@ -310,3 +334,48 @@ class NativeGrid:
         out = (ctypes.c_double * 3)()
         check(library().tfd_diagnose(self.handle, out, _stream()))
         return float(out[0]), float(out[1]), bool(out[2] == 1.0)
+
+
+class NativeBatch:
+    """Independent 2D TMz plans advanced together: one persistent launch per step over all their tiles."""
+
+    def __init__(self, grids):
+        import torch
+        lib = library()
+        self.grids = list(grids)
+        if not self.grids:
+            raise ValueError('A batch needs at least one grid.')
+        handles = (c_vp * len(self.grids))(*[g.handle.value for g in self.grids])
+        self._handles = handles
+        size = ctypes.c_size_t()
+        check(lib.tfd_batch_bytes(len(self.grids), handles, ctypes.byref(size)))
+        self.arena = torch.empty(size.value, dtype=torch.uint8, device=self.grids[0].device)
+        handle = c_vp()
+        check(lib.tfd_batch_create(len(self.grids), handles, c_vp(self.arena.data_ptr()), size, _stream(), ctypes.byref(handle)))
+        self.handle = handle
+        for g in self.grids:
+            g.batch = self
+
+    def set_ctas(self, ctas):
+        check(library().tfd_batch_set_ctas(self.handle, int(ctas)))
+
+    def tiles(self):
+        v = c_i32()
+        check(library().tfd_batch_tiles(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def step(self, n=1, stream=None):
+        check(library().tfd_batch_step(self.handle, int(n), _stream(stream)))
+
+    def close(self):
+        if getattr(self, 'handle', None):
+            library().tfd_batch_destroy(self.handle)
+            self.handle = None
+            for g in self.grids:
+                g.batch = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

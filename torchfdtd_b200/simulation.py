@@ -165,6 +165,131 @@ def resolve_selector(region):
     return 'fused'
 
 
+class Observer:
+    """Frames, divergence checks and the packaged ``Result`` of one grid during a run
+    (reference torchfdtd/solver.py:806-908; per case in torchfdtd/tensor_batch.py:228-333)."""
+
+    def __init__(self, project, plan, grid, label=''):
+        r = project.region
+        self.project, self.plan, self.grid, self.region = project, plan, grid, r
+        self.label = label
+        self.control = r.run_control
+        self.source_end = source_end_time(project)
+        self.decision = DecayDecision(self.control, self.source_end, r.time_step)
+        self.diagnose = self.control.auto_shutoff or self.control.divergence_check
+        self.warnings = list(plan.warnings)
+        if self.control.auto_shutoff and not math.isfinite(self.source_end):
+            self.warnings.append('Automatic decay shutoff is inactive while a continuous source is enabled.')
+        self.axis = 'xyz'.index(r.slice_axis)
+        self.plane_index = index_at(tuple(r.slice_position if i == self.axis else 0 for i in range(3)), r, r.field)[self.axis]
+        component = 'xyz'.index(r.field[1].lower())
+        eps = plan.epsilon
+        sl = [slice(None)] * 3
+        sl[self.axis] = self.plane_index
+        self.eps_plane = np.array(self.decimate((eps[..., component] if eps.ndim == 4 else eps)[tuple(sl)]))
+        self.interval = max(r.snapshot_interval, math.ceil(r.steps / 100))
+        self.frames, self.frame_steps = [], []
+        self.diagnostic_seconds = 0.
+
+    @staticmethod
+    def decimate(a):
+        return a[::max(1, math.ceil(a.shape[0] / 256)), ::max(1, math.ceil(a.shape[1] / 256))]
+
+    def barriers(self):
+        """Steps after which this grid is observed on the host."""
+        steps = self.region.steps
+        due = set(range(self.interval, steps + 1, self.interval)) | {steps}
+        if self.diagnose:
+            due.update(range(self.control.check_interval, steps + 1, self.control.check_interval))
+        return due
+
+    def _where(self, text):
+        return f'{self.label}{text}'
+
+    def observe(self, completed, progress=None, started=None):
+        """Observations due after ``completed`` steps; True when the decay shutoff fires."""
+        r, control, stop = self.region, self.control, False
+        if self.diagnose and (completed % control.check_interval == 0 or completed == r.steps):
+            t0 = time.perf_counter()
+            energy, peak, finite = self.grid.diagnose()
+            if not finite:
+                raise FloatingPointError(self._where(f'Non-finite CPML or incident-line memory detected. (diagnostic step {completed})'))
+            try:
+                stop = self.decision.update(completed, energy, peak)
+            except FloatingPointError as exc:
+                raise FloatingPointError(self._where(f'{exc} (diagnostic step {completed})')) from exc
+            self.diagnostic_seconds += time.perf_counter() - t0
+        if completed % self.interval == 0 or completed == r.steps or stop:
+            frame = self.decimate(self.grid.get_slice(r.field, self.axis, self.plane_index))
+            if not np.isfinite(frame).all():
+                raise FloatingPointError(self._where('Fields diverged. Check mesh, sources and precision.'))
+            frame = {'real': np.real, 'imag': np.imag, 'magnitude': np.abs, 'phase': np.angle}[r.complex_display](frame)
+            self.frames.append(frame)
+            self.frame_steps.append(completed)
+            if progress:
+                progress({'step': completed, 'total': r.steps, 'frame': frame.tolist(),
+                          'elapsed': time.perf_counter() - started,
+                          'termination_reason': 'decayed' if stop else None,
+                          'diagnostics': self.decision.history[-1] if self.decision.history else None})
+        return stop
+
+    def result(self, completed, termination_reason, seconds, setup_seconds, **extra):
+        """Read the final state back and package it as the reference's ``Result``."""
+        import torch
+        p, r, plan, grid = self.project, self.region, self.plan, self.grid
+        status = grid.device_status()
+        if status:
+            raise RuntimeError(self._where(f'A fused kernel reported device status {status}.'))
+        e, h = grid.get_fields()
+        if not np.isfinite(e).all() or not np.isfinite(h).all():
+            raise FloatingPointError(self._where('Non-finite fields detected.'))
+        traces = grid.get_traces()[:completed]
+        frequency_results = []
+        for k, pp in enumerate(plan.planes):
+            values = grid.get_plane(k)
+            frequency_results.append(plane_result(pp.monitor, pp.plan, pp.frequency, list(pp.components), values, r.dimension))
+        if frequency_results:
+            signature = run_signature(p, completed)
+            for m in frequency_results:
+                m['run_signature'] = signature
+        cells = math.prod(r.shape)
+        stats = dict(warnings=self.warnings, backend='cuda', precision=r.precision, gpu=torch.cuda.get_device_name(),
+                     cuda_kernel='fused', cuda_monitor_kernel='fused', kernel=grid.kernel,
+                     steps=completed, requested_steps=r.steps, cancelled=termination_reason == 'cancelled',
+                     termination_reason=termination_reason, auto_shutoff=termination_reason == 'decayed',
+                     diagnostics=self.decision.history, diagnostic_seconds=self.diagnostic_seconds,
+                     diagnostic_backend='fused_cuda' if self.diagnose else None,
+                     source_end_s=self.source_end if math.isfinite(self.source_end) else None,
+                     seconds=seconds, setup_seconds=setup_seconds,
+                     mcells_per_second=cells * completed / max(seconds, 1e-9) / 1e6,
+                     gcells_per_s=cells * completed / max(seconds, 1e-9) / 1e9,
+                     hbm_bytes_per_step=algorithmic_bytes_per_step(plan), arena_bytes=grid.arena_bytes,
+                     field_peak=float(np.max(np.abs(e))), slice_index=self.plane_index,
+                     slice_position=(0 if r.dimension == '2d' and self.axis == 2
+                                     else (self.plane_index + .5) * r.mesh - r.actual_size[self.axis] / 2),
+                     complex_fields=False, complex_display=r.complex_display, material_update='nondispersive',
+                     dispersive_samples=0, material_sampling=r.material_sampling,
+                     epsilon_definition='instantaneous relative permittivity (epsilon-infinity for dispersive cells)',
+                     boundaries=r.boundaries.model_dump(), bloch_phase=r.bloch_phase,
+                     units='geometry: um; time: s; E/H: reduced fields; Bloch phase: rad', engine=ENGINE)
+        stats.update(extra)
+        return Result(p, stats, np.array(self.frames), np.array(self.frame_steps), self.eps_plane, traces,
+                      np.arange(1, completed + 1) * r.time_step, e, h, frequency_results)
+
+
+def capture_graphs(step, widths):
+    """CUDA graphs of ``step(count)`` for each width, captured on the current stream."""
+    import torch
+    graphs = {}
+    for count in sorted(set(widths)):
+        g = torch.cuda.CUDAGraph()
+        g.capture_begin()
+        step(count)
+        g.capture_end()
+        graphs[count] = g
+    return graphs
+
+
 class Simulation:
     """Run the fused Yee/CPML kernels on a B200 for a ``Project``.
 
@@ -200,7 +325,7 @@ class Simulation:
         import torch
         from .native import NativeGrid
         p, r = self.project, self.project.region
-        cuda_kernel = resolve_selector(r)
+        resolve_selector(r)
         validate_graph_steps(cuda_graph_steps, cuda_graph)
         if not torch.cuda.is_available():
             raise RuntimeError('CUDA requested but unavailable. The fused B200 engine needs a CUDA GPU.')
@@ -208,13 +333,7 @@ class Simulation:
         plan = self.plan
         grid = NativeGrid(plan, kernel=kernel)
         free, _ = torch.cuda.mem_get_info()
-        control = r.run_control
-        source_end = source_end_time(p)
-        decision = DecayDecision(control, source_end, r.time_step)
-        diagnose = control.auto_shutoff or control.divergence_check
-        warnings = list(plan.warnings)
-        if control.auto_shutoff and not math.isfinite(source_end):
-            warnings.append('Automatic decay shutoff is inactive while a continuous source is enabled.')
+        observer = Observer(p, plan, grid)
         graphs = {}
         width = 1
         stream = torch.cuda.Stream()
@@ -225,34 +344,14 @@ class Simulation:
                 # One eager step loads the kernels before capture; the state is then zeroed.
                 grid.step(1, stream)
                 grid.reset()
-                for count in sorted({1, width}):
-                    g = torch.cuda.CUDAGraph()
-                    g.capture_begin()
-                    grid.step(count, stream)
-                    g.capture_end()
-                    graphs[count] = g
+                graphs = capture_graphs(lambda count: grid.step(count, stream), {1, width})
             torch.cuda.synchronize()
-        axis = 'xyz'.index(r.slice_axis)
-        plane_index = index_at(tuple(r.slice_position if i == axis else 0 for i in range(3)), r, r.field)[axis]
-        component = 'xyz'.index(r.field[1].lower())
-        eps = plan.epsilon
-
-        def decimate(a):
-            return a[::max(1, math.ceil(a.shape[0] / 256)), ::max(1, math.ceil(a.shape[1] / 256))]
-        sl = [slice(None)] * 3
-        sl[axis] = plane_index
-        eps_plane = np.array(decimate((eps[..., component] if eps.ndim == 4 else eps)[tuple(sl)]))
-        interval = max(r.snapshot_interval, math.ceil(r.steps / 100))
-        frames, frame_steps = [], []
         torch.cuda.synchronize()
         setup_seconds = time.perf_counter() - started
         compute_start = time.perf_counter()
-        completed, termination_reason, diagnostic_seconds, replays = 0, 'max_steps', 0., 0
-        barriers = set(range(interval, r.steps + 1, interval))
-        if diagnose:
-            barriers.update(range(control.check_interval, r.steps + 1, control.check_interval))
+        completed, termination_reason, replays = 0, 'max_steps', 0
         with torch.cuda.stream(stream):
-            for target, advance in observation_schedule(r.steps, width, barriers):
+            for target, advance in observation_schedule(r.steps, width, observer.barriers()):
                 if cancel is not None and cancel.is_set():
                     termination_reason = 'cancelled'
                     break
@@ -262,71 +361,12 @@ class Simulation:
                 else:
                     grid.step(advance, stream)
                 completed = target
-                stop = False
-                if diagnose and (completed % control.check_interval == 0 or completed == r.steps):
-                    t0 = time.perf_counter()
-                    energy, peak, finite = grid.diagnose()
-                    if not finite:
-                        raise FloatingPointError(f'Non-finite CPML or incident-line memory detected. (diagnostic step {completed})')
-                    try:
-                        stop = decision.update(completed, energy, peak)
-                    except FloatingPointError as exc:
-                        raise FloatingPointError(f'{exc} (diagnostic step {completed})') from exc
-                    diagnostic_seconds += time.perf_counter() - t0
-                if stop:
+                if observer.observe(completed, progress, compute_start):
                     termination_reason = 'decayed'
-                if completed % interval == 0 or completed == r.steps or stop:
-                    frame = decimate(grid.get_slice(r.field, axis, plane_index))
-                    if not np.isfinite(frame).all():
-                        raise FloatingPointError('Fields diverged. Check mesh, sources and precision.')
-                    frame = {'real': np.real, 'imag': np.imag, 'magnitude': np.abs, 'phase': np.angle}[r.complex_display](frame)
-                    frames.append(frame)
-                    frame_steps.append(completed)
-                    if progress:
-                        progress({'step': completed, 'total': r.steps, 'frame': frame.tolist(),
-                                  'elapsed': time.perf_counter() - compute_start,
-                                  'termination_reason': termination_reason if stop else None,
-                                  'diagnostics': decision.history[-1] if decision.history else None})
-                if stop:
                     break
         torch.cuda.synchronize()
         seconds = time.perf_counter() - compute_start
-        status = grid.device_status()
-        if status:
-            raise RuntimeError(f'A fused kernel reported device status {status}.')
-        e, h = grid.get_fields()
-        if not np.isfinite(e).all() or not np.isfinite(h).all():
-            raise FloatingPointError('Non-finite fields detected.')
-        traces = grid.get_traces()[:completed]
-        frequency_results = []
-        for k, pp in enumerate(plan.planes):
-            values = grid.get_plane(k)
-            frequency_results.append(plane_result(pp.monitor, pp.plan, pp.frequency, list(pp.components), values, r.dimension))
-        if frequency_results:
-            signature = run_signature(p, completed)
-            for m in frequency_results:
-                m['run_signature'] = signature
-        bytes_per_step = algorithmic_bytes_per_step(plan)
-        cells = math.prod(r.shape)
-        stats = dict(warnings=warnings, backend='cuda', precision=r.precision, gpu=torch.cuda.get_device_name(),
-                     cuda_graph=bool(graphs), cuda_graph_steps=width, cuda_graph_replays=replays,
-                     cuda_kernel=cuda_kernel, cuda_monitor_kernel='fused', kernel=grid.kernel,
-                     steps=completed, requested_steps=r.steps, cancelled=termination_reason == 'cancelled',
-                     termination_reason=termination_reason, auto_shutoff=termination_reason == 'decayed',
-                     diagnostics=decision.history, diagnostic_seconds=diagnostic_seconds,
-                     diagnostic_backend='fused_cuda' if diagnose else None,
-                     source_end_s=source_end if math.isfinite(source_end) else None,
-                     seconds=seconds, setup_seconds=setup_seconds,
-                     mcells_per_second=cells * completed / max(seconds, 1e-9) / 1e6,
-                     gcells_per_s=cells * completed / max(seconds, 1e-9) / 1e9,
-                     hbm_bytes_per_step=bytes_per_step, arena_bytes=grid.arena_bytes, free_device_bytes=free,
-                     field_peak=float(np.max(np.abs(e))), slice_index=plane_index,
-                     slice_position=(0 if r.dimension == '2d' and axis == 2 else (plane_index + .5) * r.mesh - r.actual_size[axis] / 2),
-                     complex_fields=False, complex_display=r.complex_display, material_update='nondispersive',
-                     dispersive_samples=0, material_sampling=r.material_sampling,
-                     epsilon_definition='instantaneous relative permittivity (epsilon-infinity for dispersive cells)',
-                     boundaries=r.boundaries.model_dump(), bloch_phase=r.bloch_phase,
-                     units='geometry: um; time: s; E/H: reduced fields; Bloch phase: rad', engine=ENGINE)
+        result = observer.result(completed, termination_reason, seconds, setup_seconds, cuda_graph=bool(graphs),
+                                 cuda_graph_steps=width, cuda_graph_replays=replays, free_device_bytes=free)
         grid.close()
-        return Result(p, stats, np.array(frames), np.array(frame_steps), eps_plane, traces,
-                      np.arange(1, completed + 1) * r.time_step, e, h, frequency_results)
+        return result
