@@ -1,7 +1,7 @@
 """Benchmark of the fused Yee/CPML engine: Gcell-updates/s and HBM-roofline fraction.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload roofline|strip]
+                    [--workload roofline|roofline256|strip|tmz2d|batch64]
 
 Workload (default ``roofline``): 3D full-vector Yee + CPML, FP32, 512 x 512 x 256 cells
 at 0.05 um, CPML 12 cells per face (cubic grading, sigma_max = 0.8 (m+1)/(eta0 dx),
@@ -87,7 +87,56 @@ def workload(name, steps, seed=2024):
                                                  spectrum=custom)])
         return project, None, ('3D Yee+CPML 160x120x40 (0.05 um), CPML 12, Si strip 0.65x0.4 um in SiO2, Ey dipole, '
                                'x-normal DFT plane at 1.55 um, FP32')
+    if name == 'tmz2d':
+        # 2D TMz plain-method case: 16 x 12 um at 0.05 um (320 x 240 cells), CPML 16, Courant 0.99/sqrt(2).
+        L = 16
+        b = Boundaries(**{f'{a}_{s}': baseline_face(L) for a in 'xy' for s in ('min', 'max')})
+        region = Region(dimension='2d', size=(16, 12, 1), mesh=.05, pml_cells=L, background_index=1.444, steps=steps,
+                        backend='cuda', cuda_kernel='fused', boundaries=b, run_control=control, snapshot_interval=10000)
+        custom = SpectrumSettings(sampling='custom', custom_frequencies_hz=[C0 / (lam * 1e-6)], apodization='none')
+        pulse = dict(component='Ez', wavelength=lam, pulse='broadband', time_definition='wavelength',
+                     wavelength_start=lam - .05, wavelength_stop=lam + .05)
+        project = Project(name='TMz waveguide 320x240', region=region, materials=[Material(name='core', index=3.476)],
+                          structures=[Structure(id='core', size=(16, .5, 1), material='core')],
+                          sources=[Source(id='src', center=(-2.5, 0, 0), **pulse)],
+                          monitors=[Monitor(id='probe', center=(2.5, 0, 0), component='Ez', spectrum=custom)])
+        return project, None, ('2D TMz 320x240 (0.05 um), CPML 16, eps 1.444^2 background with a 0.5 um x-directed core '
+                               'eps 3.476^2, Ez pulse at x=-2.5 um (1.50-1.60 um), Ez trace + DFT at 1.55 um, FP32')
     raise ValueError(name)
+
+
+def batch_workload(steps, seed=2024, count=64, mesh=.05, layers=16):
+    """64 independent 2D TMz grids, per-side cell counts drawn uniformly from 128 to 1024 (seeded), each with a
+    2 x 2 um design region of seeded random binary density (Gaussian-filtered, sigma 2 cells, thresholded at
+    0.5) mapping to eps in {2.085, 12.08} in an eps 2.085 background, CPML 16 cells, an Ez pulse 1.8 um left of
+    the design and an Ez trace + DFT 1.8 um right of it. Returns (projects, epsilon arrays, description)."""
+    from scipy.ndimage import gaussian_filter
+    from torchfdtd_b200 import Boundaries, Monitor, Project, Region, Source, SpectrumSettings
+    from torchfdtd_b200.models import RunControl
+    rng = np.random.default_rng(seed)
+    lam = 1.55
+    sides = rng.integers(128, 1025, size=(count, 2))
+    custom = SpectrumSettings(sampling='custom', custom_frequencies_hz=[C0 / (lam * 1e-6)], apodization='none')
+    pulse = dict(component='Ez', wavelength=lam, pulse='broadband', time_definition='wavelength', wavelength_start=lam - .05,
+                 wavelength_stop=lam + .05)
+    projects, eps = [], []
+    design = int(round(2.0 / mesh))
+    for k, (nx, ny) in enumerate(sides):
+        b = Boundaries(**{f'{a}_{s}': baseline_face(layers) for a in 'xy' for s in ('min', 'max')})
+        region = Region(dimension='2d', size=(nx * mesh, ny * mesh, 1), mesh=mesh, pml_cells=layers,
+                        background_index=2.085 ** .5, steps=steps, backend='cuda', cuda_kernel='fused', boundaries=b,
+                        run_control=RunControl(divergence_check=False), snapshot_interval=10000)
+        projects.append(Project(name=f'design {k}', region=region, sources=[Source(id='src', center=(-1.8, 0, 0), **pulse)],
+                                monitors=[Monitor(id='probe', center=(1.8, 0, 0), component='Ez', spectrum=custom)]))
+        rho = gaussian_filter(rng.integers(0, 2, size=(design, design)).astype(np.float64), 2.0) > .5
+        e = np.full((int(nx), int(ny), 1), 2.085, dtype=np.float32)
+        x0, y0 = int(nx) // 2 - design // 2, int(ny) // 2 - design // 2
+        e[x0:x0 + design, y0:y0 + design, 0] = np.where(rho, 12.08, 2.085)
+        eps.append(e)
+    cells = int(sum(int(a) * int(b) for a, b in sides))
+    return projects, eps, (f'{count} independent 2D TMz grids, sides uniform in [128, 1024] (seeded; {cells} cells in '
+                           'all), 2x2 um seeded binary design region (Gaussian sigma 2 cells, threshold 0.5) eps in '
+                           '{2.085, 12.08}, CPML 16, FP32, one persistent launch per step over all grids')
 
 
 def measured_peaks():
@@ -267,18 +316,20 @@ def run_ours(args, world, rank, local):
                     algorithmic_bytes_per_step=bytes_step, kernel=f'k_step_{kernel_used}',
                     note='achieved counts the whole step (fused step launch + observation launch)')
     # ---- end to end through the public API --------------------------------------------------
-    e2e_steps = max(10, args.steps)
-    e2e_project, e2e_eps, _ = workload(args.workload, e2e_steps)
-    barrier(world)
-    t0 = time.perf_counter()
-    result = Simulation(e2e_project, epsilon=e2e_eps).run(cuda_graph=True, cuda_graph_steps=16, kernel=args.kernel)
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    real = np.dtype(plan.dtype).itemsize
-    h2d = cells * plan.material_samples * real + sum(t.values.nbytes for t in plan.sources)
-    d2h = result.electric.nbytes + result.magnetic.nbytes + result.signals.nbytes + result.frames.nbytes
-    e2e = dict(value=world * cells * e2e_steps / e2e_s / 1e9, unit=METRIC, h2d_bytes_per_step=h2d / e2e_steps,
-               d2h_bytes_per_step=d2h / e2e_steps, seconds=e2e_s, steps=e2e_steps,
-               call='Simulation(project, epsilon).run(cuda_graph=True, cuda_graph_steps=16)')
+    e2e = None
+    if not args.no_e2e:
+        e2e_steps = max(10, args.steps)
+        e2e_project, e2e_eps, _ = workload(args.workload, e2e_steps)
+        barrier(world)
+        t0 = time.perf_counter()
+        result = Simulation(e2e_project, epsilon=e2e_eps).run(cuda_graph=True, cuda_graph_steps=16, kernel=args.kernel)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+        real = np.dtype(plan.dtype).itemsize
+        h2d = cells * plan.material_samples * real + sum(t.values.nbytes for t in plan.sources)
+        d2h = result.electric.nbytes + result.magnetic.nbytes + result.signals.nbytes + result.frames.nbytes
+        e2e = dict(value=world * cells * e2e_steps / e2e_s / 1e9, unit=METRIC, h2d_bytes_per_step=h2d / e2e_steps,
+                   d2h_bytes_per_step=d2h / e2e_steps, seconds=e2e_s, steps=e2e_steps,
+                   call='Simulation(project, epsilon).run(cuda_graph=True, cuda_graph_steps=16)')
     line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=elapsed / args.steps * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
                 data='synthetic (seeded)', config=dict(workload=desc, cells=cells, l2='inputs larger than L2 (no flush needed)',
@@ -293,28 +344,166 @@ def run_ours(args, world, rank, local):
     return line if rank == 0 else None
 
 
+def batch_cpu_rate(plans, budget_s, threads=None):
+    """Cell-updates/s of the C oracle over a batch, one grid after another (as the reference's CPU path runs
+    them), round-robin one step per grid until the budget is spent."""
+    from oracle.cpu import CpuOracle
+    oracles, cells, t0, k = {}, 0, None, 0
+    while True:
+        i = k % len(plans)
+        if i not in oracles:
+            oracles[i] = CpuOracle(plans[i], threads=threads)
+            oracles[i].run(1)                      # first touch, untimed
+        if t0 is None:
+            t0 = time.perf_counter()
+        oracles[i].run(1)
+        cells += plans[i].cells
+        k += 1
+        elapsed = time.perf_counter() - t0
+        if elapsed >= budget_s and k >= len(plans):
+            break
+        if elapsed >= budget_s * 2:
+            break
+    threads = next(iter(oracles.values())).threads
+    return cells / elapsed / 1e9, k, elapsed, threads
+
+
+def batch_plans(projects, eps):
+    from torchfdtd_b200.simulation import Simulation
+    return [Simulation(p, epsilon=e).plan for p, e in zip(projects, eps)]
+
+
+def run_reference_batch(args, world, rank):
+    if rank != 0:
+        return None
+    projects, eps, desc = batch_workload(max(10, args.steps))
+    plans = batch_plans(projects, eps)
+    budget = 120.0 * args.steps / max(1, args.steps + args.warmup)
+    rate, steps, elapsed, threads = batch_cpu_rate(plans, budget)
+    sample = (f'{steps} grid-steps (one time step of one grid each, round-robin over the {len(plans)} grids) on {threads} '
+              f'host threads (C port of the reference NumPy Yee/CPML update), {elapsed:.1f} s')
+    return dict(metric=METRIC, value=rate, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                ms_per_step=sum(p.cells for p in plans) / rate / 1e6, higher_is_better=True, scaling='weak',
+                vs_baseline=None, dtype='f32', data='synthetic', impl='reference',
+                config=dict(workload=desc, cells=sum(p.cells for p in plans), parallelism='host threads'),
+                cpu_baseline=dict(value=rate, unit=METRIC, cores=threads, kind='port', sample=sample),
+                e2e=dict(value=rate, unit=METRIC, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+
+
+def run_ours_batch(args, world, rank, local):
+    import torch
+    from torchfdtd_b200.batch import run_tensor_batch
+    from torchfdtd_b200.native import NativeBatch, NativeGrid
+    from torchfdtd_b200.simulation import algorithmic_bytes_per_step
+    from torchfdtd_b200.tuning import tune_tensor_batch
+    device = torch.device('cuda', local)
+    torch.cuda.set_device(device)
+    total_steps = args.warmup + args.steps
+    config_steps = 3000
+    projects, eps, desc = batch_workload(max(config_steps, total_steps + 64))
+    plans = batch_plans(projects, eps)
+    cells = sum(p.cells for p in plans)
+    if args.batch_launch:
+        choice = [int(v) for v in args.batch_launch.split(',')]
+        tuning = None
+    else:
+        tuning = tune_tensor_batch(projects, epsilon=eps, device=local)
+        choice = tuning.choice
+    grids = [NativeGrid(plan, kernel='tile2d') for plan in plans]
+    batch = NativeBatch(grids)
+    batch.set_launch(*choice)
+    tiles = batch.tiles()
+    stream = torch.cuda.Stream(device)
+    sampler = ClockSampler(local)
+    sampler.start()
+    with torch.cuda.stream(stream):
+        batch.step(args.warmup, stream)
+        stream.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_wall = time.time()
+        start.record(stream)
+        batch.step(args.steps, stream)
+        end.record(stream)
+        end.synchronize()
+        t_wall_end = time.time()
+    torch.cuda.synchronize()
+    barrier(world)
+    sampler.window = (t_wall, t_wall_end)
+    clocks = sampler.finish()
+    elapsed = max_over_ranks(start.elapsed_time(end) / 1e3, world)
+    status = max(g.device_status() for g in grids)
+    batch.close()
+    for g in grids:
+        g.close()
+    del grids, batch
+    torch.cuda.empty_cache()
+    value = world * cells * args.steps / elapsed / 1e9
+    bytes_step = sum(algorithmic_bytes_per_step(p) for p in plans)
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_step * args.steps / elapsed / 1e9
+    roofline = dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak,
+                    traffic=MEASURED_TRAFFIC_PER_CELL.get(('batch64', 'tile2d')), peak_source=peak_kind,
+                    algorithmic_bytes_per_step=bytes_step, kernel='k_step2d_tm',
+                    note='achieved counts the whole step (batched tile launch + batched observation launch)')
+    # ---- end to end: the public batch call over the configured 3000 steps ------------------------------
+    e2e = None
+    if not args.no_e2e:
+        e2e_projects, e2e_eps, _ = batch_workload(config_steps)
+        barrier(world)
+        t0 = time.perf_counter()
+        report = run_tensor_batch(e2e_projects, epsilon=e2e_eps, cuda_graph=True, cuda_graph_steps=16, launch=choice)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+        report.raise_for_errors()
+        h2d = sum(p.cells * 4 + sum(t.values.nbytes for t in p.sources) for p in plans)
+        d2h = sum(i.result.electric.nbytes + i.result.magnetic.nbytes + i.result.signals.nbytes + i.result.frames.nbytes
+                  for i in report.items)
+        e2e = dict(value=world * cells * config_steps / e2e_s / 1e9, unit=METRIC, h2d_bytes_per_step=h2d / config_steps,
+                   d2h_bytes_per_step=d2h / config_steps, seconds=e2e_s, steps=config_steps,
+                   loop_seconds=report.plan['loop_seconds'], setup_seconds=report.plan['setup_seconds'],
+                   call='run_tensor_batch(projects, epsilon=eps, cuda_graph=True, cuda_graph_steps=16, launch=tuned)')
+    line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                ms_per_step=elapsed / args.steps * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
+                data='synthetic (seeded)',
+                config=dict(workload=desc, cells=cells, grids=len(plans), strips=tiles, launch=choice,
+                            tuning=[(r['ctas'], r['rows'], r['strips'], round(r['median_ms_per_step'], 5))
+                                    for r in tuning.candidates] if tuning else 'fixed by --batch-launch',
+                            l2='inputs larger than L2 (no flush needed)',
+                            parallelism=f'replicas x{world}' if world > 1 else 'single GPU', kernel='tile2d'),
+                roofline=roofline, e2e=e2e, clocks=clocks, gpu_launches=2 * args.steps, device_status=status)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, steps, el, threads = batch_cpu_rate(plans, args.cpu_budget)
+        line['cpu_baseline'] = dict(value=rate, unit=METRIC, cores=threads, kind='port',
+                                    sample=f'{steps} grid-steps round-robin over the {len(plans)} grids on {threads} host '
+                                           f'threads (C port of the reference NumPy update), {el:.1f} s')
+    return line if rank == 0 else None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=200)
     ap.add_argument('--warmup', type=int, default=10)
     ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
-    ap.add_argument('--workload', choices=['roofline', 'roofline256', 'strip'], default='roofline')
-    ap.add_argument('--kernel', choices=['auto', 'march', 'gather'], default='auto')
+    ap.add_argument('--workload', choices=['roofline', 'roofline256', 'strip', 'tmz2d', 'batch64'], default='roofline')
+    ap.add_argument('--kernel', choices=['auto', 'march', 'gather', 'tile2d'], default='auto')
     ap.add_argument('--cpu-budget', type=float, default=15.0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end leg (profiling runs)')
+    ap.add_argument('--batch-launch', default=None, help='batch64: fixed "ctas,rows" instead of the autotuner')
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == 'reference':
         # Rank 0 alone times the host-core reference; other ranks exit without work.
         world, rank, local = int(os.environ.get('WORLD_SIZE', '1')), int(os.environ.get('RANK', '0')), 0
-        line = run_reference(args, world, rank)
+        line = (run_reference_batch if args.workload == 'batch64' else run_reference)(args, world, rank)
         if line is not None:
             print(json.dumps(line), flush=True)
         return
     world, rank, local = dist_setup(args)
     try:
-        line = run_reference(args, world, rank) if args.impl == 'reference' else run_ours(args, world, rank, local)
+        line = (run_ours_batch if args.workload == 'batch64' else run_ours)(args, world, rank, local)
         if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
     finally:

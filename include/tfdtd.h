@@ -168,7 +168,8 @@ int tfd_diagnose(tfd_plan *plan, double out[3], void *stream);
 /* The device step counter (synchronises the stream). */
 int tfd_counter(tfd_plan *plan, int64_t *value, void *stream);
 
-/* The device status word: 0, or the code a kernel recorded (synchronises the stream). */
+/* The device status word: 0, or the code a kernel recorded (synchronises the stream): 1 step counter out of
+ * range, 2 a bounded pipeline wait timed out, 3 a strip table entry failed the 2D kernel's own checks. */
 int tfd_device_status(tfd_plan *plan, int32_t *status, void *stream);
 
 /* Field energy and peak without any device allocation and without a plan. No counterpart in the
@@ -198,8 +199,10 @@ int tfd_kernel_in_use(const tfd_plan *plan, int32_t *kernel);
 typedef struct tfd_batch tfd_batch;
 int tfd_batch_bytes(int32_t n_plans, tfd_plan *const *plans, size_t *bytes);
 int tfd_batch_create(int32_t n_plans, tfd_plan *const *plans, void *arena, size_t arena_bytes, void *stream, tfd_batch **batch);
-/* Persistent CTA count of the batched step kernel (0: one wave of resident CTAs); the autotuner's knob. */
-int tfd_batch_set_ctas(tfd_batch *batch, int32_t ctas);
+/* Launch shape of the batched step kernel, the autotuner's knobs: ctas = persistent CTA count (0: one warp
+ * per strip), strip_rows = rows per strip (0: default for the batch's cell count; else >= 8). Rebuilds the
+ * strip table on the stream when strip_rows changes; call it outside graph capture. */
+int tfd_batch_set_launch(tfd_batch *batch, int32_t ctas, int32_t strip_rows, void *stream);
 int tfd_batch_step(tfd_batch *batch, int32_t nsteps, void *stream);
 int tfd_batch_tiles(const tfd_batch *batch, int32_t *tiles);
 void tfd_batch_destroy(tfd_batch *batch);

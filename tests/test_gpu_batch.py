@@ -208,7 +208,8 @@ def test_raw_batch_with_random_start_matches_oracle():
         grids.append(g)
         oracles.append(oracle.run())
     batch = NativeBatch(grids)
-    batch.set_ctas(7)
+    batch.set_launch(7, 9)
+    assert batch.tiles() > len(grids)
     with pytest.raises(ValueError, match='batch'):
         grids[0].step(1)
     batch.step(30)
@@ -243,3 +244,29 @@ def test_grouped_batch_runs_mixed_cases_in_input_order():
     assert [i.id for i in report.items] == [f'case-{k:04d}' for k in range(4)]
     assert report.items[1].summary['kernel'] in ('march', 'gather')
     assert_results_equal(report.items[2].result, Simulation(projects[1]).run(kernel='tile2d'))
+
+
+def test_batch_tuner_picks_a_measured_cta_count_and_results_do_not_change():
+    from torchfdtd_b200.batch import run_tensor_batch
+    from torchfdtd_b200.tuning import tune_tensor_batch
+    projects = uneven_cases()
+    shapes = [(1, 8), (4, 0), (0, 12), (0, 0)]
+    tuning = tune_tensor_batch(projects, candidates=shapes, steps=2, repeats=3)
+    assert tuning.kind == 'batch' and tuple(tuning.choice) in shapes
+    assert sorted((r['ctas'], r['rows']) for r in tuning.candidates) == sorted(shapes)
+    auto = run_tensor_batch(projects, launch='auto')
+    plain = run_tensor_batch(projects)
+    assert auto.plan['tuning']['kind'] == 'batch'
+    for a, b in zip(auto.items, plain.items):
+        assert_results_equal(a.result, b.result)
+
+
+def test_batch_accepts_per_case_epsilon():
+    from torchfdtd_b200 import Simulation
+    from torchfdtd_b200.batch import run_tensor_batch
+    projects = uneven_cases()[:3]
+    rng = np.random.default_rng(4)
+    eps = [None] + [rng.uniform(1, 4, size=tuple(plan_grid(p).shape)).astype(np.float32) for p in projects[1:]]
+    report = run_tensor_batch(projects, epsilon=eps)
+    for p, e, item in zip(projects, eps, report.items):
+        assert_results_equal(item.result, Simulation(p, epsilon=e).run(kernel='tile2d'))

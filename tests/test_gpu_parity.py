@@ -260,3 +260,48 @@ def test_invalid_descriptor_is_refused_with_a_named_error():
     size = ctypes.c_size_t()
     with pytest.raises(ValueError, match='precision'):
         nat.check(nat.library().tfd_plan_bytes(ctypes.byref(desc), ctypes.byref(size)))
+
+
+@pytest.mark.parametrize('variant', [14, 23, 32, 22, 114, 123, 4014, 7023])
+def test_march_launch_variants_match_oracle(variant):
+    """Every launch shape the autotuner may pick (prefetch depth, CTAs per SM, interior split, z-chunk)."""
+    from torchfdtd_b200.native import NativeGrid
+    project = random_project('3d', 'float32', steps=14)
+    plan = plan_grid(project)
+    rng = np.random.default_rng(variant)
+    oracle = YeeOracle(plan)
+    oracle.E[:] = rng.normal(size=oracle.E.shape).astype(plan.dtype) * .01
+    oracle.H[:] = rng.normal(size=oracle.H.shape).astype(plan.dtype) * .01
+    g = NativeGrid(plan, kernel='march', variant=variant)
+    g.set_fields(oracle.E, oracle.H)
+    oracle.run()
+    g.step(plan.steps)
+    E, H = g.get_fields()
+    np.testing.assert_array_equal(E, oracle.E)
+    np.testing.assert_array_equal(H, oracle.H)
+    assert g.device_status() == 0
+
+
+def test_invalid_launch_variant_is_refused():
+    from torchfdtd_b200.native import NativeGrid
+    plan = plan_grid(random_project('3d', 'float32'))
+    with pytest.raises(ValueError, match='launch variant'):
+        NativeGrid(plan, kernel='march', variant=15)
+    plan64 = plan_grid(random_project('3d', 'float64'))
+    with pytest.raises(ValueError, match='launch variant'):
+        NativeGrid(plan64, kernel='march', variant=14)
+
+
+def test_select_launch_measures_candidates_and_simulation_uses_the_winner():
+    from torchfdtd_b200 import Simulation
+    from torchfdtd_b200.tuning import select_launch
+    project = random_project('3d', 'float32', steps=40)
+    plan = plan_grid(project)
+    tuning = select_launch(plan, candidates=[14, 23, 4014], steps=4, repeats=3)
+    assert tuning.kind == 'grid' and tuning.choice in (14, 23, 4014)
+    assert all(r['status'] == 'completed' and len(r['samples_ms_per_step']) == 3 for r in tuning.candidates)
+    assert select_launch(plan, candidates=[14, 23, 4014], steps=4, repeats=3).cached
+    tuned = Simulation(project).run(launch='auto')
+    plain = Simulation(project).run()
+    np.testing.assert_array_equal(tuned.electric, plain.electric)
+    assert tuned.summary['launch_tuning']['kind'] == 'grid'

@@ -157,14 +157,18 @@ def _admit(cases, memory_fraction):
 
 
 def run_tensor_batch(cases, *, objective=None, output_dir=None, keep_results=True, device=0, memory_fraction=.6,
-                     cuda_graph=True, cancel=None, progress=None, cohort_size=None, cuda_graph_steps=1, ctas=None):
+                     cuda_graph=True, cancel=None, progress=None, cohort_size=None, cuda_graph_steps=1, launch=None,
+                     epsilon=None):
     """Run independent 2D TMz projects in fused cohorts of 1-64 cases (reference tensor_batch.py:45-113).
 
     Shapes, time steps, CPML depths, sources, monitors and step counts may differ between cases; one
-    precision per cohort. ``ctas`` overrides the persistent CTA count of the step kernel (``tune_tensor_batch``
-    measures it); by default one wave of resident CTAs. Auto shutoff is rejected, never silently disabled.
-    A numerical failure aborts the cohort, an invalid objective marks only its item failed. Result summary
-    seconds describe the whole cohort.
+    precision per cohort. ``launch`` sets the step kernel's launch shape: None for the default (one warp per
+    strip, strip rows sized to the cohort), a ``(ctas, strip_rows)`` pair (0 keeps a default), or 'auto' to
+    measure candidates on scratch copies first (``tune_tensor_batch``).
+    ``epsilon`` (optional): one permittivity array (or None) per case, replacing its voxelized structures as
+    ``Simulation(project, epsilon)`` does. Auto shutoff is rejected, never silently disabled. A numerical
+    failure aborts the cohort, an invalid objective marks only its item failed. Result summary seconds
+    describe the whole cohort.
     """
     import torch
     validate_graph_steps(cuda_graph_steps, cuda_graph)
@@ -176,6 +180,11 @@ def run_tensor_batch(cases, *, objective=None, output_dir=None, keep_results=Tru
     if root and ((root / 'tensor-batch.json').exists() or any((root / (c.id + '.npz')).exists() for c in cases)):
         raise FileExistsError('Tensor batch output exists. Use a new directory.')
     projects = _admit(cases, memory_fraction)
+    if epsilon is None:
+        epsilon = [None] * len(cases)
+    epsilon = list(epsilon)
+    if len(epsilon) != len(cases):
+        raise ValueError('epsilon needs one entry (an array or None) per case.')
     if not torch.cuda.is_available():
         raise RuntimeError('Tensor batch requires CUDA.')
     if isinstance(device, bool) or not isinstance(device, int) or not 0 <= device < torch.cuda.device_count():
@@ -192,7 +201,7 @@ def run_tensor_batch(cases, *, objective=None, output_dir=None, keep_results=Tru
                 progress(dict(state, cohort_offset=offset, total_cases=len(cases)))
             report = _run_cohort(cases[offset:offset + cohort_size], projects[offset:offset + cohort_size], objective, root,
                                  keep_results, memory_fraction, cuda_graph, cancel, on_progress if progress else None,
-                                 cuda_graph_steps, ctas)
+                                 cuda_graph_steps, launch, epsilon[offset:offset + cohort_size])
             items.extend(report.items)
             plans.append(report.plan)
         plan = plans[0] if len(plans) == 1 else dict(
@@ -208,11 +217,19 @@ def run_tensor_batch(cases, *, objective=None, output_dir=None, keep_results=Tru
 
 
 def _run_cohort(cases, projects, objective, root, keep_results, memory_fraction, cuda_graph, cancel, progress,
-                cuda_graph_steps, ctas):
+                cuda_graph_steps, launch, epsilon):
     import torch
     from .native import NativeBatch, NativeGrid
     started, wall_started = time.perf_counter(), time.time()
-    sims = [Simulation(p) for p in projects]
+    tuning = None
+    if launch == 'auto':
+        from .tuning import tune_tensor_batch
+        try:
+            tuning = tune_tensor_batch(cases, device=torch.cuda.current_device(), epsilon=epsilon).as_dict()
+            launch = tuning['choice']
+        except ValueError as exc:                  # runs too short to tune on scratch state
+            tuning, launch = dict(skipped=str(exc)), None
+    sims = [Simulation(p, epsilon=e) for p, e in zip(projects, epsilon)]
     plans = [s.plan for s in sims]
     estimate = sum(NativeGrid.plan_bytes(plan) for plan in plans)
     free, _ = torch.cuda.mem_get_info()
@@ -222,8 +239,8 @@ def _run_cohort(cases, projects, objective, root, keep_results, memory_fraction,
     observers = [Observer(p, plan, g, label=f'Case {c.id}: ') for c, p, plan, g in zip(cases, projects, plans, grids)]
     batch = NativeBatch(grids)
     try:
-        if ctas:
-            batch.set_ctas(ctas)
+        if launch is not None:
+            batch.set_launch(*launch)
         steps = max(p.region.steps for p in projects)
         stream = torch.cuda.Stream()
         stream.wait_stream(torch.cuda.current_stream())
@@ -297,7 +314,7 @@ def _run_cohort(cases, projects, objective, root, keep_results, memory_fraction,
     plan = dict(execution='fused_cuda_batch', batch_size=len(cases), device=str(grids[0].device),
                 estimated_memory_mb=estimate / 2**20, memory_fraction=memory_fraction, loop_seconds=seconds,
                 setup_seconds=setup_seconds, graph=bool(graphs), cuda_graph_steps=width, cuda_graph_replays=replays,
-                tiles=tiles, ctas=ctas, gcells_per_s=cells / max(seconds, 1e-9) / 1e9, resume=False)
+                tiles=tiles, launch=list(launch) if launch is not None else None, tuning=tuning, gcells_per_s=cells / max(seconds, 1e-9) / 1e9, resume=False)
     return BatchReport(items, time.perf_counter() - started, plan)
 
 
@@ -338,7 +355,7 @@ def plan_grouped_batch(cases, *, cohort_size=MAX_COHORT):
 
 
 def run_grouped_batch(cases, *, cohort_size=MAX_COHORT, objective=None, output_dir=None, keep_results=True, device=0,
-                      memory_fraction=.6, cuda_graph=True, cuda_graph_steps=1, cancel=None, progress=None, ctas=None):
+                      memory_fraction=.6, cuda_graph=True, cuda_graph_steps=1, cancel=None, progress=None, launch=None):
     """Run mixed projects: batchable 2D TMz cases in fused cohorts by precision, the rest one by one
     through ``Simulation`` (reference grouped_batch.py:90-146). Items come back in input order."""
     import torch
@@ -391,7 +408,7 @@ def run_grouped_batch(cases, *, cohort_size=MAX_COHORT, objective=None, output_d
         report = run_tensor_batch(chosen, cohort_size=len(chosen), objective=objective, output_dir=out,
                                   keep_results=keep_results, device=device, memory_fraction=memory_fraction,
                                   cuda_graph=cuda_graph, cuda_graph_steps=cuda_graph_steps, cancel=cancel,
-                                  progress=on_progress if progress else None, ctas=ctas)
+                                  progress=on_progress if progress else None, launch=launch)
         items.update((item.id, item) for item in report.items)
         executions.append(dict(cohort=number, **report.plan))
     ordered = [items.get(c.id, BatchItem(c.id, 'cancelled', c.parameters)) for c in cases]

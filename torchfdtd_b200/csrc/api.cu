@@ -1,6 +1,7 @@
 // C ABI of libtfdtd: arena layout, table upload, step dispatch, layout conversion and
 // diagnostics. Declarations and the reference interfaces they replace: include/tfdtd.h.
 #include <algorithm>
+#include <memory>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -29,6 +30,29 @@ int fail(int code, const std::string &msg) {
         cudaError_t e_ = (expr);                                                                       \
         if (e_ != cudaSuccess) return fail(TFD_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
     } while (0)
+
+#define TFD_CHECK(expr)      \
+    do {                     \
+        const int rc_ = (expr); \
+        if (rc_) return rc_; \
+    } while (0)
+
+// A side stream and its fork/join events, so that the general strips run beside the interior strips.
+struct SideStream {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    int create() {
+        TFD_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        TFD_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+        TFD_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+        return TFD_OK;
+    }
+    ~SideStream() {
+        if (stream) cudaStreamDestroy(stream);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+    }
+};
 
 constexpr int kMaskTM = 0x04 | 0x08 | 0x10;   // Ez, Hx, Hy
 constexpr int kMaskTE = 0x01 | 0x02 | 0x20;   // Ex, Ey, Hz
@@ -63,7 +87,7 @@ struct Layout {
     std::vector<PlaneLayout> planes;
     size_t counter = 0, done = 0, status = 0, diag = 0, stage = 0;
     size_t grid_tab = 0, tile_tab = 0;   // 2D tile kernel: this plan's Grid struct and its tile table
-    int tiles2d = 0;
+    int tiles2d = 0, strip_rows = 8;
     size_t stage_bytes = 0;
     size_t psi_total = 0;          // elements of the reference psi vector
     size_t total = 0;
@@ -177,8 +201,86 @@ std::vector<PsiSegment> psi_segments(const tfd_desc *d, size_t *total) {
 
 // The 2D tile kernel runs 2D TMz grids whose x and y faces are PML or PEC.
 bool tile2d_capable(const tfd_desc *d) {
-    return d->nz == 1 && d->components == kMaskTM && d->face[0][0] != TFD_FACE_PERIODIC && d->face[1][0] != TFD_FACE_PERIODIC;
+    return d->nz == 1 && d->components == kMaskTM && d->face[0][0] != TFD_FACE_PERIODIC && d->face[1][0] != TFD_FACE_PERIODIC &&
+           (long long)d->ny * ((d->nx + kPitchAlign - 1) / kPitchAlign * kPitchAlign) < (1LL << 31);
 }
+
+// What the strip table of a 2D grid depends on: its size, its CPML slabs and its source boxes.
+struct StripGeom {
+    int nx = 0, ny = 0;
+    struct Slab { int family, axis, lo, hi; };
+    std::vector<Slab> slabs;
+    std::vector<SourceTerm> sources;
+};
+
+StripGeom strip_geom(const tfd_desc *d) {
+    StripGeom G;
+    G.nx = d->nx;
+    G.ny = d->ny;
+    for (int k = 0; k < d->n_segments; ++k)
+        G.slabs.push_back({d->segments[k].forward, d->segments[k].axis, d->segments[k].lo, d->segments[k].hi});
+    for (int k = 0; k < d->n_sources; ++k) {
+        const tfd_source_term &t = d->sources[k];
+        SourceTerm q{t.family, t.component, {t.lo[0], t.lo[1], t.lo[2]}, {t.hi[0], t.hi[1], t.hi[2]}};
+        G.sources.push_back(q);
+    }
+    return G;
+}
+
+// Strips of one grid: rows split into a lower boundary band, an interior band and an upper boundary band
+// (so that whole strips avoid the y slabs), each band cut into strips of `rows` rows, columns in steps of
+// 31, x-fastest so that neighbouring strips (which share halo columns) run together. A strip is interior
+// (kind 1) when all 32 columns and its rows, halo row included, avoid the grid edges, every CPML slab and
+// every source box; the kernel then runs the bare stencil.
+std::vector<Tile2D> strips_of(const StripGeom &G, int grid_index, int rows) {
+    const int nx = G.nx, ny = G.ny;
+    int fb0 = 1, fb1 = ny - 1;                       // interior rows: y0 >= fb0 and halo row y1 <= fb1
+    for (const auto &sl : G.slabs) {
+        if (sl.axis != 1 || sl.hi <= sl.lo) continue;
+        if (sl.lo + sl.hi < ny) fb0 = std::max(fb0, sl.hi);                         // lower slab
+        else fb1 = std::min(fb1, sl.family == 0 ? sl.lo - 1 : sl.lo);                // upper slab (E rows up to y1, H up to y1-1)
+    }
+    std::vector<std::pair<int, int>> bands;
+    if (fb1 > fb0) bands = {{0, fb0}, {fb0, fb1}, {fb1, ny}};
+    else bands = {{0, ny}};
+    auto x_interior = [&](int x0) {
+        if (x0 < 1 || x0 + 31 > nx - 1) return false;
+        for (const auto &sl : G.slabs) {
+            if (sl.axis != 0 || sl.hi <= sl.lo) continue;
+            const int last = sl.family == 0 ? x0 + 31 : x0 + 30;                    // E on all 32 lanes, H on 31
+            if (sl.lo <= last && x0 < sl.hi) return false;
+        }
+        return true;
+    };
+    auto no_source = [&](int x0, int y0, int y1) {
+        for (const auto &q : G.sources) {
+            const int xe = q.family == 0 ? x0 + 32 : x0 + k2dOwnX, ye = q.family == 0 ? y1 + 1 : y1;
+            if (q.lo[0] < xe && x0 < q.hi[0] && q.lo[1] < ye && y0 < q.hi[1]) return false;
+        }
+        return true;
+    };
+    std::vector<Tile2D> t;
+    for (size_t b = 0; b < bands.size(); ++b) {
+        const bool inner = bands.size() == 3 && b == 1;
+        for (int y0 = bands[b].first; y0 < bands[b].second; y0 += rows) {
+            const int y1 = std::min(y0 + rows, bands[b].second);
+            for (int x0 = 0; x0 < nx; x0 += k2dOwnX) {
+                const int kind = inner && x_interior(x0) && no_source(x0, y0, y1) ? 1 : 0;
+                t.push_back(Tile2D{grid_index, x0, y0, y1, kind});
+            }
+        }
+    }
+    // Interior strips first: the lean kernel walks [0, interior), the general kernel the rest.
+    std::stable_partition(t.begin(), t.end(), [](const Tile2D &a) { return a.kind == 1; });
+    return t;
+}
+
+int interior_count(const std::vector<Tile2D> &t) {
+    return (int)std::count_if(t.begin(), t.end(), [](const Tile2D &a) { return a.kind == 1; });
+}
+
+// Upper bound of the strip count of a grid for strips of at least 8 rows (two band edges add two cuts).
+int strip_capacity(int nx, int ny) { return ((nx + k2dOwnX - 1) / k2dOwnX) * ((ny + 7) / 8 + 2); }
 
 void compute_layout(const tfd_desc *d, Layout &L) {
     Bump b;
@@ -237,7 +339,8 @@ void compute_layout(const tfd_desc *d, Layout &L) {
         largest_plane = std::max(largest_plane, acc);
     }
     if (tile2d_capable(d)) {
-        L.tiles2d = ((d->nx + k2dOwnX - 1) / k2dOwnX) * ((d->ny + k2dOwnY - 1) / k2dOwnY);
+        L.strip_rows = strip_rows((long long)d->nx * d->ny);
+        L.tiles2d = (int)strips_of(strip_geom(d), 0, L.strip_rows).size();
         L.grid_tab = b.take(std::max(sizeof(Grid<float>), sizeof(Grid<double>)));
         L.tile_tab = b.take((size_t)L.tiles2d * sizeof(Tile2D));
     }
@@ -286,7 +389,8 @@ struct tfd_plan {
         if (fork) cudaEventDestroy(fork);
     }
     int march_variant = 42;
-    int tile2d_ctas = 0;
+    int tile2d_interior = 0;
+    std::unique_ptr<SideStream> side2d;
     bool in_batch = false;
     long long *own_counter = nullptr;
     std::vector<int> seg_f, seg_a, seg_lo, seg_hi;
@@ -503,7 +607,7 @@ bool march_supported(const tfd_plan *p) {
 }
 
 template <typename T, int SAMPLES, int D, int MINB>
-int setup_march_s(tfd_plan *p) {
+int setup_march_s(tfd_plan *p, bool split_interior, int lz_fixed) {
     using S = MarchShape<T, SAMPLES, D>;
     Grid<T> &g = p->grid<T>();
     MarchArgs<T> &a = p->march<T>();
@@ -560,6 +664,7 @@ int setup_march_s(tfd_plan *p) {
     // Planes per chunk for a launch of `tiles` tiles sharing `share` of the resident CTA slots: balance
     // whole waves against the two extra planes a chunk loads.
     auto choose_lz = [&](long long tiles, double share) {
+        if (lz_fixed > 0) return std::min(lz_fixed, g.n[2]);
         const double slots = std::max(1.0, share * resident);
         double best = -1;
         int best_lz = g.n[2];
@@ -598,9 +703,8 @@ int setup_march_s(tfd_plan *p) {
     while (iy1 < ty && interior_y(iy1)) ++iy1;
     p->march_launches.clear();
     // The interior/boundary split is off by default: measured on B200 at 512x512x256 it is slower
-    // (50.6 vs 54.8 Gcell/s) than one general launch; TFD_MARCH_SPLIT=1 enables it.
-    const char *split = getenv("TFD_MARCH_SPLIT");
-    if (ix1 > ix0 && iy1 > iy0 && split && std::string(split) == "1") {
+    // (50.6 vs 54.8 Gcell/s) than one general launch; launch variants >= 100 enable it.
+    if (ix1 > ix0 && iy1 > iy0 && split_interior) {
         const long long all = (long long)tx * ty, inner = (long long)(ix1 - ix0) * (iy1 - iy0);
         const double inner_share = (double)inner / all, strip_share = 1.0 - inner_share;
         const int lzi = choose_lz(inner, inner_share);
@@ -631,18 +735,27 @@ int setup_march_s(tfd_plan *p) {
     return TFD_OK;
 }
 
-// Prefetch depth D / CTAs per SM of the marching kernel, as the two digits of a variant:
-// 14 (FP32 default), 23, 32 and 22 (FP64 default). TFD_MARCH_VARIANT overrides it for launch-shape sweeps.
+// Launch variant of the marching kernel, as decimal digits: lz * 1000 + split * 100 + D * 10 + MINB.
+// D / MINB: prefetch depth and CTAs per SM, one of 14 (FP32 default), 23, 32, 22 (FP64: 22 only);
+// split 1: interior tiles as their own launch; lz: z-planes per CTA chunk (0: sized to whole waves).
+// 0 selects the default (TFD_MARCH_VARIANT in the environment overrides the default, for sweeps).
 template <typename T>
 int setup_march(tfd_plan *p) {
     const char *env = getenv("TFD_MARCH_VARIANT");
-    const std::string v = p->desc.launch_variant ? std::to_string(p->desc.launch_variant)
-                                                 : (env ? env : (sizeof(T) == 4 ? "14" : "22"));
-    const bool three = p->desc.material_samples == 3;
-    if (sizeof(T) == 8 || v == "22") return three ? setup_march_s<T, 3, 2, 2>(p) : setup_march_s<T, 1, 2, 2>(p);
-    if (v == "32") return three ? setup_march_s<T, 3, 3, 2>(p) : setup_march_s<T, 1, 3, 2>(p);
-    if (v == "14") return three ? setup_march_s<T, 3, 1, 4>(p) : setup_march_s<T, 1, 1, 4>(p);
-    return three ? setup_march_s<T, 3, 2, 3>(p) : setup_march_s<T, 1, 2, 3>(p);
+    int v = p->desc.launch_variant;
+    if (v == 0) v = env ? std::atoi(env) : 0;
+    if (v == 0) v = sizeof(T) == 4 ? 14 : 22;
+    const int dm = v % 100, split = (v / 100) % 10, lz = v / 1000;
+    if (v < 0 || split > 1 || (dm != 14 && dm != 22 && dm != 23 && dm != 32) || (sizeof(T) == 8 && dm != 22))
+        return fail(TFD_ERR_INVALID, "launch variant " + std::to_string(v) + " is not lz*1000 + split*100 + one of " +
+                                         (sizeof(T) == 8 ? std::string("22 (FP64)") : std::string("14, 22, 23, 32")));
+    const bool three = p->desc.material_samples == 3, sp = split == 1;
+    switch (dm) {
+        case 22: return three ? setup_march_s<T, 3, 2, 2>(p, sp, lz) : setup_march_s<T, 1, 2, 2>(p, sp, lz);
+        case 32: return three ? setup_march_s<T, 3, 3, 2>(p, sp, lz) : setup_march_s<T, 1, 3, 2>(p, sp, lz);
+        case 14: return three ? setup_march_s<T, 3, 1, 4>(p, sp, lz) : setup_march_s<T, 1, 1, 4>(p, sp, lz);
+        default: return three ? setup_march_s<T, 3, 2, 3>(p, sp, lz) : setup_march_s<T, 1, 2, 3>(p, sp, lz);
+    }
 }
 
 template <typename T, int SAMPLES, int D, int MINB>
@@ -678,38 +791,63 @@ void launch_march_any(tfd_plan *p, cudaStream_t s) {
 // ---- 2D tile kernel set-up ---------------------------------------------------------------------------
 namespace {
 
-int resident_ctas_2d(const void *kernel) {
-    int device = 0, sms = 148, per_sm = 1;
-    if (cudaGetDevice(&device) != cudaSuccess) return 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, k2dThreads, 0);
-    return sms * std::max(1, per_sm);
+template <typename T>
+StripGeom strip_geom(tfd_plan *p) {
+    StripGeom G;
+    const Grid<T> &g = p->grid<T>();
+    G.nx = g.n[0];
+    G.ny = g.n[1];
+    for (size_t k = 0; k < p->seg_f.size(); ++k) G.slabs.push_back({p->seg_f[k], p->seg_a[k], p->seg_lo[k], p->seg_hi[k]});
+    for (int k = 0; k < g.n_src; ++k) G.sources.push_back(g.src[k]);
+    return G;
 }
 
-template <typename T>
-std::vector<Tile2D> tiles_of(const Grid<T> &g, int grid_index) {
-    std::vector<Tile2D> t;
-    for (int y0 = 0; y0 < g.n[1]; y0 += k2dOwnY)
-        for (int x0 = 0; x0 < g.n[0]; x0 += k2dOwnX) t.push_back(Tile2D{grid_index, x0, y0, 0});
-    return t;
+// CTAs of a 2D launch over `strips` strips: one warp per strip, or `ctas` persistent CTAs when set.
+inline int ctas_2d(int strips, int ctas) {
+    const int all = (strips + k2dWarps - 1) / k2dWarps;
+    return std::max(1, ctas > 0 ? std::min(ctas, all) : all);
 }
 
 template <typename T>
 int setup_tile2d(tfd_plan *p, cudaStream_t s) {
     Grid<T> &g = p->grid<T>();
-    std::vector<Tile2D> tiles = tiles_of(g, 0);
+    std::vector<Tile2D> tiles = strips_of(strip_geom<T>(p), 0, p->L.strip_rows);
+    if ((int)tiles.size() != p->L.tiles2d) return fail(TFD_ERR_INVALID, "2D strip table does not match the layout");
+    p->tile2d_interior = interior_count(tiles);
+    if (p->tile2d_interior > 0 && p->tile2d_interior < p->L.tiles2d && !p->side2d) {
+        p->side2d.reset(new SideStream());
+        TFD_CHECK(p->side2d->create());
+    }
     TFD_CUDA(cudaMemcpyAsync(p->arena + p->L.grid_tab, &g, sizeof(Grid<T>), cudaMemcpyHostToDevice, s));
     TFD_CUDA(cudaMemcpyAsync(p->arena + p->L.tile_tab, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice, s));
-    p->tile2d_ctas = std::min((int)tiles.size(), resident_ctas_2d((const void *)k_step2d_tm<T>));
-    if (p->desc.launch_variant > 0) p->tile2d_ctas = std::min((int)tiles.size(), p->desc.launch_variant);
     return TFD_OK;
+}
+
+// One 2D step over a strip table whose first `interior` strips are interior strips. The general strips
+// (latency-bound: CPML memories, edges, sources) start first on the side stream and overlap the
+// bandwidth-bound interior kernel; the caller's stream waits for both (graph capture follows the fork).
+template <typename T>
+void launch_strips(const Grid<T> *grids, const Tile2D *table, int interior, int all, int ctas, const long long *counter,
+                   cudaStream_t s, const SideStream *side) {
+    const bool both = interior > 0 && all > interior && side != nullptr && side->stream != nullptr;
+    if (both) {
+        cudaEventRecord(side->fork, s);
+        cudaStreamWaitEvent(side->stream, side->fork, 0);
+    }
+    if (all > interior)
+        k_step2d_general<T><<<ctas_2d(all - interior, ctas), k2dThreads, 0, both ? side->stream : s>>>(grids, table + interior,
+                                                                                                     all - interior, counter);
+    if (interior > 0) k_step2d_interior<T><<<ctas_2d(interior, ctas), k2dThreads, 0, s>>>(grids, table, interior, counter);
+    if (both) {
+        cudaEventRecord(side->join, side->stream);
+        cudaStreamWaitEvent(s, side->join, 0);
+    }
 }
 
 template <typename T>
 void launch_tile2d(tfd_plan *p, cudaStream_t s) {
-    k_step2d_tm<T><<<std::max(1, p->tile2d_ctas), k2dThreads, 0, s>>>((const Grid<T> *)(p->arena + p->L.grid_tab),
-                                                                     (const Tile2D *)(p->arena + p->L.tile_tab), p->L.tiles2d,
-                                                                     p->grid<T>().counter);
+    launch_strips<T>((const Grid<T> *)(p->arena + p->L.grid_tab), (const Tile2D *)(p->arena + p->L.tile_tab), p->tile2d_interior,
+                     p->L.tiles2d, p->desc.launch_variant, p->grid<T>().counter, s, p->side2d.get());
 }
 
 }  // namespace
@@ -1168,7 +1306,9 @@ struct tfd_batch {
     int precision = 4;
     char *arena = nullptr;
     size_t counter = 0, done = 0, grids = 0, tiles = 0, mon = 0, total = 0;
-    int ntiles = 0, ctas = 0, resident = 0, max_planes = 0, max_chunks = 1;
+    int ntiles = 0, interior = 0, capacity = 0, rows = 8, ctas = 0, max_planes = 0, max_chunks = 1;
+    SideStream side;
+    long long cells = 0;
 };
 
 namespace {
@@ -1178,6 +1318,8 @@ int batch_layout(tfd_batch &b, int n, tfd_plan *const *plans) {
     b.plans.assign(plans, plans + n);
     b.precision = plans[0] ? plans[0]->desc.precision : 4;
     b.ntiles = 0;
+    b.capacity = 0;
+    b.cells = 0;
     for (int i = 0; i < n; ++i) {
         tfd_plan *p = plans[i];
         if (!p) return fail(TFD_ERR_INVALID, "null plan in batch");
@@ -1186,7 +1328,9 @@ int batch_layout(tfd_batch &b, int n, tfd_plan *const *plans) {
         if (p->in_batch) return fail(TFD_ERR_INVALID, "a plan belongs to another batch");
         for (int j = 0; j < i; ++j)
             if (plans[j] == p) return fail(TFD_ERR_INVALID, "a plan appears twice in the batch");
-        b.ntiles += p->L.tiles2d;
+        // The strip table is sized for the shortest strips (8 rows) so any strip length fits later.
+        b.capacity += strip_capacity(p->desc.nx, p->desc.ny);
+        b.cells += (long long)p->desc.nx * p->desc.ny;
     }
     const size_t grid_bytes = b.precision == 8 ? sizeof(Grid<double>) : sizeof(Grid<float>);
     const size_t mon_bytes = b.precision == 8 ? sizeof(MonitorArgs<double>) : sizeof(MonitorArgs<float>);
@@ -1194,9 +1338,28 @@ int batch_layout(tfd_batch &b, int n, tfd_plan *const *plans) {
     b.counter = bump.take(sizeof(long long));
     b.done = bump.take(sizeof(unsigned));
     b.grids = bump.take(n * grid_bytes);
-    b.tiles = bump.take((size_t)b.ntiles * sizeof(Tile2D));
+    b.tiles = bump.take((size_t)b.capacity * sizeof(Tile2D));
     b.mon = bump.take(n * mon_bytes);
     b.total = bump.off + 256;
+    return TFD_OK;
+}
+
+// Rebuild the batch's strip table for strips of `rows` rows (grid by grid, x-fastest).
+template <typename T>
+int batch_strips_t(tfd_batch *b, int rows, cudaStream_t s) {
+    std::vector<Tile2D> tiles;
+    for (size_t i = 0; i < b->plans.size(); ++i) {
+        std::vector<Tile2D> t = strips_of(strip_geom<T>(b->plans[i]), (int)i, rows);
+        tiles.insert(tiles.end(), t.begin(), t.end());
+    }
+    if ((int)tiles.size() > b->capacity) return fail(TFD_ERR_INVALID, "strip table exceeds the batch arena");
+    // Interior strips of every member first: the lean kernel walks [0, interior) of the whole table.
+    std::stable_partition(tiles.begin(), tiles.end(), [](const Tile2D &a) { return a.kind == 1; });
+    TFD_CUDA(cudaMemcpyAsync(b->arena + b->tiles, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice, s));
+    TFD_CUDA(cudaStreamSynchronize(s));
+    b->ntiles = (int)tiles.size();
+    b->interior = interior_count(tiles);
+    b->rows = rows;
     return TFD_OK;
 }
 
@@ -1205,7 +1368,6 @@ int batch_create_t(tfd_batch *b, cudaStream_t s) {
     const int n = (int)b->plans.size();
     long long *counter = (long long *)(b->arena + b->counter);
     std::vector<Grid<T>> grids;
-    std::vector<Tile2D> tiles;
     std::vector<MonitorArgs<T>> mons;
     for (int i = 0; i < n; ++i) {
         tfd_plan *p = b->plans[i];
@@ -1221,8 +1383,6 @@ int batch_create_t(tfd_batch *b, cudaStream_t s) {
         g.counter = counter;                         // members read the batch's shared step counter
         p->in_batch = true;
         grids.push_back(g);
-        std::vector<Tile2D> t = tiles_of(g, i);
-        tiles.insert(tiles.end(), t.begin(), t.end());
         MonitorArgs<T> m = monitor_args<T>(p);
         mons.push_back(m);
         b->max_planes = std::max(b->max_planes, p->desc.n_planes);
@@ -1231,14 +1391,13 @@ int batch_create_t(tfd_batch *b, cudaStream_t s) {
     TFD_CUDA(cudaMemsetAsync(b->arena + b->counter, 0, sizeof(long long), s));
     TFD_CUDA(cudaMemsetAsync(b->arena + b->done, 0, sizeof(unsigned), s));
     TFD_CUDA(cudaMemcpyAsync(b->arena + b->grids, grids.data(), grids.size() * sizeof(Grid<T>), cudaMemcpyHostToDevice, s));
-    TFD_CUDA(cudaMemcpyAsync(b->arena + b->tiles, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice, s));
     TFD_CUDA(cudaMemcpyAsync(b->arena + b->mon, mons.data(), mons.size() * sizeof(MonitorArgs<T>), cudaMemcpyHostToDevice, s));
     TFD_CUDA(cudaStreamSynchronize(s));
     cudaFuncAttributes attr;                     // loads the monitor kernel now, before any graph capture
     TFD_CUDA(cudaFuncGetAttributes(&attr, (const void *)k_monitor_batch<T>));
-    b->resident = resident_ctas_2d((const void *)k_step2d_tm<T>);
-    b->ctas = std::min(b->ntiles, b->resident);
-    return TFD_OK;
+    b->ctas = 0;
+    TFD_CHECK(b->side.create());
+    return batch_strips_t<T>(b, strip_rows(b->cells), s);
 }
 
 template <typename T>
@@ -1246,8 +1405,8 @@ int batch_step_t(tfd_batch *b, int nsteps, cudaStream_t s) {
     long long *counter = (long long *)(b->arena + b->counter);
     const dim3 mgrid((unsigned)b->max_chunks, (unsigned)std::max(1, b->max_planes), (unsigned)b->plans.size());
     for (int k = 0; k < nsteps; ++k) {
-        k_step2d_tm<T><<<std::max(1, b->ctas), k2dThreads, 0, s>>>((const Grid<T> *)(b->arena + b->grids),
-                                                                   (const Tile2D *)(b->arena + b->tiles), b->ntiles, counter);
+        launch_strips<T>((const Grid<T> *)(b->arena + b->grids), (const Tile2D *)(b->arena + b->tiles), b->interior, b->ntiles,
+                         b->ctas, counter, s, &b->side);
         k_monitor_batch<T><<<mgrid, kMonitorThreads, 0, s>>>((const MonitorArgs<T> *)(b->arena + b->mon), counter,
                                                              (unsigned *)(b->arena + b->done));
     }
@@ -1308,9 +1467,16 @@ int tfd_batch_create(int32_t n_plans, tfd_plan *const *plans, void *arena, size_
     return TFD_OK;
 }
 
-int tfd_batch_set_ctas(tfd_batch *b, int32_t ctas) {
-    if (!b || ctas < 0) return fail(TFD_ERR_INVALID, "bad batch CTA count");
-    b->ctas = ctas == 0 ? std::min(b->ntiles, b->resident) : std::min(b->ntiles, (int)ctas);
+int tfd_batch_set_launch(tfd_batch *b, int32_t ctas, int32_t strip_rows, void *stream) {
+    if (!b || ctas < 0 || strip_rows < 0 || (strip_rows > 0 && strip_rows < 8))
+        return fail(TFD_ERR_INVALID, "bad batch launch: ctas >= 0, strip_rows 0 or >= 8");
+    const int rows = strip_rows == 0 ? tfd::strip_rows(b->cells) : strip_rows;
+    if (rows != b->rows) {
+        const int rc = b->precision == 8 ? batch_strips_t<double>(b, rows, as_stream(stream))
+                                         : batch_strips_t<float>(b, rows, as_stream(stream));
+        if (rc) return rc;
+    }
+    b->ctas = ctas;
     return TFD_OK;
 }
 

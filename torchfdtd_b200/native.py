@@ -82,7 +82,7 @@ SIGNATURES = {
     'tfd_field_norm_static': (ctypes.c_int, [c_vp, c_vp, c_vp, c_i64, c_i32, c_i32, c_vp, c_vp]),
     'tfd_batch_bytes': (ctypes.c_int, [c_i32, ctypes.POINTER(c_vp), ctypes.POINTER(ctypes.c_size_t)]),
     'tfd_batch_create': (ctypes.c_int, [c_i32, ctypes.POINTER(c_vp), c_vp, ctypes.c_size_t, c_vp, ctypes.POINTER(c_vp)]),
-    'tfd_batch_set_ctas': (ctypes.c_int, [c_vp, c_i32]),
+    'tfd_batch_set_launch': (ctypes.c_int, [c_vp, c_i32, c_i32, c_vp]),
     'tfd_batch_step': (ctypes.c_int, [c_vp, c_i32, c_vp]),
     'tfd_batch_tiles': (ctypes.c_int, [c_vp, P_i32]),
     'tfd_batch_destroy': (None, [c_vp]),
@@ -356,8 +356,9 @@ class NativeBatch:
         for g in self.grids:
             g.batch = self
 
-    def set_ctas(self, ctas):
-        check(library().tfd_batch_set_ctas(self.handle, int(ctas)))
+    def set_launch(self, ctas=0, rows=0, stream=None):
+        """Persistent CTA count (0: one warp per strip) and rows per strip (0: default) of the step kernel."""
+        check(library().tfd_batch_set_launch(self.handle, int(ctas), int(rows), _stream(stream)))
 
     def tiles(self):
         v = c_i32()

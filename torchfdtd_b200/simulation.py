@@ -317,11 +317,14 @@ class Simulation:
             plan.inv_eps = (1 / eps).astype(plan.dtype)
         return plan
 
-    def run(self, progress=None, cancel=None, cuda_graph=True, cuda_graph_steps=1, kernel='auto'):
+    def run(self, progress=None, cancel=None, cuda_graph=True, cuda_graph_steps=1, kernel='auto', launch=None):
+        """``kernel``: 'auto' (the marching kernel for 3D, the tile kernel for 2D TMz, else gather) or a name.
+        ``launch``: None (default launch shape), an explicit launch variant, or 'auto' to measure the
+        marching kernel's variants on scratch plans first (``tuning.select_launch``; cached per process)."""
         with ENGINE_LOCK:
-            return self._run(progress, cancel, cuda_graph, cuda_graph_steps, kernel)
+            return self._run(progress, cancel, cuda_graph, cuda_graph_steps, kernel, launch)
 
-    def _run(self, progress, cancel, cuda_graph, cuda_graph_steps, kernel):
+    def _run(self, progress, cancel, cuda_graph, cuda_graph_steps, kernel, launch=None):
         import torch
         from .native import NativeGrid
         p, r = self.project, self.project.region
@@ -331,7 +334,18 @@ class Simulation:
             raise RuntimeError('CUDA requested but unavailable. The fused B200 engine needs a CUDA GPU.')
         started = time.perf_counter()
         plan = self.plan
-        grid = NativeGrid(plan, kernel=kernel)
+        variant, tuning = 0, None
+        if launch == 'auto':
+            if plan.dimension == '3d' and kernel in ('auto', 'march'):
+                from .tuning import select_launch
+                try:
+                    tuning = select_launch(plan)
+                    variant = tuning.choice
+                except ValueError as exc:          # too few steps to tune, or no marching kernel for this scene
+                    tuning = dict(skipped=str(exc))
+        elif launch is not None:
+            variant = int(launch)
+        grid = NativeGrid(plan, kernel=kernel, variant=variant)
         free, _ = torch.cuda.mem_get_info()
         observer = Observer(p, plan, grid)
         graphs = {}
@@ -367,6 +381,8 @@ class Simulation:
         torch.cuda.synchronize()
         seconds = time.perf_counter() - compute_start
         result = observer.result(completed, termination_reason, seconds, setup_seconds, cuda_graph=bool(graphs),
-                                 cuda_graph_steps=width, cuda_graph_replays=replays, free_device_bytes=free)
+                                 cuda_graph_steps=width, cuda_graph_replays=replays, free_device_bytes=free,
+                                 launch_variant=variant or None,
+                                 launch_tuning=tuning.as_dict() if hasattr(tuning, 'as_dict') else tuning)
         grid.close()
         return result
