@@ -207,6 +207,34 @@ int tfd_batch_step(tfd_batch *batch, int32_t nsteps, void *stream);
 int tfd_batch_tiles(const tfd_batch *batch, int32_t *tiles);
 void tfd_batch_destroy(tfd_batch *batch);
 
+/* ---- restart states: the checkpoints of the discrete adjoint ----
+ * Replace _Checkpoints.save / restore (torchfdtd/differentiable.py:539-624), which clone E, H and every
+ * CPML memory as torch tensors. A snapshot is one device buffer (256-byte aligned, tfd_state_bytes long)
+ * holding the step counter, E, H and E-family memories of the current parity and the H-family memories.
+ * Save and load are stream-ordered kernels (the parity is read on the device), so they can be captured. */
+int tfd_state_bytes(tfd_plan *plan, size_t *bytes);
+int tfd_state_save(tfd_plan *plan, void *snapshot, void *stream);
+int tfd_state_load(tfd_plan *plan, const void *snapshot, void *stream);
+
+/* ---- discrete adjoint ----
+ * Replaces _System.transpose_step / FusedAdjointCUDA (torchfdtd/differentiable.py:489-519,
+ * torchfdtd/cuda_adjoint.py:16-234): the transpose of one Yee/CPML step, with the CPML memory transpose,
+ * accumulating the material sensitivity S_c = sum over steps of e_bar_c * curl_b(H)_c (the gradient with
+ * respect to the permittivity is -courant * S / eps^2). The observers are the plan's traces: they must be
+ * distinct cells. tfd_adjoint_step transposes the step that took s_n to s_{n+1}: it first adds `seeds`
+ * (one value per trace, the derivative of the objective with respect to the traces recorded after step n;
+ * device pointer in the plan's precision, or null) and then reads the forward state s_n from `snapshot`
+ * (a tfd_state_save buffer). Call it for n = steps-1 down to 0. */
+typedef struct tfd_adjoint tfd_adjoint;
+int tfd_adjoint_bytes(tfd_plan *plan, size_t *bytes);
+int tfd_adjoint_create(tfd_plan *plan, void *arena, size_t arena_bytes, void *stream, tfd_adjoint **adjoint);
+int tfd_adjoint_reset(tfd_adjoint *adjoint, void *stream);
+int tfd_adjoint_step(tfd_adjoint *adjoint, const void *snapshot, const void *seeds, void *stream);
+/* S in the reference layout (nx, ny, nz, 3), one value per E component (zero for components 2D does not
+ * advance); TFD_HOST or TFD_DEVICE destination. */
+int tfd_adjoint_sensitivity(tfd_adjoint *adjoint, void *dst, int where, void *stream);
+void tfd_adjoint_destroy(tfd_adjoint *adjoint);
+
 const char *tfd_error_string(int code);
 const char *tfd_last_error(void);
 

@@ -16,7 +16,9 @@ allocators are used by the reference), and records:
   FP32 and FP64);
 - ``sim_*.npz``: complete ``Simulation(project).run()`` results on the CPU
   (fields, point traces, DFT planes with flux) plus the voxelized permittivity,
-  for small scenes shaped like the benchmark configurations.
+  for small scenes shaped like the benchmark configurations;
+- ``adjoint_*.npz``: the reference ``DifferentiableSimulation`` (discrete adjoint, CPU) on small 2D/3D
+  scenes: seeded random epsilon, the point-monitor signals and the gradient of sum(weights * signals).
 
 The engine and the GPU tests never read the reference; they read these files.
 """
@@ -186,9 +188,48 @@ def write_scenes(ref):
                             summary=json.dumps({k: result.summary[k] for k in ('steps', 'precision', 'slice_index')}))
 
 
+def adjoint_scenes(ref):
+    """Small scenes for the discrete adjoint: kappa > 1 CPML, a PEC face, E and H point monitors."""
+    from torchfdtd.models import BoundaryFace, Monitor, Project, Region, Source
+    out = {}
+    for dim in ('2d', '3d'):
+        for precision in ('float32', 'float64'):
+            r = Region(dimension=dim, size=(1.6, 1.4, 1.2 if dim == '3d' else 1), mesh=.1, pml_cells=3, steps=30,
+                       precision=precision, backend='cpu')
+            r.boundaries.x_min = BoundaryFace(layers=4, kappa=2, alpha=.04, alpha_polynomial=1)
+            r.boundaries.y_max = BoundaryFace(kind='pec')
+            out[f'{dim}_{precision}'] = Project(
+                name=f'adjoint {dim}', region=r,
+                sources=[Source(id='src', center=(-.1, .05, 0), component='Ez', pulse_cycles=1, wavelength=.6)],
+                monitors=[Monitor(id='ez', center=(.2, .1, 0), component='Ez'),
+                          Monitor(id='hy', center=(.1, -.1, 0), component='Hy')])
+    return out
+
+
+def write_adjoint(ref):
+    """Reference DifferentiableSimulation on the CPU: signals and d/d eps of sum(w * signals)."""
+    import torch
+    from torchfdtd.differentiable import AdjointOptions, DifferentiableSimulation
+    for name, project in adjoint_scenes(ref).items():
+        dtype = torch.float32 if project.region.precision == 'float32' else torch.float64
+        rng = np.random.default_rng(17)
+        shape = tuple(project.region.shape)
+        eps = rng.uniform(1, 3, size=shape)
+        weights = rng.normal(size=(project.region.steps, 2))
+        model = DifferentiableSimulation(project, AdjointOptions(checkpoints=4))
+        epsilon = torch.tensor(eps, dtype=dtype, requires_grad=True)
+        result = model(epsilon)
+        objective = (result.signals * torch.tensor(weights, dtype=dtype)).sum()
+        objective.backward()
+        np.savez_compressed(HERE / f'adjoint_{name}.npz', project=project.model_dump_json(), epsilon=eps.astype(np.float64),
+                            weights=weights, signals=result.signals.detach().numpy(), gradient=epsilon.grad.numpy(),
+                            objective=float(objective.detach()))
+
+
 if __name__ == '__main__':
     ref = load_reference()
     write_states(ref)
     write_scenes(ref)
+    write_adjoint(ref)
     for path in sorted(HERE.glob('*.npz')):
         print(f'{path.name}: {path.stat().st_size/1024:.0f} KiB')

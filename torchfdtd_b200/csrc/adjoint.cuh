@@ -1,0 +1,248 @@
+// Discrete adjoint of one Yee/CPML step, gather form: one thread per cell.
+//
+// The forward step n maps the state s_n = (E, H, psi) to s_{n+1}:
+//     E' = E + (cn / eps) curl_b(H; psi_E)      then E sources
+//     H' = H - cn curl_f(E'; psi_H)             then H sources
+// and observations sample s_{n+1}. Its transpose (reference torchfdtd/differentiable.py:489-519,
+// _System.transpose_step, with the CPML memory transpose of curl_faces_transpose :369-432) maps the
+// adjoint lambda_{n+1} = (e_bar, h_bar, psi_bar) to lambda_n:
+//     e_bar += curl_f^T(-cn h_bar)              (psi_H bars: m = psi_bar + v, psi_bar <- b m, v <- v/kappa + c m)
+//     dJ/d eps += -cn e_bar curl_b(H_n; psi_E,n) / eps^2
+//     h_bar += curl_b^T((cn / eps) e_bar)       (psi_E bars likewise)
+// Sources are additive constants and drop out; observation seeds are added to e_bar / h_bar before
+// the transpose of the step whose result they sampled.
+//
+// curl_f^T is a backward difference of the per-H-cell values D(k) (k = 0..n-2, plus the periodic wrap or
+// PEC edge at n-1) and curl_b^T a forward difference of per-E-cell values D(k) (k = 1..n-1, plus the
+// periodic edge at 0), so the adjoint step has the forward step's stencil shape: a thread computes
+// e_bar_new at its own cell, recomputes e_bar_new at its +x, +y, +z neighbours (from the old buffers, as
+// the forward gather kernel recomputes E), and then h_bar_new at its own cell. Adjoint fields and both
+// families' adjoint CPML memories are double-buffered by reverse-step parity; each memory is written
+// once, by the thread that owns its cell. The forward state comes from a restart snapshot (tfd_state_save)
+// of s_n, so no forward buffer is disturbed.
+//
+// The material sensitivity is accumulated as S_c = sum_n e_bar_c * curl_b(H)_c per component; the host
+// forms dJ/d eps = -cn S / eps^2 (summed over components for a per-cell permittivity).
+#pragma once
+#include "internal.cuh"
+
+namespace tfd {
+
+// Terms of the curl whose INPUT is component C, in reference CURL_TERMS order (ascending axis):
+// {axis, out, sign, j}.
+struct RevTerm { int axis, out, sign, j; };
+__host__ __device__ constexpr RevTerm rev_of(int in, int k) {
+    return in == 0 ? (k == 0 ? RevTerm{1, 2, -1, 1} : RevTerm{2, 1, +1, 1})
+         : in == 1 ? (k == 0 ? RevTerm{0, 2, +1, 1} : RevTerm{2, 0, -1, 0})
+                   : (k == 0 ? RevTerm{0, 1, -1, 0} : RevTerm{1, 0, +1, 0});
+}
+
+template <typename T>
+struct AdjArgs {
+    Grid<T> g;                   // geometry, CPML tables, 1/eps; its field pointers are not used
+    long long sE[3], sH[3];      // element offsets of the snapshot's arrays (-1: absent)
+    long long sPsiE[3][2];
+    T *eb[2][3], *hb[2][3];      // adjoint fields [parity][component]
+    T *pEb[2][3][2], *pHb[2][3][2];   // adjoint CPML memories [parity][axis][term j]
+    T *S[3];                     // material sensitivity per E component
+};
+
+template <typename T>
+__device__ __forceinline__ int coord_of(int a, int x, int y, int z) { return a == 0 ? x : (a == 1 ? y : z); }
+
+// D of an H-family term (output H component `out`, axis a) at H cell k: the transposed forward-difference
+// value sign * (-cn h_bar_out[k]) through the CPML memory transpose. Writes the memory when own.
+template <typename T>
+__device__ __forceinline__ T d_h(const AdjArgs<T> &A, int q, const RevTerm t, int x, int y, int z, long long k, bool own) {
+    const Grid<T> &g = A.g;
+    const int a = t.axis;
+    const int c = coord_of<T>(a, x, y, z);
+    const T dst = -g.cn * A.hb[q][t.out][k];
+    T v = t.sign > 0 ? dst : -dst;
+    if (c < g.n[a] - 1) {
+        const int *rm = g.row[1][a];
+        if (rm != nullptr && A.pHb[q][a][t.j] != nullptr) {
+            const int r = rm[c];
+            if (r >= 0) {
+                const long long p = g.psi_index(a, x, y, z, r, g.rows[1][a]);
+                const T m = A.pHb[q][a][t.j][p] + v;
+                if (own) A.pHb[q ^ 1][a][t.j][p] = g.cb[1][a][c] * m;
+                v = v * g.ck[1][a][c] + g.cc[1][a][c] * m;
+            }
+        }
+        return v;
+    }
+    if (g.periodic[a]) return v;
+    if (g.pec_on[a]) return -g.pec_neg[a] * v;       // sign * pec * dst
+    return T(0);
+}
+
+// e_bar_new of component C at cell (x, y, z), index i.
+template <typename T, int C>
+__device__ __forceinline__ T ebar_value(const AdjArgs<T> &A, int q, int x, int y, int z, long long i, bool own) {
+    const Grid<T> &g = A.g;
+    T contrib = T(0);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const RevTerm t = rev_of(C, k);
+        const int a = t.axis;
+        if (g.n[a] == 1) continue;
+        const int out_bit = 1 << (3 + t.out);
+        if (!(g.active & out_bit)) continue;
+        const int c = coord_of<T>(a, x, y, z);
+        const int n = g.n[a];
+        const long long s = g.stride(a);
+        if (c >= 1) {                                   // src[c] += D(c-1)
+            const int xm = a == 0 ? x - 1 : x, ym = a == 1 ? y - 1 : y, zm = a == 2 ? z - 1 : z;
+            contrib = contrib + d_h(A, q, t, xm, ym, zm, i - s, false);
+        }
+        if (c <= n - 2) contrib = contrib - d_h(A, q, t, x, y, z, i, own);   // src[c] -= D(c)
+        if (g.periodic[a]) {                            // wrap edge D(n-1): src[0] += D, src[n-1] -= D
+            if (c == 0) {
+                const int xw = a == 0 ? n - 1 : x, yw = a == 1 ? n - 1 : y, zw = a == 2 ? n - 1 : z;
+                contrib = contrib + d_h(A, q, t, xw, yw, zw, i + (long long)(n - 1) * s, false);
+            }
+            if (c == n - 1) contrib = contrib - d_h(A, q, t, x, y, z, i, false);
+        } else if (g.pec_on[a] && c == n - 1) {
+            contrib = contrib - d_h(A, q, t, x, y, z, i, false);
+        }
+    }
+    return A.eb[q][C][i] + contrib;
+}
+
+// D of an E-family term (output E component `out`, axis a) at E cell k: sign * (cn / eps) e_bar_new_out[k]
+// through the CPML memory transpose. Writes the memory when own.
+template <typename T>
+__device__ __forceinline__ T d_e(const AdjArgs<T> &A, int q, const RevTerm t, int x, int y, int z, long long k, T ebar_out,
+                                 bool own) {
+    const Grid<T> &g = A.g;
+    const int a = t.axis;
+    const int c = coord_of<T>(a, x, y, z);
+    const T dst = (g.cn * g.inv_eps[t.out][k]) * ebar_out;
+    T v = t.sign > 0 ? dst : -dst;
+    if (c >= 1) {
+        const int *rm = g.row[0][a];
+        if (rm != nullptr && A.pEb[q][a][t.j] != nullptr) {
+            const int r = rm[c];
+            if (r >= 0) {
+                const long long p = g.psi_index(a, x, y, z, r, g.rows[0][a]);
+                const T m = A.pEb[q][a][t.j][p] + v;
+                if (own) A.pEb[q ^ 1][a][t.j][p] = g.cb[0][a][c] * m;
+                v = v * g.ck[0][a][c] + g.cc[0][a][c] * m;
+            }
+        }
+        return v;
+    }
+    return g.periodic[a] ? v : T(0);
+}
+
+template <typename T, int C>
+__device__ __forceinline__ T ebar_at(const AdjArgs<T> &A, int q, int x, int y, int z, long long i) {
+    return ebar_value<T, C>(A, q, x, y, z, i, false);
+}
+
+// e_bar_new of component `out` at a neighbour (runtime component).
+template <typename T>
+__device__ __forceinline__ T ebar_any(const AdjArgs<T> &A, int q, int out, int x, int y, int z, long long i) {
+    return out == 0 ? ebar_at<T, 0>(A, q, x, y, z, i) : out == 1 ? ebar_at<T, 1>(A, q, x, y, z, i) : ebar_at<T, 2>(A, q, x, y, z, i);
+}
+
+// h_bar_new of H component C at its own cell; e_own[] holds e_bar_new of the own cell.
+template <typename T, int C>
+__device__ __forceinline__ T hbar_value(const AdjArgs<T> &A, int q, int x, int y, int z, long long i, const T *e_own) {
+    const Grid<T> &g = A.g;
+    T contrib = T(0);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const RevTerm t = rev_of(C, k);
+        const int a = t.axis;
+        if (g.n[a] == 1) continue;
+        if (!(g.active & (1 << t.out))) continue;
+        const int c = coord_of<T>(a, x, y, z);
+        const int n = g.n[a];
+        const long long s = g.stride(a);
+        if (c >= 1) contrib = contrib + d_e(A, q, t, x, y, z, i, e_own[t.out], true);          // src[c] += D(c)
+        if (c + 1 <= n - 1) {                                                                   // src[c] -= D(c+1)
+            const int xp = a == 0 ? x + 1 : x, yp = a == 1 ? y + 1 : y, zp = a == 2 ? z + 1 : z;
+            const T eb = ebar_any(A, q, t.out, xp, yp, zp, i + s);
+            contrib = contrib - d_e(A, q, t, xp, yp, zp, i + s, eb, false);
+        }
+        if (g.periodic[a]) {                             // edge D(0): src[0] += D, src[n-1] -= D
+            if (c == 0) contrib = contrib + d_e(A, q, t, x, y, z, i, e_own[t.out], false);
+            if (c == n - 1) {
+                const int x0 = a == 0 ? 0 : x, y0 = a == 1 ? 0 : y, z0 = a == 2 ? 0 : z;
+                const long long i0 = i - (long long)(n - 1) * s;
+                const T eb = ebar_any(A, q, t.out, x0, y0, z0, i0);
+                contrib = contrib - d_e(A, q, t, x0, y0, z0, i0, eb, false);
+            }
+        }
+    }
+    return A.hb[q][C][i] + contrib;
+}
+
+// Forward E curl of component C from the snapshot (same arithmetic as the forward E update).
+template <typename T, int C>
+__device__ __forceinline__ T forward_curl(const AdjArgs<T> &A, const T *slot, int x, int y, int z, long long i) {
+    const Grid<T> &g = A.g;
+    T acc = T(0);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const Term t = term_of(C, k);
+        const int a = t.axis;
+        if (g.n[a] == 1) continue;
+        const int c = coord_of<T>(a, x, y, z);
+        const T *h = slot + A.sH[t.in];
+        T d = T(0);
+        if (c > 0) {
+            d = h[i] - h[i - g.stride(a)];
+            const int *rm = g.row[0][a];
+            if (rm != nullptr && A.sPsiE[a][t.j] >= 0) {
+                const int r = rm[c];
+                if (r >= 0) {
+                    const long long p = g.psi_index(a, x, y, z, r, g.rows[0][a]);
+                    const T mem = slot[A.sPsiE[a][t.j] + p] * g.cb[0][a][c] + g.cc[0][a][c] * d;
+                    d = d * g.ck[0][a][c] + mem;
+                }
+            }
+        } else if (g.periodic[a]) {
+            d = h[i] - h[i + (long long)(g.n[a] - 1) * g.stride(a)];
+        }
+        acc = acc + (t.sign > 0 ? d : -d);
+    }
+    return acc;
+}
+
+// ACTIVE: bitmask of advanced components (bit c: E_c, bit 3+c: H_c). Launch like the forward gather
+// kernel: blockIdx.x = row (z*ny + y), blockIdx.y = 128-cell chunk of the row. Reads parity q, writes q^1.
+template <typename T, int ACTIVE>
+__global__ void __launch_bounds__(128) k_adjoint_step(const __grid_constant__ AdjArgs<T> A, const T *__restrict__ slot, int q) {
+    const Grid<T> &g = A.g;
+    const int x = blockIdx.y * blockDim.x + threadIdx.x;
+    const int y = blockIdx.x % g.n[1];
+    const int z = blockIdx.x / g.n[1];
+    if (x >= g.n[0]) return;
+    const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
+    T e[3] = {T(0), T(0), T(0)};
+    if (ACTIVE & 1) e[0] = ebar_value<T, 0>(A, q, x, y, z, i, true);
+    if (ACTIVE & 2) e[1] = ebar_value<T, 1>(A, q, x, y, z, i, true);
+    if (ACTIVE & 4) e[2] = ebar_value<T, 2>(A, q, x, y, z, i, true);
+    if (ACTIVE & 1) { A.eb[q ^ 1][0][i] = e[0]; A.S[0][i] = A.S[0][i] + e[0] * forward_curl<T, 0>(A, slot, x, y, z, i); }
+    if (ACTIVE & 2) { A.eb[q ^ 1][1][i] = e[1]; A.S[1][i] = A.S[1][i] + e[1] * forward_curl<T, 1>(A, slot, x, y, z, i); }
+    if (ACTIVE & 4) { A.eb[q ^ 1][2][i] = e[2]; A.S[2][i] = A.S[2][i] + e[2] * forward_curl<T, 2>(A, slot, x, y, z, i); }
+    if (ACTIVE & 8) A.hb[q ^ 1][0][i] = hbar_value<T, 0>(A, q, x, y, z, i, e);
+    if (ACTIVE & 16) A.hb[q ^ 1][1][i] = hbar_value<T, 1>(A, q, x, y, z, i, e);
+    if (ACTIVE & 32) A.hb[q ^ 1][2][i] = hbar_value<T, 2>(A, q, x, y, z, i, e);
+}
+
+// Observation seeds of one step: bar[family][comp][offset] += seed[k] (observers are distinct cells).
+template <typename T>
+__global__ void k_adjoint_seed(const __grid_constant__ AdjArgs<T> A, const TraceDev *__restrict__ obs, int n_obs,
+                               const T *__restrict__ seed, int q) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_obs; k += gridDim.x * blockDim.x) {
+        const TraceDev o = obs[k];
+        T *bar = o.family == 0 ? A.eb[q][o.comp] : A.hb[q][o.comp];
+        if (bar != nullptr) bar[o.offset] = bar[o.offset] + seed[k];
+    }
+}
+
+}  // namespace tfd

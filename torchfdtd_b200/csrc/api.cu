@@ -12,6 +12,7 @@
 #include "step_gather.cuh"
 #include "step_march.cuh"
 #include "step2d.cuh"
+#include "adjoint.cuh"
 #include <cudaTypedefs.h>
 
 using namespace tfd;
@@ -554,6 +555,7 @@ int create_typed(tfd_plan *p, const tfd_desc *d, cudaStream_t s) {
         pd.acc = p->ptr<double>(q.acc);
         p->max_samples = std::max(p->max_samples, src.points * src.components);
     }
+    p->max_samples = std::max(p->max_samples, d->n_traces);     // the trace loop strides over the same blocks
     if ((rc = upload(s, p, L.plane_tab, planes))) return rc;
     // zero the state; the material starts as vacuum (inverse permittivity 1)
     return TFD_OK;
@@ -1497,5 +1499,265 @@ void tfd_batch_destroy(tfd_batch *b) {
     if (b->precision == 8) batch_release_t<double>(b); else batch_release_t<float>(b);
     delete b;
 }
+
+}  // extern "C"
+
+// ---- restart states and the discrete adjoint ---------------------------------------------------------
+namespace {
+
+constexpr int kStateArrays = 18;
+
+// The restart state of a plan as a compact snapshot: the step counter (first 8 bytes), then E, H and the
+// E-family CPML memories of the current parity and the H-family memories, each 256-byte aligned.
+template <typename T>
+struct StateCopy {
+    int n;
+    T *a[kStateArrays][2];       // [array][parity]; H-family memories have one buffer (both entries)
+    long long len[kStateArrays];
+    long long off[kStateArrays]; // element offset in the snapshot
+};
+
+struct StateMap {
+    long long sE[3], sH[3], sPsiE[3][2], sPsiH[3][2];
+    size_t bytes;
+};
+
+template <typename T>
+StateMap state_layout(tfd_plan *p, StateCopy<T> *sc) {
+    const Grid<T> &g = p->grid<T>();
+    StateMap m;
+    size_t off = 256;
+    auto take = [&](long long elems) {
+        const long long at = (long long)(off / sizeof(T));
+        off += ((size_t)elems * sizeof(T) + 255) / 256 * 256;
+        return at;
+    };
+    if (sc) sc->n = 0;
+    auto add = [&](T *p0, T *p1, long long len) {
+        const long long at = take(len);
+        if (sc) {
+            sc->a[sc->n][0] = p0;
+            sc->a[sc->n][1] = p1;
+            sc->len[sc->n] = len;
+            sc->off[sc->n] = at;
+            ++sc->n;
+        }
+        return at;
+    };
+    for (int c = 0; c < 3; ++c) m.sE[c] = g.E[0][c] ? add(g.E[0][c], g.E[1][c], g.count) : -1;
+    for (int c = 0; c < 3; ++c) m.sH[c] = g.H[0][c] ? add(g.H[0][c], g.H[1][c], g.count) : -1;
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 2; ++j)
+            m.sPsiE[a][j] = g.psiE[0][a][j] ? add(g.psiE[0][a][j], g.psiE[1][a][j], p->L.psi_len[0][a]) : -1;
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 2; ++j) m.sPsiH[a][j] = g.psiH[a][j] ? add(g.psiH[a][j], g.psiH[a][j], p->L.psi_len[1][a]) : -1;
+    m.bytes = off;
+    return m;
+}
+
+// Copies the state between the plan and a snapshot; the parity comes from the plan's counter (save) or
+// from the snapshot's counter (load), read on the device, so the copy is stream-ordered and capturable.
+template <typename T>
+__global__ void k_state_copy(const __grid_constant__ StateCopy<T> sc, char *slot, long long *counter, int save) {
+    const int k = blockIdx.y;
+    const long long n = save ? *counter : *(const long long *)slot;
+    const int par = (int)(n & 1);
+    T *arr = sc.a[k][par];
+    T *snap = (T *)slot + sc.off[k];
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < sc.len[k]; e += (long long)gridDim.x * blockDim.x) {
+        if (save) snap[e] = arr[e];
+        else arr[e] = snap[e];
+    }
+    if (k == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
+        if (save) *(long long *)slot = n;
+        else *counter = n;
+    }
+}
+
+template <typename T>
+int state_copy_t(tfd_plan *p, char *slot, bool save, cudaStream_t s) {
+    StateCopy<T> sc;
+    std::memset(&sc, 0, sizeof(sc));
+    state_layout<T>(p, &sc);
+    long long longest = 1;
+    for (int k = 0; k < sc.n; ++k) longest = std::max(longest, sc.len[k]);
+    const dim3 grid((unsigned)std::min<long long>((longest + 255) / 256, 1184), (unsigned)std::max(1, sc.n));
+    k_state_copy<T><<<grid, 256, 0, s>>>(sc, slot, p->grid<T>().counter, save ? 1 : 0);
+    TFD_CUDA(cudaGetLastError());
+    return TFD_OK;
+}
+
+}  // namespace
+
+struct tfd_adjoint {
+    tfd_plan *p = nullptr;
+    char *arena = nullptr;
+    size_t used = 0;
+    int q = 0;
+    AdjArgs<float> af;
+    AdjArgs<double> ad;
+    template <typename T> AdjArgs<T> &args();
+};
+template <> AdjArgs<float> &tfd_adjoint::args<float>() { return af; }
+template <> AdjArgs<double> &tfd_adjoint::args<double>() { return ad; }
+
+namespace {
+
+// Adjoint arena: e_bar, h_bar and both families' CPML memory bars by parity, and the sensitivity.
+template <typename T>
+size_t adjoint_layout(tfd_plan *p, AdjArgs<T> *A, char *arena) {
+    const Grid<T> &g = p->grid<T>();
+    Bump b;
+    auto at = [&](size_t off) { return arena ? (T *)(arena + off) : nullptr; };
+    const size_t field = (size_t)g.count * sizeof(T);
+    for (int q = 0; q < 2; ++q)
+        for (int c = 0; c < 3; ++c) {
+            T *e = g.E[0][c] ? at(b.take(field)) : nullptr;
+            T *h = g.H[0][c] ? at(b.take(field)) : nullptr;
+            if (A) { A->eb[q][c] = e; A->hb[q][c] = h; }
+        }
+    for (int q = 0; q < 2; ++q)
+        for (int a = 0; a < 3; ++a)
+            for (int j = 0; j < 2; ++j) {
+                T *pe = g.psiE[0][a][j] ? at(b.take((size_t)p->L.psi_len[0][a] * sizeof(T))) : nullptr;
+                T *ph = g.psiH[a][j] ? at(b.take((size_t)p->L.psi_len[1][a] * sizeof(T))) : nullptr;
+                if (A) { A->pEb[q][a][j] = pe; A->pHb[q][a][j] = ph; }
+            }
+    for (int c = 0; c < 3; ++c) {
+        T *sv = g.E[0][c] ? at(b.take(field)) : nullptr;
+        if (A) A->S[c] = sv;
+    }
+    return b.off;
+}
+
+template <typename T>
+int adjoint_create_t(tfd_adjoint *adj, cudaStream_t s) {
+    tfd_plan *p = adj->p;
+    AdjArgs<T> &A = adj->args<T>();
+    std::memset(&A, 0, sizeof(A));
+    A.g = p->grid<T>();
+    const StateMap m = state_layout<T>(p, nullptr);
+    for (int c = 0; c < 3; ++c) { A.sE[c] = m.sE[c]; A.sH[c] = m.sH[c]; }
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 2; ++j) A.sPsiE[a][j] = m.sPsiE[a][j];
+    adj->used = adjoint_layout<T>(p, &A, adj->arena);
+    TFD_CUDA(cudaMemsetAsync(adj->arena, 0, adj->used, s));
+    adj->q = 0;
+    return TFD_OK;
+}
+
+template <typename T>
+int adjoint_step_t(tfd_adjoint *adj, const void *snapshot, const void *seeds, cudaStream_t s) {
+    tfd_plan *p = adj->p;
+    const AdjArgs<T> &A = adj->args<T>();
+    const int n_obs = p->desc.n_traces;
+    if (seeds && n_obs > 0)
+        k_adjoint_seed<T><<<std::max(1, std::min(1184, (n_obs + 255) / 256)), 256, 0, s>>>(A, p->ptr<TraceDev>(p->L.trace_tab), n_obs,
+                                                                                       (const T *)seeds, adj->q);
+    const Grid<T> &g = A.g;
+    const dim3 grid((unsigned)((long long)g.n[1] * g.n[2]), (unsigned)((g.n[0] + 127) / 128));
+    const T *slot = (const T *)snapshot;
+    switch (p->desc.components) {
+        case kMaskTM: k_adjoint_step<T, kMaskTM><<<grid, 128, 0, s>>>(A, slot, adj->q); break;
+        case kMaskTE: k_adjoint_step<T, kMaskTE><<<grid, 128, 0, s>>>(A, slot, adj->q); break;
+        default: k_adjoint_step<T, kMaskAll><<<grid, 128, 0, s>>>(A, slot, adj->q); break;
+    }
+    TFD_CUDA(cudaGetLastError());
+    adj->q ^= 1;
+    return TFD_OK;
+}
+
+template <typename T>
+int adjoint_sensitivity_t(tfd_adjoint *adj, void *dst, int where, cudaStream_t s) {
+    tfd_plan *p = adj->p;
+    const AdjArgs<T> &A = adj->args<T>();
+    const tfd_desc &d = p->desc;
+    const size_t bytes = (size_t)d.nx * d.ny * d.nz * 3 * sizeof(T);
+    T *out = (T *)dst;
+    T *staging = nullptr;
+    if (where == TFD_HOST) {
+        TFD_CUDA(cudaMallocAsync((void **)&staging, bytes, s));
+        out = staging;
+    }
+    k_internal_to_reference<T><<<launch_blocks((long long)d.nx * d.ny * d.nz * 3), 256, 0, s>>>(out, 3, d.nx, d.ny, d.nz,
+                                                                                            p->L.pitch, A.S[0], A.S[1], A.S[2]);
+    TFD_CUDA(cudaGetLastError());
+    if (staging) {
+        TFD_CUDA(cudaMemcpyAsync(dst, staging, bytes, cudaMemcpyDeviceToHost, s));
+        TFD_CUDA(cudaFreeAsync(staging, s));
+        TFD_CUDA(cudaStreamSynchronize(s));
+    }
+    return TFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tfd_state_bytes(tfd_plan *p, size_t *bytes) {
+    if (!p || !bytes) return fail(TFD_ERR_INVALID, "null argument");
+    *bytes = p->desc.precision == 8 ? state_layout<double>(p, nullptr).bytes : state_layout<float>(p, nullptr).bytes;
+    return TFD_OK;
+}
+
+int tfd_state_save(tfd_plan *p, void *dst, void *stream) {
+    if (!p || !dst || ((uintptr_t)dst & 255)) return fail(TFD_ERR_INVALID, "snapshot must be a 256-byte aligned device buffer");
+    if (p->in_batch) return fail(TFD_ERR_INVALID, "this plan belongs to a batch");
+    return p->desc.precision == 8 ? state_copy_t<double>(p, (char *)dst, true, as_stream(stream))
+                                  : state_copy_t<float>(p, (char *)dst, true, as_stream(stream));
+}
+
+int tfd_state_load(tfd_plan *p, const void *src, void *stream) {
+    if (!p || !src || ((uintptr_t)src & 255)) return fail(TFD_ERR_INVALID, "snapshot must be a 256-byte aligned device buffer");
+    if (p->in_batch) return fail(TFD_ERR_INVALID, "this plan belongs to a batch");
+    return p->desc.precision == 8 ? state_copy_t<double>(p, (char *)src, false, as_stream(stream))
+                                  : state_copy_t<float>(p, (char *)src, false, as_stream(stream));
+}
+
+int tfd_adjoint_bytes(tfd_plan *p, size_t *bytes) {
+    if (!p || !bytes) return fail(TFD_ERR_INVALID, "null argument");
+    *bytes = (p->desc.precision == 8 ? adjoint_layout<double>(p, nullptr, nullptr) : adjoint_layout<float>(p, nullptr, nullptr)) + 256;
+    return TFD_OK;
+}
+
+int tfd_adjoint_create(tfd_plan *p, void *arena, size_t arena_bytes, void *stream, tfd_adjoint **out) {
+    if (!p || !out) return fail(TFD_ERR_INVALID, "null argument");
+    *out = nullptr;
+    size_t need = 0;
+    tfd_adjoint_bytes(p, &need);
+    if (!arena || ((uintptr_t)arena & 255) || arena_bytes < need)
+        return fail(TFD_ERR_ARENA, "adjoint arena must be 256-byte aligned and at least tfd_adjoint_bytes() long");
+    tfd_adjoint *adj = new tfd_adjoint();
+    adj->p = p;
+    adj->arena = (char *)arena;
+    const int rc = p->desc.precision == 8 ? adjoint_create_t<double>(adj, as_stream(stream)) : adjoint_create_t<float>(adj, as_stream(stream));
+    if (rc) {
+        delete adj;
+        return rc;
+    }
+    *out = adj;
+    return TFD_OK;
+}
+
+int tfd_adjoint_reset(tfd_adjoint *adj, void *stream) {
+    if (!adj) return fail(TFD_ERR_INVALID, "null adjoint");
+    TFD_CUDA(cudaMemsetAsync(adj->arena, 0, adj->used, as_stream(stream)));
+    adj->q = 0;
+    return TFD_OK;
+}
+
+int tfd_adjoint_step(tfd_adjoint *adj, const void *snapshot, const void *seeds, void *stream) {
+    if (!adj || !snapshot || ((uintptr_t)snapshot & 255)) return fail(TFD_ERR_INVALID, "bad adjoint step arguments");
+    return adj->p->desc.precision == 8 ? adjoint_step_t<double>(adj, snapshot, seeds, as_stream(stream))
+                                       : adjoint_step_t<float>(adj, snapshot, seeds, as_stream(stream));
+}
+
+int tfd_adjoint_sensitivity(tfd_adjoint *adj, void *dst, int where, void *stream) {
+    if (!adj || !dst) return fail(TFD_ERR_INVALID, "null argument");
+    return adj->p->desc.precision == 8 ? adjoint_sensitivity_t<double>(adj, dst, where, as_stream(stream))
+                                       : adjoint_sensitivity_t<float>(adj, dst, where, as_stream(stream));
+}
+
+void tfd_adjoint_destroy(tfd_adjoint *adj) { delete adj; }
 
 }  // extern "C"

@@ -25,21 +25,21 @@ struct MonitorArgs {
     T *trace_out;                // [steps][n_traces]
     int n_planes;
     const PlaneDev *planes;
-    int max_samples;             // max over planes of points*components
+    int max_samples;             // max over planes of points*components, and the trace count
 };
 
 constexpr int kMonitorThreads = 256;
 constexpr int kPhaseChunk = 256;
 
-// Observations of step n for one plan: block (bx, by) handles sample chunk bx of plane by; block
-// (0, 0) also records the point traces.
+// Observations of step n for one plan: block (bx, by) handles sample chunk bx of plane by; the blocks
+// of row by = 0 also record the point traces, strided over the row.
 template <typename T>
 __device__ __forceinline__ void monitor_work(const MonitorArgs<T> &m, int bx, int by, long long n) {
     __shared__ double2 phase_e[kPhaseChunk], phase_h[kPhaseChunk];
     const long long shift = ((n + 1) & 1) ? m.count : 0;   // current (new) parity
     if (n >= m.steps) return;
-    if (bx == 0 && by == 0) {
-        for (int k = threadIdx.x; k < m.n_traces; k += blockDim.x) {
+    if (by == 0) {
+        for (int k = bx * blockDim.x + threadIdx.x; k < m.n_traces; k += gridDim.x * blockDim.x) {
             const TraceDev t = m.traces[k];
             const T *base = m.field[3 * t.family + t.comp];   // null: a component 2D does not advance (zero)
             m.trace_out[n * m.n_traces + k] = base ? base[shift + t.offset] : T(0);

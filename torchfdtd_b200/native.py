@@ -86,6 +86,15 @@ SIGNATURES = {
     'tfd_batch_step': (ctypes.c_int, [c_vp, c_i32, c_vp]),
     'tfd_batch_tiles': (ctypes.c_int, [c_vp, P_i32]),
     'tfd_batch_destroy': (None, [c_vp]),
+    'tfd_state_bytes': (ctypes.c_int, [c_vp, ctypes.POINTER(ctypes.c_size_t)]),
+    'tfd_state_save': (ctypes.c_int, [c_vp, c_vp, c_vp]),
+    'tfd_state_load': (ctypes.c_int, [c_vp, c_vp, c_vp]),
+    'tfd_adjoint_bytes': (ctypes.c_int, [c_vp, ctypes.POINTER(ctypes.c_size_t)]),
+    'tfd_adjoint_create': (ctypes.c_int, [c_vp, c_vp, ctypes.c_size_t, c_vp, ctypes.POINTER(c_vp)]),
+    'tfd_adjoint_reset': (ctypes.c_int, [c_vp, c_vp]),
+    'tfd_adjoint_step': (ctypes.c_int, [c_vp, c_vp, c_vp, c_vp]),
+    'tfd_adjoint_sensitivity': (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, c_vp]),
+    'tfd_adjoint_destroy': (None, [c_vp]),
     'tfd_error_string': (ctypes.c_char_p, [ctypes.c_int]),
     'tfd_last_error': (ctypes.c_char_p, []),
 }
@@ -219,6 +228,19 @@ class NativeGrid:
         self.kernel = {v: k for k, v in KERNELS.items()}[kernel_used.value]
         self.set_material(plan.inv_eps)
 
+    # ---- restart states (checkpoints of the discrete adjoint) ------------------------------------
+    def state_bytes(self):
+        v = ctypes.c_size_t()
+        check(library().tfd_state_bytes(self.handle, ctypes.byref(v)))
+        return v.value
+
+    def save_state(self, snapshot, stream=None):
+        """Copy the restart state into ``snapshot`` (a 256-byte aligned uint8 device tensor)."""
+        check(library().tfd_state_save(self.handle, c_vp(snapshot.data_ptr()), _stream(stream)))
+
+    def load_state(self, snapshot, stream=None):
+        check(library().tfd_state_load(self.handle, c_vp(snapshot.data_ptr()), _stream(stream)))
+
     def close(self):
         if getattr(self, 'batch', None) is not None:
             self.batch.close()
@@ -234,6 +256,15 @@ class NativeGrid:
 
     # ---- state transfer (reference layout, host numpy arrays) --------------------------------
     def set_material(self, inv_eps):
+        """Inverse permittivity in the reference layout: a host array, or a contiguous device tensor of the
+        plan's dtype (stream-ordered, no host copy)."""
+        if hasattr(inv_eps, 'data_ptr'):
+            t = inv_eps.contiguous()
+            if t.dtype != self.torch_dtype or t.device != self.device:
+                raise ValueError('device inverse permittivity must be a tensor of the plan dtype on its device')
+            self._material_tensor = t
+            check(library().tfd_set_material(self.handle, c_vp(t.data_ptr()), TFD_DEVICE, _stream()))
+            return
         a = np.ascontiguousarray(inv_eps, dtype=self.dtype)
         check(library().tfd_set_material(self.handle, c_vp(a.ctypes.data), TFD_HOST, _stream()))
 
@@ -300,6 +331,14 @@ class NativeGrid:
         return v.value
 
     # ---- observations ----------------------------------------------------------------------------
+    def traces_device(self):
+        """The (steps, traces) record as a torch tensor on the device."""
+        import torch
+        out = torch.zeros((self.plan.steps, len(self.plan.traces)), dtype=self.torch_dtype, device=self.device)
+        if out.numel():
+            check(library().tfd_get_traces(self.handle, c_vp(out.data_ptr()), TFD_DEVICE, _stream()))
+        return out
+
     def get_traces(self):
         out = np.zeros((self.plan.steps, len(self.plan.traces)), self.dtype)
         if out.size:
@@ -374,6 +413,48 @@ class NativeBatch:
             self.handle = None
             for g in self.grids:
                 g.batch = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+
+class NativeAdjoint:
+    """The discrete adjoint of a plan (its traces are the observers); owns its arena tensor."""
+
+    def __init__(self, grid):
+        import torch
+        self.grid = grid
+        lib = library()
+        size = ctypes.c_size_t()
+        check(lib.tfd_adjoint_bytes(grid.handle, ctypes.byref(size)))
+        self.arena = torch.empty(size.value, dtype=torch.uint8, device=grid.device)
+        handle = c_vp()
+        check(lib.tfd_adjoint_create(grid.handle, c_vp(self.arena.data_ptr()), size, _stream(), ctypes.byref(handle)))
+        self.handle = handle
+
+    def reset(self, stream=None):
+        check(library().tfd_adjoint_reset(self.handle, _stream(stream)))
+
+    def step(self, snapshot, seeds=None, stream=None):
+        """Transpose the step that left ``snapshot``'s state, after adding ``seeds`` (one per trace)."""
+        check(library().tfd_adjoint_step(self.handle, c_vp(snapshot.data_ptr()),
+                                         c_vp(seeds.data_ptr()) if seeds is not None else None, _stream(stream)))
+
+    def sensitivity(self):
+        """S = sum over steps of e_bar * curl_b(H), (nx, ny, nz, 3) torch tensor on the device."""
+        import torch
+        nx, ny, nz = self.grid.plan.shape
+        out = torch.empty((nx, ny, nz, 3), dtype=self.grid.torch_dtype, device=self.grid.device)
+        check(library().tfd_adjoint_sensitivity(self.handle, c_vp(out.data_ptr()), TFD_DEVICE, _stream()))
+        return out
+
+    def close(self):
+        if getattr(self, 'handle', None):
+            library().tfd_adjoint_destroy(self.handle)
+            self.handle = None
 
     def __del__(self):
         try:
