@@ -480,13 +480,111 @@ def run_ours_batch(args, world, rank, local):
     return line if rank == 0 else None
 
 
+def adjoint_workload(steps, precision='float32', seed=2024):
+    """3D discrete-adjoint design scene: 200 x 200 x 80 cells at 0.04 um (8 x 8 x 3.2 um), CPML 12, SiO2
+    background (eps 2.085) with a 2 x 2 x 0.22 um design region of density rho (seeded uniform noise,
+    Gaussian-smoothed with sigma 2 cells, sigmoid projection beta 8 about 0.5), eps = 2.085 + rho (12.08 -
+    2.085); an Ey dipole 2.5 um before the design and an x-normal DFT plane 2.5 um after it at 1.55 um.
+    Returns (project, design index box, rho parameters as a numpy array)."""
+    from scipy.ndimage import gaussian_filter
+    from torchfdtd_b200 import Boundaries, FieldMonitor, Project, Region, Source, SpectrumSettings
+    from torchfdtd_b200.models import RunControl
+    lam, mesh, L = 1.55, .04, 12
+    b = Boundaries(**{f'{a}_{s}': baseline_face(L) for a in 'xyz' for s in ('min', 'max')})
+    region = Region(dimension='3d', size=(8, 8, 3.2), mesh=mesh, pml_cells=L, background_index=2.085 ** .5, steps=steps,
+                    precision=precision, backend='cuda', cuda_kernel='fused', boundaries=b,
+                    run_control=RunControl(divergence_check=False), snapshot_interval=10000)
+    custom = SpectrumSettings(sampling='custom', custom_frequencies_hz=[C0 / (lam * 1e-6)], apodization='none')
+    src = dict(component='Ey', wavelength=lam, pulse='gaussian', time_definition='standard', pulse_length=20e-15,
+               pulse_offset=40e-15)
+    project = Project(name='adjoint design 200x200x80', region=region, sources=[Source(id='dip', center=(-2.5, 0, 0), **src)],
+                      monitors=[FieldMonitor(id='out', normal='x', center=(2.5, 0, 0), size=(0, 2.4, 1.2), spectrum=custom)])
+    n = (200, 200, 80)
+    dn = (int(round(2 / mesh)), int(round(2 / mesh)), int(round(.22 / mesh)))
+    lo = tuple((a - d) // 2 for a, d in zip(n, dn))
+    rng = np.random.default_rng(seed)
+    raw = gaussian_filter(rng.uniform(0, 1, size=dn), 2.0)
+    raw = (raw - raw.mean()) / max(raw.std(), 1e-12) * .15 + .5
+    return project, (lo, dn), raw
+
+
+def run_ours_adjoint(args, world, rank, local):
+    """Gradient of |mode overlap|^2 of the output-plane Ey at 1.55 um with respect to the design density
+    through the discrete adjoint, timed; then central differences on 16 seeded design voxels (float64)."""
+    import torch
+    from torchfdtd_b200.adjoint import AdjointOptions, DifferentiablePlaneSimulation
+    torch.cuda.set_device(local)
+    steps = 4000
+    results = {}
+    for precision in ('float32', 'float64'):
+        project, (lo, dn), raw = adjoint_workload(steps, precision)
+        dtype = torch.float32 if precision == 'float32' else torch.float64
+        model = DifferentiablePlaneSimulation(project, AdjointOptions())
+        shape = model.plan.shape
+        base = torch.full(shape, 2.085, dtype=dtype, device='cuda')
+        sl = tuple(slice(a, a + d) for a, d in zip(lo, dn))
+        theta = torch.tensor(raw, dtype=dtype, device='cuda', requires_grad=True)
+
+        def objective(param):
+            rho = torch.sigmoid(8 * (param - .5))
+            eps = base.clone()
+            eps[sl] = 2.085 + rho * (12.08 - 2.085)
+            ey = model(eps)['out'].fields[..., 1]
+            _, ny, nz = model._maps[0][0].plan['shape']
+            y = torch.linspace(-1, 1, ny, device='cuda', dtype=torch.float64)[:, None]
+            z = torch.linspace(-1, 1, nz, device='cuda', dtype=torch.float64)[None, :]
+            mode = torch.exp(-(y / .5) ** 2 - (z / .5) ** 2).reshape(-1).to(ey.dtype)
+            return (torch.abs((ey * mode.conj()).sum(dim=1)) ** 2).sum()
+        for _ in range(1):                              # warm-up: plans, kernels, snapshot buffers
+            objective(theta).backward()
+        theta.grad = None
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        value = objective(theta)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        value.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        report = model.engine(base).report
+        cells = int(np.prod(shape))
+        entry = dict(objective=float(value.detach()), forward_s=t1 - t0, backward_s=t2 - t1, gradient_s=t2 - t0,
+                     forward_gcells=cells * steps / (t1 - t0) / 1e9, checkpoints=report['checkpoints'],
+                     segment_steps=report['segment_steps'], replayed_steps=report['replayed_steps'],
+                     checkpoint_gb=report['checkpoint_bytes'] / 1e9, restart_mb=report['restart_bytes'] / 1e6)
+        if precision == 'float64':
+            grad = theta.grad.detach().cpu().numpy()
+            rng = np.random.default_rng(16)
+            picks = [tuple(int(rng.integers(0, d)) for d in dn) for _ in range(16)]
+            h, errors = 1e-4, []
+            with torch.no_grad():
+                for idx in picks:
+                    up, down = theta.detach().clone(), theta.detach().clone()
+                    up[idx] += h
+                    down[idx] -= h
+                    fd = float(objective(up) - objective(down)) / (2 * h)
+                    errors.append(abs(grad[idx] - fd) / max(abs(fd), 1e-3 * np.abs(grad).max()))
+            entry.update(fd_voxels=16, fd_step=h, fd_max_rel_err=float(max(errors)), fd_median_rel_err=float(np.median(errors)))
+        results[precision] = entry
+        model.close()
+    f32 = results['float32']
+    cells = 200 * 200 * 80
+    return dict(metric='adjoint gradient wall time', value=f32['gradient_s'], unit='s', n_gpus=world, steps=steps, warmup=1,
+                ms_per_step=f32['gradient_s'] / steps * 1e3, higher_is_better=False, scaling='weak', vs_baseline=None,
+                dtype='f32', data='synthetic (seeded)',
+                config=dict(workload='3D discrete adjoint 200x200x80 at 0.04 um, 2x2x0.22 um design (sigmoid beta 8), '
+                                     '|mode overlap of DFT Ey at 1.55 um|^2, 4000 steps, sqrt(T) checkpoints', cells=cells),
+                adjoint=results)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=200)
     ap.add_argument('--warmup', type=int, default=10)
     ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
-    ap.add_argument('--workload', choices=['roofline', 'roofline256', 'strip', 'tmz2d', 'batch64'], default='roofline')
+    ap.add_argument('--workload', choices=['roofline', 'roofline256', 'strip', 'tmz2d', 'batch64', 'adjoint3d'],
+                    default='roofline')
     ap.add_argument('--kernel', choices=['auto', 'march', 'gather', 'tile2d'], default='auto')
     ap.add_argument('--cpu-budget', type=float, default=15.0)
     ap.add_argument('--no-cpu-baseline', action='store_true')
@@ -503,7 +601,8 @@ def main():
         return
     world, rank, local = dist_setup(args)
     try:
-        line = (run_ours_batch if args.workload == 'batch64' else run_ours)(args, world, rank, local)
+        runner = {'batch64': run_ours_batch, 'adjoint3d': run_ours_adjoint}.get(args.workload, run_ours)
+        line = runner(args, world, rank, local)
         if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
     finally:
