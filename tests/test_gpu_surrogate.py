@@ -1,0 +1,69 @@
+"""The surrogate's BF16 tensor-core kernels (forward, backward data, backward weight, head, loss, Adam)
+against the CPU network oracle, which rounds the same operands to bfloat16 and accumulates in float64.
+
+Bars: outputs within 2e-3 relative L2; parameter and input gradients within 2e-2 (the back-propagated
+pre-activation gradients are BF16, so one rounding flip moves an element by 2^-8); training lowers the loss."""
+import numpy as np
+import pytest
+
+from oracle.surrogate_oracle import NetworkOracle
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-30))
+
+
+@pytest.mark.parametrize('shape', [(3, 24, 20), (2, 33, 17)])
+def test_forward_and_every_gradient_match_the_oracle(shape):
+    import torch
+    from torchfdtd_b200.surrogate import ConvNeuralOperator
+    net = ConvNeuralOperator(outputs=6, seed=3)
+    for k in net.params:
+        if k.startswith('b'):
+            net.params[k].copy_(torch.randn(net.params[k].shape, generator=torch.Generator().manual_seed(5)) * .1)
+    net.cast_weights()
+    rng = np.random.default_rng(2)
+    rho = rng.uniform(0, 1, size=shape).astype(np.float32)
+    dout = rng.normal(size=(shape[0], 6)).astype(np.float32)
+    out = net.forward(torch.tensor(rho, device='cuda')).cpu().numpy()
+    drho = net.backward(torch.tensor(dout, device='cuda'), input_gradient=True).cpu().numpy()
+    oracle = NetworkOracle(net.state_dict(), bf16=True)
+    expected = oracle.forward(rho)
+    grads = oracle.backward(dout.astype(np.float64), input_gradient=True)
+    assert rel(out, expected) <= 2e-3
+    for k, g in net.grads.items():
+        assert rel(g.cpu().numpy(), grads[k]) <= 2e-2, k
+    assert rel(drho, grads['rho']) <= 2e-2
+
+
+def test_loss_and_adam_match_their_definitions():
+    import torch
+    from torchfdtd_b200.surrogate import ConvNeuralOperator
+    net = ConvNeuralOperator(outputs=4, seed=1)
+    rho = torch.rand((2, 16, 16), device='cuda')
+    y = torch.randn((2, 4), device='cuda')
+    out = net.forward(rho).clone()
+    loss = float(net.loss(y))
+    assert abs(loss - float(((out - y) ** 2).mean())) <= 1e-6 * max(1, loss)
+    before = {k: v.clone() for k, v in net.params.items()}
+    g = {k: torch.randn_like(v) for k, v in net.params.items()}
+    for k in g:
+        net.grads[k].copy_(g[k])
+    net.adam_step(lr=1e-2)
+    for k, p in net.params.items():           # first Adam step: p - lr * g / (|g| + eps)
+        expected = before[k] - 1e-2 * g[k] / (g[k].abs() + 1e-8)
+        torch.testing.assert_close(p, expected, rtol=1e-5, atol=1e-6)
+
+
+def test_training_fits_a_smooth_map():
+    import torch
+    from torchfdtd_b200.surrogate import ConvNeuralOperator
+    gen = torch.Generator(device='cpu').manual_seed(0)
+    rho = torch.rand((512, 20, 20), generator=gen).cuda()
+    target = torch.stack([rho.mean(dim=(1, 2)), (rho[:, :10] - rho[:, 10:]).mean(dim=(1, 2))], dim=1) * 4
+    net = ConvNeuralOperator(outputs=2, seed=0)
+    history = net.fit(rho, target, epochs=15, batch=64, lr=3e-3)
+    assert history[-1] < .1 * history[0]
