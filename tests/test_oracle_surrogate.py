@@ -4,20 +4,20 @@ import numpy as np
 from oracle.surrogate_oracle import LAYERS, NetworkOracle
 
 
-def random_params(k=6, seed=0):
+def random_params(k=6, seed=0, features=64):
     rng = np.random.default_rng(seed)
     p = {}
     for l, (ci, _) in enumerate(LAYERS):
         p[f'w{l}'] = rng.normal(size=(9, 64, ci)) * np.sqrt(2 / (9 * (4 if l == 0 else ci)))
         p[f'b{l}'] = rng.normal(size=64) * .1
-    p['wh'] = rng.normal(size=(k, 64)) / 8
+    p['wh'] = rng.normal(size=(k, features)) / np.sqrt(features)
     p['bh'] = rng.normal(size=k) * .1
     return p
 
 
 def test_network_oracle_gradients_match_central_differences():
     rng = np.random.default_rng(1)
-    params = random_params()
+    params = random_params(features=1 * 1 * 64)     # 11 x 9 input -> 1 x 1 after four stride-2 layers
     rho = rng.uniform(0, 1, size=(2, 11, 9))
     dout = rng.normal(size=(2, 6))
     net = NetworkOracle(params, bf16=False)

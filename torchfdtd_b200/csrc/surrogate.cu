@@ -2,7 +2,7 @@
 // density to its complex transmission spectrum, trained and evaluated by these kernels.
 //
 // Numerics: BF16 operands, FP32 accumulation (tensor-core mma.sync m16n8k16, bf16 x bf16 -> f32), FP32
-// master weights, bias, head, loss and Adam state. Activations are NHWC bf16 with C = 16 (the packed input:
+// master weights, bias, head (linear on the flattened last feature map), loss and Adam state. Activations are NHWC bf16 with C = 16 (the packed input:
 // density, x, y, 1, zeros) or C = 64, so one pixel is one or four 16-byte vectors.
 //
 // Each conv is 3x3, zero padding 1, stride 1 or 2, Cout = 64, followed by GELU (tanh form):
@@ -268,22 +268,23 @@ __global__ void k_pack_input(const float *__restrict__ rho, bf16 *__restrict__ x
     }
 }
 
-// pooled[n, c] = mean_p a[n, p, c]; out[n, j] = bh[j] + sum_c wh[j, c] pooled[n, c]. One block per sample.
+// Linear head on the flattened last feature map: out[n, j] = bh[j] + sum_f wh[j, f] a[n, f], f = p * 64 + c
+// (the positions stay distinct: the scene is not translation invariant). One block per sample.
 __global__ void k_head_fwd(const bf16 *__restrict__ a, const float *__restrict__ wh, const float *__restrict__ bh,
-                           float *__restrict__ pooled, float *__restrict__ out, int HW, int K) {
-    __shared__ float sp[kCo];
+                           float *__restrict__ out, int F, int K) {
+    __shared__ float red[256];
     const int n = blockIdx.x;
-    for (int c = threadIdx.x; c < kCo; c += blockDim.x) {
+    for (int j = 0; j < K; ++j) {
         float s = 0.f;
-        for (int p = 0; p < HW; ++p) s += __bfloat162float(a[((long long)n * HW + p) * kCo + c]);
-        sp[c] = s / HW;
-        pooled[n * kCo + c] = sp[c];
-    }
-    __syncthreads();
-    for (int j = threadIdx.x; j < K; j += blockDim.x) {
-        float s = bh[j];
-        for (int c = 0; c < kCo; ++c) s += wh[j * kCo + c] * sp[c];
-        out[n * K + j] = s;
+        for (int f = threadIdx.x; f < F; f += blockDim.x) s += wh[(long long)j * F + f] * __bfloat162float(a[(long long)n * F + f]);
+        red[threadIdx.x] = s;
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[n * K + j] = bh[j] + red[0];
+        __syncthreads();
     }
 }
 
@@ -306,31 +307,35 @@ __global__ void k_mse(const float *__restrict__ out, const float *__restrict__ y
     if (threadIdx.x == 0) *loss = red[0] / total;
 }
 
-// Head backward: dwh, dbh (single block, deterministic), and dz_last = dpooled / HW * gelu'(z_last).
-__global__ void k_head_bwd_params(const float *__restrict__ dout, const float *__restrict__ pooled, float *__restrict__ dwh,
-                                  float *__restrict__ dbh, int N, int K) {
-    for (int e = threadIdx.x; e < K * kCo; e += blockDim.x) {
-        const int j = e / kCo, c = e % kCo;
+// Head backward: dwh[j, f] = sum_n dout[n, j] a[n, f], dbh[j] = sum_n dout[n, j] (deterministic), and
+// dz_last[n, f] = (sum_j dout[n, j] wh[j, f]) * gelu'(z_last[n, f]).
+__global__ void k_head_bwd_params(const float *__restrict__ dout, const bf16 *__restrict__ a, float *__restrict__ dwh,
+                                  float *__restrict__ dbh, int N, int F, int K) {
+    const long long total = (long long)K * F;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(e / F);
+        const long long f = e % F;
         float s = 0.f;
-        for (int n = 0; n < N; ++n) s += dout[n * K + j] * pooled[n * kCo + c];
+        for (int n = 0; n < N; ++n) s += dout[n * K + j] * __bfloat162float(a[(long long)n * F + f]);
         dwh[e] = s;
     }
-    for (int j = threadIdx.x; j < K; j += blockDim.x) {
-        float s = 0.f;
-        for (int n = 0; n < N; ++n) s += dout[n * K + j];
-        dbh[j] = s;
-    }
+    if (blockIdx.x == 0)
+        for (int j = threadIdx.x; j < K; j += blockDim.x) {
+            float s = 0.f;
+            for (int n = 0; n < N; ++n) s += dout[n * K + j];
+            dbh[j] = s;
+        }
 }
 
 __global__ void k_head_bwd_data(const float *__restrict__ dout, const float *__restrict__ wh, const bf16 *__restrict__ z,
-                                bf16 *__restrict__ dz, int N, int HW, int K) {
-    const long long total = (long long)N * HW * kCo;
+                                bf16 *__restrict__ dz, int N, int F, int K) {
+    const long long total = (long long)N * F;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(e % kCo);
-        const int n = (int)(e / ((long long)HW * kCo));
+        const int n = (int)(e / F);
+        const long long f = e % F;
         float s = 0.f;
-        for (int j = 0; j < K; ++j) s += dout[n * K + j] * wh[j * kCo + c];
-        dz[e] = __float2bfloat16_rn(s / HW * gelu_grad(__bfloat162float(z[e])));
+        for (int j = 0; j < K; ++j) s += dout[n * K + j] * wh[(long long)j * F + f];
+        dz[e] = __float2bfloat16_rn(s * gelu_grad(__bfloat162float(z[e])));
     }
 }
 
@@ -445,10 +450,10 @@ int tfd_sg_conv_backward_weight(const void *dz, const void *x, float *dw, float 
     return check_launch("tfd_sg_conv_backward_weight reduce");
 }
 
-int tfd_sg_head_forward(const void *a, const float *wh, const float *bh, float *pooled, float *out, int32_t n, int32_t hw, int32_t k,
+int tfd_sg_head_forward(const void *a, const float *wh, const float *bh, float *out, int32_t n, int32_t features, int32_t k,
                         void *stream) {
-    if (!a || !wh || !bh || !pooled || !out || n < 1 || hw < 1 || k < 1) return bad("tfd_sg_head_forward: bad arguments");
-    k_head_fwd<<<n, 64, 0, (cudaStream_t)stream>>>((const bf16 *)a, wh, bh, pooled, out, hw, k);
+    if (!a || !wh || !bh || !out || n < 1 || features < 1 || k < 1) return bad("tfd_sg_head_forward: bad arguments");
+    k_head_fwd<<<n, 256, 0, (cudaStream_t)stream>>>((const bf16 *)a, wh, bh, out, features, k);
     return check_launch("tfd_sg_head_forward");
 }
 
@@ -458,12 +463,13 @@ int tfd_sg_mse(const float *out, const float *y, float *dout, float *loss, int32
     return check_launch("tfd_sg_mse");
 }
 
-int tfd_sg_head_backward(const float *dout, const float *pooled, const float *wh, const void *z_last, float *dwh, float *dbh,
-                         void *dz_last, int32_t n, int32_t hw, int32_t k, void *stream) {
-    if (!dout || !pooled || !wh || !z_last || !dz_last || n < 1 || hw < 1 || k < 1) return bad("tfd_sg_head_backward: bad arguments");
+int tfd_sg_head_backward(const float *dout, const void *a_last, const float *wh, const void *z_last, float *dwh, float *dbh,
+                         void *dz_last, int32_t n, int32_t features, int32_t k, void *stream) {
+    if (!dout || !a_last || !wh || !z_last || !dz_last || n < 1 || features < 1 || k < 1) return bad("tfd_sg_head_backward: bad arguments");
     cudaStream_t s = (cudaStream_t)stream;
-    if (dwh && dbh) k_head_bwd_params<<<1, 256, 0, s>>>(dout, pooled, dwh, dbh, n, k);
-    k_head_bwd_data<<<blocks_for((long long)n * hw * kCo, 256), 256, 0, s>>>(dout, wh, (const bf16 *)z_last, (bf16 *)dz_last, n, hw, k);
+    if (dwh && dbh)
+        k_head_bwd_params<<<blocks_for((long long)k * features, 256), 256, 0, s>>>(dout, (const bf16 *)a_last, dwh, dbh, n, features, k);
+    k_head_bwd_data<<<blocks_for((long long)n * features, 256), 256, 0, s>>>(dout, wh, (const bf16 *)z_last, (bf16 *)dz_last, n, features, k);
     return check_launch("tfd_sg_head_backward");
 }
 

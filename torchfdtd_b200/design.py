@@ -235,16 +235,16 @@ def adjoint_design(problem, iterations=30, lr=.2, seed=0, theta0=None, log=None)
     return history, theta.detach()
 
 
-def surrogate_design(problem, net, target_fom, iterations=200, lr=.2, verify_every=5, finetune_steps=20, data=None,
-                     theta0=None, max_seconds=None, log=None):
-    """Surrogate-assisted loop: Adam ascent on theta with the network's input gradient; every ``verify_every``-th
-    iterate is simulated and becomes training data (``finetune_steps`` Adam steps on a batch mixing it with the
-    training set); a verified FOM below the best so far restarts from the best design with one adjoint step.
-    Stops once a verified FOM reaches ``target_fom``. Returns (history of (seconds, verified fom, source)),
-    best verified fom, best theta)."""
+def surrogate_design(problem, net, target_fom, iterations=200, lr=.2, verify_every=5, finetune_steps=10, data=None,
+                     theta0=None, max_seconds=None, patience=2, adjoint_lr=.2, log=None):
+    """Surrogate-assisted loop. Phase 1: Adam ascent on theta with the network's input gradient; every
+    ``verify_every``-th iterate is simulated (FDTD judges every accepted design) and becomes training data for a
+    short fine-tune; the best verified design is kept. When ``patience`` verifications in a row fail to improve
+    on it, phase 2 falls back to the plain discrete-adjoint loop from the best verified design. Stops once a
+    verified FOM reaches ``target_fom`` (or after ``max_seconds``). Returns (history of (seconds, verified fom,
+    source), best verified fom, best theta)."""
     import torch
     from .adjoint import DifferentiableSimulation
-    model = None
     theta = torch.zeros((problem.pixels, problem.pixels), dtype=torch.float64, device='cuda') if theta0 is None else theta0.clone()
     opt = torch.optim.Adam([theta.requires_grad_(True)], lr=lr)
     half = net.outputs // 2
@@ -252,6 +252,10 @@ def surrogate_design(problem, net, target_fom, iterations=200, lr=.2, verify_eve
     verified_rho, verified_y = [], []
     rng = np.random.default_rng(0)
     started = time.perf_counter()
+    stalled = 0
+
+    def done():
+        return best >= target_fom or (max_seconds and time.perf_counter() - started > max_seconds)
     for k in range(1, iterations + 1):
         with torch.no_grad():
             rho = torch.sigmoid(theta).to(torch.float32)[None]
@@ -271,36 +275,40 @@ def surrogate_design(problem, net, target_fom, iterations=200, lr=.2, verify_eve
         rho_np = torch.sigmoid(theta.detach()).cpu().numpy()
         t = problem.transmission([rho_np])[0]
         fom = float(problem.fom(t[None])[0])
-        source = 'surrogate'
         verified_rho.append(rho_np.astype(np.float32))
         verified_y.append(np.concatenate([t.real, t.imag]).astype(np.float32))
-        if fom > best:
-            best, best_theta = fom, theta.detach().clone()
-        elif fom < best - 1e-3:
-            # Fallback: back to the best verified design and one discrete-adjoint step from it.
-            if model is None:
-                model = DifferentiableSimulation(problem.project())
-            fom_best, grad = _adjoint_value_and_grad(problem, model, best_theta)
-            with torch.no_grad():
-                theta.copy_(best_theta)
-            opt.zero_grad()
-            theta.grad = -grad
-            opt.step()
-            source = 'adjoint fallback'
-        history.append((time.perf_counter() - started, fom, source))
+        if fom > best + 1e-4:
+            best, best_theta, stalled = fom, theta.detach().clone(), 0
+        else:
+            stalled += 1
+        history.append((time.perf_counter() - started, fom, 'surrogate'))
         if log:
-            log(k, fom, source)
-        if best >= target_fom or (max_seconds and time.perf_counter() - started > max_seconds):
+            log(k, fom, 'surrogate')
+        if done() or stalled >= patience:
             break
         if finetune_steps and data is not None:
             rho_train, y_train = data
-            vr = torch.tensor(np.stack(verified_rho), device='cuda')
-            vy = torch.tensor(np.stack(verified_y), device='cuda')
+            vr = torch.tensor(np.stack(verified_rho[-16:]), device='cuda')
+            vy = torch.tensor(np.stack(verified_y[-16:]), device='cuda')
             for _ in range(finetune_steps):
-                idx = torch.as_tensor(rng.integers(0, rho_train.shape[0], 48), device='cuda')
-                rb = torch.cat([rho_train[idx], vr[-16:]])
-                yb = torch.cat([y_train[idx], vy[-16:]])
-                net.train_step(rb, yb, lr=3e-4)
-    if model is not None:
+                idx = torch.as_tensor(rng.integers(0, rho_train.shape[0], 64 - vr.shape[0]), device='cuda')
+                net.train_step(torch.cat([rho_train[idx], vr]), torch.cat([y_train[idx], vy]), lr=3e-4)
+    if not done():
+        # Phase 2: the plain adjoint loop from the best verified design (each iterate is an FDTD evaluation).
+        model = DifferentiableSimulation(problem.project())
+        theta = best_theta.clone()
+        opt = torch.optim.Adam([theta.requires_grad_(True)], lr=adjoint_lr)
+        while not done():
+            fom, grad = _adjoint_value_and_grad(problem, model, theta)
+            if fom > best:
+                best, best_theta = fom, theta.detach().clone()
+            history.append((time.perf_counter() - started, fom, 'adjoint'))
+            if log:
+                log(len(history), fom, 'adjoint')
+            if done():
+                break
+            opt.zero_grad()
+            theta.grad = -grad
+            opt.step()
         model.close()
     return history, best, best_theta

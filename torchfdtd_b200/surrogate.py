@@ -2,10 +2,11 @@
 
 The network maps a design density rho (n, H, W) in [0, 1] to K real outputs (here the real and imaginary parts
 of a complex transmission spectrum). Architecture: packed input (2 rho - 1, x, y, 1; 16 channels), 8 conv
-layers of 64 channels (3x3, zero padding 1, strides 1, 2, 1, 2, 1, 2, 1, 2, GELU), mean pooling and a linear
-head. Every op of training and inference runs in ``csrc/surrogate.cu``: BF16 tensor-core implicit GEMMs with
-FP32 accumulation for the convolutions (forward, backward data, backward weight), FP32 head, mean-squared
-loss and Adam with FP32 master weights. Torch provides the device buffers only.
+layers of 64 channels (3x3, zero padding 1, strides 1, 2, 1, 2, 1, 2, 1, 2, GELU) and a linear head on the
+flattened last feature map (positions stay distinct: the scenes are not translation invariant). Every op of
+training and inference runs in ``csrc/surrogate.cu``: BF16 tensor-core implicit GEMMs with FP32 accumulation
+for the convolutions (forward, backward data, backward weight), FP32 head, mean-squared loss and Adam with
+FP32 master weights. Torch provides the device buffers only.
 """
 from __future__ import annotations
 
@@ -24,7 +25,7 @@ _SIGNATURES = {
     'tfd_sg_conv_backward_data': [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 5 + [ctypes.c_void_p],
     'tfd_sg_wgrad_scratch': [ctypes.c_int32] * 6 + [ctypes.POINTER(ctypes.c_size_t)],
     'tfd_sg_conv_backward_weight': [ctypes.c_void_p] * 5 + [ctypes.c_size_t] + [ctypes.c_int32] * 6 + [ctypes.c_void_p],
-    'tfd_sg_head_forward': [ctypes.c_void_p] * 5 + [ctypes.c_int32] * 3 + [ctypes.c_void_p],
+    'tfd_sg_head_forward': [ctypes.c_void_p] * 4 + [ctypes.c_int32] * 3 + [ctypes.c_void_p],
     'tfd_sg_mse': [ctypes.c_void_p] * 4 + [ctypes.c_int32, ctypes.c_void_p],
     'tfd_sg_head_backward': [ctypes.c_void_p] * 7 + [ctypes.c_int32] * 3 + [ctypes.c_void_p],
     'tfd_sg_adam': [ctypes.c_void_p] * 4 + [ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -62,9 +63,14 @@ class ConvNeuralOperator:
     """The surrogate network with its Adam state; ``forward``, ``backward`` and ``train_step`` run the
     engine's kernels on CUDA tensors."""
 
-    def __init__(self, outputs=32, seed=0, device='cuda'):
+    def __init__(self, outputs=32, seed=0, device='cuda', input_shape=(100, 100)):
         import torch
         self.outputs = outputs
+        h, w = input_shape
+        for _, stride in LAYERS:
+            h, w = out_size(h, stride), out_size(w, stride)
+        self.input_shape = tuple(input_shape)
+        self.features = h * w * CO
         self.device = torch.device(device)
         g = torch.Generator(device='cpu').manual_seed(seed)
         self.params = {}
@@ -72,7 +78,7 @@ class ConvNeuralOperator:
             fan_in = 9 * (4 if l == 0 else ci)
             self.params[f'w{l}'] = (torch.randn((9, CO, ci), generator=g) * math.sqrt(2.0 / fan_in)).to(self.device)
             self.params[f'b{l}'] = torch.zeros(CO, device=self.device)
-        self.params['wh'] = (torch.randn((outputs, CO), generator=g) / math.sqrt(CO)).to(self.device)
+        self.params['wh'] = (torch.randn((outputs, self.features), generator=g) / math.sqrt(self.features)).to(self.device)
         self.params['bh'] = torch.zeros(outputs, device=self.device)
         self.adam = {k: (torch.zeros_like(v), torch.zeros_like(v)) for k, v in self.params.items()}
         self.grads = {k: torch.zeros_like(v) for k, v in self.params.items()}
@@ -133,7 +139,6 @@ class ConvNeuralOperator:
             hh, ww = ho, wo
         b['scratch'] = torch.empty(max(1, scratch // 4), dtype=torch.float32, device=self.device)
         b['scratch_bytes'] = scratch
-        b['pooled'] = torch.empty((n, CO), dtype=torch.float32, device=self.device)
         b['out'] = torch.empty((n, self.outputs), dtype=torch.float32, device=self.device)
         b['dout'] = torch.empty((n, self.outputs), dtype=torch.float32, device=self.device)
         b['loss'] = torch.empty(1, dtype=torch.float32, device=self.device)
@@ -147,6 +152,8 @@ class ConvNeuralOperator:
         lib, check = _lib()
         rho = rho.contiguous().float()
         n, h, w = rho.shape
+        if (h, w) != self.input_shape:
+            raise ValueError(f'the network was built for {self.input_shape} inputs, not {(h, w)}')
         self._hw = (h, w)
         b = self._alloc(n, h, w)
         s = _stream()
@@ -157,9 +164,8 @@ class ConvNeuralOperator:
             check(lib.tfd_sg_conv_forward(_p(x), _p(self.wb[l]), _p(self.params[f'b{l}']), _p(b['z'][l]), _p(b['a'][l]),
                                           n, hh, ww, ci, stride, s))
             x = b['a'][l]
-        _, _, ho, wo = b['shapes'][-1]
-        check(lib.tfd_sg_head_forward(_p(x), _p(self.params['wh']), _p(self.params['bh']), _p(b['pooled']), _p(b['out']),
-                                      n, ho * wo, self.outputs, s))
+        check(lib.tfd_sg_head_forward(_p(x), _p(self.params['wh']), _p(self.params['bh']), _p(b['out']),
+                                      n, self.features, self.outputs, s))
         self._last = (n, h, w)
         return b['out']
 
@@ -171,10 +177,9 @@ class ConvNeuralOperator:
         b = self._buffers[(n, h, w)]
         s = _stream()
         dout = dout.contiguous().float()
-        _, _, ho, wo = b['shapes'][-1]
-        check(lib.tfd_sg_head_backward(_p(dout), _p(b['pooled']), _p(self.params['wh']), _p(b['z'][-1]),
+        check(lib.tfd_sg_head_backward(_p(dout), _p(b['a'][-1]), _p(self.params['wh']), _p(b['z'][-1]),
                                        _p(self.grads['wh']) if parameters else None, _p(self.grads['bh']) if parameters else None,
-                                       _p(b['dz'][-1]), n, ho * wo, self.outputs, s))
+                                       _p(b['dz'][-1]), n, self.features, self.outputs, s))
         for l in range(len(LAYERS) - 1, -1, -1):
             ci, stride = LAYERS[l]
             hh, ww, _, _ = b['shapes'][l]
