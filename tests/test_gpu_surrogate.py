@@ -18,10 +18,18 @@ def rel(a, b):
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-30))
 
 
-@pytest.mark.parametrize('shape', [(3, 24, 20), (2, 33, 17)])
-def test_forward_and_every_gradient_match_the_oracle(shape):
+@pytest.fixture(params=['tcgen05', 'mma'])
+def tensor_path(request):
+    from torchfdtd_b200.surrogate import set_tensor_path
+    set_tensor_path(request.param)
+    yield request.param
+    set_tensor_path('tcgen05')
+
+
+@pytest.mark.parametrize('shape', [(3, 24, 20), (2, 33, 17), (5, 40, 40)])
+def test_forward_and_every_gradient_match_the_oracle(shape, tensor_path):
     import torch
-    from torchfdtd_b200.surrogate import ConvNeuralOperator
+    from torchfdtd_b200.surrogate import ConvNeuralOperator, device_status
     net = ConvNeuralOperator(outputs=6, seed=3, input_shape=shape[1:])
     for k in net.params:
         if k.startswith('b'):
@@ -39,6 +47,7 @@ def test_forward_and_every_gradient_match_the_oracle(shape):
     for k, g in net.grads.items():
         assert rel(g.cpu().numpy(), grads[k]) <= 2e-2, k
     assert rel(drho, grads['rho']) <= 2e-2
+    assert device_status() == 0
 
 
 def test_loss_and_adam_match_their_definitions():

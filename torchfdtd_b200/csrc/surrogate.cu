@@ -362,6 +362,216 @@ __global__ void k_cast_weights(const float *__restrict__ w, bf16 *__restrict__ w
     }
 }
 
+// ---- tcgen05 path: 5th-generation tensor cores, accumulators in tensor memory -------------------------
+// One CTA = 128 output rows (pixels) x N columns. Per tap, the 128 threads gather their row's K = 16..64
+// input channels (16-byte vectors) and the tap's weights into a shared-memory stage laid out K-major without
+// swizzle (8-row x 16-byte core matrices: rows 16 bytes apart, 8-row groups 128 bytes apart (SBO), 16-byte
+// K chunks one 128- or N-row block apart (LBO)); one thread issues the tap's tcgen05.mma instructions
+// (M = 128, K = 16 each) into the tensor-memory accumulator and commits them to the stage's mbarrier, while
+// the CTA gathers the next tap into the other stage. The epilogue reads the accumulator with tcgen05.ld
+// (warp w: tensor-memory lanes 32w..32w+31 = its 32 rows). Every wait is bounded: on a timeout the kernel
+// records g_sg_status, waits (bounded) for its own MMAs, frees its tensor memory and returns.
+__device__ int g_sg_status;
+
+__device__ __forceinline__ uint32_t sh_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;                    // descriptor version of sm_100; no swizzle, base offset 0
+    return d;
+}
+
+// kind::f16 instruction descriptor: D f32, A and B bf16, both K-major, shape M x N.
+__host__ __device__ constexpr uint32_t umma_idesc(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate) : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(sh_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void bar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sh_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t parity) {
+    const uint32_t addr = sh_addr(bar);
+    for (int it = 0; it < 2000; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done) : "r"(addr), "r"(parity), "r"(1000000u) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int COLS>
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sh_addr(slot)), "r"(COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+template <int COLS>
+__device__ __forceinline__ void tmem_free(uint32_t tmem) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS) : "memory");
+}
+
+// 32 lanes x 16 columns of 32-bit accumulators (one warp, its own lane quarter), then wait.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]),
+          "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Shared-memory bytes of one tcgen05 conv CTA: two A stages (128 x K), two B stages (N x K), barriers, slot.
+__host__ __device__ constexpr int tc_smem(int K, int N) { return 2 * (K * 128 * 2) + 2 * (K * N * 2) + 64; }
+
+// MODE 0 forward (K = CI input channels per tap, N = 64 output channels);
+// MODE 1 backward data (K = 64 output channels per tap, N = CI input channels).
+template <int MODE, int CI>
+__global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, const bf16 *__restrict__ wsrc,
+                                                const float *__restrict__ bias, const bf16 *__restrict__ zprev, bf16 *__restrict__ out0,
+                                                void *__restrict__ out1, int N, int H, int W, int Ho, int Wo, int stride) {
+    constexpr int K = MODE == 0 ? CI : kCo;              // reduction channels per tap
+    constexpr int NC = MODE == 0 ? kCo : CI;             // output columns
+    constexpr int KC = K / 8;                            // 16-byte K chunks per tap
+    constexpr int A_BYTES = KC * 128 * 16, B_BYTES = KC * NC * 16;
+    constexpr int COLS = NC < 32 ? 32 : NC;
+    constexpr uint32_t IDESC = umma_idesc(128, NC);
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *As = smem, *Bs = smem + 2 * A_BYTES;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Bs + 2 * B_BYTES);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    // Output rows: MODE 0 output pixels (n, oy, ox); MODE 1 input pixels (n, y, x).
+    const int RH = MODE == 0 ? Ho : H, RW = MODE == 0 ? Wo : W;
+    const long long rows = (long long)N * RH * RW;
+    const long long row = (long long)blockIdx.x * 128 + tid;
+    const bool live = row < rows;
+    const int n = live ? (int)(row / ((long long)RH * RW)) : 0;
+    const int rem = live ? (int)(row % ((long long)RH * RW)) : 0;
+    const int ry = rem / RW, rx = rem % RW;
+    if (warp == 0) tmem_alloc<COLS>(slot);
+    if (tid == 0) {
+        bar_init(&bar[0]);
+        bar_init(&bar[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+    bool ok = true;
+    int issued = 0;                                      // taps whose MMAs were committed
+    for (int tap = 0; tap < 9; ++tap) {
+        const int s = tap & 1, ky = tap / 3, kx = tap % 3;
+        if (tap >= 2 && !bar_wait(&bar[s], ((tap >> 1) - 1) & 1)) ok = false;
+        if (__syncthreads_or(!ok)) break;
+        // A: this thread's row, K channels of the tap's neighbour (zero outside or not on the stride grid).
+        const bf16 *a = nullptr;
+        if (live) {
+            if (MODE == 0) {
+                const int iy = ry * stride + ky - 1, ix = rx * stride + kx - 1;
+                if (iy >= 0 && iy < H && ix >= 0 && ix < W) a = src + (((long long)n * H + iy) * W + ix) * CI;
+            } else {
+                const int ty = ry + 1 - ky, tx = rx + 1 - kx;
+                if (ty >= 0 && tx >= 0 && ty % stride == 0 && tx % stride == 0 && ty / stride < Ho && tx / stride < Wo)
+                    a = src + (((long long)n * Ho + ty / stride) * Wo + tx / stride) * kCo;
+            }
+        }
+        unsigned char *as = As + s * A_BYTES;
+#pragma unroll
+        for (int kc = 0; kc < KC; ++kc)
+            *reinterpret_cast<uint4 *>(as + (kc * 128 + tid) * 16) = a ? *reinterpret_cast<const uint4 *>(a + kc * 8) : make_uint4(0, 0, 0, 0);
+        // B: the tap's weights, [K chunk][column][16 bytes]; MODE 0 w[tap][co][ci], MODE 1 w[tap][ci][co].
+        unsigned char *bs = Bs + s * B_BYTES;
+        for (int e = tid; e < NC * KC; e += 128) {
+            const int col = e / KC, kc = e % KC;
+            *reinterpret_cast<uint4 *>(bs + (kc * NC + col) * 16) =
+                *reinterpret_cast<const uint4 *>(wsrc + ((long long)tap * NC + col) * K + kc * 8);
+        }
+        proxy_fence();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int kk = 0; kk < K / 16; ++kk) {
+                const uint64_t ad = umma_desc(sh_addr(as) + kk * 2 * (128 * 16), 128 * 16, 128);
+                const uint64_t bd = umma_desc(sh_addr(bs) + kk * 2 * (NC * 16), NC * 16, 128);
+                umma_bf16(tmem, ad, bd, IDESC, (tap | kk) != 0);
+            }
+            umma_commit(&bar[s]);
+        }
+        issued = tap + 1;
+    }
+    // Wait for the last committed tap (its commit covers every earlier MMA of this thread).
+    if (issued > 0 && !bar_wait(&bar[(issued - 1) & 1], ((issued - 1) >> 1) & 1)) ok = false;
+    tc_fence_after();
+    if (__syncthreads_or(!ok) || issued < 9) {
+        if (tid == 0) atomicExch(&g_sg_status, 1);
+    } else {
+#pragma unroll
+        for (int c0 = 0; c0 < NC; c0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
+            if (!live) continue;
+            if (MODE == 0) {
+                __align__(16) bf16 zb[16], ab[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const float z = v[i] + bias[c0 + i];
+                    zb[i] = __float2bfloat16_rn(z);
+                    ab[i] = __float2bfloat16_rn(gelu(z));
+                }
+                uint4 *zd = reinterpret_cast<uint4 *>(out0 + row * kCo + c0);
+                uint4 *adst = reinterpret_cast<uint4 *>(reinterpret_cast<bf16 *>(out1) + row * kCo + c0);
+                zd[0] = reinterpret_cast<const uint4 *>(zb)[0];
+                zd[1] = reinterpret_cast<const uint4 *>(zb)[1];
+                adst[0] = reinterpret_cast<const uint4 *>(ab)[0];
+                adst[1] = reinterpret_cast<const uint4 *>(ab)[1];
+            } else if (zprev) {
+                __align__(16) bf16 db[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    db[i] = __float2bfloat16_rn(v[i] * gelu_grad(__bfloat162float(zprev[row * CI + c0 + i])));
+                uint4 *dd = reinterpret_cast<uint4 *>(out0 + row * CI + c0);
+                dd[0] = reinterpret_cast<const uint4 *>(db)[0];
+                dd[1] = reinterpret_cast<const uint4 *>(db)[1];
+            } else {
+                float *o = reinterpret_cast<float *>(out1) + row * CI + c0;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) o[i] = v[i];
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_free<COLS>(tmem);
+}
+
+int g_tensor_path = 1;       // 1: tcgen05 kernels for conv forward / backward data; 0: mma.sync kernels
+
 int blocks_for(long long work, int threads) {
     const long long b = (work + threads - 1) / threads;
     return (int)(b < 1 ? 1 : (b > 148 * 16 ? 148 * 16 : b));
@@ -387,6 +597,27 @@ int out_size(int n, int stride) { return (n - 1) / stride + 1; }
 
 extern "C" {
 
+// 1: conv forward and backward data on the tcgen05 kernels (default); 0: on the mma.sync kernels.
+int tfd_sg_set_tensor_path(int32_t mode) {
+    if (mode != 0 && mode != 1) return bad("tfd_sg_set_tensor_path: mode 0 or 1");
+    g_tensor_path = mode;
+    return TFD_OK;
+}
+
+// Device status of the surrogate kernels (1: a bounded tensor-core wait timed out); reading clears it.
+int tfd_sg_status(int32_t *status) {
+    if (!status) return bad("tfd_sg_status: null argument");
+    int v = 0, zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_sg_status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_sg_status, &zero, sizeof(int));
+    if (e != cudaSuccess) {
+        tfd::set_error(std::string("tfd_sg_status: ") + cudaGetErrorString(e));
+        return TFD_ERR_CUDA;
+    }
+    *status = v;
+    return TFD_OK;
+}
+
 int tfd_sg_pack_input(const float *rho, int32_t n, int32_t h, int32_t w, void *x0, void *stream) {
     if (!rho || !x0 || n < 1 || h < 1 || w < 1) return bad("tfd_sg_pack_input: bad arguments");
     k_pack_input<<<blocks_for((long long)n * h * w, 256), 256, 0, (cudaStream_t)stream>>>(rho, (bf16 *)x0, n, h, w);
@@ -399,8 +630,21 @@ int tfd_sg_conv_forward(const void *x, const void *w, const float *bias, void *z
         return bad("tfd_sg_conv_forward: bad arguments (ci 16 or 64, stride 1 or 2)");
     const int ho = out_size(h, stride), wo = out_size(wd, stride);
     const long long P = (long long)n * ho * wo;
-    const dim3 grid((unsigned)((P + kTile - 1) / kTile));
     cudaStream_t s = (cudaStream_t)stream;
+    if (g_tensor_path) {
+        const dim3 grid((unsigned)((P + 127) / 128));
+        if (ci == 16) {
+            static const cudaError_t attr = cudaFuncSetAttribute(k_conv_tc<0, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(16, 64));
+            (void)attr;
+            k_conv_tc<0, 16><<<grid, 128, tc_smem(16, 64), s>>>((const bf16 *)x, (const bf16 *)w, bias, nullptr, (bf16 *)z, a, n, h, wd, ho, wo, stride);
+        } else {
+            static const cudaError_t attr = cudaFuncSetAttribute(k_conv_tc<0, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(64, 64));
+            (void)attr;
+            k_conv_tc<0, 64><<<grid, 128, tc_smem(64, 64), s>>>((const bf16 *)x, (const bf16 *)w, bias, nullptr, (bf16 *)z, a, n, h, wd, ho, wo, stride);
+        }
+        return check_launch("tfd_sg_conv_forward (tcgen05)");
+    }
+    const dim3 grid((unsigned)((P + kTile - 1) / kTile));
     if (ci == 16) k_conv_fwd<16><<<grid, kThreads, 0, s>>>((const bf16 *)x, (const bf16 *)w, bias, (bf16 *)z, (bf16 *)a, n, h, wd, ho, wo, stride);
     else k_conv_fwd<64><<<grid, kThreads, 0, s>>>((const bf16 *)x, (const bf16 *)w, bias, (bf16 *)z, (bf16 *)a, n, h, wd, ho, wo, stride);
     return check_launch("tfd_sg_conv_forward");
@@ -412,8 +656,25 @@ int tfd_sg_conv_backward_data(const void *dz, const void *wt, const void *zprev,
         return bad("tfd_sg_conv_backward_data: bad arguments");
     const int ho = out_size(h, stride), wo = out_size(wd, stride);
     const long long Q = (long long)n * h * wd;
-    const dim3 grid((unsigned)((Q + kTile - 1) / kTile));
     cudaStream_t s = (cudaStream_t)stream;
+    if (g_tensor_path) {
+        const dim3 grid((unsigned)((Q + 127) / 128));
+        bf16 *o0 = zprev ? (bf16 *)out : nullptr;
+        void *o1 = zprev ? nullptr : out;
+        if (ci == 16) {
+            static const cudaError_t attr = cudaFuncSetAttribute(k_conv_tc<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(64, 16));
+            (void)attr;
+            k_conv_tc<1, 16><<<grid, 128, tc_smem(64, 16), s>>>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd,
+                                                               ho, wo, stride);
+        } else {
+            static const cudaError_t attr = cudaFuncSetAttribute(k_conv_tc<1, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(64, 64));
+            (void)attr;
+            k_conv_tc<1, 64><<<grid, 128, tc_smem(64, 64), s>>>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd,
+                                                               ho, wo, stride);
+        }
+        return check_launch("tfd_sg_conv_backward_data (tcgen05)");
+    }
+    const dim3 grid((unsigned)((Q + kTile - 1) / kTile));
     if (ci == 16) k_conv_dgrad<16><<<grid, kThreads, 0, s>>>((const bf16 *)dz, (const bf16 *)wt, (const bf16 *)zprev, out, n, h, wd, ho, wo, stride);
     else k_conv_dgrad<64><<<grid, kThreads, 0, s>>>((const bf16 *)dz, (const bf16 *)wt, (const bf16 *)zprev, out, n, h, wd, ho, wo, stride);
     return check_launch("tfd_sg_conv_backward_data");

@@ -31,6 +31,8 @@ _SIGNATURES = {
     'tfd_sg_adam': [ctypes.c_void_p] * 4 + [ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                             ctypes.c_int32, ctypes.c_void_p],
     'tfd_sg_cast_weights': [ctypes.c_void_p] * 3 + [ctypes.c_int32, ctypes.c_void_p],
+    'tfd_sg_set_tensor_path': [ctypes.c_int32],
+    'tfd_sg_status': [ctypes.POINTER(ctypes.c_int32)],
 }
 
 
@@ -44,6 +46,21 @@ def _lib():
             fn.argtypes = args
         lib._sg_bound = True
     return lib, check
+
+
+def set_tensor_path(mode):
+    """'tcgen05' (default): conv forward and backward data on the 5th-generation tensor cores with tensor-memory
+    accumulators; 'mma': on warp-level mma.sync kernels (the backward-weight kernel always uses mma.sync)."""
+    lib, check = _lib()
+    check(lib.tfd_sg_set_tensor_path({'mma': 0, 'tcgen05': 1}[mode]))
+
+
+def device_status():
+    """1 if a bounded tensor-core wait timed out since the last call, else 0 (reading clears it)."""
+    lib, check = _lib()
+    v = ctypes.c_int32()
+    check(lib.tfd_sg_status(ctypes.byref(v)))
+    return v.value
 
 
 def _p(t):
