@@ -139,6 +139,14 @@ def batch_workload(steps, seed=2024, count=64, mesh=.05, layers=16):
                            '{2.085, 12.08}, CPML 16, FP32, one persistent launch per step over all grids')
 
 
+def measured_tensor_peak():
+    path = ROOT / 'MEASURED_PEAKS.json'
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data.get('bf16_tflops', 1590.0)), 'measured (burst)'
+    return 1590.0, 'fallback'
+
+
 def measured_peaks():
     path = ROOT / 'MEASURED_PEAKS.json'
     if path.exists():
@@ -606,13 +614,23 @@ def run_ours_surrogate(args, world, rank, local):
     mse = float(((pred - y_t[val]) ** 2).mean())
     baseline = float(((y_t[val] - y_t[train].mean(dim=0)) ** 2).mean())
     flops = 3 * net.flops_per_sample * rho_aug.shape[0] * epochs
-    # inference throughput on a batch of 256
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    for _ in range(10):
+    # inference throughput on a batch of 256, on the tcgen05 kernels and on the mma.sync kernels
+    from torchfdtd_b200.surrogate import device_status, set_tensor_path
+    infer = {}
+    for path in ('mma', 'tcgen05'):
+        set_tensor_path(path)
         net.forward(rho_t[:256])
-    torch.cuda.synchronize()
-    infer_s = (time.perf_counter() - t1) / 10
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(20):
+            net.forward(rho_t[:256])
+        end.record()
+        end.synchronize()
+        infer[path] = start.elapsed_time(end) / 20 / 1e3
+    set_tensor_path('tcgen05')
+    infer_s = infer['tcgen05']
+    peak_tf = measured_tensor_peak()
     # design loops
     iterations = args.design_iterations
     plain, theta = adjoint_design(problem, iterations=iterations, lr=.2)
@@ -637,7 +655,12 @@ def run_ours_surrogate(args, world, rank, local):
                                gcells_per_s=4096 * problem.cells ** 2 * problem.steps / gen_s / 1e9),
                   training=dict(seconds=train_s, tflops=flops / train_s / 1e12, loss_first=history[0], loss_last=history[-1],
                                 validation_mse=mse, mean_predictor_mse=baseline, r2=1 - mse / baseline,
-                                inference_ms_per_256=infer_s * 1e3),
+                                inference_ms_per_256=infer_s * 1e3, inference_ms_per_256_mma_sync=infer['mma'] * 1e3,
+                                status=device_status()),
+                  roofline=dict(bound='tensor', achieved=256 * net.flops_per_sample / infer_s / 1e12, peak=peak_tf[0],
+                                unit='TFLOP/s', frac=256 * net.flops_per_sample / infer_s / 1e12 / peak_tf[0],
+                                peak_source=peak_tf[1], traffic=None,
+                                note='conv-layer FLOPs of a 256-sample inference pass (8 layers; head, packing included in time)'),
                   design=dict(plain_fom=target, plain_seconds=plain_time, plain_seconds_to_99pct=reach,
                               surrogate_best_fom=best, surrogate_seconds=sur_time, reached=reached,
                               speedup_vs_plain=plain_time / sur_time if reached else None,

@@ -251,40 +251,38 @@ __global__ void k_reduce_partials(const float *__restrict__ partial, int chunks,
 }
 
 // ---- input packing, head, loss, optimiser ---------------------------------------------------------------
-// x0[n, y, x, :] = (2 rho - 1, xc, yc, 1, 0 ...) with coordinates in [-1, 1].
-__global__ void k_pack_input(const float *__restrict__ rho, bf16 *__restrict__ x0, int N, int H, int W) {
-    const long long total = (long long)N * H * W;
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < total; p += (long long)gridDim.x * blockDim.x) {
-        const int rem = (int)(p % ((long long)H * W));
+// x0[n, y, x, :] = (2 rho - 1, xc, yc, 1, 0 ...) with coordinates in [-1, 1]; two 16-byte stores per pixel.
+__global__ void k_pack_input(const float *__restrict__ rho, bf16 *__restrict__ x0, int total, int H, int W) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+        const int rem = p % (H * W);
         const int y = rem / W, x = rem % W;
-        float v[16] = {};
-        v[0] = 2.f * rho[p] - 1.f;
-        v[1] = W > 1 ? -1.f + 2.f * x / (W - 1) : 0.f;
-        v[2] = H > 1 ? -1.f + 2.f * y / (H - 1) : 0.f;
-        v[3] = 1.f;
-        bf16 *o = x0 + p * 16;
+        __align__(16) bf16 v[16];
 #pragma unroll
-        for (int c = 0; c < 16; ++c) o[c] = __float2bfloat16_rn(v[c]);
+        for (int c = 0; c < 16; ++c) v[c] = __float2bfloat16_rn(0.f);
+        v[0] = __float2bfloat16_rn(2.f * rho[p] - 1.f);
+        v[1] = __float2bfloat16_rn(W > 1 ? -1.f + 2.f * x / (W - 1) : 0.f);
+        v[2] = __float2bfloat16_rn(H > 1 ? -1.f + 2.f * y / (H - 1) : 0.f);
+        v[3] = __float2bfloat16_rn(1.f);
+        uint4 *o = reinterpret_cast<uint4 *>(x0 + (long long)p * 16);
+        o[0] = reinterpret_cast<const uint4 *>(v)[0];
+        o[1] = reinterpret_cast<const uint4 *>(v)[1];
     }
 }
 
 // Linear head on the flattened last feature map: out[n, j] = bh[j] + sum_f wh[j, f] a[n, f], f = p * 64 + c
-// (the positions stay distinct: the scene is not translation invariant). One block per sample.
+// (the positions stay distinct: the scene is not translation invariant). One block per sample, one warp per
+// output at a time, warp-shuffle reductions.
 __global__ void k_head_fwd(const bf16 *__restrict__ a, const float *__restrict__ wh, const float *__restrict__ bh,
                            float *__restrict__ out, int F, int K) {
-    __shared__ float red[256];
-    const int n = blockIdx.x;
-    for (int j = 0; j < K; ++j) {
+    const int n = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    const bf16 *an = a + (long long)n * F;
+    for (int j = warp; j < K; j += warps) {
+        const float *w = wh + (long long)j * F;
         float s = 0.f;
-        for (int f = threadIdx.x; f < F; f += blockDim.x) s += wh[(long long)j * F + f] * __bfloat162float(a[(long long)n * F + f]);
-        red[threadIdx.x] = s;
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) out[n * K + j] = bh[j] + red[0];
-        __syncthreads();
+        for (int f = lane; f < F; f += 32) s += w[f] * __bfloat162float(an[f]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) out[n * K + j] = bh[j] + s;
     }
 }
 
@@ -444,11 +442,21 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// Shared-memory bytes of one tcgen05 conv CTA: two A stages (128 x K), two B stages (N x K), barriers, slot.
-__host__ __device__ constexpr int tc_smem(int K, int N) { return 2 * (K * 128 * 2) + 2 * (K * N * 2) + 64; }
+// Shared-memory bytes of one tcgen05 conv CTA: three A stages (128 x K), three B stages (N x K), barriers, slot.
+constexpr int kStages = 3;
+__host__ __device__ constexpr int tc_smem(int K, int N) { return kStages * (K * 128 * 2) + kStages * (K * N * 2) + 64; }
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sh_addr(dst)), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // MODE 0 forward (K = CI input channels per tap, N = 64 output channels);
 // MODE 1 backward data (K = 64 output channels per tap, N = CI input channels).
+// The gathers of tap t+2 (cp.async, zero-filled outside the image) are in flight while the tensor cores
+// work on tap t; a stage is refilled once the commit of the MMAs that read it has arrived.
 template <int MODE, int CI>
 __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, const bf16 *__restrict__ wsrc,
                                                 const float *__restrict__ bias, const bf16 *__restrict__ zprev, bf16 *__restrict__ out0,
@@ -460,9 +468,9 @@ __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, c
     constexpr int COLS = NC < 32 ? 32 : NC;
     constexpr uint32_t IDESC = umma_idesc(128, NC);
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char *As = smem, *Bs = smem + 2 * A_BYTES;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(Bs + 2 * B_BYTES);
-    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 2);
+    unsigned char *As = smem, *Bs = smem + kStages * A_BYTES;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Bs + kStages * B_BYTES);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + kStages);
     const int tid = threadIdx.x, warp = tid >> 5;
     // Output rows: MODE 0 output pixels (n, oy, ox); MODE 1 input pixels (n, y, x).
     const int RH = MODE == 0 ? Ho : H, RW = MODE == 0 ? Wo : W;
@@ -474,21 +482,18 @@ __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, c
     const int ry = rem / RW, rx = rem % RW;
     if (warp == 0) tmem_alloc<COLS>(slot);
     if (tid == 0) {
-        bar_init(&bar[0]);
-        bar_init(&bar[1]);
+        for (int s = 0; s < kStages; ++s) bar_init(&bar[s]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *slot;
-    bool ok = true;
-    int issued = 0;                                      // taps whose MMAs were committed
-    for (int tap = 0; tap < 9; ++tap) {
-        const int s = tap & 1, ky = tap / 3, kx = tap % 3;
-        if (tap >= 2 && !bar_wait(&bar[s], ((tap >> 1) - 1) & 1)) ok = false;
-        if (__syncthreads_or(!ok)) break;
-        // A: this thread's row, K channels of the tap's neighbour (zero outside or not on the stride grid).
+
+    // Gathers of one tap into its stage: this thread's row (K channels of the tap's neighbour, zero outside
+    // the image or off the stride grid) and its share of the tap's weights ([K chunk][column][16 bytes]).
+    auto issue = [&](int tap) {
+        const int s = tap % kStages, ky = tap / 3, kx = tap % 3;
         const bf16 *a = nullptr;
         if (live) {
             if (MODE == 0) {
@@ -502,19 +507,35 @@ __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, c
         }
         unsigned char *as = As + s * A_BYTES;
 #pragma unroll
-        for (int kc = 0; kc < KC; ++kc)
-            *reinterpret_cast<uint4 *>(as + (kc * 128 + tid) * 16) = a ? *reinterpret_cast<const uint4 *>(a + kc * 8) : make_uint4(0, 0, 0, 0);
-        // B: the tap's weights, [K chunk][column][16 bytes]; MODE 0 w[tap][co][ci], MODE 1 w[tap][ci][co].
+        for (int kc = 0; kc < KC; ++kc) cp_async16(as + (kc * 128 + tid) * 16, a ? a + kc * 8 : src, a ? 16 : 0);
         unsigned char *bs = Bs + s * B_BYTES;
         for (int e = tid; e < NC * KC; e += 128) {
             const int col = e / KC, kc = e % KC;
-            *reinterpret_cast<uint4 *>(bs + (kc * NC + col) * 16) =
-                *reinterpret_cast<const uint4 *>(wsrc + ((long long)tap * NC + col) * K + kc * 8);
+            cp_async16(bs + (kc * NC + col) * 16, wsrc + ((long long)tap * NC + col) * K + kc * 8, 16);
         }
+        cp_async_commit();
+    };
+
+    bool ok = true;
+    int issued = 0;                                      // taps whose MMAs were committed
+    issue(0);
+    issue(1);
+    for (int tap = 0; tap < 9; ++tap) {
+        const int s = tap % kStages;
+        if (tap + 2 < 9) {
+            // Stage (tap + 2) % 3 was last read by the MMAs of tap - 1.
+            if (tap >= 1 && !bar_wait(&bar[(tap - 1) % kStages], ((tap - 1) / kStages) & 1)) ok = false;
+            if (__syncthreads_or(!ok)) break;
+            issue(tap + 2);
+        } else {
+            cp_async_commit();                           // empty group: keeps "tap's group is 2 groups back"
+        }
+        cp_async_wait<2>();
         proxy_fence();
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
+            const unsigned char *as = As + s * A_BYTES, *bs = Bs + s * B_BYTES;
 #pragma unroll
             for (int kk = 0; kk < K / 16; ++kk) {
                 const uint64_t ad = umma_desc(sh_addr(as) + kk * 2 * (128 * 16), 128 * 16, 128);
@@ -525,8 +546,9 @@ __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, c
         }
         issued = tap + 1;
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     // Wait for the last committed tap (its commit covers every earlier MMA of this thread).
-    if (issued > 0 && !bar_wait(&bar[(issued - 1) & 1], ((issued - 1) >> 1) & 1)) ok = false;
+    if (issued > 0 && !bar_wait(&bar[(issued - 1) % kStages], ((issued - 1) / kStages) & 1)) ok = false;
     tc_fence_after();
     if (__syncthreads_or(!ok) || issued < 9) {
         if (tid == 0) atomicExch(&g_sg_status, 1);
@@ -620,7 +642,8 @@ int tfd_sg_status(int32_t *status) {
 
 int tfd_sg_pack_input(const float *rho, int32_t n, int32_t h, int32_t w, void *x0, void *stream) {
     if (!rho || !x0 || n < 1 || h < 1 || w < 1) return bad("tfd_sg_pack_input: bad arguments");
-    k_pack_input<<<blocks_for((long long)n * h * w, 256), 256, 0, (cudaStream_t)stream>>>(rho, (bf16 *)x0, n, h, w);
+    if ((long long)n * h * w >= (1LL << 31)) return bad("tfd_sg_pack_input: more than 2^31 pixels");
+    k_pack_input<<<blocks_for((long long)n * h * w, 256), 256, 0, (cudaStream_t)stream>>>(rho, (bf16 *)x0, n * h * w, h, w);
     return check_launch("tfd_sg_pack_input");
 }
 
