@@ -43,9 +43,11 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = 'Gcell-updates/s'
 C0 = 299792458.0
-# DRAM bytes per cell-update of the step kernel measured by ncu on this workload
-# (dram__bytes_read.sum + dram__bytes_write.sum per launch / cells); None until captured.
-MEASURED_TRAFFIC_PER_CELL = {}
+# DRAM bytes per cell-update of the step kernel(s) measured by ncu on the workload itself
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch / cells; profiles/ has the commands):
+# 512x512x256: 2.55 + 1.82 GB per k_step_march launch; batch64: 493.4 MB (k_step2d_interior) + 118.5 MB
+# (k_step2d_general) per step at the tuned launch shape.
+MEASURED_TRAFFIC_PER_CELL = {('roofline', 'march'): 4.37e9 / 67108864, ('batch64', 'tile2d'): 611.9e6 / 20187264}
 
 
 def baseline_face(layers):
@@ -452,7 +454,8 @@ def run_ours_batch(args, world, rank, local):
     peak, peak_kind = measured_peaks()
     achieved = bytes_step * args.steps / elapsed / 1e9
     roofline = dict(bound='hbm', achieved=achieved, peak=peak, unit='GB/s', frac=achieved / peak,
-                    traffic=MEASURED_TRAFFIC_PER_CELL.get(('batch64', 'tile2d')), peak_source=peak_kind,
+                    traffic=(MEASURED_TRAFFIC_PER_CELL[('batch64', 'tile2d')] * cells
+                             if ('batch64', 'tile2d') in MEASURED_TRAFFIC_PER_CELL else None), peak_source=peak_kind,
                     algorithmic_bytes_per_step=bytes_step, kernel='k_step2d_tm',
                     note='achieved counts the whole step (batched tile launch + batched observation launch)')
     # ---- end to end: the public batch call over the configured 3000 steps ------------------------------
