@@ -35,11 +35,11 @@ def native(plan, kernel):
 
 
 def skip_unmarchable(plan_or_project, kernel):
-    """The marching kernel tiles 3D grids without periodic x/y faces, the 2D tile kernel 2D TMz grids without
+    """The marching kernel tiles 3D grids (periodic x/y seams included), the 2D tile kernel 2D TMz grids without
     periodic x/y faces; other scenes run the gather kernel."""
     region = getattr(plan_or_project, 'region', None) or plan_or_project.project.region
     periodic_xy = any(region.boundaries.pair(a)[0].kind == 'periodic' for a in (0, 1))
-    if kernel == 'march' and (region.dimension == '2d' or periodic_xy):
+    if kernel == 'march' and region.dimension == '2d':
         pytest.skip('scene runs the gather kernel')
     if kernel == 'tile2d':
         plan = plan_or_project if hasattr(plan_or_project, 'psi_shapes') else plan_grid(plan_or_project)
@@ -206,6 +206,47 @@ def test_interior_and_boundary_tiles_match_oracle(kernel, precision):
     np.testing.assert_array_equal(H, oracle.H)
     for got, want in zip(g.get_psi(), oracle.memory_states):
         np.testing.assert_array_equal(got, want)
+
+
+def seam_project(size, precision, sampling, steps=14):
+    """Periodic x/y with z-CPML (the scene the reference's one-pass marching kernel admits), ragged tile
+    counts, and sources on the seam cells (first column / row), which halo lanes recompute."""
+    from torchfdtd_b200.models import BoundaryFace, Source, Structure
+    region = Region(dimension='3d', size=size, mesh=.05, pml_cells=5, steps=steps, precision=precision,
+                    material_sampling=sampling, backend='cuda')
+    for name in ('x_min', 'x_max', 'y_min', 'y_max'):
+        setattr(region.boundaries, name, BoundaryFace(kind='periodic'))
+    hx, hy = size[0] / 2, size[1] / 2
+    return Project(region=region, structures=[Structure(kind='sphere', radius=.3, material='Si (constant n)')],
+                   sources=[Source(center=(-hx + .025, .05, 0), component='Ey', pulse_cycles=1, wavelength=1.0),
+                            Source(center=(.1, -hy + .025, .05), component='Ex', pulse_cycles=1, wavelength=1.0),
+                            Source(center=(-hx + .025, -hy + .025, -.05), component='Ez', pulse_cycles=1, wavelength=1.0),
+                            Source(center=(.2, .1, 0), component='Hz', pulse_cycles=1, wavelength=1.0, amplitude=.2)])
+
+
+@pytest.mark.parametrize('kernel', ['gather', 'march'])
+@pytest.mark.parametrize('size,precision,sampling', [((3.3, 2.5, 1.2), 'float32', 'cell'), ((3.3, 2.5, 1.2), 'float64', 'cell'),
+                                                     ((1.0, .8, 1.0), 'float32', 'yee'), ((1.6, .8, .9), 'float64', 'yee')])
+def test_periodic_xy_seams_match_oracle(kernel, size, precision, sampling):
+    """Seam tiles of the marching kernel patch the wrapped neighbours into their stages; narrow grids (one or
+    two tiles per axis) put both seams in one tile."""
+    project = seam_project(size, precision, sampling)
+    plan = plan_grid(project)
+    rng = np.random.default_rng(13)
+    oracle = YeeOracle(plan)
+    oracle.E[:] = rng.normal(size=oracle.E.shape).astype(plan.dtype) * .01
+    oracle.H[:] = rng.normal(size=oracle.H.shape).astype(plan.dtype) * .01
+    g = native(plan, kernel)
+    assert g.kernel == kernel
+    g.set_fields(oracle.E, oracle.H)
+    oracle.run()
+    g.step(plan.steps)
+    E, H = g.get_fields()
+    np.testing.assert_array_equal(E, oracle.E)
+    np.testing.assert_array_equal(H, oracle.H)
+    for got, want in zip(g.get_psi(), oracle.memory_states):
+        np.testing.assert_array_equal(got, want)
+    assert g.device_status() == 0
 
 
 @pytest.mark.parametrize('kernel', KERNELS)

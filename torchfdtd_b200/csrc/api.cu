@@ -605,8 +605,12 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 template <typename T>
 bool march_supported(const tfd_plan *p) {
     const Grid<T> &g = const_cast<tfd_plan *>(p)->grid<T>();
-    return g.n[2] > 1 && !g.periodic[0] && !g.periodic[1] && g.active == 0x3F;
+    return g.n[2] > 1 && g.active == 0x3F;
 }
+
+// Launch variant (D * 10 + MINB) that the periodic-seam kernel (MODE 2) is built for.
+template <typename T>
+constexpr int periodic_march_variant() { return sizeof(T) == 4 ? 14 : 22; }
 
 template <typename T, int SAMPLES, int D, int MINB>
 int setup_march_s(tfd_plan *p, bool split_interior, int lz_fixed) {
@@ -615,6 +619,11 @@ int setup_march_s(tfd_plan *p, bool split_interior, int lz_fixed) {
     MarchArgs<T> &a = p->march<T>();
     std::memset(&a, 0, sizeof(a));
     a.g = g;
+    const bool seams = g.periodic[0] || g.periodic[1];
+    for (int ax = 0; ax < 2; ++ax)
+        for (int q = 0; q < p->desc.n_segments; ++q)
+            if (g.periodic[ax] && p->seg_a[q] == ax)
+                return fail(TFD_ERR_INVALID, "a periodic axis carries a CPML slab");
     for (int ax = 0; ax < 3; ++ax) a.psi_parity[ax] = (int)((p->L.psi_len[0][ax] + 63) / 64 * 64);
     if (g.count >= (1LL << 31)) return fail(TFD_ERR_UNSUPPORTED, "component arrays above 2^31 elements need the gather kernel");
     for (int f = 0; f < 2; ++f)
@@ -657,6 +666,9 @@ int setup_march_s(tfd_plan *p, bool split_interior, int lz_fixed) {
     p->march_smem = S::SMEM;
     TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
     TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
+    if constexpr (D * 10 + MINB == periodic_march_variant<T>())
+        TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
+    const int edge_mode = seams ? 2 : 0;
     int device = 0, sms = 148, per_sm = 1;
     TFD_CUDA(cudaGetDevice(&device));
     TFD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -713,14 +725,14 @@ int setup_march_s(tfd_plan *p, bool split_interior, int lz_fixed) {
         p->march_launches.push_back({1, dim3(ix1 - ix0, iy1 - iy0, chunks_of(lzi)), ix0, iy0, lzi});
         auto strip = [&](int sx, int sy, int ox, int oy) {
             const int lzs = choose_lz((long long)sx * sy, strip_share * sx * sy / std::max(1LL, all - inner));
-            p->march_launches.push_back({0, dim3(sx, sy, chunks_of(lzs)), ox, oy, lzs});
+            p->march_launches.push_back({edge_mode, dim3(sx, sy, chunks_of(lzs)), ox, oy, lzs});
         };
         if (ix0 > 0) strip(ix0, ty, 0, 0);
         if (ix1 < tx) strip(tx - ix1, ty, ix1, 0);
         if (iy0 > 0) strip(ix1 - ix0, iy0, ix0, 0);
         if (iy1 < ty) strip(ix1 - ix0, ty - iy1, ix0, iy1);
     } else {
-        p->march_launches.push_back({0, dim3(tx, ty, chunks_of(lz_all)), 0, 0, lz_all});
+        p->march_launches.push_back({edge_mode, dim3(tx, ty, chunks_of(lz_all)), 0, 0, lz_all});
     }
     if (p->aux.empty() && p->march_launches.size() > 1) {
         TFD_CUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
@@ -740,6 +752,7 @@ int setup_march_s(tfd_plan *p, bool split_interior, int lz_fixed) {
 // Launch variant of the marching kernel, as decimal digits: lz * 1000 + split * 100 + D * 10 + MINB.
 // D / MINB: prefetch depth and CTAs per SM, one of 14 (FP32 default), 23, 32, 22 (FP64: 22 only);
 // split 1: interior tiles as their own launch; lz: z-planes per CTA chunk (0: sized to whole waves).
+// Grids with periodic x/y faces run D / MINB = 14 (FP32) or 22 (FP64) whatever the variant asks.
 // 0 selects the default (TFD_MARCH_VARIANT in the environment overrides the default, for sweeps).
 template <typename T>
 int setup_march(tfd_plan *p) {
@@ -752,7 +765,8 @@ int setup_march(tfd_plan *p) {
         return fail(TFD_ERR_INVALID, "launch variant " + std::to_string(v) + " is not lz*1000 + split*100 + one of " +
                                          (sizeof(T) == 8 ? std::string("22 (FP64)") : std::string("14, 22, 23, 32")));
     const bool three = p->desc.material_samples == 3, sp = split == 1;
-    switch (dm) {
+    const Grid<T> &g = p->grid<T>();
+    switch ((g.periodic[0] || g.periodic[1]) ? periodic_march_variant<T>() : dm) {
         case 22: return three ? setup_march_s<T, 3, 2, 2>(p, sp, lz) : setup_march_s<T, 1, 2, 2>(p, sp, lz);
         case 32: return three ? setup_march_s<T, 3, 3, 2>(p, sp, lz) : setup_march_s<T, 1, 3, 2>(p, sp, lz);
         case 14: return three ? setup_march_s<T, 3, 1, 4>(p, sp, lz) : setup_march_s<T, 1, 1, 4>(p, sp, lz);
@@ -770,7 +784,10 @@ void launch_march(tfd_plan *p, cudaStream_t s) {
         if (k > 0) cudaStreamWaitEvent(st, p->fork, 0);
         if (l.mode == 1)
             k_step_march<T, SAMPLES, D, MINB, 1><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz);
-        else
+        else if (l.mode == 2) {
+            if constexpr (D * 10 + MINB == periodic_march_variant<T>())
+                k_step_march<T, SAMPLES, D, MINB, 2><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz);
+        } else
             k_step_march<T, SAMPLES, D, MINB, 0><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz);
         if (k > 0) cudaEventRecord(p->join[k - 1], st);
     }
@@ -1169,7 +1186,7 @@ int tfd_plan_create(const tfd_desc *desc, void *arena, size_t arena_bytes, void 
         const bool march_ok = desc->precision == 8 ? march_supported<double>(p) : march_supported<float>(p);
         const bool tile_ok = tile2d_capable(desc);
         if (desc->kernel == TFD_KERNEL_MARCH && !march_ok)
-            rc = fail(TFD_ERR_UNSUPPORTED, "the marching kernel needs a 3D grid without periodic x/y faces");
+            rc = fail(TFD_ERR_UNSUPPORTED, "the marching kernel needs a 3D grid");
         else if (desc->kernel == TFD_KERNEL_TILE2D && !tile_ok)
             rc = fail(TFD_ERR_UNSUPPORTED, "the 2D tile kernel needs a 2D TMz grid without periodic x/y faces");
         if (desc->kernel == TFD_KERNEL_GATHER) p->kernel = TFD_KERNEL_GATHER;

@@ -23,8 +23,12 @@
 // outside slabs); coefficients are read only on slab cells. Index arithmetic is 32-bit
 // (the plan refuses grids whose component arrays exceed 2^31 elements).
 //
-// Supported here: x/y faces PML or PEC (periodic x/y run the gather kernel), z faces
-// PML, PEC or periodic, 3D grids. Every mbarrier wait is bounded: on timeout the
+// Supported here: x/y faces PML, PEC or periodic, z faces PML, PEC or periodic, 3D grids.
+// Periodic x/y run the MODE 2 instantiation: after a stage lands, tiles at a periodic seam
+// overwrite the box cells that fall outside the domain (TMA fills them with zeros) with the
+// cells one period away, so the seam columns / rows difference the same two values as the
+// reference's periodic branch, and the +x / +y halo lane or row that lies one past the last
+// cell recomputes E of the first column / row. Every mbarrier wait is bounded: on timeout the
 // kernel records kStatusPipelineTimeout in the device status word and returns.
 #pragma once
 #include <cuda.h>
@@ -205,7 +209,9 @@ struct Rows { int x, y, z; int po[3], pn[3]; Coef<T> qx, qy, qz; };
 // FAST: the warp row meets no CPML slab, no domain face and no source, and plane z has a previous
 // plane; the same arithmetic without the checks.
 // PZ: the z-term's old CPML memory comes from pz[j] (prefetched by the caller) instead of a load.
-template <typename T, int SAMPLES, int D, int C, bool FAST = false, bool PZ = false>
+// WRAP: x / y are periodic where the grid says so: the first column / row differences against the
+// wrapped neighbour that the caller placed in the stage.
+template <typename T, int SAMPLES, int D, int C, bool FAST = false, bool PZ = false, bool WRAP = false>
 __device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, int x, int y, int z,
                                      bool zprev, bool own, const Rows<T> &rw, const T *pz = nullptr) {
     using S = MarchShape<T, SAMPLES, D>;
@@ -225,11 +231,11 @@ __device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm,
             d = h[s] - h[s - S::BXW];
         } else if (t.axis == 0) {
             const T diff = h[s] - h[s - 1];
-            d = x > 0 ? diff : T(0);
+            d = (x > 0 || (WRAP && g.periodic[0])) ? diff : T(0);
             if (rw.x >= 0) d = cpml_e32(g, rw.po[0], rw.pn[0], 0, t.j, rw.qx, rw.x, x, y, z, own, d);
         } else if (t.axis == 1) {
             const T diff = h[s] - h[s - S::BXW];
-            d = y > 0 ? diff : T(0);
+            d = (y > 0 || (WRAP && g.periodic[1])) ? diff : T(0);
             if (rw.y >= 0) d = cpml_e32(g, rw.po[1], rw.pn[1], 1, t.j, rw.qy, rw.y, x, y, z, own, d);
         } else {
             d = T(0);
@@ -258,11 +264,13 @@ __device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm,
 // the general kernel over the boundary strips), so only the z-CPML memories remain, and those are
 // loaded into registers at the top of each plane, ahead of the TMA wait. Tile (tx, ty) of a launch
 // is (blockIdx.x + tx_off, blockIdx.y + ty_off); lz planes per z chunk (blockIdx.z).
+// MODE 2 is MODE 0 with periodic x / y seams (the host launches it when the grid has them).
 template <typename T, int SAMPLES, int D, int MINB, int MODE>
 __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid_constant__ MarchArgs<T> args, int tx_off, int ty_off,
                                                                     int lz) {
     using S = MarchShape<T, SAMPLES, D>;
     constexpr bool INTERIOR = MODE == 1;
+    constexpr bool PXY = MODE == 2;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
     const Grid<T> &g = args.g;
@@ -333,21 +341,26 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     auto wait_e = [&](int i) -> bool { return mbar_wait(&bare[i % S::NE], (uint32_t)((i / S::NE) & 1)); };
 
     // Per-thread invariants: column, rows of this warp, CPML slab rows and coefficients.
+    // px / py: periodic seams (MODE 2 only). xc: the cell this lane computes E of (the lane one past
+    // the last column wraps to column 0).
+    const bool px = PXY && g.periodic[0] != 0, py = PXY && g.periodic[1] != 0;
     const int x = x0 + lane;
+    const int xc = (px && x == nx) ? 0 : x;
     const bool lane_own = lane < kMarchOwnX && x < nx;
-    const bool lane_in = x < nx;
-    const int rxE = TFD_SLAB_ROW(args, 0, 0, x), rxH = TFD_SLAB_ROW(args, 1, 0, x);
+    const bool lane_in = x < nx || (px && x == nx);
+    const int rxE = TFD_SLAB_ROW(args, 0, 0, xc), rxH = TFD_SLAB_ROW(args, 1, 0, x);
     int yrow[2], ryE[2], ryH[2];
     Coef<T> qyE[2], qyH[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         yrow[h] = y0 + warp + 8 * h;
-        ryE[h] = TFD_SLAB_ROW(args, 0, 1, yrow[h]);
+        const int yc = (py && yrow[h] == ny) ? 0 : yrow[h];
+        ryE[h] = TFD_SLAB_ROW(args, 0, 1, yc);
         ryH[h] = TFD_SLAB_ROW(args, 1, 1, yrow[h]);
-        qyE[h] = coef_at(g, 0, 1, yrow[h], ryE[h]);
+        qyE[h] = coef_at(g, 0, 1, yc, ryE[h]);
         qyH[h] = coef_at(g, 1, 1, yrow[h], ryH[h]);
     }
-    const Coef<T> qxE = coef_at(g, 0, 0, x, rxE), qxH = coef_at(g, 1, 0, x, rxH);
+    const Coef<T> qxE = coef_at(g, 0, 0, xc, rxE), qxH = coef_at(g, 1, 0, x, rxH);
     // Warp-uniform fast-path conditions of this tile (x, y) and of each warp row.
     const bool tile_in = x0 > 0 && x0 + kMarchLanes <= nx;            // all computed columns inside, x-1 exists
     const bool fast_x_e = INTERIOR || (tile_in && !TFD_SLAB_MEETS(args, 0, 0, x0, x0 + kMarchLanes));
@@ -360,15 +373,42 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     }
     // Source terms whose x/y box meets this tile (E: with the halo), tested once per CTA.
     unsigned tile_src_e = 0, tile_src_h = 0;
+    // A tile at a periodic seam also computes E of the wrapped first column / row: test every x / y.
+    const bool wrap_x = px && x0 + kMarchLanes > nx, wrap_y = py && y0 + kMarchRows > ny;
     for (int t = 0; t < g.n_src; ++t) {
         const SourceTerm &st = g.src[t];
-        const bool e_hit = st.lo[0] < x0 + kMarchLanes && x0 < st.hi[0] && st.lo[1] < y0 + kMarchRows && y0 < st.hi[1];
+        const bool e_hit = (wrap_x || (st.lo[0] < x0 + kMarchLanes && x0 < st.hi[0])) &&
+                           (wrap_y || (st.lo[1] < y0 + kMarchRows && y0 < st.hi[1]));
         const bool h_hit = st.lo[0] < x0 + kMarchOwnX && x0 < st.hi[0] && st.lo[1] < y0 + kMarchOwnY && y0 < st.hi[1];
         if (st.family == 0 && e_hit) tile_src_e |= 1u << t;
         if (st.family == 1 && h_hit) tile_src_h |= 1u << t;
     }
     // New-parity offset of the fields; old/new offsets of the E-family CPML memories.
     const size_t fn = par ? 0 : (size_t)g.count;
+    // Periodic seams: box cells outside the domain on a periodic axis take the cell one period away
+    // (old fields at parity par, inverse permittivity), written over the TMA zero fill once the
+    // stage has landed. Only tiles whose box crosses a seam do this.
+    const bool patch = wrap_x || wrap_y || (px && x0 == 0) || (py && y0 == 0);
+    // kind 0: H fields, 1: E fields, 2: inverse permittivity.
+    auto patch_box = [&](T *dst, int stride, int rows, int ry0, int z, int comps, int kind) {
+        const size_t zo = (size_t)z * g.plane;
+        for (int q = tid; q < S::BXW * rows; q += kMarchThreads) {
+            const int cx = bx + q % S::BXW, cy = ry0 + q / S::BXW;
+            const bool ox = cx < 0 || cx >= nx, oy = cy < 0 || cy >= ny;
+            if ((!ox && !oy) || (ox && !px) || (oy && !py)) continue;
+            const size_t gi = zo + (size_t)(((cy % ny) + ny) % ny) * g.pitch + (((cx % nx) + nx) % nx);
+            for (int c = 0; c < comps; ++c) {
+                const T *src = kind == 2 ? g.inv_eps[c] : (kind == 0 ? g.H[0][c] : g.E[0][c]) + (size_t)par * g.count;
+                dst[c * stride + q] = src[gi];
+            }
+        }
+    };
+    auto patch_h = [&](int i) { patch_box(sm + (i % S::NH) * HSLOT_E, HS, S::BYH, y0 - 1, wrap(z0 - 1 + i), 3, 0); };
+    auto patch_e = [&](int i) {
+        T *dst = sm + ERING_OFF + (i % S::NE) * ESLOT_E;
+        patch_box(dst, ES, S::BYE, y0, wrap(z0 + i), 3, 1);
+        patch_box(dst + 3 * ES, ES, S::BYE, y0, wrap(z0 + i), SAMPLES, 2);
+    };
     Rows<T> rw0;
     for (int a = 0; a < 3; ++a) {
         rw0.po[a] = par ? args.psi_parity[a] : 0;
@@ -411,6 +451,13 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
             if (tid == 0) atomicExch(g.status, kStatusPipelineTimeout);
             return;
         }
+        if (PXY && patch && compute_e) {
+            if (t == 0 && has_prev) patch_h(0);
+            patch_h(t + 1);
+            patch_e(t);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+        }
         const int kz = k >= nz ? k - nz : k;
         T *ecur = sm + EBUF_OFF + (k & 1) * 3 * S::EBUF;
         const T *eprv = sm + EBUF_OFF + ((k - 1) & 1) * 3 * S::EBUF;
@@ -419,15 +466,19 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
             const bool zprev = kz > 0 || zper;
             const int rzE = TFD_SLAB_ROW(args, 0, 2, kz);
             const Coef<T> qzE = coef_at(g, 0, 2, kz, rzE);
-            const unsigned smask = tile_src_e ? source_mask(g, 0, x0, x0 + kMarchLanes, y0, y0 + kMarchRows, kz, n) & tile_src_e : 0u;
+            const unsigned smask = tile_src_e ? source_mask(g, 0, wrap_x ? 0 : x0, wrap_x ? nx : x0 + kMarchLanes, wrap_y ? 0 : y0,
+                                                            wrap_y ? ny : y0 + kMarchRows, kz, n) & tile_src_e
+                                              : 0u;
             T *gE0 = g.E[0][0] + fn + (size_t)kz * g.plane, *gE1 = g.E[0][1] + fn + (size_t)kz * g.plane,
               *gE2 = g.E[0][2] + fn + (size_t)kz * g.plane;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int r = warp + 8 * h;
                 const int y = yrow[h];
-                if (!lane_in || y >= ny) continue;
-                const bool own = !halo_plane && lane_own && r < kMarchOwnY;
+                const bool row_wraps = py && y == ny;               // computes E of row 0
+                if (!lane_in || (y >= ny && !row_wraps)) continue;
+                const int yc = row_wraps ? 0 : y;
+                const bool own = !halo_plane && lane_own && r < kMarchOwnY && !row_wraps;
                 const int sh = (r + 1) * S::BXW + off + lane;
                 const int se = r * S::BXW + off + lane;
                 Rows<T> rw = rw0;
@@ -448,14 +499,14 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                     ey = march_e<T, SAMPLES, D, 1, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw, pzE[h]);
                     ez = march_e<T, SAMPLES, D, 2, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw, pzE[h]);
                 } else {
-                    ex = march_e<T, SAMPLES, D, 0>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
-                    ey = march_e<T, SAMPLES, D, 1>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
-                    ez = march_e<T, SAMPLES, D, 2>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
+                    ex = march_e<T, SAMPLES, D, 0, false, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw);
+                    ey = march_e<T, SAMPLES, D, 1, false, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw);
+                    ez = march_e<T, SAMPLES, D, 2, false, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw);
                 }
                 if (smask) {
-                    ex = inject_masked(g, smask, 0, 0, n, x, y, kz, ex);
-                    ey = inject_masked(g, smask, 0, 1, n, x, y, kz, ey);
-                    ez = inject_masked(g, smask, 0, 2, n, x, y, kz, ez);
+                    ex = inject_masked(g, smask, 0, 0, n, xc, yc, kz, ex);
+                    ey = inject_masked(g, smask, 0, 1, n, xc, yc, kz, ey);
+                    ez = inject_masked(g, smask, 0, 2, n, xc, yc, kz, ez);
                 }
                 const int e = r * kMarchLanes + lane;
                 ecur[e] = ex;
@@ -521,7 +572,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                         if (tm.axis == 0) {
                             if (INTERIOR) {
                                 d = ep[e + 1] - ep[e];
-                            } else if (x < nx - 1) {
+                            } else if (x < nx - 1 || px) {
                                 d = ep[e + 1] - ep[e];
                                 if (rxH >= 0) d = cpml_h32q(g, 0, tm.j, qxH, rxH, x, y, km, d);
                             } else if (g.pec_on[0]) {
@@ -530,7 +581,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                         } else if (tm.axis == 1) {
                             if (INTERIOR) {
                                 d = ep[e + kMarchLanes] - ep[e];
-                            } else if (y < ny - 1) {
+                            } else if (y < ny - 1 || py) {
                                 d = ep[e + kMarchLanes] - ep[e];
                                 if (ryH[h] >= 0) d = cpml_h32q(g, 1, tm.j, qyH[h], ryH[h], x, y, km, d);
                             } else if (g.pec_on[1]) {
