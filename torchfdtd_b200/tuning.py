@@ -88,7 +88,7 @@ def grid_candidates(plan):
         base = [22, 122]
     else:
         base = [14, 23, 32, 22, 114]
-    lz = [v for v in (16, 32, 64) if v < nz]
+    lz = [v for v in (4, 8, 16) if v < nz]            # planes per chunk around the default (about 12)
     return base + [z * 1000 + 14 for z in lz] if plan.dtype != np.float64 else base + [z * 1000 + 22 for z in lz]
 
 
