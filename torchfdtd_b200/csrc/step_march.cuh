@@ -258,6 +258,135 @@ __device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm,
     return ek[C * ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? C : 0)) * ES + se]) * acc;
 }
 
+// E_new of the three components of one cell on a row that is not on the fast path (general kernel).
+// Faces become selects (x / y / z > 0, or a periodic seam). CPML: the row meets a CPML slab; the old
+// memories of the cell's active slabs are loaded first, so their loads are in flight together, then
+// the terms run in the reference order (y-term, z-term of Ex; x, z of Ey; x, y of Ez) and the owner
+// stores the new memories. rw.x / rw.y / rw.z: slab rows (-1 outside); x, y: the cell's coordinates.
+template <typename T, int SAMPLES, int D, bool CPML, bool WRAP>
+__device__ __forceinline__ void march_e_row(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, int x, int y,
+                                            int z, bool zprev, bool own, const Rows<T> &rw, T &ex, T &ey, T &ez) {
+    using S = MarchShape<T, SAMPLES, D>;
+    constexpr int HS = S::BOXH_STRIDE / sizeof(T);
+    constexpr int ES = S::BOXE_STRIDE / sizeof(T);
+    const bool xin = x > 0 || (WRAP && g.periodic[0]);
+    const bool yin = y > 0 || (WRAP && g.periodic[1]);
+    const T *Hx = hk, *Hy = hk + HS, *Hz = hk + 2 * HS;
+    bool ax = false, ay = false, az = false;
+    int ix = 0, iy = 0, iz = 0;
+    T ox0 = T(0), ox1 = T(0), oy0 = T(0), oy1 = T(0), oz0 = T(0), oz1 = T(0);
+    if (CPML) {
+        const int ny = g.n[1], pitch = g.pitch;
+        ax = rw.x >= 0;
+        ay = rw.y >= 0;
+        az = zprev && rw.z >= 0;
+        ix = (z * ny + y) * g.rows[0][0] + rw.x;
+        iy = (z * g.rows[0][1] + rw.y) * pitch + x;
+        iz = (rw.z * ny + y) * pitch + x;
+        if (ax) { ox0 = g.psiE[0][0][0][rw.po[0] + ix]; ox1 = g.psiE[0][0][1][rw.po[0] + ix]; }
+        if (ay) { oy0 = g.psiE[0][1][0][rw.po[1] + iy]; oy1 = g.psiE[0][1][1][rw.po[1] + iy]; }
+        if (az) { oz0 = g.psiE[0][2][0][rw.po[2] + iz]; oz1 = g.psiE[0][2][1][rw.po[2] + iz]; }
+    }
+    auto mem = [&](int a, int j, int idx, T old, const Coef<T> &q, T d) -> T {
+        const T m = old * q.b + q.c * d;
+        if (own) g.psiE[0][a][j][rw.pn[a] + idx] = m;
+        return d * q.k + m;
+    };
+    T d, acc;
+    // Ex: (y, Hz, +, j0), (z, Hy, -, j0)
+    d = yin ? Hz[s] - Hz[s - S::BXW] : T(0);
+    if (CPML && ay) d = mem(1, 0, iy, oy0, rw.qy, d);
+    acc = T(0);
+    acc = acc + d;
+    d = zprev ? Hy[s] - hm[HS + s] : T(0);
+    if (CPML && az) d = mem(2, 0, iz, oz0, rw.qz, d);
+    acc = acc + (-d);
+    ex = ek[se] + (g.cn * ek[3 * ES + se]) * acc;
+    // Ey: (x, Hz, -, j0), (z, Hx, +, j1)
+    d = xin ? Hz[s] - Hz[s - 1] : T(0);
+    if (CPML && ax) d = mem(0, 0, ix, ox0, rw.qx, d);
+    acc = T(0);
+    acc = acc + (-d);
+    d = zprev ? Hx[s] - hm[s] : T(0);
+    if (CPML && az) d = mem(2, 1, iz, oz1, rw.qz, d);
+    acc = acc + d;
+    ey = ek[ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? 1 : 0)) * ES + se]) * acc;
+    // Ez: (x, Hy, +, j1), (y, Hx, -, j1)
+    d = xin ? Hy[s] - Hy[s - 1] : T(0);
+    if (CPML && ax) d = mem(0, 1, ix, ox1, rw.qx, d);
+    acc = T(0);
+    acc = acc + d;
+    d = yin ? Hx[s] - Hx[s - S::BXW] : T(0);
+    if (CPML && ay) d = mem(1, 1, iy, oy1, rw.qy, d);
+    acc = acc + (-d);
+    ez = ek[2 * ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? 2 : 0)) * ES + se]) * acc;
+}
+
+// H_new of the three components of one owned cell on a row that is not on the fast path. Upper faces
+// become selects: the difference to the +x / +y / +z neighbour, else the PEC ghost term, else 0.
+// CPML: as for E, with the H-family memories updated in place. ep: E_new of plane km (the cell's
+// plane, with the +x column and +y row), ec: E_new of plane km + 1; e: the cell's index in both.
+template <typename T, int SAMPLES, int D, bool CPML>
+__device__ __forceinline__ void march_h_row(const Grid<T> &g, const T *ep, const T *ec, const T *hs, int sh, int e, int x, int y,
+                                            int km, bool xn, bool yn, bool znext, int rx, int ry, int rz, const Coef<T> &qx,
+                                            const Coef<T> &qy, const Coef<T> &qz, T &hx, T &hy, T &hz) {
+    using S = MarchShape<T, SAMPLES, D>;
+    constexpr int HS = S::BOXH_STRIDE / sizeof(T);
+    constexpr int EB = S::EBUF;
+    bool ax = false, ay = false, az = false;
+    int ix = 0, iy = 0, iz = 0;
+    T ox0 = T(0), ox1 = T(0), oy0 = T(0), oy1 = T(0), oz0 = T(0), oz1 = T(0);
+    if (CPML) {
+        const int ny = g.n[1], pitch = g.pitch;
+        ax = xn && rx >= 0;
+        ay = yn && ry >= 0;
+        az = znext && rz >= 0;
+        ix = (km * ny + y) * g.rows[1][0] + rx;
+        iy = (km * g.rows[1][1] + ry) * pitch + x;
+        iz = (rz * ny + y) * pitch + x;
+        if (ax) { ox0 = g.psiH[0][0][ix]; ox1 = g.psiH[0][1][ix]; }
+        if (ay) { oy0 = g.psiH[1][0][iy]; oy1 = g.psiH[1][1][iy]; }
+        if (az) { oz0 = g.psiH[2][0][iz]; oz1 = g.psiH[2][1][iz]; }
+    }
+    auto mem = [&](int a, int j, int idx, T old, const Coef<T> &q, T d) -> T {
+        const T m = old * q.b + q.c * d;
+        g.psiH[a][j][idx] = m;
+        return d * q.k + m;
+    };
+    auto dx = [&](const T *f) -> T { return xn ? f[e + 1] - f[e] : (g.pec_on[0] ? g.pec_neg[0] * f[e] : T(0)); };
+    auto dy = [&](const T *f) -> T { return yn ? f[e + kMarchLanes] - f[e] : (g.pec_on[1] ? g.pec_neg[1] * f[e] : T(0)); };
+    auto dz = [&](int c) -> T { return znext ? ec[c * EB + e] - ep[c * EB + e] : (g.pec_on[2] ? g.pec_neg[2] * ep[c * EB + e] : T(0)); };
+    const T *Ex = ep, *Ey = ep + EB, *Ez = ep + 2 * EB;
+    T d, acc;
+    // Hx: (y, Ez, +, j0), (z, Ey, -, j0)
+    d = dy(Ez);
+    if (CPML && ay) d = mem(1, 0, iy, oy0, qy, d);
+    acc = T(0);
+    acc = acc + d;
+    d = dz(1);
+    if (CPML && az) d = mem(2, 0, iz, oz0, qz, d);
+    acc = acc + (-d);
+    hx = hs[sh] - g.cn * acc;
+    // Hy: (x, Ez, -, j0), (z, Ex, +, j1)
+    d = dx(Ez);
+    if (CPML && ax) d = mem(0, 0, ix, ox0, qx, d);
+    acc = T(0);
+    acc = acc + (-d);
+    d = dz(0);
+    if (CPML && az) d = mem(2, 1, iz, oz1, qz, d);
+    acc = acc + d;
+    hy = hs[HS + sh] - g.cn * acc;
+    // Hz: (x, Ey, +, j1), (y, Ex, -, j1)
+    d = dx(Ey);
+    if (CPML && ax) d = mem(0, 1, ix, ox1, qx, d);
+    acc = T(0);
+    acc = acc + d;
+    d = dy(Ex);
+    if (CPML && ay) d = mem(1, 1, iy, oy1, qy, d);
+    acc = acc + (-d);
+    hz = hs[2 * HS + sh] - g.cn * acc;
+}
+
 // D planes of TMA prefetch; MINB CTAs per SM requested from the register allocator.
 // MODE 0 (general) runs any tile; MODE 1 (interior) runs tiles whose computed 32 x 16 cells lie
 // inside the domain and outside every x/y CPML slab (the host launches it over that tile range and
@@ -348,28 +477,45 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     const int xc = (px && x == nx) ? 0 : x;
     const bool lane_own = lane < kMarchOwnX && x < nx;
     const bool lane_in = x < nx || (px && x == nx);
-    const int rxE = TFD_SLAB_ROW(args, 0, 0, xc), rxH = TFD_SLAB_ROW(args, 1, 0, x);
-    int yrow[2], ryE[2], ryH[2];
-    Coef<T> qyE[2], qyH[2];
+    // Per-thread CPML state (slab rows, coefficients) is built on the rows that meet a slab, where it
+    // is used, and not kept across the plane loop: under the 64-register budget of 4 CTAs per SM it
+    // would crowd the fast path. yslab bit h: row h meets an E-family y slab; bit 2 + h: an H one.
+    int yrow[2];
+    unsigned yslab = 0;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         yrow[h] = y0 + warp + 8 * h;
         const int yc = (py && yrow[h] == ny) ? 0 : yrow[h];
-        ryE[h] = TFD_SLAB_ROW(args, 0, 1, yc);
-        ryH[h] = TFD_SLAB_ROW(args, 1, 1, yrow[h]);
-        qyE[h] = coef_at(g, 0, 1, yc, ryE[h]);
-        qyH[h] = coef_at(g, 1, 1, yrow[h], ryH[h]);
+        if (TFD_SLAB_ROW(args, 0, 1, yc) >= 0) yslab |= 1u << h;
+        if (TFD_SLAB_ROW(args, 1, 1, yrow[h]) >= 0) yslab |= 4u << h;
     }
-    const Coef<T> qxE = coef_at(g, 0, 0, xc, rxE), qxH = coef_at(g, 1, 0, x, rxH);
-    // Warp-uniform fast-path conditions of this tile (x, y) and of each warp row.
-    const bool tile_in = x0 > 0 && x0 + kMarchLanes <= nx;            // all computed columns inside, x-1 exists
-    const bool fast_x_e = INTERIOR || (tile_in && !TFD_SLAB_MEETS(args, 0, 0, x0, x0 + kMarchLanes));
-    const bool fast_x_h = INTERIOR || (x0 + kMarchLanes < nx && !TFD_SLAB_MEETS(args, 1, 0, x0, x0 + kMarchOwnX));
-    bool fast_y_e[2], fast_y_h[2];
+    auto e_rows = [&](int xx, int yy, int kz, int rz) {
+        Rows<T> rw;
+        rw.x = TFD_SLAB_ROW(args, 0, 0, xx);
+        rw.y = TFD_SLAB_ROW(args, 0, 1, yy);
+        rw.z = rz;
+        rw.qx = coef_at(g, 0, 0, xx, rw.x);
+        rw.qy = coef_at(g, 0, 1, yy, rw.y);
+        rw.qz = coef_at(g, 0, 2, kz, rz);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            rw.po[a] = par ? args.psi_parity[a] : 0;
+            rw.pn[a] = par ? 0 : args.psi_parity[a];
+        }
+        return rw;
+    };
+    // Warp-uniform path of each row: fast (plain differences: no face, CPML slab or source), edge (faces
+    // as selects) or CPML (the row meets a slab). Lanes past the last column skip the row, so the last
+    // tile column takes the fast E path; its H update has the x = nx-1 face unless x is periodic.
+    const bool slab_x_e = !INTERIOR && TFD_SLAB_MEETS(args, 0, 0, x0, x0 + kMarchLanes);
+    const bool slab_x_h = !INTERIOR && TFD_SLAB_MEETS(args, 1, 0, x0, x0 + kMarchOwnX);
+    const bool face_x_e = !INTERIOR && x0 == 0 && !px;
+    const bool face_x_h = !INTERIOR && x0 + kMarchLanes > nx && !px;
+    bool face_y_e[2], face_y_h[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-        fast_y_e[h] = INTERIOR || (yrow[h] > 0 && yrow[h] < ny && ryE[h] < 0);
-        fast_y_h[h] = INTERIOR || (yrow[h] < ny - 1 && ryH[h] < 0);
+        face_y_e[h] = !INTERIOR && yrow[h] == 0 && !py;
+        face_y_h[h] = !INTERIOR && yrow[h] >= ny - 1 && !py;
     }
     // Source terms whose x/y box meets this tile (E: with the halo), tested once per CTA.
     unsigned tile_src_e = 0, tile_src_h = 0;
@@ -409,11 +555,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
         patch_box(dst, ES, S::BYE, y0, wrap(z0 + i), 3, 1);
         patch_box(dst + 3 * ES, ES, S::BYE, y0, wrap(z0 + i), SAMPLES, 2);
     };
-    Rows<T> rw0;
-    for (int a = 0; a < 3; ++a) {
-        rw0.po[a] = par ? args.psi_parity[a] : 0;
-        rw0.pn[a] = par ? 0 : args.psi_parity[a];
-    }
+    const Rows<T> no_rows{};
 
     if (!wait_h(0)) {
         if (tid == 0) atomicExch(g.status, kStatusPipelineTimeout);
@@ -436,7 +578,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                     if (yrow[h] < ny)
 #pragma unroll
                         for (int j = 0; j < 2; ++j)
-                            pzE[h][j] = g.psiE[0][2][j][rw0.po[2] + psi_index32(2, x, yrow[h], kzp, rzE_pre, g.rows[0][2], ny, g.pitch)];
+                            pzE[h][j] = g.psiE[0][2][j][(par ? args.psi_parity[2] : 0) + psi_index32(2, x, yrow[h], kzp, rzE_pre, g.rows[0][2], ny, g.pitch)];
             }
             if (rzH_pre >= 0) {
 #pragma unroll
@@ -465,7 +607,6 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
             const T *hk = hstage(t + 1), *hm = hstage(t), *ek = estage(t);
             const bool zprev = kz > 0 || zper;
             const int rzE = TFD_SLAB_ROW(args, 0, 2, kz);
-            const Coef<T> qzE = coef_at(g, 0, 2, kz, rzE);
             const unsigned smask = tile_src_e ? source_mask(g, 0, wrap_x ? 0 : x0, wrap_x ? nx : x0 + kMarchLanes, wrap_y ? 0 : y0,
                                                             wrap_y ? ny : y0 + kMarchRows, kz, n) & tile_src_e
                                               : 0u;
@@ -481,27 +622,24 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                 const bool own = !halo_plane && lane_own && r < kMarchOwnY && !row_wraps;
                 const int sh = (r + 1) * S::BXW + off + lane;
                 const int se = r * S::BXW + off + lane;
-                Rows<T> rw = rw0;
-                rw.x = rxE;
-                rw.y = ryE[h];
-                rw.z = rzE;
-                rw.qx = qxE;
-                rw.qy = qyE[h];
-                rw.qz = qzE;
+                const Rows<T> &rw = no_rows;
                 T ex, ey, ez;
-                if (fast_x_e && fast_y_e[h] && zprev && rzE < 0 && !smask) {
+                const bool cpml_row = slab_x_e || ((yslab >> h) & 1u) || rzE >= 0;
+                if (!cpml_row && !face_x_e && !face_y_e[h] && zprev && !smask) {
                     ex = march_e<T, SAMPLES, D, 0, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
                     ey = march_e<T, SAMPLES, D, 1, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
                     ez = march_e<T, SAMPLES, D, 2, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
                 } else if (INTERIOR) {
                     // only the z-CPML memories and sources can apply here
-                    ex = march_e<T, SAMPLES, D, 0, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw, pzE[h]);
-                    ey = march_e<T, SAMPLES, D, 1, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw, pzE[h]);
-                    ez = march_e<T, SAMPLES, D, 2, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw, pzE[h]);
+                    const Rows<T> rz = e_rows(x, y, kz, rzE);
+                    ex = march_e<T, SAMPLES, D, 0, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rz, pzE[h]);
+                    ey = march_e<T, SAMPLES, D, 1, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rz, pzE[h]);
+                    ez = march_e<T, SAMPLES, D, 2, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rz, pzE[h]);
+                } else if (!cpml_row) {
+                    march_e_row<T, SAMPLES, D, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw, ex, ey, ez);
                 } else {
-                    ex = march_e<T, SAMPLES, D, 0, false, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw);
-                    ey = march_e<T, SAMPLES, D, 1, false, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw);
-                    ez = march_e<T, SAMPLES, D, 2, false, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw);
+                    const Rows<T> rc = e_rows(xc, yc, kz, rzE);
+                    march_e_row<T, SAMPLES, D, true, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rc, ex, ey, ez);
                 }
                 if (smask) {
                     ex = inject_masked(g, smask, 0, 0, n, xc, yc, kz, ex);
@@ -532,7 +670,6 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
             const T *hs = hstage(t);
             const bool znext = compute_e;
             const int rzH = TFD_SLAB_ROW(args, 1, 2, km);
-            const Coef<T> qzH = coef_at(g, 1, 2, km, rzH);
             const unsigned hmask = tile_src_h ? source_mask(g, 1, x0, x0 + kMarchOwnX, y0, y0 + kMarchOwnY, km, n) & tile_src_h : 0u;
             T *gH[3] = {g.H[0][0] + fn + (size_t)km * g.plane, g.H[0][1] + fn + (size_t)km * g.plane,
                         g.H[0][2] + fn + (size_t)km * g.plane};
@@ -544,7 +681,8 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                 const int sh = (r + 1) * S::BXW + off + lane;
                 const int e = r * kMarchLanes + lane;
                 const int i = y * g.pitch + x;
-                if (fast_x_h && fast_y_h[h] && znext && rzH < 0 && !hmask) {
+                const bool cpml_row = slab_x_h || ((yslab >> (2 + h)) & 1u) || rzH >= 0;
+                if (!cpml_row && !face_x_h && !face_y_h[h] && znext && !hmask) {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const Term t0 = term_of(c, 0), t1 = term_of(c, 1);
@@ -561,6 +699,27 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                     }
                     continue;
                 }
+                if constexpr (!INTERIOR) {
+                    const bool xn = x < nx - 1 || px, yn = y < ny - 1 || py;
+                    T hv[3];
+                    if (cpml_row) {
+                        const int rx = TFD_SLAB_ROW(args, 1, 0, x), ry = TFD_SLAB_ROW(args, 1, 1, y);
+                        march_h_row<T, SAMPLES, D, true>(g, eprv, ecur, hs, sh, e, x, y, km, xn, yn, znext, rx, ry, rzH,
+                                                         coef_at(g, 1, 0, x, rx), coef_at(g, 1, 1, y, ry), coef_at(g, 1, 2, km, rzH),
+                                                         hv[0], hv[1], hv[2]);
+                    } else {
+                        const Coef<T> q0{T(0), T(0), T(1)};
+                        march_h_row<T, SAMPLES, D, false>(g, eprv, ecur, hs, sh, e, x, y, km, xn, yn, znext, -1, -1, -1, q0, q0, q0,
+                                                          hv[0], hv[1], hv[2]);
+                    }
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        if (hmask) hv[c] = inject_masked(g, hmask, 1, c, n, x, y, km, hv[c]);
+                        gH[c][i] = hv[c];
+                    }
+                } else {
+                const int rxH = TFD_SLAB_ROW(args, 1, 0, x), ryHh = TFD_SLAB_ROW(args, 1, 1, y);
+                const Coef<T> qxH = coef_at(g, 1, 0, x, rxH), qyHh = coef_at(g, 1, 1, y, ryHh), qzH = coef_at(g, 1, 2, km, rzH);
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     T acc = T(0);
@@ -583,7 +742,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                                 d = ep[e + kMarchLanes] - ep[e];
                             } else if (y < ny - 1 || py) {
                                 d = ep[e + kMarchLanes] - ep[e];
-                                if (ryH[h] >= 0) d = cpml_h32q(g, 1, tm.j, qyH[h], ryH[h], x, y, km, d);
+                                if (ryHh >= 0) d = cpml_h32q(g, 1, tm.j, qyHh, ryHh, x, y, km, d);
                             } else if (g.pec_on[1]) {
                                 d = g.pec_neg[1] * ep[e];
                             }
@@ -608,6 +767,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                     T hv = hs[c * HS + sh] - g.cn * acc;
                     if (hmask) hv = inject_masked(g, hmask, 1, c, n, x, y, km, hv);
                     gH[c][i] = hv;
+                }
                 }
             }
         }
