@@ -1,13 +1,16 @@
 """Benchmark of the fused Yee/CPML engine: Gcell-updates/s and HBM-roofline fraction.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload roofline|roofline256|strip|tmz2d|batch64]
+                    [--workload roofline|roofline256|strip|periodic|tmz2d|batch64|adjoint3d|surrogate]
 
 Workload (default ``roofline``): 3D full-vector Yee + CPML, FP32, 512 x 512 x 256 cells
 at 0.05 um, CPML 12 cells per face (cubic grading, sigma_max = 0.8 (m+1)/(eta0 dx),
 kappa_max 1, alpha_max 0.05), seeded random piecewise-constant permittivity in [1, 12.1]
 on 8^3-cell blocks, Ey dipole at the centre, one Ey point trace. ``strip`` is the
-160 x 120 x 40 Si-strip scene with an x-normal DFT plane. All inputs are synthetic and
+160 x 120 x 40 Si-strip scene with an x-normal DFT plane. ``periodic`` is 512 x 512 x 128 with
+periodic x/y faces and CPML on z only, the scenes the reference's one-pass marching kernel admits;
+its line adds ``restated_reference``, that kernel restated in CUDA (baseline/fused_eh_marching.cu)
+and timed on the same device, scene and steps. All inputs are synthetic and
 seeded. A bench step is one FDTD time step over the whole grid (one fused step launch
 plus one observation launch).
 

@@ -41,7 +41,14 @@ constexpr int kMarchLanes = 32;     // computed columns: 31 owned + the +x halo
 constexpr int kMarchOwnX = 31;
 constexpr int kMarchRows = 16;      // computed E rows: 15 owned + the +y halo
 constexpr int kMarchOwnY = 15;
-constexpr int kMarchThreads = 256;
+// Warps per CTA; each thread computes kMarchRows / kMarchWarps rows of the tile per plane.
+#ifndef TFD_MARCH_WARPS
+#define TFD_MARCH_WARPS 8
+#endif
+constexpr int kMarchWarps = TFD_MARCH_WARPS;
+constexpr int kMarchThreads = 32 * kMarchWarps;
+constexpr int kMarchRowsPerThread = kMarchRows / kMarchWarps;
+static_assert(kMarchRows % kMarchWarps == 0, "tile rows must split evenly over the warps");
 
 template <typename T>
 struct MarchArgs {
@@ -479,15 +486,16 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     const bool lane_in = x < nx || (px && x == nx);
     // Per-thread CPML state (slab rows, coefficients) is built on the rows that meet a slab, where it
     // is used, and not kept across the plane loop: under the 64-register budget of 4 CTAs per SM it
-    // would crowd the fast path. yslab bit h: row h meets an E-family y slab; bit 2 + h: an H one.
-    int yrow[2];
+    // would crowd the fast path. yslab bit h: row h meets an E-family y slab; bit R + h (R rows per
+    // thread): an H-family one.
+    int yrow[kMarchRowsPerThread];
     unsigned yslab = 0;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        yrow[h] = y0 + warp + 8 * h;
+    for (int h = 0; h < kMarchRowsPerThread; ++h) {
+        yrow[h] = y0 + warp + kMarchWarps * h;
         const int yc = (py && yrow[h] == ny) ? 0 : yrow[h];
         if (TFD_SLAB_ROW(args, 0, 1, yc) >= 0) yslab |= 1u << h;
-        if (TFD_SLAB_ROW(args, 1, 1, yrow[h]) >= 0) yslab |= 4u << h;
+        if (TFD_SLAB_ROW(args, 1, 1, yrow[h]) >= 0) yslab |= 1u << (kMarchRowsPerThread + h);
     }
     auto e_rows = [&](int xx, int yy, int kz, int rz) {
         Rows<T> rw;
@@ -511,9 +519,9 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     const bool slab_x_h = !INTERIOR && TFD_SLAB_MEETS(args, 1, 0, x0, x0 + kMarchOwnX);
     const bool face_x_e = !INTERIOR && x0 == 0 && !px;
     const bool face_x_h = !INTERIOR && x0 + kMarchLanes > nx && !px;
-    bool face_y_e[2], face_y_h[2];
+    bool face_y_e[kMarchRowsPerThread], face_y_h[kMarchRowsPerThread];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < kMarchRowsPerThread; ++h) {
         face_y_e[h] = !INTERIOR && yrow[h] == 0 && !py;
         face_y_h[h] = !INTERIOR && yrow[h] >= ny - 1 && !py;
     }
@@ -566,7 +574,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
         const bool halo_plane = k == z1;
         const bool compute_e = !halo_plane || has_halo;
         // Interior tiles: issue this plane's z-slab CPML memory loads before waiting for the TMA stages.
-        T pzE[2][2], pzH[2][2];
+        T pzE[kMarchRowsPerThread][2], pzH[kMarchRowsPerThread][2];
         int rzE_pre = -1, rzH_pre = -1;
         if (INTERIOR) {
             const int kzp = k >= nz ? k - nz : k;
@@ -574,7 +582,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
             rzH_pre = k > z0 ? TFD_SLAB_ROW(args, 1, 2, k - 1) : -1;
             if (rzE_pre >= 0) {
 #pragma unroll
-                for (int h = 0; h < 2; ++h)
+                for (int h = 0; h < kMarchRowsPerThread; ++h)
                     if (yrow[h] < ny)
 #pragma unroll
                         for (int j = 0; j < 2; ++j)
@@ -582,8 +590,8 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
             }
             if (rzH_pre >= 0) {
 #pragma unroll
-                for (int h = 0; h < 2; ++h)
-                    if (yrow[h] < ny && warp + 8 * h < kMarchOwnY && lane_own)
+                for (int h = 0; h < kMarchRowsPerThread; ++h)
+                    if (yrow[h] < ny && warp + kMarchWarps * h < kMarchOwnY && lane_own)
 #pragma unroll
                         for (int j = 0; j < 2; ++j)
                             pzH[h][j] = g.psiH[2][j][psi_index32(2, x, yrow[h], k - 1, rzH_pre, g.rows[1][2], ny, g.pitch)];
@@ -613,8 +621,8 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
             T *gE0 = g.E[0][0] + fn + (size_t)kz * g.plane, *gE1 = g.E[0][1] + fn + (size_t)kz * g.plane,
               *gE2 = g.E[0][2] + fn + (size_t)kz * g.plane;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = warp + 8 * h;
+            for (int h = 0; h < kMarchRowsPerThread; ++h) {
+                const int r = warp + kMarchWarps * h;
                 const int y = yrow[h];
                 const bool row_wraps = py && y == ny;               // computes E of row 0
                 if (!lane_in || (y >= ny && !row_wraps)) continue;
@@ -674,14 +682,14 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
             T *gH[3] = {g.H[0][0] + fn + (size_t)km * g.plane, g.H[0][1] + fn + (size_t)km * g.plane,
                         g.H[0][2] + fn + (size_t)km * g.plane};
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = warp + 8 * h;
+            for (int h = 0; h < kMarchRowsPerThread; ++h) {
+                const int r = warp + kMarchWarps * h;
                 const int y = yrow[h];
                 if (!lane_own || r >= kMarchOwnY || y >= ny) continue;
                 const int sh = (r + 1) * S::BXW + off + lane;
                 const int e = r * kMarchLanes + lane;
                 const int i = y * g.pitch + x;
-                const bool cpml_row = slab_x_h || ((yslab >> (2 + h)) & 1u) || rzH >= 0;
+                const bool cpml_row = slab_x_h || ((yslab >> (kMarchRowsPerThread + h)) & 1u) || rzH >= 0;
                 if (!cpml_row && !face_x_h && !face_y_h[h] && znext && !hmask) {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
