@@ -14,11 +14,13 @@
 //
 // curl_f^T is a backward difference of the per-H-cell values D(k) (k = 0..n-2, plus the periodic wrap or
 // PEC edge at n-1) and curl_b^T a forward difference of per-E-cell values D(k) (k = 1..n-1, plus the
-// periodic edge at 0), so the adjoint step has the forward step's stencil shape: a thread computes
-// e_bar_new at its own cell, recomputes e_bar_new at its +x, +y, +z neighbours (from the old buffers, as
-// the forward gather kernel recomputes E), and then h_bar_new at its own cell. Adjoint fields and both
-// families' adjoint CPML memories are double-buffered by reverse-step parity; each memory is written
-// once, by the thread that owns its cell. The forward state comes from a restart snapshot (tfd_state_save)
+// periodic edge at 0), so the adjoint step has the forward step's stencil shape. It runs as two
+// launches, one thread per cell: k_adjoint_e writes e_bar_new (and accumulates the sensitivity),
+// k_adjoint_h reads e_bar_new of its own cell and its +x, +y, +z neighbours back and writes h_bar_new.
+// (A single launch that recomputes the neighbours' e_bar_new, as the forward gather kernel recomputes E,
+// ran about 4x slower: each h_bar term needs a neighbour's e_bar, which needs CPML-transposed D values
+// at two cells.) Adjoint fields and both families' adjoint CPML memories are double-buffered by
+// reverse-step parity; each memory is written once, by the thread that owns its cell. The forward state comes from a restart snapshot (tfd_state_save)
 // of s_n, so no forward buffer is disturbed.
 //
 // The material sensitivity is accumulated as S_c = sum_n e_bar_c * curl_b(H)_c per component; the host
@@ -147,8 +149,9 @@ __device__ __forceinline__ T ebar_any(const AdjArgs<T> &A, int q, int out, int x
     return out == 0 ? ebar_at<T, 0>(A, q, x, y, z, i) : out == 1 ? ebar_at<T, 1>(A, q, x, y, z, i) : ebar_at<T, 2>(A, q, x, y, z, i);
 }
 
-// h_bar_new of H component C at its own cell; e_own[] holds e_bar_new of the own cell.
-template <typename T, int C>
+// h_bar_new of H component C at its own cell; e_own[] holds e_bar_new of the own cell. STORED: the
+// neighbours' e_bar_new are read from the new buffer (written by k_adjoint_e) instead of recomputed.
+template <typename T, int C, bool STORED = false>
 __device__ __forceinline__ T hbar_value(const AdjArgs<T> &A, int q, int x, int y, int z, long long i, const T *e_own) {
     const Grid<T> &g = A.g;
     T contrib = T(0);
@@ -164,7 +167,7 @@ __device__ __forceinline__ T hbar_value(const AdjArgs<T> &A, int q, int x, int y
         if (c >= 1) contrib = contrib + d_e(A, q, t, x, y, z, i, e_own[t.out], true);          // src[c] += D(c)
         if (c + 1 <= n - 1) {                                                                   // src[c] -= D(c+1)
             const int xp = a == 0 ? x + 1 : x, yp = a == 1 ? y + 1 : y, zp = a == 2 ? z + 1 : z;
-            const T eb = ebar_any(A, q, t.out, xp, yp, zp, i + s);
+            const T eb = STORED ? A.eb[q ^ 1][t.out][i + s] : ebar_any(A, q, t.out, xp, yp, zp, i + s);
             contrib = contrib - d_e(A, q, t, xp, yp, zp, i + s, eb, false);
         }
         if (g.periodic[a]) {                             // edge D(0): src[0] += D, src[n-1] -= D
@@ -172,7 +175,7 @@ __device__ __forceinline__ T hbar_value(const AdjArgs<T> &A, int q, int x, int y
             if (c == n - 1) {
                 const int x0 = a == 0 ? 0 : x, y0 = a == 1 ? 0 : y, z0 = a == 2 ? 0 : z;
                 const long long i0 = i - (long long)(n - 1) * s;
-                const T eb = ebar_any(A, q, t.out, x0, y0, z0, i0);
+                const T eb = STORED ? A.eb[q ^ 1][t.out][i0] : ebar_any(A, q, t.out, x0, y0, z0, i0);
                 contrib = contrib - d_e(A, q, t, x0, y0, z0, i0, eb, false);
             }
         }
@@ -214,8 +217,35 @@ __device__ __forceinline__ T forward_curl(const AdjArgs<T> &A, const T *slot, in
 
 // ACTIVE: bitmask of advanced components (bit c: E_c, bit 3+c: H_c). Launch like the forward gather
 // kernel: blockIdx.x = row (z*ny + y), blockIdx.y = 128-cell chunk of the row. Reads parity q, writes q^1.
+// Part 1 of the reverse step: e_bar_new of the own cell, and S += e_bar_new * curl_b(H_n).
 template <typename T, int ACTIVE>
-__global__ void __launch_bounds__(128) k_adjoint_step(const __grid_constant__ AdjArgs<T> A, const T *__restrict__ slot, int q) {
+__global__ void __launch_bounds__(128) k_adjoint_e(const __grid_constant__ AdjArgs<T> A, const T *__restrict__ slot, int q) {
+    const Grid<T> &g = A.g;
+    const int x = blockIdx.y * blockDim.x + threadIdx.x;
+    const int y = blockIdx.x % g.n[1];
+    const int z = blockIdx.x / g.n[1];
+    if (x >= g.n[0]) return;
+    const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
+    if (ACTIVE & 1) {
+        const T e = ebar_value<T, 0>(A, q, x, y, z, i, true);
+        A.eb[q ^ 1][0][i] = e;
+        A.S[0][i] = A.S[0][i] + e * forward_curl<T, 0>(A, slot, x, y, z, i);
+    }
+    if (ACTIVE & 2) {
+        const T e = ebar_value<T, 1>(A, q, x, y, z, i, true);
+        A.eb[q ^ 1][1][i] = e;
+        A.S[1][i] = A.S[1][i] + e * forward_curl<T, 1>(A, slot, x, y, z, i);
+    }
+    if (ACTIVE & 4) {
+        const T e = ebar_value<T, 2>(A, q, x, y, z, i, true);
+        A.eb[q ^ 1][2][i] = e;
+        A.S[2][i] = A.S[2][i] + e * forward_curl<T, 2>(A, slot, x, y, z, i);
+    }
+}
+
+// Part 2: h_bar_new of the own cell from the e_bar_new that part 1 stored (own cell and +x/+y/+z).
+template <typename T, int ACTIVE>
+__global__ void __launch_bounds__(128) k_adjoint_h(const __grid_constant__ AdjArgs<T> A, int q) {
     const Grid<T> &g = A.g;
     const int x = blockIdx.y * blockDim.x + threadIdx.x;
     const int y = blockIdx.x % g.n[1];
@@ -223,15 +253,12 @@ __global__ void __launch_bounds__(128) k_adjoint_step(const __grid_constant__ Ad
     if (x >= g.n[0]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
     T e[3] = {T(0), T(0), T(0)};
-    if (ACTIVE & 1) e[0] = ebar_value<T, 0>(A, q, x, y, z, i, true);
-    if (ACTIVE & 2) e[1] = ebar_value<T, 1>(A, q, x, y, z, i, true);
-    if (ACTIVE & 4) e[2] = ebar_value<T, 2>(A, q, x, y, z, i, true);
-    if (ACTIVE & 1) { A.eb[q ^ 1][0][i] = e[0]; A.S[0][i] = A.S[0][i] + e[0] * forward_curl<T, 0>(A, slot, x, y, z, i); }
-    if (ACTIVE & 2) { A.eb[q ^ 1][1][i] = e[1]; A.S[1][i] = A.S[1][i] + e[1] * forward_curl<T, 1>(A, slot, x, y, z, i); }
-    if (ACTIVE & 4) { A.eb[q ^ 1][2][i] = e[2]; A.S[2][i] = A.S[2][i] + e[2] * forward_curl<T, 2>(A, slot, x, y, z, i); }
-    if (ACTIVE & 8) A.hb[q ^ 1][0][i] = hbar_value<T, 0>(A, q, x, y, z, i, e);
-    if (ACTIVE & 16) A.hb[q ^ 1][1][i] = hbar_value<T, 1>(A, q, x, y, z, i, e);
-    if (ACTIVE & 32) A.hb[q ^ 1][2][i] = hbar_value<T, 2>(A, q, x, y, z, i, e);
+    if (ACTIVE & 1) e[0] = A.eb[q ^ 1][0][i];
+    if (ACTIVE & 2) e[1] = A.eb[q ^ 1][1][i];
+    if (ACTIVE & 4) e[2] = A.eb[q ^ 1][2][i];
+    if (ACTIVE & 8) A.hb[q ^ 1][0][i] = hbar_value<T, 0, true>(A, q, x, y, z, i, e);
+    if (ACTIVE & 16) A.hb[q ^ 1][1][i] = hbar_value<T, 1, true>(A, q, x, y, z, i, e);
+    if (ACTIVE & 32) A.hb[q ^ 1][2][i] = hbar_value<T, 2, true>(A, q, x, y, z, i, e);
 }
 
 // Observation seeds of one step: bar[family][comp][offset] += seed[k] (observers are distinct cells).

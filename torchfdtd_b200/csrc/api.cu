@@ -1679,9 +1679,18 @@ int adjoint_step_t(tfd_adjoint *adj, const void *snapshot, const void *seeds, cu
     const dim3 grid((unsigned)((long long)g.n[1] * g.n[2]), (unsigned)((g.n[0] + 127) / 128));
     const T *slot = (const T *)snapshot;
     switch (p->desc.components) {
-        case kMaskTM: k_adjoint_step<T, kMaskTM><<<grid, 128, 0, s>>>(A, slot, adj->q); break;
-        case kMaskTE: k_adjoint_step<T, kMaskTE><<<grid, 128, 0, s>>>(A, slot, adj->q); break;
-        default: k_adjoint_step<T, kMaskAll><<<grid, 128, 0, s>>>(A, slot, adj->q); break;
+        case kMaskTM:
+            k_adjoint_e<T, kMaskTM><<<grid, 128, 0, s>>>(A, slot, adj->q);
+            k_adjoint_h<T, kMaskTM><<<grid, 128, 0, s>>>(A, adj->q);
+            break;
+        case kMaskTE:
+            k_adjoint_e<T, kMaskTE><<<grid, 128, 0, s>>>(A, slot, adj->q);
+            k_adjoint_h<T, kMaskTE><<<grid, 128, 0, s>>>(A, adj->q);
+            break;
+        default:
+            k_adjoint_e<T, kMaskAll><<<grid, 128, 0, s>>>(A, slot, adj->q);
+            k_adjoint_h<T, kMaskAll><<<grid, 128, 0, s>>>(A, adj->q);
+            break;
     }
     TFD_CUDA(cudaGetLastError());
     adj->q ^= 1;
