@@ -47,7 +47,14 @@ struct AdjArgs {
     T *eb[2][3], *hb[2][3];      // adjoint fields [parity][component]
     T *pEb[2][3][2], *pHb[2][3][2];   // adjoint CPML memories [parity][axis][term j]
     T *S[3];                     // material sensitivity per E component
+    int slab[2][3][4];           // per family and axis: lo0, hi0, lo1, hi1 of the two CPML slabs
 };
+
+// Slab row of coordinate c from the (lo, hi) bounds of a (family, axis), or -1: rows of the low slab first.
+// The bounds sit in the kernel parameters, so no dependent table load precedes the CPML work.
+__device__ __forceinline__ int adj_slab_row(const int *b, int c) {
+    return (c >= b[0] && c < b[1]) ? c - b[0] : (c >= b[2] && c < b[3]) ? (b[1] - b[0]) + (c - b[2]) : -1;
+}
 
 template <typename T>
 __device__ __forceinline__ int coord_of(int a, int x, int y, int z) { return a == 0 ? x : (a == 1 ? y : z); }
@@ -62,9 +69,8 @@ __device__ __forceinline__ T d_h(const AdjArgs<T> &A, int q, const RevTerm t, in
     const T dst = -g.cn * A.hb[q][t.out][k];
     T v = t.sign > 0 ? dst : -dst;
     if (c < g.n[a] - 1) {
-        const int *rm = g.row[1][a];
-        if (rm != nullptr && A.pHb[q][a][t.j] != nullptr) {
-            const int r = rm[c];
+        if (A.pHb[q][a][t.j] != nullptr) {
+            const int r = adj_slab_row(A.slab[1][a], c);
             if (r >= 0) {
                 const long long p = g.psi_index(a, x, y, z, r, g.rows[1][a]);
                 const T m = A.pHb[q][a][t.j][p] + v;
@@ -123,9 +129,8 @@ __device__ __forceinline__ T d_e(const AdjArgs<T> &A, int q, const RevTerm t, in
     const T dst = (g.cn * g.inv_eps[t.out][k]) * ebar_out;
     T v = t.sign > 0 ? dst : -dst;
     if (c >= 1) {
-        const int *rm = g.row[0][a];
-        if (rm != nullptr && A.pEb[q][a][t.j] != nullptr) {
-            const int r = rm[c];
+        if (A.pEb[q][a][t.j] != nullptr) {
+            const int r = adj_slab_row(A.slab[0][a], c);
             if (r >= 0) {
                 const long long p = g.psi_index(a, x, y, z, r, g.rows[0][a]);
                 const T m = A.pEb[q][a][t.j][p] + v;
@@ -198,9 +203,8 @@ __device__ __forceinline__ T forward_curl(const AdjArgs<T> &A, const T *slot, in
         T d = T(0);
         if (c > 0) {
             d = h[i] - h[i - g.stride(a)];
-            const int *rm = g.row[0][a];
-            if (rm != nullptr && A.sPsiE[a][t.j] >= 0) {
-                const int r = rm[c];
+            if (A.sPsiE[a][t.j] >= 0) {
+                const int r = adj_slab_row(A.slab[0][a], c);
                 if (r >= 0) {
                     const long long p = g.psi_index(a, x, y, z, r, g.rows[0][a]);
                     const T mem = slot[A.sPsiE[a][t.j] + p] * g.cb[0][a][c] + g.cc[0][a][c] * d;

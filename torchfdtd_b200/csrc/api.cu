@@ -602,6 +602,23 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
+// CPML slab bounds per (family, axis): segments sorted by lo, as lo0, hi0, lo1, hi1; empty slabs are [0, 0).
+int slab_bounds(const tfd_plan *p, int out[2][3][4]) {
+    for (int f = 0; f < 2; ++f)
+        for (int ax = 0; ax < 3; ++ax) {
+            int k = 0;
+            int b[4] = {0, 0, 0, 0};
+            std::vector<std::pair<int, int>> segs;
+            for (int q = 0; q < p->desc.n_segments; ++q)
+                if (p->seg_f[q] == f && p->seg_a[q] == ax) segs.push_back({p->seg_lo[q], p->seg_hi[q]});
+            std::sort(segs.begin(), segs.end());
+            if (segs.size() > 2) return fail(TFD_ERR_INVALID, "more than two CPML slabs on one axis");
+            for (auto &sg : segs) { b[2 * k] = sg.first; b[2 * k + 1] = sg.second; ++k; }
+            for (int q = 0; q < 4; ++q) out[f][ax][q] = b[q];
+        }
+    return TFD_OK;
+}
+
 template <typename T>
 bool march_supported(const tfd_plan *p) {
     const Grid<T> &g = const_cast<tfd_plan *>(p)->grid<T>();
@@ -630,19 +647,9 @@ int setup_march_s(tfd_plan *p, bool split_interior, int lz_fixed) {
     for (int ax = 0; ax < 3; ++ax) a.psi_parity[ax] = (int)((p->L.psi_len[0][ax] + 63) / 64 * 64);
     if (g.count >= (1LL << 31)) return fail(TFD_ERR_UNSUPPORTED, "component arrays above 2^31 elements need the gather kernel");
     for (int f = 0; f < 2; ++f)
-        for (int ax = 0; ax < 3; ++ax) {
+        for (int ax = 0; ax < 3; ++ax)
             if (p->L.psi_len[f][ax] >= (1LL << 31)) return fail(TFD_ERR_UNSUPPORTED, "CPML memory above 2^31 elements");
-            // slab bounds: segments of (family, axis) sorted by lo; empty slabs are [0, 0)
-            int k = 0;
-            int b[4] = {0, 0, 0, 0};
-            std::vector<std::pair<int, int>> segs;
-            for (int q = 0; q < p->desc.n_segments; ++q)
-                if (p->seg_f[q] == f && p->seg_a[q] == ax) segs.push_back({p->seg_lo[q], p->seg_hi[q]});
-            std::sort(segs.begin(), segs.end());
-            if (segs.size() > 2) return fail(TFD_ERR_INVALID, "more than two CPML slabs on one axis");
-            for (auto &sg : segs) { b[2 * k] = sg.first; b[2 * k + 1] = sg.second; ++k; }
-            for (int q = 0; q < 4; ++q) a.slab[f][ax][q] = b[q];
-        }
+    if (int rc = slab_bounds(p, a.slab)) return rc;
     auto encode = tensor_map_encoder();
     if (!encode) return fail(TFD_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable from the driver");
     const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
@@ -1661,6 +1668,7 @@ int adjoint_create_t(tfd_adjoint *adj, cudaStream_t s) {
     for (int c = 0; c < 3; ++c) { A.sE[c] = m.sE[c]; A.sH[c] = m.sH[c]; }
     for (int a = 0; a < 3; ++a)
         for (int j = 0; j < 2; ++j) A.sPsiE[a][j] = m.sPsiE[a][j];
+    if (int rc = slab_bounds(p, A.slab)) return rc;
     adj->used = adjoint_layout<T>(p, &A, adj->arena);
     TFD_CUDA(cudaMemsetAsync(adj->arena, 0, adj->used, s));
     adj->q = 0;
