@@ -387,8 +387,10 @@ def _plane(project, monitor, dtype):
 
 
 # ---- the plan ----------------------------------------------------------------------------------
-def plan_grid(project, polarization=None):
-    """Resolve a project into a ``GridPlan`` for the fused kernels (refusing unsupported features)."""
+def plan_grid(project, polarization=None, material=True):
+    """Resolve a project into a ``GridPlan`` for the fused kernels (refusing unsupported features).
+    ``material=False`` skips voxelization (``epsilon`` / ``inv_eps`` stay None) for callers that supply the
+    permittivity themselves."""
     check_supported(project)
     r = project.region
     dtype = np.float64 if r.precision == 'float64' else np.float32
@@ -397,10 +399,14 @@ def plan_grid(project, polarization=None):
     pec_upper = {a: float(r.reference_step / (r.mesh_nodes[a][-1] - r.mesh_nodes[a][-2]))
                  for a in range(3) if r.shape[a] > 1 and faces[a][1] in ('pec', 'antisymmetric')}
     segments = cpml_segments(r, courant)
-    eps, counts = voxelize(project, dtype)
-    inv_eps = (1 / eps).astype(dtype)
-    warnings = [f'{obj.name}: no cells intersect this object. Refine mesh or reposition it.'
-                for obj in project.structures if obj.enabled and counts.get(obj.id) == 0]
+    if material:
+        eps, counts = voxelize(project, dtype)
+        inv_eps = (1 / eps).astype(dtype)
+        warnings = [f'{obj.name}: no cells intersect this object. Refine mesh or reposition it.'
+                    for obj in project.structures if obj.enabled and counts.get(obj.id) == 0]
+    else:
+        eps = inv_eps = None
+        counts, warnings = {}, []
     sources = []
     times = np.arange(1, r.steps + 1) * r.time_step
     for raw in project.sources:

@@ -186,7 +186,10 @@ class Observer:
         eps = plan.epsilon
         sl = [slice(None)] * 3
         sl[self.axis] = self.plane_index
-        self.eps_plane = np.array(self.decimate((eps[..., component] if eps.ndim == 4 else eps)[tuple(sl)]))
+        plane = (eps[..., component] if eps.ndim == 4 else eps)[tuple(sl)]
+        if hasattr(plane, 'cpu'):                          # a permittivity tensor given to Simulation
+            plane = plane.detach().cpu().numpy()
+        self.eps_plane = np.array(self.decimate(np.asarray(plane, dtype=plan.dtype)))
         self.interval = max(r.snapshot_interval, math.ceil(r.steps / 100))
         self.frames, self.frame_steps = [], []
         self.diagnostic_seconds = 0.
@@ -236,13 +239,19 @@ class Observer:
     def result(self, completed, termination_reason, seconds, setup_seconds, **extra):
         """Read the final state back and package it as the reference's ``Result``."""
         import torch
+        from .native import download
         p, r, plan, grid = self.project, self.region, self.plan, self.grid
         status = grid.device_status()
         if status:
             raise RuntimeError(self._where(f'A fused kernel reported device status {status}.'))
-        e, h = grid.get_fields()
-        if not np.isfinite(e).all() or not np.isfinite(h).all():
+        # Finiteness and the peak are checked on the device; the fields then come back through a pinned
+        # staging ring (native.download).
+        e_dev, h_dev = grid.fields_device()
+        if not bool(torch.isfinite(e_dev).all()) or not bool(torch.isfinite(h_dev).all()):
             raise FloatingPointError(self._where('Non-finite fields detected.'))
+        field_peak = float(e_dev.abs().amax()) if e_dev.numel() else 0.0
+        e, h = download(e_dev), download(h_dev)
+        del e_dev, h_dev
         traces = grid.get_traces()[:completed]
         frequency_results = []
         for k, pp in enumerate(plan.planes):
@@ -264,7 +273,7 @@ class Observer:
                      mcells_per_second=cells * completed / max(seconds, 1e-9) / 1e6,
                      gcells_per_s=cells * completed / max(seconds, 1e-9) / 1e9,
                      hbm_bytes_per_step=algorithmic_bytes_per_step(plan), arena_bytes=grid.arena_bytes,
-                     field_peak=float(np.max(np.abs(e))), slice_index=self.plane_index,
+                     field_peak=field_peak, slice_index=self.plane_index,
                      slice_position=(0 if r.dimension == '2d' and self.axis == 2
                                      else (self.plane_index + .5) * r.mesh - r.actual_size[self.axis] / 2),
                      complex_fields=False, complex_display=r.complex_display, material_update='nondispersive',
@@ -317,6 +326,28 @@ class Simulation:
             plan.inv_eps = (1 / eps).astype(plan.dtype)
         return plan
 
+    def _run_plan(self):
+        """(plan, material) for ``run``. With ``epsilon`` the structures are not voxelized and the array is
+        uploaded once, checked and inverted on the device (IEEE division: the same values as the host's
+        1 / eps): ``plan.inv_eps`` is then that device tensor."""
+        if self.epsilon is None:
+            return self.plan, None
+        import torch
+        plan = plan_grid(self.project, material=False)
+        shape = tuple(np.shape(self.epsilon))
+        if shape not in (tuple(plan.shape), (*plan.shape, 3)):
+            raise ValueError(f'epsilon must have shape {tuple(plan.shape)} or {(*plan.shape, 3)}, not {shape}.')
+        dtype = torch.float64 if plan.dtype == np.float64 else torch.float32
+        if isinstance(self.epsilon, torch.Tensor):
+            eps = self.epsilon.detach().to(device='cuda', dtype=dtype).contiguous()
+        else:
+            eps = torch.from_numpy(np.ascontiguousarray(np.asarray(self.epsilon, dtype=plan.dtype))).to('cuda')
+        if not bool(torch.isfinite(eps).all()) or bool((eps < 1).any()):
+            raise ValueError('epsilon must be finite and at least 1.')
+        plan.epsilon = self.epsilon
+        plan.inv_eps = torch.reciprocal(eps)
+        return plan, plan.inv_eps
+
     def run(self, progress=None, cancel=None, cuda_graph=True, cuda_graph_steps=1, kernel='auto', launch=None):
         """``kernel``: 'auto' (the marching kernel for 3D, the tile kernel for 2D TMz, else gather) or a name.
         ``launch``: None (default launch shape), an explicit launch variant, or 'auto' to measure the
@@ -333,7 +364,7 @@ class Simulation:
         if not torch.cuda.is_available():
             raise RuntimeError('CUDA requested but unavailable. The fused B200 engine needs a CUDA GPU.')
         started = time.perf_counter()
-        plan = self.plan
+        plan, material = self._run_plan()
         variant, tuning = 0, None
         if launch == 'auto':
             if plan.dimension == '3d' and kernel in ('auto', 'march'):
@@ -345,7 +376,7 @@ class Simulation:
                     tuning = dict(skipped=str(exc))
         elif launch is not None:
             variant = int(launch)
-        grid = NativeGrid(plan, kernel=kernel, variant=variant)
+        grid = NativeGrid(plan, kernel=kernel, variant=variant, material=material)
         free, _ = torch.cuda.mem_get_info()
         observer = Observer(p, plan, grid)
         graphs = {}
