@@ -145,13 +145,16 @@ def _stream(stream=None):
 _STAGING = {}
 
 
-def download(tensor, chunk_bytes=32 << 20, depth=4):
-    """A contiguous device tensor as a host numpy array: device-to-host copies of chunk_bytes into a ring of
-    ``depth`` pinned staging buffers (allocated once per process and dtype), each drained into the pageable
-    result by a host thread while later chunks are in flight. Page-locking the whole result would cost more
-    than it saves on a first call (about 0.5 s per GB here); a plain pageable copy runs at about 5 GB/s."""
+def download(tensor, chunk_bytes=32 << 20, depth=4, direct_bytes=64 << 20):
+    """A contiguous device tensor as a host numpy array. Up to ``direct_bytes``: one plain copy. Larger:
+    device-to-host copies of chunk_bytes into a ring of ``depth`` pinned staging buffers (allocated once per
+    process and dtype), each drained into the pageable result by a host thread while later chunks are in
+    flight. Page-locking the whole result would cost more than it saves on a first call (about 0.5 s per GB
+    here); a plain pageable copy runs at about 5 GB/s."""
     import torch
     from concurrent.futures import ThreadPoolExecutor
+    if tensor.numel() * tensor.element_size() <= direct_bytes:
+        return tensor.detach().cpu().numpy()
     src = tensor.detach().reshape(-1)
     out = np.empty(tuple(tensor.shape), dtype=torch.empty(0, dtype=tensor.dtype).numpy().dtype)
     flat = out.reshape(-1)

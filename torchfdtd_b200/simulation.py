@@ -244,14 +244,21 @@ class Observer:
         status = grid.device_status()
         if status:
             raise RuntimeError(self._where(f'A fused kernel reported device status {status}.'))
-        # Finiteness and the peak are checked on the device; the fields then come back through a pinned
-        # staging ring (native.download).
-        e_dev, h_dev = grid.fields_device()
-        if not bool(torch.isfinite(e_dev).all()) or not bool(torch.isfinite(h_dev).all()):
-            raise FloatingPointError(self._where('Non-finite fields detected.'))
-        field_peak = float(e_dev.abs().amax()) if e_dev.numel() else 0.0
-        e, h = download(e_dev), download(h_dev)
-        del e_dev, h_dev
+        if math.prod(plan.shape) * 3 * np.dtype(plan.dtype).itemsize > LARGE_FIELD_BYTES:
+            # Large grids: finiteness and the peak are checked on the device, and the fields come back through
+            # a pinned staging ring (native.download). Small grids keep the host path, whose fixed costs are
+            # lower than the first use of the device reductions.
+            e_dev, h_dev = grid.fields_device()
+            if not bool(torch.isfinite(e_dev).all()) or not bool(torch.isfinite(h_dev).all()):
+                raise FloatingPointError(self._where('Non-finite fields detected.'))
+            field_peak = float(e_dev.abs().amax())
+            e, h = download(e_dev), download(h_dev)
+            del e_dev, h_dev
+        else:
+            e, h = grid.get_fields()
+            if not np.isfinite(e).all() or not np.isfinite(h).all():
+                raise FloatingPointError(self._where('Non-finite fields detected.'))
+            field_peak = float(np.max(np.abs(e)))
         traces = grid.get_traces()[:completed]
         frequency_results = []
         for k, pp in enumerate(plan.planes):
@@ -284,6 +291,11 @@ class Observer:
         stats.update(extra)
         return Result(p, stats, np.array(self.frames), np.array(self.frame_steps), self.eps_plane, traces,
                       np.arange(1, completed + 1) * r.time_step, e, h, frequency_results)
+
+
+# Field arrays above this size take the device-side checks and the staged download in Observer.result, and
+# a given permittivity above it is checked and inverted on the device.
+LARGE_FIELD_BYTES = 64 << 20
 
 
 def capture_graphs(step, widths):
@@ -330,7 +342,7 @@ class Simulation:
         """(plan, material) for ``run``. With ``epsilon`` the structures are not voxelized and the array is
         uploaded once, checked and inverted on the device (IEEE division: the same values as the host's
         1 / eps): ``plan.inv_eps`` is then that device tensor."""
-        if self.epsilon is None:
+        if self.epsilon is None or np.size(self.epsilon) * 4 <= LARGE_FIELD_BYTES:
             return self.plan, None
         import torch
         plan = plan_grid(self.project, material=False)
