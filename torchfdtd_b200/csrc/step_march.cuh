@@ -486,17 +486,10 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     const bool lane_in = x < nx || (px && x == nx);
     // Per-thread CPML state (slab rows, coefficients) is built on the rows that meet a slab, where it
     // is used, and not kept across the plane loop: under the 64-register budget of 4 CTAs per SM it
-    // would crowd the fast path. yslab bit h: row h meets an E-family y slab; bit R + h (R rows per
-    // thread): an H-family one.
+    // would crowd the fast path.
     int yrow[kMarchRowsPerThread];
-    unsigned yslab = 0;
 #pragma unroll
-    for (int h = 0; h < kMarchRowsPerThread; ++h) {
-        yrow[h] = y0 + warp + kMarchWarps * h;
-        const int yc = (py && yrow[h] == ny) ? 0 : yrow[h];
-        if (TFD_SLAB_ROW(args, 0, 1, yc) >= 0) yslab |= 1u << h;
-        if (TFD_SLAB_ROW(args, 1, 1, yrow[h]) >= 0) yslab |= 1u << (kMarchRowsPerThread + h);
-    }
+    for (int h = 0; h < kMarchRowsPerThread; ++h) yrow[h] = y0 + warp + kMarchWarps * h;
     auto e_rows = [&](int xx, int yy, int kz, int rz) {
         Rows<T> rw;
         rw.x = TFD_SLAB_ROW(args, 0, 0, xx);
@@ -515,15 +508,23 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     // Warp-uniform path of each row: fast (plain differences: no face, CPML slab or source), edge (faces
     // as selects) or CPML (the row meets a slab). Lanes past the last column skip the row, so the last
     // tile column takes the fast E path; its H update has the x = nx-1 face unless x is periodic.
-    const bool slab_x_e = !INTERIOR && TFD_SLAB_MEETS(args, 0, 0, x0, x0 + kMarchLanes);
-    const bool slab_x_h = !INTERIOR && TFD_SLAB_MEETS(args, 1, 0, x0, x0 + kMarchOwnX);
-    const bool face_x_e = !INTERIOR && x0 == 0 && !px;
-    const bool face_x_h = !INTERIOR && x0 + kMarchLanes > nx && !px;
-    bool face_y_e[kMarchRowsPerThread], face_y_h[kMarchRowsPerThread];
+    // The tile and row parts of that choice, packed in one register (R rows per thread): bit h, the E row
+    // meets an x or y slab; bit R + h, it has a domain face; bits 2R + h and 3R + h, the same for H.
+    constexpr int R = kMarchRowsPerThread;
+    unsigned rowbits = 0;
+    if (!INTERIOR) {
+        const bool slab_x_e = TFD_SLAB_MEETS(args, 0, 0, x0, x0 + kMarchLanes);
+        const bool slab_x_h = TFD_SLAB_MEETS(args, 1, 0, x0, x0 + kMarchOwnX);
+        const bool face_x_e = x0 == 0 && !px;
+        const bool face_x_h = x0 + kMarchLanes > nx && !px;
 #pragma unroll
-    for (int h = 0; h < kMarchRowsPerThread; ++h) {
-        face_y_e[h] = !INTERIOR && yrow[h] == 0 && !py;
-        face_y_h[h] = !INTERIOR && yrow[h] >= ny - 1 && !py;
+        for (int h = 0; h < R; ++h) {
+            const int yc = (py && yrow[h] == ny) ? 0 : yrow[h];
+            if (slab_x_e || TFD_SLAB_ROW(args, 0, 1, yc) >= 0) rowbits |= 1u << h;
+            if (face_x_e || (yrow[h] == 0 && !py)) rowbits |= 1u << (R + h);
+            if (slab_x_h || TFD_SLAB_ROW(args, 1, 1, yrow[h]) >= 0) rowbits |= 1u << (2 * R + h);
+            if (face_x_h || (yrow[h] >= ny - 1 && !py)) rowbits |= 1u << (3 * R + h);
+        }
     }
     // Source terms whose x/y box meets this tile (E: with the halo), tested once per CTA.
     unsigned tile_src_e = 0, tile_src_h = 0;
@@ -632,8 +633,8 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                 const int se = r * S::BXW + off + lane;
                 const Rows<T> &rw = no_rows;
                 T ex, ey, ez;
-                const bool cpml_row = slab_x_e || ((yslab >> h) & 1u) || rzE >= 0;
-                if (!cpml_row && !face_x_e && !face_y_e[h] && zprev && !smask) {
+                const bool cpml_row = ((rowbits >> h) & 1u) || rzE >= 0;
+                if (!cpml_row && !((rowbits >> (R + h)) & 1u) && zprev && !smask) {
                     ex = march_e<T, SAMPLES, D, 0, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
                     ey = march_e<T, SAMPLES, D, 1, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
                     ez = march_e<T, SAMPLES, D, 2, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
@@ -689,8 +690,8 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                 const int sh = (r + 1) * S::BXW + off + lane;
                 const int e = r * kMarchLanes + lane;
                 const int i = y * g.pitch + x;
-                const bool cpml_row = slab_x_h || ((yslab >> (kMarchRowsPerThread + h)) & 1u) || rzH >= 0;
-                if (!cpml_row && !face_x_h && !face_y_h[h] && znext && !hmask) {
+                const bool cpml_row = ((rowbits >> (2 * R + h)) & 1u) || rzH >= 0;
+                if (!cpml_row && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask) {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const Term t0 = term_of(c, 0), t1 = term_of(c, 1);
