@@ -179,11 +179,12 @@ def test_z_faces_periodic_and_pec_match_oracle(kernel, zfaces):
         np.testing.assert_array_equal(got, want)
 
 
-@pytest.mark.parametrize('kernel', KERNELS)
+@pytest.mark.parametrize('kernel,variant', [(k, 0) for k in KERNELS] + [('march', 114)])
 @pytest.mark.parametrize('precision', ['float32', 'float64'])
-def test_interior_and_boundary_tiles_match_oracle(kernel, precision):
-    """A grid large enough for interior tiles (lean kernel, prefetched z-CPML memories) and boundary
-    strips (general kernel) in one step, with sources in the interior and a DFT plane."""
+def test_interior_and_boundary_tiles_match_oracle(kernel, variant, precision):
+    """A grid large enough for interior tiles and boundary strips, with sources in the interior and a DFT
+    plane. Variant 114 splits the march: the pure fast kernel over the interior tiles' planes outside the
+    z slabs, the general kernel over their z-slab planes and over the boundary strips (concurrent launches)."""
     from torchfdtd_b200.models import FieldMonitor, Source, SpectrumSettings, Structure
     region = Region(dimension='3d', size=(5.0, 3.0, 1.5), mesh=.05, pml_cells=6, steps=24, precision=precision, backend='cuda')
     project = Project(region=region, structures=[Structure(kind='sphere', radius=.6, material='Si (constant n)')],
@@ -197,7 +198,10 @@ def test_interior_and_boundary_tiles_match_oracle(kernel, precision):
     oracle = YeeOracle(plan)
     oracle.E[:] = rng.normal(size=oracle.E.shape).astype(plan.dtype) * .01
     oracle.H[:] = rng.normal(size=oracle.H.shape).astype(plan.dtype) * .01
-    g = native(plan, kernel)
+    if variant and precision == 'float64':
+        variant = 122                             # FP64 runs D / MINB = 22
+    from torchfdtd_b200.native import NativeGrid
+    g = NativeGrid(plan, kernel=kernel, variant=variant)
     g.set_fields(oracle.E, oracle.H)
     oracle.run()
     g.step(plan.steps)

@@ -377,7 +377,7 @@ struct tfd_plan {
     MarchArgs<double> md;
     dim3 march_grid;
     size_t march_smem = 0;
-    struct MarchLaunch { int mode; dim3 grid; int tx_off, ty_off, lz; };
+    struct MarchLaunch { int mode; dim3 grid; int tx_off, ty_off, lz, z_lo, z_hi; };
     std::vector<MarchLaunch> march_launches;
     // Boundary strips run on auxiliary streams, forked from and joined back to the caller's stream
     // (a CUDA graph capture records them as parallel branches).
@@ -691,20 +691,31 @@ int setup_march_s(tfd_plan *p, bool split_interior, int lz_fixed) {
     // per step at 23 % L2 hits, 12-plane chunks 4.1 GB at 41 %, and ran 2.8x faster), while short
     // chunks reload more halo planes (4 planes: 9 % slower than 12). Small grids take shorter chunks,
     // down to 2 planes, until the launch has two waves of CTAs.
-    auto choose_lz = [&](long long tiles, double share) {
-        if (lz_fixed > 0) return std::min(lz_fixed, g.n[2]);
+    auto choose_lz = [&](long long tiles, int planes, double share) {
+        if (lz_fixed > 0) return std::min(lz_fixed, planes);
         const double slots = std::max(1.0, share * resident);
-        int chunks = (g.n[2] + kMarchChunkPlanes - 1) / kMarchChunkPlanes;
+        int chunks = (planes + kMarchChunkPlanes - 1) / kMarchChunkPlanes;
         while ((double)tiles * chunks < 2 * slots) {
             const int next = chunks + 1;
-            if ((g.n[2] + next - 1) / next < 2) break;
+            if ((planes + next - 1) / next < 2) break;
             chunks = next;
         }
-        return (g.n[2] + chunks - 1) / chunks;
+        return (planes + chunks - 1) / chunks;
     };
-    auto chunks_of = [&](int lz) { return (unsigned)((g.n[2] + lz - 1) / lz); };
-    const int lz_all = choose_lz((long long)tx * ty, 1.0);
-    p->march_grid = dim3(tx, ty, chunks_of(lz_all));
+    auto chunks_of = [&](int lz, int planes) { return (unsigned)((planes + lz - 1) / lz); };
+    const int nzp = g.n[2];
+    const int lz_all = choose_lz((long long)tx * ty, nzp, 1.0);
+    p->march_grid = dim3(tx, ty, chunks_of(lz_all, nzp));
+    p->march_launches.clear();
+    // One launch of `mode` over tiles [ox, ox + sx) x [oy, oy + sy) and planes [zlo, zhi); share: its
+    // fraction of the step's tile-planes (for the chunk length).
+    const double tile_planes = (double)tx * ty * nzp;
+    auto push = [&](int mode, int sx, int sy, int ox, int oy, int zlo, int zhi) {
+        if (sx <= 0 || sy <= 0 || zhi <= zlo) return;
+        const int planes = zhi - zlo;
+        const int lz = choose_lz((long long)sx * sy, planes, (double)sx * sy * planes / tile_planes);
+        p->march_launches.push_back({mode, dim3(sx, sy, chunks_of(lz, planes)), ox, oy, lz, zlo, zhi});
+    };
     // Interior tiles: all 32 x 16 computed cells inside the domain, x-1 / y-1 present, H neighbours
     // x+1 / y+1 present, and no E or H CPML slab on x or y. They form a contiguous tile range.
     auto meets = [&](int f, int ax, int lo, int hi) {
@@ -726,24 +737,40 @@ int setup_march_s(tfd_plan *p, bool split_interior, int lz_fixed) {
     while (iy0 < ty && !interior_y(iy0)) ++iy0;
     iy1 = iy0;
     while (iy1 < ty && interior_y(iy1)) ++iy1;
-    p->march_launches.clear();
-    // The interior/boundary split is off by default: measured on B200 at 512x512x256 it is slower
-    // (50.6 vs 54.8 Gcell/s) than one general launch; launch variants >= 100 enable it.
-    if (ix1 > ix0 && iy1 > iy0 && split_interior) {
-        const long long all = (long long)tx * ty, inner = (long long)(ix1 - ix0) * (iy1 - iy0);
-        const double inner_share = (double)inner / all, strip_share = 1.0 - inner_share;
-        const int lzi = choose_lz(inner, inner_share);
-        p->march_launches.push_back({1, dim3(ix1 - ix0, iy1 - iy0, chunks_of(lzi)), ix0, iy0, lzi});
-        auto strip = [&](int sx, int sy, int ox, int oy) {
-            const int lzs = choose_lz((long long)sx * sy, strip_share * sx * sy / std::max(1LL, all - inner));
-            p->march_launches.push_back({edge_mode, dim3(sx, sy, chunks_of(lzs)), ox, oy, lzs});
-        };
-        if (ix0 > 0) strip(ix0, ty, 0, 0);
-        if (ix1 < tx) strip(tx - ix1, ty, ix1, 0);
-        if (iy0 > 0) strip(ix1 - ix0, iy0, ix0, 0);
-        if (iy1 < ty) strip(ix1 - ix0, ty - iy1, ix0, iy1);
+    // Pure planes: the longest range [za, zb) whose chunks meet no z slab: E planes za..zb (zb is a
+    // chunk's halo plane) outside every E-family z slab, H planes za..zb-1 outside every H-family one,
+    // za >= 1 and zb <= nz - 1 (the first and last planes have faces).
+    int za = 0, zb = 0;
+    {
+        std::vector<char> ebad(nzp + 1, 0), hbad(nzp + 1, 0);
+        for (int q = 0; q < 2; ++q) {
+            for (int z = a.slab[0][2][2 * q]; z < a.slab[0][2][2 * q + 1]; ++z) ebad[z] = 1;
+            for (int z = a.slab[1][2][2 * q]; z < a.slab[1][2][2 * q + 1]; ++z) hbad[z] = 1;
+        }
+        for (int z = 1; z < nzp - 1; ++z) {
+            if (ebad[z] || hbad[z]) continue;
+            int e = z;
+            while (e + 1 <= nzp - 1 && !ebad[e + 1] && !hbad[e]) ++e;
+            if (e - z > zb - za) { za = z; zb = e; }
+            z = e;
+        }
+    }
+    if (split_interior && ix1 > ix0 && iy1 > iy0 && zb - za >= 2) {
+        // The pure fast kernel over the interior block; the general kernel over its z-slab planes and
+        // over the boundary strips (all planes). Concurrent launches on forked streams.
+        // Measured on B200 this split is slower than one general launch (512x512x256: 1.16 vs 1.02 ms per
+        // step, in either launch order; 256^3: 0.41 vs 0.37 ms), so it is a launch variant the tuner may
+        // pick (split digit 1), not the default.
+        const int ni = ix1 - ix0, nj = iy1 - iy0;
+        push(edge_mode, ix0, ty, 0, 0, 0, nzp);
+        push(edge_mode, tx - ix1, ty, ix1, 0, 0, nzp);
+        push(edge_mode, ni, iy0, ix0, 0, 0, nzp);
+        push(edge_mode, ni, ty - iy1, ix0, iy1, 0, nzp);
+        push(edge_mode, ni, nj, ix0, iy0, 0, za);
+        push(edge_mode, ni, nj, ix0, iy0, zb, nzp);
+        push(1, ni, nj, ix0, iy0, za, zb);
     } else {
-        p->march_launches.push_back({edge_mode, dim3(tx, ty, chunks_of(lz_all)), 0, 0, lz_all});
+        push(edge_mode, tx, ty, 0, 0, 0, nzp);
     }
     if (p->aux.empty() && p->march_launches.size() > 1) {
         TFD_CUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
@@ -794,12 +821,15 @@ void launch_march(tfd_plan *p, cudaStream_t s) {
         cudaStream_t st = k == 0 ? s : p->aux[k - 1];
         if (k > 0) cudaStreamWaitEvent(st, p->fork, 0);
         if (l.mode == 1)
-            k_step_march<T, SAMPLES, D, MINB, 1><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz);
+            k_step_march<T, SAMPLES, D, MINB, 1><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz,
+                                                                                             l.z_lo, l.z_hi);
         else if (l.mode == 2) {
             if constexpr (D * 10 + MINB == periodic_march_variant<T>())
-                k_step_march<T, SAMPLES, D, MINB, 2><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz);
+                k_step_march<T, SAMPLES, D, MINB, 2><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off,
+                                                                                                 l.lz, l.z_lo, l.z_hi);
         } else
-            k_step_march<T, SAMPLES, D, MINB, 0><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz);
+            k_step_march<T, SAMPLES, D, MINB, 0><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz,
+                                                                                             l.z_lo, l.z_hi);
         if (k > 0) cudaEventRecord(p->join[k - 1], st);
     }
     for (size_t k = 1; k < n; ++k) cudaStreamWaitEvent(s, p->join[k - 1], 0);

@@ -150,35 +150,6 @@ __device__ __forceinline__ Coef<T> coef_at(const Grid<T> &g, int f, int a, int c
     return q;
 }
 
-// E-family memories of both parities sit one psi_parity apart; `po`/`pn` are the old/new offsets.
-template <typename T>
-__device__ __forceinline__ T cpml_e32(const Grid<T> &g, int po, int pn, int a, int j, const Coef<T> &q, int r, int x, int y, int z,
-                                      bool own, T d) {
-    const int p = psi_index32(a, x, y, z, r, g.rows[0][a], g.n[1], g.pitch);
-    T *base = g.psiE[0][a][j];
-    const T mem = base[po + p] * q.b + q.c * d;
-    if (own) base[pn + p] = mem;
-    return d * q.k + mem;
-}
-
-template <typename T>
-__device__ __forceinline__ T cpml_h32q(const Grid<T> &g, int a, int j, const Coef<T> &q, int r, int x, int y, int z, T d) {
-    const int p = psi_index32(a, x, y, z, r, g.rows[1][a], g.n[1], g.pitch);
-    T *psi = g.psiH[a][j];
-    const T mem = psi[p] * q.b + q.c * d;
-    psi[p] = mem;
-    return d * q.k + mem;
-}
-
-template <typename T>
-__device__ __forceinline__ T cpml_h32(const Grid<T> &g, int a, int j, int coord, int r, int x, int y, int z, T d) {
-    const int p = psi_index32(a, x, y, z, r, g.rows[1][a], g.n[1], g.pitch);
-    T *psi = g.psiH[a][j];
-    const T mem = psi[p] * __ldg(&g.cb[1][a][coord]) + __ldg(&g.cc[1][a][coord]) * d;
-    psi[p] = mem;
-    return d * __ldg(&g.ck[1][a][coord]) + mem;
-}
-
 // Source injection restricted to the terms that touch this tile and plane (bit s of mask).
 template <typename T>
 __device__ __noinline__ T inject_masked(const Grid<T> &g, unsigned mask, int family, int comp, long long n, int x, int y, int z, T v) {
@@ -210,17 +181,12 @@ __device__ __forceinline__ unsigned source_mask(const Grid<T> &g, int family, in
 template <typename T>
 struct Rows { int x, y, z; int po[3], pn[3]; Coef<T> qx, qy, qz; };
 
-// E_new of component C at stage index s. hk: plane k stage base, hm: plane k-1 stage base.
-// hk / hm: H stage of plane k / k-1 (box row 0 = y0-1, stride HS); ek: E stage of plane k
-// (box row 0 = y0, stride ES); sh / se: the cell's element index in those boxes.
-// FAST: the warp row meets no CPML slab, no domain face and no source, and plane z has a previous
-// plane; the same arithmetic without the checks.
-// PZ: the z-term's old CPML memory comes from pz[j] (prefetched by the caller) instead of a load.
-// WRAP: x / y are periodic where the grid says so: the first column / row differences against the
-// wrapped neighbour that the caller placed in the stage.
-template <typename T, int SAMPLES, int D, int C, bool FAST = false, bool PZ = false, bool WRAP = false>
-__device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, int x, int y, int z,
-                                     bool zprev, bool own, const Rows<T> &rw, const T *pz = nullptr) {
+// E_new of component C on the fast path (the row meets no CPML slab, no domain face and no source, and
+// plane z has a previous plane): plain differences in the reference order. hk / hm: H stage of plane
+// k / k-1 (box row 0 = y0-1, stride HS); ek: E stage of plane k (box row 0 = y0, stride ES); s / se: the
+// cell's element index in those boxes.
+template <typename T, int SAMPLES, int D, int C>
+__device__ __forceinline__ T march_e_fast(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se) {
     using S = MarchShape<T, SAMPLES, D>;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
@@ -229,37 +195,7 @@ __device__ __forceinline__ T march_e(const Grid<T> &g, const T *hk, const T *hm,
     for (int k = 0; k < 2; ++k) {
         const Term t = term_of(C, k);
         const T *h = hk + t.in * HS;
-        T d;
-        if (FAST) {
-            d = t.axis == 0 ? h[s] - h[s - 1] : t.axis == 1 ? h[s] - h[s - S::BXW] : h[s] - hm[t.in * HS + s];
-        } else if (PZ && t.axis == 0) {       // interior tile: x > 0, no x slab
-            d = h[s] - h[s - 1];
-        } else if (PZ && t.axis == 1) {       // interior tile: y > 0, no y slab
-            d = h[s] - h[s - S::BXW];
-        } else if (t.axis == 0) {
-            const T diff = h[s] - h[s - 1];
-            d = (x > 0 || (WRAP && g.periodic[0])) ? diff : T(0);
-            if (rw.x >= 0) d = cpml_e32(g, rw.po[0], rw.pn[0], 0, t.j, rw.qx, rw.x, x, y, z, own, d);
-        } else if (t.axis == 1) {
-            const T diff = h[s] - h[s - S::BXW];
-            d = (y > 0 || (WRAP && g.periodic[1])) ? diff : T(0);
-            if (rw.y >= 0) d = cpml_e32(g, rw.po[1], rw.pn[1], 1, t.j, rw.qy, rw.y, x, y, z, own, d);
-        } else {
-            d = T(0);
-            if (zprev) {
-                d = h[s] - hm[t.in * HS + s];
-                if (rw.z >= 0) {
-                    if (PZ) {
-                        const T mem = pz[t.j] * rw.qz.b + rw.qz.c * d;
-                        if (own)
-                            g.psiE[0][2][t.j][rw.pn[2] + psi_index32(2, x, y, z, rw.z, g.rows[0][2], g.n[1], g.pitch)] = mem;
-                        d = d * rw.qz.k + mem;
-                    } else {
-                        d = cpml_e32(g, rw.po[2], rw.pn[2], 2, t.j, rw.qz, rw.z, x, y, z, own, d);
-                    }
-                }
-            }
-        }
+        const T d = t.axis == 0 ? h[s] - h[s - 1] : t.axis == 1 ? h[s] - h[s - S::BXW] : h[s] - hm[t.in * HS + s];
         acc = acc + (t.sign > 0 ? d : -d);
     }
     return ek[C * ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? C : 0)) * ES + se]) * acc;
@@ -395,15 +331,16 @@ __device__ __forceinline__ void march_h_row(const Grid<T> &g, const T *ep, const
 }
 
 // D planes of TMA prefetch; MINB CTAs per SM requested from the register allocator.
-// MODE 0 (general) runs any tile; MODE 1 (interior) runs tiles whose computed 32 x 16 cells lie
-// inside the domain and outside every x/y CPML slab (the host launches it over that tile range and
-// the general kernel over the boundary strips), so only the z-CPML memories remain, and those are
-// loaded into registers at the top of each plane, ahead of the TMA wait. Tile (tx, ty) of a launch
-// is (blockIdx.x + tx_off, blockIdx.y + ty_off); lz planes per z chunk (blockIdx.z).
-// MODE 2 is MODE 0 with periodic x / y seams (the host launches it when the grid has them).
+// MODE 0 (general) runs any tile. MODE 1 (pure) has only the fast path (plus source injection): the host
+// launches it over tiles whose computed 32 x 16 cells lie inside the domain and outside every x/y CPML
+// slab, and over planes whose chunks (with their halo plane) meet no z slab of either family, and the
+// general kernel over the rest; compiled without the face and CPML code, the fast path gets the whole
+// 64-register budget. MODE 2 is MODE 0 with periodic x / y seams (the host launches it when the grid has
+// them). Tile (tx, ty) of a launch is (blockIdx.x + tx_off, blockIdx.y + ty_off); chunk blockIdx.z
+// covers planes [z_lo + blockIdx.z * lz, min(that + lz, z_hi)).
 template <typename T, int SAMPLES, int D, int MINB, int MODE>
 __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid_constant__ MarchArgs<T> args, int tx_off, int ty_off,
-                                                                    int lz) {
+                                                                    int lz, int z_lo, int z_hi) {
     using S = MarchShape<T, SAMPLES, D>;
     constexpr bool INTERIOR = MODE == 1;
     constexpr bool PXY = MODE == 2;
@@ -425,9 +362,9 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     const int par = (int)(n & 1);
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const int x0 = (blockIdx.x + tx_off) * kMarchOwnX, y0 = (blockIdx.y + ty_off) * kMarchOwnY;
-    const int z0 = blockIdx.z * lz;
-    if (z0 >= nz) return;
-    const int z1 = min(z0 + lz, nz);
+    const int z0 = z_lo + blockIdx.z * lz;
+    if (z0 >= z_hi) return;
+    const int z1 = min(z0 + lz, z_hi);
     const bool zper = g.periodic[2] != 0;
     const bool has_prev = z0 > 0 || zper;                    // plane z0-1 exists (wrapped when periodic)
     const bool has_halo = z1 < nz || zper;                   // plane z1 exists (wrapped when periodic)
@@ -574,30 +511,6 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
         const int t = k - z0;                                // E sequence index of plane k; H index is t + 1
         const bool halo_plane = k == z1;
         const bool compute_e = !halo_plane || has_halo;
-        // Interior tiles: issue this plane's z-slab CPML memory loads before waiting for the TMA stages.
-        T pzE[kMarchRowsPerThread][2], pzH[kMarchRowsPerThread][2];
-        int rzE_pre = -1, rzH_pre = -1;
-        if (INTERIOR) {
-            const int kzp = k >= nz ? k - nz : k;
-            rzE_pre = compute_e && (kzp > 0 || zper) ? TFD_SLAB_ROW(args, 0, 2, kzp) : -1;
-            rzH_pre = k > z0 ? TFD_SLAB_ROW(args, 1, 2, k - 1) : -1;
-            if (rzE_pre >= 0) {
-#pragma unroll
-                for (int h = 0; h < kMarchRowsPerThread; ++h)
-                    if (yrow[h] < ny)
-#pragma unroll
-                        for (int j = 0; j < 2; ++j)
-                            pzE[h][j] = g.psiE[0][2][j][(par ? args.psi_parity[2] : 0) + psi_index32(2, x, yrow[h], kzp, rzE_pre, g.rows[0][2], ny, g.pitch)];
-            }
-            if (rzH_pre >= 0) {
-#pragma unroll
-                for (int h = 0; h < kMarchRowsPerThread; ++h)
-                    if (yrow[h] < ny && warp + kMarchWarps * h < kMarchOwnY && lane_own)
-#pragma unroll
-                        for (int j = 0; j < 2; ++j)
-                            pzH[h][j] = g.psiH[2][j][psi_index32(2, x, yrow[h], k - 1, rzH_pre, g.rows[1][2], ny, g.pitch)];
-            }
-        }
         if (compute_e && !(wait_h(t + 1) && wait_e(t))) {
             if (tid == 0) atomicExch(g.status, kStatusPipelineTimeout);
             return;
@@ -634,16 +547,10 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                 const Rows<T> &rw = no_rows;
                 T ex, ey, ez;
                 const bool cpml_row = ((rowbits >> h) & 1u) || rzE >= 0;
-                if (!cpml_row && !((rowbits >> (R + h)) & 1u) && zprev && !smask) {
-                    ex = march_e<T, SAMPLES, D, 0, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
-                    ey = march_e<T, SAMPLES, D, 1, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
-                    ez = march_e<T, SAMPLES, D, 2, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rw);
-                } else if (INTERIOR) {
-                    // only the z-CPML memories and sources can apply here
-                    const Rows<T> rz = e_rows(x, y, kz, rzE);
-                    ex = march_e<T, SAMPLES, D, 0, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rz, pzE[h]);
-                    ey = march_e<T, SAMPLES, D, 1, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rz, pzE[h]);
-                    ez = march_e<T, SAMPLES, D, 2, false, true>(g, hk, hm, ek, sh, se, x, y, kz, zprev, own, rz, pzE[h]);
+                if (INTERIOR || (!cpml_row && !((rowbits >> (R + h)) & 1u) && zprev && !smask)) {
+                    ex = march_e_fast<T, SAMPLES, D, 0>(g, hk, hm, ek, sh, se);
+                    ey = march_e_fast<T, SAMPLES, D, 1>(g, hk, hm, ek, sh, se);
+                    ez = march_e_fast<T, SAMPLES, D, 2>(g, hk, hm, ek, sh, se);
                 } else if (!cpml_row) {
                     march_e_row<T, SAMPLES, D, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw, ex, ey, ez);
                 } else {
@@ -691,7 +598,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                 const int e = r * kMarchLanes + lane;
                 const int i = y * g.pitch + x;
                 const bool cpml_row = ((rowbits >> (2 * R + h)) & 1u) || rzH >= 0;
-                if (!cpml_row && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask) {
+                if (INTERIOR || (!cpml_row && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask)) {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const Term t0 = term_of(c, 0), t1 = term_of(c, 1);
@@ -704,7 +611,9 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                         T acc = T(0);
                         acc = acc + (t0.sign > 0 ? d0 : -d0);
                         acc = acc + (t1.sign > 0 ? d1 : -d1);
-                        gH[c][i] = hs[c * HS + sh] - g.cn * acc;
+                        T hv = hs[c * HS + sh] - g.cn * acc;
+                        if (INTERIOR && hmask) hv = inject_masked(g, hmask, 1, c, n, x, y, km, hv);
+                        gH[c][i] = hv;
                     }
                     continue;
                 }
@@ -726,57 +635,6 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
                         if (hmask) hv[c] = inject_masked(g, hmask, 1, c, n, x, y, km, hv[c]);
                         gH[c][i] = hv[c];
                     }
-                } else {
-                const int rxH = TFD_SLAB_ROW(args, 1, 0, x), ryHh = TFD_SLAB_ROW(args, 1, 1, y);
-                const Coef<T> qxH = coef_at(g, 1, 0, x, rxH), qyHh = coef_at(g, 1, 1, y, ryHh), qzH = coef_at(g, 1, 2, km, rzH);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    T acc = T(0);
-#pragma unroll
-                    for (int kk = 0; kk < 2; ++kk) {
-                        const Term tm = term_of(c, kk);
-                        const T *ep = eprv + tm.in * S::EBUF;
-                        T d = T(0);
-                        if (tm.axis == 0) {
-                            if (INTERIOR) {
-                                d = ep[e + 1] - ep[e];
-                            } else if (x < nx - 1 || px) {
-                                d = ep[e + 1] - ep[e];
-                                if (rxH >= 0) d = cpml_h32q(g, 0, tm.j, qxH, rxH, x, y, km, d);
-                            } else if (g.pec_on[0]) {
-                                d = g.pec_neg[0] * ep[e];
-                            }
-                        } else if (tm.axis == 1) {
-                            if (INTERIOR) {
-                                d = ep[e + kMarchLanes] - ep[e];
-                            } else if (y < ny - 1 || py) {
-                                d = ep[e + kMarchLanes] - ep[e];
-                                if (ryHh >= 0) d = cpml_h32q(g, 1, tm.j, qyHh, ryHh, x, y, km, d);
-                            } else if (g.pec_on[1]) {
-                                d = g.pec_neg[1] * ep[e];
-                            }
-                        } else {
-                            if (znext) {
-                                d = ecur[tm.in * S::EBUF + e] - ep[e];
-                                if (rzH >= 0) {
-                                    if (INTERIOR) {
-                                        const T mem = pzH[h][tm.j] * qzH.b + qzH.c * d;
-                                        g.psiH[2][tm.j][psi_index32(2, x, y, km, rzH, g.rows[1][2], ny, g.pitch)] = mem;
-                                        d = d * qzH.k + mem;
-                                    } else {
-                                        d = cpml_h32q(g, 2, tm.j, qzH, rzH, x, y, km, d);
-                                    }
-                                }
-                            } else if (g.pec_on[2]) {
-                                d = g.pec_neg[2] * ep[e];
-                            }
-                        }
-                        acc = acc + (tm.sign > 0 ? d : -d);
-                    }
-                    T hv = hs[c * HS + sh] - g.cn * acc;
-                    if (hmask) hv = inject_masked(g, hmask, 1, c, n, x, y, km, hv);
-                    gH[c][i] = hv;
-                }
                 }
             }
         }
