@@ -329,6 +329,7 @@ def run_ours(args, world, rank, local):
     elapsed = max_over_ranks(start.elapsed_time(end) / 1e3, world)
     status = grid.device_status()
     kernel_used = grid.kernel
+    launches = grid.step_launches(args.steps)
     grid.close()
     del grid
     torch.cuda.empty_cache()
@@ -362,7 +363,7 @@ def run_ours(args, world, rank, local):
                 data='synthetic (seeded)', config=dict(workload=desc, cells=cells, l2='inputs larger than L2 (no flush needed)',
                                                        parallelism=f'replicas x{world}' if world > 1 else 'single GPU',
                                                        kernel=kernel_used),
-                roofline=roofline, e2e=e2e, clocks=clocks, gpu_launches=2 * args.steps, device_status=status)
+                roofline=roofline, e2e=e2e, clocks=clocks, gpu_launches=launches, device_status=status)
     if args.workload == 'periodic':
         line['restated_reference'] = time_restated_marching(plan, args, device, bytes_step, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -187,6 +187,10 @@ int tfd_field_norm_static(const void *E, const void *H, const void *inv_eps, int
 /* Which step kernel the plan runs (enum tfd_kernel) after TFD_KERNEL_AUTO is resolved. */
 int tfd_kernel_in_use(const tfd_plan *plan, int32_t *kernel);
 
+/* How many kernel launches tfd_step(plan, nsteps) issues (small 2D TMz plans run all their steps in one
+ * persistent launch; the other paths launch per step). No counterpart in the reference. */
+int tfd_step_launches(const tfd_plan *plan, int32_t nsteps, int64_t *launches);
+
 /* ---- batches: many independent 2D TMz grids of uneven size advanced by one launch per step ----
  * Replaces run_tensor_batch / run_grouped_batch cohorts (torchfdtd/tensor_batch.py:45-337,
  * torchfdtd/grouped_batch.py:38-146, torchfdtd/cuda_batch.py:19-169), which need identical shapes per

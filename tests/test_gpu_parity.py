@@ -350,3 +350,51 @@ def test_select_launch_measures_candidates_and_simulation_uses_the_winner():
     plain = Simulation(project).run()
     np.testing.assert_array_equal(tuned.electric, plain.electric)
     assert tuned.summary['launch_tuning']['kind'] == 'grid'
+
+
+@pytest.mark.parametrize('precision', ['float32', 'float64'])
+def test_persistent_2d_launch_equals_per_step_launches(golden, monkeypatch, precision):
+    """Small 2D TMz grids step in one persistent cooperative launch (grid barrier between steps, observations
+    of step n-1 taken during step n). Against the per-step launches: fields, CPML memories, traces, DFT planes
+    and the step counter bitwise equal, for uneven step counts per call and a call that runs past the end."""
+    from torchfdtd_b200.native import NativeGrid
+    d = np.load(golden / 'sim_tmz.npz')
+    project = Project.model_validate_json(str(d['project']))
+    project.region.precision = precision
+    plan = plan_grid(project)
+    grids = {}
+    for mode in ('0', '1'):
+        monkeypatch.setenv('TFD_PERSIST2D', mode)
+        grids[mode] = NativeGrid(plan, kernel='tile2d')
+    for count in (1, 7, 64, 3, plan.steps):
+        for g in grids.values():
+            g.step(count)
+    a, b = grids['0'], grids['1']
+    assert a.counter() == b.counter() == plan.steps
+    for x, y in zip(a.get_fields(), b.get_fields()):
+        np.testing.assert_array_equal(x, y)
+    for x, y in zip(a.get_psi(), b.get_psi()):
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(a.get_traces(), b.get_traces())
+    for k in range(len(plan.planes)):
+        np.testing.assert_array_equal(a.get_plane(k), b.get_plane(k))
+    assert a.device_status() == b.device_status() == 0
+
+
+@pytest.mark.parametrize('kernel', ['gather', 'march'])
+def test_steps_past_the_last_step_are_no_ops(kernel):
+    """Stepping a plan past its configured step count changes nothing: fields, CPML memories (the H family's
+    are updated in place), traces and the counter stay those of the last step."""
+    project = random_project('3d', 'float32', steps=14)
+    plan = plan_grid(project)
+    a, b = native(plan, kernel), native(plan, kernel)
+    a.step(14)
+    b.step(10)
+    b.step(9)
+    b.step(2)
+    assert a.counter() == b.counter() == 14
+    for x, y in zip(a.get_fields(), b.get_fields()):
+        np.testing.assert_array_equal(x, y)
+    for x, y in zip(a.get_psi(), b.get_psi()):
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(a.get_traces(), b.get_traces())

@@ -9,6 +9,7 @@
 
 #include "aux.cuh"
 #include "internal.cuh"
+#include "persist2d.cuh"
 #include "step_gather.cuh"
 #include "step_march.cuh"
 #include "step2d.cuh"
@@ -87,6 +88,7 @@ struct Layout {
     size_t src_values = 0, trace_tab = 0, trace_out = 0, plane_tab = 0;
     std::vector<PlaneLayout> planes;
     size_t counter = 0, done = 0, status = 0, diag = 0, stage = 0;
+    size_t grid_bar = 0;           // persistent 2D stepping: arrival count and generation
     size_t grid_tab = 0, tile_tab = 0;   // 2D tile kernel: this plan's Grid struct and its tile table
     int tiles2d = 0, strip_rows = 8;
     size_t stage_bytes = 0;
@@ -283,6 +285,23 @@ int interior_count(const std::vector<Tile2D> &t) {
 // Upper bound of the strip count of a grid for strips of at least 8 rows (two band edges add two cuts).
 int strip_capacity(int nx, int ny) { return ((nx + k2dOwnX - 1) / k2dOwnX) * ((ny + 7) / 8 + 2); }
 
+// 2D TMz grids up to this many cells step in one persistent launch (see setup_tile2d), over strips of
+// persist2d_strip_rows() rows. TFD_PERSIST2D=0/1 and TFD_PERSIST_ROWS in the environment override both,
+// for sweeps.
+constexpr long long kPersist2dMaxCells = 1LL << 19;
+constexpr int kPersist2dStripRows = 4;
+
+inline bool persist2d_eligible(long long cells) {
+    const char *env = getenv("TFD_PERSIST2D");
+    return env ? std::atoi(env) != 0 : cells <= kPersist2dMaxCells;
+}
+
+inline int persist2d_strip_rows() {
+    const char *env = getenv("TFD_PERSIST_ROWS");
+    const int rows = env ? std::atoi(env) : 0;
+    return rows >= 1 ? rows : kPersist2dStripRows;
+}
+
 void compute_layout(const tfd_desc *d, Layout &L) {
     Bump b;
     const int n[3] = {d->nx, d->ny, d->nz};
@@ -340,13 +359,14 @@ void compute_layout(const tfd_desc *d, Layout &L) {
         largest_plane = std::max(largest_plane, acc);
     }
     if (tile2d_capable(d)) {
-        L.strip_rows = strip_rows((long long)d->nx * d->ny);
+        L.strip_rows = persist2d_eligible((long long)d->nx * d->ny) ? persist2d_strip_rows() : strip_rows((long long)d->nx * d->ny);
         L.tiles2d = (int)strips_of(strip_geom(d), 0, L.strip_rows).size();
         L.grid_tab = b.take(std::max(sizeof(Grid<float>), sizeof(Grid<double>)));
         L.tile_tab = b.take((size_t)L.tiles2d * sizeof(Tile2D));
     }
     L.counter = b.take(sizeof(long long));
     L.done = b.take(sizeof(unsigned));
+    L.grid_bar = b.take(2 * sizeof(unsigned));
     L.status = b.take(sizeof(int));
     L.diag = b.take((size_t)kDiagBlocks * 4 * sizeof(double));
     psi_segments(d, &L.psi_total);
@@ -391,6 +411,7 @@ struct tfd_plan {
     }
     int march_variant = 42;
     int tile2d_interior = 0;
+    int persist_ctas = 0;          // > 0: 2D steps run as one persistent cooperative launch of this many CTAs
     std::unique_ptr<SideStream> side2d;
     bool in_batch = false;
     long long *own_counter = nullptr;
@@ -581,6 +602,7 @@ int zero_state(tfd_plan *p, cudaStream_t s) {
     }
     TFD_CUDA(cudaMemsetAsync(p->arena + L.counter, 0, sizeof(long long), s));
     TFD_CUDA(cudaMemsetAsync(p->arena + L.done, 0, sizeof(unsigned), s));
+    TFD_CUDA(cudaMemsetAsync(p->arena + L.grid_bar, 0, 2 * sizeof(unsigned), s));
     TFD_CUDA(cudaMemsetAsync(p->arena + L.status, 0, sizeof(int), s));
     return TFD_OK;
 }
@@ -624,6 +646,7 @@ bool march_supported(const tfd_plan *p) {
     const Grid<T> &g = const_cast<tfd_plan *>(p)->grid<T>();
     return g.n[2] > 1 && g.active == 0x3F;
 }
+
 
 // Target z-planes per CTA chunk of the marching kernel (see choose_lz in setup_march_s).
 constexpr int kMarchChunkPlanes = 12;
@@ -880,6 +903,18 @@ int setup_tile2d(tfd_plan *p, cudaStream_t s) {
     }
     TFD_CUDA(cudaMemcpyAsync(p->arena + p->L.grid_tab, &g, sizeof(Grid<T>), cudaMemcpyHostToDevice, s));
     TFD_CUDA(cudaMemcpyAsync(p->arena + p->L.tile_tab, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice, s));
+    // Small grids step in one persistent launch (TFD_PERSIST2D=0/1 in the environment overrides the size
+    // rule, for sweeps): a warp per strip, and no more CTAs than can be resident together.
+    p->persist_ctas = 0;
+    if (persist2d_eligible((long long)g.n[0] * g.n[1])) {
+        int device = 0, sms = 148, per_sm = 0;
+        TFD_CUDA(cudaGetDevice(&device));
+        TFD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        TFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step2d_persistent<T>, k2dThreads, 0));
+        const int mblocks = std::max(1, (p->max_samples + kMonitorThreads - 1) / kMonitorThreads) * std::max(1, p->desc.n_planes);
+        const int want = std::max({1, (p->L.tiles2d + k2dWarps - 1) / k2dWarps, mblocks});
+        if (per_sm > 0) p->persist_ctas = std::min(want, per_sm * sms);
+    }
     return TFD_OK;
 }
 
@@ -1080,8 +1115,33 @@ int launch_step_gather(tfd_plan *p, cudaStream_t s) {
     return TFD_OK;
 }
 
+// One persistent launch of `nsteps` 2D steps with their observations (cooperative: every CTA resident).
+template <typename T>
+int launch_persist2d(tfd_plan *p, int nsteps, cudaStream_t s) {
+    const MonitorArgs<T> m = monitor_args<T>(p);
+    const int mgx = std::max(1, (p->max_samples + kMonitorThreads - 1) / kMonitorThreads), mgy = std::max(1, p->desc.n_planes);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)p->persist_ctas);
+    cfg.blockDim = dim3(k2dThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TFD_CUDA(cudaLaunchKernelEx(&cfg, k_step2d_persistent<T>, (const Grid<T> *)(p->arena + p->L.grid_tab),
+                                (const Tile2D *)(p->arena + p->L.tile_tab), p->tile2d_interior, p->L.tiles2d, m, mgx, mgy, nsteps,
+                                p->ptr<unsigned>(p->L.grid_bar)));
+    return TFD_OK;
+}
+
 template <typename T>
 int step_t(tfd_plan *p, int nsteps, cudaStream_t s) {
+    if (p->kernel == TFD_KERNEL_TILE2D && p->persist_ctas > 0 && !p->in_batch) {
+        if (nsteps > 0) TFD_CHECK(launch_persist2d<T>(p, nsteps, s));
+        return TFD_OK;
+    }
     const MonitorArgs<T> m = monitor_args<T>(p);
     dim3 mgrid((unsigned)std::max(1, (p->max_samples + kMonitorThreads - 1) / kMonitorThreads), (unsigned)std::max(1, p->desc.n_planes));
     for (int k = 0; k < nsteps; ++k) {
@@ -1355,6 +1415,23 @@ int tfd_device_status(tfd_plan *p, int32_t *status, void *stream) {
 int tfd_kernel_in_use(const tfd_plan *p, int32_t *kernel) {
     if (!p || !kernel) return fail(TFD_ERR_INVALID, "null argument");
     *kernel = p->kernel;
+    return TFD_OK;
+}
+
+int tfd_step_launches(const tfd_plan *p, int32_t nsteps, int64_t *launches) {
+    if (!p || !launches) return fail(TFD_ERR_INVALID, "null argument");
+    if (nsteps < 0) return fail(TFD_ERR_INVALID, "nsteps must be non-negative");
+    long long per_step = 2;                                   // gather: step + observation
+    if (p->kernel == TFD_KERNEL_TILE2D) {
+        if (p->persist_ctas > 0 && !p->in_batch) {
+            *launches = nsteps > 0 ? 1 : 0;
+            return TFD_OK;
+        }
+        per_step = (p->tile2d_interior > 0) + (p->L.tiles2d > p->tile2d_interior) + 1;
+    } else if (p->kernel == TFD_KERNEL_MARCH) {
+        per_step = (long long)p->march_launches.size() + 1;
+    }
+    *launches = per_step * nsteps;
     return TFD_OK;
 }
 

@@ -31,15 +31,15 @@ struct MonitorArgs {
 constexpr int kMonitorThreads = 256;
 constexpr int kPhaseChunk = 256;
 
-// Observations of step n for one plan: block (bx, by) handles sample chunk bx of plane by; the blocks
-// of row by = 0 also record the point traces, strided over the row.
+// Observations of step n for one plan: block (bx, by) of a (gx x ...) grid handles sample chunk bx of plane
+// by; the blocks of row by = 0 also record the point traces, strided over the row.
 template <typename T>
-__device__ __forceinline__ void monitor_work(const MonitorArgs<T> &m, int bx, int by, long long n) {
+__device__ __forceinline__ void monitor_work(const MonitorArgs<T> &m, int bx, int by, long long n, int gx) {
     __shared__ double2 phase_e[kPhaseChunk], phase_h[kPhaseChunk];
     const long long shift = ((n + 1) & 1) ? m.count : 0;   // current (new) parity
     if (n >= m.steps) return;
     if (by == 0) {
-        for (int k = bx * blockDim.x + threadIdx.x; k < m.n_traces; k += gridDim.x * blockDim.x) {
+        for (int k = bx * blockDim.x + threadIdx.x; k < m.n_traces; k += gx * blockDim.x) {
             const TraceDev t = m.traces[k];
             const T *base = m.field[3 * t.family + t.comp];   // null: a component 2D does not advance (zero)
             m.trace_out[n * m.n_traces + k] = base ? base[shift + t.offset] : T(0);
@@ -111,7 +111,8 @@ __device__ __forceinline__ void finish_step(long long *counter, unsigned *done, 
 template <typename T>
 __global__ void __launch_bounds__(kMonitorThreads) k_monitor(const __grid_constant__ MonitorArgs<T> m) {
     const long long n = *m.counter;
-    monitor_work(m, blockIdx.x, blockIdx.y, n);
+    if (n >= m.steps) return;                  // past the plan's last step: no observation, the counter stays
+    monitor_work(m, blockIdx.x, blockIdx.y, n, gridDim.x);
     finish_step(m.counter, m.done, n);
 }
 
@@ -120,7 +121,7 @@ template <typename T>
 __global__ void __launch_bounds__(kMonitorThreads) k_monitor_batch(const MonitorArgs<T> *__restrict__ args, long long *counter,
                                                                   unsigned *done) {
     const long long n = *counter;
-    monitor_work(args[blockIdx.z], blockIdx.x, blockIdx.y, n);
+    monitor_work(args[blockIdx.z], blockIdx.x, blockIdx.y, n, gridDim.x);
     finish_step(counter, done, n);
 }
 

@@ -79,7 +79,7 @@ struct Grid {
 };
 
 // Device status codes (reported through tfd_device_status).
-enum : int { kStatusOk = 0, kStatusCounterRange = 1, kStatusPipelineTimeout = 2, kStatusBadStrip = 3 };
+enum : int { kStatusOk = 0, kStatusCounterRange = 1, kStatusPipelineTimeout = 2, kStatusBadStrip = 3, kStatusBarrierTimeout = 4 };
 
 struct PlaneDev {
     int points, frequencies, components, corners, ne;

@@ -120,6 +120,7 @@ __device__ __forceinline__ T h_value(const Grid<T> &g, int par, long long n, int
 template <typename T, int ACTIVE>
 __global__ void __launch_bounds__(128) k_step_gather_rows(const __grid_constant__ Grid<T> g) {
     const long long n = *g.counter;
+    if (n >= g.steps) return;                   // past the plan's last step: a step is a no-op
     const int par = (int)(n & 1);
     const int x = blockIdx.y * blockDim.x + threadIdx.x;
     const int y = blockIdx.x % g.n[1];

@@ -359,6 +359,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     uint64_t *bare = barh + S::NH;
 
     const long long n = *g.counter;
+    if (n >= g.steps) return;                   // past the plan's last step: a step is a no-op
     const int par = (int)(n & 1);
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
     const int x0 = (blockIdx.x + tx_off) * kMarchOwnX, y0 = (blockIdx.y + ty_off) * kMarchOwnY;

@@ -79,6 +79,7 @@ SIGNATURES = {
     'tfd_counter': (ctypes.c_int, [c_vp, P_i64, c_vp]),
     'tfd_device_status': (ctypes.c_int, [c_vp, P_i32, c_vp]),
     'tfd_kernel_in_use': (ctypes.c_int, [c_vp, P_i32]),
+    'tfd_step_launches': (ctypes.c_int, [c_vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
     'tfd_field_norm_static': (ctypes.c_int, [c_vp, c_vp, c_vp, c_i64, c_i32, c_i32, c_vp, c_vp]),
     'tfd_batch_bytes': (ctypes.c_int, [c_i32, ctypes.POINTER(c_vp), ctypes.POINTER(ctypes.c_size_t)]),
     'tfd_batch_create': (ctypes.c_int, [c_i32, ctypes.POINTER(c_vp), c_vp, ctypes.c_size_t, c_vp, ctypes.POINTER(c_vp)]),
@@ -369,6 +370,12 @@ class NativeGrid:
 
     def reset(self):
         check(library().tfd_reset(self.handle, _stream()))
+
+    def step_launches(self, n):
+        """Kernel launches that ``step(n)`` issues."""
+        v = c_i64()
+        check(library().tfd_step_launches(self.handle, int(n), ctypes.byref(v)))
+        return v.value
 
     def counter(self):
         v = c_i64()
