@@ -219,16 +219,19 @@ __device__ __forceinline__ T forward_curl(const AdjArgs<T> &A, const T *slot, in
     return acc;
 }
 
-// ACTIVE: bitmask of advanced components (bit c: E_c, bit 3+c: H_c). Launch like the forward gather
-// kernel: blockIdx.x = row (z*ny + y), blockIdx.y = 128-cell chunk of the row. Reads parity q, writes q^1.
+// ACTIVE: bitmask of advanced components (bit c: E_c, bit 3+c: H_c). Blocks of kAdjX x kAdjY cells of one
+// z plane (blockIdx.x, blockIdx.y: x and y tile; blockIdx.z: plane), so the x and y neighbours a cell reads
+// are mostly in its block's L1 lines. Reads parity q, writes q^1.
 // Part 1 of the reverse step: e_bar_new of the own cell, and S += e_bar_new * curl_b(H_n).
+constexpr int kAdjX = 32, kAdjY = 8;
+
 template <typename T, int ACTIVE>
-__global__ void __launch_bounds__(128) k_adjoint_e(const __grid_constant__ AdjArgs<T> A, const T *__restrict__ slot, int q) {
+__global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_e(const __grid_constant__ AdjArgs<T> A, const T *__restrict__ slot, int q) {
     const Grid<T> &g = A.g;
-    const int x = blockIdx.y * blockDim.x + threadIdx.x;
-    const int y = blockIdx.x % g.n[1];
-    const int z = blockIdx.x / g.n[1];
-    if (x >= g.n[0]) return;
+    const int x = blockIdx.x * kAdjX + threadIdx.x;
+    const int y = blockIdx.y * kAdjY + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= g.n[0] || y >= g.n[1]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
     if (ACTIVE & 1) {
         const T e = ebar_value<T, 0>(A, q, x, y, z, i, true);
@@ -249,12 +252,12 @@ __global__ void __launch_bounds__(128) k_adjoint_e(const __grid_constant__ AdjAr
 
 // Part 2: h_bar_new of the own cell from the e_bar_new that part 1 stored (own cell and +x/+y/+z).
 template <typename T, int ACTIVE>
-__global__ void __launch_bounds__(128) k_adjoint_h(const __grid_constant__ AdjArgs<T> A, int q) {
+__global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_h(const __grid_constant__ AdjArgs<T> A, int q) {
     const Grid<T> &g = A.g;
-    const int x = blockIdx.y * blockDim.x + threadIdx.x;
-    const int y = blockIdx.x % g.n[1];
-    const int z = blockIdx.x / g.n[1];
-    if (x >= g.n[0]) return;
+    const int x = blockIdx.x * kAdjX + threadIdx.x;
+    const int y = blockIdx.y * kAdjY + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= g.n[0] || y >= g.n[1]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
     T e[3] = {T(0), T(0), T(0)};
     if (ACTIVE & 1) e[0] = A.eb[q ^ 1][0][i];

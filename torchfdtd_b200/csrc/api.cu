@@ -1776,6 +1776,7 @@ int adjoint_create_t(tfd_adjoint *adj, cudaStream_t s) {
     for (int a = 0; a < 3; ++a)
         for (int j = 0; j < 2; ++j) A.sPsiE[a][j] = m.sPsiE[a][j];
     if (int rc = slab_bounds(p, A.slab)) return rc;
+    if (A.g.n[2] > 65535) return fail(TFD_ERR_UNSUPPORTED, "the adjoint step launches one z plane per grid row: nz above 65535");
     adj->used = adjoint_layout<T>(p, &A, adj->arena);
     TFD_CUDA(cudaMemsetAsync(adj->arena, 0, adj->used, s));
     adj->q = 0;
@@ -1791,20 +1792,21 @@ int adjoint_step_t(tfd_adjoint *adj, const void *snapshot, const void *seeds, cu
         k_adjoint_seed<T><<<std::max(1, std::min(1184, (n_obs + 255) / 256)), 256, 0, s>>>(A, p->ptr<TraceDev>(p->L.trace_tab), n_obs,
                                                                                        (const T *)seeds, adj->q);
     const Grid<T> &g = A.g;
-    const dim3 grid((unsigned)((long long)g.n[1] * g.n[2]), (unsigned)((g.n[0] + 127) / 128));
+    const dim3 grid((unsigned)((g.n[0] + kAdjX - 1) / kAdjX), (unsigned)((g.n[1] + kAdjY - 1) / kAdjY), (unsigned)g.n[2]);
+    const dim3 block(kAdjX, kAdjY);
     const T *slot = (const T *)snapshot;
     switch (p->desc.components) {
         case kMaskTM:
-            k_adjoint_e<T, kMaskTM><<<grid, 128, 0, s>>>(A, slot, adj->q);
-            k_adjoint_h<T, kMaskTM><<<grid, 128, 0, s>>>(A, adj->q);
+            k_adjoint_e<T, kMaskTM><<<grid, block, 0, s>>>(A, slot, adj->q);
+            k_adjoint_h<T, kMaskTM><<<grid, block, 0, s>>>(A, adj->q);
             break;
         case kMaskTE:
-            k_adjoint_e<T, kMaskTE><<<grid, 128, 0, s>>>(A, slot, adj->q);
-            k_adjoint_h<T, kMaskTE><<<grid, 128, 0, s>>>(A, adj->q);
+            k_adjoint_e<T, kMaskTE><<<grid, block, 0, s>>>(A, slot, adj->q);
+            k_adjoint_h<T, kMaskTE><<<grid, block, 0, s>>>(A, adj->q);
             break;
         default:
-            k_adjoint_e<T, kMaskAll><<<grid, 128, 0, s>>>(A, slot, adj->q);
-            k_adjoint_h<T, kMaskAll><<<grid, 128, 0, s>>>(A, adj->q);
+            k_adjoint_e<T, kMaskAll><<<grid, block, 0, s>>>(A, slot, adj->q);
+            k_adjoint_h<T, kMaskAll><<<grid, block, 0, s>>>(A, adj->q);
             break;
     }
     TFD_CUDA(cudaGetLastError());
