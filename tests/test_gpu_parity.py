@@ -179,12 +179,13 @@ def test_z_faces_periodic_and_pec_match_oracle(kernel, zfaces):
         np.testing.assert_array_equal(got, want)
 
 
-@pytest.mark.parametrize('kernel,variant', [(k, 0) for k in KERNELS] + [('march', 114)])
+@pytest.mark.parametrize('kernel,variant', [(k, 0) for k in KERNELS] + [('march', 114), ('march', 314)])
 @pytest.mark.parametrize('precision', ['float32', 'float64'])
 def test_interior_and_boundary_tiles_match_oracle(kernel, variant, precision):
     """A grid large enough for interior tiles and boundary strips, with sources in the interior and a DFT
     plane. Variant 114 splits the march: the pure fast kernel over the interior tiles' planes outside the
-    z slabs, the general kernel over their z-slab planes and over the boundary strips (concurrent launches)."""
+    z slabs, the general kernel over their z-slab planes and over the boundary strips (concurrent launches);
+    variant 314 runs both bodies in one launch, chosen per CTA."""
     from torchfdtd_b200.models import FieldMonitor, Source, SpectrumSettings, Structure
     region = Region(dimension='3d', size=(5.0, 3.0, 1.5), mesh=.05, pml_cells=6, steps=24, precision=precision, backend='cuda')
     project = Project(region=region, structures=[Structure(kind='sphere', radius=.6, material='Si (constant n)')],
@@ -199,7 +200,7 @@ def test_interior_and_boundary_tiles_match_oracle(kernel, variant, precision):
     oracle.E[:] = rng.normal(size=oracle.E.shape).astype(plan.dtype) * .01
     oracle.H[:] = rng.normal(size=oracle.H.shape).astype(plan.dtype) * .01
     if variant and precision == 'float64':
-        variant = 122                             # FP64 runs D / MINB = 22
+        variant = variant // 100 * 100 + 22       # FP64 runs D / MINB = 22
     from torchfdtd_b200.native import NativeGrid
     g = NativeGrid(plan, kernel=kernel, variant=variant)
     g.set_fields(oracle.E, oracle.H)
@@ -307,7 +308,7 @@ def test_invalid_descriptor_is_refused_with_a_named_error():
         nat.check(nat.library().tfd_plan_bytes(ctypes.byref(desc), ctypes.byref(size)))
 
 
-@pytest.mark.parametrize('variant', [14, 23, 32, 22, 114, 123, 4014, 7023])
+@pytest.mark.parametrize('variant', [14, 23, 32, 22, 114, 123, 214, 314, 4014, 7023])
 def test_march_launch_variants_match_oracle(variant):
     """Every launch shape the autotuner may pick (prefetch depth, CTAs per SM, interior split, z-chunk)."""
     from torchfdtd_b200.native import NativeGrid

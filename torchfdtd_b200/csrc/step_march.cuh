@@ -338,9 +338,9 @@ __device__ __forceinline__ void march_h_row(const Grid<T> &g, const T *ep, const
 // 64-register budget. MODE 2 is MODE 0 with periodic x / y seams (the host launches it when the grid has
 // them). Tile (tx, ty) of a launch is (blockIdx.x + tx_off, blockIdx.y + ty_off); chunk blockIdx.z
 // covers planes [z_lo + blockIdx.z * lz, min(that + lz, z_hi)).
-template <typename T, int SAMPLES, int D, int MINB, int MODE>
-__global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid_constant__ MarchArgs<T> args, int tx_off, int ty_off,
-                                                                    int lz, int z_lo, int z_hi) {
+// The body of one CTA: tile (tx, ty), planes [z0, z1).
+template <typename T, int SAMPLES, int D, int MODE>
+__device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int ty, int z0, int z1) {
     using S = MarchShape<T, SAMPLES, D>;
     constexpr bool INTERIOR = MODE == 1;
     constexpr bool PXY = MODE == 2;
@@ -362,10 +362,8 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
     if (n >= g.steps) return;                   // past the plan's last step: a step is a no-op
     const int par = (int)(n & 1);
     const int nx = g.n[0], ny = g.n[1], nz = g.n[2];
-    const int x0 = (blockIdx.x + tx_off) * kMarchOwnX, y0 = (blockIdx.y + ty_off) * kMarchOwnY;
-    const int z0 = z_lo + blockIdx.z * lz;
-    if (z0 >= z_hi) return;
-    const int z1 = min(z0 + lz, z_hi);
+    const int x0 = tx * kMarchOwnX, y0 = ty * kMarchOwnY;
+    if (z0 >= z1) return;
     const bool zper = g.periodic[2] != 0;
     const bool has_prev = z0 > 0 || zper;                    // plane z0-1 exists (wrapped when periodic)
     const bool has_halo = z1 < nz || zper;                   // plane z1 exists (wrapped when periodic)
@@ -646,6 +644,42 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
             issue_h(t + S::NH);
         }
     }
+}
+
+template <typename T, int SAMPLES, int D, int MINB, int MODE>
+__global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid_constant__ MarchArgs<T> args, int tx_off, int ty_off,
+                                                                    int lz, int z_lo, int z_hi) {
+    const int z0 = z_lo + blockIdx.z * lz;
+    march_body<T, SAMPLES, D, MODE>(args, blockIdx.x + tx_off, blockIdx.y + ty_off, z0, min(z0 + lz, z_hi));
+}
+
+// One launch over every tile and z chunk in which each CTA takes the pure body (MODE 1) when its tile is in
+// the interior block [ix0, ix1) x [iy0, iy1) and its chunk in the pure z segment, else the general body
+// (GEN: 0, or 2 with periodic seams). The planes are cut into three segments, [zb0, zb1), [zb1, zb2) (the
+// pure one) and [zb2, zb3), chunked separately (chunks[s] of lz[s] planes; blockIdx.z runs over all).
+// The two bodies share no state inside the plane loop, so the pure one is compiled as lean as in its own
+// kernel, while its CTAs interleave with the general ones as in one launch.
+struct MarchMix {
+    int ix0, ix1, iy0, iy1;
+    int zb[4];
+    int lz[3], chunks[3];
+};
+
+template <typename T, int SAMPLES, int D, int MINB, int GEN>
+__global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march_mixed(const __grid_constant__ MarchArgs<T> args,
+                                                                          const __grid_constant__ MarchMix mx) {
+    int zc = blockIdx.z, seg = 0;
+    while (seg < 2 && zc >= mx.chunks[seg]) {
+        zc -= mx.chunks[seg];
+        ++seg;
+    }
+    const int z0 = mx.zb[seg] + zc * mx.lz[seg];
+    const int z1 = min(z0 + mx.lz[seg], mx.zb[seg + 1]);
+    const int tx = blockIdx.x, ty = blockIdx.y;
+    if (seg == 1 && tx >= mx.ix0 && tx < mx.ix1 && ty >= mx.iy0 && ty < mx.iy1)
+        march_body<T, SAMPLES, D, 1>(args, tx, ty, z0, z1);
+    else
+        march_body<T, SAMPLES, D, GEN>(args, tx, ty, z0, z1);
 }
 
 }  // namespace tfd
