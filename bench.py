@@ -48,9 +48,9 @@ METRIC = 'Gcell-updates/s'
 C0 = 299792458.0
 # DRAM bytes per cell-update of the step kernel(s) measured by ncu on the workload itself
 # (dram__bytes_read.sum + dram__bytes_write.sum of one launch / cells; profiles/ has the commands):
-# 512x512x256: 2.357 + 1.782 GB per k_step_march launch; batch64: 493.4 MB (k_step2d_interior) + 118.5 MB
+# 512x512x256: 2.428 + 1.776 GB per k_step_march_mixed launch; batch64: 493.4 MB (k_step2d_interior) + 118.5 MB
 # (k_step2d_general) per step at the tuned launch shape.
-MEASURED_TRAFFIC_PER_CELL = {('roofline', 'march'): 4.139e9 / 67108864, ('batch64', 'tile2d'): 611.9e6 / 20187264}
+MEASURED_TRAFFIC_PER_CELL = {('roofline', 'march'): 4.204e9 / 67108864, ('batch64', 'tile2d'): 611.9e6 / 20187264}
 
 
 def baseline_face(layers):

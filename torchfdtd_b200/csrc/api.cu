@@ -659,10 +659,9 @@ constexpr int periodic_march_variant() { return sizeof(T) == 4 ? 14 : 22; }
 template <typename T, int SAMPLES, int D, int MINB>
 int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
     const bool split_interior = split == 1;
-    const bool seams0 = p->grid<T>().periodic[0] || p->grid<T>().periodic[1];
-    // Split digit 0: the mixed launch for grids with periodic seams (measured 9 % faster at 512x512x128),
-    // the general kernel alone otherwise (the mixed launch measured 1-2.5 % slower on the CPML scenes).
-    if (split == 0) split = seams0 ? 3 : 2;
+    // Split digit 0: the mixed launch where the grid has an interior block (measured on B200: 0.963 vs
+    // 1.038 ms per step at 512x512x256, 0.612 vs 0.691 ms at 512x512x128 periodic), else the general kernel.
+    if (split == 0) split = 3;
     using S = MarchShape<T, SAMPLES, D>;
     Grid<T> &g = p->grid<T>();
     MarchArgs<T> &a = p->march<T>();
@@ -840,8 +839,8 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
 // D / MINB: prefetch depth and CTAs per SM, one of 14 (FP32 default), 23, 32, 22 (FP64: 22 only);
 // split 1: the interior block and the boundary as separate concurrent launches; 2: the general kernel only;
 // 3: one launch, the pure body on the interior block's planes outside the z slabs (k_step_march_mixed), when
-// the grid has such a block; 0: 3 for grids with periodic x/y seams, else 2. lz: z-planes per CTA chunk (0:
-// about 12, shorter on small grids).
+// the grid has such a block (else the general kernel); 0: 3. lz: z-planes per CTA chunk (0: about 12, shorter
+// on small grids).
 // Grids with periodic x/y faces run D / MINB = 14 (FP32) or 22 (FP64) whatever the variant asks.
 // 0 selects the default (TFD_MARCH_VARIANT in the environment overrides the default, for sweeps).
 template <typename T>

@@ -344,6 +344,9 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     using S = MarchShape<T, SAMPLES, D>;
     constexpr bool INTERIOR = MODE == 1;
     constexpr bool PXY = MODE == 2;
+    // The general body keeps its row loops rolled: unrolled, its three row tiers exist once per row and the
+    // code outgrows the instruction cache once a pure body shares the SM (measured: 75 % vs 94 % hits).
+    constexpr int kRowUnroll = INTERIOR ? kMarchRowsPerThread : 1;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
     const Grid<T> &g = args.g;
@@ -533,10 +536,10 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                                               : 0u;
             T *gE0 = g.E[0][0] + fn + (size_t)kz * g.plane, *gE1 = g.E[0][1] + fn + (size_t)kz * g.plane,
               *gE2 = g.E[0][2] + fn + (size_t)kz * g.plane;
-#pragma unroll
+#pragma unroll kRowUnroll
             for (int h = 0; h < kMarchRowsPerThread; ++h) {
                 const int r = warp + kMarchWarps * h;
-                const int y = yrow[h];
+                const int y = y0 + warp + kMarchWarps * h;
                 const bool row_wraps = py && y == ny;               // computes E of row 0
                 if (!lane_in || (y >= ny && !row_wraps)) continue;
                 const int yc = row_wraps ? 0 : y;
@@ -588,10 +591,10 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
             const unsigned hmask = tile_src_h ? source_mask(g, 1, x0, x0 + kMarchOwnX, y0, y0 + kMarchOwnY, km, n) & tile_src_h : 0u;
             T *gH[3] = {g.H[0][0] + fn + (size_t)km * g.plane, g.H[0][1] + fn + (size_t)km * g.plane,
                         g.H[0][2] + fn + (size_t)km * g.plane};
-#pragma unroll
+#pragma unroll kRowUnroll
             for (int h = 0; h < kMarchRowsPerThread; ++h) {
                 const int r = warp + kMarchWarps * h;
-                const int y = yrow[h];
+                const int y = y0 + warp + kMarchWarps * h;
                 if (!lane_own || r >= kMarchOwnY || y >= ny) continue;
                 const int sh = (r + 1) * S::BXW + off + lane;
                 const int e = r * kMarchLanes + lane;
