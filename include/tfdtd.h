@@ -131,6 +131,16 @@ void tfd_plan_destroy(tfd_plan *plan);
  * field precision. Replaces g.inverse_permittivity[:] = 1/eps (torchfdtd/solver.py:742-745). */
 int tfd_set_material(tfd_plan *plan, const void *inv_eps, int where, void *stream);
 
+/* The relative permittivity itself, same layout: every value is checked (finite, at least 1) and inverted on
+ * the device (IEEE division, the host's 1/eps values) into the plan's material, saving the caller a host pass
+ * over the array. Returns TFD_ERR_INVALID when a value fails the check; synchronizes the stream. No
+ * counterpart in the reference (its solver inverts on the host). */
+int tfd_set_permittivity(tfd_plan *plan, const void *eps, int where, void *stream);
+
+/* The largest |E| over the current fields and whether every E and H value is finite (1) or not (0);
+ * synchronizes the stream. No counterpart in the reference (its Result checks the host copies). */
+int tfd_field_check(tfd_plan *plan, double *peak_e, int32_t *finite, void *stream);
+
 /* E and H in the reference layout (nx, ny, nz, 3), field precision (g.E, g.H). */
 int tfd_set_fields(tfd_plan *plan, const void *E, const void *H, int where, void *stream);
 int tfd_get_fields(tfd_plan *plan, void *E, void *H, int where, void *stream);

@@ -399,3 +399,43 @@ def test_steps_past_the_last_step_are_no_ops(kernel):
     for x, y in zip(a.get_psi(), b.get_psi()):
         np.testing.assert_array_equal(x, y)
     np.testing.assert_array_equal(a.get_traces(), b.get_traces())
+
+
+@pytest.mark.parametrize('precision', ['float32', 'float64'])
+def test_device_permittivity_inversion_and_field_check(precision):
+    """tfd_set_permittivity loads the same material as tfd_set_material(1 / eps) (bitwise equal fields after
+    stepping), refuses non-finite or sub-unity values, and tfd_field_check reports the host's peak |E|."""
+    project = random_project('3d', precision, sampling='yee')
+    plan = plan_grid(project)
+    eps = np.asarray(plan.epsilon, plan.dtype) * np.asarray(1 + .3 * np.random.default_rng(3).random(plan.epsilon.shape), plan.dtype)
+    plan.epsilon, plan.inv_eps = eps, (1 / eps).astype(plan.dtype)
+    a = native(plan, 'march')
+    from torchfdtd_b200.native import NativeGrid
+    b = NativeGrid(plan, kernel='march', permittivity=eps)
+    a.step(plan.steps)
+    b.step(plan.steps)
+    for x, y in zip(a.get_fields(), b.get_fields()):
+        np.testing.assert_array_equal(x, y)
+    E, H = b.get_fields()
+    peak, finite = b.field_check()
+    assert finite and peak == float(np.max(np.abs(E)))
+    for bad in (np.nan, np.inf, .5):
+        wrong = eps.copy()
+        wrong[3, 4, 5, 1] = bad
+        with pytest.raises(ValueError, match='epsilon must be finite and at least 1'):
+            b.set_permittivity(wrong)
+
+
+def test_simulation_device_material_and_checks_equal_host_path(monkeypatch):
+    """Simulation(project, epsilon).run() through the large-grid path (device permittivity inversion, device
+    field check, staged download) returns the host path's fields, traces and peak."""
+    import torchfdtd_b200.simulation as sim
+    project = random_project('3d', 'float32', steps=16)
+    eps = np.asarray(plan_grid(project).epsilon, np.float32)
+    want = sim.Simulation(project, epsilon=eps).run(cuda_graph=False)
+    monkeypatch.setattr(sim, 'LARGE_FIELD_BYTES', 0)
+    got = sim.Simulation(project, epsilon=eps).run(cuda_graph=False)
+    np.testing.assert_array_equal(got.electric, want.electric)
+    np.testing.assert_array_equal(got.magnetic, want.magnetic)
+    np.testing.assert_array_equal(got.signals, want.signals)
+    assert got.summary['field_peak'] == want.summary['field_peak']

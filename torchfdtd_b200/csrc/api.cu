@@ -89,6 +89,7 @@ struct Layout {
     std::vector<PlaneLayout> planes;
     size_t counter = 0, done = 0, status = 0, diag = 0, stage = 0;
     size_t grid_bar = 0;           // persistent 2D stepping: arrival count and generation
+    size_t check = 0;              // tfd_set_permittivity / tfd_field_check results
     size_t grid_tab = 0, tile_tab = 0;   // 2D tile kernel: this plan's Grid struct and its tile table
     int tiles2d = 0, strip_rows = 8;
     size_t stage_bytes = 0;
@@ -367,6 +368,7 @@ void compute_layout(const tfd_desc *d, Layout &L) {
     L.counter = b.take(sizeof(long long));
     L.done = b.take(sizeof(unsigned));
     L.grid_bar = b.take(2 * sizeof(unsigned));
+    L.check = b.take(4 * sizeof(unsigned long long));
     L.status = b.take(sizeof(int));
     L.diag = b.take((size_t)kDiagBlocks * 4 * sizeof(double));
     psi_segments(d, &L.psi_total);
@@ -1048,6 +1050,51 @@ int set_material_t(tfd_plan *p, const void *src, int where, cudaStream_t s) {
 }
 
 template <typename T>
+int set_permittivity_t(tfd_plan *p, const void *src, int where, cudaStream_t s) {
+    const tfd_desc &d = p->desc;
+    const int S = d.material_samples;
+    const size_t bytes = (size_t)d.nx * d.ny * d.nz * S * sizeof(T);
+    const void *dev;
+    int rc = stage_in(p, src, bytes, where, s, &dev);
+    if (rc) return rc;
+    Grid<T> &g = p->grid<T>();
+    int *bad = p->ptr<int>(p->L.check);
+    TFD_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+    k_permittivity_to_internal<T><<<launch_blocks((long long)d.nx * d.ny * d.nz * S), 256, 0, s>>>(
+        (const T *)dev, S, d.nx, d.ny, d.nz, g.pitch, (T *)g.inv_eps[0], (T *)(S == 3 ? g.inv_eps[1] : nullptr),
+        (T *)(S == 3 ? g.inv_eps[2] : nullptr), bad);
+    TFD_CUDA(cudaGetLastError());
+    int flag = 0;
+    TFD_CUDA(cudaMemcpyAsync(&flag, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TFD_CUDA(cudaStreamSynchronize(s));
+    if (flag) return fail(TFD_ERR_INVALID, "epsilon must be finite and at least 1.");
+    return TFD_OK;
+}
+
+template <typename T>
+int field_check_t(tfd_plan *p, double *peak_e, int32_t *finite, cudaStream_t s) {
+    unsigned long long *out = p->ptr<unsigned long long>(p->L.check);
+    TFD_CUDA(cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), s));
+    k_field_check<T><<<launch_blocks(p->L.count), 256, 0, s>>>(field_set<T>(p), p->L.count, p->grid<T>().counter, out);
+    TFD_CUDA(cudaGetLastError());
+    unsigned long long host[2] = {0, 0};
+    TFD_CUDA(cudaMemcpyAsync(host, out, sizeof(host), cudaMemcpyDeviceToHost, s));
+    TFD_CUDA(cudaStreamSynchronize(s));
+    double peak;
+    if (sizeof(T) == 4) {
+        const unsigned bits = (unsigned)host[0];
+        float f;
+        std::memcpy(&f, &bits, sizeof(f));
+        peak = f;
+    } else {
+        std::memcpy(&peak, &host[0], sizeof(peak));
+    }
+    *peak_e = peak;
+    *finite = host[1] ? 0 : 1;
+    return TFD_OK;
+}
+
+template <typename T>
 int set_fields_t(tfd_plan *p, const void *E, const void *H, int where, cudaStream_t s) {
     const tfd_desc &d = p->desc;
     const long long total = (long long)d.nx * d.ny * d.nz * 3;
@@ -1357,6 +1404,16 @@ void tfd_plan_destroy(tfd_plan *plan) { delete plan; }
 int tfd_set_material(tfd_plan *p, const void *inv_eps, int where, void *stream) {
     if (!p || !inv_eps) return fail(TFD_ERR_INVALID, "null argument");
     return TFD_DISPATCH(p, set_material_t, p, inv_eps, where, as_stream(stream));
+}
+
+int tfd_set_permittivity(tfd_plan *p, const void *eps, int where, void *stream) {
+    if (!p || !eps) return fail(TFD_ERR_INVALID, "null argument");
+    return TFD_DISPATCH(p, set_permittivity_t, p, eps, where, as_stream(stream));
+}
+
+int tfd_field_check(tfd_plan *p, double *peak_e, int32_t *finite, void *stream) {
+    if (!p || !peak_e || !finite) return fail(TFD_ERR_INVALID, "null argument");
+    return TFD_DISPATCH(p, field_check_t, p, peak_e, finite, as_stream(stream));
 }
 
 int tfd_set_fields(tfd_plan *p, const void *E, const void *H, int where, void *stream) {

@@ -142,6 +142,25 @@ __global__ void k_reference_to_internal(const T *__restrict__ src, int S, int nx
     }
 }
 
+// Permittivity in the reference layout to the internal inverse-permittivity arrays: 1 / eps by IEEE division
+// (the host's values); *bad is set when a value is not finite or below 1.
+template <typename T>
+__global__ void k_permittivity_to_internal(const T *__restrict__ src, int S, int nx, int ny, int nz, int pitch, T *d0, T *d1,
+                                           T *d2, int *bad) {
+    const long long total = (long long)nx * ny * nz * S;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int s = (int)(e % S);
+        const long long cell = e / S;
+        const int z = (int)(cell % nz);
+        const int y = (int)((cell / nz) % ny);
+        const int x = (int)(cell / ((long long)nz * ny));
+        T *d = s == 0 ? d0 : (s == 1 ? d1 : d2);
+        const T v = src[e];
+        if (!(v >= T(1)) || !isfinite(v)) atomicExch(bad, 1);
+        d[((long long)z * ny + y) * pitch + x] = T(1) / v;
+    }
+}
+
 template <typename T>
 __global__ void k_internal_to_reference(T *__restrict__ dst, int S, int nx, int ny, int nz, int pitch, const T *s0,
                                         const T *s1, const T *s2) {
@@ -161,6 +180,38 @@ __global__ void k_internal_to_reference(T *__restrict__ dst, int S, int nx, int 
 // is not advanced (2D) has a null pointer and reads as zero / ignores writes.
 template <typename T>
 struct FieldSet { T *f[2][6]; };
+
+// The largest |E| and whether any E or H value of the current parity is not finite. out[0]: the bit pattern of
+// the largest |E| (non-negative values order like their bit patterns); out[1]: 1 when a value is NaN or
+// infinite. Both start at zero.
+template <typename T>
+__global__ void k_field_check(const __grid_constant__ FieldSet<T> fs, long long count, const long long *counter,
+                              unsigned long long *out) {
+    const int par = (int)(*counter & 1);
+    T peak = T(0);
+    int bad = 0;
+#pragma unroll 1
+    for (int c = 0; c < 6; ++c) {
+        const T *f = fs.f[par][c];
+        if (f == nullptr) continue;
+        for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count; e += (long long)gridDim.x * blockDim.x) {
+            const T v = f[e];
+            if (!isfinite(v)) bad = 1;
+            else if (c < 3) peak = fmax(peak, fabs(v));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        peak = fmax(peak, __shfl_xor_sync(0xffffffffu, peak, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        const unsigned long long bits = sizeof(T) == 4 ? (unsigned long long)__float_as_uint((float)peak)
+                                                       : (unsigned long long)__double_as_longlong((double)peak);
+        atomicMax(&out[0], bits);
+        if (bad) atomicOr(&out[1], 1ull);
+    }
+}
 
 template <typename T>
 __global__ void k_fields_to_reference(T *__restrict__ E, T *__restrict__ H, int nx, int ny, int nz, int pitch,

@@ -65,6 +65,8 @@ SIGNATURES = {
     'tfd_plan_create': (ctypes.c_int, [ctypes.POINTER(Desc), c_vp, ctypes.c_size_t, c_vp, ctypes.POINTER(c_vp)]),
     'tfd_plan_destroy': (None, [c_vp]),
     'tfd_set_material': (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, c_vp]),
+    'tfd_set_permittivity': (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, c_vp]),
+    'tfd_field_check': (ctypes.c_int, [c_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(c_i32), c_vp]),
     'tfd_set_fields': (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int, c_vp]),
     'tfd_get_fields': (ctypes.c_int, [c_vp, c_vp, c_vp, ctypes.c_int, c_vp]),
     'tfd_psi_count': (ctypes.c_int, [c_vp, ctypes.POINTER(ctypes.c_size_t)]),
@@ -253,9 +255,10 @@ class NativeGrid:
         check(library().tfd_plan_bytes(ctypes.byref(desc), ctypes.byref(size)))
         return size.value
 
-    def __init__(self, plan, kernel='auto', device=None, variant=0, material=None):
+    def __init__(self, plan, kernel='auto', device=None, variant=0, material=None, permittivity=None):
         """``material``: the inverse permittivity to load instead of ``plan.inv_eps`` (a host array or a device
-        tensor, as for ``set_material``)."""
+        tensor, as for ``set_material``). ``permittivity``: the relative permittivity instead, checked and
+        inverted on the device (``set_permittivity``)."""
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError('CUDA requested but unavailable: the fused B200 engine runs on a CUDA GPU only.')
@@ -277,7 +280,10 @@ class NativeGrid:
         kernel_used = c_i32()
         check(lib.tfd_kernel_in_use(self.handle, ctypes.byref(kernel_used)))
         self.kernel = {v: k for k, v in KERNELS.items()}[kernel_used.value]
-        self.set_material(plan.inv_eps if material is None else material)
+        if permittivity is not None:
+            self.set_permittivity(permittivity)
+        else:
+            self.set_material(plan.inv_eps if material is None else material)
 
     # ---- restart states (checkpoints of the discrete adjoint) ------------------------------------
     def state_bytes(self):
@@ -318,6 +324,24 @@ class NativeGrid:
             return
         a = np.ascontiguousarray(inv_eps, dtype=self.dtype)
         check(library().tfd_set_material(self.handle, c_vp(a.ctypes.data), TFD_HOST, _stream()))
+
+    def set_permittivity(self, eps):
+        """Relative permittivity in the reference layout (a host array, or a contiguous device tensor of the
+        plan's dtype): checked (finite, at least 1; ValueError otherwise) and inverted on the device."""
+        if hasattr(eps, 'data_ptr'):
+            t = eps.contiguous()
+            if t.dtype != self.torch_dtype or t.device != self.device:
+                raise ValueError('device permittivity must be a tensor of the plan dtype on its device')
+            check(library().tfd_set_permittivity(self.handle, c_vp(t.data_ptr()), TFD_DEVICE, _stream()))
+            return
+        a = np.ascontiguousarray(eps, dtype=self.dtype)
+        check(library().tfd_set_permittivity(self.handle, c_vp(a.ctypes.data), TFD_HOST, _stream()))
+
+    def field_check(self):
+        """(largest |E|, every E and H value finite) over the current fields, computed on the device."""
+        peak, finite = ctypes.c_double(), c_i32()
+        check(library().tfd_field_check(self.handle, ctypes.byref(peak), ctypes.byref(finite), _stream()))
+        return peak.value, bool(finite.value)
 
     def set_fields(self, E=None, H=None):
         e = None if E is None else np.ascontiguousarray(E, dtype=self.dtype)

@@ -132,7 +132,7 @@ class GridPlan:
 
     @property
     def material_samples(self):
-        return 1 if self.inv_eps.ndim == 3 else 3
+        return 1 if (self.inv_eps if self.inv_eps is not None else self.epsilon).ndim == 3 else 3
 
     def psi_shapes(self):
         """Shapes of every CPML memory, in the order the reference allocates them (``YeeGrid.memory_states``)."""

@@ -248,10 +248,10 @@ class Observer:
             # Large grids: finiteness and the peak are checked on the device, and the fields come back through
             # a pinned staging ring (native.download). Small grids keep the host path, whose fixed costs are
             # lower than the first use of the device reductions.
-            e_dev, h_dev = grid.fields_device()
-            if not bool(torch.isfinite(e_dev).all()) or not bool(torch.isfinite(h_dev).all()):
+            field_peak, finite = grid.field_check()
+            if not finite:
                 raise FloatingPointError(self._where('Non-finite fields detected.'))
-            field_peak = float(e_dev.abs().amax())
+            e_dev, h_dev = grid.fields_device()
             e, h = download(e_dev), download(h_dev)
             del e_dev, h_dev
         else:
@@ -339,9 +339,9 @@ class Simulation:
         return plan
 
     def _run_plan(self):
-        """(plan, material) for ``run``. With ``epsilon`` the structures are not voxelized and the array is
-        uploaded once, checked and inverted on the device (IEEE division: the same values as the host's
-        1 / eps): ``plan.inv_eps`` is then that device tensor."""
+        """(plan, permittivity) for ``run``. A large ``epsilon`` skips voxelization and the host pass: the
+        library checks and inverts it on the device (IEEE division: the same values as the host's 1 / eps), and
+        ``plan.inv_eps`` stays None."""
         if self.epsilon is None or np.size(self.epsilon) * 4 <= LARGE_FIELD_BYTES:
             return self.plan, None
         import torch
@@ -350,15 +350,12 @@ class Simulation:
         if shape not in (tuple(plan.shape), (*plan.shape, 3)):
             raise ValueError(f'epsilon must have shape {tuple(plan.shape)} or {(*plan.shape, 3)}, not {shape}.')
         dtype = torch.float64 if plan.dtype == np.float64 else torch.float32
-        if isinstance(self.epsilon, torch.Tensor):
+        if isinstance(self.epsilon, torch.Tensor) and self.epsilon.is_cuda:
             eps = self.epsilon.detach().to(device='cuda', dtype=dtype).contiguous()
         else:
-            eps = torch.from_numpy(np.ascontiguousarray(np.asarray(self.epsilon, dtype=plan.dtype))).to('cuda')
-        if not bool(torch.isfinite(eps).all()) or bool((eps < 1).any()):
-            raise ValueError('epsilon must be finite and at least 1.')
+            eps = np.ascontiguousarray(np.asarray(self.epsilon, dtype=plan.dtype))
         plan.epsilon = self.epsilon
-        plan.inv_eps = torch.reciprocal(eps)
-        return plan, plan.inv_eps
+        return plan, eps
 
     def run(self, progress=None, cancel=None, cuda_graph=True, cuda_graph_steps=1, kernel='auto', launch=None):
         """``kernel``: 'auto' (the marching kernel for 3D, the tile kernel for 2D TMz, else gather) or a name.
@@ -376,7 +373,7 @@ class Simulation:
         if not torch.cuda.is_available():
             raise RuntimeError('CUDA requested but unavailable. The fused B200 engine needs a CUDA GPU.')
         started = time.perf_counter()
-        plan, material = self._run_plan()
+        plan, permittivity = self._run_plan()
         variant, tuning = 0, None
         if launch == 'auto':
             if plan.dimension == '3d' and kernel in ('auto', 'march'):
@@ -388,7 +385,7 @@ class Simulation:
                     tuning = dict(skipped=str(exc))
         elif launch is not None:
             variant = int(launch)
-        grid = NativeGrid(plan, kernel=kernel, variant=variant, material=material)
+        grid = NativeGrid(plan, kernel=kernel, variant=variant, permittivity=permittivity)
         free, _ = torch.cuda.mem_get_info()
         observer = Observer(p, plan, grid)
         graphs = {}
