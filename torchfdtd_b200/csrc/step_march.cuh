@@ -201,6 +201,82 @@ __device__ __forceinline__ T march_e_fast(const Grid<T> &g, const T *hk, const T
     return ek[C * ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? C : 0)) * ES + se]) * acc;
 }
 
+// E_new of one cell on a z-slab row (general kernel): the row meets no x / y slab, domain face or source and
+// plane z has a previous plane, but z lies in a z slab. The x / y terms are plain differences, the z terms of
+// Ex and Ey go through the z memories (old at po + iz, new at pn + iz, stored by the owner); the terms and
+// their order are those of march_e_row on such a row.
+template <typename T, int SAMPLES, int D>
+__device__ __forceinline__ void march_e_zslab(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, int iz, int po,
+                                              int pn, bool own, const Coef<T> &q, T &ex, T &ey, T &ez) {
+    using S = MarchShape<T, SAMPLES, D>;
+    constexpr int HS = S::BOXH_STRIDE / sizeof(T);
+    constexpr int ES = S::BOXE_STRIDE / sizeof(T);
+    const T o0 = g.psiE[0][2][0][po + iz], o1 = g.psiE[0][2][1][po + iz];
+    const T *Hx = hk, *Hy = hk + HS, *Hz = hk + 2 * HS;
+    T d, acc, m;
+    // Ex: (y, Hz, +), (z, Hy, -, memory j0)
+    d = Hz[s] - Hz[s - S::BXW];
+    acc = T(0);
+    acc = acc + d;
+    d = Hy[s] - hm[HS + s];
+    m = o0 * q.b + q.c * d;
+    if (own) g.psiE[0][2][0][pn + iz] = m;
+    d = d * q.k + m;
+    acc = acc + (-d);
+    ex = ek[se] + (g.cn * ek[3 * ES + se]) * acc;
+    // Ey: (x, Hz, -), (z, Hx, +, memory j1)
+    d = Hz[s] - Hz[s - 1];
+    acc = T(0);
+    acc = acc + (-d);
+    d = Hx[s] - hm[s];
+    m = o1 * q.b + q.c * d;
+    if (own) g.psiE[0][2][1][pn + iz] = m;
+    d = d * q.k + m;
+    acc = acc + d;
+    ey = ek[ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? 1 : 0)) * ES + se]) * acc;
+    ez = march_e_fast<T, SAMPLES, D, 2>(g, hk, hm, ek, s, se);
+}
+
+// H_new of one owned cell on a z-slab row: no x / y slab, face or source, plane km + 1 computed, km in a z slab
+// of the H family (memories at iz, updated in place); the terms and their order are those of march_h_row.
+template <typename T, int SAMPLES, int D>
+__device__ __forceinline__ void march_h_zslab(const Grid<T> &g, const T *ep, const T *ec, const T *hs, int sh, int e, int iz,
+                                              const Coef<T> &q, T &hx, T &hy, T &hz) {
+    using S = MarchShape<T, SAMPLES, D>;
+    constexpr int HS = S::BOXH_STRIDE / sizeof(T);
+    constexpr int EB = S::EBUF;
+    const T o0 = g.psiH[2][0][iz], o1 = g.psiH[2][1][iz];
+    const T *Ex = ep, *Ey = ep + EB, *Ez = ep + 2 * EB;
+    T d, acc, m;
+    // Hx: (y, Ez, +), (z, Ey, -, memory j0)
+    d = Ez[e + kMarchLanes] - Ez[e];
+    acc = T(0);
+    acc = acc + d;
+    d = ec[EB + e] - Ey[e];
+    m = o0 * q.b + q.c * d;
+    g.psiH[2][0][iz] = m;
+    d = d * q.k + m;
+    acc = acc + (-d);
+    hx = hs[sh] - g.cn * acc;
+    // Hy: (x, Ez, -), (z, Ex, +, memory j1)
+    d = Ez[e + 1] - Ez[e];
+    acc = T(0);
+    acc = acc + (-d);
+    d = ec[e] - Ex[e];
+    m = o1 * q.b + q.c * d;
+    g.psiH[2][1][iz] = m;
+    d = d * q.k + m;
+    acc = acc + d;
+    hy = hs[HS + sh] - g.cn * acc;
+    // Hz: (x, Ey, +), (y, Ex, -)
+    d = Ey[e + 1] - Ey[e];
+    acc = T(0);
+    acc = acc + d;
+    d = Ex[e + kMarchLanes] - Ex[e];
+    acc = acc + (-d);
+    hz = hs[2 * HS + sh] - g.cn * acc;
+}
+
 // E_new of the three components of one cell on a row that is not on the fast path (general kernel).
 // Faces become selects (x / y / z > 0, or a periodic seam). CPML: the row meets a CPML slab; the old
 // memories of the cell's active slabs are loaded first, so their loads are in flight together, then
@@ -344,6 +420,11 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     using S = MarchShape<T, SAMPLES, D>;
     constexpr bool INTERIOR = MODE == 1;
     constexpr bool PXY = MODE == 2;
+    // Rows that meet only a z slab get their own tier (plain x / y differences, z memories) in the periodic
+    // x / y body, where such rows are most of the general work (CPML on z only): 0.575 against 0.612 ms per
+    // step at 512 x 512 x 128. With x / y slabs the general work is mostly x / y slab rows, and the extra tier
+    // cost the 512 x 512 x 256 CPML step 1.3 % (instruction cache).
+    constexpr bool ZTIER = MODE == 2;
     // The general body keeps its row loops rolled: unrolled, its three row tiers exist once per row and the
     // code outgrows the instruction cache once a pure body shares the SM (measured: 75 % vs 94 % hits).
     constexpr int kRowUnroll = INTERIOR ? kMarchRowsPerThread : 1;
@@ -549,10 +630,16 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                 const Rows<T> &rw = no_rows;
                 T ex, ey, ez;
                 const bool cpml_row = ((rowbits >> h) & 1u) || rzE >= 0;
-                if (INTERIOR || (!cpml_row && !((rowbits >> (R + h)) & 1u) && zprev && !smask)) {
+                const bool plain_xy = !((rowbits >> h) & 1u) && !((rowbits >> (R + h)) & 1u) && zprev && !smask;
+                if (INTERIOR || (!cpml_row && plain_xy)) {
                     ex = march_e_fast<T, SAMPLES, D, 0>(g, hk, hm, ek, sh, se);
                     ey = march_e_fast<T, SAMPLES, D, 1>(g, hk, hm, ek, sh, se);
                     ez = march_e_fast<T, SAMPLES, D, 2>(g, hk, hm, ek, sh, se);
+                } else if (ZTIER && plain_xy) {
+                    // Only the z slab: rzE >= 0.
+                    const int pz = args.psi_parity[2];
+                    march_e_zslab<T, SAMPLES, D>(g, hk, hm, ek, sh, se, (rzE * ny + yc) * g.pitch + xc, par ? pz : 0, par ? 0 : pz, own,
+                                                 coef_at(g, 0, 2, kz, rzE), ex, ey, ez);
                 } else if (!cpml_row) {
                     march_e_row<T, SAMPLES, D, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw, ex, ey, ez);
                 } else {
@@ -622,7 +709,11 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                 if constexpr (!INTERIOR) {
                     const bool xn = x < nx - 1 || px, yn = y < ny - 1 || py;
                     T hv[3];
-                    if (cpml_row) {
+                    if (ZTIER && !((rowbits >> (2 * R + h)) & 1u) && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask) {
+                        // Only the z slab: rzH >= 0.
+                        march_h_zslab<T, SAMPLES, D>(g, eprv, ecur, hs, sh, e, (rzH * ny + y) * g.pitch + x, coef_at(g, 1, 2, km, rzH),
+                                                     hv[0], hv[1], hv[2]);
+                    } else if (cpml_row) {
                         const int rx = TFD_SLAB_ROW(args, 1, 0, x), ry = TFD_SLAB_ROW(args, 1, 1, y);
                         march_h_row<T, SAMPLES, D, true>(g, eprv, ecur, hs, sh, e, x, y, km, xn, yn, znext, rx, ry, rzH,
                                                          coef_at(g, 1, 0, x, rx), coef_at(g, 1, 1, y, ry), coef_at(g, 1, 2, km, rzH),
