@@ -213,6 +213,40 @@ def test_interior_and_boundary_tiles_match_oracle(kernel, variant, precision):
         np.testing.assert_array_equal(got, want)
 
 
+@pytest.mark.parametrize('variant', [0, 314])
+@pytest.mark.parametrize('zmax', ['pml', 'pec'])
+@pytest.mark.parametrize('precision', ['float32', 'float64'])
+def test_interior_block_on_z_slab_and_z_face_planes_matches_oracle(variant, zmax, precision):
+    """The mixed launch's z-pure body: interior tiles on the chunks outside the pure z segment, with rows that
+    meet only a z slab, the z-face planes (PML or PEC above) and, with PEC above, sources on E and H in the
+    top plane."""
+    from torchfdtd_b200.models import BoundaryFace, Source, Structure
+    region = Region(dimension='3d', size=(5.0, 3.0, 1.5), mesh=.05, pml_cells=6, steps=20, precision=precision, backend='cuda')
+    if zmax == 'pec':
+        region.boundaries.z_max = BoundaryFace(kind='pec')
+    zs = .72 if zmax == 'pec' else .3               # with PEC above: the top plane, in the last z segment
+    project = Project(region=region, structures=[Structure(kind='sphere', radius=.6, material='Si (constant n)')],
+                      sources=[Source(center=(-.4, .1, zs), component='Ez', pulse_cycles=1, wavelength=1.0),
+                               Source(center=(.6, -.2, zs), component='Hx', pulse_cycles=1, wavelength=1.0, amplitude=.2)])
+    plan = plan_grid(project)
+    rng = np.random.default_rng(9)
+    oracle = YeeOracle(plan)
+    oracle.E[:] = rng.normal(size=oracle.E.shape).astype(plan.dtype) * .01
+    oracle.H[:] = rng.normal(size=oracle.H.shape).astype(plan.dtype) * .01
+    if variant and precision == 'float64':
+        variant = variant // 100 * 100 + 22
+    from torchfdtd_b200.native import NativeGrid
+    g = NativeGrid(plan, kernel='march', variant=variant)
+    g.set_fields(oracle.E, oracle.H)
+    oracle.run()
+    g.step(plan.steps)
+    E, H = g.get_fields()
+    np.testing.assert_array_equal(E, oracle.E)
+    np.testing.assert_array_equal(H, oracle.H)
+    for got, want in zip(g.get_psi(), oracle.memory_states):
+        np.testing.assert_array_equal(got, want)
+
+
 def seam_project(size, precision, sampling, steps=14):
     """Periodic x/y with z-CPML (the scene the reference's one-pass marching kernel admits), ragged tile
     counts, and sources on the seam cells (first column / row), which halo lanes recompute."""

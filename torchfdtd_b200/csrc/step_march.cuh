@@ -418,16 +418,19 @@ __device__ __forceinline__ void march_h_row(const Grid<T> &g, const T *ep, const
 template <typename T, int SAMPLES, int D, int MODE>
 __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int ty, int z0, int z1) {
     using S = MarchShape<T, SAMPLES, D>;
-    constexpr bool INTERIOR = MODE == 1;
+    // MODE 4 (z-pure) runs interior tiles (as MODE 1) on any planes: fast rows, rows that meet only a z slab,
+    // and the z-face planes on the edge path.
+    constexpr bool ZPURE = MODE == 4;
+    constexpr bool INTERIOR = MODE == 1 || ZPURE;
     constexpr bool PXY = MODE == 2;
     // Rows that meet only a z slab get their own tier (plain x / y differences, z memories) in the periodic
     // x / y body, where such rows are most of the general work (CPML on z only): 0.575 against 0.612 ms per
     // step at 512 x 512 x 128. With x / y slabs the general work is mostly x / y slab rows, and the extra tier
-    // cost the 512 x 512 x 256 CPML step 1.3 % (instruction cache).
-    constexpr bool ZTIER = MODE == 2;
+    // cost the 512 x 512 x 256 CPML step 1.3 % (instruction cache); there the z-pure body takes them.
+    constexpr bool ZTIER = MODE == 2 || ZPURE;
     // The general body keeps its row loops rolled: unrolled, its three row tiers exist once per row and the
     // code outgrows the instruction cache once a pure body shares the SM (measured: 75 % vs 94 % hits).
-    constexpr int kRowUnroll = INTERIOR ? kMarchRowsPerThread : 1;
+    constexpr int kRowUnroll = MODE == 1 ? kMarchRowsPerThread : 1;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
     const Grid<T> &g = args.g;
@@ -631,16 +634,17 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                 T ex, ey, ez;
                 const bool cpml_row = ((rowbits >> h) & 1u) || rzE >= 0;
                 const bool plain_xy = !((rowbits >> h) & 1u) && !((rowbits >> (R + h)) & 1u) && zprev && !smask;
-                if (INTERIOR || (!cpml_row && plain_xy)) {
+                const bool fast = MODE == 1 || (ZPURE ? rzE < 0 && zprev : !cpml_row && plain_xy);
+                if (fast) {
                     ex = march_e_fast<T, SAMPLES, D, 0>(g, hk, hm, ek, sh, se);
                     ey = march_e_fast<T, SAMPLES, D, 1>(g, hk, hm, ek, sh, se);
                     ez = march_e_fast<T, SAMPLES, D, 2>(g, hk, hm, ek, sh, se);
-                } else if (ZTIER && plain_xy) {
+                } else if (ZPURE ? zprev : ZTIER && plain_xy) {
                     // Only the z slab: rzE >= 0.
                     const int pz = args.psi_parity[2];
                     march_e_zslab<T, SAMPLES, D>(g, hk, hm, ek, sh, se, (rzE * ny + yc) * g.pitch + xc, par ? pz : 0, par ? 0 : pz, own,
                                                  coef_at(g, 0, 2, kz, rzE), ex, ey, ez);
-                } else if (!cpml_row) {
+                } else if (ZPURE || !cpml_row) {
                     march_e_row<T, SAMPLES, D, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw, ex, ey, ez);
                 } else {
                     const Rows<T> rc = e_rows(xc, yc, kz, rzE);
@@ -687,7 +691,8 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                 const int e = r * kMarchLanes + lane;
                 const int i = y * g.pitch + x;
                 const bool cpml_row = ((rowbits >> (2 * R + h)) & 1u) || rzH >= 0;
-                if (INTERIOR || (!cpml_row && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask)) {
+                const bool fast = MODE == 1 || (ZPURE ? rzH < 0 && znext : !cpml_row && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask);
+                if (fast) {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const Term t0 = term_of(c, 0), t1 = term_of(c, 1);
@@ -706,14 +711,15 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                     }
                     continue;
                 }
-                if constexpr (!INTERIOR) {
-                    const bool xn = x < nx - 1 || px, yn = y < ny - 1 || py;
+                if constexpr (!INTERIOR || ZPURE) {
+                    // Interior tiles have their +x / +y neighbours.
+                    const bool xn = ZPURE || x < nx - 1 || px, yn = ZPURE || y < ny - 1 || py;
                     T hv[3];
-                    if (ZTIER && !((rowbits >> (2 * R + h)) & 1u) && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask) {
+                    if (ZPURE ? znext : ZTIER && !((rowbits >> (2 * R + h)) & 1u) && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask) {
                         // Only the z slab: rzH >= 0.
                         march_h_zslab<T, SAMPLES, D>(g, eprv, ecur, hs, sh, e, (rzH * ny + y) * g.pitch + x, coef_at(g, 1, 2, km, rzH),
                                                      hv[0], hv[1], hv[2]);
-                    } else if (cpml_row) {
+                    } else if (!ZPURE && cpml_row) {
                         const int rx = TFD_SLAB_ROW(args, 1, 0, x), ry = TFD_SLAB_ROW(args, 1, 1, y);
                         march_h_row<T, SAMPLES, D, true>(g, eprv, ecur, hs, sh, e, x, y, km, xn, yn, znext, rx, ry, rzH,
                                                          coef_at(g, 1, 0, x, rx), coef_at(g, 1, 1, y, ry), coef_at(g, 1, 2, km, rzH),
@@ -748,8 +754,8 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
 }
 
 // One launch over every tile and z chunk in which each CTA takes the pure body (MODE 1) when its tile is in
-// the interior block [ix0, ix1) x [iy0, iy1) and its chunk in the pure z segment, else the general body
-// (GEN: 0, or 2 with periodic seams). The planes are cut into three segments, [zb0, zb1), [zb1, zb2) (the
+// the interior block [ix0, ix1) x [iy0, iy1) and its chunk in the pure z segment, the z-pure body (MODE 4)
+// for the interior block's other chunks, else the general body (GEN: 0, or 2 with periodic seams). The planes are cut into three segments, [zb0, zb1), [zb1, zb2) (the
 // pure one) and [zb2, zb3), chunked separately (chunks[s] of lz[s] planes; blockIdx.z runs over all).
 // The two bodies share no state inside the plane loop, so the pure one is compiled as lean as in its own
 // kernel, while its CTAs interleave with the general ones as in one launch.
@@ -770,8 +776,11 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march_mixed(const 
     const int z0 = mx.zb[seg] + zc * mx.lz[seg];
     const int z1 = min(z0 + mx.lz[seg], mx.zb[seg + 1]);
     const int tx = blockIdx.x, ty = blockIdx.y;
-    if (seg == 1 && tx >= mx.ix0 && tx < mx.ix1 && ty >= mx.iy0 && ty < mx.iy1)
+    const bool interior = tx >= mx.ix0 && tx < mx.ix1 && ty >= mx.iy0 && ty < mx.iy1;
+    if (interior && seg == 1)
         march_body<T, SAMPLES, D, 1>(args, tx, ty, z0, z1);
+    else if (interior)
+        march_body<T, SAMPLES, D, 4>(args, tx, ty, z0, z1);
     else
         march_body<T, SAMPLES, D, GEN>(args, tx, ty, z0, z1);
 }
