@@ -50,7 +50,7 @@ C0 = 299792458.0
 # (dram__bytes_read.sum + dram__bytes_write.sum of one launch / cells; profiles/ has the commands):
 # 512x512x256: 2.428 + 1.776 GB per k_step_march_mixed launch; batch64: 493.4 MB (k_step2d_interior) + 118.5 MB
 # (k_step2d_general) per step at the tuned launch shape.
-MEASURED_TRAFFIC_PER_CELL = {('roofline', 'march'): 4.204e9 / 67108864, ('batch64', 'tile2d'): 611.9e6 / 20187264}
+MEASURED_TRAFFIC_PER_CELL = {('roofline', 'march'): 4.218e9 / 67108864, ('batch64', 'tile2d'): 611.9e6 / 20187264}
 
 
 def baseline_face(layers):

@@ -1032,6 +1032,33 @@ int stage_in(tfd_plan *p, const void *src, size_t bytes, int where, cudaStream_t
     return TFD_OK;
 }
 
+// Blocks of the tiled layout conversions (one per 32 x 32 (x, z) tile of each y row), or 0 when the grid is
+// too thin in z for them or has more tiles than one launch holds.
+inline unsigned tiled_blocks(const tfd_desc &d) {
+    if (d.nz < kTileMinNz) return 0;
+    const long long b = (long long)((d.nx + kTile - 1) / kTile) * ((d.nz + kTile - 1) / kTile) * d.ny;
+    return b < (1ll << 31) ? (unsigned)b : 0u;
+}
+
+template <typename T>
+TileArrays<T> tile_arrays(T *a, T *b, T *c) {
+    TileArrays<T> t{};
+    for (int par = 0; par < 2; ++par) {
+        t.p[par][0] = a;
+        t.p[par][1] = b;
+        t.p[par][2] = c;
+    }
+    return t;
+}
+
+template <typename T>
+TileArrays<T> tile_arrays(const FieldSet<T> &fs, int family) {
+    TileArrays<T> t{};
+    for (int par = 0; par < 2; ++par)
+        for (int c = 0; c < 3; ++c) t.p[par][c] = fs.f[par][3 * family + c];
+    return t;
+}
+
 template <typename T>
 int set_material_t(tfd_plan *p, const void *src, int where, cudaStream_t s) {
     const tfd_desc &d = p->desc;
@@ -1041,9 +1068,14 @@ int set_material_t(tfd_plan *p, const void *src, int where, cudaStream_t s) {
     int rc = stage_in(p, src, bytes, where, s, &dev);
     if (rc) return rc;
     Grid<T> &g = p->grid<T>();
-    k_reference_to_internal<T><<<launch_blocks((long long)d.nx * d.ny * d.nz * S), 256, 0, s>>>(
-        (const T *)dev, S, d.nx, d.ny, d.nz, g.pitch, (T *)g.inv_eps[0], (T *)(S == 3 ? g.inv_eps[1] : nullptr),
-        (T *)(S == 3 ? g.inv_eps[2] : nullptr));
+    if (const unsigned tb = tiled_blocks(d))
+        k_from_reference_tiled<T, false><<<tb, kTileThreads, 0, s>>>(
+            (const T *)dev, tile_arrays<T>((T *)g.inv_eps[0], (T *)(S == 3 ? g.inv_eps[1] : nullptr), (T *)(S == 3 ? g.inv_eps[2] : nullptr)),
+            nullptr, S, d.nx, d.ny, d.nz, g.pitch, nullptr);
+    else
+        k_reference_to_internal<T><<<launch_blocks((long long)d.nx * d.ny * d.nz * S), 256, 0, s>>>(
+            (const T *)dev, S, d.nx, d.ny, d.nz, g.pitch, (T *)g.inv_eps[0], (T *)(S == 3 ? g.inv_eps[1] : nullptr),
+            (T *)(S == 3 ? g.inv_eps[2] : nullptr));
     TFD_CUDA(cudaGetLastError());
     if (where == TFD_HOST) TFD_CUDA(cudaStreamSynchronize(s));
     return TFD_OK;
@@ -1060,9 +1092,14 @@ int set_permittivity_t(tfd_plan *p, const void *src, int where, cudaStream_t s) 
     Grid<T> &g = p->grid<T>();
     int *bad = p->ptr<int>(p->L.check);
     TFD_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
-    k_permittivity_to_internal<T><<<launch_blocks((long long)d.nx * d.ny * d.nz * S), 256, 0, s>>>(
-        (const T *)dev, S, d.nx, d.ny, d.nz, g.pitch, (T *)g.inv_eps[0], (T *)(S == 3 ? g.inv_eps[1] : nullptr),
-        (T *)(S == 3 ? g.inv_eps[2] : nullptr), bad);
+    if (const unsigned tb = tiled_blocks(d))
+        k_from_reference_tiled<T, true><<<tb, kTileThreads, 0, s>>>(
+            (const T *)dev, tile_arrays<T>((T *)g.inv_eps[0], (T *)(S == 3 ? g.inv_eps[1] : nullptr), (T *)(S == 3 ? g.inv_eps[2] : nullptr)),
+            nullptr, S, d.nx, d.ny, d.nz, g.pitch, bad);
+    else
+        k_permittivity_to_internal<T><<<launch_blocks((long long)d.nx * d.ny * d.nz * S), 256, 0, s>>>(
+            (const T *)dev, S, d.nx, d.ny, d.nz, g.pitch, (T *)g.inv_eps[0], (T *)(S == 3 ? g.inv_eps[1] : nullptr),
+            (T *)(S == 3 ? g.inv_eps[2] : nullptr), bad);
     TFD_CUDA(cudaGetLastError());
     int flag = 0;
     TFD_CUDA(cudaMemcpyAsync(&flag, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1106,9 +1143,13 @@ int set_fields_t(tfd_plan *p, const void *E, const void *H, int where, cudaStrea
         const void *dev;
         int rc = stage_in(p, src, bytes, where, s, &dev);
         if (rc) return rc;
-        k_reference_to_fields<T><<<launch_blocks(total), 256, 0, s>>>(fam == 0 ? (const T *)dev : nullptr,
-                                                                       fam == 1 ? (const T *)dev : nullptr, d.nx, d.ny, d.nz,
-                                                                       p->L.pitch, fs, p->grid<T>().counter);
+        if (const unsigned tb = tiled_blocks(d))
+            k_from_reference_tiled<T, false><<<tb, kTileThreads, 0, s>>>((const T *)dev, tile_arrays<T>(fs, fam), p->grid<T>().counter, 3,
+                                                                         d.nx, d.ny, d.nz, p->L.pitch, nullptr);
+        else
+            k_reference_to_fields<T><<<launch_blocks(total), 256, 0, s>>>(fam == 0 ? (const T *)dev : nullptr,
+                                                                           fam == 1 ? (const T *)dev : nullptr, d.nx, d.ny, d.nz,
+                                                                           p->L.pitch, fs, p->grid<T>().counter);
         TFD_CUDA(cudaGetLastError());
         if (where == TFD_HOST) TFD_CUDA(cudaStreamSynchronize(s));
     }
@@ -1126,8 +1167,12 @@ int get_fields_t(tfd_plan *p, void *E, void *H, int where, cudaStream_t s) {
         if (!dst) continue;
         void *dev = where == TFD_DEVICE ? dst : p->arena + p->L.stage;
         if (where == TFD_HOST && bytes > p->L.stage_bytes) return fail(TFD_ERR_INVALID, "transfer larger than the stage buffer");
-        k_fields_to_reference<T><<<launch_blocks(total), 256, 0, s>>>(fam == 0 ? (T *)dev : nullptr, fam == 1 ? (T *)dev : nullptr,
-                                                                       d.nx, d.ny, d.nz, p->L.pitch, fs, p->grid<T>().counter);
+        if (const unsigned tb = tiled_blocks(d))
+            k_to_reference_tiled<T><<<tb, kTileThreads, 0, s>>>((T *)dev, tile_arrays<T>(fs, fam), p->grid<T>().counter, 3, d.nx, d.ny,
+                                                                d.nz, p->L.pitch);
+        else
+            k_fields_to_reference<T><<<launch_blocks(total), 256, 0, s>>>(fam == 0 ? (T *)dev : nullptr, fam == 1 ? (T *)dev : nullptr,
+                                                                           d.nx, d.ny, d.nz, p->L.pitch, fs, p->grid<T>().counter);
         TFD_CUDA(cudaGetLastError());
         if (where == TFD_HOST) {
             TFD_CUDA(cudaMemcpyAsync(dst, dev, bytes, cudaMemcpyDeviceToHost, s));
@@ -1919,8 +1964,12 @@ int adjoint_sensitivity_t(tfd_adjoint *adj, void *dst, int where, cudaStream_t s
         TFD_CUDA(cudaMallocAsync((void **)&staging, bytes, s));
         out = staging;
     }
-    k_internal_to_reference<T><<<launch_blocks((long long)d.nx * d.ny * d.nz * 3), 256, 0, s>>>(out, 3, d.nx, d.ny, d.nz,
-                                                                                            p->L.pitch, A.S[0], A.S[1], A.S[2]);
+    if (const unsigned tb = tiled_blocks(d))
+        k_to_reference_tiled<T><<<tb, kTileThreads, 0, s>>>(out, tile_arrays<T>(A.S[0], A.S[1], A.S[2]), nullptr, 3, d.nx, d.ny, d.nz,
+                                                            p->L.pitch);
+    else
+        k_internal_to_reference<T><<<launch_blocks((long long)d.nx * d.ny * d.nz * 3), 256, 0, s>>>(out, 3, d.nx, d.ny, d.nz,
+                                                                                                p->L.pitch, A.S[0], A.S[1], A.S[2]);
     TFD_CUDA(cudaGetLastError());
     if (staging) {
         TFD_CUDA(cudaMemcpyAsync(dst, staging, bytes, cudaMemcpyDeviceToHost, s));

@@ -181,6 +181,95 @@ __global__ void k_internal_to_reference(T *__restrict__ dst, int S, int nx, int 
 template <typename T>
 struct FieldSet { T *f[2][6]; };
 
+// ---- tiled layout conversion ---------------------------------------------------------------------
+// The reference layout is z (then sample) fastest, the internal one x fastest: converting is a transpose of
+// (x, z) for every y. A block of kTileThreads takes a 32 x 32 (x, z) tile of one y row through shared memory,
+// so both sides move in coalesced runs: internal rows of 32 x values, reference runs of 32 * S values per x.
+// Used when nz >= kTileMinNz (below it a tile would be mostly empty); the grid-stride kernels above serve the
+// rest. Arrays: [parity][sample], parity from *counter (or 0 without a counter); a null array reads as zero
+// and ignores writes.
+constexpr int kTile = 32;
+constexpr int kTileThreads = 256;
+constexpr int kTileMinNz = 16;
+constexpr int kTileStride = kTile * (kTile + 1) + 1;          // per sample; +1 keeps the samples' banks apart
+
+template <typename T>
+struct TileArrays { T *p[2][3]; };
+
+__device__ __forceinline__ void tile_coords(int nx, int nz, int &x0, int &z0, int &y) {
+    const int tx = (nx + kTile - 1) / kTile, tz = (nz + kTile - 1) / kTile;
+    int b = blockIdx.x;
+    x0 = (b % tx) * kTile;
+    b /= tx;
+    z0 = (b % tz) * kTile;
+    y = b / tz;
+}
+
+// Internal -> reference: dst (nx, ny, nz, S) from src[parity][s] ([nz][ny][pitch]).
+template <typename T>
+__global__ void __launch_bounds__(kTileThreads) k_to_reference_tiled(T *__restrict__ dst, const __grid_constant__ TileArrays<T> src,
+                                                                    const long long *counter, int S, int nx, int ny, int nz,
+                                                                    int pitch) {
+    __shared__ T tile[3 * kTileStride];
+    int x0, z0, y;
+    tile_coords(nx, nz, x0, z0, y);
+    const int par = counter ? (int)(*counter & 1) : 0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = kTileThreads / 32;
+    const int x = x0 + lane;
+    for (int s = 0; s < S; ++s) {
+        const T *a = src.p[par][s];
+        for (int zz = w; zz < kTile; zz += nw) {
+            const int z = z0 + zz;
+            tile[s * kTileStride + zz * (kTile + 1) + lane] = (a && z < nz && x < nx) ? a[((long long)z * ny + y) * pitch + x] : T(0);
+        }
+    }
+    __syncthreads();
+    const int run = min(kTile, nz - z0) * S;
+    for (int xx = w; xx < kTile && x0 + xx < nx; xx += nw) {
+        T *out = dst + (((long long)(x0 + xx) * ny + y) * nz + z0) * S;
+        for (int q = lane; q < run; q += 32) {
+            const int zz = q / S, s = q - zz * S;
+            out[q] = tile[s * kTileStride + zz * (kTile + 1) + xx];
+        }
+    }
+}
+
+// Reference -> internal: dst[parity][s] from src (nx, ny, nz, S). INVERT: the source is the permittivity;
+// 1 / eps (IEEE division) is stored and *bad set when a value is not finite or below 1.
+template <typename T, bool INVERT>
+__global__ void __launch_bounds__(kTileThreads) k_from_reference_tiled(const T *__restrict__ src, const __grid_constant__ TileArrays<T> dst,
+                                                                      const long long *counter, int S, int nx, int ny, int nz,
+                                                                      int pitch, int *bad) {
+    __shared__ T tile[3 * kTileStride];
+    int x0, z0, y;
+    tile_coords(nx, nz, x0, z0, y);
+    const int par = counter ? (int)(*counter & 1) : 0;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = kTileThreads / 32;
+    const int zn = min(kTile, nz - z0), run = zn * S;
+    bool wrong = false;
+    for (int xx = w; xx < kTile && x0 + xx < nx; xx += nw) {
+        const T *in = src + (((long long)(x0 + xx) * ny + y) * nz + z0) * S;
+        for (int q = lane; q < run; q += 32) {
+            const int zz = q / S, s = q - zz * S;
+            T v = in[q];
+            if (INVERT) {
+                wrong |= !(v >= T(1)) || !isfinite(v);
+                v = T(1) / v;
+            }
+            tile[s * kTileStride + zz * (kTile + 1) + xx] = v;
+        }
+    }
+    if (INVERT && wrong) atomicExch(bad, 1);
+    __syncthreads();
+    const int x = x0 + lane;
+    if (x >= nx) return;
+    for (int s = 0; s < S; ++s) {
+        T *a = dst.p[par][s];
+        if (!a) continue;
+        for (int zz = w; zz < zn; zz += nw) a[((long long)(z0 + zz) * ny + y) * pitch + x] = tile[s * kTileStride + zz * (kTile + 1) + lane];
+    }
+}
+
 // The largest |E| and whether any E or H value of the current parity is not finite. out[0]: the bit pattern of
 // the largest |E| (non-negative values order like their bit patterns); out[1]: 1 when a value is NaN or
 // infinite. Both start at zero.
