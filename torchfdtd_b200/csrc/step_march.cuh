@@ -201,71 +201,90 @@ __device__ __forceinline__ T march_e_fast(const Grid<T> &g, const T *hk, const T
     return ek[C * ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? C : 0)) * ES + se]) * acc;
 }
 
-// E_new of one cell on a z-slab row (general kernel): the row meets no x / y slab, domain face or source and
-// plane z has a previous plane, but z lies in a z slab. The x / y terms are plain differences, the z terms of
-// Ex and Ey go through the z memories (old at po + iz, new at pn + iz, stored by the owner); the terms and
-// their order are those of march_e_row on such a row.
+// E_new of one cell on a z row (general and z-pure bodies): the row meets no x / y slab, x / y face or source.
+// The x / y terms are plain differences. The z terms of Ex and Ey: zero on the first plane of a grid without
+// a previous plane (zprev false), through the z memories when zm (z in a z slab and zprev; old at po + iz,
+// new at pn + iz, stored by the owner). The terms and their order are those of march_e_row on such a row.
 template <typename T, int SAMPLES, int D>
-__device__ __forceinline__ void march_e_zslab(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, int iz, int po,
-                                              int pn, bool own, const Coef<T> &q, T &ex, T &ey, T &ez) {
+__device__ __forceinline__ void march_e_zslab(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, bool zprev,
+                                              bool zm, int iz, int po, int pn, bool own, const Coef<T> &q, T &ex, T &ey, T &ez) {
     using S = MarchShape<T, SAMPLES, D>;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
-    const T o0 = g.psiE[0][2][0][po + iz], o1 = g.psiE[0][2][1][po + iz];
+    T o0 = T(0), o1 = T(0);
+    if (zm) {
+        o0 = g.psiE[0][2][0][po + iz];
+        o1 = g.psiE[0][2][1][po + iz];
+    }
     const T *Hx = hk, *Hy = hk + HS, *Hz = hk + 2 * HS;
     T d, acc, m;
     // Ex: (y, Hz, +), (z, Hy, -, memory j0)
     d = Hz[s] - Hz[s - S::BXW];
     acc = T(0);
     acc = acc + d;
-    d = Hy[s] - hm[HS + s];
-    m = o0 * q.b + q.c * d;
-    if (own) g.psiE[0][2][0][pn + iz] = m;
-    d = d * q.k + m;
+    d = zprev ? Hy[s] - hm[HS + s] : T(0);
+    if (zm) {
+        m = o0 * q.b + q.c * d;
+        if (own) g.psiE[0][2][0][pn + iz] = m;
+        d = d * q.k + m;
+    }
     acc = acc + (-d);
     ex = ek[se] + (g.cn * ek[3 * ES + se]) * acc;
     // Ey: (x, Hz, -), (z, Hx, +, memory j1)
     d = Hz[s] - Hz[s - 1];
     acc = T(0);
     acc = acc + (-d);
-    d = Hx[s] - hm[s];
-    m = o1 * q.b + q.c * d;
-    if (own) g.psiE[0][2][1][pn + iz] = m;
-    d = d * q.k + m;
+    d = zprev ? Hx[s] - hm[s] : T(0);
+    if (zm) {
+        m = o1 * q.b + q.c * d;
+        if (own) g.psiE[0][2][1][pn + iz] = m;
+        d = d * q.k + m;
+    }
     acc = acc + d;
     ey = ek[ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? 1 : 0)) * ES + se]) * acc;
     ez = march_e_fast<T, SAMPLES, D, 2>(g, hk, hm, ek, s, se);
 }
 
-// H_new of one owned cell on a z-slab row: no x / y slab, face or source, plane km + 1 computed, km in a z slab
-// of the H family (memories at iz, updated in place); the terms and their order are those of march_h_row.
+// H_new of one owned cell on a z row: no x / y slab, x / y face or source. The z terms: the difference to plane
+// km + 1 when znext, else the PEC ghost term or 0 (the last plane of a grid without a next plane); through the
+// H-family z memories (at iz, updated in place) when zm (km in a z slab and znext). The terms and their order
+// are those of march_h_row.
 template <typename T, int SAMPLES, int D>
-__device__ __forceinline__ void march_h_zslab(const Grid<T> &g, const T *ep, const T *ec, const T *hs, int sh, int e, int iz,
-                                              const Coef<T> &q, T &hx, T &hy, T &hz) {
+__device__ __forceinline__ void march_h_zslab(const Grid<T> &g, const T *ep, const T *ec, const T *hs, int sh, int e, bool znext,
+                                              bool zm, int iz, const Coef<T> &q, T &hx, T &hy, T &hz) {
     using S = MarchShape<T, SAMPLES, D>;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int EB = S::EBUF;
-    const T o0 = g.psiH[2][0][iz], o1 = g.psiH[2][1][iz];
+    T o0 = T(0), o1 = T(0);
+    if (zm) {
+        o0 = g.psiH[2][0][iz];
+        o1 = g.psiH[2][1][iz];
+    }
     const T *Ex = ep, *Ey = ep + EB, *Ez = ep + 2 * EB;
+    auto dz = [&](int c) -> T { return znext ? ec[c * EB + e] - ep[c * EB + e] : (g.pec_on[2] ? g.pec_neg[2] * ep[c * EB + e] : T(0)); };
     T d, acc, m;
     // Hx: (y, Ez, +), (z, Ey, -, memory j0)
     d = Ez[e + kMarchLanes] - Ez[e];
     acc = T(0);
     acc = acc + d;
-    d = ec[EB + e] - Ey[e];
-    m = o0 * q.b + q.c * d;
-    g.psiH[2][0][iz] = m;
-    d = d * q.k + m;
+    d = dz(1);
+    if (zm) {
+        m = o0 * q.b + q.c * d;
+        g.psiH[2][0][iz] = m;
+        d = d * q.k + m;
+    }
     acc = acc + (-d);
     hx = hs[sh] - g.cn * acc;
     // Hy: (x, Ez, -), (z, Ex, +, memory j1)
     d = Ez[e + 1] - Ez[e];
     acc = T(0);
     acc = acc + (-d);
-    d = ec[e] - Ex[e];
-    m = o1 * q.b + q.c * d;
-    g.psiH[2][1][iz] = m;
-    d = d * q.k + m;
+    d = dz(0);
+    if (zm) {
+        m = o1 * q.b + q.c * d;
+        g.psiH[2][1][iz] = m;
+        d = d * q.k + m;
+    }
     acc = acc + d;
     hy = hs[HS + sh] - g.cn * acc;
     // Hz: (x, Ey, +), (y, Ex, -)
@@ -418,8 +437,8 @@ __device__ __forceinline__ void march_h_row(const Grid<T> &g, const T *ep, const
 template <typename T, int SAMPLES, int D, int MODE>
 __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int ty, int z0, int z1) {
     using S = MarchShape<T, SAMPLES, D>;
-    // MODE 4 (z-pure) runs interior tiles (as MODE 1) on any planes: fast rows, rows that meet only a z slab,
-    // and the z-face planes on the edge path.
+    // MODE 4 (z-pure) runs interior tiles (as MODE 1) on any planes: fast rows, and z rows (a z slab, or the
+    // first / last plane of a grid with z faces) in march_e_zslab / march_h_zslab.
     constexpr bool ZPURE = MODE == 4;
     constexpr bool INTERIOR = MODE == 1 || ZPURE;
     constexpr bool PXY = MODE == 2;
@@ -639,12 +658,12 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                     ex = march_e_fast<T, SAMPLES, D, 0>(g, hk, hm, ek, sh, se);
                     ey = march_e_fast<T, SAMPLES, D, 1>(g, hk, hm, ek, sh, se);
                     ez = march_e_fast<T, SAMPLES, D, 2>(g, hk, hm, ek, sh, se);
-                } else if (ZPURE ? zprev : ZTIER && plain_xy) {
-                    // Only the z slab: rzE >= 0.
+                } else if (ZPURE || (ZTIER && plain_xy)) {
+                    // A z-slab row (rzE >= 0), or in the z-pure body also the first plane of the grid (!zprev).
                     const int pz = args.psi_parity[2];
-                    march_e_zslab<T, SAMPLES, D>(g, hk, hm, ek, sh, se, (rzE * ny + yc) * g.pitch + xc, par ? pz : 0, par ? 0 : pz, own,
-                                                 coef_at(g, 0, 2, kz, rzE), ex, ey, ez);
-                } else if (ZPURE || !cpml_row) {
+                    march_e_zslab<T, SAMPLES, D>(g, hk, hm, ek, sh, se, zprev, zprev && rzE >= 0, (rzE * ny + yc) * g.pitch + xc,
+                                                 par ? pz : 0, par ? 0 : pz, own, coef_at(g, 0, 2, kz, rzE), ex, ey, ez);
+                } else if (!cpml_row) {
                     march_e_row<T, SAMPLES, D, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw, ex, ey, ez);
                 } else {
                     const Rows<T> rc = e_rows(xc, yc, kz, rzE);
@@ -715,11 +734,11 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                     // Interior tiles have their +x / +y neighbours.
                     const bool xn = ZPURE || x < nx - 1 || px, yn = ZPURE || y < ny - 1 || py;
                     T hv[3];
-                    if (ZPURE ? znext : ZTIER && !((rowbits >> (2 * R + h)) & 1u) && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask) {
-                        // Only the z slab: rzH >= 0.
-                        march_h_zslab<T, SAMPLES, D>(g, eprv, ecur, hs, sh, e, (rzH * ny + y) * g.pitch + x, coef_at(g, 1, 2, km, rzH),
-                                                     hv[0], hv[1], hv[2]);
-                    } else if (!ZPURE && cpml_row) {
+                    if (ZPURE || (ZTIER && !((rowbits >> (2 * R + h)) & 1u) && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask)) {
+                        // A z-slab row (rzH >= 0), or in the z-pure body also the last plane of the grid (!znext).
+                        march_h_zslab<T, SAMPLES, D>(g, eprv, ecur, hs, sh, e, znext, znext && rzH >= 0, (rzH * ny + y) * g.pitch + x,
+                                                     coef_at(g, 1, 2, km, rzH), hv[0], hv[1], hv[2]);
+                    } else if (cpml_row) {
                         const int rx = TFD_SLAB_ROW(args, 1, 0, x), ry = TFD_SLAB_ROW(args, 1, 1, y);
                         march_h_row<T, SAMPLES, D, true>(g, eprv, ecur, hs, sh, e, x, y, km, xn, yn, znext, rx, ry, rzH,
                                                          coef_at(g, 1, 0, x, rx), coef_at(g, 1, 1, y, ry), coef_at(g, 1, 2, km, rzH),
