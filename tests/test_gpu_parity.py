@@ -462,13 +462,14 @@ def test_device_permittivity_inversion_and_field_check(precision):
 
 def test_simulation_device_material_and_checks_equal_host_path(monkeypatch):
     """Simulation(project, epsilon).run() through the large-grid path (device permittivity inversion, device
-    field check, staged download) returns the host path's fields, traces and peak."""
+    field check, result arrays prepared on a helper thread, staged download), with CUDA graphs, returns the
+    host path's fields, traces and peak."""
     import torchfdtd_b200.simulation as sim
     project = random_project('3d', 'float32', steps=16)
     eps = np.asarray(plan_grid(project).epsilon, np.float32)
     want = sim.Simulation(project, epsilon=eps).run(cuda_graph=False)
     monkeypatch.setattr(sim, 'LARGE_FIELD_BYTES', 0)
-    got = sim.Simulation(project, epsilon=eps).run(cuda_graph=False)
+    got = sim.Simulation(project, epsilon=eps).run(cuda_graph=True, cuda_graph_steps=4)
     np.testing.assert_array_equal(got.electric, want.electric)
     np.testing.assert_array_equal(got.magnetic, want.magnetic)
     np.testing.assert_array_equal(got.signals, want.signals)

@@ -192,6 +192,7 @@ class Observer:
         self.eps_plane = np.array(self.decimate(np.asarray(plane, dtype=plan.dtype)))
         self.interval = max(r.snapshot_interval, math.ceil(r.steps / 100))
         self.frames, self.frame_steps = [], []
+        self.host_fields = None                     # future of prefaulted (E, H) host arrays, large grids
         self.diagnostic_seconds = 0.
 
     @staticmethod
@@ -236,6 +237,10 @@ class Observer:
                           'diagnostics': self.decision.history[-1] if self.decision.history else None})
         return stop
 
+    def large_fields(self):
+        """Whether the field arrays take the device-side checks and the staged download."""
+        return math.prod(self.plan.shape) * 3 * np.dtype(self.plan.dtype).itemsize > LARGE_FIELD_BYTES
+
     def result(self, completed, termination_reason, seconds, setup_seconds, **extra):
         """Read the final state back and package it as the reference's ``Result``."""
         import torch
@@ -244,7 +249,7 @@ class Observer:
         status = grid.device_status()
         if status:
             raise RuntimeError(self._where(f'A fused kernel reported device status {status}.'))
-        if math.prod(plan.shape) * 3 * np.dtype(plan.dtype).itemsize > LARGE_FIELD_BYTES:
+        if self.large_fields():
             # Large grids: finiteness and the peak are checked on the device, and the fields come back through
             # a pinned staging ring (native.download). Small grids keep the host path, whose fixed costs are
             # lower than the first use of the device reductions.
@@ -252,7 +257,8 @@ class Observer:
             if not finite:
                 raise FloatingPointError(self._where('Non-finite fields detected.'))
             e_dev, h_dev = grid.fields_device()
-            e, h = download(e_dev), download(h_dev)
+            e_out, h_out = self.host_fields.result() if self.host_fields is not None else (None, None)
+            e, h = download(e_dev, out=e_out), download(h_dev, out=h_out)
             del e_dev, h_dev
         else:
             e, h = grid.get_fields()
@@ -401,6 +407,16 @@ class Simulation:
                 graphs = capture_graphs(lambda count: grid.step(count, stream), {1, width})
             torch.cuda.synchronize()
         torch.cuda.synchronize()
+        helper = None
+        if observer.large_fields():
+            # The result's host arrays are mapped and the download's staging ring pinned on a helper thread
+            # while the device steps (after graph capture: pinning memory during a capture would end it).
+            from concurrent.futures import ThreadPoolExecutor
+            from .native import host_buffer, staging_ring
+            helper = ThreadPoolExecutor(max_workers=1)
+            shape, dtype = (*plan.shape, 3), np.dtype(plan.dtype)
+            observer.host_fields = helper.submit(
+                lambda: (staging_ring(grid.torch_dtype), (host_buffer(shape, dtype), host_buffer(shape, dtype)))[1])
         setup_seconds = time.perf_counter() - started
         compute_start = time.perf_counter()
         completed, termination_reason, replays = 0, 'max_steps', 0
@@ -425,4 +441,6 @@ class Simulation:
                                  launch_variant=variant or None,
                                  launch_tuning=tuning.as_dict() if hasattr(tuning, 'as_dict') else tuning)
         grid.close()
+        if helper is not None:
+            helper.shutdown()
         return result
