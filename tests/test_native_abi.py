@@ -115,3 +115,19 @@ def test_no_gpu_means_a_loud_error_not_a_fallback(monkeypatch):
         Simulation(p).run()
     with pytest.raises(RuntimeError, match='CUDA'):
         native.NativeGrid(plan_grid(p))
+
+
+def test_host_buffer_and_download_into_a_given_array():
+    """The helpers of the large-grid result path: host_buffer returns a writable C-contiguous array of the
+    requested shape and dtype (every page touched), and download(out=...) fills that array or refuses one of
+    the wrong shape, dtype or layout. A CPU tensor takes the plain-copy branch here."""
+    import torch
+    a = native.host_buffer((5, 7, 300, 3), np.float32, slab_bytes=4096)
+    assert a.shape == (5, 7, 300, 3) and a.dtype == np.float32 and a.flags.c_contiguous and a.flags.writeable
+    t = torch.arange(a.size, dtype=torch.float32).reshape(a.shape)
+    assert native.download(t, out=a) is a
+    np.testing.assert_array_equal(a, t.numpy())
+    for wrong in (np.empty((5, 7, 300, 3), np.float64), np.empty((5, 7, 299, 3), np.float32),
+                  np.empty((3, 300, 7, 5), np.float32).T):
+        with pytest.raises(ValueError, match='out must be'):
+            native.download(t, out=wrong)
