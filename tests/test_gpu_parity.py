@@ -247,6 +247,35 @@ def test_interior_block_on_z_slab_and_z_face_planes_matches_oracle(variant, zmax
         np.testing.assert_array_equal(got, want)
 
 
+@pytest.mark.parametrize('zfaces', ['periodic', 'pec'])
+def test_interior_block_with_periodic_or_pec_z_faces_matches_oracle(zfaces):
+    """The mixed launch on a grid with interior tiles and no z slab: the first and last planes (periodic: with
+    the wrapped neighbour plane; PEC: the H ghost above, no previous plane below) run the z-pure body, with
+    sources on E and H in the first plane."""
+    from torchfdtd_b200.models import BoundaryFace, Source, Structure
+    region = Region(dimension='3d', size=(5.0, 3.0, 1.5), mesh=.05, pml_cells=6, steps=18, precision='float32', backend='cuda')
+    region.boundaries.z_min = BoundaryFace(kind=zfaces)
+    region.boundaries.z_max = BoundaryFace(kind=zfaces)
+    project = Project(region=region, structures=[Structure(kind='sphere', radius=.6, material='Si (constant n)')],
+                      sources=[Source(center=(-.4, .1, -.73), component='Ez', pulse_cycles=1, wavelength=1.0),
+                               Source(center=(.6, -.2, -.73), component='Hy', pulse_cycles=1, wavelength=1.0, amplitude=.2)])
+    plan = plan_grid(project)
+    assert not [s for s in plan.segments if s.axis == 2]
+    rng = np.random.default_rng(13)
+    oracle = YeeOracle(plan)
+    oracle.E[:] = rng.normal(size=oracle.E.shape).astype(plan.dtype) * .01
+    oracle.H[:] = rng.normal(size=oracle.H.shape).astype(plan.dtype) * .01
+    g = native(plan, 'march')
+    g.set_fields(oracle.E, oracle.H)
+    oracle.run()
+    g.step(plan.steps)
+    E, H = g.get_fields()
+    np.testing.assert_array_equal(E, oracle.E)
+    np.testing.assert_array_equal(H, oracle.H)
+    for got, want in zip(g.get_psi(), oracle.memory_states):
+        np.testing.assert_array_equal(got, want)
+
+
 def seam_project(size, precision, sampling, steps=14):
     """Periodic x/y with z-CPML (the scene the reference's one-pass marching kernel admits), ragged tile
     counts, and sources on the seam cells (first column / row), which halo lanes recompute."""
