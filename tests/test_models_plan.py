@@ -26,7 +26,7 @@ def test_every_golden_project_round_trips_through_json():
 def test_reference_demo_projects_load_when_the_reference_tree_is_present():
     root = Path('/root/reference/tests/fixtures/projects')
     if not root.exists():
-        pytest.skip('reference tree not present (GPU box)')
+        pytest.skip('reference tree not present')
     for name in ('demo_3d.json', 'demo_waveguide.json', 'demo_scatterer.json', 'minimal_defaults.json', 'tiny_result.json'):
         p = Project.load(root / name)
         assert p.region.shape

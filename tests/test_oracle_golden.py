@@ -76,7 +76,7 @@ def test_reference_fixture_itself_when_the_reference_tree_is_present():
     """The reference's own golden result (tests/fixtures/npz/tiny_2d_complete.npz), read in place."""
     root = Path('/root/reference/tests/fixtures')
     if not root.exists():
-        pytest.skip('reference tree not present (GPU box)')
+        pytest.skip('reference tree not present')
     p = Project.load(root / 'projects' / 'tiny_result.json')
     d = np.load(root / 'npz' / 'tiny_2d_complete.npz')
     o = YeeOracle(plan_grid(p)).run()
