@@ -431,7 +431,8 @@ __device__ __forceinline__ void march_h_row(const Grid<T> &g, const T *ep, const
 // slab, and over planes whose chunks (with their halo plane) meet no z slab of either family, and the
 // general kernel over the rest; compiled without the face and CPML code, the fast path gets the whole
 // 64-register budget. MODE 2 is MODE 0 with periodic x / y seams (the host launches it when the grid has
-// them). Tile (tx, ty) of a launch is (blockIdx.x + tx_off, blockIdx.y + ty_off); chunk blockIdx.z
+// them). MODE 4 (z-pure) takes the same interior tiles on the other planes (k_step_march_mixed only): fast
+// rows, and z rows in march_e_zslab / march_h_zslab. Tile (tx, ty) of a launch is (blockIdx.x + tx_off, blockIdx.y + ty_off); chunk blockIdx.z
 // covers planes [z_lo + blockIdx.z * lz, min(that + lz, z_hi)).
 // The body of one CTA: tile (tx, ty), planes [z0, z1).
 template <typename T, int SAMPLES, int D, int MODE>
@@ -447,8 +448,9 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     // step at 512 x 512 x 128. With x / y slabs the general work is mostly x / y slab rows, and the extra tier
     // cost the 512 x 512 x 256 CPML step 1.3 % (instruction cache); there the z-pure body takes them.
     constexpr bool ZTIER = MODE == 2 || ZPURE;
-    // The general body keeps its row loops rolled: unrolled, its three row tiers exist once per row and the
-    // code outgrows the instruction cache once a pure body shares the SM (measured: 75 % vs 94 % hits).
+    // The general and z-pure bodies keep their row loops rolled: unrolled, the general body's three row tiers
+    // exist once per row and the code outgrows the instruction cache once a pure body shares the SM
+    // (measured: 75 % vs 94 % hits).
     constexpr int kRowUnroll = MODE == 1 ? kMarchRowsPerThread : 1;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
