@@ -1,7 +1,8 @@
 """Benchmark of the fused Yee/CPML engine: Gcell-updates/s and HBM-roofline fraction.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload roofline|roofline256|strip|periodic|tmz2d|batch64|adjoint3d|surrogate]
+                    [--workload roofline|roofline256|strip|periodic|tmz2d|batch64|adjoint3d|surrogate|
+                                adjoint_probe|surrogate_kernels]
 
 Workload (default ``roofline``): 3D full-vector Yee + CPML, FP32, 512 x 512 x 256 cells
 at 0.05 um, CPML 12 cells per face (cubic grading, sigma_max = 0.8 (m+1)/(eta0 dx),
@@ -50,6 +51,7 @@ C0 = 299792458.0
 # (dram__bytes_read.sum + dram__bytes_write.sum of one launch / cells; profiles/ has the commands):
 # 512x512x256: 2.428 + 1.776 GB per k_step_march_mixed launch; batch64: 493.4 MB (k_step2d_interior) + 118.5 MB
 # (k_step2d_general) per step at the tuned launch shape.
+L2_NOTE = 'inputs larger than L2 (no flush needed)'
 MEASURED_TRAFFIC_PER_CELL = {('roofline', 'march'): 4.218e9 / 67108864, ('batch64', 'tile2d'): 611.9e6 / 20187264}
 
 
@@ -286,8 +288,8 @@ def run_reference(args, world, rank):
               f'(C port of the reference NumPy Yee/CPML update, bitwise equal to it), after 1 warm-up step')
     line = dict(metric=METRIC, value=rate, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=elapsed / steps * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
-                data='synthetic', impl='reference',
-                config=dict(workload=desc, cells=plan.cells, parallelism='host threads'),
+                data='synthetic', impl='reference', parallelism='host threads',
+                config=dict(workload=desc, cells=plan.cells, l2=L2_NOTE),
                 cpu_baseline=dict(value=rate, unit=METRIC, cores=threads, kind='port', sample=sample),
                 e2e=dict(value=rate, unit=METRIC, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     return line
@@ -355,14 +357,16 @@ def run_ours(args, world, rank, local):
         real = np.dtype(plan.dtype).itemsize
         h2d = cells * plan.material_samples * real + sum(t.values.nbytes for t in plan.sources)
         d2h = result.electric.nbytes + result.magnetic.nbytes + result.signals.nbytes + result.frames.nbytes
+        phases = dict(result.summary.get('phase_seconds', {}))
+        phases['outside_phases'] = e2e_s - sum(phases.values())
         e2e = dict(value=world * cells * e2e_steps / e2e_s / 1e9, unit=METRIC, h2d_bytes_per_step=h2d / e2e_steps,
                    d2h_bytes_per_step=d2h / e2e_steps, seconds=e2e_s, steps=e2e_steps,
+                   breakdown_s={k: round(v, 4) for k, v in phases.items()},
                    call='Simulation(project, epsilon).run(cuda_graph=True, cuda_graph_steps=16)')
     line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=elapsed / args.steps * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
-                data='synthetic (seeded)', config=dict(workload=desc, cells=cells, l2='inputs larger than L2 (no flush needed)',
-                                                       parallelism=f'replicas x{world}' if world > 1 else 'single GPU',
-                                                       kernel=kernel_used),
+                data='synthetic (seeded)', config=dict(workload=desc, cells=cells, l2=L2_NOTE),
+                parallelism=f'replicas x{world}' if world > 1 else 'single GPU', kernel=kernel_used,
                 roofline=roofline, e2e=e2e, clocks=clocks, gpu_launches=launches, device_status=status)
     if args.workload == 'periodic':
         line['restated_reference'] = time_restated_marching(plan, args, device, bytes_step, peak)
@@ -442,8 +446,8 @@ def run_reference_batch(args, world, rank):
               f'host threads (C port of the reference NumPy Yee/CPML update), {elapsed:.1f} s')
     return dict(metric=METRIC, value=rate, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=sum(p.cells for p in plans) / rate / 1e6, higher_is_better=True, scaling='weak',
-                vs_baseline=None, dtype='f32', data='synthetic', impl='reference',
-                config=dict(workload=desc, cells=sum(p.cells for p in plans), parallelism='host threads'),
+                vs_baseline=None, dtype='f32', data='synthetic', impl='reference', parallelism='host threads',
+                config=dict(workload=desc, cells=sum(p.cells for p in plans), l2=L2_NOTE),
                 cpu_baseline=dict(value=rate, unit=METRIC, cores=threads, kind='port', sample=sample),
                 e2e=dict(value=rate, unit=METRIC, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
 
@@ -525,11 +529,11 @@ def run_ours_batch(args, world, rank, local):
     line = dict(metric=METRIC, value=value, unit=METRIC, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=elapsed / args.steps * 1e3, higher_is_better=True, scaling='weak', vs_baseline=None, dtype='f32',
                 data='synthetic (seeded)',
-                config=dict(workload=desc, cells=cells, grids=len(plans), strips=tiles, launch=choice,
-                            tuning=[(r['ctas'], r['rows'], r['strips'], round(r['median_ms_per_step'], 5))
-                                    for r in tuning.candidates] if tuning else 'fixed by --batch-launch',
-                            l2='inputs larger than L2 (no flush needed)',
-                            parallelism=f'replicas x{world}' if world > 1 else 'single GPU', kernel='tile2d'),
+                config=dict(workload=desc, cells=cells, l2=L2_NOTE),
+                grids=len(plans), strips=tiles, launch=choice,
+                tuning=[(r['ctas'], r['rows'], r['strips'], round(r['median_ms_per_step'], 5))
+                        for r in tuning.candidates] if tuning else 'fixed by --batch-launch',
+                parallelism=f'replicas x{world}' if world > 1 else 'single GPU', kernel='tile2d',
                 roofline=roofline, e2e=e2e, clocks=clocks, gpu_launches=2 * args.steps, device_status=status)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, steps, el, threads = batch_cpu_rate(plans, args.cpu_budget)
@@ -567,7 +571,7 @@ def adjoint_workload(steps, precision='float32', seed=2024):
     return project, (lo, dn), raw
 
 
-def run_ours_adjoint(args, world, rank, local):
+def run_ours_adjoint(args, world, rank, local, precisions=('float32', 'float64')):
     """Gradient of |mode overlap|^2 of the output-plane Ey at 1.55 um with respect to the design density
     through the discrete adjoint, timed; then central differences on 16 seeded design voxels (float64)."""
     import torch
@@ -575,7 +579,7 @@ def run_ours_adjoint(args, world, rank, local):
     torch.cuda.set_device(local)
     steps = 4000
     results = {}
-    for precision in ('float32', 'float64'):
+    for precision in precisions:
         project, (lo, dn), raw = adjoint_workload(steps, precision)
         dtype = torch.float32 if precision == 'float32' else torch.float64
         model = DifferentiablePlaneSimulation(project, AdjointOptions())
@@ -720,14 +724,164 @@ def run_ours_surrogate(args, world, rank, local):
     return result
 
 
+def run_adjoint_probe(args, world, rank, local):
+    """Profiling case of the discrete adjoint: one gradient (no warm-up) of a small 3D scene (--probe-cells per side in
+    x and y, half that in z, 0.05 um, CPML 8, an Ey dipole and an Ey point monitor, --steps steps), timed on the host."""
+    import torch
+    from torchfdtd_b200 import Monitor, Project, Region, Source
+    from torchfdtd_b200.adjoint import DifferentiableSimulation
+    torch.cuda.set_device(local)
+    n, steps = args.probe_cells, args.steps
+    region = Region(dimension='3d', size=(n * .05, n * .05, n * .025), mesh=.05, pml_cells=8, steps=steps, backend='cuda')
+    project = Project(region=region, sources=[Source(center=(-.5, 0, 0), component='Ey', pulse_cycles=1, wavelength=1.0)],
+                      monitors=[Monitor(center=(.5, 0, 0), component='Ey')])
+    model = DifferentiableSimulation(project)
+    eps = torch.full(tuple(region.shape), 2.0, device='cuda', requires_grad=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()                                # one cold gradient: the launch list of a profiler capture
+    (model(eps).signals ** 2).sum().backward()
+    torch.cuda.synchronize()
+    seconds = time.perf_counter() - t0
+    report = {k: v for k, v in model.engine(eps).report.items() if isinstance(v, (int, float, str))}
+    cells = int(np.prod(region.shape))
+    return dict(metric='adjoint gradient wall time', value=seconds, unit='s', n_gpus=world, steps=steps, warmup=1,
+                ms_per_step=seconds / steps * 1e3, higher_is_better=False, scaling='weak', vs_baseline=None, dtype='f32',
+                data='synthetic', config=dict(workload=f'3D adjoint probe {region.shape}, CPML 8, Ey dipole', cells=cells,
+                                              l2=L2_NOTE), report=report)
+
+
+def run_surrogate_kernels(args, world, rank, local):
+    """Profiling case of the surrogate's kernels: forward and forward+backward passes of the 8-layer network on
+    --probe-batch random densities, --steps passes, on the tcgen05 and on the mma.sync kernels."""
+    import torch
+    from torchfdtd_b200.surrogate import ConvNeuralOperator, device_status, set_tensor_path
+    torch.cuda.set_device(local)
+    batch, passes = args.probe_batch, args.steps
+    net = ConvNeuralOperator(outputs=32, seed=0)
+    rho = torch.rand((batch, 100, 100), device='cuda', generator=torch.Generator(device='cuda').manual_seed(0))
+    target = torch.zeros((batch, 32), device='cuda')
+    result = {}
+    for path in ('tcgen05', 'mma'):
+        set_tensor_path(path)
+        net.forward(rho)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(passes):
+            net.forward(rho)
+        end.record()
+        end.synchronize()
+        fwd = start.elapsed_time(end) / passes
+        start.record()
+        for _ in range(passes):
+            net.forward(rho)
+            net.loss(target)
+            net.backward(net._buffers[net._last]['dout'])
+        end.record()
+        end.synchronize()
+        result[path] = dict(forward_ms=fwd, conv_tflops=batch * net.flops_per_sample / fwd / 1e9,
+                            forward_backward_ms=start.elapsed_time(end) / passes)
+    set_tensor_path('tcgen05')
+    return dict(metric='surrogate forward time', value=result['tcgen05']['forward_ms'], unit='ms', n_gpus=world, steps=passes,
+                warmup=1, ms_per_step=result['tcgen05']['forward_ms'], higher_is_better=False, scaling='weak', vs_baseline=None,
+                dtype='bf16', data='synthetic', config=dict(workload=f'surrogate kernels, batch {batch} of 100x100 densities',
+                                                            cells=batch * 100 * 100, l2=L2_NOTE),
+                paths=result, device_status=device_status())
+
+
+def device_rate(project, eps, steps, warmup, device, kernel='auto'):
+    """Device-timed stepping of one workload through NativeGrid (CUDA events on the launching stream)."""
+    import torch
+    from torchfdtd_b200.native import NativeGrid
+    from torchfdtd_b200.plan import plan_grid
+    from torchfdtd_b200.simulation import algorithmic_bytes_per_step
+    plan = plan_grid(project)
+    if eps is not None:
+        plan.epsilon, plan.inv_eps = eps, (1 / eps).astype(plan.dtype)
+    grid = NativeGrid(plan, kernel=kernel)
+    stream = torch.cuda.Stream(device)
+    with torch.cuda.stream(stream):
+        grid.step(warmup, stream)
+        stream.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        grid.step(steps, stream)
+        end.record(stream)
+        end.synchronize()
+    elapsed = start.elapsed_time(end) / 1e3
+    out = dict(value=plan.cells * steps / elapsed / 1e9, unit=METRIC, ms_per_step=elapsed / steps * 1e3, steps=steps,
+               kernel=grid.kernel, roofline_frac=algorithmic_bytes_per_step(plan) * steps / elapsed / 1e9 / measured_peaks()[0],
+               device_status=grid.device_status(), gpu_launches=grid.step_launches(steps))
+    grid.close()
+    del grid
+    torch.cuda.empty_cache()
+    return plan, out
+
+
+def extra_workloads(args, local):
+    """The other benchmark configurations, device-timed in the same process (compact records; a failure is
+    recorded, not raised): the periodic scene with the reference's marching kernel restated beside ours, the 2D
+    TMz and Si-strip configurations at their own step counts, the 64-grid batch and the 3D adjoint gradient."""
+    import copy
+    import torch
+    device = torch.device('cuda', local)
+    extras = {}
+
+    def attempt(name, fn):
+        t0 = time.perf_counter()
+        try:
+            extras[name] = fn()
+        except Exception as exc:  # noqa: BLE001 - one failed extra must not void the headline line
+            extras[name] = dict(error=f'{type(exc).__name__}: {exc}')
+        extras[name]['wall_s'] = round(time.perf_counter() - t0, 2)
+        torch.cuda.empty_cache()
+
+    def periodic():
+        project, eps, desc = workload('periodic', args.warmup + args.steps)
+        plan, ours = device_rate(project, eps, args.steps, args.warmup, device)
+        from torchfdtd_b200.simulation import algorithmic_bytes_per_step
+        ref = time_restated_marching(plan, args, device, algorithmic_bytes_per_step(plan), measured_peaks()[0])
+        return dict(workload=desc, ours=ours, restated_reference=ref, speedup=ref['ms_per_step'] and ref['ms_per_step'] / ours['ms_per_step'])
+
+    def fixed(name, steps, warmup):
+        def run():
+            project, eps, desc = workload(name, warmup + steps)
+            _, out = device_rate(project, eps, steps, warmup, device)
+            return dict(workload=desc, **out)
+        return run
+
+    def batch():
+        a = copy.copy(args)
+        a.no_e2e, a.no_cpu_baseline = True, True
+        line = run_ours_batch(a, 1, 0, local)
+        return dict(workload=line['config']['workload'], value=line['value'], unit=METRIC, ms_per_step=line['ms_per_step'],
+                    roofline_frac=line['roofline']['frac'], launch=line['launch'], device_status=line['device_status'])
+
+    def adjoint():
+        line = run_ours_adjoint(args, 1, 0, local, precisions=('float32',))
+        f32 = line['adjoint']['float32']
+        return dict(workload=line['config']['workload'], gradient_s=f32['gradient_s'], forward_s=f32['forward_s'],
+                    backward_s=f32['backward_s'], replayed_steps=f32['replayed_steps'], checkpoints=f32['checkpoints'])
+
+    attempt('periodic', periodic)
+    attempt('tmz2d', fixed('tmz2d', 2000, 100))
+    attempt('strip', fixed('strip', 1000, 50))
+    attempt('batch64', batch)
+    attempt('adjoint3d', adjoint)
+    return extras
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=200)
     ap.add_argument('--warmup', type=int, default=10)
     ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
-    ap.add_argument('--workload', choices=['roofline', 'roofline256', 'strip', 'periodic', 'tmz2d', 'batch64', 'adjoint3d', 'surrogate'],
+    ap.add_argument('--workload', choices=['roofline', 'roofline256', 'strip', 'periodic', 'tmz2d', 'batch64', 'adjoint3d', 'surrogate',
+                                           'adjoint_probe', 'surrogate_kernels'],
                     default='roofline')
+    ap.add_argument('--probe-cells', type=int, default=128, help='adjoint_probe: cells per side in x and y')
+    ap.add_argument('--probe-batch', type=int, default=256, help='surrogate_kernels: densities per pass')
     ap.add_argument('--surrogate-epochs', type=int, default=30)
     ap.add_argument('--design-iterations', type=int, default=30)
     ap.add_argument('--kernel', choices=['auto', 'march', 'gather', 'tile2d'], default='auto')
@@ -735,6 +889,8 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end leg (profiling runs)')
     ap.add_argument('--batch-launch', default=None, help='batch64: fixed "ctas,rows" instead of the autotuner')
+    ap.add_argument('--no-extras', action='store_true',
+                    help='roofline workload: skip the device-timed records of the other configurations')
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == 'reference':
@@ -746,8 +902,11 @@ def main():
         return
     world, rank, local = dist_setup(args)
     try:
-        runner = {'batch64': run_ours_batch, 'adjoint3d': run_ours_adjoint, 'surrogate': run_ours_surrogate}.get(args.workload, run_ours)
+        runner = {'batch64': run_ours_batch, 'adjoint3d': run_ours_adjoint, 'surrogate': run_ours_surrogate,
+                  'adjoint_probe': run_adjoint_probe, 'surrogate_kernels': run_surrogate_kernels}.get(args.workload, run_ours)
         line = runner(args, world, rank, local)
+        if line is not None and args.workload == 'roofline' and world == 1 and not args.no_extras:
+            line['extra_workloads'] = extra_workloads(args, local)
         if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
     finally:

@@ -1,9 +1,9 @@
 """Write the golden vectors in tests/golden/*.npz from the reference's own CPU path.
 
-Run in a container that has the reference source tree (read-only) at
-/root/reference:
+Run where the reference source tree (read-only) is present, given as the first argument, as
+$TORCHFDTD_REFERENCE, or as a ``reference`` directory beside this repository:
 
-    python tests/golden/make_golden.py [/root/reference]
+    python tests/golden/make_golden.py [path/to/reference [states|scenes|adjoint|results ...]]
 
 It imports the reference package, with ``tests/golden/fdtd_standin`` standing
 in for the uninstalled third-party ``fdtd`` 0.2.2 (only its constructor and
@@ -23,13 +23,14 @@ allocators are used by the reference), and records:
 The engine and the GPU tests never read the reference; they read these files.
 """
 import json
+import os
 import sys
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REFERENCE = Path(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+REFERENCE = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get('TORCHFDTD_REFERENCE', HERE.parents[2] / 'reference'))
 C0 = 299792458.0
 
 
@@ -226,10 +227,20 @@ def write_adjoint(ref):
                             objective=float(objective.detach()))
 
 
+def write_results(ref):
+    """The reference's own ``Result.save`` of complete CPU runs: the NPZ layout a result written here must
+    reproduce and that ``Result.load`` here must read."""
+    for name in ('strip3d', 'yee_periodic'):
+        result = ref.Simulation(scenes(ref)[name]).run()
+        result.save(HERE / f'result_{name}.npz')
+
+
+WRITERS = {'states': write_states, 'scenes': write_scenes, 'adjoint': write_adjoint, 'results': write_results}
+
 if __name__ == '__main__':
+    # Optional names after the reference path select writers (default: all of them).
     ref = load_reference()
-    write_states(ref)
-    write_scenes(ref)
-    write_adjoint(ref)
+    for name in (sys.argv[2:] or WRITERS):
+        WRITERS[name](ref)
     for path in sorted(HERE.glob('*.npz')):
         print(f'{path.name}: {path.stat().st_size/1024:.0f} KiB')

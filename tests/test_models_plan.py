@@ -23,10 +23,8 @@ def test_every_golden_project_round_trips_through_json():
         assert json.loads(p.model_dump_json()) == json.loads(text)
 
 
-def test_reference_demo_projects_load_when_the_reference_tree_is_present():
-    root = Path('/root/reference/tests/fixtures/projects')
-    if not root.exists():
-        pytest.skip('reference tree not present')
+def test_reference_demo_projects_load_when_the_reference_tree_is_present(reference_tree):
+    root = reference_tree / 'tests' / 'fixtures' / 'projects'
     for name in ('demo_3d.json', 'demo_waveguide.json', 'demo_scatterer.json', 'minimal_defaults.json', 'tiny_result.json'):
         p = Project.load(root / name)
         assert p.region.shape

@@ -72,11 +72,9 @@ def test_oracles_reproduce_reference_cpml_states(name, impl):
         np.testing.assert_array_equal(got, want)
 
 
-def test_reference_fixture_itself_when_the_reference_tree_is_present():
+def test_reference_fixture_itself_when_the_reference_tree_is_present(reference_tree):
     """The reference's own golden result (tests/fixtures/npz/tiny_2d_complete.npz), read in place."""
-    root = Path('/root/reference/tests/fixtures')
-    if not root.exists():
-        pytest.skip('reference tree not present')
+    root = reference_tree / 'tests' / 'fixtures'
     p = Project.load(root / 'projects' / 'tiny_result.json')
     d = np.load(root / 'npz' / 'tiny_2d_complete.npz')
     o = YeeOracle(plan_grid(p)).run()

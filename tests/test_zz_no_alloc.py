@@ -3,7 +3,8 @@
 tfd_field_norm_static serves callers that cannot allocate device memory (a health check running after an
 out-of-memory failure, or a host whose memory belongs to a pool it must not bypass): its scratch is a static
 device array in the library. Two calls in a row on different states must each agree with tfd_diagnose, which
-uses the plan's own arena: energy to the FP64 summation tolerance, peak exactly.
+uses the plan's own arena: energy to the FP64 summation tolerance, peak exactly, in both field precisions
+and with one (cell) or three (Yee) stored permittivity samples per cell.
 """
 import numpy as np
 import pytest
@@ -11,13 +12,15 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_static_scratch_norm_matches_diagnose_on_two_calls_in_a_row():
+@pytest.mark.parametrize('precision', ['float32', 'float64'])
+@pytest.mark.parametrize('sampling', ['cell', 'yee'])
+def test_static_scratch_norm_matches_diagnose_on_two_calls_in_a_row(precision, sampling):
     import torch
     from torchfdtd_b200 import Project, Region, Source, Structure
     from torchfdtd_b200.native import NativeGrid
     from torchfdtd_b200.plan import plan_grid
     project = Project(region=Region(dimension='3d', size=(2.0, 1.6, 1.2), mesh=.05, pml_cells=6, steps=40, backend='cuda',
-                                    precision='float64', material_sampling='yee'),
+                                    precision=precision, material_sampling=sampling),
                       structures=[Structure(kind='sphere', radius=.4, material='Si (constant n)')],
                       sources=[Source(center=(-.3, .1, 0), component='Ey', pulse_cycles=1, wavelength=1.0)])
     plan = plan_grid(project)

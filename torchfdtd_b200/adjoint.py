@@ -364,25 +364,3 @@ class DifferentiablePlaneSimulation(_Differentiable):
                 tuple(pp.plan['shape']), pp.monitor.normal, engine.report)
         return out
 
-
-def _main():
-    """One gradient of a small 3D scene: ``python -m torchfdtd_b200.adjoint [cells] [steps]`` (cells per side
-    in x and y, half that in z, 0.05 um, CPML 8, an Ey dipole and an Ey point monitor)."""
-    import json
-    import sys
-    import torch
-    from .models import Monitor, Region, Source
-    n = int(sys.argv[1]) if len(sys.argv) > 1 else 128
-    steps = int(sys.argv[2]) if len(sys.argv) > 2 else 200
-    region = Region(dimension='3d', size=(n * .05, n * .05, n * .025), mesh=.05, pml_cells=8, steps=steps, backend='cuda')
-    project = Project(region=region, sources=[Source(center=(-.5, 0, 0), component='Ey', pulse_cycles=1, wavelength=1.0)],
-                      monitors=[Monitor(center=(.5, 0, 0), component='Ey')])
-    model = DifferentiableSimulation(project)
-    eps = torch.full(tuple(region.shape), 2.0, device='cuda', requires_grad=True)
-    (model(eps).signals ** 2).sum().backward()
-    torch.cuda.synchronize()
-    print(json.dumps({k: v for k, v in model.engine(eps).report.items() if isinstance(v, (int, float, str))}))
-
-
-if __name__ == '__main__':
-    _main()

@@ -1258,6 +1258,8 @@ int launch_persist2d(tfd_plan *p, int nsteps, cudaStream_t s) {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    // The barrier words start every launch at zero: a launch that timed out leaves its arrival count behind.
+    TFD_CUDA(cudaMemsetAsync(p->arena + p->L.grid_bar, 0, 2 * sizeof(unsigned), s));
     TFD_CUDA(cudaLaunchKernelEx(&cfg, k_step2d_persistent<T>, (const Grid<T> *)(p->arena + p->L.grid_tab),
                                 (const Tile2D *)(p->arena + p->L.tile_tab), p->tile2d_interior, p->L.tiles2d, m, mgx, mgy, nsteps,
                                 p->ptr<unsigned>(p->L.grid_bar)));

@@ -34,8 +34,9 @@ constexpr long long kNoAllocMaxCells = (long long)kNoAllocBlocks * kNoAllocThrea
 
 static __device__ __align__(256) double g_norm_scratch[kNoAllocBlocks * 4];
 
+constexpr int kMaxDevices = 64;         // devices per process whose scratch address is cached
 std::mutex g_symbol_mutex;
-void *g_symbol_ptr[64] = {nullptr};
+void *g_symbol_ptr[kMaxDevices] = {nullptr};
 
 template <typename T>
 __global__ void __launch_bounds__(kNoAllocThreads) k_norm_partial(const T *__restrict__ E, const T *__restrict__ H,
@@ -87,9 +88,14 @@ __global__ void k_norm_final(const double *partial, int blocks, double *out) {
 int scratch_pointer(double **ptr) {
     int device = -1;
     cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess || device < 0 || device >= 64) {
+    if (e != cudaSuccess || device < 0) {
         tfd::set_error(std::string("tfd_field_norm_static: no current CUDA device: ") + cudaGetErrorString(e));
         return TFD_ERR_CUDA;
+    }
+    if (device >= kMaxDevices) {
+        tfd::set_error("tfd_field_norm_static: device index " + std::to_string(device) + " exceeds the " +
+                       std::to_string(kMaxDevices) + " devices whose scratch address this library caches");
+        return TFD_ERR_INVALID;
     }
     std::lock_guard<std::mutex> lock(g_symbol_mutex);
     if (!g_symbol_ptr[device]) {

@@ -67,7 +67,8 @@ __device__ __forceinline__ void observe_step(const MonitorArgs<T> &m, int mgx, i
 }
 
 // `count` steps of one 2D TMz plan: strips [0, interior) take the lean path, [interior, all) the general
-// one; warps are strided over the table. bar: the plan's barrier words (zero between launches).
+// one; warps are strided over the table. bar: the plan's barrier words (the launcher zeroes them before
+// every launch, so a launch that timed out leaves no stale arrival count to the next one).
 template <typename T>
 __global__ void __launch_bounds__(k2dThreads, 2) k_step2d_persistent(const Grid<T> *__restrict__ grids,
                                                                     const Tile2D *__restrict__ strips, int interior, int all,

@@ -28,8 +28,11 @@
 // overwrite the box cells that fall outside the domain (TMA fills them with zeros) with the
 // cells one period away, so the seam columns / rows difference the same two values as the
 // reference's periodic branch, and the +x / +y halo lane or row that lies one past the last
-// cell recomputes E of the first column / row. Every mbarrier wait is bounded: on timeout the
-// kernel records kStatusPipelineTimeout in the device status word and returns.
+// cell recomputes E of the first column / row. Every mbarrier wait is bounded, and the decision
+// is taken by the whole CTA (a barrier reduction): on timeout the kernel records
+// kStatusPipelineTimeout in the device status word, waits once more (bounded) for the copies it
+// issued, and every thread of the CTA returns together. The fields of a timed-out launch are
+// undefined; the plan must be reset (tfd_reset) before it steps again.
 #pragma once
 #include <cuda.h>
 
@@ -94,9 +97,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
 // not take issue slots from the computing ones; the loop bounds the total wait to about 2 s.
 constexpr uint32_t kSuspendNs = 1000000;
 constexpr int kWaitTries = 2000;
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+constexpr int kDrainTries = 500;     // the second wait of a timed-out CTA for its copies in flight (about 0.5 s)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int tries = kWaitTries) {
     const uint32_t addr = smem_u32(bar);
-    for (int it = 0; it < kWaitTries; ++it) {
+    for (int it = 0; it < tries; ++it) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -609,19 +613,30 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
         patch_box(dst + 3 * ES, ES, S::BYE, y0, wrap(z0 + i), SAMPLES, 2);
     };
     const Rows<T> no_rows{};
+    // A wait of plane step t ran out: the status is recorded, thread 0 waits once more (bounded) for the copies
+    // still in flight, and the caller returns with the whole CTA. Before the waits of step t, thread 0 has issued
+    // the H sequence up to min(nh, NH + t) and the E sequence up to min(ne, NE + t); everything older than one
+    // ring was waited on.
+    auto give_up = [&](int t) {
+        if (tid == 0) {
+            atomicExch(g.status, kStatusPipelineTimeout);
+            const int issued_h = min(nh, S::NH + t), issued_e = min(ne, S::NE + t);
+            for (int i = max(0, issued_h - S::NH); i < issued_h; ++i) mbar_wait(&barh[i % S::NH], (uint32_t)((i / S::NH) & 1), kDrainTries);
+            for (int i = max(0, issued_e - S::NE); i < issued_e; ++i) mbar_wait(&bare[i % S::NE], (uint32_t)((i / S::NE) & 1), kDrainTries);
+        }
+    };
 
-    if (!wait_h(0)) {
-        if (tid == 0) atomicExch(g.status, kStatusPipelineTimeout);
+    if (__syncthreads_or(!wait_h(0))) {
+        give_up(0);
         return;
     }
     for (int k = z0; k <= z1; ++k) {
         const int t = k - z0;                                // E sequence index of plane k; H index is t + 1
         const bool halo_plane = k == z1;
         const bool compute_e = !halo_plane || has_halo;
-        if (compute_e && !(wait_h(t + 1) && wait_e(t))) {
-            if (tid == 0) atomicExch(g.status, kStatusPipelineTimeout);
-            return;
-        }
+        // A thread whose wait runs out still computes this plane (in-bounds shared-memory reads of a stage that
+        // may not have landed); the barrier after the E phase then takes the CTA-wide decision.
+        const bool late = compute_e && !(wait_h(t + 1) && wait_e(t));
         if (PXY && patch && compute_e) {
             if (t == 0 && has_prev) patch_h(0);
             patch_h(t + 1);
@@ -688,7 +703,10 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                 }
             }
         }
-        __syncthreads();
+        if (__syncthreads_or(late)) {
+            give_up(t);
+            return;
+        }
         // The E slot of plane k is free: refill it D+1 planes ahead.
         if (tid == 0 && compute_e && t + S::NE < ne) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

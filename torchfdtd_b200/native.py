@@ -286,9 +286,11 @@ class NativeGrid:
         """``material``: the inverse permittivity to load instead of ``plan.inv_eps`` (a host array or a device
         tensor, as for ``set_material``). ``permittivity``: the relative permittivity instead, checked and
         inverted on the device (``set_permittivity``)."""
+        import time
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError('CUDA requested but unavailable: the fused B200 engine runs on a CUDA GPU only.')
+        t0 = time.perf_counter()
         lib = library()
         self.plan = plan
         self.device = torch.device('cuda', torch.cuda.current_device() if device is None else device)
@@ -307,10 +309,16 @@ class NativeGrid:
         kernel_used = c_i32()
         check(lib.tfd_kernel_in_use(self.handle, ctypes.byref(kernel_used)))
         self.kernel = {v: k for k, v in KERNELS.items()}[kernel_used.value]
+        torch.cuda.synchronize(self.device)
+        t1 = time.perf_counter()
         if permittivity is not None:
             self.set_permittivity(permittivity)
         else:
             self.set_material(plan.inv_eps if material is None else material)
+        torch.cuda.synchronize(self.device)
+        # Host seconds of the set-up phases (device work included): arena allocation + plan creation, and the
+        # material upload (with the permittivity check and inversion when it is done on the device).
+        self.timing = {'arena_and_plan_create': t1 - t0, 'material_upload': time.perf_counter() - t1}
 
     # ---- restart states (checkpoints of the discrete adjoint) ------------------------------------
     def state_bytes(self):

@@ -107,9 +107,11 @@ class Result:
                                self.signals[::m.time_downsample, k], m.spectrum)
                 for k, m in enumerate(self.point_monitors)]
 
-    def save(self, path):
-        """NPZ layout of the reference ``Result.save`` (torchfdtd/solver.py:536-564)."""
+    def save(self, path, format=None):
+        """NPZ layout of the reference ``Result.save`` (torchfdtd/solver.py:536-564). The reference's chunked HDF5
+        layout (``format='hdf5'`` or a .h5 / .hdf5 path, torchfdtd/result_store.py) needs h5py and is refused."""
         path = Path(path)
+        _refuse_hdf5(path, format)
         path.parent.mkdir(parents=True, exist_ok=True)
         spectral_arrays, metadata, plane_metadata = {}, [], []
         for k, (m, spec) in enumerate(zip(self.point_monitors, self.spectra)):
@@ -122,6 +124,8 @@ class Result:
             for key, v in result.items():
                 if isinstance(v, np.ndarray):
                     spectral_arrays[f'field_monitor_{k}_{key}'] = v
+        if self.endpoint_fields is not None:
+            spectral_arrays.update({'endpoint_' + key: value for key, value in self.endpoint_fields.items()})
         np.savez_compressed(path, project=self.project.model_dump_json(), summary=json.dumps(self.summary, default=str),
                             field_monitors=json.dumps(plane_metadata, default=str),
                             **{f'mesh_{a}_um': nodes for a, nodes in zip('xyz', self.project.region.mesh_nodes)},
@@ -131,14 +135,18 @@ class Result:
 
     @classmethod
     def load(cls, path):
+        """Read the NPZ layout (a reference-written file included; reference torchfdtd/solver.py:603-618)."""
+        _refuse_hdf5(Path(path), None)
         with np.load(path, allow_pickle=False) as data:
             planes = json.loads(str(data['field_monitors'])) if 'field_monitors' in data else []
             for k, plane in enumerate(planes):
                 prefix = f'field_monitor_{k}_'
                 plane.update({key[len(prefix):]: data[key].copy() for key in data.files if key.startswith(prefix)})
+            endpoint = ({key: data['endpoint_' + key].copy() for key in ('E_upper', 'H_upper')}
+                        if 'endpoint_E_upper' in data.files else None)
             return cls(Project.model_validate_json(str(data['project'])), json.loads(str(data['summary'])),
                        *(data[key].copy() for key in ('frames', 'frame_steps', 'epsilon', 'signals', 'times', 'E', 'H')),
-                       planes, None)
+                       planes, endpoint)
 
     def field_monitor(self, name_or_id):
         matches = [m for m in self.frequency_fields if name_or_id in (m['id'], m['name'])]
@@ -151,6 +159,60 @@ class Result:
                      wavelength_um=(C0 / m['frequency_hz'] * 1e6).tolist(), flux=m['flux'].tolist(), units=m['flux_units'],
                      points=len(m['weights']), shape=m['shape'], settings=m['settings'])
                 for m in self.frequency_fields if m['flux'] is not None]
+
+
+def _refuse_hdf5(path, format):
+    if format == 'hdf5' or (format is None and path.suffix.lower() in ('.h5', '.hdf5')):
+        raise ValueError('The HDF5 result layout needs h5py, which this engine does not use; save and load results as NPZ.')
+    if format not in (None, 'npz', 'hdf5'):
+        raise ValueError(f'Unknown result format {format!r}; use "npz".')
+
+
+def snapshot_frames(project):
+    """Frame cadence against the shortest enabled source wavelength: a frame every max(snapshot_interval,
+    ceil(steps / 100)) steps; fewer than four frames per optical period alias the carrier in playback."""
+    r = project.region
+    interval = max(r.snapshot_interval, math.ceil(r.steps / 100))
+    lengths = [s.wavelength_start if s.time_definition in ('wavelength', 'frequency') else s.wavelength
+               for s in map(project.resolved_source, project.sources) if s.enabled]
+    shortest = min(lengths) if lengths else None
+    period = shortest * 1e-6 / C0 / r.time_step if shortest else None
+    per_period = period / interval if period else None
+    return dict(interval=r.snapshot_interval, effective_interval=interval, frames=r.steps // interval,
+                shortest_wavelength_um=shortest, period_steps=period, frames_per_period=per_period,
+                aliased=bool(per_period is not None and per_period < 4))
+
+
+def run_estimates(project, plan, arena_bytes):
+    """The scene and memory keys of the reference's run summary (torchfdtd/solver.py:456-466, with the mesh
+    summary of torchfdtd/mesh.py:100-107), computed for this engine: device memory is the plan's arena."""
+    r = project.region
+    dims = 2 if r.dimension == '2d' else 3
+    widths = [np.diff(a) for a in r.mesh_nodes[:dims]]
+    real = np.dtype(plan.dtype).itemsize
+    cells = math.prod(r.shape)
+    traces = 0
+    for t in plan.traces:
+        m = t.monitor
+        samples = len(range(0, r.steps, m.time_downsample))
+        traces += r.steps * real + 16 * (samples // 2 + 1 if m.spectrum.sampling == 'fft' else len(frequency_samples_of(m)))
+    waveform = sum(t.values.size * real for t in plan.sources)
+    host = 2 * cells * 3 * real + traces
+    ratios = [max(float((w[1:] / w[:-1]).max()), float((w[:-1] / w[1:]).max())) if w.size > 1 else 1.0 for w in widths]
+    return dict(mesh_type=r.mesh_type, material_sampling=r.material_sampling, uniform_reference_cells=math.prod(r.base_shape),
+                cell_reduction_percent=100 * (1 - cells / math.prod(r.base_shape)),
+                axis_min_step_um=[float(w.min()) for w in widths], axis_max_step_um=[float(w.max()) for w in widths],
+                coarse_limit_um=getattr(r, '_coarse_limit', None) or r.reference_step, max_adjacent_ratio=max(ratios),
+                shape=list(r.shape), actual_size_um=list(r.actual_size), cells=cells, dt_fs=r.time_step * 1e15,
+                duration_fs=r.time_step * r.steps * 1e15, estimated_memory_mb=round((arena_bytes + waveform) / 2**20, 1),
+                memory_model='fused_b200_arena', host_estimated_mb=round(host / 2**20, 1), oneway_planes=[], tfsf_boxes=[],
+                tfsf_auxiliary_estimated_bytes=0, point_trace_estimated_bytes=traces,
+                source_waveform_estimated_bytes=waveform, snapshot=snapshot_frames(project))
+
+
+def frequency_samples_of(monitor):
+    from .spectra import frequency_samples
+    return frequency_samples(monitor.spectrum)
 
 
 def resolve_selector(region):
@@ -241,10 +303,12 @@ class Observer:
         """Whether the field arrays take the device-side checks and the staged download."""
         return math.prod(self.plan.shape) * 3 * np.dtype(self.plan.dtype).itemsize > LARGE_FIELD_BYTES
 
-    def result(self, completed, termination_reason, seconds, setup_seconds, **extra):
-        """Read the final state back and package it as the reference's ``Result``."""
+    def result(self, completed, termination_reason, seconds, setup_seconds, phases=None, **extra):
+        """Read the final state back and package it as the reference's ``Result``. ``phases``: the caller's
+        per-phase host seconds; the field download and the rest of the packaging are added to it."""
         import torch
         from .native import download
+        t_start = time.perf_counter()
         p, r, plan, grid = self.project, self.region, self.plan, self.grid
         status = grid.device_status()
         if status:
@@ -257,11 +321,16 @@ class Observer:
             if not finite:
                 raise FloatingPointError(self._where('Non-finite fields detected.'))
             e_dev, h_dev = grid.fields_device()
+            t_wait = time.perf_counter()
             e_out, h_out = self.host_fields.result() if self.host_fields is not None else (None, None)
+            t_copy = time.perf_counter()
             e, h = download(e_dev, out=e_out), download(h_dev, out=h_out)
+            t_done = time.perf_counter()
             del e_dev, h_dev
         else:
+            t_wait = t_copy = time.perf_counter()
             e, h = grid.get_fields()
+            t_done = time.perf_counter()
             if not np.isfinite(e).all() or not np.isfinite(h).all():
                 raise FloatingPointError(self._where('Non-finite fields detected.'))
             field_peak = float(np.max(np.abs(e)))
@@ -275,7 +344,15 @@ class Observer:
             for m in frequency_results:
                 m['run_signature'] = signature
         cells = math.prod(r.shape)
-        stats = dict(warnings=self.warnings, backend='cuda', precision=r.precision, gpu=torch.cuda.get_device_name(),
+        if r.material_sampling == 'yee':
+            from .plan import field_axes
+            slice_position = float(field_axes(r, r.field)[self.axis][self.plane_index])
+        else:
+            slice_position = (0 if r.dimension == '2d' and self.axis == 2
+                              else (self.plane_index + .5) * r.mesh - r.actual_size[self.axis] / 2)
+        stats = run_estimates(p, plan, grid.arena_bytes)
+        stats.update(warnings=self.warnings, plan_hash=run_signature(p, r.steps), backend='cuda', precision=r.precision,
+                     gpu=torch.cuda.get_device_name(),
                      cuda_kernel='fused', cuda_monitor_kernel='fused', kernel=grid.kernel,
                      steps=completed, requested_steps=r.steps, cancelled=termination_reason == 'cancelled',
                      termination_reason=termination_reason, auto_shutoff=termination_reason == 'decayed',
@@ -286,15 +363,19 @@ class Observer:
                      mcells_per_second=cells * completed / max(seconds, 1e-9) / 1e6,
                      gcells_per_s=cells * completed / max(seconds, 1e-9) / 1e9,
                      hbm_bytes_per_step=algorithmic_bytes_per_step(plan), arena_bytes=grid.arena_bytes,
-                     field_peak=field_peak, slice_index=self.plane_index,
-                     slice_position=(0 if r.dimension == '2d' and self.axis == 2
-                                     else (self.plane_index + .5) * r.mesh - r.actual_size[self.axis] / 2),
+                     field_peak=field_peak, slice_index=self.plane_index, slice_position=slice_position,
                      complex_fields=False, complex_display=r.complex_display, material_update='nondispersive',
                      dispersive_samples=0, material_sampling=r.material_sampling,
                      epsilon_definition='instantaneous relative permittivity (epsilon-infinity for dispersive cells)',
                      boundaries=r.boundaries.model_dump(), bloch_phase=r.bloch_phase,
                      units='geometry: um; time: s; E/H: reduced fields; Bloch phase: rad', engine=ENGINE)
         stats.update(extra)
+        if phases is not None:
+            phases['field_check'] = t_wait - t_start
+            phases['host_result_arrays_wait'] = t_copy - t_wait
+            phases['field_download'] = t_done - t_copy
+            phases['result_packaging'] = time.perf_counter() - t_done
+            stats['phase_seconds'] = dict(phases)
         return Result(p, stats, np.array(self.frames), np.array(self.frame_steps), self.eps_plane, traces,
                       np.arange(1, completed + 1) * r.time_step, e, h, frequency_results)
 
@@ -379,7 +460,16 @@ class Simulation:
         if not torch.cuda.is_available():
             raise RuntimeError('CUDA requested but unavailable. The fused B200 engine needs a CUDA GPU.')
         started = time.perf_counter()
+        # Host seconds of each phase of the call (device work included where the phase waits for it).
+        phases, mark = {}, [started]
+
+        def lap(name):
+            now = time.perf_counter()
+            phases[name] = now - mark[0]
+            mark[0] = now
+
         plan, permittivity = self._run_plan()
+        lap('plan')
         variant, tuning = 0, None
         if launch == 'auto':
             if plan.dimension == '3d' and kernel in ('auto', 'march'):
@@ -391,7 +481,11 @@ class Simulation:
                     tuning = dict(skipped=str(exc))
         elif launch is not None:
             variant = int(launch)
+        if tuning is not None:
+            lap('launch_tuning')
         grid = NativeGrid(plan, kernel=kernel, variant=variant, permittivity=permittivity)
+        phases.update(grid.timing)
+        mark[0] = time.perf_counter()
         free, _ = torch.cuda.mem_get_info()
         observer = Observer(p, plan, grid)
         graphs = {}
@@ -407,6 +501,7 @@ class Simulation:
                 graphs = capture_graphs(lambda count: grid.step(count, stream), {1, width})
             torch.cuda.synchronize()
         torch.cuda.synchronize()
+        lap('observer_and_graph_capture')
         helper = None
         if observer.large_fields():
             # The result's host arrays are mapped and the download's staging ring pinned on a helper thread
@@ -420,27 +515,33 @@ class Simulation:
         setup_seconds = time.perf_counter() - started
         compute_start = time.perf_counter()
         completed, termination_reason, replays = 0, 'max_steps', 0
-        with torch.cuda.stream(stream):
-            for target, advance in observation_schedule(r.steps, width, observer.barriers()):
-                if cancel is not None and cancel.is_set():
-                    termination_reason = 'cancelled'
-                    break
-                if graphs:
-                    graphs[advance].replay()
-                    replays += 1
-                else:
-                    grid.step(advance, stream)
-                completed = target
-                if observer.observe(completed, progress, compute_start):
-                    termination_reason = 'decayed'
-                    break
-        torch.cuda.synchronize()
-        seconds = time.perf_counter() - compute_start
-        result = observer.result(completed, termination_reason, seconds, setup_seconds, cuda_graph=bool(graphs),
-                                 cuda_graph_steps=width, cuda_graph_replays=replays, free_device_bytes=free,
-                                 launch_variant=variant or None,
-                                 launch_tuning=tuning.as_dict() if hasattr(tuning, 'as_dict') else tuning)
-        grid.close()
-        if helper is not None:
-            helper.shutdown()
+        try:
+            with torch.cuda.stream(stream):
+                for target, advance in observation_schedule(r.steps, width, observer.barriers()):
+                    if cancel is not None and cancel.is_set():
+                        termination_reason = 'cancelled'
+                        break
+                    if graphs:
+                        graphs[advance].replay()
+                        replays += 1
+                    else:
+                        grid.step(advance, stream)
+                    completed = target
+                    if observer.observe(completed, progress, compute_start):
+                        termination_reason = 'decayed'
+                        break
+            torch.cuda.synchronize()
+            seconds = time.perf_counter() - compute_start
+            phases['stepping'] = seconds
+            mark[0] = time.perf_counter()
+            result = observer.result(completed, termination_reason, seconds, setup_seconds, phases, cuda_graph=bool(graphs),
+                                     cuda_graph_steps=width, cuda_graph_replays=replays, free_device_bytes=free,
+                                     launch_variant=variant or None,
+                                     launch_tuning=tuning.as_dict() if hasattr(tuning, 'as_dict') else tuning)
+        finally:
+            # The helper thread (pinned staging ring, mapped result arrays) is joined on every path.
+            if helper is not None:
+                helper.shutdown(wait=True)
+            graphs.clear()
+            grid.close()
         return result

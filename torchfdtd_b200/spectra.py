@@ -1,33 +1,43 @@
-"""Frequency samples, apodization windows and the host DFT of point traces.
+"""Frequency samples, apodization windows and the host transform of point traces.
 
-Restates reference ``torchfdtd/spectra.py``: ``apodization_window`` :14-27,
-``frequency_samples`` :30-44, ``highest_frequency`` :54-73,
-``direct_transform`` :76-92 and ``point_spectrum`` :95-116. Point traces are
-recorded on the device every step and transformed here after the run, with
-the convention dt * sum(x * w * exp(+2 pi i f t)).
+What the engine must reproduce is the reference's spectral convention (``torchfdtd/spectra.py``:
+windows :14-27, sample grids :30-44, :54-73, transforms :76-116), written here from its definition:
+
+* custom / wavelength / frequency / Chebyshev samples: ``X(f) = dt * sum_n x[n] w[n] exp(+2 pi i f t[n])``,
+  a field integral in "reduced field * s";
+* ``fft`` sampling: ``X(f_k) = s * sum_n x[n] w[n] exp(-2 pi i f_k t[n])`` at the positive FFT frequencies
+  ``f_k = k / (N dt)``, ``s = 2/N`` for a real trace and ``1/N`` for a complex one (an amplitude spectrum,
+  with no window-gain correction);
+* windows: ``1``, a Hann taper, or a Gaussian in ``t - center`` whose ``|w|^2`` has the full width at half
+  maximum ``apodization_time_width`` (``start`` / ``end`` keep it flat after / before the centre).
+
+Point traces are recorded on the device every step and transformed here after the run.
 """
 import numpy as np
 
 C0 = 299792458.0
+# Largest phase table the custom-sample transform builds at once (complex entries).
+_PHASE_TABLE = 1 << 20
 
 
 def apodization_window(times, settings):
+    """Window samples at ``times`` (s) for a ``SpectrumSettings``."""
     t = np.asarray(times, dtype=np.float64)
     mode = settings.apodization
     if mode == 'none':
         return np.ones_like(t)
     if mode == 'hann':
-        return np.hanning(len(t))
-    d = t - settings.apodization_center
-    if mode == 'start':
-        d = np.minimum(d, 0)
-    elif mode == 'end':
-        d = np.maximum(d, 0)
-    # apodization_time_width is the FWHM of |window|^2.
-    return np.exp(-2 * np.log(2) * (d / settings.apodization_time_width)**2)
+        return np.hanning(t.size)
+    offset = t - settings.apodization_center
+    if mode in ('start', 'end'):
+        # One-sided: the Gaussian acts only before ('start') or after ('end') the centre.
+        offset = np.clip(offset, None, 0) if mode == 'start' else np.clip(offset, 0, None)
+    # |w|^2 = exp(-4 ln2 (d / width)^2) has its half maximum at d = width / 2.
+    return np.exp(-2 * np.log(2) * (offset / settings.apodization_time_width)**2)
 
 
 def frequency_samples(settings):
+    """The sample frequencies (Hz) of a non-FFT ``SpectrumSettings``."""
     if settings.sampling == 'custom':
         return np.asarray(settings.custom_frequencies_hz, dtype=np.float64)
     a, b, n = settings.wavelength_start, settings.wavelength_stop, settings.frequency_points
@@ -49,9 +59,10 @@ def frequency_samples(settings):
 
 
 def frequency_count(settings):
+    """How many samples ``frequency_samples`` returns, without building them."""
     if settings.sampling == 'fft':
         raise ValueError('FFT samples depend on the recorded time grid.')
-    return len(settings.custom_frequencies_hz) if settings.sampling == 'custom' else settings.frequency_points
+    return settings.frequency_points if settings.sampling != 'custom' else len(settings.custom_frequencies_hz)
 
 
 def highest_frequency(settings):
@@ -60,41 +71,65 @@ def highest_frequency(settings):
     return float(np.max(frequency_samples(settings)))
 
 
+def _uniform_step(t):
+    """The step of a uniform, increasing time grid of at least two samples."""
+    if t.ndim != 1 or t.size < 2:
+        raise ValueError('A point spectrum needs a one-dimensional trace of two or more samples.')
+    steps = np.diff(t)
+    dt = steps[0]
+    if not dt > 0 or np.any(np.abs(steps - dt) > 1e-7 * abs(dt)):
+        raise ValueError('A point spectrum needs samples on a uniform, increasing time grid.')
+    return dt
+
+
 def direct_transform(times, signal, frequencies, window=None):
-    t, e, f = np.asarray(times), np.asarray(signal), np.asarray(frequencies)
-    if t.ndim != 1 or e.shape != t.shape or f.ndim != 1 or len(t) < 2:
-        raise ValueError('DFT requires a one-dimensional trace with at least two time samples.')
+    """``dt * sum_n x[n] w[n] exp(+2 pi i f t[n])`` for each ``f`` (complex128).
+
+    The sum runs over blocks of time samples, so the phase table stays bounded for long traces."""
+    t = np.asarray(times, dtype=np.float64)
+    f = np.asarray(frequencies, dtype=np.float64)
+    x = np.asarray(signal)
+    if x.shape != t.shape or f.ndim != 1:
+        raise ValueError('A point spectrum needs one trace value per time sample and a list of frequencies.')
+    dt = _uniform_step(t)
+    if not np.all(np.isfinite(f)) or np.any(f <= 0) or np.any(f * dt >= .5):
+        raise ValueError('Spectrum frequencies must be positive and below half the sampling rate 1/(2 dt).')
+    weighted = x * np.asarray(window) if window is not None else x
+    total = np.zeros(f.size, dtype=np.complex128)
+    block = max(1, _PHASE_TABLE // max(1, f.size))
+    omega = 2 * np.pi * f
+    for lo in range(0, t.size, block):
+        phase = np.multiply.outer(omega, t[lo:lo + block])
+        total += np.exp(1j * phase) @ weighted[lo:lo + block]
+    return total * dt
+
+
+def _fft_amplitudes(times, signal, window):
+    """Amplitude spectrum at the positive FFT frequencies, phase referred to t = 0."""
+    t = np.asarray(times, dtype=np.float64)
     dt = t[1] - t[0]
-    if dt <= 0 or not np.allclose(np.diff(t), dt, rtol=1e-7, atol=0):
-        raise ValueError('DFT requires a uniform increasing time grid.')
-    if not np.all(np.isfinite(f)) or np.any(f <= 0) or np.any(f >= .5 / dt):
-        raise ValueError('DFT frequencies must be positive and below the temporal Nyquist limit.')
-    weighted = e if window is None else e * np.asarray(window)
-    values = np.empty(len(f), dtype=np.complex128)
-    chunk = max(1, 1_000_000 // len(t))  # bounded phase table, whatever the run length
-    for start in range(0, len(f), chunk):
-        block = f[start:start + chunk]
-        values[start:start + chunk] = (np.exp(2j * np.pi * block[:, None] * t) @ weighted) * dt
-    return values
+    x = np.asarray(signal) * window
+    n = x.size
+    if np.iscomplexobj(x):
+        freq, raw, scale = np.fft.fftfreq(n, dt), np.fft.fft(x), 1 / n
+    else:
+        freq, raw, scale = np.fft.rfftfreq(n, dt), np.fft.rfft(x), 2 / n
+    # The FFT's sum runs over n dt; the samples sit at t[0] + n dt, hence the factor exp(-2 pi i f t[0]).
+    value = raw * scale * np.exp(-2j * np.pi * freq * t[0])
+    positive = freq > 0
+    return freq[positive], value[positive]
 
 
 def point_spectrum(times, signal, settings):
+    """The spectrum record of one point trace: frequencies, values, units and the transform used."""
     window = apodization_window(times, settings)
     if len(times) < 2:
         return {'frequency_hz': np.array([]), 'value': np.array([], dtype=complex),
                 'units': 'unavailable', 'transform': 'insufficient time samples'}
-    dt = times[1] - times[0]
-    if settings.sampling != 'fft':
-        f = frequency_samples(settings)
-        return {'frequency_hz': f, 'value': direct_transform(times, signal, f, window),
-                'units': 'reduced field * s', 'transform': 'dt * sum(field * window * exp(+2pi i f t))'}
-    if np.iscomplexobj(signal):
-        f = np.fft.fftfreq(len(signal), dt)
-        values = np.fft.fft(signal * window) / len(signal)
-    else:
-        f = np.fft.rfftfreq(len(signal), dt)
-        values = np.fft.rfft(signal * window) / (len(signal) / 2)
-    keep = f > 0
-    values = values * np.exp(-2j * np.pi * f * times[0])
-    return {'frequency_hz': f[keep], 'value': values[keep], 'units': 'reduced field',
-            'transform': 'FFT exp(-2pi i f t); scale 2/N real or 1/N complex; no window-gain correction'}
+    if settings.sampling == 'fft':
+        f, value = _fft_amplitudes(times, signal, window)
+        return {'frequency_hz': f, 'value': value, 'units': 'reduced field',
+                'transform': 'FFT exp(-2pi i f t); scale 2/N real or 1/N complex; no window-gain correction'}
+    f = frequency_samples(settings)
+    return {'frequency_hz': f, 'value': direct_transform(times, signal, f, window),
+            'units': 'reduced field * s', 'transform': 'dt * sum(field * window * exp(+2pi i f t))'}

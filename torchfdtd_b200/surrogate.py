@@ -272,42 +272,3 @@ class ConvNeuralOperator:
                 log(epoch, history[-1])
         return history
 
-
-def _main():
-    """Timing of the network's kernels on random inputs: ``python -m torchfdtd_b200.surrogate [batch] [passes]``."""
-    import json
-    import sys
-    import torch
-    batch = int(sys.argv[1]) if len(sys.argv) > 1 else 256
-    passes = int(sys.argv[2]) if len(sys.argv) > 2 else 20
-    net = ConvNeuralOperator(outputs=32, seed=0)
-    rho = torch.rand((batch, 100, 100), device='cuda', generator=torch.Generator(device='cuda').manual_seed(0))
-    target = torch.zeros((batch, 32), device='cuda')
-    result = {}
-    for path in ('tcgen05', 'mma'):
-        set_tensor_path(path)
-        net.forward(rho)
-        torch.cuda.synchronize()
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record()
-        for _ in range(passes):
-            net.forward(rho)
-        end.record()
-        end.synchronize()
-        fwd = start.elapsed_time(end) / passes
-        start.record()
-        for _ in range(passes):
-            net.forward(rho)
-            net.loss(target)
-            net.backward(net._buffers[net._last]['dout'])
-        end.record()
-        end.synchronize()
-        result[path] = dict(forward_ms=fwd, conv_tflops=batch * net.flops_per_sample / fwd / 1e9,
-                            forward_backward_ms=start.elapsed_time(end) / passes)
-    set_tensor_path('tcgen05')
-    result['status'] = device_status()
-    print(json.dumps(result))
-
-
-if __name__ == '__main__':
-    _main()
