@@ -95,6 +95,18 @@ class CpuOracle:
         self._keep += [segs, srcs, trs]
         self.desc = d
 
+    def run_with_planes(self, steps=None, dft_float64=True):
+        """Step one step at a time and accumulate the plan's DFT planes on the host after each step (the NumPy
+        oracle's accumulation); returns the accumulators."""
+        from .yee_oracle import accumulate_planes, plane_entries
+        if not hasattr(self, 'planes'):
+            self.planes = plane_entries(self.plan, dft_float64)
+        for _ in range(self.plan.steps if steps is None else steps):
+            n = self.counter
+            self.run(1)
+            accumulate_planes(self.planes, self.E, self.H, n)
+        return [e['value'] for e in self.planes]
+
     def run(self, steps=None):
         n = self.plan.steps if steps is None else steps
         psi = (c_vp * max(1, len(self.memory_states)))(*[m.ctypes.data for m in self.memory_states])

@@ -39,6 +39,38 @@ def _slice(axis, value, component=None):
     return tuple(parts)
 
 
+def plane_entries(plan, dft_float64=False):
+    """DFT accumulators of the plan's planes (reference torchfdtd/field_monitors.py:121-164)."""
+    entries = []
+    for p in plan.planes:
+        cdtype = np.complex128 if dft_float64 else p.complex_dtype
+        value = np.zeros((len(p.frequency), p.corner_cells.shape[2], len(p.components)), dtype=cdtype)
+        omega = 2j * np.pi * p.frequency * plan.time_step
+        half = np.exp(1j * np.pi * p.frequency * plan.time_step).astype(cdtype)
+        entries.append(dict(plan=p, value=value, omega=omega, half=half))
+    return entries
+
+
+def accumulate_planes(entries, E, H, n):
+    """One step of the online plane DFT after step n (reference torchfdtd/field_monitors.py:144-160): the
+    trilinear sample of each component times the window, times exp(i w (n+1) dt), H half a step later."""
+    for entry in entries:
+        p = entry['plan']
+        fields = []
+        for k, comp in enumerate(p.components):
+            family = int(comp.startswith('H'))
+            flat = (H if family else E).reshape(-1)
+            c = 'xyz'.index(comp[1].lower())
+            sampled = (flat[p.corner_cells[k] * 3 + c] * p.corner_weights[k]).sum(axis=0)
+            fields.append(sampled * p.windows[family][n])
+        value = entry['value']
+        phase = np.exp(entry['omega'] * (n + 1)).astype(value.dtype)
+        values = np.stack(fields, axis=-1)
+        ne = p.ne
+        value[..., :ne] += phase[:, None, None] * values[None, :, :ne]
+        value[..., ne:] += (phase * entry['half'])[:, None, None] * values[None, :, ne:]
+
+
 class YeeOracle:
     def __init__(self, plan, dft_float64=False):
         self.plan = plan
@@ -82,13 +114,7 @@ class YeeOracle:
             self.sources[term.family].append((term.values.astype(dtype), loc, term.comp))
         self.counter = 0
         self.traces = np.zeros((plan.steps, len(plan.traces)), dtype=dtype)
-        self.planes = []
-        for p in plan.planes:
-            cdtype = np.complex128 if dft_float64 else p.complex_dtype
-            value = np.zeros((len(p.frequency), p.corner_cells.shape[2], len(p.components)), dtype=cdtype)
-            omega = 2j * np.pi * p.frequency * plan.time_step
-            half = np.exp(1j * np.pi * p.frequency * plan.time_step).astype(cdtype)
-            self.planes.append(dict(plan=p, value=value, omega=omega, half=half))
+        self.planes = plane_entries(plan, dft_float64)
 
     # -- reference YeeGrid.curl ---------------------------------------------------------------
     def curl(self, field, forward):
@@ -129,22 +155,7 @@ class YeeOracle:
             field[loc + (component,)] += values[self.counter]
 
     def _planes(self):
-        n = self.counter
-        for entry in self.planes:
-            p = entry['plan']
-            fields = []
-            for k, comp in enumerate(p.components):
-                family = int(comp.startswith('H'))
-                flat = (self.H if family else self.E).reshape(-1)
-                c = 'xyz'.index(comp[1].lower())
-                sampled = (flat[p.corner_cells[k] * 3 + c] * p.corner_weights[k]).sum(axis=0)
-                fields.append(sampled * p.windows[family][n])
-            value = entry['value']
-            phase = np.exp(entry['omega'] * (n + 1)).astype(value.dtype)
-            values = np.stack(fields, axis=-1)
-            ne = p.ne
-            value[..., :ne] += phase[:, None, None] * values[None, :, :ne]
-            value[..., ne:] += (phase * entry['half'])[:, None, None] * values[None, :, ne:]
+        accumulate_planes(self.planes, self.E, self.H, self.counter)
 
     def step(self):
         self.update_E()
