@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define TFD_ABI_VERSION 1
+#define TFD_ABI_VERSION 2
 
 enum tfd_code {
     TFD_OK = 0,
@@ -112,6 +112,14 @@ typedef struct tfd_desc {
     const tfd_trace *traces;
     int32_t n_planes;
     const tfd_plane *planes;
+    /* Nonuniform meshes: per family (0 E, 1 H) and axis, n float64 factors indexed by the updated cell, or NULL on
+     * an axis whose cells all have the reference step. The plain difference of the cell's curl term along that axis
+     * is multiplied by the factor (rounded to the field precision) before the CPML terms: E at cell i >= 1 by
+     * h / ((w[i-1] + w[i]) / 2), at i = 0 by the periodic wrap factor 2 h / (w[0] + w[n-1]); H at cell i <= n-2 by
+     * h / w[i], at i = n-1 by the wrap factor h / w[n-1] (h: reference step, w: cell widths). PEC ghost terms are
+     * not scaled. Reference: the metric of YeeGrid._prepare_boundaries / curl, torchfdtd/boundaries.py:276-284,
+     * 376-393, and its fused kernel, torchfdtd/cuda_kernels.py:203-236. */
+    const double *metric[2][3];
 } tfd_desc;
 
 typedef struct tfd_plan tfd_plan;

@@ -7,7 +7,8 @@ of the CPML curl (``curl_faces_transpose`` :369-432, without PMC faces) in numpy
 
 - observation seeds are added to e_bar / h_bar first (the traces sample the state after the step);
 - e_bar += curl_f^T(-cn h_bar), with the CPML memory transpose m = psi_bar + v; psi_bar <- b m;
-  v <- v / kappa + c m;
+  v <- v / kappa + c m; then, on a nonuniform mesh, v <- v * metric (the forward scales the difference
+  before its CPML terms, so the transpose scales after them);
 - dJ/d eps += -cn e_bar curl_b(H_n; psi_n) / eps^2, summed over components for a per-cell eps;
 - h_bar += curl_b^T((cn / eps) e_bar).
 
@@ -56,6 +57,9 @@ class AdjointOracle:
             if n == 1:
                 continue
             derivative = H[_slice(axis, slice(1, None), component)] - H[_slice(axis, slice(None, -1), component)]
+            metric = self.fwd.metric.get((False, axis))
+            if metric:
+                derivative = derivative * metric[0]
             for i, seg in self._segments(False, axis, component):
                 data = derivative[seg['slice']]
                 psi = psis[i] * seg['b'] + seg['c'] * data
@@ -63,6 +67,8 @@ class AdjointOracle:
             result[_slice(axis, slice(1, None), output)] += sign * derivative
             if axis in self.fwd.wrap:
                 edge = H[_slice(axis, 0, component)] - H[_slice(axis, -1, component)]
+                if metric:
+                    edge = edge * metric[1]
                 result[_slice(axis, 0, output)] += sign * edge
         return result
 
@@ -82,11 +88,16 @@ class AdjointOracle:
                 previous[i] = seg['b'] * memory_bar
                 derivative = derivative.copy()
                 derivative[seg['slice']] = value * seg['inv_k'] + seg['c'] * memory_bar
+            metric = self.fwd.metric.get((forward, axis))
+            if metric:
+                derivative = derivative * metric[0]
             src = result[..., component]
             src[_slice(axis, slice(1, n))] += derivative
             src[_slice(axis, slice(0, n - 1))] -= derivative
             if axis in self.fwd.wrap:
                 edge = sign * dst[_slice(axis, n - 1 if forward else 0)]
+                if metric:
+                    edge = edge * metric[1]
                 src[_slice(axis, 0)] += edge
                 src[_slice(axis, n - 1)] -= edge
             elif forward and axis in self.fwd.pec_upper:

@@ -31,7 +31,8 @@ class Desc(ctypes.Structure):
     _fields_ = [('nx', c_i32), ('ny', c_i32), ('nz', c_i32), ('steps', c_i32), ('material_samples', c_i32),
                 ('courant', c_dbl), ('periodic', c_i32 * 3), ('pec_on', c_i32 * 3), ('pec_upper', c_dbl * 3),
                 ('n_segments', c_i32), ('segments', ctypes.POINTER(Segment)), ('n_sources', c_i32),
-                ('sources', ctypes.POINTER(Source)), ('n_traces', c_i32), ('traces', ctypes.POINTER(Trace))]
+                ('sources', ctypes.POINTER(Source)), ('n_traces', c_i32), ('traces', ctypes.POINTER(Trace)),
+                ('metric', (P_dbl * 3) * 2)]
 
 
 _lib = None
@@ -92,6 +93,13 @@ class CpuOracle:
         for k, t in enumerate(plan.traces):
             trs[k] = Trace(t.family, t.comp, (c_i32 * 3)(*t.index))
         d.n_traces, d.traces = len(plan.traces), trs
+        for f in range(2):
+            for a in range(3):
+                table = plan.metric_table(f, a)
+                if table is not None:
+                    table = np.ascontiguousarray(table, dtype=np.float64)
+                    self._keep.append(table)
+                    d.metric[f][a] = _p(table)
         self._keep += [segs, srcs, trs]
         self.desc = d
 

@@ -7,7 +7,7 @@
  * or as the timed CPU baseline. It restates, per element and in the same
  * floating-point operation order, the reference CPU path
  * (torchfdtd/boundaries.py:363-438, torchfdtd/solver.py:778-797):
- *   E pass:  d = H[i]-H[i-1]; (CPML) psi = psi*b + c*d; d = d*(1/kappa) + psi;
+ *   E pass:  d = H[i]-H[i-1]; (nonuniform mesh) d = d*metric; (CPML) psi = psi*b + c*d; d = d*(1/kappa) + psi;
  *            acc = (0 + s0*d0) + s1*d1; E = E + (cn*inv_eps)*acc; then E sources;
  *   H pass:  d = E[i+1]-E[i] (periodic wrap / PEC ghost at the upper end), CPML,
  *            H = H - cn*acc; then H sources; then point traces.
@@ -35,6 +35,9 @@ typedef struct oc_desc {
     const oc_source *sources;
     int32_t n_traces;
     const oc_trace *traces;
+    /* nonuniform mesh: per family and axis n factors indexed by the updated cell, or NULL (uniform axis);
+     * reference torchfdtd/boundaries.py:276-284,376-393 */
+    const double *metric[2][3];
 } oc_desc;
 
 /* Curl terms grouped by output component, in reference accumulation order:
@@ -85,9 +88,14 @@ int oc_run_##SUFFIX(const oc_desc *d, REAL *E, REAL *H, const REAL *inv_eps, REA
     oc_rows rows[2][3];                                                                                          \
     if (build_rows(d, rows)) return -1;                                                                          \
     /* coefficient tables rounded to REAL, as the reference stores them */                                        \
-    REAL *cb[2][3], *cc[2][3], *ck[2][3];                                                                        \
+    REAL *cb[2][3], *cc[2][3], *ck[2][3], *mt[2][3];                                                             \
     for (int f = 0; f < 2; ++f)                                                                                  \
         for (int a = 0; a < 3; ++a) {                                                                            \
+            mt[f][a] = NULL;                                                                                     \
+            if (d->metric[f][a]) {                                                                               \
+                mt[f][a] = (REAL *)calloc(n[a], sizeof(REAL));                                                   \
+                for (int i = 0; i < n[a]; ++i) mt[f][a][i] = (REAL)d->metric[f][a][i];                           \
+            }                                                                                                    \
             cb[f][a] = (REAL *)calloc(n[a], sizeof(REAL));                                                       \
             cc[f][a] = (REAL *)calloc(n[a], sizeof(REAL));                                                       \
             ck[f][a] = (REAL *)calloc(n[a], sizeof(REAL));                                                       \
@@ -134,6 +142,7 @@ int oc_run_##SUFFIX(const oc_desc *d, REAL *E, REAL *H, const REAL *inv_eps, REA
                             REAL dd = (REAL)0;                                                                   \
                             if (co[a] > 0) {                                                                     \
                                 dd = H[cell * 3 + in] - H[cell * 3 - st[a] + in];                                \
+                                if (mt[0][a]) dd = dd * mt[0][a][co[a]];                                         \
                                 const int k = rows[0][a].seg[co[a]];                                             \
                                 if (k >= 0) {                                                                    \
                                     int e[3] = {nx, ny, nz}, q[3] = {x, y, z};                                   \
@@ -146,6 +155,7 @@ int oc_run_##SUFFIX(const oc_desc *d, REAL *E, REAL *H, const REAL *inv_eps, REA
                                 }                                                                                \
                             } else if (d->periodic[a]) {                                                         \
                                 dd = H[cell * 3 + in] - H[cell * 3 + (long long)(n[a] - 1) * st[a] + in];        \
+                                if (mt[0][a]) dd = dd * mt[0][a][0];                                             \
                             }                                                                                    \
                             acc = acc + (sg > 0 ? dd : -dd);                                                     \
                         }                                                                                        \
@@ -179,6 +189,7 @@ int oc_run_##SUFFIX(const oc_desc *d, REAL *E, REAL *H, const REAL *inv_eps, REA
                             REAL dd = (REAL)0;                                                                   \
                             if (co[a] < n[a] - 1) {                                                              \
                                 dd = E[cell * 3 + st[a] + in] - E[cell * 3 + in];                                \
+                                if (mt[1][a]) dd = dd * mt[1][a][co[a]];                                         \
                                 const int k = rows[1][a].seg[co[a]];                                             \
                                 if (k >= 0) {                                                                    \
                                     int e[3] = {nx, ny, nz}, q[3] = {x, y, z};                                   \
@@ -191,6 +202,7 @@ int oc_run_##SUFFIX(const oc_desc *d, REAL *E, REAL *H, const REAL *inv_eps, REA
                                 }                                                                                \
                             } else if (d->periodic[a]) {                                                         \
                                 dd = E[cell * 3 - (long long)(n[a] - 1) * st[a] + in] - E[cell * 3 + in];        \
+                                if (mt[1][a]) dd = dd * mt[1][a][co[a]];                                         \
                             } else if (d->pec_on[a]) {                                                           \
                                 dd = pec_neg[a] * E[cell * 3 + in];                                              \
                             }                                                                                    \
@@ -218,7 +230,7 @@ int oc_run_##SUFFIX(const oc_desc *d, REAL *E, REAL *H, const REAL *inv_eps, REA
             }                                                                                                    \
     }                                                                                                            \
     for (int f = 0; f < 2; ++f)                                                                                  \
-        for (int a = 0; a < 3; ++a) { free(cb[f][a]); free(cc[f][a]); free(ck[f][a]); }                          \
+        for (int a = 0; a < 3; ++a) { free(cb[f][a]); free(cc[f][a]); free(ck[f][a]); free(mt[f][a]); }          \
     free_rows(rows);                                                                                             \
     return 0;                                                                                                    \
 }

@@ -8,7 +8,8 @@ reference CPU path that the reference's fused CUDA kernels are pinned to
 (bitwise in FP32, reference ``tests/test_cuda_kernels.py:149-170``):
 
 - ``YeeGrid.curl`` (reference ``torchfdtd/boundaries.py:363-394``): backward
-  differences for E, forward for H, curl terms summed in ``CURL_TERMS`` order,
+  differences for E, forward for H, scaled by the nonuniform-mesh metric where the
+  mesh has one, curl terms summed in ``CURL_TERMS`` order,
   CPML ``psi <- b*psi + c*d; d <- d/kappa + psi`` inside the slabs, periodic
   wrap, the PEC upper ghost for H;
 - ``update_E`` / ``update_H`` (:413-438): ``E += (cn*inv_eps)*curl H``,
@@ -85,6 +86,12 @@ class YeeOracle:
         self.inverse_permeability = np.ones((1,), dtype=dtype)
         self.courant = plan.courant
         self.wrap = {a for a in range(3) if shape[a] > 1 and plan.faces[a][0] == 'periodic'}
+        # Nonuniform mesh factors (reference torchfdtd/boundaries.py:276-284), stored in the field precision.
+        self.metric = {}
+        for (forward, axis), (values, wrap) in plan.metrics.items():
+            shape_m = [1, 1, 1]
+            shape_m[axis] = len(values)
+            self.metric[forward, axis] = (values.reshape(shape_m).astype(dtype), wrap)
         self.pec_upper = dict(plan.pec_upper)
         self.cpml = {}
         self.memory_states = []
@@ -125,6 +132,8 @@ class YeeOracle:
             low = _slice(axis, slice(None, -1), component)
             high = _slice(axis, slice(1, None), component)
             derivative = field[high] - field[low]
+            if (forward, axis) in self.metric:
+                derivative *= self.metric[forward, axis][0]
             for segment in self.cpml[forward, axis, component]:
                 data = derivative[segment['slice']]
                 psi = segment['psi']
@@ -137,6 +146,8 @@ class YeeOracle:
             if axis in self.wrap:
                 first, last = _slice(axis, 0, component), _slice(axis, -1, component)
                 edge = 1.0 * field[first] - field[last] if forward else field[first] - field[last] / 1.0
+                if (forward, axis) in self.metric:
+                    edge *= self.metric[forward, axis][1]
                 result[_slice(axis, -1 if forward else 0, output)] += sign * edge
             elif forward and axis in self.pec_upper:
                 edge = -self.pec_upper[axis] * field[_slice(axis, -1, component)]

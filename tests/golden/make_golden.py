@@ -3,7 +3,7 @@
 Run where the reference source tree (read-only) is present, given as the first argument, as
 $TORCHFDTD_REFERENCE, or as a ``reference`` directory beside this repository:
 
-    python tests/golden/make_golden.py [path/to/reference [states|scenes|adjoint|results ...]]
+    python tests/golden/make_golden.py [path/to/reference [states|scenes|adjoint|results|mesh|sources ...]]
 
 It imports the reference package, with ``tests/golden/fdtd_standin`` standing
 in for the uninstalled third-party ``fdtd`` 0.2.2 (only its constructor and
@@ -64,10 +64,38 @@ def state_regions(ref):
     return out
 
 
-def write_states(ref):
+def mesh_state_regions(ref):
+    """Nonuniform meshes for the random-state CPML goldens: a graded mesh (a refinement box, coarse gaps) with
+    the kappa=3 face and a PEC face, and explicit coordinates with periodic x (the wrap metric) and physically
+    graded CPML on y and z."""
+    from torchfdtd.models import BoundaryFace, MeshRefinement
+    out = {}
+    r = ref.Region(dimension='3d', size=(3.0, 2.4, 2.0), mesh=.1, pml_cells=3, mesh_type='graded', mesh_max=.25,
+                   mesh_grading=1.4, material_sampling='yee', backend='cpu',
+                   mesh_refinements=[MeshRefinement(center=(.3, -.2, .1), size=(.4, .5, .3))])
+    r.boundaries.x_min = BoundaryFace(layers=5, kappa=3, alpha=.03, alpha_polynomial=1)
+    r.boundaries.z_max = BoundaryFace(kind='pec')
+    out['graded'] = r
+    rng = np.random.default_rng(77)
+    coords = []
+    for span, cells in ((1.6, 14), (1.4, 13), (1.2, 12)):
+        w = rng.uniform(.7, 1.3, cells)
+        w = w / w.sum() * span
+        nodes = np.r_[0, np.cumsum(w)] - span / 2
+        nodes[0], nodes[-1] = -span / 2, span / 2
+        coords.append(tuple(float(v) for v in nodes))
+    r = ref.Region(dimension='3d', size=(1.6, 1.4, 1.2), mesh=.1, pml_cells=3, mesh_type='explicit',
+                   mesh_coordinates=tuple(coords), material_sampling='yee', backend='cpu')
+    r.boundaries.x_min = BoundaryFace(kind='periodic')
+    r.boundaries.x_max = BoundaryFace(kind='periodic')
+    out['explicit'] = r
+    return out
+
+
+def write_states(ref, regions=None):
     import fdtd
     from torchfdtd.boundaries import YeeGrid
-    for layout, region in state_regions(ref).items():
+    for layout, region in (regions or state_regions(ref)).items():
         for precision in ('float32', 'float64'):
             region = region.model_copy(update={'precision': precision})
             dtype = np.float32 if precision == 'float32' else np.float64
@@ -171,9 +199,9 @@ def scenes(ref):
     return out
 
 
-def write_scenes(ref):
+def write_scenes(ref, projects=None):
     from torchfdtd.solver import voxelize
-    for name, project in scenes(ref).items():
+    for name, project in (projects or scenes(ref)).items():
         result = ref.Simulation(project).run()
         eps, _ = voxelize(project)
         arrays = dict(E=result.electric, H=result.magnetic, signals=result.signals, times=result.times, epsilon=eps,
@@ -207,11 +235,44 @@ def adjoint_scenes(ref):
     return out
 
 
-def write_adjoint(ref):
+def adjoint_mesh_scenes(ref):
+    """The adjoint scenes on nonuniform meshes: graded (2D, with a refinement box) and explicit coordinates
+    with a periodic axis (3D), FP32 and FP64."""
+    from torchfdtd.models import BoundaryFace, MeshRefinement, Monitor, Project, Region, Source
+    out = {}
+    for dim in ('2d', '3d'):
+        for precision in ('float32', 'float64'):
+            if dim == '2d':
+                r = Region(dimension='2d', size=(2.4, 2.0, 1), mesh=.08, pml_cells=3, steps=40, precision=precision,
+                           backend='cpu', mesh_type='graded', mesh_max=.2, mesh_grading=1.4, material_sampling='yee',
+                           mesh_refinements=[MeshRefinement(center=(.3, .2, 0), size=(.3, .3, 1))])
+                r.boundaries.y_max = BoundaryFace(kind='pec')
+            else:
+                rng = np.random.default_rng(5)
+                coords = []
+                for span, cells in ((1.6, 16), (1.4, 14), (1.2, 12)):
+                    w = rng.uniform(.8, 1.25, cells)
+                    w = w / w.sum() * span
+                    nodes = np.r_[0, np.cumsum(w)] - span / 2
+                    nodes[0], nodes[-1] = -span / 2, span / 2
+                    coords.append(tuple(float(v) for v in nodes))
+                r = Region(dimension='3d', size=(1.6, 1.4, 1.2), mesh=.1, pml_cells=3, steps=30, precision=precision,
+                           backend='cpu', mesh_type='explicit', mesh_coordinates=tuple(coords), material_sampling='yee')
+                r.boundaries.x_min = BoundaryFace(kind='periodic')
+                r.boundaries.x_max = BoundaryFace(kind='periodic')
+            out[f'mesh{dim}_{precision}'] = Project(
+                name=f'adjoint mesh {dim}', region=r,
+                sources=[Source(id='src', center=(-.1, .05, 0), component='Ez', pulse_cycles=1, wavelength=.6)],
+                monitors=[Monitor(id='ez', center=(.2, .1, 0), component='Ez'),
+                          Monitor(id='hy', center=(.1, -.1, 0), component='Hy')])
+    return out
+
+
+def write_adjoint(ref, projects=None):
     """Reference DifferentiableSimulation on the CPU: signals and d/d eps of sum(w * signals)."""
     import torch
     from torchfdtd.differentiable import AdjointOptions, DifferentiableSimulation
-    for name, project in adjoint_scenes(ref).items():
+    for name, project in (projects or adjoint_scenes(ref)).items():
         dtype = torch.float32 if project.region.precision == 'float32' else torch.float64
         rng = np.random.default_rng(17)
         shape = tuple(project.region.shape)
@@ -227,6 +288,108 @@ def write_adjoint(ref):
                             objective=float(objective.detach()))
 
 
+def mesh_scenes(ref):
+    """Complete runs on nonuniform meshes: graded (automatic refinement around the objects), axis-specific steps
+    and explicit coordinates with a periodic axis; 3D and 2D TMz, E and H sources, point traces and DFT planes."""
+    from torchfdtd.models import Boundaries, BoundaryFace, MeshRefinement
+    P, R, S, M, F, St, Sp = (ref.Project, ref.Region, ref.Source, ref.Monitor, ref.FieldMonitor, ref.Structure,
+                             ref.SpectrumSettings)
+    lam = 1.55
+    custom = Sp(sampling='custom', custom_frequencies_hz=[C0 / (lam * 1e-6)], apodization='none')
+    out = {}
+    out['graded3d'] = P(name='graded3d', region=R(dimension='3d', size=(3.2, 2.4, 2.0), mesh=.05, pml_cells=5, steps=160,
+                                                  mesh_type='graded', mesh_max=.16, material_sampling='yee', backend='cpu',
+                                                  background_index=1.444),
+                        structures=[St(id='wg', name='wg', size=(3.2, .5, .3), material='Si (constant n)'),
+                                    St(id='ball', name='ball', kind='sphere', center=(.6, .4, .2), radius=.2, material='Si (constant n)')],
+                        sources=[S(id='dip', center=(-.9, 0, 0), component='Ey', wavelength=lam, pulse='gaussian',
+                                   time_definition='standard', pulse_length=12e-15, pulse_offset=25e-15)],
+                        monitors=[M(id='probe', center=(.9, 0, 0), component='Ey', spectrum=custom),
+                                  F(id='plane', normal='x', center=(1.0, 0, 0), size=(0, .8, .6), dft_precision='float64',
+                                    spectrum=custom)])
+    b = Boundaries(**{f'{a}_{s}': BoundaryFace(layers=8) for a in 'xy' for s in ('min', 'max')})
+    b.y_max = BoundaryFace(kind='pec')
+    out['graded2d'] = P(name='graded2d', region=R(dimension='2d', size=(4.0, 3.0, 1), mesh=.04, pml_cells=8, steps=300,
+                                                  mesh_type='graded', mesh_max=.12, mesh_grading=1.3, material_sampling='yee',
+                                                  backend='cpu', boundaries=b,
+                                                  mesh_refinements=[MeshRefinement(center=(.8, -.6, 0), size=(.3, .3, 1))]),
+                        structures=[St(id='c', name='c', kind='circle', center=(.5, .3, 0), radius=.3, material='Si (constant n)')],
+                        sources=[S(id='src', center=(-1.0, 0, 0), component='Ez', wavelength=1.3, pulse_cycles=2),
+                                 S(id='mag', center=(-.5, .4, 0), component='Hx', wavelength=1.3, pulse_cycles=2, amplitude=.3)],
+                        monitors=[M(id='probe', center=(1.0, -.2, 0), component='Ez'),
+                                  F(id='plane', normal='x', center=(1.2, 0, 0), size=(0, 1.2, 1),
+                                    spectrum=Sp(sampling='frequency', frequency_points=2, apodization='none'))])
+    out['steps3d'] = P(name='steps3d', region=R(dimension='3d', size=(2.0, 1.6, 1.5), mesh=.05, mesh_steps=(.05, .04, .06),
+                                                pml_cells=5, steps=120, material_sampling='yee', backend='cpu'),
+                       structures=[St(id='blk', name='blk', size=(.6, .4, .3), material='Si (constant n)')],
+                       sources=[S(id='src', center=(-.4, 0, 0), component='Ez', wavelength=1.3, pulse_cycles=2)],
+                       monitors=[M(id='probe', center=(.4, .1, 0), component='Ez'),
+                                 F(id='plane', normal='z', center=(0, 0, .2), size=(.8, .6, 0),
+                                   spectrum=Sp(sampling='frequency', frequency_points=2, apodization='none'))])
+    rng = np.random.default_rng(91)
+    coords = []
+    for span, cells in ((1.6, 30), (1.6, 34), (1.2, 26)):
+        w = rng.uniform(.8, 1.25, cells)
+        w = w / w.sum() * span
+        nodes = np.r_[0, np.cumsum(w)] - span / 2
+        nodes[0], nodes[-1] = -span / 2, span / 2
+        coords.append(tuple(float(v) for v in nodes))
+    b = Boundaries(x_min=BoundaryFace(kind='periodic'), x_max=BoundaryFace(kind='periodic'),
+                   y_min=BoundaryFace(layers=5), y_max=BoundaryFace(layers=5), z_min=BoundaryFace(layers=4), z_max=BoundaryFace(layers=4))
+    out['explicit3d'] = P(name='explicit3d', region=R(dimension='3d', size=(1.6, 1.6, 1.2), mesh=.05, mesh_type='explicit',
+                                                      mesh_coordinates=tuple(coords), pml_cells=5, steps=120, material_sampling='yee',
+                                                      backend='cpu', boundaries=b),
+                          structures=[St(id='rod', name='rod', kind='circle', radius=.15, size=(1, 1, 1.2), material='Si (constant n)')],
+                          sources=[S(id='sheet', kind='plane', center=(0, -.3, 0), size=(1.6, 0, .5), normal='y', component='Ex',
+                                     wavelength=1.2, pulse_cycles=2)],
+                          monitors=[M(id='h', center=(.1, .3, 0), component='Hz'),
+                                    F(id='plane', normal='y', center=(0, .35, 0), size=(1.6, 0, .6),
+                                      spectrum=Sp(sampling='frequency', frequency_points=2, apodization='none'))])
+    return out
+
+
+def write_mesh(ref):
+    write_states(ref, mesh_state_regions(ref))
+    write_scenes(ref, mesh_scenes(ref))
+    write_adjoint(ref, adjoint_mesh_scenes(ref))
+
+
+def source_scenes(ref):
+    """One-way (Huygens) plane sources: 3D with periodic x/y and a dielectric slab downstream (Ex, travelling +z),
+    and 2D TMz with periodic y (Ez, travelling -x); traces on both sides of the plane and a DFT plane."""
+    from torchfdtd.models import Boundaries, BoundaryFace
+    P, R, S, M, F, St, Sp = (ref.Project, ref.Region, ref.Source, ref.Monitor, ref.FieldMonitor, ref.Structure,
+                             ref.SpectrumSettings)
+    out = {}
+    b = Boundaries(x_min=BoundaryFace(kind='periodic'), x_max=BoundaryFace(kind='periodic'),
+                   y_min=BoundaryFace(kind='periodic'), y_max=BoundaryFace(kind='periodic'),
+                   z_min=BoundaryFace(layers=8), z_max=BoundaryFace(layers=8))
+    out['oneway3d'] = P(name='oneway3d', region=R(dimension='3d', size=(0.8, 0.6, 3.0), mesh=.05, pml_cells=8, steps=180,
+                                                  backend='cpu', boundaries=b),
+                        structures=[St(id='slab', name='slab', size=(0.8, 0.6, .3), center=(0, 0, .6), material='Si (constant n)')],
+                        sources=[S(id='pw', kind='plane', injection='oneway', normal='z', direction='+', center=(0, 0, -.5),
+                                   size=(0.8, 0.6, 0), component='Ex', wavelength=1.3, pulse_cycles=2)],
+                        monitors=[M(id='up', center=(0, 0, .2), component='Ex'), M(id='down', center=(0, 0, -.9), component='Ex'),
+                                  M(id='hy', center=(0.1, 0, .1), component='Hy'),
+                                  F(id='plane', normal='z', center=(0, 0, 1.0), size=(0.8, 0.6, 0),
+                                    spectrum=Sp(sampling='frequency', frequency_points=2, apodization='none'))])
+    b = Boundaries(x_min=BoundaryFace(layers=10), x_max=BoundaryFace(layers=10),
+                   y_min=BoundaryFace(kind='periodic'), y_max=BoundaryFace(kind='periodic'))
+    out['oneway2d'] = P(name='oneway2d', region=R(dimension='2d', size=(4.0, 1.0, 1), mesh=.05, pml_cells=10, steps=260,
+                                                  backend='cpu', boundaries=b),
+                        structures=[St(id='c', name='c', kind='circle', center=(-1.0, 0, 0), radius=.2, material='Si (constant n)')],
+                        sources=[S(id='pw', kind='plane', injection='oneway', normal='x', direction='-', center=(.5, 0, 0),
+                                   size=(0, 1.0, 0), component='Ez', wavelength=1.2, pulse_cycles=2, amplitude=.7)],
+                        monitors=[M(id='left', center=(-.5, 0, 0), component='Ez'), M(id='right', center=(1.2, 0, 0), component='Ez'),
+                                  F(id='plane', normal='x', center=(-1.5, 0, 0), size=(0, 1.0, 1),
+                                    spectrum=Sp(sampling='frequency', frequency_points=2, apodization='none'))])
+    return out
+
+
+def write_sources(ref):
+    write_scenes(ref, source_scenes(ref))
+
+
 def write_results(ref):
     """The reference's own ``Result.save`` of complete CPU runs: the NPZ layout a result written here must
     reproduce and that ``Result.load`` here must read."""
@@ -235,7 +398,8 @@ def write_results(ref):
         result.save(HERE / f'result_{name}.npz')
 
 
-WRITERS = {'states': write_states, 'scenes': write_scenes, 'adjoint': write_adjoint, 'results': write_results}
+WRITERS = {'states': write_states, 'scenes': write_scenes, 'adjoint': write_adjoint, 'results': write_results, 'mesh': write_mesh,
+           'sources': write_sources}
 
 if __name__ == '__main__':
     # Optional names after the reference path select writers (default: all of them).

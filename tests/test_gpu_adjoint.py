@@ -27,7 +27,8 @@ def cuda_project(d):
     return project
 
 
-@pytest.mark.parametrize('name', ['2d_float32', '2d_float64', '3d_float32', '3d_float64'])
+@pytest.mark.parametrize('name', ['2d_float32', '2d_float64', '3d_float32', '3d_float64', 'mesh2d_float32', 'mesh2d_float64',
+                                  'mesh3d_float32', 'mesh3d_float64'])
 def test_gradient_matches_reference_adjoint(golden, name):
     import torch
     from torchfdtd_b200.adjoint import DifferentiableSimulation

@@ -52,7 +52,7 @@ def state_files(golden):
 
 
 @pytest.mark.parametrize('kernel', KERNELS)
-@pytest.mark.parametrize('name', ['pml2d', 'pml3d', 'periodic', 'pec'])
+@pytest.mark.parametrize('name', ['pml2d', 'pml3d', 'periodic', 'pec', 'graded', 'explicit'])
 @pytest.mark.parametrize('precision', ['float32', 'float64'])
 def test_random_state_and_every_cpml_memory_match_reference_bitwise(golden, kernel, name, precision):
     d = np.load(golden / f'state_{name}_{precision}.npz')
@@ -75,7 +75,8 @@ def test_random_state_and_every_cpml_memory_match_reference_bitwise(golden, kern
     assert g.device_status() == 0
 
 
-SIMS = ['tmz', 'strip3d', 'strip3d_f64', 'yee_periodic', 'te2d', 'both2d', 'tiny']
+SIMS = ['tmz', 'strip3d', 'strip3d_f64', 'yee_periodic', 'te2d', 'both2d', 'tiny', 'graded3d', 'graded2d', 'steps3d', 'explicit3d',
+        'oneway3d', 'oneway2d']
 
 
 @pytest.mark.parametrize('kernel', KERNELS)

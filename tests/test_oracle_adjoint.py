@@ -16,7 +16,8 @@ def rel(a, b):
     return float(np.linalg.norm((np.asarray(a) - np.asarray(b)).ravel()) / np.linalg.norm(np.asarray(b).ravel()))
 
 
-@pytest.mark.parametrize('name', ['2d_float32', '2d_float64', '3d_float32', '3d_float64'])
+@pytest.mark.parametrize('name', ['2d_float32', '2d_float64', '3d_float32', '3d_float64', 'mesh2d_float32', 'mesh2d_float64',
+                                  'mesh3d_float32', 'mesh3d_float64'])
 def test_oracle_adjoint_matches_reference_adjoint(golden, name):
     d = np.load(golden / f'adjoint_{name}.npz')
     project = Project.model_validate_json(str(d['project']))

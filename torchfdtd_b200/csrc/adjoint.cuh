@@ -10,7 +10,9 @@
 //     dJ/d eps += -cn e_bar curl_b(H_n; psi_E,n) / eps^2
 //     h_bar += curl_b^T((cn / eps) e_bar)       (psi_E bars likewise)
 // Sources are additive constants and drop out; observation seeds are added to e_bar / h_bar before
-// the transpose of the step whose result they sampled.
+// the transpose of the step whose result they sampled. On a nonuniform mesh the forward scales each plain
+// difference by the cell's metric factor before its CPML terms, so the transpose scales each D value after
+// the CPML memory transpose (reference torchfdtd/differentiable.py:409-418).
 //
 // curl_f^T is a backward difference of the per-H-cell values D(k) (k = 0..n-2, plus the periodic wrap or
 // PEC edge at n-1) and curl_b^T a forward difference of per-E-cell values D(k) (k = 1..n-1, plus the
@@ -68,6 +70,7 @@ __device__ __forceinline__ T d_h(const AdjArgs<T> &A, int q, const RevTerm t, in
     const int c = coord_of<T>(a, x, y, z);
     const T dst = -g.cn * A.hb[q][t.out][k];
     T v = t.sign > 0 ? dst : -dst;
+    const T *mt = g.metric[1][a];
     if (c < g.n[a] - 1) {
         if (A.pHb[q][a][t.j] != nullptr) {
             const int r = adj_slab_row(A.slab[1][a], c);
@@ -78,9 +81,9 @@ __device__ __forceinline__ T d_h(const AdjArgs<T> &A, int q, const RevTerm t, in
                 v = v * g.ck[1][a][c] + g.cc[1][a][c] * m;
             }
         }
-        return v;
+        return mt != nullptr ? v * mt[c] : v;       // the forward scales before its CPML terms
     }
-    if (g.periodic[a]) return v;
+    if (g.periodic[a]) return mt != nullptr ? v * mt[c] : v;
     if (g.pec_on[a]) return -g.pec_neg[a] * v;       // sign * pec * dst
     return T(0);
 }
@@ -128,6 +131,7 @@ __device__ __forceinline__ T d_e(const AdjArgs<T> &A, int q, const RevTerm t, in
     const int c = coord_of<T>(a, x, y, z);
     const T dst = (g.cn * g.inv_eps[t.out][k]) * ebar_out;
     T v = t.sign > 0 ? dst : -dst;
+    const T *mt = g.metric[0][a];
     if (c >= 1) {
         if (A.pEb[q][a][t.j] != nullptr) {
             const int r = adj_slab_row(A.slab[0][a], c);
@@ -138,9 +142,9 @@ __device__ __forceinline__ T d_e(const AdjArgs<T> &A, int q, const RevTerm t, in
                 v = v * g.ck[0][a][c] + g.cc[0][a][c] * m;
             }
         }
-        return v;
+        return mt != nullptr ? v * mt[c] : v;
     }
-    return g.periodic[a] ? v : T(0);
+    return g.periodic[a] ? (mt != nullptr ? v * mt[0] : v) : T(0);
 }
 
 template <typename T, int C>
@@ -200,9 +204,11 @@ __device__ __forceinline__ T forward_curl(const AdjArgs<T> &A, const T *slot, in
         if (g.n[a] == 1) continue;
         const int c = coord_of<T>(a, x, y, z);
         const T *h = slot + A.sH[t.in];
+        const T *mt = g.metric[0][a];
         T d = T(0);
         if (c > 0) {
             d = h[i] - h[i - g.stride(a)];
+            if (mt != nullptr) d = d * mt[c];
             if (A.sPsiE[a][t.j] >= 0) {
                 const int r = adj_slab_row(A.slab[0][a], c);
                 if (r >= 0) {
@@ -213,6 +219,7 @@ __device__ __forceinline__ T forward_curl(const AdjArgs<T> &A, const T *slot, in
             }
         } else if (g.periodic[a]) {
             d = h[i] - h[i + (long long)(g.n[a] - 1) * g.stride(a)];
+            if (mt != nullptr) d = d * mt[0];
         }
         acc = acc + (t.sign > 0 ? d : -d);
     }

@@ -82,6 +82,7 @@ struct Layout {
     size_t E[3], H[3];             // both parities, contiguous
     size_t inv[3];
     size_t cb[2][3], cc[2][3], ck[2][3], row[2][3];
+    size_t metric[2][3];
     int rows[2][3];
     long long psi_len[2][3];
     size_t psiE[3][2], psiH[3][2];
@@ -215,6 +216,7 @@ struct StripGeom {
     struct Slab { int family, axis, lo, hi; };
     std::vector<Slab> slabs;
     std::vector<SourceTerm> sources;
+    bool metric = false;             // nonuniform mesh: every strip takes the general path
 };
 
 StripGeom strip_geom(const tfd_desc *d) {
@@ -228,6 +230,8 @@ StripGeom strip_geom(const tfd_desc *d) {
         SourceTerm q{t.family, t.component, {t.lo[0], t.lo[1], t.lo[2]}, {t.hi[0], t.hi[1], t.hi[2]}};
         G.sources.push_back(q);
     }
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 2; ++a) G.metric = G.metric || d->metric[f][a] != nullptr;
     return G;
 }
 
@@ -235,7 +239,7 @@ StripGeom strip_geom(const tfd_desc *d) {
 // (so that whole strips avoid the y slabs), each band cut into strips of `rows` rows, columns in steps of
 // 31, x-fastest so that neighbouring strips (which share halo columns) run together. A strip is interior
 // (kind 1) when all 32 columns and its rows, halo row included, avoid the grid edges, every CPML slab and
-// every source box; the kernel then runs the bare stencil.
+// every source box, on a uniform mesh; the kernel then runs the bare stencil.
 std::vector<Tile2D> strips_of(const StripGeom &G, int grid_index, int rows) {
     const int nx = G.nx, ny = G.ny;
     int fb0 = 1, fb1 = ny - 1;                       // interior rows: y0 >= fb0 and halo row y1 <= fb1
@@ -269,7 +273,7 @@ std::vector<Tile2D> strips_of(const StripGeom &G, int grid_index, int rows) {
         for (int y0 = bands[b].first; y0 < bands[b].second; y0 += rows) {
             const int y1 = std::min(y0 + rows, bands[b].second);
             for (int x0 = 0; x0 < nx; x0 += k2dOwnX) {
-                const int kind = inner && x_interior(x0) && no_source(x0, y0, y1) ? 1 : 0;
+                const int kind = inner && !G.metric && x_interior(x0) && no_source(x0, y0, y1) ? 1 : 0;
                 t.push_back(Tile2D{grid_index, x0, y0, y1, kind});
             }
         }
@@ -316,6 +320,8 @@ void compute_layout(const tfd_desc *d, Layout &L) {
         L.H[c] = active(d->components, 3 + c) ? b.take(2 * comp_bytes) : 0;
     }
     for (int s = 0; s < 3; ++s) L.inv[s] = s < d->material_samples ? b.take(comp_bytes) : 0;
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 3; ++a) L.metric[f][a] = (d->metric[f][a] && n[a] > 1) ? b.take((size_t)n[a] * L.elem) : 0;
     for (int f = 0; f < 2; ++f)
         for (int a = 0; a < 3; ++a) {
             int rows = 0;
@@ -402,6 +408,7 @@ struct tfd_plan {
     struct MarchLaunch { int mode; dim3 grid; int tx_off, ty_off, lz, z_lo, z_hi; };   // mode 3: the mixed kernel
     MarchMix march_mix{};
     std::vector<MarchLaunch> march_launches;
+    bool march_metric = false;     // nonuniform mesh: the general body with metric factors
     // Boundary strips run on auxiliary streams, forked from and joined back to the caller's stream
     // (a CUDA graph capture records them as parallel branches).
     std::vector<cudaStream_t> aux;
@@ -499,6 +506,16 @@ int create_typed(tfd_plan *p, const tfd_desc *d, cudaStream_t s) {
             g.cc[f][a] = p->ptr<T>(L.cc[f][a]);
             g.ck[f][a] = p->ptr<T>(L.ck[f][a]);
             g.row[f][a] = p->ptr<int>(L.row[f][a]);
+        }
+    // nonuniform-mesh factors
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 3; ++a) {
+            g.metric[f][a] = nullptr;
+            if (!L.metric[f][a]) continue;
+            std::vector<T> vm(n[a]);
+            for (int i = 0; i < n[a]; ++i) vm[i] = (T)d->metric[f][a][i];
+            if (int rc = upload(s, p, L.metric[f][a], vm)) return rc;
+            g.metric[f][a] = p->ptr<T>(L.metric[f][a]);
         }
     for (int a = 0; a < 3; ++a)
         for (int j = 0; j < 2; ++j) {
@@ -712,6 +729,10 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
         TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
         TFD_CUDA(cudaFuncSetAttribute(k_step_march_mixed<T, SAMPLES, D, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)p->march_smem));
+        TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)p->march_smem));
+        TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)p->march_smem));
     }
     const int edge_mode = seams ? 2 : 0;
     int device = 0, sms = 148, per_sm = 1;
@@ -856,9 +877,14 @@ int setup_march(tfd_plan *p) {
         return fail(TFD_ERR_INVALID, "launch variant " + std::to_string(v) + " is not lz*1000 + split*100 + one of " +
                                          (sizeof(T) == 8 ? std::string("22 (FP64)") : std::string("14, 22, 23, 32")));
     const bool three = p->desc.material_samples == 3;
-    const int sp = split;
     const Grid<T> &g = p->grid<T>();
-    switch ((g.periodic[0] || g.periodic[1]) ? periodic_march_variant<T>() : dm) {
+    // A nonuniform mesh runs the general body with its metric factors, one launch over all tiles, at the
+    // launch shape the periodic-seam body is built for.
+    p->march_metric = false;
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 3; ++a) p->march_metric = p->march_metric || g.metric[f][a] != nullptr;
+    const int sp = p->march_metric ? 2 : split;
+    switch ((g.periodic[0] || g.periodic[1] || p->march_metric) ? periodic_march_variant<T>() : dm) {
         case 22: return three ? setup_march_s<T, 3, 2, 2>(p, sp, lz) : setup_march_s<T, 1, 2, 2>(p, sp, lz);
         case 32: return three ? setup_march_s<T, 3, 3, 2>(p, sp, lz) : setup_march_s<T, 1, 3, 2>(p, sp, lz);
         case 14: return three ? setup_march_s<T, 3, 1, 4>(p, sp, lz) : setup_march_s<T, 1, 1, 4>(p, sp, lz);
@@ -880,6 +906,15 @@ void launch_march(tfd_plan *p, cudaStream_t s) {
                     k_step_march_mixed<T, SAMPLES, D, MINB, 2><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), p->march_mix);
             } else {
                 k_step_march_mixed<T, SAMPLES, D, MINB, 0><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), p->march_mix);
+            }
+        } else if (p->march_metric) {
+            if constexpr (D * 10 + MINB == periodic_march_variant<T>()) {
+                if (l.mode == 2)
+                    k_step_march<T, SAMPLES, D, MINB, 2, true><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off,
+                                                                                                           l.ty_off, l.lz, l.z_lo, l.z_hi);
+                else
+                    k_step_march<T, SAMPLES, D, MINB, 0, true><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off,
+                                                                                                           l.ty_off, l.lz, l.z_lo, l.z_hi);
             }
         } else if (l.mode == 1)
             k_step_march<T, SAMPLES, D, MINB, 1><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz,
@@ -920,6 +955,8 @@ StripGeom strip_geom(tfd_plan *p) {
     G.ny = g.n[1];
     for (size_t k = 0; k < p->seg_f.size(); ++k) G.slabs.push_back({p->seg_f[k], p->seg_a[k], p->seg_lo[k], p->seg_hi[k]});
     for (int k = 0; k < g.n_src; ++k) G.sources.push_back(g.src[k]);
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 2; ++a) G.metric = G.metric || g.metric[f][a] != nullptr;
     return G;
 }
 

@@ -62,6 +62,8 @@ struct Grid {
     const T *cb[2][3], *cc[2][3], *ck[2][3];
     const int *row[2][3];
     int rows[2][3];
+    // Nonuniform-mesh factors per family and axis, indexed by the updated cell (nullptr: uniform axis).
+    const T *metric[2][3];
     T *psiE[2][3][2];            // [parity][axis][term j]
     T *psiH[3][2];               // [axis][term j]
     int n_src;

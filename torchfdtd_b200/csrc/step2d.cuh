@@ -21,7 +21,8 @@
 // slabs, soft sources added after each family's update (E sources before Ez_new feeds the H update).
 // Grids of a batch may have different step counts: a grid whose run has ended is skipped, so its state stays
 // that of its last step while longer grids continue. Supported: x/y faces PML or PEC (periodic 2D grids run
-// the gather kernel).
+// the gather kernel). A grid on a nonuniform mesh has no interior strips: the general path multiplies each
+// plain difference by the metric factor of the updated cell before its CPML terms.
 #pragma once
 #include <algorithm>
 
@@ -155,6 +156,11 @@ __device__ __forceinline__ void strip_general(const Grid<T> &g, const Tile2D &st
     T *psiHx = g.psiH[0][0];                           // Hy term dx(Ez), updated in place
     const bool pec_x = g.pec_on[0] != 0, pec_y = g.pec_on[1] != 0;
     const T pneg_x = g.pec_neg[0], pneg_y = g.pec_neg[1];
+    // Nonuniform mesh: x factors of this lane's column, y factors read per row (nullptr: uniform axis).
+    const T *my_e = g.metric[0][1], *my_h = g.metric[1][1];
+    const T mx_e = (g.metric[0][0] != nullptr && in_x) ? g.metric[0][0][x] : T(1);
+    const T mx_h = (g.metric[1][0] != nullptr && in_x) ? g.metric[1][0][x] : T(1);
+    const bool mx = g.metric[0][0] != nullptr;
     // Sources meeting this strip (E with the halo lane and halo row), tested once per strip.
     unsigned src_e = 0, src_hx = 0, src_hy = 0;
     for (int t = 0; t < g.n_src; ++t) {
@@ -210,6 +216,7 @@ __device__ __forceinline__ void strip_general(const Grid<T> &g, const Tile2D &st
                 if (lane == 0) hy_left = r.hyl;
                 // Ez: dx(Hy) ...
                 T d = x > 0 ? r.hy - hy_left : T(0);
+                if (mx && x > 0) d = d * mx_e;
                 if (rxE >= 0) {
                     const T mem = r.pex * bxE + cxE * d;
                     if (own && y < y1) psiExn[(long long)y * RxE + rxE] = mem;
@@ -218,6 +225,7 @@ __device__ __forceinline__ void strip_general(const Grid<T> &g, const Tile2D &st
                 T acc = T(0) + d;
                 // ... then -dy(Hx)
                 d = y > 0 ? r.hx - hx_prev : T(0);
+                if (my_e != nullptr && y > 0) d = d * my_e[y];
                 if (r.rye >= 0 && in_x) {
                     const T mem = r.pey * g.cb[0][1][y] + g.cc[0][1][y] * d;
                     if (own && y < y1) psiEyn[(long long)r.rye * pitch + x] = mem;
@@ -235,6 +243,7 @@ __device__ __forceinline__ void strip_general(const Grid<T> &g, const Tile2D &st
                 T d = T(0);
                 if (h < ny - 1) {
                     d = ez_new - ez_prev;
+                    if (my_h != nullptr) d = d * my_h[h];
                     if (r.ryh >= 0 && in_x) {
                         const T mem = r.phy * g.cb[1][1][h] + g.cc[1][1][h] * d;
                         if (own) psiHy[(long long)r.ryh * pitch + x] = mem;
@@ -249,6 +258,7 @@ __device__ __forceinline__ void strip_general(const Grid<T> &g, const Tile2D &st
                 d = T(0);
                 if (x < nx - 1) {
                     d = ez_right - ez_prev;
+                    if (mx) d = d * mx_h;
                     if (rxH >= 0) {
                         const T mem = r.phx * bxH + cxH * d;
                         if (own) psiHx[(long long)h * RxH + rxH] = mem;

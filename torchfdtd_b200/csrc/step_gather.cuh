@@ -9,7 +9,8 @@
 // reference operation order (torchfdtd/boundaries.py:363-438, torchfdtd/cuda_kernels.py:
 // 186-259,327-347): d = F[i] - F[i-1]; psi = psi*b + c*d; d = d*(1/kappa) + psi;
 // curl = (0 + s0*d0) + s1*d1; E += (cn*inv_eps)*curl; H -= cn*curl; soft sources are
-// added after the family update. The library is compiled with --fmad=false so no
+// added after the family update. On a nonuniform mesh each plain difference (periodic wrap
+// included, PEC ghost excluded) is first multiplied by the metric factor of the updated cell. The library is compiled with --fmad=false so no
 // multiply-add is contracted, as in the reference's NVRTC build.
 //
 // This kernel is the parity baseline and the fallback for shapes the marching
@@ -41,9 +42,11 @@ __device__ __forceinline__ void e_term(const Grid<T> &g, int par, int x, int y, 
     if (g.n[a] == 1) return;
     const int coord = a == 0 ? x : (a == 1 ? y : z);
     const T *h = g.H[par][t.in];
+    const T *mt = g.metric[0][a];
     T d = T(0);
     if (coord > 0) {
         d = h[i] - h[i - g.stride(a)];
+        if (mt != nullptr) d = d * mt[coord];
         const int *rm = g.row[0][a];
         if (rm != nullptr) {
             const int r = rm[coord];
@@ -56,6 +59,7 @@ __device__ __forceinline__ void e_term(const Grid<T> &g, int par, int x, int y, 
         }
     } else if (g.periodic[a]) {
         d = h[i] - h[i + (long long)(g.n[a] - 1) * g.stride(a)];
+        if (mt != nullptr) d = d * mt[0];
     }
     acc = acc + (t.sign > 0 ? d : -d);
 }
@@ -84,9 +88,11 @@ __device__ __forceinline__ void h_term(const Grid<T> &g, int par, long long n, i
     const int a = t.axis;
     if (g.n[a] == 1) return;
     const int coord = a == 0 ? x : (a == 1 ? y : z);
+    const T *mt = g.metric[1][a];
     T d = T(0);
     if (coord < g.n[a] - 1) {
         d = e_neighbour<T, t.in>(g, par, n, a, x, y, z, i, coord + 1) - e_own[t.in];
+        if (mt != nullptr) d = d * mt[coord];
         const int *rm = g.row[1][a];
         if (rm != nullptr) {
             const int r = rm[coord];
@@ -100,6 +106,7 @@ __device__ __forceinline__ void h_term(const Grid<T> &g, int par, long long n, i
         }
     } else if (g.periodic[a]) {
         d = e_neighbour<T, t.in>(g, par, n, a, x, y, z, i, 0) - e_own[t.in];
+        if (mt != nullptr) d = d * mt[coord];
     } else if (g.pec_on[a]) {
         d = g.pec_neg[a] * e_own[t.in];
     }

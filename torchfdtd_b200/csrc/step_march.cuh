@@ -189,8 +189,10 @@ struct Rows { int x, y, z; int po[3], pn[3]; Coef<T> qx, qy, qz; };
 // plane z has a previous plane): plain differences in the reference order. hk / hm: H stage of plane
 // k / k-1 (box row 0 = y0-1, stride HS); ek: E stage of plane k (box row 0 = y0, stride ES); s / se: the
 // cell's element index in those boxes.
-template <typename T, int SAMPLES, int D, int C>
-__device__ __forceinline__ T march_e_fast(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se) {
+// METRIC: nonuniform mesh, each difference times the cell's factor of its axis (m[0..2]).
+template <typename T, int SAMPLES, int D, int C, bool METRIC = false>
+__device__ __forceinline__ T march_e_fast(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se,
+                                         const T *m = nullptr) {
     using S = MarchShape<T, SAMPLES, D>;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
@@ -199,7 +201,8 @@ __device__ __forceinline__ T march_e_fast(const Grid<T> &g, const T *hk, const T
     for (int k = 0; k < 2; ++k) {
         const Term t = term_of(C, k);
         const T *h = hk + t.in * HS;
-        const T d = t.axis == 0 ? h[s] - h[s - 1] : t.axis == 1 ? h[s] - h[s - S::BXW] : h[s] - hm[t.in * HS + s];
+        T d = t.axis == 0 ? h[s] - h[s - 1] : t.axis == 1 ? h[s] - h[s - S::BXW] : h[s] - hm[t.in * HS + s];
+        if constexpr (METRIC) d = d * m[t.axis];
         acc = acc + (t.sign > 0 ? d : -d);
     }
     return ek[C * ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? C : 0)) * ES + se]) * acc;
@@ -305,9 +308,10 @@ __device__ __forceinline__ void march_h_zslab(const Grid<T> &g, const T *ep, con
 // memories of the cell's active slabs are loaded first, so their loads are in flight together, then
 // the terms run in the reference order (y-term, z-term of Ex; x, z of Ey; x, y of Ez) and the owner
 // stores the new memories. rw.x / rw.y / rw.z: slab rows (-1 outside); x, y: the cell's coordinates.
-template <typename T, int SAMPLES, int D, bool CPML, bool WRAP>
+template <typename T, int SAMPLES, int D, bool CPML, bool WRAP, bool METRIC = false>
 __device__ __forceinline__ void march_e_row(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, int x, int y,
-                                            int z, bool zprev, bool own, const Rows<T> &rw, T &ex, T &ey, T &ez) {
+                                            int z, bool zprev, bool own, const Rows<T> &rw, T &ex, T &ey, T &ez,
+                                            const T *m = nullptr) {
     using S = MarchShape<T, SAMPLES, D>;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
@@ -336,29 +340,34 @@ __device__ __forceinline__ void march_e_row(const Grid<T> &g, const T *hk, const
     };
     T d, acc;
     // Ex: (y, Hz, +, j0), (z, Hy, -, j0)
-    d = yin ? Hz[s] - Hz[s - S::BXW] : T(0);
+    // Nonuniform mesh: a plain difference (periodic seam included) times the cell's factor of its axis.
+    auto scale = [&](bool live, int a, T d) -> T {
+        if constexpr (METRIC) return live ? d * m[a] : d;
+        return d;
+    };
+    d = scale(yin, 1, yin ? Hz[s] - Hz[s - S::BXW] : T(0));
     if (CPML && ay) d = mem(1, 0, iy, oy0, rw.qy, d);
     acc = T(0);
     acc = acc + d;
-    d = zprev ? Hy[s] - hm[HS + s] : T(0);
+    d = scale(zprev, 2, zprev ? Hy[s] - hm[HS + s] : T(0));
     if (CPML && az) d = mem(2, 0, iz, oz0, rw.qz, d);
     acc = acc + (-d);
     ex = ek[se] + (g.cn * ek[3 * ES + se]) * acc;
     // Ey: (x, Hz, -, j0), (z, Hx, +, j1)
-    d = xin ? Hz[s] - Hz[s - 1] : T(0);
+    d = scale(xin, 0, xin ? Hz[s] - Hz[s - 1] : T(0));
     if (CPML && ax) d = mem(0, 0, ix, ox0, rw.qx, d);
     acc = T(0);
     acc = acc + (-d);
-    d = zprev ? Hx[s] - hm[s] : T(0);
+    d = scale(zprev, 2, zprev ? Hx[s] - hm[s] : T(0));
     if (CPML && az) d = mem(2, 1, iz, oz1, rw.qz, d);
     acc = acc + d;
     ey = ek[ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? 1 : 0)) * ES + se]) * acc;
     // Ez: (x, Hy, +, j1), (y, Hx, -, j1)
-    d = xin ? Hy[s] - Hy[s - 1] : T(0);
+    d = scale(xin, 0, xin ? Hy[s] - Hy[s - 1] : T(0));
     if (CPML && ax) d = mem(0, 1, ix, ox1, rw.qx, d);
     acc = T(0);
     acc = acc + d;
-    d = yin ? Hx[s] - Hx[s - S::BXW] : T(0);
+    d = scale(yin, 1, yin ? Hx[s] - Hx[s - S::BXW] : T(0));
     if (CPML && ay) d = mem(1, 1, iy, oy1, rw.qy, d);
     acc = acc + (-d);
     ez = ek[2 * ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? 2 : 0)) * ES + se]) * acc;
@@ -368,10 +377,10 @@ __device__ __forceinline__ void march_e_row(const Grid<T> &g, const T *hk, const
 // become selects: the difference to the +x / +y / +z neighbour, else the PEC ghost term, else 0.
 // CPML: as for E, with the H-family memories updated in place. ep: E_new of plane km (the cell's
 // plane, with the +x column and +y row), ec: E_new of plane km + 1; e: the cell's index in both.
-template <typename T, int SAMPLES, int D, bool CPML>
+template <typename T, int SAMPLES, int D, bool CPML, bool METRIC = false>
 __device__ __forceinline__ void march_h_row(const Grid<T> &g, const T *ep, const T *ec, const T *hs, int sh, int e, int x, int y,
                                             int km, bool xn, bool yn, bool znext, int rx, int ry, int rz, const Coef<T> &qx,
-                                            const Coef<T> &qy, const Coef<T> &qz, T &hx, T &hy, T &hz) {
+                                            const Coef<T> &qy, const Coef<T> &qz, T &hx, T &hy, T &hz, const T *m = nullptr) {
     using S = MarchShape<T, SAMPLES, D>;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int EB = S::EBUF;
@@ -395,9 +404,17 @@ __device__ __forceinline__ void march_h_row(const Grid<T> &g, const T *ep, const
         g.psiH[a][j][idx] = m;
         return d * q.k + m;
     };
-    auto dx = [&](const T *f) -> T { return xn ? f[e + 1] - f[e] : (g.pec_on[0] ? g.pec_neg[0] * f[e] : T(0)); };
-    auto dy = [&](const T *f) -> T { return yn ? f[e + kMarchLanes] - f[e] : (g.pec_on[1] ? g.pec_neg[1] * f[e] : T(0)); };
-    auto dz = [&](int c) -> T { return znext ? ec[c * EB + e] - ep[c * EB + e] : (g.pec_on[2] ? g.pec_neg[2] * ep[c * EB + e] : T(0)); };
+    // A neighbour difference (periodic seam included) times the cell's factor of its axis on a nonuniform mesh;
+    // the PEC ghost term is not scaled.
+    auto nb = [&](int a, T d) -> T {
+        if constexpr (METRIC) return d * m[a];
+        return d;
+    };
+    auto dx = [&](const T *f) -> T { return xn ? nb(0, f[e + 1] - f[e]) : (g.pec_on[0] ? g.pec_neg[0] * f[e] : T(0)); };
+    auto dy = [&](const T *f) -> T { return yn ? nb(1, f[e + kMarchLanes] - f[e]) : (g.pec_on[1] ? g.pec_neg[1] * f[e] : T(0)); };
+    auto dz = [&](int c) -> T {
+        return znext ? nb(2, ec[c * EB + e] - ep[c * EB + e]) : (g.pec_on[2] ? g.pec_neg[2] * ep[c * EB + e] : T(0));
+    };
     const T *Ex = ep, *Ey = ep + EB, *Ez = ep + 2 * EB;
     T d, acc;
     // Hx: (y, Ez, +, j0), (z, Ey, -, j0)
@@ -439,7 +456,9 @@ __device__ __forceinline__ void march_h_row(const Grid<T> &g, const T *ep, const
 // rows, and z rows in march_e_zslab / march_h_zslab. Tile (tx, ty) of a launch is (blockIdx.x + tx_off, blockIdx.y + ty_off); chunk blockIdx.z
 // covers planes [z_lo + blockIdx.z * lz, min(that + lz, z_hi)).
 // The body of one CTA: tile (tx, ty), planes [z0, z1).
-template <typename T, int SAMPLES, int D, int MODE>
+// METRIC (general bodies only): a nonuniform mesh; every plain difference is scaled by the updated cell's factor
+// of its axis (1 on a uniform axis), the z tier is off and z-slab rows take the general CPML rows.
+template <typename T, int SAMPLES, int D, int MODE, bool METRIC = false>
 __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int ty, int z0, int z1) {
     using S = MarchShape<T, SAMPLES, D>;
     // MODE 4 (z-pure) runs interior tiles (as MODE 1) on any planes: fast rows, and z rows (a z slab, or the
@@ -451,7 +470,8 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     // x / y body, where such rows are most of the general work (CPML on z only): 0.575 against 0.612 ms per
     // step at 512 x 512 x 128. With x / y slabs the general work is mostly x / y slab rows, and the extra tier
     // cost the 512 x 512 x 256 CPML step 1.3 % (instruction cache); there the z-pure body takes them.
-    constexpr bool ZTIER = MODE == 2 || ZPURE;
+    constexpr bool ZTIER = (MODE == 2 || ZPURE) && !METRIC;
+    static_assert(!METRIC || MODE == 0 || MODE == 2, "the metric variant is a general body");
     // The general and z-pure bodies keep their row loops rolled: unrolled, the general body's three row tiers
     // exist once per row and the code outgrows the instruction cache once a pure body shares the SM
     // (measured: 75 % vs 94 % hits).
@@ -532,6 +552,12 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     const int xc = (px && x == nx) ? 0 : x;
     const bool lane_own = lane < kMarchOwnX && x < nx;
     const bool lane_in = x < nx || (px && x == nx);
+    // Nonuniform mesh: this lane's x factors (E at column xc, H at column x), 1 on a uniform axis.
+    T mxE = T(1), mxH = T(1);
+    if constexpr (METRIC) {
+        if (g.metric[0][0] != nullptr && lane_in) mxE = g.metric[0][0][xc];
+        if (g.metric[1][0] != nullptr && x < nx) mxH = g.metric[1][0][x];
+    }
     // Per-thread CPML state (slab rows, coefficients) is built on the rows that meet a slab, where it
     // is used, and not kept across the plane loop: under the 64-register budget of 4 CTAs per SM it
     // would crowd the fast path.
@@ -656,6 +682,10 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                                               : 0u;
             T *gE0 = g.E[0][0] + fn + (size_t)kz * g.plane, *gE1 = g.E[0][1] + fn + (size_t)kz * g.plane,
               *gE2 = g.E[0][2] + fn + (size_t)kz * g.plane;
+            T mzE = T(1);
+            if constexpr (METRIC) {
+                if (g.metric[0][2] != nullptr) mzE = g.metric[0][2][kz];
+            }
 #pragma unroll kRowUnroll
             for (int h = 0; h < kMarchRowsPerThread; ++h) {
                 const int r = warp + kMarchWarps * h;
@@ -667,24 +697,28 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                 const int sh = (r + 1) * S::BXW + off + lane;
                 const int se = r * S::BXW + off + lane;
                 const Rows<T> &rw = no_rows;
+                T mE[3] = {mxE, T(1), mzE};
+                if constexpr (METRIC) {
+                    if (g.metric[0][1] != nullptr) mE[1] = g.metric[0][1][yc];
+                }
                 T ex, ey, ez;
                 const bool cpml_row = ((rowbits >> h) & 1u) || rzE >= 0;
                 const bool plain_xy = !((rowbits >> h) & 1u) && !((rowbits >> (R + h)) & 1u) && zprev && !smask;
                 const bool fast = MODE == 1 || (ZPURE ? rzE < 0 && zprev : !cpml_row && plain_xy);
                 if (fast) {
-                    ex = march_e_fast<T, SAMPLES, D, 0>(g, hk, hm, ek, sh, se);
-                    ey = march_e_fast<T, SAMPLES, D, 1>(g, hk, hm, ek, sh, se);
-                    ez = march_e_fast<T, SAMPLES, D, 2>(g, hk, hm, ek, sh, se);
+                    ex = march_e_fast<T, SAMPLES, D, 0, METRIC>(g, hk, hm, ek, sh, se, mE);
+                    ey = march_e_fast<T, SAMPLES, D, 1, METRIC>(g, hk, hm, ek, sh, se, mE);
+                    ez = march_e_fast<T, SAMPLES, D, 2, METRIC>(g, hk, hm, ek, sh, se, mE);
                 } else if (ZPURE || (ZTIER && plain_xy)) {
                     // A z-slab row (rzE >= 0), or in the z-pure body also the first plane of the grid (!zprev).
                     const int pz = args.psi_parity[2];
                     march_e_zslab<T, SAMPLES, D>(g, hk, hm, ek, sh, se, zprev, zprev && rzE >= 0, (rzE * ny + yc) * g.pitch + xc,
                                                  par ? pz : 0, par ? 0 : pz, own, coef_at(g, 0, 2, kz, rzE), ex, ey, ez);
                 } else if (!cpml_row) {
-                    march_e_row<T, SAMPLES, D, false, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw, ex, ey, ez);
+                    march_e_row<T, SAMPLES, D, false, PXY, METRIC>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rw, ex, ey, ez, mE);
                 } else {
                     const Rows<T> rc = e_rows(xc, yc, kz, rzE);
-                    march_e_row<T, SAMPLES, D, true, PXY>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rc, ex, ey, ez);
+                    march_e_row<T, SAMPLES, D, true, PXY, METRIC>(g, hk, hm, ek, sh, se, xc, yc, kz, zprev, own, rc, ex, ey, ez, mE);
                 }
                 if (smask) {
                     ex = inject_masked(g, smask, 0, 0, n, xc, yc, kz, ex);
@@ -721,6 +755,10 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
             const unsigned hmask = tile_src_h ? source_mask(g, 1, x0, x0 + kMarchOwnX, y0, y0 + kMarchOwnY, km, n) & tile_src_h : 0u;
             T *gH[3] = {g.H[0][0] + fn + (size_t)km * g.plane, g.H[0][1] + fn + (size_t)km * g.plane,
                         g.H[0][2] + fn + (size_t)km * g.plane};
+            T mzH = T(1);
+            if constexpr (METRIC) {
+                if (g.metric[1][2] != nullptr) mzH = g.metric[1][2][km];
+            }
 #pragma unroll kRowUnroll
             for (int h = 0; h < kMarchRowsPerThread; ++h) {
                 const int r = warp + kMarchWarps * h;
@@ -731,14 +769,20 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                 const int i = y * g.pitch + x;
                 const bool cpml_row = ((rowbits >> (2 * R + h)) & 1u) || rzH >= 0;
                 const bool fast = MODE == 1 || (ZPURE ? rzH < 0 && znext : !cpml_row && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask);
+                T mH[3] = {mxH, T(1), mzH};
+                if constexpr (METRIC) {
+                    if (g.metric[1][1] != nullptr) mH[1] = g.metric[1][1][y];
+                }
                 if (fast) {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const Term t0 = term_of(c, 0), t1 = term_of(c, 1);
                         auto dif = [&](const Term &tm) -> T {
                             const T *ep = eprv + tm.in * S::EBUF;
-                            return tm.axis == 0 ? ep[e + 1] - ep[e]
-                                 : tm.axis == 1 ? ep[e + kMarchLanes] - ep[e] : ecur[tm.in * S::EBUF + e] - ep[e];
+                            const T d = tm.axis == 0 ? ep[e + 1] - ep[e]
+                                      : tm.axis == 1 ? ep[e + kMarchLanes] - ep[e] : ecur[tm.in * S::EBUF + e] - ep[e];
+                            if constexpr (METRIC) return d * mH[tm.axis];
+                            return d;
                         };
                         const T d0 = dif(t0), d1 = dif(t1);
                         T acc = T(0);
@@ -760,13 +804,13 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                                                      coef_at(g, 1, 2, km, rzH), hv[0], hv[1], hv[2]);
                     } else if (cpml_row) {
                         const int rx = TFD_SLAB_ROW(args, 1, 0, x), ry = TFD_SLAB_ROW(args, 1, 1, y);
-                        march_h_row<T, SAMPLES, D, true>(g, eprv, ecur, hs, sh, e, x, y, km, xn, yn, znext, rx, ry, rzH,
-                                                         coef_at(g, 1, 0, x, rx), coef_at(g, 1, 1, y, ry), coef_at(g, 1, 2, km, rzH),
-                                                         hv[0], hv[1], hv[2]);
+                        march_h_row<T, SAMPLES, D, true, METRIC>(g, eprv, ecur, hs, sh, e, x, y, km, xn, yn, znext, rx, ry, rzH,
+                                                                 coef_at(g, 1, 0, x, rx), coef_at(g, 1, 1, y, ry),
+                                                                 coef_at(g, 1, 2, km, rzH), hv[0], hv[1], hv[2], mH);
                     } else {
                         const Coef<T> q0{T(0), T(0), T(1)};
-                        march_h_row<T, SAMPLES, D, false>(g, eprv, ecur, hs, sh, e, x, y, km, xn, yn, znext, -1, -1, -1, q0, q0, q0,
-                                                          hv[0], hv[1], hv[2]);
+                        march_h_row<T, SAMPLES, D, false, METRIC>(g, eprv, ecur, hs, sh, e, x, y, km, xn, yn, znext, -1, -1, -1, q0, q0,
+                                                                  q0, hv[0], hv[1], hv[2], mH);
                     }
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
@@ -785,11 +829,11 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     }
 }
 
-template <typename T, int SAMPLES, int D, int MINB, int MODE>
+template <typename T, int SAMPLES, int D, int MINB, int MODE, bool METRIC = false>
 __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid_constant__ MarchArgs<T> args, int tx_off, int ty_off,
                                                                     int lz, int z_lo, int z_hi) {
     const int z0 = z_lo + blockIdx.z * lz;
-    march_body<T, SAMPLES, D, MODE>(args, blockIdx.x + tx_off, blockIdx.y + ty_off, z0, min(z0 + lz, z_hi));
+    march_body<T, SAMPLES, D, MODE, METRIC>(args, blockIdx.x + tx_off, blockIdx.y + ty_off, z0, min(z0 + lz, z_hi));
 }
 
 // One launch over every tile and z chunk in which each CTA takes the pure body (MODE 1) when its tile is in

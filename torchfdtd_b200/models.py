@@ -97,6 +97,12 @@ class MeshRefinement(Model):
     size: tuple[float, float, float] = (1, 1, 1)
     enabled: bool = True
 
+    @model_validator(mode='after')
+    def positive_size(self):
+        if min(self.size) <= 0:
+            raise ValueError('Refinement spans must be positive.')
+        return self
+
 
 class RunControl(Model):
     auto_shutoff: bool = False
@@ -156,6 +162,15 @@ class Region(Model):
     slice_axis: Literal['x', 'y', 'z'] = 'z'
     slice_position: float = 0
     complex_display: Literal['real', 'imag', 'magnitude', 'phase'] = 'real'
+    def __eq__(self, other):
+        # The cached node arrays are derived state; the automatic refinement boxes and coarse limit are not.
+        if not isinstance(other, Region):
+            return NotImplemented
+        return (self.model_dump() == other.model_dump() and self._auto_boxes == other._auto_boxes
+                and self._coarse_limit == other._coarse_limit)
+
+    _auto_boxes: tuple = PrivateAttr(default=())
+    _coarse_limit: float | None = PrivateAttr(default=None)
     _nodes: object = PrivateAttr(default=None)
 
     @model_serializer(mode='wrap')
@@ -216,23 +231,9 @@ class Region(Model):
 
     @property
     def mesh_nodes(self):
-        """Node coordinates (um) per axis. Uniform meshes only; others are refused by the planner."""
-        key = (self.mesh_type, self.dimension, tuple(self.size), self.mesh, self.mesh_steps, self.mesh_coordinates)
-        if self._nodes is None or self._nodes[0] != key:
-            if self.mesh_type != 'uniform' and self.mesh_type != 'explicit':
-                raise ValueError('Graded meshes are not implemented by the fused B200 engine; use mesh_type="uniform".')
-            nodes = []
-            for axis, n in enumerate(self.base_shape):
-                if self.mesh_type == 'explicit':
-                    a = np.asarray(self.mesh_coordinates[axis], dtype=float)
-                elif self.dimension == '2d' and axis == 2:
-                    a = np.array([-self.size[2] / 2, self.size[2] / 2])
-                else:
-                    a = np.arange(n + 1) * self.axis_steps[axis] - n * self.axis_steps[axis] / 2
-                a.setflags(write=False)
-                nodes.append(a)
-            self._nodes = (key, tuple(nodes))
-        return self._nodes[1]
+        """Node coordinates (um) per axis (uniform, axis-specific, explicit or graded; ``mesh.mesh_nodes``)."""
+        from .mesh import mesh_nodes
+        return mesh_nodes(self)
 
     @property
     def time_step(self):
@@ -285,8 +286,6 @@ class Region(Model):
             raise ValueError('Graded, explicit and axis-specific meshes require Yee material sampling.')
         if self.time_step_override is not None and self.time_step_override > self.cfl_time_step * (1 + 1e-12):
             raise ValueError('The time-step override exceeds the configured conservative CFL limit.')
-        if self.mesh_type == 'graded':
-            return self  # refused by the planner; the graded node generator is outside this engine
         active = self.shape[:2] if self.dimension == '2d' else self.shape
         for axis, n in enumerate(active):
             low, high = self.boundaries.pair(axis)
@@ -578,8 +577,14 @@ class Project(Model):
         if self.global_source is None and any(s.use_global_source for s in self.sources):
             raise ValueError('Global source settings are unavailable. Configure them before enabling inheritance.')
         r = self.region
-        if r.mesh_type == 'graded':
-            return self
+        from .mesh import configure_auto_mesh
+        configure_auto_mesh(self)
+        r.valid_grid()
+        for source in self.sources:
+            resolved = self.resolved_source(source)
+            if resolved.enabled and resolved.injection == 'oneway' and resolved.kind != 'tfsf':
+                from .injection import oneway_plan
+                oneway_plan(resolved, r)
         dt = r.time_step
         from .spectra import highest_frequency
         from .waveforms import pulse_parameters

@@ -17,7 +17,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / 'libtfdtd.so'
 
-TFD_ABI_VERSION = 1
+TFD_ABI_VERSION = 2
 TFD_DEVICE, TFD_HOST = 0, 1
 KERNELS = {'auto': 0, 'march': 1, 'gather': 2, 'tile2d': 3}
 FACE = {'pml': 0, 'periodic': 1, 'pec': 2, 'antisymmetric': 2}
@@ -56,7 +56,7 @@ class Desc(ctypes.Structure):
                 ('n_segments', c_i32), ('segments', ctypes.POINTER(CpmlSegment)),
                 ('n_sources', c_i32), ('sources', ctypes.POINTER(SourceTermC)),
                 ('n_traces', c_i32), ('traces', ctypes.POINTER(TraceC)),
-                ('n_planes', c_i32), ('planes', ctypes.POINTER(PlaneC))]
+                ('n_planes', c_i32), ('planes', ctypes.POINTER(PlaneC)), ('metric', (P_dbl * 3) * 2)]
 
 
 # Every entry point of include/tfdtd.h with its ctypes signature.
@@ -267,6 +267,13 @@ def describe(plan, kernel='auto', variant=0):
                            _ptr(weights, ctypes.c_double), _ptr(freq, ctypes.c_double), _ptr(we, ctypes.c_double),
                            _ptr(wh, ctypes.c_double))
     desc.n_planes, desc.planes = len(plan.planes), planes
+    for f in range(2):
+        for a in range(3):
+            table = plan.metric_table(f, a) if hasattr(plan, 'metric_table') else None
+            if table is not None:
+                table = np.ascontiguousarray(table, dtype=np.float64)
+                keep.append(table)
+                desc.metric[f][a] = _ptr(table, ctypes.c_double)
     keep.extend([segs, srcs, traces, planes])
     return desc, keep
 

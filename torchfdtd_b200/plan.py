@@ -125,6 +125,7 @@ class GridPlan:
     planes: list
     polarization: str | None = None
     warnings: list = field(default_factory=list)
+    metrics: dict = field(default_factory=dict)   # (forward, axis) -> (float64 (n-1,) interior values, wrap value)
 
     @property
     def cells(self):
@@ -147,6 +148,18 @@ class GridPlan:
                         s[axis] = seg.hi - seg.lo
                         shapes.append(((forward, axis, comp, seg.side), tuple(s)))
         return shapes
+
+    def metric_table(self, family, axis):
+        """Per-target-cell metric factors of one family and axis (float64, length n), or None on an axis whose
+        cells all have the reference step. E (family 0) at cell i differences H across the dual cell i-1/i: entry
+        i >= 1 is the dual factor i-1, entry 0 the periodic wrap factor. H (family 1) at cell i differences E across
+        cell i: entry i <= n-2 is that cell's factor, entry n-1 the wrap factor. A kernel multiplies the plain
+        difference by the entry of the cell it updates, before the CPML terms."""
+        forward = family == 1
+        if (forward, axis) not in self.metrics:
+            return None
+        values, wrap = self.metrics[forward, axis]
+        return np.r_[values, wrap] if forward else np.r_[wrap, values]
 
     def active_components(self):
         """Field components the kernels advance: all six in 3D, one 2D polarization (or both) in 2D."""
@@ -208,8 +221,6 @@ def source_slice(src, r):
 # ---- refusal of features outside the fused nondispersive path -------------------------------
 def check_supported(project):
     r = project.region
-    if r.mesh_type != 'uniform' or r.mesh_steps is not None:
-        raise ValueError('Graded, explicit and axis-specific meshes are not implemented by the fused B200 engine; use a uniform mesh.')
     if r.interface_method != 'staircase':
         raise ValueError('Subpixel interfaces are not implemented by the fused B200 engine; use interface_method="staircase".')
     if r.complex_fields:
@@ -228,9 +239,32 @@ def check_supported(project):
         s = project.resolved_source(raw)
         if not s.enabled:
             continue
-        if s.kind == 'tfsf' or s.injection == 'oneway':
-            raise ValueError(f'{s.name}: one-way and TFSF injection are not implemented by the fused B200 engine; use soft sources.')
+        if s.kind == 'tfsf':
+            raise ValueError(f'{s.name}: TFSF injection is not implemented by the fused B200 engine; use soft or one-way sources.')
     r.require_resident()
+
+
+# ---- nonuniform meshes ----------------------------------------------------------------------------
+def mesh_metrics(region):
+    """Difference scale factors of a nonuniform mesh (reference ``torchfdtd/boundaries.py:276-284``).
+
+    The update works in units of the reference step: on an axis whose cell widths w are not all the reference
+    step h, a forward (H) difference across cell i is scaled by h / w[i] and a backward (E) difference across
+    the dual cell between centres i and i+1 by h / ((w[i] + w[i+1]) / 2); the periodic wrap uses the last cell
+    (H) and the mean of the first and last cells (E). Returns {(forward, axis): (interior float64, wrap)}."""
+    out = {}
+    if region.mesh_type == 'uniform' and region.mesh_steps is None:
+        return out
+    h = region.reference_step
+    for axis, nodes in enumerate(region.mesh_nodes):
+        if region.shape[axis] == 1:
+            continue
+        widths = np.diff(nodes)
+        if np.allclose(widths, h, rtol=1e-10, atol=0):
+            continue
+        out[True, axis] = (h / widths[:-1], float(h / widths[-1]))
+        out[False, axis] = (h / ((widths[1:] + widths[:-1]) / 2), float(2 * h / (widths[0] + widths[-1])))
+    return out
 
 
 # ---- CPML ------------------------------------------------------------------------------------
@@ -256,6 +290,16 @@ def cpml_segments(region, courant):
                 depth = layers - target - (1 if forward else .5) if side == 0 else target + (1 if forward else .5)
                 rho = depth / (layers + 1)
                 sigma = face.sigma_scale * 40 * rho**face.polynomial / (layers + 1)
+                if region.mesh_type == 'explicit' or region.mesh_steps is not None:
+                    # Physical grading: depth measured in um from the slab's inner interface, over the slab
+                    # thickness plus one cell; sigma scaled by reference step / that length.
+                    nodes = region.mesh_nodes[axis]
+                    widths = np.diff(nodes)
+                    where = nodes[lo + 1:hi + 1] if forward else (nodes[lo:hi] + nodes[lo + 1:hi + 1]) / 2
+                    inner = nodes[layers] if side == 0 else nodes[base]
+                    span = (nodes[layers] - nodes[0] + widths[layers]) if side == 0 else (nodes[-1] - nodes[base] + widths[base - 1])
+                    rho = ((inner - where) if side == 0 else (where - inner)) / span
+                    sigma = face.sigma_scale * 40 * region.reference_step / span * rho**face.polynomial
                 kappa = 1 + (face.kappa - 1) * rho**face.polynomial
                 alpha = face.alpha * (1 - rho)**face.alpha_polynomial
                 decay = np.exp(-(sigma / kappa + alpha) * courant)
@@ -399,8 +443,11 @@ def plan_grid(project, polarization=None, material=True):
     pec_upper = {a: float(r.reference_step / (r.mesh_nodes[a][-1] - r.mesh_nodes[a][-2]))
                  for a in range(3) if r.shape[a] > 1 and faces[a][1] in ('pec', 'antisymmetric')}
     segments = cpml_segments(r, courant)
+    metrics = mesh_metrics(r)
     if material:
         eps, counts = voxelize(project, dtype)
+        from .injection import validate_oneway_materials
+        validate_oneway_materials(project, eps)
         inv_eps = (1 / eps).astype(dtype)
         warnings = [f'{obj.name}: no cells intersect this object. Refine mesh or reposition it.'
                     for obj in project.structures if obj.enabled and counts.get(obj.id) == 0]
@@ -412,6 +459,11 @@ def plan_grid(project, polarization=None, material=True):
     for raw in project.sources:
         s = project.resolved_source(raw)
         if not s.enabled:
+            continue
+        if s.injection == 'oneway':
+            # A one-way plane: E and H sheets fed by the incident line (injection.oneway_terms).
+            from .injection import oneway_terms
+            sources.extend(SourceTerm(c, lo, hi, v) for c, lo, hi, v in oneway_terms(s, r))
             continue
         waveform = source_time_signal(s, times + s.time_offset_steps * r.time_step)
         for component, weight in s.polarization_components:
@@ -434,4 +486,4 @@ def plan_grid(project, polarization=None, material=True):
         polarization = 'both' if tm and te else ('TE' if te else 'TM')
     return GridPlan(project, tuple(r.shape), r.dimension, dtype, courant, r.time_step, r.steps, faces, pec_upper,
                     segments, eps, inv_eps, counts, sources, traces, planes,
-                    polarization if r.dimension == '2d' else None, warnings)
+                    polarization if r.dimension == '2d' else None, warnings, metrics)

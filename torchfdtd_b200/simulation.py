@@ -421,6 +421,8 @@ class Simulation:
                 raise ValueError(f'epsilon must have shape {tuple(plan.shape)} or {(*plan.shape, 3)}, not {eps.shape}.')
             if not np.all(np.isfinite(eps)) or np.any(eps < 1):
                 raise ValueError('epsilon must be finite and at least 1.')
+            from .injection import validate_oneway_materials
+            validate_oneway_materials(self.project, eps)
             plan.epsilon = eps
             plan.inv_eps = (1 / eps).astype(plan.dtype)
         return plan
