@@ -91,6 +91,30 @@ typedef struct tfd_plane {
     const double *window_h;        /* steps, H samples (half a step later) */
 } tfd_plane;
 
+/* A total-field / scattered-field box: a live scalar incident line stepped with the grid and the sparse
+ * corrections on the box faces. Per step, after the grid's E update and soft sources: the line's E half-step
+ *   diff[i] = h[i] - h[i-1] (0 at i = 0); pe[i] = b_e[i] pe[i] + c_e[i] diff[i]; e[i] -= courant_e (diff[i] + pe[i]);
+ *   e[drive_at] += drive[n]
+ * then E[target] += weight * h[sample] for every E correction; after the H update and H sources the line's H
+ * half-step (forward differences of e, 0 at the last cell, b_h / c_h, courant_h) and H[target] += weight *
+ * e[sample]. Line arithmetic runs in the field precision. Targets are flat reference-layout elements
+ * ((x*ny + y)*nz + z)*3 + component, one correction per target and family.
+ * Reference: torchfdtd/tfsf.py:19-176 (tfsf_plan, surface_maps, IncidentLine, TfsfState.inject),
+ * torchfdtd/cuda_tfsf.py:19-49 (the fused line + correction kernel). */
+typedef struct tfd_tfsf {
+    int32_t count;                 /* incident-line cells */
+    int32_t drive_at;              /* line cell of the soft drive */
+    double courant_e, courant_h;   /* line update factors: courant / index^2 (E), courant (H) */
+    double index;                  /* background index (the diagnostics weigh line E by it) */
+    double norm_weight;            /* diagnostics weight of every line cell */
+    const double *b[2], *c[2];     /* line CPML decay / coupling per family (0 E, 1 H), count values each */
+    const double *drive;           /* steps waveform samples */
+    int32_t n_targets[2];          /* corrections per family */
+    const int64_t *target[2];
+    const int64_t *sample[2];      /* line cell each correction reads */
+    const double *weight[2];
+} tfd_tfsf;
+
 typedef struct tfd_desc {
     int32_t abi_version;           /* TFD_ABI_VERSION */
     int32_t nx, ny, nz;            /* Yee cells; nz = 1 for 2D */
@@ -120,6 +144,12 @@ typedef struct tfd_desc {
      * not scaled. Reference: the metric of YeeGrid._prepare_boundaries / curl, torchfdtd/boundaries.py:276-284,
      * 376-393, and its fused kernel, torchfdtd/cuda_kernels.py:203-236. */
     const double *metric[2][3];
+    /* Diagnostics cell volumes: per axis the cell widths over the reference step (n values), or NULL for 1. The
+     * state norm weighs E^2 / inv_eps and H^2 by (w_x * w_y) * w_z rounded to the field precision (reference
+     * StateDiagnostics, torchfdtd/run_control.py:88-146). */
+    const double *volume[3];
+    int32_t n_tfsf;                /* TFSF boxes, in source order (at most 4) */
+    const tfd_tfsf *tfsf;
 } tfd_desc;
 
 typedef struct tfd_plan tfd_plan;

@@ -119,6 +119,16 @@ class YeeOracle:
         for term in plan.sources:
             loc = tuple(slice(lo, hi) for lo, hi in zip(term.lo, term.hi))
             self.sources[term.family].append((term.values.astype(dtype), loc, term.comp))
+        # TFSF boxes: the live incident line in the field precision and the two correction maps
+        # (reference torchfdtd/tfsf.py:125-176).
+        self.lines = []
+        for box in plan.tfsf:
+            line = dict(box=box, e=np.zeros(box.count, dtype), h=np.zeros(box.count, dtype), pe=np.zeros(box.count, dtype),
+                        ph=np.zeros(box.count, dtype), diff=np.zeros(box.count, dtype),
+                        coef=[tuple(v.astype(dtype) for v in pair) for pair in box.coefficients],
+                        drive=box.drive.astype(dtype),
+                        maps={f: (t, smp, w.astype(dtype)) for f, (t, smp, w) in box.maps.items()})
+            self.lines.append(line)
         self.counter = 0
         self.traces = np.zeros((plan.steps, len(plan.traces)), dtype=dtype)
         self.planes = plane_entries(plan, dft_float64)
@@ -164,6 +174,30 @@ class YeeOracle:
         field = self.E if family == 0 else self.H
         for values, loc, component in self.sources[family]:
             field[loc + (component,)] += values[self.counter]
+        for line in self.lines:
+            self._tfsf(line, family)
+
+    def _tfsf(self, line, family):
+        """Advance the incident line by one half step of `family`, then add the corrections of that family."""
+        box, forward = line['box'], family == 1
+        e, h, diff = line['e'], line['h'], line['diff']
+        if forward:
+            diff[:-1] = e[1:] - e[:-1]
+            diff[-1] = 0
+        else:
+            diff[1:] = h[1:] - h[:-1]
+            diff[0] = 0
+        b, c = line['coef'][int(forward)]
+        psi = line['ph'] if forward else line['pe']
+        psi *= b
+        psi += c * diff
+        field_line = h if forward else e
+        field_line -= (box.courant if forward else box.courant_e) * (diff + psi)
+        if not forward:
+            e[box.drive_at] += line['drive'][self.counter]
+        target, sample, weight = line['maps']['H' if forward else 'E']
+        flat = (self.H if forward else self.E).reshape(-1)
+        flat[target] += weight * (e if forward else h)[sample]
 
     def _planes(self):
         accumulate_planes(self.planes, self.E, self.H, self.counter)

@@ -386,8 +386,36 @@ def source_scenes(ref):
     return out
 
 
+def tfsf_scenes(ref):
+    """TFSF boxes: 3D (Ey, travelling +x, a sphere inside the box) and 2D TMz (Ez, travelling -y, a circle
+    inside); traces inside (total field) and outside (scattered field), a DFT plane in the scattered region."""
+    P, R, S, M, F, St, Sp = (ref.Project, ref.Region, ref.Source, ref.Monitor, ref.FieldMonitor, ref.Structure,
+                             ref.SpectrumSettings)
+    out = {}
+    out['tfsf3d'] = P(name='tfsf3d', region=R(dimension='3d', size=(2.4, 2.2, 2.0), mesh=.05, pml_cells=6, steps=150,
+                                              backend='cpu'),
+                      structures=[St(id='ball', name='ball', kind='sphere', radius=.25, material='Si (constant n)')],
+                      sources=[S(id='box', kind='tfsf', normal='x', direction='+', center=(0, 0, 0), size=(1.0, 1.1, .9),
+                                 component='Ey', wavelength=1.3, pulse_cycles=2)],
+                      monitors=[M(id='inside', center=(-.3, .1, 0), component='Ey'),
+                                M(id='outside', center=(-.8, .1, 0), component='Ey'),
+                                M(id='hz', center=(.7, 0, .1), component='Hz'),
+                                F(id='plane', normal='x', center=(.75, 0, 0), size=(0, 1.2, 1.0),
+                                  spectrum=Sp(sampling='frequency', frequency_points=2, apodization='none'))])
+    out['tfsf2d'] = P(name='tfsf2d', region=R(dimension='2d', size=(3.0, 3.0, 1), mesh=.04, pml_cells=10, steps=300,
+                                              backend='cpu'),
+                      structures=[St(id='c', name='c', kind='circle', radius=.3, center=(.1, 0, 0), material='Si (constant n)')],
+                      sources=[S(id='box', kind='tfsf', normal='y', direction='-', center=(0, 0, 0), size=(1.4, 1.2, 0),
+                                 component='Ez', wavelength=1.1, pulse_cycles=2, amplitude=.8)],
+                      monitors=[M(id='inside', center=(.2, .3, 0), component='Ez'), M(id='outside', center=(.9, .2, 0), component='Ez'),
+                                F(id='plane', normal='x', center=(-1.0, 0, 0), size=(0, 1.6, 1),
+                                  spectrum=Sp(sampling='frequency', frequency_points=2, apodization='none'))])
+    return out
+
+
 def write_sources(ref):
     write_scenes(ref, source_scenes(ref))
+    write_scenes(ref, tfsf_scenes(ref))
 
 
 def write_results(ref):

@@ -95,7 +95,7 @@ def test_selector_refuses_other_paths_before_any_gpu_work(change, match):
     (lambda p: p.materials.append(Material(name='metal', model='drude')) or
      p.structures.append(Structure(material='metal', size=(.2, .2, 1))), 'drude'),
     (lambda p: p.sources.append(Source(kind='plane', injection='oneway', normal='x', size=(0, 2, 0), center=(-.5, 0, 0))),
-     'one-way'),
+     'periodic transverse'),
     (lambda p: setattr(p.region, 'interface_method', 'subpixel'), 'Subpixel'),
 ])
 def test_unsupported_features_are_refused_by_name(build, match):

@@ -263,6 +263,8 @@ class DifferentiableSimulation(_Differentiable):
     @cached_property
     def plan(self):
         plan = plan_grid(self.project)
+        if plan.tfsf:
+            raise ValueError('TFSF boxes are not differentiated by the B200 engine; use soft or one-way sources.')
         observers = [(t.component, t.index) for t in plan.traces]
         unique, self._columns = _unique_observers(observers)
         return _observer_plan(plan, unique)
@@ -310,6 +312,8 @@ class DifferentiablePlaneSimulation(_Differentiable):
     @cached_property
     def plan(self):
         plan = plan_grid(self.project)
+        if plan.tfsf:
+            raise ValueError('TFSF boxes are not differentiated by the B200 engine; use soft or one-way sources.')
         nx, ny, nz = plan.shape
         observers, self._maps = [], []
         for pp in plan.planes:

@@ -14,6 +14,7 @@
 #include "step_march.cuh"
 #include "step2d.cuh"
 #include "adjoint.cuh"
+#include "tfsf.cuh"
 #include <cudaTypedefs.h>
 
 using namespace tfd;
@@ -75,6 +76,13 @@ struct PlaneLayout {
     size_t cell, weight, omega, half, window, acc;
 };
 
+struct TfsfLayout {
+    size_t line;                   // e, h, pe, ph: 4 x count elements
+    size_t coef;                   // b_e, c_e, b_h, c_h: 4 x count elements
+    size_t drive;                  // steps elements
+    size_t tgt[2], w[2];           // corrections per family
+};
+
 struct Layout {
     int elem = 4;
     int pitch = 0;
@@ -88,6 +96,8 @@ struct Layout {
     size_t psiE[3][2], psiH[3][2];
     size_t src_values = 0, trace_tab = 0, trace_out = 0, plane_tab = 0;
     std::vector<PlaneLayout> planes;
+    std::vector<TfsfLayout> tfsf;
+    size_t volume[3];              // diagnostics cell volumes per axis (double), 0: unit
     size_t counter = 0, done = 0, status = 0, diag = 0, stage = 0;
     size_t grid_bar = 0;           // persistent 2D stepping: arrival count and generation
     size_t check = 0;              // tfd_set_permittivity / tfd_field_check results
@@ -154,6 +164,24 @@ int validate(const tfd_desc *d) {
             if (t.index[a] < 0 || t.index[a] >= n[a]) return fail(TFD_ERR_INVALID, "trace index outside the grid");
     }
     if (d->n_planes < 0 || d->n_planes > 65535 || (d->n_planes && !d->planes)) return fail(TFD_ERR_INVALID, "bad plane list");
+    if (d->n_tfsf < 0 || d->n_tfsf > kMaxTfsf || (d->n_tfsf && !d->tfsf)) return fail(TFD_ERR_INVALID, "at most 4 TFSF boxes are supported per plan");
+    for (int k = 0; k < d->n_tfsf; ++k) {
+        const tfd_tfsf &t = d->tfsf[k];
+        if (t.count < 2 || t.drive_at < 0 || t.drive_at >= t.count || !t.drive || !t.b[0] || !t.b[1] || !t.c[0] || !t.c[1])
+            return fail(TFD_ERR_INVALID, "bad TFSF incident line");
+        for (int f = 0; f < 2; ++f) {
+            if (t.n_targets[f] < 0 || (t.n_targets[f] && (!t.target[f] || !t.sample[f] || !t.weight[f])))
+                return fail(TFD_ERR_INVALID, "bad TFSF correction list");
+            const long long cells = (long long)d->nx * d->ny * d->nz;
+            for (int j = 0; j < t.n_targets[f]; ++j) {
+                const int64_t q = t.target[f][j];
+                if (q < 0 || q >= 3 * cells || t.sample[f][j] < 0 || t.sample[f][j] >= t.count)
+                    return fail(TFD_ERR_INVALID, "a TFSF correction lies outside the grid or its incident line");
+                if (!active(d->components, 3 * f + (int)(q % 3)))
+                    return fail(TFD_ERR_INVALID, "a TFSF correction drives a component this plan does not advance");
+            }
+        }
+    }
     const long long cells = (long long)n[0] * n[1] * n[2];
     for (int k = 0; k < d->n_planes; ++k) {
         const tfd_plane &p = d->planes[k];
@@ -365,6 +393,19 @@ void compute_layout(const tfd_desc *d, Layout &L) {
         q.acc = b.take(std::max<size_t>(1, acc));
         largest_plane = std::max(largest_plane, acc);
     }
+    L.tfsf.resize(d->n_tfsf);
+    for (int k = 0; k < d->n_tfsf; ++k) {
+        const tfd_tfsf &t = d->tfsf[k];
+        TfsfLayout &q = L.tfsf[k];
+        q.line = b.take((size_t)4 * t.count * L.elem);
+        q.coef = b.take((size_t)4 * t.count * L.elem);
+        q.drive = b.take((size_t)std::max(1, d->steps) * L.elem);
+        for (int f = 0; f < 2; ++f) {
+            q.tgt[f] = b.take(std::max<size_t>(1, t.n_targets[f]) * sizeof(TfsfTarget));
+            q.w[f] = b.take(std::max<size_t>(1, t.n_targets[f]) * L.elem);
+        }
+    }
+    for (int a = 0; a < 3; ++a) L.volume[a] = d->volume[a] ? b.take((size_t)n[a] * sizeof(double)) : 0;
     if (tile2d_capable(d)) {
         L.strip_rows = persist2d_eligible((long long)d->nx * d->ny) ? persist2d_strip_rows() : strip_rows((long long)d->nx * d->ny);
         L.tiles2d = (int)strips_of(strip_geom(d), 0, L.strip_rows).size();
@@ -409,6 +450,10 @@ struct tfd_plan {
     MarchMix march_mix{};
     std::vector<MarchLaunch> march_launches;
     bool march_metric = false;     // nonuniform mesh: the general body with metric factors
+    TfsfArgs<float> tf{};          // TFSF boxes (the step runs the split gather kernels when there are any)
+    TfsfArgs<double> td{};
+    double tfsf_index[kMaxTfsf] = {}, tfsf_norm[kMaxTfsf] = {};   // diagnostics: background index, norm weight
+    template <typename T> TfsfArgs<T> &tfsf();
     // Boundary strips run on auxiliary streams, forked from and joined back to the caller's stream
     // (a CUDA graph capture records them as parallel branches).
     std::vector<cudaStream_t> aux;
@@ -435,6 +480,8 @@ template <> Grid<float> &tfd_plan::grid<float>() { return gf; }
 template <> Grid<double> &tfd_plan::grid<double>() { return gd; }
 template <> MarchArgs<float> &tfd_plan::march<float>() { return mf; }
 template <> MarchArgs<double> &tfd_plan::march<double>() { return md; }
+template <> TfsfArgs<float> &tfd_plan::tfsf<float>() { return tf; }
+template <> TfsfArgs<double> &tfd_plan::tfsf<double>() { return td; }
 
 namespace {
 
@@ -506,6 +553,67 @@ int create_typed(tfd_plan *p, const tfd_desc *d, cudaStream_t s) {
             g.cc[f][a] = p->ptr<T>(L.cc[f][a]);
             g.ck[f][a] = p->ptr<T>(L.ck[f][a]);
             g.row[f][a] = p->ptr<int>(L.row[f][a]);
+        }
+    // TFSF boxes: line coefficients and drive rounded to T, corrections with internal element indices
+    {
+        TfsfArgs<T> &ta = p->tfsf<T>();
+        std::memset(&ta, 0, sizeof(ta));
+        ta.boxes = d->n_tfsf;
+        ta.steps = d->steps;
+        for (int k = 0; k < d->n_tfsf; ++k) {
+            const tfd_tfsf &t = d->tfsf[k];
+            p->tfsf_index[k] = t.index;
+            p->tfsf_norm[k] = t.norm_weight;
+            const TfsfLayout &q = L.tfsf[k];
+            TfsfBoxDev<T> &bx = ta.box[k];
+            bx.count = t.count;
+            bx.drive_at = t.drive_at;
+            bx.fac[0] = (T)t.courant_e;
+            bx.fac[1] = (T)t.courant_h;
+            T *line = p->ptr<T>(q.line);
+            bx.e = line;
+            bx.h = line + t.count;
+            bx.pe = line + 2 * t.count;
+            bx.ph = line + 3 * t.count;
+            std::vector<T> coef((size_t)4 * t.count);
+            for (int f = 0; f < 2; ++f)
+                for (int i = 0; i < t.count; ++i) {
+                    coef[(size_t)(2 * f) * t.count + i] = (T)t.b[f][i];
+                    coef[(size_t)(2 * f + 1) * t.count + i] = (T)t.c[f][i];
+                }
+            if (int rc = upload(s, p, q.coef, coef)) return rc;
+            const T *cp = p->ptr<T>(q.coef);
+            for (int f = 0; f < 2; ++f) {
+                bx.b[f] = cp + (size_t)(2 * f) * t.count;
+                bx.c[f] = cp + (size_t)(2 * f + 1) * t.count;
+            }
+            std::vector<T> drive((size_t)std::max(1, d->steps), T(0));
+            for (int i = 0; i < d->steps; ++i) drive[i] = (T)t.drive[i];
+            if (int rc = upload(s, p, q.drive, drive)) return rc;
+            bx.drive = p->ptr<T>(q.drive);
+            for (int f = 0; f < 2; ++f) {
+                std::vector<TfsfTarget> tg(t.n_targets[f]);
+                std::vector<T> w(t.n_targets[f]);
+                for (int j = 0; j < t.n_targets[f]; ++j) {
+                    const long long cell = t.target[f][j] / 3;
+                    const int x = (int)(cell / ((long long)n[1] * n[2])), y = (int)((cell / n[2]) % n[1]), z = (int)(cell % n[2]);
+                    tg[j].idx = (long long)z * g.plane + (long long)y * L.pitch + x;
+                    tg[j].comp = (int)(t.target[f][j] % 3);
+                    tg[j].sample = (int)t.sample[f][j];
+                    w[j] = (T)t.weight[f][j];
+                }
+                if (int rc = upload(s, p, q.tgt[f], tg)) return rc;
+                if (int rc = upload(s, p, q.w[f], w)) return rc;
+                bx.n[f] = t.n_targets[f];
+                bx.tgt[f] = p->ptr<TfsfTarget>(q.tgt[f]);
+                bx.w[f] = p->ptr<T>(q.w[f]);
+            }
+        }
+    }
+    for (int a = 0; a < 3; ++a)
+        if (L.volume[a]) {
+            std::vector<double> v(d->volume[a], d->volume[a] + n[a]);
+            if (int rc = upload(s, p, L.volume[a], v)) return rc;
         }
     // nonuniform-mesh factors
     for (int f = 0; f < 2; ++f)
@@ -620,6 +728,8 @@ int zero_state(tfd_plan *p, cudaStream_t s) {
         const size_t acc = (size_t)p->planes_f[k] * p->planes_p[k] * p->planes_c[k] * 2 * sizeof(double);
         if (acc) TFD_CUDA(cudaMemsetAsync(p->arena + L.planes[k].acc, 0, acc, s));
     }
+    for (size_t k = 0; k < L.tfsf.size(); ++k)
+        TFD_CUDA(cudaMemsetAsync(p->arena + L.tfsf[k].line, 0, (size_t)4 * p->tfsf<T>().box[k].count * L.elem, s));
     TFD_CUDA(cudaMemsetAsync(p->arena + L.counter, 0, sizeof(long long), s));
     TFD_CUDA(cudaMemsetAsync(p->arena + L.done, 0, sizeof(unsigned), s));
     TFD_CUDA(cudaMemsetAsync(p->arena + L.grid_bar, 0, 2 * sizeof(unsigned), s));
@@ -1303,6 +1413,37 @@ int launch_persist2d(tfd_plan *p, int nsteps, cudaStream_t s) {
     return TFD_OK;
 }
 
+// One step of a plan with TFSF boxes: the split gather E kernel, the boxes' E half step and E corrections, the
+// split gather H kernel, the H half step and H corrections (the observation launch follows in step_t).
+template <typename T>
+int launch_tfsf_step(tfd_plan *p, cudaStream_t s) {
+    const Grid<T> &g = p->grid<T>();
+    TfsfArgs<T> a = p->tfsf<T>();
+    for (int par = 0; par < 2; ++par)
+        for (int c = 0; c < 3; ++c) {
+            a.E[par][c] = g.E[par][c];
+            a.H[par][c] = g.H[par][c];
+        }
+    a.counter = g.counter;
+    int longest = 1;
+    for (int k = 0; k < a.boxes; ++k) longest = std::max(longest, a.box[k].count + std::max(a.box[k].n[0], a.box[k].n[1]));
+    const dim3 tgrid((unsigned)((longest + kTfsfThreads - 1) / kTfsfThreads), (unsigned)a.boxes);
+    dim3 block(128), grid((unsigned)((long long)g.n[1] * g.n[2]), (unsigned)((g.n[0] + 127) / 128));
+    switch (g.active) {
+        case kMaskTM: k_step_gather_e<T, kMaskTM><<<grid, block, 0, s>>>(g); break;
+        case kMaskTE: k_step_gather_e<T, kMaskTE><<<grid, block, 0, s>>>(g); break;
+        default: k_step_gather_e<T, kMaskAll><<<grid, block, 0, s>>>(g); break;
+    }
+    k_tfsf<T><<<tgrid, kTfsfThreads, 0, s>>>(a, 0);
+    switch (g.active) {
+        case kMaskTM: k_step_gather_h<T, kMaskTM><<<grid, block, 0, s>>>(g); break;
+        case kMaskTE: k_step_gather_h<T, kMaskTE><<<grid, block, 0, s>>>(g); break;
+        default: k_step_gather_h<T, kMaskAll><<<grid, block, 0, s>>>(g); break;
+    }
+    k_tfsf<T><<<tgrid, kTfsfThreads, 0, s>>>(a, 1);
+    return TFD_OK;
+}
+
 template <typename T>
 int step_t(tfd_plan *p, int nsteps, cudaStream_t s) {
     if (p->kernel == TFD_KERNEL_TILE2D && p->persist_ctas > 0 && !p->in_batch) {
@@ -1312,7 +1453,9 @@ int step_t(tfd_plan *p, int nsteps, cudaStream_t s) {
     const MonitorArgs<T> m = monitor_args<T>(p);
     dim3 mgrid((unsigned)std::max(1, (p->max_samples + kMonitorThreads - 1) / kMonitorThreads), (unsigned)std::max(1, p->desc.n_planes));
     for (int k = 0; k < nsteps; ++k) {
-        if (p->kernel == TFD_KERNEL_MARCH) {
+        if (p->tfsf<T>().boxes > 0) {
+            TFD_CHECK(launch_tfsf_step<T>(p, s));
+        } else if (p->kernel == TFD_KERNEL_MARCH) {
             launch_march_any<T>(p, s);
         } else if (p->kernel == TFD_KERNEL_TILE2D) {
             launch_tile2d<T>(p, s);
@@ -1348,6 +1491,24 @@ int diagnose_t(tfd_plan *p, double out[3], cudaStream_t s) {
             if (g.psiE[par][a][j]) { d.psi[d.n_psi] = g.psiE[par][a][j]; d.psi_len[d.n_psi++] = L.psi_len[0][a]; }
             if (g.psiH[a][j]) { d.psi[d.n_psi] = g.psiH[a][j]; d.psi_len[d.n_psi++] = L.psi_len[1][a]; }
         }
+    for (int a = 0; a < 3; ++a) d.volume[a] = L.volume[a] ? p->ptr<double>(L.volume[a]) : nullptr;
+    const TfsfArgs<T> &ta = p->tfsf<T>();
+    for (int k = 0; k < ta.boxes; ++k) {
+        const TfsfBoxDev<T> &bx = ta.box[k];
+        // Line E weighed like E times the background index, line H like H; both CPML memories checked finite.
+        d.line[d.n_lines] = bx.e;
+        d.line_len[d.n_lines] = bx.count;
+        d.line_factor[d.n_lines] = p->tfsf_index[k];
+        d.line_weight[d.n_lines++] = (double)(T)p->tfsf_norm[k];
+        d.line[d.n_lines] = bx.h;
+        d.line_len[d.n_lines] = bx.count;
+        d.line_factor[d.n_lines] = 1.0;
+        d.line_weight[d.n_lines++] = (double)(T)p->tfsf_norm[k];
+        d.psi[d.n_psi] = bx.pe;
+        d.psi_len[d.n_psi++] = bx.count;
+        d.psi[d.n_psi] = bx.ph;
+        d.psi_len[d.n_psi++] = bx.count;
+    }
     d.partial = p->ptr<double>(L.diag);
     k_diag<T><<<kDiagBlocks, kDiagThreads, 0, s>>>(d);
     TFD_CUDA(cudaGetLastError());
@@ -1457,12 +1618,14 @@ int tfd_plan_create(const tfd_desc *desc, void *arena, size_t arena_bytes, void 
             rc = fail(TFD_ERR_UNSUPPORTED, "the marching kernel needs a 3D grid");
         else if (desc->kernel == TFD_KERNEL_TILE2D && !tile_ok)
             rc = fail(TFD_ERR_UNSUPPORTED, "the 2D tile kernel needs a 2D TMz grid without periodic x/y faces");
-        if (desc->kernel == TFD_KERNEL_GATHER) p->kernel = TFD_KERNEL_GATHER;
+        if (desc->n_tfsf > 0 && (desc->kernel == TFD_KERNEL_MARCH || desc->kernel == TFD_KERNEL_TILE2D))
+            rc = fail(TFD_ERR_UNSUPPORTED, "plans with TFSF boxes run the split gather kernels");
+        if (desc->kernel == TFD_KERNEL_GATHER || desc->n_tfsf > 0) p->kernel = TFD_KERNEL_GATHER;
         else if (march_ok) p->kernel = TFD_KERNEL_MARCH;
         else if (tile_ok) p->kernel = TFD_KERNEL_TILE2D;
         else p->kernel = TFD_KERNEL_GATHER;
         if (!rc && p->kernel == TFD_KERNEL_MARCH) rc = TFD_DISPATCH(p, setup_march, p);
-        if (!rc && tile_ok) rc = TFD_DISPATCH(p, setup_tile2d, p, s);
+        if (!rc && tile_ok && desc->n_tfsf == 0) rc = TFD_DISPATCH(p, setup_tile2d, p, s);
     }
     if (!rc) rc = TFD_DISPATCH(p, zero_state, p, s);
     if (!rc) {
@@ -1599,7 +1762,9 @@ int tfd_step_launches(const tfd_plan *p, int32_t nsteps, int64_t *launches) {
     if (!p || !launches) return fail(TFD_ERR_INVALID, "null argument");
     if (nsteps < 0) return fail(TFD_ERR_INVALID, "nsteps must be non-negative");
     long long per_step = 2;                                   // gather: step + observation
-    if (p->kernel == TFD_KERNEL_TILE2D) {
+    if (p->desc.n_tfsf > 0) {
+        per_step = 5;                                         // split E, TFSF E, split H, TFSF H, observation
+    } else if (p->kernel == TFD_KERNEL_TILE2D) {
         if (p->persist_ctas > 0 && !p->in_batch) {
             *launches = nsteps > 0 ? 1 : 0;
             return TFD_OK;

@@ -419,6 +419,12 @@ struct DiagArgs {
     int n_psi;
     const T *psi[40];
     long long psi_len[40];
+    const double *volume[3];     // per-axis cell widths over the reference step (nullptr: 1)
+    // Incident lines of TFSF boxes: their E (times the background index) and H enter the norm with a weight.
+    int n_lines;
+    const T *line[8];
+    int line_len[8];
+    double line_factor[8], line_weight[8];
     double *partial;             // [gridDim.x][4]
 };
 
@@ -439,23 +445,37 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag(const __grid_constant__ D
     const int par = (int)(*d.counter & 1);
     const long long cells = (long long)d.nx * d.ny * d.nz;
     double energy = 0.0, peak = 0.0, finite = 1.0, nan_seen = 0.0;
+    const bool weighted = d.volume[0] || d.volume[1] || d.volume[2];
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < cells; e += (long long)gridDim.x * blockDim.x) {
         const int x = (int)(e % d.nx);
         const long long i = (e / d.nx) * d.pitch + x;   // e / nx = z*ny + y
+        // Cell volume in reference-step units, rounded to the field precision as the reference stores it.
+        double vol = 1.0;
+        if (weighted) {
+            const int y = (int)((e / d.nx) % d.ny), z = (int)(e / ((long long)d.nx * d.ny));
+            const double wx = d.volume[0] ? d.volume[0][x] : 1.0, wy = d.volume[1] ? d.volume[1][y] : 1.0,
+                         wz = d.volume[2] ? d.volume[2][z] : 1.0;
+            vol = (double)(T)((wx * wy) * wz);
+        }
         for (int c = 0; c < 3; ++c) {
             const T *a = d.fs.f[par][c], *b = d.fs.f[par][3 + c];
             if (a) {
                 const double v = (double)a[i];
-                energy += v * v * (1.0 / (double)d.inv_eps[c][i]);
+                energy += v * v * ((weighted ? vol : 1.0) / (double)d.inv_eps[c][i]);
                 if (isnan(v)) nan_seen = 1.0; else peak = fmax(peak, fabs(v));
             }
             if (b) {
                 const double v = (double)b[i];
-                energy += v * v;
+                energy += weighted ? v * v * vol : v * v;
                 if (isnan(v)) nan_seen = 1.0; else peak = fmax(peak, fabs(v));
             }
         }
     }
+    for (int k = 0; k < d.n_lines; ++k)
+        for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < d.line_len[k]; e += (long long)gridDim.x * blockDim.x) {
+            const double v = (double)d.line[k][e] * d.line_factor[k];
+            energy += v * v * d.line_weight[k];
+        }
     for (int k = 0; k < d.n_psi; ++k)
         for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < d.psi_len[k]; e += (long long)gridDim.x * blockDim.x)
             if (!isfinite((double)d.psi[k][e])) finite = 0.0;

@@ -81,7 +81,9 @@ __device__ __forceinline__ T e_neighbour(const Grid<T> &g, int par, long long n,
     return e_value<T, IN>(g, par, n, xx, yy, zz, j, false);
 }
 
-template <typename T, int C, int K>
+// STORED: the neighbour's E_new is read from the new buffer (written by the split E kernel, with the TFSF E
+// corrections) instead of recomputed.
+template <typename T, int C, int K, bool STORED = false>
 __device__ __forceinline__ void h_term(const Grid<T> &g, int par, long long n, int x, int y, int z, long long i, const T *e_own,
                                        T &acc) {
     constexpr Term t = term_of(C, K);
@@ -89,9 +91,13 @@ __device__ __forceinline__ void h_term(const Grid<T> &g, int par, long long n, i
     if (g.n[a] == 1) return;
     const int coord = a == 0 ? x : (a == 1 ? y : z);
     const T *mt = g.metric[1][a];
+    auto e_at = [&](int to) -> T {
+        if constexpr (STORED) return g.E[par ^ 1][t.in][i + (long long)(to - coord) * g.stride(a)];
+        return e_neighbour<T, t.in>(g, par, n, a, x, y, z, i, to);
+    };
     T d = T(0);
     if (coord < g.n[a] - 1) {
-        d = e_neighbour<T, t.in>(g, par, n, a, x, y, z, i, coord + 1) - e_own[t.in];
+        d = e_at(coord + 1) - e_own[t.in];
         if (mt != nullptr) d = d * mt[coord];
         const int *rm = g.row[1][a];
         if (rm != nullptr) {
@@ -105,7 +111,7 @@ __device__ __forceinline__ void h_term(const Grid<T> &g, int par, long long n, i
             }
         }
     } else if (g.periodic[a]) {
-        d = e_neighbour<T, t.in>(g, par, n, a, x, y, z, i, 0) - e_own[t.in];
+        d = e_at(0) - e_own[t.in];
         if (mt != nullptr) d = d * mt[coord];
     } else if (g.pec_on[a]) {
         d = g.pec_neg[a] * e_own[t.in];
@@ -113,11 +119,11 @@ __device__ __forceinline__ void h_term(const Grid<T> &g, int par, long long n, i
     acc = acc + (t.sign > 0 ? d : -d);
 }
 
-template <typename T, int C>
+template <typename T, int C, bool STORED = false>
 __device__ __forceinline__ T h_value(const Grid<T> &g, int par, long long n, int x, int y, int z, long long i, const T *e_own) {
     T acc = T(0);
-    h_term<T, C, 0>(g, par, n, x, y, z, i, e_own, acc);
-    h_term<T, C, 1>(g, par, n, x, y, z, i, e_own, acc);
+    h_term<T, C, 0, STORED>(g, par, n, x, y, z, i, e_own, acc);
+    h_term<T, C, 1, STORED>(g, par, n, x, y, z, i, e_own, acc);
     const T h = g.H[par][C][i] - g.cn * acc;
     return inject(g, 1, C, n, x, y, z, h);
 }
@@ -141,6 +147,42 @@ __global__ void __launch_bounds__(128) k_step_gather_rows(const __grid_constant_
     if (ACTIVE & 8) g.H[par ^ 1][0][i] = h_value<T, 0>(g, par, n, x, y, z, i, e);
     if (ACTIVE & 16) g.H[par ^ 1][1][i] = h_value<T, 1>(g, par, n, x, y, z, i, e);
     if (ACTIVE & 32) g.H[par ^ 1][2][i] = h_value<T, 2>(g, par, n, x, y, z, i, e);
+}
+
+// The step split in two launches (plans with TFSF boxes, whose E corrections must land between the E and the
+// H update): the E kernel writes E_new and the E-family CPML memories, the H kernel reads E_new back.
+template <typename T, int ACTIVE>
+__global__ void __launch_bounds__(128) k_step_gather_e(const __grid_constant__ Grid<T> g) {
+    const long long n = *g.counter;
+    if (n >= g.steps) return;
+    const int par = (int)(n & 1);
+    const int x = blockIdx.y * blockDim.x + threadIdx.x;
+    const int y = blockIdx.x % g.n[1];
+    const int z = blockIdx.x / g.n[1];
+    if (x >= g.n[0]) return;
+    const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
+    if (ACTIVE & 1) g.E[par ^ 1][0][i] = e_value<T, 0>(g, par, n, x, y, z, i, true);
+    if (ACTIVE & 2) g.E[par ^ 1][1][i] = e_value<T, 1>(g, par, n, x, y, z, i, true);
+    if (ACTIVE & 4) g.E[par ^ 1][2][i] = e_value<T, 2>(g, par, n, x, y, z, i, true);
+}
+
+template <typename T, int ACTIVE>
+__global__ void __launch_bounds__(128) k_step_gather_h(const __grid_constant__ Grid<T> g) {
+    const long long n = *g.counter;
+    if (n >= g.steps) return;
+    const int par = (int)(n & 1);
+    const int x = blockIdx.y * blockDim.x + threadIdx.x;
+    const int y = blockIdx.x % g.n[1];
+    const int z = blockIdx.x / g.n[1];
+    if (x >= g.n[0]) return;
+    const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
+    T e[3] = {T(0), T(0), T(0)};
+    if (ACTIVE & 1) e[0] = g.E[par ^ 1][0][i];
+    if (ACTIVE & 2) e[1] = g.E[par ^ 1][1][i];
+    if (ACTIVE & 4) e[2] = g.E[par ^ 1][2][i];
+    if (ACTIVE & 8) g.H[par ^ 1][0][i] = h_value<T, 0, true>(g, par, n, x, y, z, i, e);
+    if (ACTIVE & 16) g.H[par ^ 1][1][i] = h_value<T, 1, true>(g, par, n, x, y, z, i, e);
+    if (ACTIVE & 32) g.H[par ^ 1][2][i] = h_value<T, 2, true>(g, par, n, x, y, z, i, e);
 }
 
 }  // namespace tfd

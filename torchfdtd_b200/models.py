@@ -582,7 +582,10 @@ class Project(Model):
         r.valid_grid()
         for source in self.sources:
             resolved = self.resolved_source(source)
-            if resolved.enabled and resolved.injection == 'oneway' and resolved.kind != 'tfsf':
+            if resolved.enabled and resolved.kind == 'tfsf':
+                from .tfsf import tfsf_plan
+                tfsf_plan(resolved, r)
+            elif resolved.enabled and resolved.injection == 'oneway':
                 from .injection import oneway_plan
                 oneway_plan(resolved, r)
         dt = r.time_step

@@ -48,6 +48,12 @@ class PlaneC(ctypes.Structure):
                 ('frequency_hz', P_dbl), ('window_e', P_dbl), ('window_h', P_dbl)]
 
 
+class TfsfC(ctypes.Structure):
+    _fields_ = [('count', c_i32), ('drive_at', c_i32), ('courant_e', c_dbl), ('courant_h', c_dbl), ('index', c_dbl),
+                ('norm_weight', c_dbl), ('b', P_dbl * 2), ('c', P_dbl * 2), ('drive', P_dbl), ('n_targets', c_i32 * 2),
+                ('target', P_i64 * 2), ('sample', P_i64 * 2), ('weight', P_dbl * 2)]
+
+
 class Desc(ctypes.Structure):
     _fields_ = [('abi_version', c_i32), ('nx', c_i32), ('ny', c_i32), ('nz', c_i32), ('precision', c_i32),
                 ('material_samples', c_i32), ('components', c_i32), ('steps', c_i32), ('kernel', c_i32),
@@ -56,7 +62,8 @@ class Desc(ctypes.Structure):
                 ('n_segments', c_i32), ('segments', ctypes.POINTER(CpmlSegment)),
                 ('n_sources', c_i32), ('sources', ctypes.POINTER(SourceTermC)),
                 ('n_traces', c_i32), ('traces', ctypes.POINTER(TraceC)),
-                ('n_planes', c_i32), ('planes', ctypes.POINTER(PlaneC)), ('metric', (P_dbl * 3) * 2)]
+                ('n_planes', c_i32), ('planes', ctypes.POINTER(PlaneC)), ('metric', (P_dbl * 3) * 2),
+                ('volume', P_dbl * 3), ('n_tfsf', c_i32), ('tfsf', ctypes.POINTER(TfsfC))]
 
 
 # Every entry point of include/tfdtd.h with its ctypes signature.
@@ -274,7 +281,34 @@ def describe(plan, kernel='auto', variant=0):
                 table = np.ascontiguousarray(table, dtype=np.float64)
                 keep.append(table)
                 desc.metric[f][a] = _ptr(table, ctypes.c_double)
-    keep.extend([segs, srcs, traces, planes])
+    region = plan.project.region if plan.project is not None else None
+    if region is not None and (region.mesh_type != 'uniform' or region.mesh_steps is not None):
+        # Diagnostics cell volumes of a nonuniform mesh: widths over the reference step, every axis.
+        for a, nodes in enumerate(region.mesh_nodes):
+            if plan.shape[a] > 1:
+                w = np.ascontiguousarray(np.diff(nodes) / region.reference_step, dtype=np.float64)
+                keep.append(w)
+                desc.volume[a] = _ptr(w, ctypes.c_double)
+    boxes = getattr(plan, 'tfsf', [])
+    tf = (TfsfC * max(1, len(boxes)))()
+    for k, box in enumerate(boxes):
+        t = tf[k]
+        t.count, t.drive_at = box.count, box.drive_at
+        t.courant_e, t.courant_h, t.index, t.norm_weight = box.courant_e, box.courant, box.index, box.norm_weight
+        drive = np.ascontiguousarray(box.drive, dtype=np.float64)
+        keep.append(drive)
+        t.drive = _ptr(drive, ctypes.c_double)
+        for f, family in enumerate(('E', 'H')):
+            b, c = (np.ascontiguousarray(v, dtype=np.float64) for v in box.coefficients[f])
+            target, sample, weight = (np.ascontiguousarray(box.maps[family][0], dtype=np.int64),
+                                      np.ascontiguousarray(box.maps[family][1], dtype=np.int64),
+                                      np.ascontiguousarray(box.maps[family][2], dtype=np.float64))
+            keep.extend([b, c, target, sample, weight])
+            t.b[f], t.c[f] = _ptr(b, ctypes.c_double), _ptr(c, ctypes.c_double)
+            t.n_targets[f] = len(target)
+            t.target[f], t.sample[f], t.weight[f] = _ptr(target, c_i64), _ptr(sample, c_i64), _ptr(weight, ctypes.c_double)
+    desc.n_tfsf, desc.tfsf = len(boxes), tf
+    keep.extend([segs, srcs, traces, planes, tf])
     return desc, keep
 
 

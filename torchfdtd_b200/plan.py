@@ -126,6 +126,7 @@ class GridPlan:
     polarization: str | None = None
     warnings: list = field(default_factory=list)
     metrics: dict = field(default_factory=dict)   # (forward, axis) -> (float64 (n-1,) interior values, wrap value)
+    tfsf: list = field(default_factory=list)      # tfsf.TfsfBox per enabled TFSF source, in source order
 
     @property
     def cells(self):
@@ -239,8 +240,6 @@ def check_supported(project):
         s = project.resolved_source(raw)
         if not s.enabled:
             continue
-        if s.kind == 'tfsf':
-            raise ValueError(f'{s.name}: TFSF injection is not implemented by the fused B200 engine; use soft or one-way sources.')
     r.require_resident()
 
 
@@ -447,18 +446,24 @@ def plan_grid(project, polarization=None, material=True):
     if material:
         eps, counts = voxelize(project, dtype)
         from .injection import validate_oneway_materials
+        from .tfsf import validate_tfsf_materials
         validate_oneway_materials(project, eps)
+        validate_tfsf_materials(project, eps)
         inv_eps = (1 / eps).astype(dtype)
         warnings = [f'{obj.name}: no cells intersect this object. Refine mesh or reposition it.'
                     for obj in project.structures if obj.enabled and counts.get(obj.id) == 0]
     else:
         eps = inv_eps = None
         counts, warnings = {}, []
-    sources = []
+    sources, boxes = [], []
     times = np.arange(1, r.steps + 1) * r.time_step
     for raw in project.sources:
         s = project.resolved_source(raw)
         if not s.enabled:
+            continue
+        if s.kind == 'tfsf':
+            from .tfsf import tfsf_box
+            boxes.append(tfsf_box(s, r))
             continue
         if s.injection == 'oneway':
             # A one-way plane: E and H sheets fed by the incident line (injection.oneway_terms).
@@ -486,4 +491,4 @@ def plan_grid(project, polarization=None, material=True):
         polarization = 'both' if tm and te else ('TE' if te else 'TM')
     return GridPlan(project, tuple(r.shape), r.dimension, dtype, courant, r.time_step, r.steps, faces, pec_upper,
                     segments, eps, inv_eps, counts, sources, traces, planes,
-                    polarization if r.dimension == '2d' else None, warnings, metrics)
+                    polarization if r.dimension == '2d' else None, warnings, metrics, boxes)

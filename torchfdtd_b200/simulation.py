@@ -422,7 +422,9 @@ class Simulation:
             if not np.all(np.isfinite(eps)) or np.any(eps < 1):
                 raise ValueError('epsilon must be finite and at least 1.')
             from .injection import validate_oneway_materials
+            from .tfsf import validate_tfsf_materials
             validate_oneway_materials(self.project, eps)
+            validate_tfsf_materials(self.project, eps)
             plan.epsilon = eps
             plan.inv_eps = (1 / eps).astype(plan.dtype)
         return plan
