@@ -115,6 +115,22 @@ typedef struct tfd_tfsf {
     const double *weight[2];
 } tfd_tfsf;
 
+/* The samples one dispersive material owns and its poles (coupled trapezoidal ADE). Per step, after the free
+ * E update of a sample (with 1 / eps_inf) and before the soft sources:
+ *   r_p = (Q_p - a_p P_p) / d_p;  E = (eps_inf E_free - k_sum E_old - sum_p r_p) / (eps_inf + k_sum);
+ *   delta_p = r_p + k_p (E + E_old);  P_p += delta_p;  Q_p = -Q_p + 2 delta_p.
+ * multiple = 0 (one pole): a, d, k rounded to the field precision at each use and eps_inf + k rounded once;
+ * multiple = 1: a, d, k rounded to the field precision, k_sum and eps_inf + k_sum summed in it (pole order).
+ * Reference: MaterialADE, torchfdtd/materials.py:29-88, configure_materials :117-193. */
+typedef struct tfd_ade {
+    int32_t samples, poles, multiple;
+    const int64_t *target;         /* samples: flat reference-layout element ((x*ny + y)*nz + z)*3 + component */
+    double eps_inf;
+    const double *a, *d, *k;       /* poles values */
+    const double *w0, *strength;   /* poles: the state norm adds (Q / (dt sqrt(strength)))^2 + (P w0 / sqrt(strength))^2 */
+    const double *weight;          /* samples: diagnostics volume weights, or NULL for 1 */
+} tfd_ade;
+
 typedef struct tfd_desc {
     int32_t abi_version;           /* TFD_ABI_VERSION */
     int32_t nx, ny, nz;            /* Yee cells; nz = 1 for 2D */
@@ -150,6 +166,8 @@ typedef struct tfd_desc {
     const double *volume[3];
     int32_t n_tfsf;                /* TFSF boxes, in source order (at most 4) */
     const tfd_tfsf *tfsf;
+    int32_t n_ade;                 /* dispersive material states (at most 8), samples disjoint */
+    const tfd_ade *ade;
 } tfd_desc;
 
 typedef struct tfd_plan tfd_plan;

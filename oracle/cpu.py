@@ -57,8 +57,8 @@ def _p(a):
 
 class CpuOracle:
     def __init__(self, plan, threads=None):
-        if getattr(plan, 'tfsf', None):
-            raise ValueError('The C oracle does not implement TFSF boxes; use oracle.yee_oracle.YeeOracle.')
+        if getattr(plan, 'tfsf', None) or getattr(plan, 'ade', None):
+            raise ValueError('The C oracle does not implement TFSF boxes or dispersive materials; use oracle.yee_oracle.YeeOracle.')
         self.plan = plan
         self.threads = threads or os.cpu_count() or 1
         dt = plan.dtype

@@ -129,6 +129,19 @@ class YeeOracle:
                         drive=box.drive.astype(dtype),
                         maps={f: (t, smp, w.astype(dtype)) for f, (t, smp, w) in box.maps.items()})
             self.lines.append(line)
+        # Dispersive materials (reference torchfdtd/materials.py:29-88): per state its samples, P and Q per pole,
+        # and the coefficients as the reference holds them (float64 scalars for one pole, the field precision for
+        # several).
+        self.ade = []
+        for st in getattr(plan, 'ade', []):
+            if st.multiple:
+                coef = {k: getattr(st, k).reshape(-1, 1).astype(dtype) for k in ('a', 'd', 'k')}
+                shape = (st.poles, st.samples)
+            else:
+                coef = {k: float(getattr(st, k)[0]) for k in ('a', 'd', 'k')}
+                shape = (st.samples,)
+            k_sum = coef['k'].sum(axis=0) if st.multiple else coef['k']
+            self.ade.append(dict(state=st, P=np.zeros(shape, dtype), Q=np.zeros(shape, dtype), k_sum=k_sum, **coef))
         self.counter = 0
         self.traces = np.zeros((plan.steps, len(plan.traces)), dtype=dtype)
         self.planes = plane_entries(plan, dft_float64)
@@ -165,7 +178,19 @@ class YeeOracle:
         return result
 
     def update_E(self):
+        flat = self.E.reshape(-1)
+        prepared = [(flat[m['state'].target], (m['Q'] - m['a'] * m['P']) / m['d']) for m in self.ade]
         self.E += self.courant * self.inverse_permittivity * self.curl(self.H, False)
+        for m, (old, response) in zip(self.ade, prepared):
+            free = flat[m['state'].target]
+            total = response.sum(axis=0) if m['state'].multiple else response
+            eps = m['state'].eps_inf
+            new = (eps * free - m['k_sum'] * old - total) / (eps + m['k_sum'])
+            delta = response + m['k'] * (new + old)
+            m['P'] += delta
+            m['Q'] *= -1
+            m['Q'] += 2 * delta
+            flat[m['state'].target] = new
 
     def update_H(self):
         self.H -= self.courant * self.inverse_permeability * self.curl(self.E, True)

@@ -413,9 +413,42 @@ def tfsf_scenes(ref):
     return out
 
 
+def dispersive_scenes(ref):
+    """Dispersive materials through the coupled trapezoidal ADE: 3D with a Drude sphere and a Lorentz slab (cell
+    sampling); 2D TMz with a two-pole material reaching into the PML under pml_dispersion='frozen' and a Lorentz
+    circle (Yee sampling)."""
+    from torchfdtd.models import LorentzPole
+    P, R, S, M, F, St, Sp, Mat = (ref.Project, ref.Region, ref.Source, ref.Monitor, ref.FieldMonitor, ref.Structure,
+                                  ref.SpectrumSettings, ref.Material)
+    out = {}
+    metal = Mat(name='metal', model='drude', epsilon_inf=1.5, plasma_rad_s=9e15, collision_rad_s=1e14)
+    glass = Mat(name='disp', model='lorentz', epsilon_inf=2.0, resonance_rad_s=3e15, linewidth_rad_s=2e14, delta_epsilon=1.2)
+    out['drude3d'] = P(name='drude3d', region=R(dimension='3d', size=(2.0, 1.6, 1.4), mesh=.05, pml_cells=6, steps=160, backend='cpu'),
+                       materials=[metal, glass],
+                       structures=[St(id='ball', name='ball', kind='sphere', center=(.3, 0, 0), radius=.2, material='metal'),
+                                   St(id='slab', name='slab', size=(.2, 1.6, 1.4), center=(-.35, 0, 0), material='disp')],
+                       sources=[S(id='src', center=(-.6, .1, 0), component='Ey', wavelength=1.2, pulse_cycles=2)],
+                       monitors=[M(id='probe', center=(.55, 0, 0), component='Ey'), M(id='in', center=(-.35, .1, .05), component='Ey'),
+                                 F(id='plane', normal='x', center=(.6, 0, 0), size=(0, .8, .6),
+                                   spectrum=Sp(sampling='frequency', frequency_points=2, apodization='none'))])
+    multi = Mat(name='multi', model='multipole', epsilon_inf=1.8,
+                poles=[LorentzPole(resonance_rad_s=2.5e15, strength_rad_s_squared=6e30, damping_rad_s=1e14),
+                       LorentzPole(resonance_rad_s=0, strength_rad_s_squared=2e30, damping_rad_s=3e14)])
+    lor = Mat(name='lor', model='lorentz', epsilon_inf=1.2, resonance_rad_s=4e15, linewidth_rad_s=1e14, delta_epsilon=2.0)
+    out['frozen2d'] = P(name='frozen2d', region=R(dimension='2d', size=(3.0, 2.4, 1), mesh=.04, pml_cells=8, steps=300,
+                                                  material_sampling='yee', pml_dispersion='frozen', backend='cpu'),
+                        materials=[multi, lor],
+                        structures=[St(id='bar', name='bar', size=(3.0, .3, 1), center=(0, -.5, 0), material='multi'),
+                                    St(id='c', name='c', kind='circle', center=(.4, .3, 0), radius=.25, material='lor')],
+                        sources=[S(id='src', center=(-.8, 0, 0), component='Ez', wavelength=1.3, pulse_cycles=2)],
+                        monitors=[M(id='probe', center=(.9, .1, 0), component='Ez'), M(id='inbar', center=(0, -.5, 0), component='Ez')])
+    return out
+
+
 def write_sources(ref):
     write_scenes(ref, source_scenes(ref))
     write_scenes(ref, tfsf_scenes(ref))
+    write_scenes(ref, dispersive_scenes(ref))
 
 
 def write_results(ref):

@@ -39,8 +39,10 @@ def skip_unmarchable(plan_or_project, kernel):
     periodic x/y faces; other scenes run the gather kernel."""
     region = getattr(plan_or_project, 'region', None) or plan_or_project.project.region
     project = plan_or_project if hasattr(plan_or_project, 'region') else plan_or_project.project
-    if kernel != 'gather' and project is not None and any(s.enabled and s.kind == 'tfsf' for s in project.sources):
-        pytest.skip('TFSF scenes run the split gather kernels')
+    if kernel != 'gather' and project is not None and (
+            any(s.enabled and s.kind == 'tfsf' for s in project.sources)
+            or any(m.oscillators for m in project.materials if m.name in {s.material for s in project.structures if s.enabled})):
+        pytest.skip('TFSF and dispersive scenes run the split gather kernels')
     periodic_xy = any(region.boundaries.pair(a)[0].kind == 'periodic' for a in (0, 1))
     if kernel == 'march' and region.dimension == '2d':
         pytest.skip('scene runs the gather kernel')
@@ -79,7 +81,7 @@ def test_random_state_and_every_cpml_memory_match_reference_bitwise(golden, kern
 
 
 SIMS = ['tmz', 'strip3d', 'strip3d_f64', 'yee_periodic', 'te2d', 'both2d', 'tiny', 'graded3d', 'graded2d', 'steps3d', 'explicit3d',
-        'oneway3d', 'oneway2d', 'tfsf3d', 'tfsf2d']
+        'oneway3d', 'oneway2d', 'tfsf3d', 'tfsf2d', 'drude3d', 'frozen2d']
 
 
 @pytest.mark.parametrize('kernel', KERNELS)

@@ -92,8 +92,10 @@ def test_selector_refuses_other_paths_before_any_gpu_work(change, match):
     (lambda p: setattr(p.region.boundaries, 'y_min', BoundaryFace(kind='bloch')) or
      setattr(p.region.boundaries, 'y_max', BoundaryFace(kind='bloch')), 'Bloch'),
     (lambda p: setattr(p.region.boundaries, 'x_max', BoundaryFace(kind='pmc')), 'PMC'),
-    (lambda p: p.materials.append(Material(name='metal', model='drude')) or
-     p.structures.append(Structure(material='metal', size=(.2, .2, 1))), 'drude'),
+    (lambda p: p.materials.append(Material(name='aniso', model='tensor')) or
+     p.structures.append(Structure(material='aniso', size=(.2, .2, 1))), 'tensor'),
+    (lambda p: setattr(p.region, 'pml_dispersion', 'absorber') or p.materials.append(Material(name='metal', model='drude')) or
+     p.structures.append(Structure(material='metal', size=(.2, .2, 1))), 'absorber'),
     (lambda p: p.sources.append(Source(kind='plane', injection='oneway', normal='x', size=(0, 2, 0), center=(-.5, 0, 0))),
      'periodic transverse'),
     (lambda p: setattr(p.region, 'interface_method', 'subpixel'), 'Subpixel'),

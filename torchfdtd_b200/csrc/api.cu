@@ -76,6 +76,12 @@ struct PlaneLayout {
     size_t cell, weight, omega, half, window, acc;
 };
 
+struct AdeLayout {
+    size_t state;                  // P then Q: 2 x poles x samples elements
+    size_t coef;                   // a, d, k: 3 x poles elements
+    size_t weight;                 // samples doubles (diagnostics), 0: unit
+};
+
 struct TfsfLayout {
     size_t line;                   // e, h, pe, ph: 4 x count elements
     size_t coef;                   // b_e, c_e, b_h, c_h: 4 x count elements
@@ -97,6 +103,8 @@ struct Layout {
     size_t src_values = 0, trace_tab = 0, trace_out = 0, plane_tab = 0;
     std::vector<PlaneLayout> planes;
     std::vector<TfsfLayout> tfsf;
+    std::vector<AdeLayout> ade;
+    size_t ade_map = 0;            // 3 x count int32 sample indices
     size_t volume[3];              // diagnostics cell volumes per axis (double), 0: unit
     size_t counter = 0, done = 0, status = 0, diag = 0, stage = 0;
     size_t grid_bar = 0;           // persistent 2D stepping: arrival count and generation
@@ -165,6 +173,17 @@ int validate(const tfd_desc *d) {
     }
     if (d->n_planes < 0 || d->n_planes > 65535 || (d->n_planes && !d->planes)) return fail(TFD_ERR_INVALID, "bad plane list");
     if (d->n_tfsf < 0 || d->n_tfsf > kMaxTfsf || (d->n_tfsf && !d->tfsf)) return fail(TFD_ERR_INVALID, "at most 4 TFSF boxes are supported per plan");
+    if (d->n_ade < 0 || d->n_ade > kMaxAde || (d->n_ade && !d->ade)) return fail(TFD_ERR_INVALID, "at most 8 dispersive material states are supported per plan");
+    for (int k = 0; k < d->n_ade; ++k) {
+        const tfd_ade &m = d->ade[k];
+        if (m.samples < 0 || m.poles < 1 || m.poles > kMaxPoles || (m.samples && !m.target) || !m.a || !m.d || !m.k || !m.w0 ||
+            !m.strength || !(m.eps_inf > 0))
+            return fail(TFD_ERR_INVALID, "bad dispersive material state");
+        const long long cells = (long long)d->nx * d->ny * d->nz;
+        for (int j = 0; j < m.samples; ++j)
+            if (m.target[j] < 0 || m.target[j] >= 3 * cells || !active(d->components, (int)(m.target[j] % 3)))
+                return fail(TFD_ERR_INVALID, "a dispersive sample lies outside the grid or on a component this plan does not advance");
+    }
     for (int k = 0; k < d->n_tfsf; ++k) {
         const tfd_tfsf &t = d->tfsf[k];
         if (t.count < 2 || t.drive_at < 0 || t.drive_at >= t.count || !t.drive || !t.b[0] || !t.b[1] || !t.c[0] || !t.c[1])
@@ -406,6 +425,14 @@ void compute_layout(const tfd_desc *d, Layout &L) {
         }
     }
     for (int a = 0; a < 3; ++a) L.volume[a] = d->volume[a] ? b.take((size_t)n[a] * sizeof(double)) : 0;
+    L.ade.resize(d->n_ade);
+    L.ade_map = d->n_ade > 0 ? b.take((size_t)3 * L.count * sizeof(int)) : 0;
+    for (int k = 0; k < d->n_ade; ++k) {
+        const tfd_ade &m = d->ade[k];
+        L.ade[k].state = b.take(std::max<size_t>(1, (size_t)2 * m.poles * m.samples) * L.elem);
+        L.ade[k].coef = b.take((size_t)3 * m.poles * L.elem);
+        L.ade[k].weight = m.weight ? b.take(std::max<size_t>(1, m.samples) * sizeof(double)) : 0;
+    }
     if (tile2d_capable(d)) {
         L.strip_rows = persist2d_eligible((long long)d->nx * d->ny) ? persist2d_strip_rows() : strip_rows((long long)d->nx * d->ny);
         L.tiles2d = (int)strips_of(strip_geom(d), 0, L.strip_rows).size();
@@ -453,6 +480,9 @@ struct tfd_plan {
     TfsfArgs<float> tf{};          // TFSF boxes (the step runs the split gather kernels when there are any)
     TfsfArgs<double> td{};
     double tfsf_index[kMaxTfsf] = {}, tfsf_norm[kMaxTfsf] = {};   // diagnostics: background index, norm weight
+    bool split = false;            // TFSF boxes or dispersive materials: the split gather step
+    // Diagnostics of the dispersive states: per state and pole the divisors of Q and the factors of P.
+    std::vector<std::vector<double>> ade_cq, ade_cp;
     template <typename T> TfsfArgs<T> &tfsf();
     // Boundary strips run on auxiliary streams, forked from and joined back to the caller's stream
     // (a CUDA graph capture records them as parallel branches).
@@ -615,6 +645,54 @@ int create_typed(tfd_plan *p, const tfd_desc *d, cudaStream_t s) {
             std::vector<double> v(d->volume[a], d->volume[a] + n[a]);
             if (int rc = upload(s, p, L.volume[a], v)) return rc;
         }
+    // dispersive materials: the per-component sample map, pole coefficients, states (zeroed by zero_state)
+    g.n_ade = d->n_ade;
+    for (int c = 0; c < 3; ++c) g.ade_map[c] = nullptr;
+    if (d->n_ade > 0) {
+        std::vector<int> map((size_t)3 * L.count, -1);
+        int start = 0;
+        for (int k = 0; k < d->n_ade; ++k) {
+            const tfd_ade &m = d->ade[k];
+            AdeDev<T> &st = g.ade[k];
+            st.start = start;
+            st.samples = m.samples;
+            st.poles = m.poles;
+            for (int j = 0; j < m.samples; ++j) {
+                const long long cell = m.target[j] / 3;
+                const int comp = (int)(m.target[j] % 3);
+                const int x = (int)(cell / ((long long)n[1] * n[2])), y = (int)((cell / n[2]) % n[1]), z = (int)(cell % n[2]);
+                int &slot = map[(size_t)comp * L.count + (size_t)z * g.plane + (size_t)y * L.pitch + x];
+                if (slot >= 0) return fail(TFD_ERR_INVALID, "dispersive material states overlap");
+                slot = start + j;
+            }
+            start += m.samples;
+            std::vector<T> coef((size_t)3 * m.poles);
+            T ksum = T(0);
+            for (int q = 0; q < m.poles; ++q) {
+                coef[q] = (T)m.a[q];
+                coef[m.poles + q] = (T)m.d[q];
+                coef[2 * m.poles + q] = (T)m.k[q];
+                ksum = q == 0 ? (T)m.k[0] : ksum + (T)m.k[q];
+            }
+            st.eps = (T)m.eps_inf;
+            st.ksum = ksum;
+            // One pole: eps_inf + k added in float64 and rounded once; several: summed in the field precision.
+            st.denom = m.multiple ? (T)m.eps_inf + ksum : (T)(m.eps_inf + m.k[0]);
+            if (int rc = upload(s, p, L.ade[k].coef, coef)) return rc;
+            const T *cp = p->ptr<T>(L.ade[k].coef);
+            st.a = cp;
+            st.d = cp + m.poles;
+            st.k = cp + 2 * m.poles;
+            st.P = p->ptr<T>(L.ade[k].state);
+            st.Q = st.P + (size_t)m.poles * m.samples;
+            if (L.ade[k].weight) {
+                std::vector<double> w(m.weight, m.weight + m.samples);
+                if (int rc = upload(s, p, L.ade[k].weight, w)) return rc;
+            }
+        }
+        if (int rc = upload(s, p, L.ade_map, map)) return rc;
+        for (int c = 0; c < 3; ++c) g.ade_map[c] = p->ptr<int>(L.ade_map) + (size_t)c * L.count;
+    }
     // nonuniform-mesh factors
     for (int f = 0; f < 2; ++f)
         for (int a = 0; a < 3; ++a) {
@@ -730,6 +808,10 @@ int zero_state(tfd_plan *p, cudaStream_t s) {
     }
     for (size_t k = 0; k < L.tfsf.size(); ++k)
         TFD_CUDA(cudaMemsetAsync(p->arena + L.tfsf[k].line, 0, (size_t)4 * p->tfsf<T>().box[k].count * L.elem, s));
+    for (size_t k = 0; k < L.ade.size(); ++k) {
+        const AdeDev<T> &st = p->grid<T>().ade[k];
+        TFD_CUDA(cudaMemsetAsync(p->arena + L.ade[k].state, 0, (size_t)2 * st.poles * st.samples * L.elem, s));
+    }
     TFD_CUDA(cudaMemsetAsync(p->arena + L.counter, 0, sizeof(long long), s));
     TFD_CUDA(cudaMemsetAsync(p->arena + L.done, 0, sizeof(unsigned), s));
     TFD_CUDA(cudaMemsetAsync(p->arena + L.grid_bar, 0, 2 * sizeof(unsigned), s));
@@ -1413,10 +1495,11 @@ int launch_persist2d(tfd_plan *p, int nsteps, cudaStream_t s) {
     return TFD_OK;
 }
 
-// One step of a plan with TFSF boxes: the split gather E kernel, the boxes' E half step and E corrections, the
-// split gather H kernel, the H half step and H corrections (the observation launch follows in step_t).
+// One split step (plans with TFSF boxes or dispersive materials): the split gather E kernel, the boxes' E half
+// step and E corrections, the split gather H kernel, the H half step and H corrections (the observation launch
+// follows in step_t).
 template <typename T>
-int launch_tfsf_step(tfd_plan *p, cudaStream_t s) {
+int launch_split_step(tfd_plan *p, cudaStream_t s) {
     const Grid<T> &g = p->grid<T>();
     TfsfArgs<T> a = p->tfsf<T>();
     for (int par = 0; par < 2; ++par)
@@ -1434,13 +1517,13 @@ int launch_tfsf_step(tfd_plan *p, cudaStream_t s) {
         case kMaskTE: k_step_gather_e<T, kMaskTE><<<grid, block, 0, s>>>(g); break;
         default: k_step_gather_e<T, kMaskAll><<<grid, block, 0, s>>>(g); break;
     }
-    k_tfsf<T><<<tgrid, kTfsfThreads, 0, s>>>(a, 0);
+    if (a.boxes > 0) k_tfsf<T><<<tgrid, kTfsfThreads, 0, s>>>(a, 0);
     switch (g.active) {
         case kMaskTM: k_step_gather_h<T, kMaskTM><<<grid, block, 0, s>>>(g); break;
         case kMaskTE: k_step_gather_h<T, kMaskTE><<<grid, block, 0, s>>>(g); break;
         default: k_step_gather_h<T, kMaskAll><<<grid, block, 0, s>>>(g); break;
     }
-    k_tfsf<T><<<tgrid, kTfsfThreads, 0, s>>>(a, 1);
+    if (a.boxes > 0) k_tfsf<T><<<tgrid, kTfsfThreads, 0, s>>>(a, 1);
     return TFD_OK;
 }
 
@@ -1453,8 +1536,8 @@ int step_t(tfd_plan *p, int nsteps, cudaStream_t s) {
     const MonitorArgs<T> m = monitor_args<T>(p);
     dim3 mgrid((unsigned)std::max(1, (p->max_samples + kMonitorThreads - 1) / kMonitorThreads), (unsigned)std::max(1, p->desc.n_planes));
     for (int k = 0; k < nsteps; ++k) {
-        if (p->tfsf<T>().boxes > 0) {
-            TFD_CHECK(launch_tfsf_step<T>(p, s));
+        if (p->split) {
+            TFD_CHECK(launch_split_step<T>(p, s));
         } else if (p->kernel == TFD_KERNEL_MARCH) {
             launch_march_any<T>(p, s);
         } else if (p->kernel == TFD_KERNEL_TILE2D) {
@@ -1508,6 +1591,18 @@ int diagnose_t(tfd_plan *p, double out[3], cudaStream_t s) {
         d.psi_len[d.n_psi++] = bx.count;
         d.psi[d.n_psi] = bx.ph;
         d.psi_len[d.n_psi++] = bx.count;
+    }
+    d.n_ade = g.n_ade;
+    for (int k = 0; k < g.n_ade; ++k) {
+        d.ade_P[k] = g.ade[k].P;
+        d.ade_Q[k] = g.ade[k].Q;
+        d.ade_samples[k] = g.ade[k].samples;
+        d.ade_poles[k] = g.ade[k].poles;
+        for (int q = 0; q < g.ade[k].poles; ++q) {
+            d.ade_cq[k][q] = p->ade_cq[k][q];
+            d.ade_cp[k][q] = p->ade_cp[k][q];
+        }
+        d.ade_weight[k] = L.ade[k].weight ? p->ptr<double>(L.ade[k].weight) : nullptr;
     }
     d.partial = p->ptr<double>(L.diag);
     k_diag<T><<<kDiagBlocks, kDiagThreads, 0, s>>>(d);
@@ -1604,6 +1699,16 @@ int tfd_plan_create(const tfd_desc *desc, void *arena, size_t arena_bytes, void 
         p->seg_lo.push_back(desc->segments[k].lo);
         p->seg_hi.push_back(desc->segments[k].hi);
     }
+    for (int k = 0; k < desc->n_ade; ++k) {
+        const tfd_ade &m = desc->ade[k];
+        std::vector<double> cq(m.poles), cp(m.poles);
+        for (int q = 0; q < m.poles; ++q) {
+            cq[q] = desc->time_step * std::sqrt(m.strength[q]);
+            cp[q] = m.w0[q] / std::sqrt(m.strength[q]);
+        }
+        p->ade_cq.push_back(cq);
+        p->ade_cp.push_back(cp);
+    }
     for (int k = 0; k < desc->n_planes; ++k) {
         p->planes_f.push_back(desc->planes[k].frequencies);
         p->planes_p.push_back(desc->planes[k].points);
@@ -1618,14 +1723,15 @@ int tfd_plan_create(const tfd_desc *desc, void *arena, size_t arena_bytes, void 
             rc = fail(TFD_ERR_UNSUPPORTED, "the marching kernel needs a 3D grid");
         else if (desc->kernel == TFD_KERNEL_TILE2D && !tile_ok)
             rc = fail(TFD_ERR_UNSUPPORTED, "the 2D tile kernel needs a 2D TMz grid without periodic x/y faces");
-        if (desc->n_tfsf > 0 && (desc->kernel == TFD_KERNEL_MARCH || desc->kernel == TFD_KERNEL_TILE2D))
-            rc = fail(TFD_ERR_UNSUPPORTED, "plans with TFSF boxes run the split gather kernels");
-        if (desc->kernel == TFD_KERNEL_GATHER || desc->n_tfsf > 0) p->kernel = TFD_KERNEL_GATHER;
+        p->split = desc->n_tfsf > 0 || desc->n_ade > 0;
+        if (p->split && (desc->kernel == TFD_KERNEL_MARCH || desc->kernel == TFD_KERNEL_TILE2D))
+            rc = fail(TFD_ERR_UNSUPPORTED, "plans with TFSF boxes or dispersive materials run the split gather kernels");
+        if (desc->kernel == TFD_KERNEL_GATHER || p->split) p->kernel = TFD_KERNEL_GATHER;
         else if (march_ok) p->kernel = TFD_KERNEL_MARCH;
         else if (tile_ok) p->kernel = TFD_KERNEL_TILE2D;
         else p->kernel = TFD_KERNEL_GATHER;
         if (!rc && p->kernel == TFD_KERNEL_MARCH) rc = TFD_DISPATCH(p, setup_march, p);
-        if (!rc && tile_ok && desc->n_tfsf == 0) rc = TFD_DISPATCH(p, setup_tile2d, p, s);
+        if (!rc && tile_ok && !p->split) rc = TFD_DISPATCH(p, setup_tile2d, p, s);
     }
     if (!rc) rc = TFD_DISPATCH(p, zero_state, p, s);
     if (!rc) {
@@ -1762,8 +1868,8 @@ int tfd_step_launches(const tfd_plan *p, int32_t nsteps, int64_t *launches) {
     if (!p || !launches) return fail(TFD_ERR_INVALID, "null argument");
     if (nsteps < 0) return fail(TFD_ERR_INVALID, "nsteps must be non-negative");
     long long per_step = 2;                                   // gather: step + observation
-    if (p->desc.n_tfsf > 0) {
-        per_step = 5;                                         // split E, TFSF E, split H, TFSF H, observation
+    if (p->split) {
+        per_step = p->desc.n_tfsf > 0 ? 5 : 3;                // split E, (TFSF E), split H, (TFSF H), observation
     } else if (p->kernel == TFD_KERNEL_TILE2D) {
         if (p->persist_ctas > 0 && !p->in_batch) {
             *launches = nsteps > 0 ? 1 : 0;

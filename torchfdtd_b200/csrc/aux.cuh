@@ -425,6 +425,13 @@ struct DiagArgs {
     const T *line[8];
     int line_len[8];
     double line_factor[8], line_weight[8];
+    // Dispersive states: per state P and Q ([poles][samples]); the norm adds (Q / cq_p)^2 + (P cp_p)^2 per pole,
+    // weighed by the sample's volume (rounded to the field precision; nullptr: 1).
+    int n_ade;
+    const T *ade_P[kMaxAde], *ade_Q[kMaxAde];
+    int ade_samples[kMaxAde], ade_poles[kMaxAde];
+    double ade_cq[kMaxAde][kMaxPoles], ade_cp[kMaxAde][kMaxPoles];
+    const double *ade_weight[kMaxAde];
     double *partial;             // [gridDim.x][4]
 };
 
@@ -476,6 +483,17 @@ __global__ void __launch_bounds__(kDiagThreads) k_diag(const __grid_constant__ D
             const double v = (double)d.line[k][e] * d.line_factor[k];
             energy += v * v * d.line_weight[k];
         }
+    for (int k = 0; k < d.n_ade; ++k) {
+        const int ns = d.ade_samples[k];
+        for (int p = 0; p < d.ade_poles[k]; ++p)
+            for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ns; e += (long long)gridDim.x * blockDim.x) {
+                const double w = d.ade_weight[k] ? (double)(T)d.ade_weight[k][e] : 1.0;
+                const double q = (double)d.ade_Q[k][p * ns + e] / d.ade_cq[k][p];
+                const double v = (double)d.ade_P[k][p * ns + e] * d.ade_cp[k][p];
+                energy += q * q * w;
+                energy += v * v * w;
+            }
+    }
     for (int k = 0; k < d.n_psi; ++k)
         for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < d.psi_len[k]; e += (long long)gridDim.x * blockDim.x)
             if (!isfinite((double)d.psi[k][e])) finite = 0.0;

@@ -44,6 +44,19 @@ struct SourceTerm {
     int lo[3], hi[3];
 };
 
+constexpr int kMaxAde = 8;
+constexpr int kMaxPoles = 16;
+
+// One dispersive material state on the device: samples [start, start + samples) of the plan's sample list,
+// P and Q as [poles][samples], coefficients in the field precision.
+template <typename T>
+struct AdeDev {
+    int start, samples, poles;
+    T eps, ksum, denom;          // eps_inf, sum of k, the denominator eps_inf + k_sum
+    const T *a, *d, *k;          // [poles]
+    T *P, *Q;
+};
+
 template <typename T>
 struct Grid {
     int n[3];
@@ -69,6 +82,10 @@ struct Grid {
     int n_src;
     SourceTerm src[kMaxSources];
     const T *src_values;         // [n_src][steps]
+    // Dispersive materials: per E component the sample index of each cell (-1: none); nullptr without any.
+    const int *ade_map[3];
+    int n_ade;
+    AdeDev<T> ade[kMaxAde];
     long long *counter;
     int *status;
 

@@ -64,12 +64,38 @@ __device__ __forceinline__ void e_term(const Grid<T> &g, int par, int x, int y, 
     acc = acc + (t.sign > 0 ? d : -d);
 }
 
+// The coupled trapezoidal ADE of dispersive sample j: E_new from the free update and the old E, and (when own)
+// the pole states advanced. Reference operation order (torchfdtd/materials.py:67-88).
+template <typename T>
+__device__ __forceinline__ T ade_correct(const Grid<T> &g, int j, T old, T free, bool own) {
+    int s = 0;
+    while (s + 1 < g.n_ade && j >= g.ade[s + 1].start) ++s;
+    const AdeDev<T> &st = g.ade[s];
+    const int l = j - st.start, ns = st.samples;
+    auto response = [&](int p) -> T { return (st.Q[p * ns + l] - st.a[p] * st.P[p * ns + l]) / st.d[p]; };
+    T total = response(0);
+    for (int p = 1; p < st.poles; ++p) total = total + response(p);
+    const T e = (st.eps * free - st.ksum * old - total) / st.denom;
+    if (own) {
+        for (int p = 0; p < st.poles; ++p) {
+            const T delta = response(p) + st.k[p] * (e + old);
+            st.P[p * ns + l] = st.P[p * ns + l] + delta;
+            st.Q[p * ns + l] = -st.Q[p * ns + l] + T(2) * delta;
+        }
+    }
+    return e;
+}
+
 template <typename T, int C>
 __device__ __forceinline__ T e_value(const Grid<T> &g, int par, long long n, int x, int y, int z, long long i, bool own) {
     T acc = T(0);
     e_term<T, C, 0>(g, par, x, y, z, i, own, acc);
     e_term<T, C, 1>(g, par, x, y, z, i, own, acc);
-    const T e = g.E[par][C][i] + (g.cn * g.inv_eps[C][i]) * acc;
+    T e = g.E[par][C][i] + (g.cn * g.inv_eps[C][i]) * acc;
+    if (g.ade_map[C] != nullptr) {
+        const int j = g.ade_map[C][i];
+        if (j >= 0) e = ade_correct(g, j, g.E[par][C][i], e, own);
+    }
     return inject(g, 0, C, n, x, y, z, e);
 }
 
@@ -150,7 +176,8 @@ __global__ void __launch_bounds__(128) k_step_gather_rows(const __grid_constant_
 }
 
 // The step split in two launches (plans with TFSF boxes, whose E corrections must land between the E and the
-// H update): the E kernel writes E_new and the E-family CPML memories, the H kernel reads E_new back.
+// H update, and plans with dispersive materials, whose pole states each E sample advances exactly once): the E
+// kernel writes E_new and the E-family CPML memories, the H kernel reads E_new back.
 template <typename T, int ACTIVE>
 __global__ void __launch_bounds__(128) k_step_gather_e(const __grid_constant__ Grid<T> g) {
     const long long n = *g.counter;

@@ -58,9 +58,32 @@ class Material(Model):
     fit_dt_s: float | None = Field(default=None, gt=0)
     provenance: dict[str, Any] | None = None
 
+    @model_validator(mode='after')
+    def valid_poles(self):
+        if self.model == 'multipole' and not self.poles:
+            raise ValueError('A multipole material requires at least one passive pole.')
+        return self
+
     @property
     def dispersive(self):
         return self.model in ('drude', 'lorentz', 'multipole')
+
+    @property
+    def oscillator(self):
+        """(resonance w0, strength, damping) of a single-pole Drude or Lorentz material, else None:
+        Drude (0, wp^2, collision rate), Lorentz (w0, delta_eps w0^2, 2 x linewidth)."""
+        if self.model == 'drude':
+            return 0., self.plasma_rad_s**2, self.collision_rad_s
+        if self.model == 'lorentz':
+            return self.resonance_rad_s, self.delta_epsilon * self.resonance_rad_s**2, 2 * self.linewidth_rad_s
+        return None
+
+    @property
+    def oscillators(self):
+        """Every pole as (w0, strength, damping): chi(w) = sum strength / (w0^2 - w^2 - i damping w)."""
+        if self.model == 'multipole':
+            return tuple(pole.coefficients for pole in self.poles)
+        return (self.oscillator,) if self.oscillator else ()
 
     @property
     def instantaneous_epsilon(self):

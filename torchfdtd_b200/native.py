@@ -54,6 +54,11 @@ class TfsfC(ctypes.Structure):
                 ('target', P_i64 * 2), ('sample', P_i64 * 2), ('weight', P_dbl * 2)]
 
 
+class AdeC(ctypes.Structure):
+    _fields_ = [('samples', c_i32), ('poles', c_i32), ('multiple', c_i32), ('target', P_i64), ('eps_inf', c_dbl),
+                ('a', P_dbl), ('d', P_dbl), ('k', P_dbl), ('w0', P_dbl), ('strength', P_dbl), ('weight', P_dbl)]
+
+
 class Desc(ctypes.Structure):
     _fields_ = [('abi_version', c_i32), ('nx', c_i32), ('ny', c_i32), ('nz', c_i32), ('precision', c_i32),
                 ('material_samples', c_i32), ('components', c_i32), ('steps', c_i32), ('kernel', c_i32),
@@ -63,7 +68,8 @@ class Desc(ctypes.Structure):
                 ('n_sources', c_i32), ('sources', ctypes.POINTER(SourceTermC)),
                 ('n_traces', c_i32), ('traces', ctypes.POINTER(TraceC)),
                 ('n_planes', c_i32), ('planes', ctypes.POINTER(PlaneC)), ('metric', (P_dbl * 3) * 2),
-                ('volume', P_dbl * 3), ('n_tfsf', c_i32), ('tfsf', ctypes.POINTER(TfsfC))]
+                ('volume', P_dbl * 3), ('n_tfsf', c_i32), ('tfsf', ctypes.POINTER(TfsfC)),
+                ('n_ade', c_i32), ('ade', ctypes.POINTER(AdeC))]
 
 
 # Every entry point of include/tfdtd.h with its ctypes signature.
@@ -308,7 +314,28 @@ def describe(plan, kernel='auto', variant=0):
             t.n_targets[f] = len(target)
             t.target[f], t.sample[f], t.weight[f] = _ptr(target, c_i64), _ptr(sample, c_i64), _ptr(weight, ctypes.c_double)
     desc.n_tfsf, desc.tfsf = len(boxes), tf
-    keep.extend([segs, srcs, traces, planes, tf])
+    states = getattr(plan, 'ade', [])
+    ade = (AdeC * max(1, len(states)))()
+    nonuniform = region is not None and (region.mesh_type != 'uniform' or region.mesh_steps is not None)
+    for k, st in enumerate(states):
+        m = ade[k]
+        m.samples, m.poles, m.multiple, m.eps_inf = st.samples, st.poles, int(st.multiple), st.eps_inf
+        arrays = [np.ascontiguousarray(st.target, dtype=np.int64)] + [np.ascontiguousarray(getattr(st, f), dtype=np.float64)
+                                                                      for f in ('a', 'd', 'k', 'w0', 'strength')]
+        keep.extend(arrays)
+        m.target = _ptr(arrays[0], c_i64)
+        m.a, m.d, m.k, m.w0, m.strength = (_ptr(v, ctypes.c_double) for v in arrays[1:])
+        if nonuniform:
+            # The state norm weighs each sample by its cell's volume in reference-step units.
+            widths = [np.diff(nodes) / region.reference_step if n > 1 else np.ones(1)
+                      for nodes, n in zip(region.mesh_nodes, plan.shape)]
+            cell = st.target // 3
+            x, y, z = np.unravel_index(cell, plan.shape)
+            w = np.ascontiguousarray(widths[0][x] * widths[1][y] * widths[2][z], dtype=np.float64)
+            keep.append(w)
+            m.weight = _ptr(w, ctypes.c_double)
+    desc.n_ade, desc.ade = len(states), ade
+    keep.extend([segs, srcs, traces, planes, tf, ade])
     return desc, keep
 
 

@@ -127,6 +127,7 @@ class GridPlan:
     warnings: list = field(default_factory=list)
     metrics: dict = field(default_factory=dict)   # (forward, axis) -> (float64 (n-1,) interior values, wrap value)
     tfsf: list = field(default_factory=list)      # tfsf.TfsfBox per enabled TFSF source, in source order
+    ade: list = field(default_factory=list)       # materials.ADEState per dispersive material state
 
     @property
     def cells(self):
@@ -234,8 +235,8 @@ def check_supported(project):
         raise ValueError('pml_dispersion="absorber" is not implemented by the fused B200 engine.')
     active = {s.material for s in project.structures if s.enabled}
     for m in project.materials:
-        if m.name in active and m.model != 'dielectric':
-            raise ValueError(f'{m.name}: {m.model} materials are not implemented by the fused B200 engine (nondispersive dielectrics only).')
+        if m.name in active and m.model == 'tensor':
+            raise ValueError(f'{m.name}: tensor materials are not implemented by the fused B200 engine.')
     for raw in project.sources:
         s = project.resolved_source(raw)
         if not s.enabled:
@@ -315,6 +316,8 @@ def _voxelize_at(project, axes, dtype):
     eps = np.full(shape, r.background_index**2, dtype=dtype)
     active = {obj.material for obj in project.structures if obj.enabled}
     materials = {m.name: m.instantaneous_epsilon for m in project.materials if m.name in active}
+    ids = {m.name: i for i, m in enumerate(project.materials)}
+    owner = np.full(shape, -1, dtype=np.int32)     # material index of each sample (-1: background)
     counts = {}
     # Lower mesh order wins; at equal order the later object wins.
     for obj in sorted(project.structures, key=lambda s: -s.mesh_order):
@@ -333,21 +336,26 @@ def _voxelize_at(project, axes, dtype):
         xyz = np.meshgrid(*(axis[s] for axis, s in zip(axes, slices)), indexing='ij', sparse=True)
         mask = contains(obj, *xyz)
         eps[slices][mask] = materials[obj.material]
+        owner[slices][mask] = ids[obj.material]
         counts[obj.id] = int(np.count_nonzero(mask))
-    return eps, counts
+    return eps, counts, owner
 
 
-def voxelize(project, dtype):
+def voxelize(project, dtype, with_ownership=False):
+    """Staircase permittivity (and, with_ownership, the material index of every sample, -1 for background):
+    (nx, ny, nz) at cell centres, or (nx, ny, nz, 3) at the E samples with Yee sampling."""
     r = project.region
     if r.material_sampling == 'yee':
         parts = [_voxelize_at(project, field_axes(r, c), dtype) for c in ('Ex', 'Ey', 'Ez')]
         eps = np.stack([p[0] for p in parts], axis=-1)
         counts = {k: max(p[1].get(k, 0) for p in parts) for k in parts[0][1]}
-        return eps, counts
-    axes = [(np.arange(n) + .5) * r.mesh - s / 2 for n, s in zip(r.shape, r.actual_size)]
-    if r.dimension == '2d':
-        axes[2] = np.array([0.])
-    return _voxelize_at(project, axes, dtype)
+        owner = np.stack([p[2] for p in parts], axis=-1)
+    else:
+        axes = [(np.arange(n) + .5) * r.mesh - s / 2 for n, s in zip(r.shape, r.actual_size)]
+        if r.dimension == '2d':
+            axes[2] = np.array([0.])
+        eps, counts, owner = _voxelize_at(project, axes, dtype)
+    return (eps, counts, owner) if with_ownership else (eps, counts)
 
 
 # ---- monitors ----------------------------------------------------------------------------------
@@ -443,13 +451,16 @@ def plan_grid(project, polarization=None, material=True):
                  for a in range(3) if r.shape[a] > 1 and faces[a][1] in ('pec', 'antisymmetric')}
     segments = cpml_segments(r, courant)
     metrics = mesh_metrics(r)
+    ade = []
     if material:
-        eps, counts = voxelize(project, dtype)
+        eps, counts, owner = voxelize(project, dtype, with_ownership=True)
         from .injection import validate_oneway_materials
         from .tfsf import validate_tfsf_materials
         validate_oneway_materials(project, eps)
         validate_tfsf_materials(project, eps)
         inv_eps = (1 / eps).astype(dtype)
+        from .materials import ade_states
+        ade = ade_states(project, owner, inv_eps)
         warnings = [f'{obj.name}: no cells intersect this object. Refine mesh or reposition it.'
                     for obj in project.structures if obj.enabled and counts.get(obj.id) == 0]
     else:
@@ -491,4 +502,4 @@ def plan_grid(project, polarization=None, material=True):
         polarization = 'both' if tm and te else ('TE' if te else 'TM')
     return GridPlan(project, tuple(r.shape), r.dimension, dtype, courant, r.time_step, r.steps, faces, pec_upper,
                     segments, eps, inv_eps, counts, sources, traces, planes,
-                    polarization if r.dimension == '2d' else None, warnings, metrics, boxes)
+                    polarization if r.dimension == '2d' else None, warnings, metrics, boxes, ade)

@@ -364,8 +364,9 @@ class Observer:
                      gcells_per_s=cells * completed / max(seconds, 1e-9) / 1e9,
                      hbm_bytes_per_step=algorithmic_bytes_per_step(plan), arena_bytes=grid.arena_bytes,
                      field_peak=field_peak, slice_index=self.plane_index, slice_position=slice_position,
-                     complex_fields=False, complex_display=r.complex_display, material_update='nondispersive',
-                     dispersive_samples=0, material_sampling=r.material_sampling,
+                     complex_fields=False, complex_display=r.complex_display,
+                     material_update='trapezoidal ADE' if plan.ade else 'nondispersive',
+                     dispersive_samples=sum(st.poles * st.samples for st in plan.ade), material_sampling=r.material_sampling,
                      epsilon_definition='instantaneous relative permittivity (epsilon-infinity for dispersive cells)',
                      boundaries=r.boundaries.model_dump(), bloch_phase=r.bloch_phase,
                      units='geometry: um; time: s; E/H: reduced fields; Bloch phase: rad', engine=ENGINE)
