@@ -473,7 +473,8 @@ def run_ours_batch(args, world, rank, local):
         choice = tuning.choice
     grids = [NativeGrid(plan, kernel='tile2d') for plan in plans]
     batch = NativeBatch(grids)
-    batch.set_launch(*choice)
+    batch.set_launch(*choice[:2])
+    batch.set_persistent(bool(choice[2]) if len(choice) > 2 else False)
     tiles = batch.tiles()
     stream = torch.cuda.Stream(device)
     sampler = ClockSampler(local)
@@ -531,10 +532,11 @@ def run_ours_batch(args, world, rank, local):
                 data='synthetic (seeded)',
                 config=dict(workload=desc, cells=cells, l2=L2_NOTE),
                 grids=len(plans), strips=tiles, launch=choice,
-                tuning=[(r['ctas'], r['rows'], r['strips'], round(r['median_ms_per_step'], 5))
+                tuning=[(r['ctas'], r['rows'], r.get('persistent', 0), r['strips'], round(r['median_ms_per_step'], 5))
                         for r in tuning.candidates] if tuning else 'fixed by --batch-launch',
                 parallelism=f'replicas x{world}' if world > 1 else 'single GPU', kernel='tile2d',
-                roofline=roofline, e2e=e2e, clocks=clocks, gpu_launches=2 * args.steps, device_status=status)
+                roofline=roofline, e2e=e2e, clocks=clocks,
+                gpu_launches=1 if len(choice) > 2 and choice[2] else 2 * args.steps, device_status=status)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, steps, el, threads = batch_cpu_rate(plans, args.cpu_budget)
         line['cpu_baseline'] = dict(value=rate, unit=METRIC, cores=threads, kind='port',

@@ -273,6 +273,12 @@ int tfd_batch_create(int32_t n_plans, tfd_plan *const *plans, void *arena, size_
  * per strip), strip_rows = rows per strip (0: default for the batch's cell count; else >= 8). Rebuilds the
  * strip table on the stream when strip_rows changes; call it outside graph capture. */
 int tfd_batch_set_launch(tfd_batch *batch, int32_t ctas, int32_t strip_rows, void *stream);
+/* persistent = 1: every tfd_batch_step call runs all its steps in ONE cooperative launch over the strip table
+ * (with the observations of every member, a bounded grid barrier between steps; ctas as set above, capped at
+ * the resident limit), bitwise equal to the per-step launches; 0: one strip launch and one observation launch
+ * per step. Call it outside graph capture (it queries the occupancy). The north-star shape of the batched
+ * path; the reference has no counterpart (its cohorts launch per step, torchfdtd/cuda_batch.py:139-169). */
+int tfd_batch_set_persistent(tfd_batch *batch, int32_t persistent, void *stream);
 int tfd_batch_step(tfd_batch *batch, int32_t nsteps, void *stream);
 int tfd_batch_tiles(const tfd_batch *batch, int32_t *tiles);
 void tfd_batch_destroy(tfd_batch *batch);

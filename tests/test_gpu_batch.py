@@ -183,6 +183,20 @@ def test_uneven_batch_equals_cases_run_alone(precision):
         assert_results_equal(item.result, alone)
 
 
+@pytest.mark.parametrize('precision', ['float32', 'float64'])
+@pytest.mark.parametrize('graph', [False, True])
+def test_persistent_batch_equals_cases_run_alone(precision, graph):
+    """All steps of a replay in one cooperative launch over every member (uneven sizes, step counts, planes)."""
+    from torchfdtd_b200 import Simulation
+    from torchfdtd_b200.batch import run_tensor_batch
+    projects = uneven_cases(precision, steps=(30, 12, 41, 10, 30))
+    report = run_tensor_batch(projects, cuda_graph=graph, cuda_graph_steps=8, launch=(0, 16, 1))
+    assert report.successful and report.plan['launch'] == [0, 16, 1]
+    for p, item in zip(projects, report.items):
+        assert item.summary['steps'] == p.region.steps
+        assert_results_equal(item.result, Simulation(p).run(kernel='tile2d'))
+
+
 def test_batch_members_with_different_step_counts():
     from torchfdtd_b200 import Simulation
     from torchfdtd_b200.batch import run_tensor_batch

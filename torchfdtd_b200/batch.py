@@ -163,7 +163,8 @@ def run_tensor_batch(cases, *, objective=None, output_dir=None, keep_results=Tru
 
     Shapes, time steps, CPML depths, sources, monitors and step counts may differ between cases; one
     precision per cohort. ``launch`` sets the step kernel's launch shape: None for the default (one warp per
-    strip, strip rows sized to the cohort), a ``(ctas, strip_rows)`` pair (0 keeps a default), or 'auto' to
+    strip, strip rows sized to the cohort, one launch per step), a ``(ctas, strip_rows[, persistent])`` tuple (0
+    keeps a default; persistent 1 runs every replayed width of steps as one cooperative launch), or 'auto' to
     measure candidates on scratch copies first (``tune_tensor_batch``).
     ``epsilon`` (optional): one permittivity array (or None) per case, replacing its voxelized structures as
     ``Simulation(project, epsilon)`` does. Auto shutoff is rejected, never silently disabled. A numerical
@@ -240,7 +241,8 @@ def _run_cohort(cases, projects, objective, root, keep_results, memory_fraction,
     batch = NativeBatch(grids)
     try:
         if launch is not None:
-            batch.set_launch(*launch)
+            batch.set_launch(*launch[:2])
+            batch.set_persistent(bool(launch[2]) if len(launch) > 2 else False)
         steps = max(p.region.steps for p in projects)
         stream = torch.cuda.Stream()
         stream.wait_stream(torch.cuda.current_stream())

@@ -1894,6 +1894,8 @@ struct tfd_batch {
     int ntiles = 0, interior = 0, capacity = 0, rows = 8, ctas = 0, max_planes = 0, max_chunks = 1;
     SideStream side;
     long long cells = 0;
+    size_t bar = 0;                // persistent stepping: arrival count and generation
+    int persist_ctas = 0;          // > 0: all steps of a tfd_batch_step call in one cooperative launch
 };
 
 namespace {
@@ -1925,6 +1927,7 @@ int batch_layout(tfd_batch &b, int n, tfd_plan *const *plans) {
     b.grids = bump.take(n * grid_bytes);
     b.tiles = bump.take((size_t)b.capacity * sizeof(Tile2D));
     b.mon = bump.take(n * mon_bytes);
+    b.bar = bump.take(2 * sizeof(unsigned));
     b.total = bump.off + 256;
     return TFD_OK;
 }
@@ -1985,8 +1988,43 @@ int batch_create_t(tfd_batch *b, cudaStream_t s) {
     return batch_strips_t<T>(b, strip_rows(b->cells), s);
 }
 
+// The CTAs of a persistent batch launch: a warp per strip (or b->ctas when set), at least one CTA per
+// observation work item, no more than can be resident together.
+template <typename T>
+int batch_persist_ctas(tfd_batch *b, int &ctas) {
+    int device = 0, sms = 148, per_sm = 0;
+    TFD_CUDA(cudaGetDevice(&device));
+    TFD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    TFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step2d_batch_persistent<T>, k2dThreads, 0));
+    const int items = (int)b->plans.size() * b->max_chunks * std::max(1, b->max_planes);
+    const int want = b->ctas > 0 ? b->ctas : std::max({1, (b->ntiles + k2dWarps - 1) / k2dWarps, items});
+    ctas = per_sm > 0 ? std::min(want, per_sm * sms) : 0;
+    return ctas > 0 ? TFD_OK : fail(TFD_ERR_UNSUPPORTED, "the persistent batch kernel cannot be resident on this device");
+}
+
+template <typename T>
+int batch_persistent_step(tfd_batch *b, int nsteps, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)b->persist_ctas);
+    cfg.blockDim = dim3(k2dThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const Grid<T> *grids = (const Grid<T> *)(b->arena + b->grids);
+    TFD_CUDA(cudaMemsetAsync(b->arena + b->bar, 0, 2 * sizeof(unsigned), s));
+    TFD_CUDA(cudaLaunchKernelEx(&cfg, k_step2d_batch_persistent<T>, grids, (const Tile2D *)(b->arena + b->tiles), b->interior,
+                                b->ntiles, (const MonitorArgs<T> *)(b->arena + b->mon), (int)b->plans.size(), b->max_chunks,
+                                std::max(1, b->max_planes), (long long *)(b->arena + b->counter), nsteps,
+                                (unsigned *)(b->arena + b->bar), b->plans[0]->grid<T>().status));
+    return TFD_OK;
+}
+
 template <typename T>
 int batch_step_t(tfd_batch *b, int nsteps, cudaStream_t s) {
+    if (b->persist_ctas > 0) return nsteps > 0 ? batch_persistent_step<T>(b, nsteps, s) : TFD_OK;
     long long *counter = (long long *)(b->arena + b->counter);
     const dim3 mgrid((unsigned)b->max_chunks, (unsigned)std::max(1, b->max_planes), (unsigned)b->plans.size());
     for (int k = 0; k < nsteps; ++k) {
@@ -2062,6 +2100,26 @@ int tfd_batch_set_launch(tfd_batch *b, int32_t ctas, int32_t strip_rows, void *s
         if (rc) return rc;
     }
     b->ctas = ctas;
+    if (b->persist_ctas > 0) {                   // keep a persistent launch sized for the new table
+        int n = 0;
+        const int rc = b->precision == 8 ? batch_persist_ctas<double>(b, n) : batch_persist_ctas<float>(b, n);
+        if (rc) return rc;
+        b->persist_ctas = n;
+    }
+    return TFD_OK;
+}
+
+int tfd_batch_set_persistent(tfd_batch *b, int32_t persistent, void *stream) {
+    (void)stream;
+    if (!b) return fail(TFD_ERR_INVALID, "null batch");
+    if (!persistent) {
+        b->persist_ctas = 0;
+        return TFD_OK;
+    }
+    int ctas = 0;
+    const int rc = b->precision == 8 ? batch_persist_ctas<double>(b, ctas) : batch_persist_ctas<float>(b, ctas);
+    if (rc) return rc;
+    b->persist_ctas = ctas;
     return TFD_OK;
 }
 

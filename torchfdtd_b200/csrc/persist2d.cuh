@@ -102,4 +102,51 @@ __global__ void __launch_bounds__(k2dThreads, 2) k_step2d_persistent(const Grid<
     if (blockIdx.x == 0 && threadIdx.x == 0) *m.counter = n;
 }
 
+// `count` steps of a batch of 2D TMz plans of any sizes in one cooperative launch: the batch's strip table
+// (interior strips of every member first) walked by all warps each step, a member whose run has ended skipped
+// (its state stays that of its last step), the observations of every member for step n - 1 taken while step n
+// computes (plan = work item / (mgx * mgy)), a bounded grid barrier between steps, and the batch's shared step
+// counter written once at the end. Per strip the arithmetic is the per-step kernels' (strip_interior /
+// strip_general), so the fields are bitwise the same as with one launch per step.
+template <typename T>
+__global__ void __launch_bounds__(k2dThreads, 2) k_step2d_batch_persistent(const Grid<T> *__restrict__ grids,
+                                                                          const Tile2D *__restrict__ strips, int interior, int all,
+                                                                          const MonitorArgs<T> *__restrict__ mons, int plans, int mgx,
+                                                                          int mgy, long long *counter, int count, unsigned *bar,
+                                                                          int *status) {
+    const long long n0 = *counter;
+    const int lane = threadIdx.x & 31;
+    const int warps_total = gridDim.x * k2dWarps;
+    const int w0 = blockIdx.x * k2dWarps + (threadIdx.x >> 5);
+    const int items = plans * mgx * mgy;
+    auto observe = [&](long long step) {
+        for (int b = blockIdx.x; b < items; b += gridDim.x) {
+            const int q = b / (mgx * mgy), r = b % (mgx * mgy);
+            monitor_work(mons[q], r % mgx, r / mgx, step, mgx);
+        }
+    };
+    long long n = n0;
+    for (int k = 0; k < count; ++k, ++n) {
+        const int par = (int)(n & 1);
+        if (k > 0) observe(n - 1);
+        for (int s = w0; s < all; s += warps_total) {
+            const Tile2D st = strips[s];
+            const Grid<T> &g = grids[st.grid];
+            if (n >= g.steps) continue;                // this member has finished its run (warp-uniform)
+            if (s < interior) {
+                if (st.kind != 1 || st.x0 < 1 || st.x0 + 31 > g.n[0] - 1 || st.y0 < 1 || st.y1 > g.n[1] - 1 || st.y1 < st.y0) {
+                    if (lane == 0) atomicExch(g.status, kStatusBadStrip);
+                    continue;
+                }
+                strip_interior(g, st, par, lane);
+            } else {
+                strip_general(g, st, n, par, lane);
+            }
+        }
+        if (!grid_barrier(bar, status)) return;
+    }
+    if (n > n0) observe(n - 1);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *counter = n;
+}
+
 }  // namespace tfd

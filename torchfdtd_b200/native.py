@@ -99,6 +99,7 @@ SIGNATURES = {
     'tfd_batch_bytes': (ctypes.c_int, [c_i32, ctypes.POINTER(c_vp), ctypes.POINTER(ctypes.c_size_t)]),
     'tfd_batch_create': (ctypes.c_int, [c_i32, ctypes.POINTER(c_vp), c_vp, ctypes.c_size_t, c_vp, ctypes.POINTER(c_vp)]),
     'tfd_batch_set_launch': (ctypes.c_int, [c_vp, c_i32, c_i32, c_vp]),
+    'tfd_batch_set_persistent': (ctypes.c_int, [c_vp, c_i32, c_vp]),
     'tfd_batch_step': (ctypes.c_int, [c_vp, c_i32, c_vp]),
     'tfd_batch_tiles': (ctypes.c_int, [c_vp, P_i32]),
     'tfd_batch_destroy': (None, [c_vp]),
@@ -582,6 +583,11 @@ class NativeBatch:
     def set_launch(self, ctas=0, rows=0, stream=None):
         """Persistent CTA count (0: one warp per strip) and rows per strip (0: default) of the step kernel."""
         check(library().tfd_batch_set_launch(self.handle, int(ctas), int(rows), _stream(stream)))
+
+    def set_persistent(self, on=True, stream=None):
+        """All steps of a ``step`` call in one cooperative launch (True) or one launch per step (False)."""
+        check(library().tfd_batch_set_persistent(self.handle, int(bool(on)), _stream(stream)))
+        self.persistent = bool(on)
 
     def tiles(self):
         v = c_i32()

@@ -157,9 +157,11 @@ def _plan_sha(plan):
 
 
 def batch_candidates(sms):
-    """Launch shapes worth measuring, as (persistent CTA count, rows per strip) pairs: one warp per strip
-    (ctas 0) at 8-64 rows, and persistent grids of 4 or 8 CTAs per SM at the default rows (0)."""
-    return [(0, 8), (0, 16), (0, 32), (0, 64), (0, 0), (4 * sms, 0), (8 * sms, 0)]
+    """Launch shapes worth measuring, as (CTA count, rows per strip, persistent) triples: one launch per step with
+    one warp per strip (ctas 0) at 8-64 rows or with 4 or 8 CTAs per SM at the default rows (0); and all steps in
+    one cooperative launch (persistent 1) at 16-64 rows."""
+    return [(0, 8, 0), (0, 16, 0), (0, 32, 0), (0, 64, 0), (0, 0, 0), (4 * sms, 0, 0), (8 * sms, 0, 0),
+            (0, 16, 1), (0, 32, 1), (0, 64, 1)]
 
 
 def tune_tensor_batch(cases, candidates=None, *, steps=8, repeats=5, device=0, epsilon=None):
@@ -167,8 +169,8 @@ def tune_tensor_batch(cases, candidates=None, *, steps=8, repeats=5, device=0, e
     2D TMz projects.
 
     Each candidate runs on its own scratch copy of the cohort (same plans, zero state); all candidates must
-    end with bitwise identical fields. Returns a ``LaunchTuning`` whose ``choice`` is the ``[ctas, rows]``
-    pair to pass as ``run_tensor_batch(..., launch=choice)``."""
+    end with bitwise identical fields. Returns a ``LaunchTuning`` whose ``choice`` is the ``[ctas, rows,
+    persistent]`` triple to pass as ``run_tensor_batch(..., launch=choice)``."""
     import torch
     from .batch import _admit, as_cases
     from .native import NativeBatch, NativeGrid
@@ -183,7 +185,7 @@ def tune_tensor_batch(cases, candidates=None, *, steps=8, repeats=5, device=0, e
     plans = [Simulation(p, epsilon=e).plan for p, e in zip(projects, epsilon or [None] * len(projects))]
     dev = torch.device('cuda', device)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
-    candidates = [tuple(int(v) for v in c) for c in dict.fromkeys(tuple(c) for c in (candidates or batch_candidates(sms)))]
+    candidates = [tuple(int(v) for v in (*c, 0)[:3]) for c in dict.fromkeys(tuple(c) for c in (candidates or batch_candidates(sms)))]
     key = ('batch', torch.cuda.get_device_name(dev), tuple(tuple(p.shape) for p in plans), str(plans[0].dtype),
            tuple(candidates), steps, repeats)
     if key in _CACHE:
@@ -199,7 +201,8 @@ def tune_tensor_batch(cases, candidates=None, *, steps=8, repeats=5, device=0, e
         def scratch(c):
             grids = [NativeGrid(plan, kernel='tile2d') for plan in plans]
             b = NativeBatch(grids)
-            b.set_launch(*c, stream=stream)
+            b.set_launch(c[0], c[1], stream=stream)
+            b.set_persistent(bool(c[2]), stream=stream)
             strips[c] = b.tiles()
             return grids, b
 
@@ -222,11 +225,12 @@ def tune_tensor_batch(cases, candidates=None, *, steps=8, repeats=5, device=0, e
                     finish(c, grids, b)
     if len(set(digests.values())) != 1:
         raise ArithmeticError('Launch shapes changed the physical fields; refusing to tune.')
-    records = [dict(ctas=c[0], rows=c[1], strips=strips[c], status='completed', samples_ms_per_step=v,
+    records = [dict(ctas=c[0], rows=c[1], persistent=c[2], strips=strips[c], status='completed', samples_ms_per_step=v,
                     median_ms_per_step=statistics.median(v)) for c, v in samples.items()]
-    winner = min(records, key=lambda r: (r['median_ms_per_step'], r['ctas'], r['rows']))
+    winner = min(records, key=lambda r: (r['median_ms_per_step'], -r['persistent'], r['ctas'], r['rows']))
     fingerprint = hashlib.sha256(json.dumps([p.model_dump() for p in projects], sort_keys=True, default=str).encode()).hexdigest()
-    tuning = LaunchTuning('batch', [winner['ctas'], winner['rows']], winner['median_ms_per_step'], records, repeats, steps,
+    tuning = LaunchTuning('batch', [winner['ctas'], winner['rows'], winner['persistent']], winner['median_ms_per_step'], records,
+                          repeats, steps,
                           time.perf_counter() - started, fingerprint, _hardware(dev))
     _CACHE[key] = tuning.as_dict()
     return tuning
