@@ -475,6 +475,15 @@ class Simulation:
 
         plan, permittivity = self._run_plan()
         lap('plan')
+        helper, host_fields = None, None
+        shape, dtype = (*plan.shape, 3), np.dtype(plan.dtype)
+        if math.prod(shape) * dtype.itemsize > LARGE_FIELD_BYTES:
+            # The result's host arrays are mapped on a helper thread (host memory only, no CUDA call, so it may
+            # overlap the plan creation, the uploads and the graph capture) while the main thread works on.
+            from concurrent.futures import ThreadPoolExecutor
+            from .native import host_buffer
+            helper = ThreadPoolExecutor(max_workers=1)
+            host_fields = helper.submit(lambda: (host_buffer(shape, dtype), host_buffer(shape, dtype)))
         variant, tuning = 0, None
         if launch == 'auto':
             if plan.dimension == '3d' and kernel in ('auto', 'march'):
@@ -488,11 +497,20 @@ class Simulation:
             variant = int(launch)
         if tuning is not None:
             lap('launch_tuning')
-        grid = NativeGrid(plan, kernel=kernel, variant=variant, permittivity=permittivity)
+        try:
+            grid = NativeGrid(plan, kernel=kernel, variant=variant, permittivity=permittivity)
+        except BaseException:
+            if helper is not None:
+                helper.shutdown(wait=True)
+            raise
         phases.update(grid.timing)
         mark[0] = time.perf_counter()
         free, _ = torch.cuda.mem_get_info()
         observer = Observer(p, plan, grid)
+        observer.host_fields = host_fields
+        if host_fields is not None:
+            from .native import staging_ring
+            staging_ring(grid.torch_dtype)          # pinned once per process, before any capture
         graphs = {}
         width = 1
         stream = torch.cuda.Stream()
@@ -507,16 +525,6 @@ class Simulation:
             torch.cuda.synchronize()
         torch.cuda.synchronize()
         lap('observer_and_graph_capture')
-        helper = None
-        if observer.large_fields():
-            # The result's host arrays are mapped and the download's staging ring pinned on a helper thread
-            # while the device steps (after graph capture: pinning memory during a capture would end it).
-            from concurrent.futures import ThreadPoolExecutor
-            from .native import host_buffer, staging_ring
-            helper = ThreadPoolExecutor(max_workers=1)
-            shape, dtype = (*plan.shape, 3), np.dtype(plan.dtype)
-            observer.host_fields = helper.submit(
-                lambda: (staging_ring(grid.torch_dtype), (host_buffer(shape, dtype), host_buffer(shape, dtype)))[1])
         setup_seconds = time.perf_counter() - started
         compute_start = time.perf_counter()
         completed, termination_reason, replays = 0, 'max_steps', 0
