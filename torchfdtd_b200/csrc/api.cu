@@ -473,8 +473,10 @@ struct tfd_plan {
     MarchArgs<double> md;
     dim3 march_grid;
     size_t march_smem = 0;
-    struct MarchLaunch { int mode; dim3 grid; int tx_off, ty_off, lz, z_lo, z_hi; };   // mode 3: the mixed kernel
+    struct MarchLaunch { int mode; dim3 grid; int tx_off, ty_off, lz, z_lo, z_hi; };   // mode 3: the mixed kernel, 5: the ring
     MarchMix march_mix{};
+    MarchRing march_ring{};
+    bool march_sequential = false; // every march launch of a step on the caller's stream, in order
     std::vector<MarchLaunch> march_launches;
     bool march_metric = false;     // nonuniform mesh: the general body with metric factors
     TfsfArgs<float> tf{};          // TFSF boxes (the step runs the split gather kernels when there are any)
@@ -917,11 +919,15 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
     TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
     TFD_CUDA(cudaFuncSetAttribute(k_step_march_mixed<T, SAMPLES, D, MINB, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)p->march_smem));
+    TFD_CUDA(cudaFuncSetAttribute(k_step_march_ring<T, SAMPLES, D, MINB, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)p->march_smem));
     if constexpr (D * 10 + MINB == periodic_march_variant<T>()) {
         TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
         TFD_CUDA(cudaFuncSetAttribute(k_step_march_mixed<T, SAMPLES, D, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)p->march_smem));
         TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)p->march_smem));
+        TFD_CUDA(cudaFuncSetAttribute(k_step_march_ring<T, SAMPLES, D, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)p->march_smem));
         TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)p->march_smem));
@@ -1003,7 +1009,40 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
             z = e;
         }
     }
-    if (split_interior && ix1 > ix0 && iy1 > iy0 && zb - za >= 2) {
+    p->march_sequential = false;
+    if (split == 4 && ix1 > ix0 && iy1 > iy0 && zb - za >= 2) {
+        // The boundary tiles first (general body, one launch over the ring of tiles), then the interior block
+        // (pure and z-pure bodies), both on the caller's stream: no SM holds both kinds of CTA at once.
+        MarchRing &rg = p->march_ring;
+        rg = MarchRing{};
+        const int rects[4][4] = {{0, 0, ix0, ty}, {ix1, 0, tx - ix1, ty}, {ix0, 0, ix1 - ix0, iy0}, {ix0, iy1, ix1 - ix0, ty - iy1}};
+        int count = 0;
+        for (const auto &q : rects) {
+            if (q[2] <= 0 || q[3] <= 0) continue;
+            for (int j = 0; j < 4; ++j) rg.rect[rg.n_rect][j] = q[j];
+            rg.start[rg.n_rect++] = count;
+            count += q[2] * q[3];
+        }
+        rg.start[rg.n_rect] = count;
+        rg.nz = nzp;
+        rg.lz = choose_lz(count, nzp, (double)count / ((double)tx * ty));
+        p->march_launches.push_back({5, dim3(count, 1, chunks_of(rg.lz, nzp)), 0, 0, rg.lz, 0, nzp});
+        MarchMix &mx = p->march_mix;
+        mx = MarchMix{};
+        mx.ix0 = ix0; mx.ix1 = ix1; mx.iy0 = iy0; mx.iy1 = iy1;
+        mx.tx_off = ix0; mx.ty_off = iy0;
+        mx.zb[0] = 0; mx.zb[1] = za; mx.zb[2] = zb; mx.zb[3] = nzp;
+        const long long inner = (long long)(ix1 - ix0) * (iy1 - iy0);
+        int total = 0;
+        for (int q = 0; q < 3; ++q) {
+            const int planes = mx.zb[q + 1] - mx.zb[q];
+            mx.lz[q] = planes > 0 ? choose_lz(inner, planes, (double)inner * planes / tile_planes) : 1;
+            mx.chunks[q] = planes > 0 ? (int)chunks_of(mx.lz[q], planes) : 0;
+            total += mx.chunks[q];
+        }
+        p->march_launches.push_back({3, dim3(ix1 - ix0, iy1 - iy0, total), 0, 0, 0, 0, nzp});
+        p->march_sequential = true;
+    } else if (split_interior && ix1 > ix0 && iy1 > iy0 && zb - za >= 2) {
         // The pure fast kernel over the interior block; the general kernel over its z-slab planes and
         // over the boundary strips (all planes). Concurrent launches on forked streams.
         // Measured on B200 this split is slower than one general launch (512x512x256: 1.16 vs 1.02 ms per
@@ -1035,7 +1074,7 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
     } else {
         push(edge_mode, tx, ty, 0, 0, 0, nzp);
     }
-    if (p->aux.empty() && p->march_launches.size() > 1) {
+    if (p->aux.empty() && p->march_launches.size() > 1 && !p->march_sequential) {
         TFD_CUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
         for (size_t k = 1; k < p->march_launches.size(); ++k) {
             cudaStream_t st;
@@ -1053,6 +1092,7 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
 // Launch variant of the marching kernel, as decimal digits: lz * 1000 + split * 100 + D * 10 + MINB.
 // D / MINB: prefetch depth and CTAs per SM, one of 14 (FP32 default), 23, 32, 22 (FP64: 22 only);
 // split 1: the interior block and the boundary as separate concurrent launches; 2: the general kernel only;
+// 4: the boundary tiles (one launch over the ring of tiles) and then the interior block, both on the caller's stream;
 // 3: one launch, the pure body on the interior block's planes outside the z slabs (k_step_march_mixed), when
 // the grid has such a block (else the general kernel); 0: 3. lz: z-planes per CTA chunk (0: about 12, shorter
 // on small grids).
@@ -1065,7 +1105,7 @@ int setup_march(tfd_plan *p) {
     if (v == 0) v = env ? std::atoi(env) : 0;
     if (v == 0) v = sizeof(T) == 4 ? 14 : 22;
     const int dm = v % 100, split = (v / 100) % 10, lz = v / 1000;
-    if (v < 0 || split > 3 || (dm != 14 && dm != 22 && dm != 23 && dm != 32) || (sizeof(T) == 8 && dm != 22))
+    if (v < 0 || split > 4 || (dm != 14 && dm != 22 && dm != 23 && dm != 32) || (sizeof(T) == 8 && dm != 22))
         return fail(TFD_ERR_INVALID, "launch variant " + std::to_string(v) + " is not lz*1000 + split*100 + one of " +
                                          (sizeof(T) == 8 ? std::string("22 (FP64)") : std::string("14, 22, 23, 32")));
     const bool three = p->desc.material_samples == 3;
@@ -1087,12 +1127,20 @@ int setup_march(tfd_plan *p) {
 template <typename T, int SAMPLES, int D, int MINB>
 void launch_march(tfd_plan *p, cudaStream_t s) {
     const size_t n = p->march_launches.size();
-    if (n > 1) cudaEventRecord(p->fork, s);
+    const bool fork = n > 1 && !p->march_sequential;
+    if (fork) cudaEventRecord(p->fork, s);
     for (size_t k = 0; k < n; ++k) {
         const auto &l = p->march_launches[k];
-        cudaStream_t st = k == 0 ? s : p->aux[k - 1];
-        if (k > 0) cudaStreamWaitEvent(st, p->fork, 0);
-        if (l.mode == 3) {
+        cudaStream_t st = (k == 0 || !fork) ? s : p->aux[k - 1];
+        if (k > 0 && fork) cudaStreamWaitEvent(st, p->fork, 0);
+        if (l.mode == 5) {
+            if (p->grid<T>().periodic[0] || p->grid<T>().periodic[1]) {
+                if constexpr (D * 10 + MINB == periodic_march_variant<T>())
+                    k_step_march_ring<T, SAMPLES, D, MINB, 2><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), p->march_ring);
+            } else {
+                k_step_march_ring<T, SAMPLES, D, MINB, 0><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), p->march_ring);
+            }
+        } else if (l.mode == 3) {
             if (p->grid<T>().periodic[0] || p->grid<T>().periodic[1]) {
                 if constexpr (D * 10 + MINB == periodic_march_variant<T>())
                     k_step_march_mixed<T, SAMPLES, D, MINB, 2><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), p->march_mix);
@@ -1118,9 +1166,10 @@ void launch_march(tfd_plan *p, cudaStream_t s) {
         } else
             k_step_march<T, SAMPLES, D, MINB, 0><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz,
                                                                                              l.z_lo, l.z_hi);
-        if (k > 0) cudaEventRecord(p->join[k - 1], st);
+        if (k > 0 && fork) cudaEventRecord(p->join[k - 1], st);
     }
-    for (size_t k = 1; k < n; ++k) cudaStreamWaitEvent(s, p->join[k - 1], 0);
+    if (fork)
+        for (size_t k = 1; k < n; ++k) cudaStreamWaitEvent(s, p->join[k - 1], 0);
 }
 
 template <typename T>
