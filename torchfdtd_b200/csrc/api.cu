@@ -14,6 +14,7 @@
 #include "step_march.cuh"
 #include "step2d.cuh"
 #include "adjoint.cuh"
+#include "adjoint_march.cuh"
 #include "tfsf.cuh"
 #include <cudaTypedefs.h>
 
@@ -2284,6 +2285,7 @@ struct tfd_adjoint {
     char *arena = nullptr;
     size_t used = 0;
     int q = 0;
+    int march_lz = 0;              // > 0: the marching reverse step with chunks of this many planes
     AdjArgs<float> af;
     AdjArgs<double> ad;
     template <typename T> AdjArgs<T> &args();
@@ -2335,6 +2337,25 @@ int adjoint_create_t(tfd_adjoint *adj, cudaStream_t s) {
     adj->used = adjoint_layout<T>(p, &A, adj->arena);
     TFD_CUDA(cudaMemsetAsync(adj->arena, 0, adj->used, s));
     adj->q = 0;
+    // The marching reverse step serves 3D grids with all components and no periodic face (TFD_ADJOINT_KERNEL=gather
+    // in the environment keeps the gather pair, for comparisons).
+    adj->march_lz = 0;
+    const char *env = getenv("TFD_ADJOINT_KERNEL");
+    const bool gather = env && std::string(env) == "gather";
+    const Grid<T> &g = A.g;
+    if (!gather && p->desc.components == kMaskAll && g.n[0] >= 2 && g.n[1] >= 2 && g.n[2] >= 2 && !g.periodic[0] && !g.periodic[1] &&
+        !g.periodic[2]) {
+        int device = 0, sms = 148, per_sm = 0;
+        TFD_CUDA(cudaGetDevice(&device));
+        TFD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        TFD_CUDA(cudaFuncSetAttribute(k_adjoint_march<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdjMarchSmem<T>)));
+        TFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint_march<T>, kAmThreads, sizeof(AdjMarchSmem<T>)));
+        // Chunks of about 16 planes, shorter (down to 4) until the launch has two waves of CTAs.
+        const long long tiles = (long long)((g.n[0] + kAmX - 1) / kAmX) * ((g.n[1] + kAmY - 1) / kAmY);
+        int chunks = (g.n[2] + 15) / 16;
+        while (tiles * chunks < 2LL * sms * std::max(1, per_sm) && (g.n[2] + chunks) / (chunks + 1) >= 4) ++chunks;
+        adj->march_lz = (g.n[2] + chunks - 1) / chunks;
+    }
     return TFD_OK;
 }
 
@@ -2350,6 +2371,14 @@ int adjoint_step_t(tfd_adjoint *adj, const void *snapshot, const void *seeds, cu
     const dim3 grid((unsigned)((g.n[0] + kAdjX - 1) / kAdjX), (unsigned)((g.n[1] + kAdjY - 1) / kAdjY), (unsigned)g.n[2]);
     const dim3 block(kAdjX, kAdjY);
     const T *slot = (const T *)snapshot;
+    if (adj->march_lz > 0) {
+        const dim3 mgrid((unsigned)((g.n[0] + kAmX - 1) / kAmX), (unsigned)((g.n[1] + kAmY - 1) / kAmY),
+                         (unsigned)((g.n[2] + adj->march_lz - 1) / adj->march_lz));
+        k_adjoint_march<T><<<mgrid, kAmThreads, sizeof(AdjMarchSmem<T>), s>>>(A, slot, adj->q, adj->march_lz);
+        TFD_CUDA(cudaGetLastError());
+        adj->q ^= 1;
+        return TFD_OK;
+    }
     switch (p->desc.components) {
         case kMaskTM:
             k_adjoint_e<T, kMaskTM><<<grid, block, 0, s>>>(A, slot, adj->q);
