@@ -144,45 +144,3 @@ def test_plane_fields_match_the_forward_simulation_planes():
     fields = model(torch.tensor(eps, device='cuda'))['out'].fields.detach().cpu().numpy()
     plane = Simulation(project, epsilon=eps).run().field_monitor('out')
     assert rel(fields, plane['fields']) <= 1e-12
-
-
-def graded_adjoint_project(precision):
-    from torchfdtd_b200.models import BoundaryFace, MeshRefinement, Monitor, Source
-    region = Region(dimension='3d', size=(6.0, 3.0, 1.5), mesh=.1, pml_cells=3, steps=24, precision=precision, backend='cuda',
-                    mesh_type='graded', mesh_max=.22, mesh_grading=1.4, mesh_ppw=6, material_sampling='yee',
-                    mesh_refinements=[MeshRefinement(center=(.2, .1, 0), size=(.3, .3, .3))])
-    region.boundaries.x_min = BoundaryFace(layers=4, kappa=2, alpha=.04, alpha_polynomial=1)
-    region.boundaries.z_max = BoundaryFace(kind='pec')
-    return Project(region=region, sources=[Source(center=(-.4, .05, 0), component='Ez', pulse_cycles=1, wavelength=1.6)],
-                   monitors=[Monitor(center=(.5, .1, 0), component='Ez'), Monitor(center=(.3, -.1, .1), component='Hy')])
-
-
-@pytest.mark.parametrize('name', ['3d_float32', '3d_float64', 'graded_float32', 'graded_float64'])
-def test_marching_reverse_step_equals_the_gather_pair_bitwise(golden, name, monkeypatch):
-    """The marching reverse step (one launch, each transposed D value once per cell) against the gather pair:
-    the golden 3D scenes (kappa > 1 CPML, a PEC face) and a graded 3D mesh (metric factors, partial tiles)."""
-    import torch
-    from torchfdtd_b200.adjoint import DifferentiableSimulation
-    grads = {}
-    for kernel in ('gather', 'march'):
-        if kernel == 'gather':
-            monkeypatch.setenv('TFD_ADJOINT_KERNEL', 'gather')
-        else:
-            monkeypatch.delenv('TFD_ADJOINT_KERNEL', raising=False)
-        if name.startswith('graded'):
-            project = graded_adjoint_project(name.split('_')[1])
-            shape = tuple(project.region.shape) + (3,)
-            eps = np.random.default_rng(4).uniform(1, 3, size=shape)
-            weights = np.random.default_rng(5).normal(size=(project.region.steps, 2))
-        else:
-            d = np.load(golden / f'adjoint_{name}.npz')
-            project, eps, weights = cuda_project(d), d['epsilon'], d['weights']
-        dtype = torch.float32 if project.region.precision == 'float32' else torch.float64
-        model = DifferentiableSimulation(project)
-        epsilon = torch.tensor(eps, dtype=dtype, device='cuda', requires_grad=True)
-        (model(epsilon).signals * torch.tensor(weights, dtype=dtype, device='cuda')).sum().backward()
-        grads[kernel] = epsilon.grad.cpu().numpy()
-        model.close()
-    assert np.abs(grads['march']).max() > 0
-    np.testing.assert_array_equal(grads['march'], grads['gather'])
-

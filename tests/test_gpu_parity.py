@@ -509,3 +509,43 @@ def test_simulation_device_material_and_checks_equal_host_path(monkeypatch):
     np.testing.assert_array_equal(got.magnetic, want.magnetic)
     np.testing.assert_array_equal(got.signals, want.signals)
     assert got.summary['field_peak'] == want.summary['field_peak']
+
+
+@pytest.mark.parametrize('precision', ['float32', 'float64'])
+@pytest.mark.parametrize('mesh', ['uniform', 'graded'])
+def test_on_chip_cluster_2d_path_equals_the_strip_launches(monkeypatch, precision, mesh):
+    """Small 2D TMz plans without planes run every step of a call in one thread-block cluster (fields in
+    distributed shared memory): bitwise equal to the persistent strip launch and to the per-step launches, with
+    E and H sources, a PEC face, CPML and (graded) metric factors; traces included."""
+    from torchfdtd_b200 import Project, Region, Source, Monitor, Structure
+    from torchfdtd_b200.models import BoundaryFace
+    extra = dict(mesh_type='graded', mesh_max=.12, mesh_ppw=6, material_sampling='yee') if mesh == 'graded' else {}
+    region = Region(dimension='2d', size=(4.8, 3.2, 1), mesh=.04, pml_cells=10, steps=180, precision=precision, backend='cuda', **extra)
+    region.boundaries.y_max = BoundaryFace(kind='pec')
+    project = Project(region=region, structures=[Structure(kind='circle', center=(.4, .2, 0), radius=.3, material='Si (constant n)')],
+                      sources=[Source(center=(-.8, 0, 0), component='Ez', pulse_cycles=2, wavelength=1.6),
+                               Source(center=(-.3, .3, 0), component='Hx', pulse_cycles=2, wavelength=1.6, amplitude=.4)],
+                      monitors=[Monitor(center=(.9, .1, 0), component='Ez'), Monitor(center=(.2, -.4, 0), component='Hy')])
+    out = {}
+    for mode, env in (('cluster', {}), ('persistent', {'TFD_CLUSTER2D': '0'}), ('per_step', {'TFD_CLUSTER2D': '0', 'TFD_PERSIST2D': '0'})):
+        for k in ('TFD_CLUSTER2D', 'TFD_PERSIST2D'):
+            monkeypatch.delenv(k, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        plan = plan_grid(project)
+        g = native(plan, 'tile2d')
+        g.step(70)
+        g.step(110)
+        out[mode] = (*g.get_fields(), g.get_traces(), g.get_psi(), g.counter())
+        g.close()
+    oracle = YeeOracle(plan_grid(project)).run()
+    for mode in ('persistent', 'per_step'):
+        for a, b in zip(out['cluster'][:3], out[mode][:3]):
+            np.testing.assert_array_equal(a, b)
+        for a, b in zip(out['cluster'][3], out[mode][3]):
+            np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(out['cluster'][0], oracle.E)
+    np.testing.assert_array_equal(out['cluster'][1], oracle.H)
+    np.testing.assert_array_equal(out['cluster'][2], oracle.traces)
+    assert out['cluster'][4] == 180 and np.abs(out['cluster'][0]).max() > 0
+

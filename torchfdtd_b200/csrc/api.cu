@@ -14,7 +14,7 @@
 #include "step_march.cuh"
 #include "step2d.cuh"
 #include "adjoint.cuh"
-#include "adjoint_march.cuh"
+#include "cluster2d.cuh"
 #include "tfsf.cuh"
 #include <cudaTypedefs.h>
 
@@ -474,10 +474,8 @@ struct tfd_plan {
     MarchArgs<double> md;
     dim3 march_grid;
     size_t march_smem = 0;
-    struct MarchLaunch { int mode; dim3 grid; int tx_off, ty_off, lz, z_lo, z_hi; };   // mode 3: the mixed kernel, 5: the ring
+    struct MarchLaunch { int mode; dim3 grid; int tx_off, ty_off, lz, z_lo, z_hi; };   // mode 3: the mixed kernel
     MarchMix march_mix{};
-    MarchRing march_ring{};
-    bool march_sequential = false; // every march launch of a step on the caller's stream, in order
     std::vector<MarchLaunch> march_launches;
     bool march_metric = false;     // nonuniform mesh: the general body with metric factors
     TfsfArgs<float> tf{};          // TFSF boxes (the step runs the split gather kernels when there are any)
@@ -500,6 +498,8 @@ struct tfd_plan {
     int march_variant = 42;
     int tile2d_interior = 0;
     int persist_ctas = 0;          // > 0: 2D steps run as one persistent cooperative launch of this many CTAs
+    Cluster2D cluster2d{};         // ranks > 0: 2D steps run on chip in one thread-block cluster
+    size_t cluster2d_smem = 0;
     std::unique_ptr<SideStream> side2d;
     bool in_batch = false;
     long long *own_counter = nullptr;
@@ -920,15 +920,11 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
     TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
     TFD_CUDA(cudaFuncSetAttribute(k_step_march_mixed<T, SAMPLES, D, MINB, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)p->march_smem));
-    TFD_CUDA(cudaFuncSetAttribute(k_step_march_ring<T, SAMPLES, D, MINB, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)p->march_smem));
     if constexpr (D * 10 + MINB == periodic_march_variant<T>()) {
         TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->march_smem));
         TFD_CUDA(cudaFuncSetAttribute(k_step_march_mixed<T, SAMPLES, D, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)p->march_smem));
         TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)p->march_smem));
-        TFD_CUDA(cudaFuncSetAttribute(k_step_march_ring<T, SAMPLES, D, MINB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)p->march_smem));
         TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)p->march_smem));
@@ -1010,40 +1006,7 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
             z = e;
         }
     }
-    p->march_sequential = false;
-    if (split == 4 && ix1 > ix0 && iy1 > iy0 && zb - za >= 2) {
-        // The boundary tiles first (general body, one launch over the ring of tiles), then the interior block
-        // (pure and z-pure bodies), both on the caller's stream: no SM holds both kinds of CTA at once.
-        MarchRing &rg = p->march_ring;
-        rg = MarchRing{};
-        const int rects[4][4] = {{0, 0, ix0, ty}, {ix1, 0, tx - ix1, ty}, {ix0, 0, ix1 - ix0, iy0}, {ix0, iy1, ix1 - ix0, ty - iy1}};
-        int count = 0;
-        for (const auto &q : rects) {
-            if (q[2] <= 0 || q[3] <= 0) continue;
-            for (int j = 0; j < 4; ++j) rg.rect[rg.n_rect][j] = q[j];
-            rg.start[rg.n_rect++] = count;
-            count += q[2] * q[3];
-        }
-        rg.start[rg.n_rect] = count;
-        rg.nz = nzp;
-        rg.lz = choose_lz(count, nzp, (double)count / ((double)tx * ty));
-        p->march_launches.push_back({5, dim3(count, 1, chunks_of(rg.lz, nzp)), 0, 0, rg.lz, 0, nzp});
-        MarchMix &mx = p->march_mix;
-        mx = MarchMix{};
-        mx.ix0 = ix0; mx.ix1 = ix1; mx.iy0 = iy0; mx.iy1 = iy1;
-        mx.tx_off = ix0; mx.ty_off = iy0;
-        mx.zb[0] = 0; mx.zb[1] = za; mx.zb[2] = zb; mx.zb[3] = nzp;
-        const long long inner = (long long)(ix1 - ix0) * (iy1 - iy0);
-        int total = 0;
-        for (int q = 0; q < 3; ++q) {
-            const int planes = mx.zb[q + 1] - mx.zb[q];
-            mx.lz[q] = planes > 0 ? choose_lz(inner, planes, (double)inner * planes / tile_planes) : 1;
-            mx.chunks[q] = planes > 0 ? (int)chunks_of(mx.lz[q], planes) : 0;
-            total += mx.chunks[q];
-        }
-        p->march_launches.push_back({3, dim3(ix1 - ix0, iy1 - iy0, total), 0, 0, 0, 0, nzp});
-        p->march_sequential = true;
-    } else if (split_interior && ix1 > ix0 && iy1 > iy0 && zb - za >= 2) {
+    if (split_interior && ix1 > ix0 && iy1 > iy0 && zb - za >= 2) {
         // The pure fast kernel over the interior block; the general kernel over its z-slab planes and
         // over the boundary strips (all planes). Concurrent launches on forked streams.
         // Measured on B200 this split is slower than one general launch (512x512x256: 1.16 vs 1.02 ms per
@@ -1075,7 +1038,7 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
     } else {
         push(edge_mode, tx, ty, 0, 0, 0, nzp);
     }
-    if (p->aux.empty() && p->march_launches.size() > 1 && !p->march_sequential) {
+    if (p->aux.empty() && p->march_launches.size() > 1) {
         TFD_CUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
         for (size_t k = 1; k < p->march_launches.size(); ++k) {
             cudaStream_t st;
@@ -1093,7 +1056,6 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
 // Launch variant of the marching kernel, as decimal digits: lz * 1000 + split * 100 + D * 10 + MINB.
 // D / MINB: prefetch depth and CTAs per SM, one of 14 (FP32 default), 23, 32, 22 (FP64: 22 only);
 // split 1: the interior block and the boundary as separate concurrent launches; 2: the general kernel only;
-// 4: the boundary tiles (one launch over the ring of tiles) and then the interior block, both on the caller's stream;
 // 3: one launch, the pure body on the interior block's planes outside the z slabs (k_step_march_mixed), when
 // the grid has such a block (else the general kernel); 0: 3. lz: z-planes per CTA chunk (0: about 12, shorter
 // on small grids).
@@ -1106,7 +1068,7 @@ int setup_march(tfd_plan *p) {
     if (v == 0) v = env ? std::atoi(env) : 0;
     if (v == 0) v = sizeof(T) == 4 ? 14 : 22;
     const int dm = v % 100, split = (v / 100) % 10, lz = v / 1000;
-    if (v < 0 || split > 4 || (dm != 14 && dm != 22 && dm != 23 && dm != 32) || (sizeof(T) == 8 && dm != 22))
+    if (v < 0 || split > 3 || (dm != 14 && dm != 22 && dm != 23 && dm != 32) || (sizeof(T) == 8 && dm != 22))
         return fail(TFD_ERR_INVALID, "launch variant " + std::to_string(v) + " is not lz*1000 + split*100 + one of " +
                                          (sizeof(T) == 8 ? std::string("22 (FP64)") : std::string("14, 22, 23, 32")));
     const bool three = p->desc.material_samples == 3;
@@ -1128,20 +1090,12 @@ int setup_march(tfd_plan *p) {
 template <typename T, int SAMPLES, int D, int MINB>
 void launch_march(tfd_plan *p, cudaStream_t s) {
     const size_t n = p->march_launches.size();
-    const bool fork = n > 1 && !p->march_sequential;
-    if (fork) cudaEventRecord(p->fork, s);
+    if (n > 1) cudaEventRecord(p->fork, s);
     for (size_t k = 0; k < n; ++k) {
         const auto &l = p->march_launches[k];
-        cudaStream_t st = (k == 0 || !fork) ? s : p->aux[k - 1];
-        if (k > 0 && fork) cudaStreamWaitEvent(st, p->fork, 0);
-        if (l.mode == 5) {
-            if (p->grid<T>().periodic[0] || p->grid<T>().periodic[1]) {
-                if constexpr (D * 10 + MINB == periodic_march_variant<T>())
-                    k_step_march_ring<T, SAMPLES, D, MINB, 2><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), p->march_ring);
-            } else {
-                k_step_march_ring<T, SAMPLES, D, MINB, 0><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), p->march_ring);
-            }
-        } else if (l.mode == 3) {
+        cudaStream_t st = k == 0 ? s : p->aux[k - 1];
+        if (k > 0) cudaStreamWaitEvent(st, p->fork, 0);
+        if (l.mode == 3) {
             if (p->grid<T>().periodic[0] || p->grid<T>().periodic[1]) {
                 if constexpr (D * 10 + MINB == periodic_march_variant<T>())
                     k_step_march_mixed<T, SAMPLES, D, MINB, 2><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), p->march_mix);
@@ -1167,10 +1121,9 @@ void launch_march(tfd_plan *p, cudaStream_t s) {
         } else
             k_step_march<T, SAMPLES, D, MINB, 0><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), l.tx_off, l.ty_off, l.lz,
                                                                                              l.z_lo, l.z_hi);
-        if (k > 0 && fork) cudaEventRecord(p->join[k - 1], st);
+        if (k > 0) cudaEventRecord(p->join[k - 1], st);
     }
-    if (fork)
-        for (size_t k = 1; k < n; ++k) cudaStreamWaitEvent(s, p->join[k - 1], 0);
+    for (size_t k = 1; k < n; ++k) cudaStreamWaitEvent(s, p->join[k - 1], 0);
 }
 
 template <typename T>
@@ -1209,6 +1162,9 @@ inline int ctas_2d(int strips, int ctas) {
 }
 
 template <typename T>
+int setup_cluster2d(tfd_plan *p);
+
+template <typename T>
 int setup_tile2d(tfd_plan *p, cudaStream_t s) {
     Grid<T> &g = p->grid<T>();
     std::vector<Tile2D> tiles = strips_of(strip_geom<T>(p), 0, p->L.strip_rows);
@@ -1232,7 +1188,7 @@ int setup_tile2d(tfd_plan *p, cudaStream_t s) {
         const int want = std::max({1, (p->L.tiles2d + k2dWarps - 1) / k2dWarps, mblocks});
         if (per_sm > 0) p->persist_ctas = std::min(want, per_sm * sms);
     }
-    return TFD_OK;
+    return setup_cluster2d<T>(p);
 }
 
 // One 2D step over a strip table whose first `interior` strips are interior strips. The general strips
@@ -1522,6 +1478,102 @@ int launch_step_gather(tfd_plan *p, cudaStream_t s) {
     return TFD_OK;
 }
 
+// The on-chip cluster path for small 2D TMz plans without DFT planes (TFD_CLUSTER2D=0 in the environment
+// turns it off, for comparisons): the smallest cluster of 8 or 16 CTAs whose per-rank bands fit in shared memory.
+template <typename T>
+int setup_cluster2d(tfd_plan *p) {
+    Cluster2D &c = p->cluster2d;
+    c = Cluster2D{};
+    p->cluster2d_smem = 0;
+    const char *env = getenv("TFD_CLUSTER2D");
+    if ((env && std::atoi(env) == 0) || p->desc.n_planes > 0 || p->desc.n_tfsf > 0 || p->desc.n_ade > 0) return TFD_OK;
+    const Grid<T> &g = p->grid<T>();
+    const int nx = g.n[0], ny = g.n[1];
+    int device = 0, max_smem = 0;
+    TFD_CUDA(cudaGetDevice(&device));
+    TFD_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    // y-slab memory rows of a band: rows y of the band with a slab row (E: y > 0, H: y < ny - 1), contiguous.
+    auto slab_rows = [&](int f, int lo, int hi, int &first, int &count) {
+        std::vector<std::pair<int, int>> segs;
+        for (size_t q = 0; q < p->seg_f.size(); ++q)
+            if (p->seg_f[q] == f && p->seg_a[q] == 1) segs.push_back({p->seg_lo[q], p->seg_hi[q]});
+        std::sort(segs.begin(), segs.end());
+        int base = 0;
+        first = -1;
+        count = 0;
+        for (auto &sg : segs) {
+            const int a = std::max(sg.first, lo), b = std::min(sg.second, hi);
+            if (a < b) {
+                if (first < 0) first = base + (a - sg.first);
+                count += b - a;
+            }
+            base += sg.second - sg.first;
+        }
+        if (first < 0) first = 0;
+    };
+    for (int ranks : {8, 16}) {
+        if (ranks > ny) break;
+        Cluster2D t{};
+        t.ranks = ranks;
+        t.w = nx;
+        t.rx_e = g.rows[0][0];
+        t.rx_h = g.rows[1][0];
+        for (int r = 0; r <= ranks; ++r) t.r0[r] = (int)((long long)r * ny / ranks);
+        for (int r = 0; r < ranks; ++r) {
+            t.rows_max = std::max(t.rows_max, t.r0[r + 1] - t.r0[r]);
+            slab_rows(0, t.r0[r], t.r0[r + 1], t.rye_lo[r], t.rye_n[r]);
+            slab_rows(1, t.r0[r], t.r0[r + 1], t.ryh_lo[r], t.ryh_n[r]);
+            t.rye_max = std::max(t.rye_max, t.rye_n[r]);
+            t.ryh_max = std::max(t.ryh_max, t.ryh_n[r]);
+        }
+        const size_t bytes = (size_t)cl2d_layout(t).total * sizeof(T);
+        if (bytes > (size_t)max_smem) continue;
+        TFD_CUDA(cudaFuncSetAttribute(k_step2d_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+        if (ranks > 8) TFD_CUDA(cudaFuncSetAttribute(k_step2d_cluster<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)ranks);
+        cfg.blockDim = dim3(kCl2dThreads);
+        cfg.dynamicSmemBytes = bytes;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)ranks;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, k_step2d_cluster<T>, &cfg) != cudaSuccess || clusters < 1) {
+            cudaGetLastError();
+            continue;
+        }
+        c = t;
+        p->cluster2d_smem = bytes;
+        break;
+    }
+    return TFD_OK;
+}
+
+template <typename T>
+int launch_cluster2d(tfd_plan *p, int nsteps, cudaStream_t s) {
+    Cluster2D c = p->cluster2d;
+    c.count = nsteps;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)c.ranks);
+    cfg.blockDim = dim3(kCl2dThreads);
+    cfg.dynamicSmemBytes = p->cluster2d_smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)c.ranks;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    TFD_CUDA(cudaLaunchKernelEx(&cfg, k_step2d_cluster<T>, p->grid<T>(), c, (const TraceDev *)(p->arena + p->L.trace_tab),
+                                p->desc.n_traces, p->ptr<T>(p->L.trace_out)));
+    return TFD_OK;
+}
+
 // One persistent launch of `nsteps` 2D steps with their observations (cooperative: every CTA resident).
 template <typename T>
 int launch_persist2d(tfd_plan *p, int nsteps, cudaStream_t s) {
@@ -1579,6 +1631,10 @@ int launch_split_step(tfd_plan *p, cudaStream_t s) {
 
 template <typename T>
 int step_t(tfd_plan *p, int nsteps, cudaStream_t s) {
+    if (p->kernel == TFD_KERNEL_TILE2D && p->cluster2d.ranks > 0 && !p->in_batch) {
+        if (nsteps > 0) TFD_CHECK(launch_cluster2d<T>(p, nsteps, s));
+        return TFD_OK;
+    }
     if (p->kernel == TFD_KERNEL_TILE2D && p->persist_ctas > 0 && !p->in_batch) {
         if (nsteps > 0) TFD_CHECK(launch_persist2d<T>(p, nsteps, s));
         return TFD_OK;
@@ -1921,7 +1977,7 @@ int tfd_step_launches(const tfd_plan *p, int32_t nsteps, int64_t *launches) {
     if (p->split) {
         per_step = p->desc.n_tfsf > 0 ? 5 : 3;                // split E, (TFSF E), split H, (TFSF H), observation
     } else if (p->kernel == TFD_KERNEL_TILE2D) {
-        if (p->persist_ctas > 0 && !p->in_batch) {
+        if ((p->persist_ctas > 0 || p->cluster2d.ranks > 0) && !p->in_batch) {
             *launches = nsteps > 0 ? 1 : 0;
             return TFD_OK;
         }
@@ -2285,7 +2341,6 @@ struct tfd_adjoint {
     char *arena = nullptr;
     size_t used = 0;
     int q = 0;
-    int march_lz = 0;              // > 0: the marching reverse step with chunks of this many planes
     AdjArgs<float> af;
     AdjArgs<double> ad;
     template <typename T> AdjArgs<T> &args();
@@ -2337,25 +2392,6 @@ int adjoint_create_t(tfd_adjoint *adj, cudaStream_t s) {
     adj->used = adjoint_layout<T>(p, &A, adj->arena);
     TFD_CUDA(cudaMemsetAsync(adj->arena, 0, adj->used, s));
     adj->q = 0;
-    // The marching reverse step serves 3D grids with all components and no periodic face (TFD_ADJOINT_KERNEL=gather
-    // in the environment keeps the gather pair, for comparisons).
-    adj->march_lz = 0;
-    const char *env = getenv("TFD_ADJOINT_KERNEL");
-    const bool gather = env && std::string(env) == "gather";
-    const Grid<T> &g = A.g;
-    if (!gather && p->desc.components == kMaskAll && g.n[0] >= 2 && g.n[1] >= 2 && g.n[2] >= 2 && !g.periodic[0] && !g.periodic[1] &&
-        !g.periodic[2]) {
-        int device = 0, sms = 148, per_sm = 0;
-        TFD_CUDA(cudaGetDevice(&device));
-        TFD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-        TFD_CUDA(cudaFuncSetAttribute(k_adjoint_march<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdjMarchSmem<T>)));
-        TFD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint_march<T>, kAmThreads, sizeof(AdjMarchSmem<T>)));
-        // Chunks of about 16 planes, shorter (down to 4) until the launch has two waves of CTAs.
-        const long long tiles = (long long)((g.n[0] + kAmX - 1) / kAmX) * ((g.n[1] + kAmY - 1) / kAmY);
-        int chunks = (g.n[2] + 15) / 16;
-        while (tiles * chunks < 2LL * sms * std::max(1, per_sm) && (g.n[2] + chunks) / (chunks + 1) >= 4) ++chunks;
-        adj->march_lz = (g.n[2] + chunks - 1) / chunks;
-    }
     return TFD_OK;
 }
 
@@ -2371,14 +2407,6 @@ int adjoint_step_t(tfd_adjoint *adj, const void *snapshot, const void *seeds, cu
     const dim3 grid((unsigned)((g.n[0] + kAdjX - 1) / kAdjX), (unsigned)((g.n[1] + kAdjY - 1) / kAdjY), (unsigned)g.n[2]);
     const dim3 block(kAdjX, kAdjY);
     const T *slot = (const T *)snapshot;
-    if (adj->march_lz > 0) {
-        const dim3 mgrid((unsigned)((g.n[0] + kAmX - 1) / kAmX), (unsigned)((g.n[1] + kAmY - 1) / kAmY),
-                         (unsigned)((g.n[2] + adj->march_lz - 1) / adj->march_lz));
-        k_adjoint_march<T><<<mgrid, kAmThreads, sizeof(AdjMarchSmem<T>), s>>>(A, slot, adj->q, adj->march_lz);
-        TFD_CUDA(cudaGetLastError());
-        adj->q ^= 1;
-        return TFD_OK;
-    }
     switch (p->desc.components) {
         case kMaskTM:
             k_adjoint_e<T, kMaskTM><<<grid, block, 0, s>>>(A, slot, adj->q);

@@ -1,0 +1,231 @@
+// 2D TMz stepping entirely on chip: one thread-block cluster holds a whole small grid in distributed shared
+// memory and runs every step of a tfd_step call without touching HBM between steps.
+//
+// A 320 x 240 TMz grid is about 1.4 MB of fields, inverse permittivity and CPML memories: more than one CTA's
+// shared memory, less than a cluster's (8 or 16 CTAs of up to 227 KB on a B200). Each CTA of the cluster owns a
+// band of rows [r0, r1) and keeps Ez, Hx, Hy, 1/eps and the CPML memories of its rows in its own shared memory.
+// A step is
+//   E phase: Ez of every own cell from Hy (same row) and Hx (row y - 1: the CTA below for the first row, read
+//            through distributed shared memory), the E-family CPML memories, the E soft sources;
+//   cluster barrier;
+//   H phase: Hx from Ez (row y + 1: the CTA above for the last row), Hy from Ez (x + 1), the H-family memories,
+//            the H soft sources, then the point traces of the step (the owning CTA writes them to HBM);
+//   cluster barrier.
+// Each phase reads only the other family, so the updates are in place. The arithmetic per cell is that of
+// the strip kernels' general path (step2d.cuh: strip_general), so the fields are bitwise the same. The state
+// is loaded from the parity the step counter names at the start of the launch and written back, with the
+// counter, at the end. Scope: 2D TMz plans without DFT planes (the traces are the only observations).
+#pragma once
+#include <cooperative_groups.h>
+
+#include "internal.cuh"
+
+namespace tfd {
+
+namespace cg = cooperative_groups;
+
+constexpr int kCl2dThreads = 1024;
+constexpr int kCl2dMaxRanks = 16;
+
+struct Cluster2D {
+    int ranks;                       // CTAs in the cluster
+    int r0[kCl2dMaxRanks + 1];       // band of rank c: rows [r0[c], r0[c + 1])
+    int rows_max;                    // the largest band
+    int w;                           // shared-memory row width (nx)
+    int rx_e, rx_h;                  // x-slab memory widths (rows of both x slabs) of the E and H families
+    int rye_lo[kCl2dMaxRanks], rye_n[kCl2dMaxRanks];   // per rank: first y-slab memory row of its band, count (E)
+    int ryh_lo[kCl2dMaxRanks], ryh_n[kCl2dMaxRanks];   // the same for the H family
+    int rye_max, ryh_max;
+    int count;                       // steps of this launch
+};
+
+// Shared-memory arrays of one rank, at element offsets fixed by the launch (every rank uses the same layout, so
+// a neighbour's row sits at the same offset in its shared memory).
+struct Cl2dLayout {
+    int ez, hx, hy, ie, pex, pey, phx, phy, total;
+};
+
+__host__ __device__ inline Cl2dLayout cl2d_layout(const Cluster2D &c) {
+    Cl2dLayout L;
+    const int cells = c.rows_max * c.w;
+    L.ez = 0;
+    L.hx = L.ez + cells;
+    L.hy = L.hx + cells;
+    L.ie = L.hy + cells;
+    L.pex = L.ie + cells;
+    L.pey = L.pex + c.rows_max * c.rx_e;
+    L.phx = L.pey + c.rye_max * c.w;
+    L.phy = L.phx + c.rows_max * c.rx_h;
+    L.total = L.phy + c.ryh_max * c.w;
+    return L;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid_constant__ Grid<T> g, const __grid_constant__ Cluster2D c,
+                                                                   const TraceDev *__restrict__ traces, int n_traces, T *trace_out) {
+    extern __shared__ __align__(16) unsigned char cl_raw[];
+    T *const sm = reinterpret_cast<T *>(cl_raw);
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    const Cl2dLayout L = cl2d_layout(c);
+    const int nx = g.n[0], ny = g.n[1], W = c.w, pitch = g.pitch;
+    const int r0 = c.r0[rank], r1 = c.r0[rank + 1], rows = r1 - r0;
+    const int tid = threadIdx.x;
+    const long long n0 = *g.counter;
+    const int par0 = (int)(n0 & 1);
+    T *Ez = sm + L.ez, *Hx = sm + L.hx, *Hy = sm + L.hy, *ie = sm + L.ie;
+    T *pex = sm + L.pex, *pey = sm + L.pey, *phx = sm + L.phx, *phy = sm + L.phy;
+    // The neighbours' bands: the last Hx row of the rank below, the first Ez row of the rank above.
+    const T *hx_below = rank > 0 ? cluster.map_shared_rank(sm + L.hx, rank - 1) : nullptr;
+    const T *ez_above = rank + 1 < c.ranks ? cluster.map_shared_rank(sm + L.ez, rank + 1) : nullptr;
+    const int rows_below = rank > 0 ? c.r0[rank] - c.r0[rank - 1] : 0;
+    const int RxE = g.rows[0][0], RxH = g.rows[1][0];
+    const int *rxp_e = g.row[0][0], *rxp_h = g.row[1][0], *ryp_e = g.row[0][1], *ryp_h = g.row[1][1];
+
+    // Load the band (parity par0) and its CPML memories.
+    for (int q = tid; q < rows * W; q += kCl2dThreads) {
+        const int y = r0 + q / W, x = q % W;
+        const long long i = (long long)y * pitch + x;
+        Ez[q] = g.E[par0][2][i];
+        Hx[q] = g.H[par0][0][i];
+        Hy[q] = g.H[par0][1][i];
+        ie[q] = g.inv_eps[2][i];
+    }
+    if (RxE) for (int q = tid; q < rows * RxE; q += kCl2dThreads) pex[q] = g.psiE[par0][0][1][(long long)(r0 + q / RxE) * RxE + q % RxE];
+    if (RxH) for (int q = tid; q < rows * RxH; q += kCl2dThreads) phx[q] = g.psiH[0][0][(long long)(r0 + q / RxH) * RxH + q % RxH];
+    for (int q = tid; q < c.rye_n[rank] * W; q += kCl2dThreads) pey[q] = g.psiE[par0][1][1][(long long)(c.rye_lo[rank] + q / W) * pitch + q % W];
+    for (int q = tid; q < c.ryh_n[rank] * W; q += kCl2dThreads) phy[q] = g.psiH[1][0][(long long)(c.ryh_lo[rank] + q / W) * pitch + q % W];
+    // Sources that meet the band (E: its rows; H: its rows), tested once.
+    unsigned src_e = 0, src_hx = 0, src_hy = 0;
+    for (int t = 0; t < g.n_src; ++t) {
+        const SourceTerm &s = g.src[t];
+        const bool hit = s.lo[1] < r1 && r0 < s.hi[1];
+        if (s.family == 0 && s.comp == 2 && hit) src_e |= 1u << t;
+        if (s.family == 1 && s.comp == 0 && hit) src_hx |= 1u << t;
+        if (s.family == 1 && s.comp == 1 && hit) src_hy |= 1u << t;
+    }
+    auto add_sources = [&](unsigned mask, int x, int y, long long n, T v) {
+        for (; mask; mask &= mask - 1) {
+            const int t = __ffs(mask) - 1;
+            const SourceTerm &s = g.src[t];
+            if (x >= s.lo[0] && x < s.hi[0] && y >= s.lo[1] && y < s.hi[1]) v = v + g.src_values[(long long)t * g.steps + n];
+        }
+        return v;
+    };
+    const bool pec_x = g.pec_on[0] != 0, pec_y = g.pec_on[1] != 0;
+    const T pneg_x = g.pec_neg[0], pneg_y = g.pec_neg[1], cn = g.cn;
+    const T *mxe = g.metric[0][0], *mye = g.metric[0][1], *mxh = g.metric[1][0], *myh = g.metric[1][1];
+    cluster.sync();                                       // every band loaded before any neighbour reads it
+
+    long long n = n0;
+    for (int k = 0; k < c.count && n < g.steps; ++k, ++n) {
+        // ---- E phase ----
+        for (int q = tid; q < rows * nx; q += kCl2dThreads) {
+            const int yl = q / nx, x = q % nx, y = r0 + yl;
+            const int e = yl * W + x;
+            T d = x > 0 ? Hy[e] - Hy[e - 1] : T(0);
+            if (mxe != nullptr && x > 0) d = d * mxe[x];
+            const int rxE = (rxp_e != nullptr && x > 0) ? rxp_e[x] : -1;
+            if (rxE >= 0) {
+                const T mem = pex[yl * RxE + rxE] * g.cb[0][0][x] + g.cc[0][0][x] * d;
+                pex[yl * RxE + rxE] = mem;
+                d = d * g.ck[0][0][x] + mem;
+            }
+            T acc = T(0) + d;
+            if (y > 0) {
+                const T below = yl > 0 ? Hx[e - W] : hx_below[(rows_below - 1) * W + x];
+                d = Hx[e] - below;
+            } else {
+                d = T(0);
+            }
+            if (mye != nullptr && y > 0) d = d * mye[y];
+            const int rye = (ryp_e != nullptr && y > 0) ? ryp_e[y] : -1;
+            if (rye >= 0) {
+                const int pi = (rye - c.rye_lo[rank]) * W + x;
+                const T mem = pey[pi] * g.cb[0][1][y] + g.cc[0][1][y] * d;
+                pey[pi] = mem;
+                d = d * g.ck[0][1][y] + mem;
+            }
+            acc = acc + (-d);
+            T ez = Ez[e] + (cn * ie[e]) * acc;
+            if (src_e) ez = add_sources(src_e, x, y, n, ez);
+            Ez[e] = ez;
+        }
+        cluster.sync();
+        // ---- H phase ----
+        for (int q = tid; q < rows * nx; q += kCl2dThreads) {
+            const int yl = q / nx, x = q % nx, h = r0 + yl;
+            const int e = yl * W + x;
+            const T ezc = Ez[e];
+            // Hx: dy(Ez)
+            T d = T(0);
+            if (h < ny - 1) {
+                const T up = yl + 1 < rows ? Ez[e + W] : ez_above[x];
+                d = up - ezc;
+                if (myh != nullptr) d = d * myh[h];
+                const int ryh = ryp_h != nullptr ? ryp_h[h] : -1;
+                if (ryh >= 0) {
+                    const int pi = (ryh - c.ryh_lo[rank]) * W + x;
+                    const T mem = phy[pi] * g.cb[1][1][h] + g.cc[1][1][h] * d;
+                    phy[pi] = mem;
+                    d = d * g.ck[1][1][h] + mem;
+                }
+            } else if (pec_y) {
+                d = pneg_y * ezc;
+            }
+            T acc = T(0) + d;
+            T hxn = Hx[e] - cn * acc;
+            // Hy: -dx(Ez)
+            d = T(0);
+            if (x < nx - 1) {
+                d = Ez[e + 1] - ezc;
+                if (mxh != nullptr) d = d * mxh[x];
+                const int rxH = rxp_h != nullptr ? rxp_h[x] : -1;
+                if (rxH >= 0) {
+                    const T mem = phx[yl * RxH + rxH] * g.cb[1][0][x] + g.cc[1][0][x] * d;
+                    phx[yl * RxH + rxH] = mem;
+                    d = d * g.ck[1][0][x] + mem;
+                }
+            } else if (pec_x) {
+                d = pneg_x * ezc;
+            }
+            acc = T(0) + (-d);
+            T hyn = Hy[e] - cn * acc;
+            if (src_hx) hxn = add_sources(src_hx, x, h, n, hxn);
+            if (src_hy) hyn = add_sources(src_hy, x, h, n, hyn);
+            Hx[e] = hxn;
+            Hy[e] = hyn;
+        }
+        __syncthreads();
+        // Point traces of step n sampled by the rank that owns the cell.
+        for (int t = tid; t < n_traces; t += kCl2dThreads) {
+            const TraceDev tr = traces[t];
+            const int y = (int)(tr.offset / pitch), x = (int)(tr.offset % pitch);
+            if (y < r0 || y >= r1) continue;
+            const int e = (y - r0) * W + x;
+            T v = T(0);
+            if (tr.family == 0 && tr.comp == 2) v = Ez[e];
+            else if (tr.family == 1 && tr.comp == 0) v = Hx[e];
+            else if (tr.family == 1 && tr.comp == 1) v = Hy[e];
+            trace_out[n * n_traces + t] = v;
+        }
+        cluster.sync();
+    }
+    // Write the band back at the parity of the step count reached, and the counter.
+    const int par = (int)(n & 1);
+    for (int q = tid; q < rows * W; q += kCl2dThreads) {
+        const int y = r0 + q / W, x = q % W;
+        const long long i = (long long)y * pitch + x;
+        g.E[par][2][i] = Ez[q];
+        g.H[par][0][i] = Hx[q];
+        g.H[par][1][i] = Hy[q];
+    }
+    if (RxE) for (int q = tid; q < rows * RxE; q += kCl2dThreads) g.psiE[par][0][1][(long long)(r0 + q / RxE) * RxE + q % RxE] = pex[q];
+    if (RxH) for (int q = tid; q < rows * RxH; q += kCl2dThreads) g.psiH[0][0][(long long)(r0 + q / RxH) * RxH + q % RxH] = phx[q];
+    for (int q = tid; q < c.rye_n[rank] * W; q += kCl2dThreads) g.psiE[par][1][1][(long long)(c.rye_lo[rank] + q / W) * pitch + q % W] = pey[q];
+    for (int q = tid; q < c.ryh_n[rank] * W; q += kCl2dThreads) g.psiH[1][0][(long long)(c.ryh_lo[rank] + q / W) * pitch + q % W] = phy[q];
+    if (rank == 0 && tid == 0) *g.counter = n;
+    cluster.sync();                                       // no rank leaves while a neighbour may still read it
+}
+
+}  // namespace tfd

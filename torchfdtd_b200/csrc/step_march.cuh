@@ -846,15 +846,6 @@ struct MarchMix {
     int ix0, ix1, iy0, iy1;
     int zb[4];
     int lz[3], chunks[3];
-    int tx_off, ty_off;          // tile of CTA (blockIdx.x, blockIdx.y) is (blockIdx.x + tx_off, blockIdx.y + ty_off)
-};
-
-// The boundary tiles of a grid (every tile outside the interior block) as up to four rectangles of tiles,
-// enumerated by blockIdx.x; blockIdx.z is the z chunk of lz planes.
-struct MarchRing {
-    int rect[4][4];              // tile x0, tile y0, width, height
-    int start[5];                // prefix sums of the rectangles' tile counts
-    int n_rect, lz, nz;
 };
 
 template <typename T, int SAMPLES, int D, int MINB, int GEN>
@@ -867,7 +858,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march_mixed(const 
     }
     const int z0 = mx.zb[seg] + zc * mx.lz[seg];
     const int z1 = min(z0 + mx.lz[seg], mx.zb[seg + 1]);
-    const int tx = blockIdx.x + mx.tx_off, ty = blockIdx.y + mx.ty_off;
+    const int tx = blockIdx.x, ty = blockIdx.y;
     const bool interior = tx >= mx.ix0 && tx < mx.ix1 && ty >= mx.iy0 && ty < mx.iy1;
     if (interior && seg == 1)
         march_body<T, SAMPLES, D, 1>(args, tx, ty, z0, z1);
@@ -875,21 +866,6 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march_mixed(const 
         march_body<T, SAMPLES, D, 4>(args, tx, ty, z0, z1);
     else
         march_body<T, SAMPLES, D, GEN>(args, tx, ty, z0, z1);
-}
-
-// The general body (GEN: 0, or 2 with periodic seams) over the boundary tiles of a MarchRing: launched before
-// the interior block's launch on the same stream, so boundary and interior CTAs never share an SM's
-// instruction cache (a launch variant the tuner measures against the mixed launch).
-template <typename T, int SAMPLES, int D, int MINB, int GEN>
-__global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march_ring(const __grid_constant__ MarchArgs<T> args,
-                                                                         const __grid_constant__ MarchRing ring) {
-    const int t = blockIdx.x;
-    int r = 0;
-    while (r + 1 < ring.n_rect && t >= ring.start[r + 1]) ++r;
-    const int local = t - ring.start[r];
-    const int tx = ring.rect[r][0] + local % ring.rect[r][2], ty = ring.rect[r][1] + local / ring.rect[r][2];
-    const int z0 = blockIdx.z * ring.lz;
-    march_body<T, SAMPLES, D, GEN>(args, tx, ty, z0, min(z0 + ring.lz, ring.nz));
 }
 
 }  // namespace tfd

@@ -508,9 +508,11 @@ class Simulation:
         free, _ = torch.cuda.mem_get_info()
         observer = Observer(p, plan, grid)
         observer.host_fields = host_fields
+        lap('observer')
         if host_fields is not None:
             from .native import staging_ring
             staging_ring(grid.torch_dtype)          # pinned once per process, before any capture
+            lap('staging_ring')
         graphs = {}
         width = 1
         stream = torch.cuda.Stream()
@@ -521,10 +523,12 @@ class Simulation:
                 # One eager step loads the kernels before capture; the state is then zeroed.
                 grid.step(1, stream)
                 grid.reset()
+                stream.synchronize()
+                lap('warm_step_and_reset')
                 graphs = capture_graphs(lambda count: grid.step(count, stream), {1, width})
             torch.cuda.synchronize()
         torch.cuda.synchronize()
-        lap('observer_and_graph_capture')
+        lap('graph_capture')
         setup_seconds = time.perf_counter() - started
         compute_start = time.perf_counter()
         completed, termination_reason, replays = 0, 'max_steps', 0

@@ -85,9 +85,9 @@ def grid_candidates(plan):
     """Marching-kernel launch variants worth measuring for a plan."""
     nz = plan.shape[2]
     if plan.dtype == np.float64:
-        base = [22, 122, 422]
+        base = [22, 122]
     else:
-        base = [14, 23, 32, 22, 114, 314, 414, 423]
+        base = [14, 23, 32, 22, 114, 314]
     lz = [v for v in (4, 8, 16) if v < nz]            # planes per chunk around the default (about 12)
     return base + [z * 1000 + 14 for z in lz] if plan.dtype != np.float64 else base + [z * 1000 + 22 for z in lz]
 
