@@ -108,6 +108,45 @@ def workload(name, steps, seed=2024):
                                                  spectrum=custom)])
         return project, None, ('3D Yee+CPML 160x120x40 (0.05 um), CPML 12, Si strip 0.65x0.4 um in SiO2, Ey dipole, '
                                'x-normal DFT plane at 1.55 um, FP32')
+    if name == 'graded':
+        # A graded mesh (nonuniform x / y / z): fine 0.05 um lattice around a Si block, coarsened up to 0.15 um
+        # (1.4 grading) between it and the PML; the march kernel's metric body.
+        L = 12
+        b = Boundaries(**{f'{a}_{s}': baseline_face(L) for a in 'xyz' for s in ('min', 'max')})
+        region = Region(dimension='3d', size=(30.0, 30.0, 16.0), mesh=.05, pml_cells=L, steps=steps, backend='cuda',
+                        cuda_kernel='fused', boundaries=b, run_control=control, snapshot_interval=10000, mesh_type='graded',
+                        mesh_max=.15, mesh_grading=1.4, mesh_ppw=6, material_sampling='yee')
+        project = Project(name='graded mesh', region=region, materials=[Material(name='Si', index=3.476)],
+                          structures=[Structure(id='blk', size=(6, 6, 3), material='Si')],
+                          sources=[Source(id='dip', center=(-2.0, 0, 0), **src)],
+                          monitors=[Monitor(id='probe', center=(2.0, 0, 0), component='Ey')])
+        return project, None, ('3D Yee+CPML on a graded mesh (30x30x16 um, 0.05 um lattice coarsened to 0.15 um at grading '
+                               '1.4 outside a 6x6x3 um Si block), CPML 12, Yee sampling, Ey dipole, FP32')
+    if name in ('tfsf', 'dispersive'):
+        # 256^3 at 0.05 um, CPML 12: a TFSF box (plane wave along +x) around a Si sphere, or a Drude sphere and a
+        # Lorentz slab lit by an Ey dipole; both run the split gather step.
+        n, L = (256, 256, 256), 12
+        b = Boundaries(**{f'{a}_{s}': baseline_face(L) for a in 'xyz' for s in ('min', 'max')})
+        region = Region(dimension='3d', size=tuple(v * .05 for v in n), mesh=.05, pml_cells=L, steps=steps, backend='cuda',
+                        cuda_kernel='fused', boundaries=b, run_control=control, snapshot_interval=10000)
+        if name == 'tfsf':
+            project = Project(name='TFSF 256^3', region=region, materials=[Material(name='Si', index=3.476)],
+                              structures=[Structure(id='ball', kind='sphere', radius=2.0, material='Si')],
+                              sources=[Source(id='box', kind='tfsf', normal='x', direction='+', size=(8, 8, 8), component='Ey',
+                                              wavelength=lam, pulse='gaussian', time_definition='standard', pulse_length=20e-15,
+                                              pulse_offset=40e-15)],
+                              monitors=[Monitor(id='probe', center=(5.0, 0, 0), component='Ey')])
+            return project, None, ('3D Yee+CPML 256^3 (0.05 um), CPML 12, an 8 um TFSF box (Ey plane wave along +x) around a '
+                                   '2 um Si sphere, FP32')
+        metal = Material(name='metal', model='drude', epsilon_inf=1.5, plasma_rad_s=9e15, collision_rad_s=1e14)
+        glass = Material(name='disp', model='lorentz', epsilon_inf=2.0, resonance_rad_s=3e15, linewidth_rad_s=2e14, delta_epsilon=1.2)
+        project = Project(name='dispersive 256^3', region=region, materials=[metal, glass],
+                          structures=[Structure(id='ball', kind='sphere', center=(2.0, 0, 0), radius=1.5, material='metal'),
+                                      Structure(id='slab', size=(1.0, 11.6, 11.6), center=(-2.0, 0, 0), material='disp')],
+                          sources=[Source(id='dip', center=(-4.0, 0, 0), **src)],
+                          monitors=[Monitor(id='probe', center=(4.5, 0, 0), component='Ey')])
+        return project, None, ('3D Yee+CPML 256^3 (0.05 um), CPML 12, a 1.5 um Drude sphere and a 1 um Lorentz slab '
+                               '(coupled trapezoidal ADE), Ey dipole, FP32')
     if name == 'tmz2d':
         # 2D TMz plain-method case: 16 x 12 um at 0.05 um (320 x 240 cells), CPML 16, Courant 0.99/sqrt(2).
         L = 16
@@ -870,6 +909,8 @@ def extra_workloads(args, local):
     attempt('strip', fixed('strip', 1000, 50))
     attempt('batch64', batch)
     attempt('adjoint3d', adjoint)
+    for name in ('graded', 'tfsf', 'dispersive'):
+        attempt(name, fixed(name, 100, 5))
     return extras
 
 
@@ -880,7 +921,7 @@ def main():
     ap.add_argument('--warmup', type=int, default=10)
     ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
     ap.add_argument('--workload', choices=['roofline', 'roofline256', 'strip', 'periodic', 'tmz2d', 'batch64', 'adjoint3d', 'surrogate',
-                                           'adjoint_probe', 'surrogate_kernels'],
+                                           'adjoint_probe', 'surrogate_kernels', 'graded', 'tfsf', 'dispersive'],
                     default='roofline')
     ap.add_argument('--probe-cells', type=int, default=128, help='adjoint_probe: cells per side in x and y')
     ap.add_argument('--probe-batch', type=int, default=256, help='surrogate_kernels: densities per pass')

@@ -33,12 +33,15 @@ ENGINE = 'TorchFDTD-B200 fused Yee/CPML (sm_100a)'
 
 def algorithmic_bytes_per_step(plan):
     """Compulsory HBM bytes of one step: each advanced field component read and written once,
-    each stored permittivity sample read once and each CPML memory read and written once."""
+    each stored permittivity sample read once, each CPML memory and each dispersive pole state (P, Q) read and
+    written once."""
     real = np.dtype(plan.dtype).itemsize
     comps = len(plan.active_components())
     samples = plan.material_samples if plan.dimension == '3d' else 1
     psi = sum(int(np.prod(s)) for (f, a, c, side), s in plan.psi_shapes() if _psi_active(plan, f, a, c))
-    return plan.cells * (2 * real * comps + real * samples) + 2 * real * psi
+    # Dispersive samples: P and Q of every pole read and written once.
+    ade = sum(2 * st.poles * st.samples for st in getattr(plan, 'ade', []))
+    return plan.cells * (2 * real * comps + real * samples) + 2 * real * psi + 2 * real * ade
 
 
 def _psi_active(plan, forward, axis, comp):
