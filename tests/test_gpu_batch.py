@@ -266,7 +266,7 @@ def test_batch_tuner_picks_a_measured_cta_count_and_results_do_not_change():
     projects = uneven_cases()
     shapes = [(1, 8), (4, 0), (0, 12), (0, 0)]
     tuning = tune_tensor_batch(projects, candidates=shapes, steps=2, repeats=3)
-    assert tuning.kind == 'batch' and tuple(tuning.choice) in shapes
+    assert tuning.kind == 'batch' and tuple(tuning.choice[:2]) in shapes and tuning.choice[2] == 0
     assert sorted((r['ctas'], r['rows']) for r in tuning.candidates) == sorted(shapes)
     auto = run_tensor_batch(projects, launch='auto')
     plain = run_tensor_batch(projects)

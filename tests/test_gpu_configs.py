@@ -71,7 +71,7 @@ def test_config1_strip_160x120x40_1000_steps_with_dft_plane(precision):
 
 def test_roofline_512x512x256_mixed_launch_8_steps_every_memory():
     from torchfdtd_b200.native import NativeGrid
-    project, eps = config_project('roofline', 8)
+    project, eps = config_project('roofline', 10)      # a Region runs at least 10 steps; 8 of them here
     plan = plan_grid(project)
     plan.epsilon, plan.inv_eps = eps, (1 / eps).astype(plan.dtype)
     grid = NativeGrid(plan)

@@ -103,3 +103,24 @@ def test_loaded_project_is_the_reference_project(golden):
         project = Project.model_validate_json(str(raw['project']))
         for axis, name in enumerate('xyz'):
             np.testing.assert_array_equal(project.region.mesh_nodes[axis], raw[f'mesh_{name}_um'])
+
+
+@pytest.mark.parametrize('name', ['graded3d', 'graded2d', 'explicit3d', 'steps3d', 'strip3d'])
+def test_frames_sample_the_reference_display_grid(golden, name):
+    """The last stored frame and the permittivity plane are the reference's: on nonuniform meshes the cells
+    nearest to a uniform pixel grid, else a stride decimation (reference torchfdtd/solver.py:810-828)."""
+    from torchfdtd_b200.simulation import Observer, Simulation
+    d = np.load(golden / f'sim_{name}.npz')
+    project = Project.model_validate_json(str(d['project']))
+    r = project.region
+    plan = Simulation(project).plan
+
+    class Final:                       # stands in for the device grid: the reference's final fields
+        def get_slice(self, component, axis, index):
+            field = (d['E'] if component[0] == 'E' else d['H'])[..., 'xyz'.index(component[1].lower())]
+            return np.take(field, index, axis=axis)
+
+    observer = Observer(project, plan, Final())
+    np.testing.assert_array_equal(observer.decimate(Final().get_slice(r.field, observer.axis, observer.plane_index)),
+                                  d['frames'][-1])
+    assert observer.eps_plane.shape == d['frames'][-1].shape

@@ -1511,11 +1511,13 @@ int setup_cluster2d(tfd_plan *p) {
         }
         if (first < 0) first = 0;
     };
-    for (int ranks : {8, 16}) {
-        if (ranks > ny) break;
+    // 16 CTAs first: the band work is spread over twice the SMs of a portable 8-CTA cluster.
+    for (int ranks : {16, 8}) {
+        if (ranks > ny) continue;
         Cluster2D t{};
         t.ranks = ranks;
         t.w = nx;
+        t.h = ny;
         t.rx_e = g.rows[0][0];
         t.rx_h = g.rows[1][0];
         for (int r = 0; r <= ranks; ++r) t.r0[r] = (int)((long long)r * ny / ranks);
@@ -1526,7 +1528,7 @@ int setup_cluster2d(tfd_plan *p) {
             t.rye_max = std::max(t.rye_max, t.rye_n[r]);
             t.ryh_max = std::max(t.ryh_max, t.ryh_n[r]);
         }
-        const size_t bytes = (size_t)cl2d_layout(t).total * sizeof(T);
+        const size_t bytes = (size_t)cl2d_layout(t, (int)sizeof(T)).total * sizeof(T);
         if (bytes > (size_t)max_smem) continue;
         TFD_CUDA(cudaFuncSetAttribute(k_step2d_cluster<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
         if (ranks > 8) TFD_CUDA(cudaFuncSetAttribute(k_step2d_cluster<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));

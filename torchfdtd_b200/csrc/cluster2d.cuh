@@ -25,6 +25,7 @@ namespace tfd {
 namespace cg = cooperative_groups;
 
 constexpr int kCl2dThreads = 1024;
+constexpr int kCl2dWarps = kCl2dThreads / 32;
 constexpr int kCl2dMaxRanks = 16;
 
 struct Cluster2D {
@@ -32,6 +33,7 @@ struct Cluster2D {
     int r0[kCl2dMaxRanks + 1];       // band of rank c: rows [r0[c], r0[c + 1])
     int rows_max;                    // the largest band
     int w;                           // shared-memory row width (nx)
+    int h;                           // rows of the grid (ny): length of the per-row coefficient tables
     int rx_e, rx_h;                  // x-slab memory widths (rows of both x slabs) of the E and H families
     int rye_lo[kCl2dMaxRanks], rye_n[kCl2dMaxRanks];   // per rank: first y-slab memory row of its band, count (E)
     int ryh_lo[kCl2dMaxRanks], ryh_n[kCl2dMaxRanks];   // the same for the H family
@@ -40,12 +42,18 @@ struct Cluster2D {
 };
 
 // Shared-memory arrays of one rank, at element offsets fixed by the launch (every rank uses the same layout, so
-// a neighbour's row sits at the same offset in its shared memory).
+// a neighbour's row sits at the same offset in its shared memory). After the fields and memories: per family f
+// and axis a (x: nx entries, y: ny entries) the CPML coefficients b, c, 1/kappa and the metric factor of each
+// column / row (tab), and the memory row of each column / row (-1: no CPML term there; slab).
 struct Cl2dLayout {
-    int ez, hx, hy, ie, pex, pey, phx, phy, total;
+    int ez, hx, hy, ie, pex, pey, phx, phy;
+    int tab[2][2];                   // 4 consecutive T arrays (b, c, k, metric) of n[a] entries
+    int slab[2][2];                  // int arrays, element offsets from the start of the int region
+    int ints;                        // start of the int region (in T elements)
+    int total;                       // T elements including the int region
 };
 
-__host__ __device__ inline Cl2dLayout cl2d_layout(const Cluster2D &c) {
+__host__ __device__ inline Cl2dLayout cl2d_layout(const Cluster2D &c, int tsize) {
     Cl2dLayout L;
     const int cells = c.rows_max * c.w;
     L.ez = 0;
@@ -56,7 +64,18 @@ __host__ __device__ inline Cl2dLayout cl2d_layout(const Cluster2D &c) {
     L.pey = L.pex + c.rows_max * c.rx_e;
     L.phx = L.pey + c.rye_max * c.w;
     L.phy = L.phx + c.rows_max * c.rx_h;
-    L.total = L.phy + c.ryh_max * c.w;
+    int o = L.phy + c.ryh_max * c.w;
+    int io = 0;
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 2; ++a) {
+            const int n = a == 0 ? c.w : c.h;
+            L.tab[f][a] = o;
+            o += 4 * n;
+            L.slab[f][a] = io;
+            io += n;
+        }
+    L.ints = o;
+    L.total = o + (io * 4 + tsize - 1) / tsize;
     return L;
 }
 
@@ -67,20 +86,20 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
     T *const sm = reinterpret_cast<T *>(cl_raw);
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
-    const Cl2dLayout L = cl2d_layout(c);
+    const Cl2dLayout L = cl2d_layout(c, (int)sizeof(T));
     const int nx = g.n[0], ny = g.n[1], W = c.w, pitch = g.pitch;
     const int r0 = c.r0[rank], r1 = c.r0[rank + 1], rows = r1 - r0;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const long long n0 = *g.counter;
     const int par0 = (int)(n0 & 1);
     T *Ez = sm + L.ez, *Hx = sm + L.hx, *Hy = sm + L.hy, *ie = sm + L.ie;
     T *pex = sm + L.pex, *pey = sm + L.pey, *phx = sm + L.phx, *phy = sm + L.phy;
+    int *const ints = reinterpret_cast<int *>(sm + L.ints);
     // The neighbours' bands: the last Hx row of the rank below, the first Ez row of the rank above.
     const T *hx_below = rank > 0 ? cluster.map_shared_rank(sm + L.hx, rank - 1) : nullptr;
     const T *ez_above = rank + 1 < c.ranks ? cluster.map_shared_rank(sm + L.ez, rank + 1) : nullptr;
     const int rows_below = rank > 0 ? c.r0[rank] - c.r0[rank - 1] : 0;
     const int RxE = g.rows[0][0], RxH = g.rows[1][0];
-    const int *rxp_e = g.row[0][0], *rxp_h = g.row[1][0], *ryp_e = g.row[0][1], *ryp_h = g.row[1][1];
 
     // Load the band (parity par0) and its CPML memories.
     for (int q = tid; q < rows * W; q += kCl2dThreads) {
@@ -95,6 +114,25 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
     if (RxH) for (int q = tid; q < rows * RxH; q += kCl2dThreads) phx[q] = g.psiH[0][0][(long long)(r0 + q / RxH) * RxH + q % RxH];
     for (int q = tid; q < c.rye_n[rank] * W; q += kCl2dThreads) pey[q] = g.psiE[par0][1][1][(long long)(c.rye_lo[rank] + q / W) * pitch + q % W];
     for (int q = tid; q < c.ryh_n[rank] * W; q += kCl2dThreads) phy[q] = g.psiH[1][0][(long long)(c.ryh_lo[rank] + q / W) * pitch + q % W];
+    // Coefficient tables. A column / row whose difference the update does not take (E: x = 0, y = 0; H: the last
+    // column / row) gets no memory row, so the tables alone decide where CPML terms apply.
+    for (int f = 0; f < 2; ++f)
+        for (int a = 0; a < 2; ++a) {
+            const int len = a == 0 ? nx : ny;
+            T *tb = sm + L.tab[f][a];
+            int *ts = ints + L.slab[f][a];
+            const int *rowp = g.row[f][a];
+            const T *m = g.metric[f][a];
+            for (int i = tid; i < len; i += kCl2dThreads) {
+                const bool diff = f == 0 ? i > 0 : i < len - 1;
+                const int r = (rowp != nullptr && diff) ? rowp[i] : -1;
+                ts[i] = r;
+                tb[i] = r >= 0 ? g.cb[f][a][i] : T(0);
+                tb[len + i] = r >= 0 ? g.cc[f][a][i] : T(0);
+                tb[2 * len + i] = r >= 0 ? g.ck[f][a][i] : T(1);
+                tb[3 * len + i] = m != nullptr ? m[i] : T(1);
+            }
+        }
     // Sources that meet the band (E: its rows; H: its rows), tested once.
     unsigned src_e = 0, src_hx = 0, src_hy = 0;
     for (int t = 0; t < g.n_src; ++t) {
@@ -103,6 +141,11 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
         if (s.family == 0 && s.comp == 2 && hit) src_e |= 1u << t;
         if (s.family == 1 && s.comp == 0 && hit) src_hx |= 1u << t;
         if (s.family == 1 && s.comp == 1 && hit) src_hy |= 1u << t;
+    }
+    bool band_traces = false;
+    for (int t = 0; t < n_traces; ++t) {
+        const int y = (int)(traces[t].offset / pitch);
+        band_traces |= y >= r0 && y < r1;
     }
     auto add_sources = [&](unsigned mask, int x, int y, long long n, T v) {
         for (; mask; mask &= mask - 1) {
@@ -114,100 +157,125 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
     };
     const bool pec_x = g.pec_on[0] != 0, pec_y = g.pec_on[1] != 0;
     const T pneg_x = g.pec_neg[0], pneg_y = g.pec_neg[1], cn = g.cn;
-    const T *mxe = g.metric[0][0], *mye = g.metric[0][1], *mxh = g.metric[1][0], *myh = g.metric[1][1];
-    cluster.sync();                                       // every band loaded before any neighbour reads it
+    const bool mx_e = g.metric[0][0] != nullptr, my_e = g.metric[0][1] != nullptr;
+    const bool mx_h = g.metric[1][0] != nullptr, my_h = g.metric[1][1] != nullptr;
+    const T *const xb_e = sm + L.tab[0][0], *const yb_e = sm + L.tab[0][1];
+    const T *const xb_h = sm + L.tab[1][0], *const yb_h = sm + L.tab[1][1];
+    const int *const xs_e = ints + L.slab[0][0], *const ys_e = ints + L.slab[0][1];
+    const int *const xs_h = ints + L.slab[1][0], *const ys_h = ints + L.slab[1][1];
+    // Work units: a warp takes 32 consecutive cells of one row. Unit u is row u / XU, columns 32 (u % XU) ...;
+    // a warp's units advance by kCl2dWarps, kept as (row, segment) without a division per unit.
+    const int XU = (nx + 31) / 32;
+    const int dq = kCl2dWarps / XU, dr = kCl2dWarps % XU;
+    const int yl_first = warp / XU, xs_first = warp % XU;
+    cluster.sync();                                       // every band and table loaded before any neighbour reads it
 
     long long n = n0;
     for (int k = 0; k < c.count && n < g.steps; ++k, ++n) {
         // ---- E phase ----
-        for (int q = tid; q < rows * nx; q += kCl2dThreads) {
-            const int yl = q / nx, x = q % nx, y = r0 + yl;
-            const int e = yl * W + x;
-            T d = x > 0 ? Hy[e] - Hy[e - 1] : T(0);
-            if (mxe != nullptr && x > 0) d = d * mxe[x];
-            const int rxE = (rxp_e != nullptr && x > 0) ? rxp_e[x] : -1;
-            if (rxE >= 0) {
-                const T mem = pex[yl * RxE + rxE] * g.cb[0][0][x] + g.cc[0][0][x] * d;
-                pex[yl * RxE + rxE] = mem;
-                d = d * g.ck[0][0][x] + mem;
+        for (int yl = yl_first, xs = xs_first; yl < rows;) {
+            const int y = r0 + yl, x = xs * 32 + lane;
+            // Row-uniform terms of dy(Hx).
+            const int rye = ys_e[y];
+            const T *hxb = yl > 0 ? Hx + (yl - 1) * W : (hx_below != nullptr ? hx_below + (rows_below - 1) * W : Hx);
+            if (x < nx) {
+                const int e = yl * W + x;
+                T d = x > 0 ? Hy[e] - Hy[e - 1] : T(0);
+                if (mx_e && x > 0) d = d * xb_e[3 * nx + x];
+                const int rxE = xs_e[x];
+                if (rxE >= 0) {
+                    const T mem = pex[yl * RxE + rxE] * xb_e[x] + xb_e[nx + x] * d;
+                    pex[yl * RxE + rxE] = mem;
+                    d = d * xb_e[2 * nx + x] + mem;
+                }
+                T acc = T(0) + d;
+                d = y > 0 ? Hx[e] - hxb[x] : T(0);
+                if (my_e && y > 0) d = d * yb_e[3 * ny + y];
+                if (rye >= 0) {
+                    const int pi = (rye - c.rye_lo[rank]) * W + x;
+                    const T mem = pey[pi] * yb_e[y] + yb_e[ny + y] * d;
+                    pey[pi] = mem;
+                    d = d * yb_e[2 * ny + y] + mem;
+                }
+                acc = acc + (-d);
+                T ez = Ez[e] + (cn * ie[e]) * acc;
+                if (src_e) ez = add_sources(src_e, x, y, n, ez);
+                Ez[e] = ez;
             }
-            T acc = T(0) + d;
-            if (y > 0) {
-                const T below = yl > 0 ? Hx[e - W] : hx_below[(rows_below - 1) * W + x];
-                d = Hx[e] - below;
-            } else {
-                d = T(0);
+            yl += dq;
+            xs += dr;
+            if (xs >= XU) {
+                xs -= XU;
+                ++yl;
             }
-            if (mye != nullptr && y > 0) d = d * mye[y];
-            const int rye = (ryp_e != nullptr && y > 0) ? ryp_e[y] : -1;
-            if (rye >= 0) {
-                const int pi = (rye - c.rye_lo[rank]) * W + x;
-                const T mem = pey[pi] * g.cb[0][1][y] + g.cc[0][1][y] * d;
-                pey[pi] = mem;
-                d = d * g.ck[0][1][y] + mem;
-            }
-            acc = acc + (-d);
-            T ez = Ez[e] + (cn * ie[e]) * acc;
-            if (src_e) ez = add_sources(src_e, x, y, n, ez);
-            Ez[e] = ez;
         }
         cluster.sync();
         // ---- H phase ----
-        for (int q = tid; q < rows * nx; q += kCl2dThreads) {
-            const int yl = q / nx, x = q % nx, h = r0 + yl;
-            const int e = yl * W + x;
-            const T ezc = Ez[e];
-            // Hx: dy(Ez)
-            T d = T(0);
-            if (h < ny - 1) {
-                const T up = yl + 1 < rows ? Ez[e + W] : ez_above[x];
-                d = up - ezc;
-                if (myh != nullptr) d = d * myh[h];
-                const int ryh = ryp_h != nullptr ? ryp_h[h] : -1;
-                if (ryh >= 0) {
-                    const int pi = (ryh - c.ryh_lo[rank]) * W + x;
-                    const T mem = phy[pi] * g.cb[1][1][h] + g.cc[1][1][h] * d;
-                    phy[pi] = mem;
-                    d = d * g.ck[1][1][h] + mem;
+        for (int yl = yl_first, xs = xs_first; yl < rows;) {
+            const int h = r0 + yl, x = xs * 32 + lane;
+            const int ryh = ys_h[h];
+            const T *ezu = yl + 1 < rows ? Ez + (yl + 1) * W : (ez_above != nullptr ? ez_above : Ez);
+            if (x < nx) {
+                const int e = yl * W + x;
+                const T ezc = Ez[e];
+                // Hx: dy(Ez)
+                T d = T(0);
+                if (h < ny - 1) {
+                    d = ezu[x] - ezc;
+                    if (my_h) d = d * yb_h[3 * ny + h];
+                    if (ryh >= 0) {
+                        const int pi = (ryh - c.ryh_lo[rank]) * W + x;
+                        const T mem = phy[pi] * yb_h[h] + yb_h[ny + h] * d;
+                        phy[pi] = mem;
+                        d = d * yb_h[2 * ny + h] + mem;
+                    }
+                } else if (pec_y) {
+                    d = pneg_y * ezc;
                 }
-            } else if (pec_y) {
-                d = pneg_y * ezc;
-            }
-            T acc = T(0) + d;
-            T hxn = Hx[e] - cn * acc;
-            // Hy: -dx(Ez)
-            d = T(0);
-            if (x < nx - 1) {
-                d = Ez[e + 1] - ezc;
-                if (mxh != nullptr) d = d * mxh[x];
-                const int rxH = rxp_h != nullptr ? rxp_h[x] : -1;
-                if (rxH >= 0) {
-                    const T mem = phx[yl * RxH + rxH] * g.cb[1][0][x] + g.cc[1][0][x] * d;
-                    phx[yl * RxH + rxH] = mem;
-                    d = d * g.ck[1][0][x] + mem;
+                T acc = T(0) + d;
+                T hxn = Hx[e] - cn * acc;
+                // Hy: -dx(Ez)
+                d = T(0);
+                if (x < nx - 1) {
+                    d = Ez[e + 1] - ezc;
+                    if (mx_h) d = d * xb_h[3 * nx + x];
+                    const int rxH = xs_h[x];
+                    if (rxH >= 0) {
+                        const T mem = phx[yl * RxH + rxH] * xb_h[x] + xb_h[nx + x] * d;
+                        phx[yl * RxH + rxH] = mem;
+                        d = d * xb_h[2 * nx + x] + mem;
+                    }
+                } else if (pec_x) {
+                    d = pneg_x * ezc;
                 }
-            } else if (pec_x) {
-                d = pneg_x * ezc;
+                acc = T(0) + (-d);
+                T hyn = Hy[e] - cn * acc;
+                if (src_hx) hxn = add_sources(src_hx, x, h, n, hxn);
+                if (src_hy) hyn = add_sources(src_hy, x, h, n, hyn);
+                Hx[e] = hxn;
+                Hy[e] = hyn;
             }
-            acc = T(0) + (-d);
-            T hyn = Hy[e] - cn * acc;
-            if (src_hx) hxn = add_sources(src_hx, x, h, n, hxn);
-            if (src_hy) hyn = add_sources(src_hy, x, h, n, hyn);
-            Hx[e] = hxn;
-            Hy[e] = hyn;
+            yl += dq;
+            xs += dr;
+            if (xs >= XU) {
+                xs -= XU;
+                ++yl;
+            }
         }
-        __syncthreads();
-        // Point traces of step n sampled by the rank that owns the cell.
-        for (int t = tid; t < n_traces; t += kCl2dThreads) {
-            const TraceDev tr = traces[t];
-            const int y = (int)(tr.offset / pitch), x = (int)(tr.offset % pitch);
-            if (y < r0 || y >= r1) continue;
-            const int e = (y - r0) * W + x;
-            T v = T(0);
-            if (tr.family == 0 && tr.comp == 2) v = Ez[e];
-            else if (tr.family == 1 && tr.comp == 0) v = Hx[e];
-            else if (tr.family == 1 && tr.comp == 1) v = Hy[e];
-            trace_out[n * n_traces + t] = v;
+        if (band_traces) {
+            // Point traces of step n sampled by the rank that owns the cell (a CTA-uniform branch).
+            __syncthreads();
+            for (int t = tid; t < n_traces; t += kCl2dThreads) {
+                const TraceDev tr = traces[t];
+                const int y = (int)(tr.offset / pitch), x = (int)(tr.offset % pitch);
+                if (y < r0 || y >= r1) continue;
+                const int e = (y - r0) * W + x;
+                T v = T(0);
+                if (tr.family == 0 && tr.comp == 2) v = Ez[e];
+                else if (tr.family == 1 && tr.comp == 0) v = Hx[e];
+                else if (tr.family == 1 && tr.comp == 1) v = Hy[e];
+                trace_out[n * n_traces + t] = v;
+            }
         }
         cluster.sync();
     }

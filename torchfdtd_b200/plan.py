@@ -20,7 +20,7 @@ Features outside the fused nondispersive path are refused here with a
 from __future__ import annotations
 
 import math
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 from itertools import product
 
 import numpy as np
@@ -500,6 +500,11 @@ def plan_grid(project, polarization=None, material=True):
         tm = any(t.component in ('Ez', 'Hx', 'Hy') for t in sources)
         te = any(t.component in ('Ex', 'Ey', 'Hz') for t in sources)
         polarization = 'both' if tm and te else ('TE' if te else 'TM')
+    if r.dimension == '2d' and polarization != 'both':
+        # A 2D polarization leaves the other E components at zero: their pole states stay zero too, so only the
+        # samples of the advanced components carry an ADE state.
+        keep = (2,) if polarization == 'TM' else (0, 1)
+        ade = [st for st in (replace(st, target=st.target[np.isin(st.target % 3, keep)]) for st in ade) if st.samples]
     return GridPlan(project, tuple(r.shape), r.dimension, dtype, courant, r.time_step, r.steps, faces, pec_upper,
                     segments, eps, inv_eps, counts, sources, traces, planes,
                     polarization if r.dimension == '2d' else None, warnings, metrics, boxes, ade)

@@ -22,7 +22,7 @@ from pathlib import Path
 import numpy as np
 
 from .models import Project
-from .plan import index_at, plan_grid
+from .plan import field_axes, index_at, plan_grid
 from .run_control import DecayDecision, observation_schedule, source_end_time, validate_graph_steps
 from .spectra import point_spectrum
 
@@ -248,6 +248,17 @@ class Observer:
         self.axis = 'xyz'.index(r.slice_axis)
         self.plane_index = index_at(tuple(r.slice_position if i == self.axis else 0 for i in range(3)), r, r.field)[self.axis]
         component = 'xyz'.index(r.field[1].lower())
+        # Nonuniform meshes: frames (and the permittivity plane) are sampled at the cells nearest to a uniform
+        # grid of min(256, uniform cells) pixels per in-plane axis (reference torchfdtd/solver.py:810-818).
+        self.display = None
+        if r.mesh_type != 'uniform':
+            self.display = []
+            for i, coords in enumerate(field_axes(r, r.field)):
+                if i == self.axis:
+                    continue
+                count = min(256, r.base_shape[i])
+                pixels = (np.arange(count) + .5) * r.actual_size[i] / count - r.actual_size[i] / 2
+                self.display.append(np.abs(coords[:, None] - pixels).argmin(axis=0))
         eps = plan.epsilon
         sl = [slice(None)] * 3
         sl[self.axis] = self.plane_index
@@ -260,8 +271,9 @@ class Observer:
         self.host_fields = None                     # future of prefaulted (E, H) host arrays, large grids
         self.diagnostic_seconds = 0.
 
-    @staticmethod
-    def decimate(a):
+    def decimate(self, a):
+        if self.display is not None:
+            return a[self.display[0][:, None], self.display[1][None, :]]
         return a[::max(1, math.ceil(a.shape[0] / 256)), ::max(1, math.ceil(a.shape[1] / 256))]
 
     def barriers(self):
