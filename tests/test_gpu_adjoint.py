@@ -144,3 +144,35 @@ def test_plane_fields_match_the_forward_simulation_planes():
     fields = model(torch.tensor(eps, device='cuda'))['out'].fields.detach().cpu().numpy()
     plane = Simulation(project, epsilon=eps).run().field_monitor('out')
     assert rel(fields, plane['fields']) <= 1e-12
+
+
+@pytest.mark.parametrize('precision', ['float32', 'float64'])
+def test_interior_tiles_fast_path_is_the_general_path(monkeypatch, precision):
+    """A grid with whole interior tiles (80 x 40 x 30 cells, CPML 6): the reverse-step kernels' interior fast path
+    gives the general path's gradient bitwise, and (FP64) the oracle's."""
+    import torch
+    from torchfdtd_b200.adjoint import DifferentiableSimulation
+    from torchfdtd_b200.models import Monitor, Source
+    region = Region(dimension='3d', size=(4.0, 2.0, 1.5), mesh=.05, pml_cells=6, steps=30, precision=precision, backend='cuda')
+    project = Project(region=region, sources=[Source(center=(-.6, .05, 0), component='Ey', pulse_cycles=1, wavelength=.6)],
+                      monitors=[Monitor(center=(.5, .1, .1), component='Ey'), Monitor(center=(.2, -.2, -.1), component='Hz')])
+    plan = plan_grid(project)
+    assert plan.shape == (80, 40, 30)
+    dtype = torch.float32 if precision == 'float32' else torch.float64
+    eps = np.random.default_rng(5).uniform(1, 3, size=plan.shape)
+    w = np.random.default_rng(6).normal(size=(plan.steps, 2))
+    grads = {}
+    for fast in ('1', '0'):
+        monkeypatch.setenv('TFD_ADJ_FAST', fast)
+        model = DifferentiableSimulation(project)
+        epsilon = torch.tensor(eps, dtype=dtype, device='cuda', requires_grad=True)
+        result = model(epsilon)
+        (result.signals * torch.tensor(w, dtype=dtype, device='cuda')).sum().backward()
+        grads[fast] = epsilon.grad.cpu().numpy()
+        model.close()
+    np.testing.assert_array_equal(grads['1'], grads['0'])
+    assert np.abs(grads['1']).max() > 0
+    if precision == 'float64':
+        oracle = AdjointOracle(plan, eps)
+        oracle.forward()
+        assert rel(grads['1'], oracle.backward(w)) <= 1e-11

@@ -33,7 +33,7 @@ def test_saved_result_matches_the_reference_file(golden, tmp_path, name):
     with np.load(ref_path, allow_pickle=False) as want, np.load(out, allow_pickle=False) as got:
         assert sorted(got.files) == sorted(want.files)
         for key in want.files:
-            if key != 'project':     # the run here switched the region to the CUDA backend
+            if key not in ('project', 'summary'):     # JSON texts: compared field by field below
                 assert got[key].dtype == want[key].dtype and got[key].shape == want[key].shape, key
         saved = json.loads(str(got['project']))
         assert saved['region'].pop('backend') == 'cuda' and saved['region'].pop('cuda_kernel') == 'fused'

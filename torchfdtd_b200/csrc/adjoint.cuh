@@ -228,18 +228,84 @@ __device__ __forceinline__ T forward_curl(const AdjArgs<T> &A, const T *slot, in
 
 // ACTIVE: bitmask of advanced components (bit c: E_c, bit 3+c: H_c). Blocks of kAdjX x kAdjY cells of one
 // z plane (blockIdx.x, blockIdx.y: x and y tile; blockIdx.z: plane), so the x and y neighbours a cell reads
-// are mostly in its block's L1 lines. Reads parity q, writes q^1.
-// Part 1 of the reverse step: e_bar_new of the own cell, and S += e_bar_new * curl_b(H_n).
+// are mostly in its block's L1 lines. The tile origins are shifted by (xs, ys) cells (tile (bx, by) starts at
+// (bx kAdjX - xs, by kAdjY - ys)) so that a tile edge falls where the interior of the grid begins; interior
+// tiles take a fast path unless `fast` is 0 (the general path alone, for comparisons). Reads parity q,
+// writes q^1.
 constexpr int kAdjX = 32, kAdjY = 8;
 
-template <typename T, int ACTIVE>
-__global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_e(const __grid_constant__ AdjArgs<T> A, const T *__restrict__ slot, int q) {
+// Whether the CPML slab bounds b = {lo0, hi0, lo1, hi1} (half-open) meet the coordinates [lo, hi].
+__host__ __device__ __forceinline__ bool adj_meets(const int *b, int lo, int hi) {
+    return (lo < b[1] && b[0] <= hi) || (lo < b[3] && b[2] <= hi);
+}
+
+// An interior block: on every axis its cells lie in [1, n-2] (both neighbours inside the grid, no face or
+// periodic edge), and no CPML term applies to any D value the block's cells evaluate: the H family on
+// [lo + h_lo, hi] (h_lo = -1 for the e_bar update, which differences D(c-1) and D(c); HFAM false skips it) and
+// the E family on [lo, hi + e_hi]. There every D value is the plain transposed difference, and the general
+// path's arithmetic reduces to the operations of the fast path below, in the same order.
+template <typename T>
+__device__ __forceinline__ bool adj_interior(const AdjArgs<T> &A, int x0, int y0, int z, bool hfam, int e_hi) {
     const Grid<T> &g = A.g;
-    const int x = blockIdx.x * kAdjX + threadIdx.x;
-    const int y = blockIdx.y * kAdjY + threadIdx.y;
+    const int lo[3] = {max(x0, 0), max(y0, 0), z};
+    const int hi[3] = {min(x0 + kAdjX, g.n[0]) - 1, min(y0 + kAdjY, g.n[1]) - 1, z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (lo[a] < 1 || hi[a] > g.n[a] - 2) return false;
+        if (hfam && adj_meets(A.slab[1][a], lo[a] - 1, hi[a])) return false;
+        if (adj_meets(A.slab[0][a], lo[a], hi[a] + e_hi)) return false;
+    }
+    return true;
+}
+
+// Part 1 of the reverse step: e_bar_new of the own cell, and S += e_bar_new * curl_b(H_n).
+template <typename T, int ACTIVE>
+__global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_e(const __grid_constant__ AdjArgs<T> A, const T *__restrict__ slot, int q,
+                                                             int xs, int ys, int fast) {
+    const Grid<T> &g = A.g;
+    const int x0 = blockIdx.x * kAdjX - xs, y0 = blockIdx.y * kAdjY - ys;
+    const int x = x0 + threadIdx.x;
+    const int y = y0 + threadIdx.y;
     const int z = blockIdx.z;
-    if (x >= g.n[0] || y >= g.n[1]) return;
+    if (x < 0 || y < 0 || x >= g.n[0] || y >= g.n[1]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
+    if (ACTIVE == 63 && fast && g.active == 63 && adj_interior(A, x0, y0, z, true, 0)) {
+        const int co[3] = {x, y, z};
+#pragma unroll
+        for (int C = 0; C < 3; ++C) {
+            T contrib = T(0);
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const RevTerm t = rev_of(C, k);
+                const int a = t.axis, c = co[a];
+                const long long st = g.stride(a);
+                const T *hb = A.hb[q][t.out];
+                const T *mt = g.metric[1][a];
+                auto dh = [&](long long kk, int cc) -> T {
+                    const T dst = -g.cn * hb[kk];
+                    const T v = t.sign > 0 ? dst : -dst;
+                    return mt != nullptr ? v * mt[cc] : v;
+                };
+                contrib = contrib + dh(i - st, c - 1);      // src[c] += D(c-1)
+                contrib = contrib - dh(i, c);               // src[c] -= D(c)
+            }
+            const T e = A.eb[q][C][i] + contrib;
+            A.eb[q ^ 1][C][i] = e;
+            T acc = T(0);
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const Term t = term_of(C, k);
+                const int a = t.axis;
+                const T *h = slot + A.sH[t.in];
+                const T *mt = g.metric[0][a];
+                T d = h[i] - h[i - g.stride(a)];
+                if (mt != nullptr) d = d * mt[co[a]];
+                acc = acc + (t.sign > 0 ? d : -d);
+            }
+            A.S[C][i] = A.S[C][i] + e * acc;
+        }
+        return;
+    }
     if (ACTIVE & 1) {
         const T e = ebar_value<T, 0>(A, q, x, y, z, i, true);
         A.eb[q ^ 1][0][i] = e;
@@ -259,17 +325,42 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_e(const __grid_consta
 
 // Part 2: h_bar_new of the own cell from the e_bar_new that part 1 stored (own cell and +x/+y/+z).
 template <typename T, int ACTIVE>
-__global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_h(const __grid_constant__ AdjArgs<T> A, int q) {
+__global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_h(const __grid_constant__ AdjArgs<T> A, int q, int xs, int ys, int fast) {
     const Grid<T> &g = A.g;
-    const int x = blockIdx.x * kAdjX + threadIdx.x;
-    const int y = blockIdx.y * kAdjY + threadIdx.y;
+    const int x0 = blockIdx.x * kAdjX - xs, y0 = blockIdx.y * kAdjY - ys;
+    const int x = x0 + threadIdx.x;
+    const int y = y0 + threadIdx.y;
     const int z = blockIdx.z;
-    if (x >= g.n[0] || y >= g.n[1]) return;
+    if (x < 0 || y < 0 || x >= g.n[0] || y >= g.n[1]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
     T e[3] = {T(0), T(0), T(0)};
     if (ACTIVE & 1) e[0] = A.eb[q ^ 1][0][i];
     if (ACTIVE & 2) e[1] = A.eb[q ^ 1][1][i];
     if (ACTIVE & 4) e[2] = A.eb[q ^ 1][2][i];
+    if (ACTIVE == 63 && fast && g.active == 63 && adj_interior(A, x0, y0, z, false, 1)) {
+        const int co[3] = {x, y, z};
+#pragma unroll
+        for (int C = 0; C < 3; ++C) {
+            T contrib = T(0);
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const RevTerm t = rev_of(C, k);
+                const int a = t.axis, c = co[a];
+                const long long st = g.stride(a);
+                const T *ie = g.inv_eps[t.out];
+                const T *mt = g.metric[0][a];
+                auto de = [&](long long kk, int cc, T eb) -> T {
+                    const T dst = (g.cn * ie[kk]) * eb;
+                    const T v = t.sign > 0 ? dst : -dst;
+                    return mt != nullptr ? v * mt[cc] : v;
+                };
+                contrib = contrib + de(i, c, e[t.out]);                               // src[c] += D(c)
+                contrib = contrib - de(i + st, c + 1, A.eb[q ^ 1][t.out][i + st]);   // src[c] -= D(c+1)
+            }
+            A.hb[q ^ 1][C][i] = A.hb[q][C][i] + contrib;
+        }
+        return;
+    }
     if (ACTIVE & 8) A.hb[q ^ 1][0][i] = hbar_value<T, 0, true>(A, q, x, y, z, i, e);
     if (ACTIVE & 16) A.hb[q ^ 1][1][i] = hbar_value<T, 1, true>(A, q, x, y, z, i, e);
     if (ACTIVE & 32) A.hb[q ^ 1][2][i] = hbar_value<T, 2, true>(A, q, x, y, z, i, e);

@@ -2406,21 +2406,37 @@ int adjoint_step_t(tfd_adjoint *adj, const void *snapshot, const void *seeds, cu
         k_adjoint_seed<T><<<std::max(1, std::min(1184, (n_obs + 255) / 256)), 256, 0, s>>>(A, p->ptr<TraceDev>(p->L.trace_tab), n_obs,
                                                                                        (const T *)seeds, adj->q);
     const Grid<T> &g = A.g;
-    const dim3 grid((unsigned)((g.n[0] + kAdjX - 1) / kAdjX), (unsigned)((g.n[1] + kAdjY - 1) / kAdjY), (unsigned)g.n[2]);
+    // Tile origins shifted so that a tile edge falls on the first interior cell of x and y (after the low CPML
+    // slab; the e_bar update also differences D(c-1), one cell further): the interior tiles then take the fast
+    // path of the kernels whole.
+    auto low_end = [&](const int *b, int a) { return (b[1] > b[0] && b[0] < g.n[a] / 2) ? b[1] : 0; };
+    auto shift = [&](int a, bool e_kernel, int tile) {
+        int start = std::max(1, low_end(A.slab[0][a], a));
+        if (e_kernel) start = std::max(start, low_end(A.slab[1][a], a) + 1);
+        return (tile - start % tile) % tile;
+    };
+    const int exs = shift(0, true, kAdjX), eys = shift(1, true, kAdjY);
+    const int hxs = shift(0, false, kAdjX), hys = shift(1, false, kAdjY);
+    auto grid_of = [&](int xs, int ys) {
+        return dim3((unsigned)((g.n[0] + xs + kAdjX - 1) / kAdjX), (unsigned)((g.n[1] + ys + kAdjY - 1) / kAdjY), (unsigned)g.n[2]);
+    };
+    const dim3 ge = grid_of(exs, eys), gh = grid_of(hxs, hys);
+    const char *env = getenv("TFD_ADJ_FAST");
+    const int fast = (env && std::atoi(env) == 0) ? 0 : 1;
     const dim3 block(kAdjX, kAdjY);
     const T *slot = (const T *)snapshot;
     switch (p->desc.components) {
         case kMaskTM:
-            k_adjoint_e<T, kMaskTM><<<grid, block, 0, s>>>(A, slot, adj->q);
-            k_adjoint_h<T, kMaskTM><<<grid, block, 0, s>>>(A, adj->q);
+            k_adjoint_e<T, kMaskTM><<<ge, block, 0, s>>>(A, slot, adj->q, exs, eys, fast);
+            k_adjoint_h<T, kMaskTM><<<gh, block, 0, s>>>(A, adj->q, hxs, hys, fast);
             break;
         case kMaskTE:
-            k_adjoint_e<T, kMaskTE><<<grid, block, 0, s>>>(A, slot, adj->q);
-            k_adjoint_h<T, kMaskTE><<<grid, block, 0, s>>>(A, adj->q);
+            k_adjoint_e<T, kMaskTE><<<ge, block, 0, s>>>(A, slot, adj->q, exs, eys, fast);
+            k_adjoint_h<T, kMaskTE><<<gh, block, 0, s>>>(A, adj->q, hxs, hys, fast);
             break;
         default:
-            k_adjoint_e<T, kMaskAll><<<grid, block, 0, s>>>(A, slot, adj->q);
-            k_adjoint_h<T, kMaskAll><<<grid, block, 0, s>>>(A, adj->q);
+            k_adjoint_e<T, kMaskAll><<<ge, block, 0, s>>>(A, slot, adj->q, exs, eys, fast);
+            k_adjoint_h<T, kMaskAll><<<gh, block, 0, s>>>(A, adj->q, hxs, hys, fast);
             break;
     }
     TFD_CUDA(cudaGetLastError());

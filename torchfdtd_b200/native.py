@@ -173,12 +173,15 @@ def staging_ring(dtype, chunk_bytes=32 << 20, depth=4):
     return _STAGING[key]
 
 
-def host_buffer(shape, dtype, slab_bytes=64 << 20):
+def host_buffer(shape, dtype, slab_bytes=64 << 20, workers=8):
     """A pageable host array whose pages are already mapped (one byte written per 4 KiB page, a slab at a
     time), so that a later ``download(..., out=...)`` copies without page faults. Large arrays come from an
     anonymous mapping advised for transparent huge pages where the kernel offers them (one fault per 2 MiB
-    instead of per 4 KiB). Host memory only: meant to run on a helper thread while the device works."""
+    instead of per 4 KiB). The cost is the kernel zeroing each new page on the faulting core, so up to
+    ``workers`` threads touch the slabs (numpy releases the GIL while it writes). Host memory only: meant to
+    run on a helper thread while the device works."""
     import mmap
+    import os
     dtype = np.dtype(dtype)
     nbytes = int(np.prod(shape)) * dtype.itemsize
     out = None
@@ -192,8 +195,20 @@ def host_buffer(shape, dtype, slab_bytes=64 << 20):
     if out is None:
         out = np.empty(shape, dtype=dtype)
     raw = out.reshape(-1).view(np.uint8)
-    for a in range(0, raw.size, slab_bytes):
+    slabs = range(0, raw.size, slab_bytes)
+
+    def touch(a):
         raw[a:a + slab_bytes:4096] = 0
+
+    workers = max(1, min(workers, len(os.sched_getaffinity(0)) if hasattr(os, 'sched_getaffinity') else os.cpu_count() or 1,
+                         len(slabs)))
+    if workers > 1:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(workers) as pool:
+            list(pool.map(touch, slabs))
+    else:
+        for a in slabs:
+            touch(a)
     return out
 
 

@@ -490,64 +490,60 @@ class Simulation:
 
         plan, permittivity = self._run_plan()
         lap('plan')
-        helper, host_fields = None, None
+        helper, host_fields, ring = None, None, None
         shape, dtype = (*plan.shape, 3), np.dtype(plan.dtype)
         if math.prod(shape) * dtype.itemsize > LARGE_FIELD_BYTES:
-            # The result's host arrays are mapped on a helper thread (host memory only, no CUDA call, so it may
-            # overlap the plan creation, the uploads and the graph capture) while the main thread works on.
+            # Helper threads map the result's host arrays (host memory only, so it may overlap everything up to
+            # the download) and pin the download's staging ring (a CUDA host allocation: it overlaps the plan
+            # creation and the uploads and is waited for before the graph capture, which must not see it).
             from concurrent.futures import ThreadPoolExecutor
-            from .native import host_buffer
-            helper = ThreadPoolExecutor(max_workers=1)
+            from .native import host_buffer, staging_ring
+            helper = ThreadPoolExecutor(max_workers=2)
             host_fields = helper.submit(lambda: (host_buffer(shape, dtype), host_buffer(shape, dtype)))
-        variant, tuning = 0, None
-        if launch == 'auto':
-            if plan.dimension == '3d' and kernel in ('auto', 'march'):
-                from .tuning import select_launch
-                try:
-                    tuning = select_launch(plan)
-                    variant = tuning.choice
-                except ValueError as exc:          # too few steps to tune, or no marching kernel for this scene
-                    tuning = dict(skipped=str(exc))
-        elif launch is not None:
-            variant = int(launch)
-        if tuning is not None:
-            lap('launch_tuning')
+            ring = helper.submit(staging_ring, torch.float32 if dtype == np.float32 else torch.float64)
+        grid, graphs = None, {}
         try:
+            variant, tuning = 0, None
+            if launch == 'auto':
+                if plan.dimension == '3d' and kernel in ('auto', 'march'):
+                    from .tuning import select_launch
+                    try:
+                        tuning = select_launch(plan)
+                        variant = tuning.choice
+                    except ValueError as exc:          # too few steps to tune, or no marching kernel for this scene
+                        tuning = dict(skipped=str(exc))
+            elif launch is not None:
+                variant = int(launch)
+            if tuning is not None:
+                lap('launch_tuning')
             grid = NativeGrid(plan, kernel=kernel, variant=variant, permittivity=permittivity)
-        except BaseException:
-            if helper is not None:
-                helper.shutdown(wait=True)
-            raise
-        phases.update(grid.timing)
-        mark[0] = time.perf_counter()
-        free, _ = torch.cuda.mem_get_info()
-        observer = Observer(p, plan, grid)
-        observer.host_fields = host_fields
-        lap('observer')
-        if host_fields is not None:
-            from .native import staging_ring
-            staging_ring(grid.torch_dtype)          # pinned once per process, before any capture
-            lap('staging_ring')
-        graphs = {}
-        width = 1
-        stream = torch.cuda.Stream()
-        stream.wait_stream(torch.cuda.current_stream())
-        if cuda_graph:
-            width = min(cuda_graph_steps, r.steps)
-            with torch.cuda.stream(stream):
-                # One eager step loads the kernels before capture; the state is then zeroed.
-                grid.step(1, stream)
-                grid.reset()
-                stream.synchronize()
-                lap('warm_step_and_reset')
-                graphs = capture_graphs(lambda count: grid.step(count, stream), {1, width})
+            phases.update(grid.timing)
+            mark[0] = time.perf_counter()
+            free, _ = torch.cuda.mem_get_info()
+            observer = Observer(p, plan, grid)
+            observer.host_fields = host_fields
+            lap('observer')
+            if ring is not None:
+                ring.result()                           # pinned once per process, before any capture
+                lap('staging_ring')
+            width = 1
+            stream = torch.cuda.Stream()
+            stream.wait_stream(torch.cuda.current_stream())
+            if cuda_graph:
+                width = min(cuda_graph_steps, r.steps)
+                with torch.cuda.stream(stream):
+                    # One eager step loads the kernels before capture; the state is then zeroed.
+                    grid.step(1, stream)
+                    grid.reset()
+                    stream.synchronize()
+                    lap('warm_step_and_reset')
+                    graphs = capture_graphs(lambda count: grid.step(count, stream), {1, width})
+                torch.cuda.synchronize()
             torch.cuda.synchronize()
-        torch.cuda.synchronize()
-        lap('graph_capture')
-        setup_seconds = time.perf_counter() - started
-        compute_start = time.perf_counter()
-        completed, termination_reason, replays = 0, 'max_steps', 0
-        try:
+            lap('graph_capture')
+            setup_seconds = time.perf_counter() - started
+            compute_start = time.perf_counter()
+            completed, termination_reason, replays = 0, 'max_steps', 0
             with torch.cuda.stream(stream):
                 for target, advance in observation_schedule(r.steps, width, observer.barriers()):
                     if cancel is not None and cancel.is_set():
@@ -571,9 +567,10 @@ class Simulation:
                                      launch_variant=variant or None,
                                      launch_tuning=tuning.as_dict() if hasattr(tuning, 'as_dict') else tuning)
         finally:
-            # The helper thread (pinned staging ring, mapped result arrays) is joined on every path.
+            # The helper threads (pinned staging ring, mapped result arrays) are joined on every path.
             if helper is not None:
                 helper.shutdown(wait=True)
             graphs.clear()
-            grid.close()
+            if grid is not None:
+                grid.close()
         return result
