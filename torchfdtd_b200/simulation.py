@@ -492,14 +492,15 @@ class Simulation:
         lap('plan')
         helper, host_fields, ring = None, None, None
         shape, dtype = (*plan.shape, 3), np.dtype(plan.dtype)
-        if math.prod(shape) * dtype.itemsize > LARGE_FIELD_BYTES:
-            # Helper threads map the result's host arrays (host memory only, so it may overlap everything up to
-            # the download) and pin the download's staging ring (a CUDA host allocation: it overlaps the plan
-            # creation and the uploads and is waited for before the graph capture, which must not see it).
+        large = math.prod(shape) * dtype.itemsize > LARGE_FIELD_BYTES
+        if large:
+            # Helper threads pin the download's staging ring (a CUDA host allocation: it overlaps the plan creation
+            # and the uploads and is waited for before the graph capture, which must not see it) and, once the
+            # device arena exists, map the result's host arrays (host memory only; started after the arena
+            # because the page zeroing slows a concurrent device allocation).
             from concurrent.futures import ThreadPoolExecutor
             from .native import host_buffer, staging_ring
             helper = ThreadPoolExecutor(max_workers=2)
-            host_fields = helper.submit(lambda: (host_buffer(shape, dtype), host_buffer(shape, dtype)))
             ring = helper.submit(staging_ring, torch.float32 if dtype == np.float32 else torch.float64)
         grid, graphs = None, {}
         try:
@@ -517,6 +518,8 @@ class Simulation:
             if tuning is not None:
                 lap('launch_tuning')
             grid = NativeGrid(plan, kernel=kernel, variant=variant, permittivity=permittivity)
+            if large:
+                host_fields = helper.submit(lambda: (host_buffer(shape, dtype), host_buffer(shape, dtype)))
             phases.update(grid.timing)
             mark[0] = time.perf_counter()
             free, _ = torch.cuda.mem_get_info()
