@@ -270,7 +270,28 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_e(const __grid_consta
     if (x < 0 || y < 0 || x >= g.n[0] || y >= g.n[1]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
     if (ACTIVE == 63 && fast && g.active == 63 && adj_interior(A, x0, y0, z, true, 0)) {
+        // Every input is loaded before the first store (the stores could alias the loads for the compiler, which
+        // would otherwise serialise the three components' memory round trips).
         const int co[3] = {x, y, z};
+        const long long st[3] = {1, g.pitch, g.plane};
+        T hc[3], sc[3], hm[3][2], sm[3][2], eb[3], S0[3];
+#pragma unroll
+        for (int o = 0; o < 3; ++o) {
+            hc[o] = __ldg(A.hb[q][o] + i);
+            sc[o] = __ldg(slot + A.sH[o] + i);
+            eb[o] = __ldg(A.eb[q][o] + i);
+            S0[o] = A.S[o][i];
+        }
+#pragma unroll
+        for (int C = 0; C < 3; ++C)
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const RevTerm t = rev_of(C, k);
+                hm[C][k] = __ldg(A.hb[q][t.out] + i - st[t.axis]);
+                const Term f = term_of(C, k);
+                sm[C][k] = __ldg(slot + A.sH[f.in] + i - st[f.axis]);
+            }
+        T e[3], s[3];
 #pragma unroll
         for (int C = 0; C < 3; ++C) {
             T contrib = T(0);
@@ -278,31 +299,32 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_e(const __grid_consta
             for (int k = 0; k < 2; ++k) {
                 const RevTerm t = rev_of(C, k);
                 const int a = t.axis, c = co[a];
-                const long long st = g.stride(a);
-                const T *hb = A.hb[q][t.out];
                 const T *mt = g.metric[1][a];
-                auto dh = [&](long long kk, int cc) -> T {
-                    const T dst = -g.cn * hb[kk];
+                auto dh = [&](T h, int cc) -> T {
+                    const T dst = -g.cn * h;
                     const T v = t.sign > 0 ? dst : -dst;
                     return mt != nullptr ? v * mt[cc] : v;
                 };
-                contrib = contrib + dh(i - st, c - 1);      // src[c] += D(c-1)
-                contrib = contrib - dh(i, c);               // src[c] -= D(c)
+                contrib = contrib + dh(hm[C][k], c - 1);      // src[c] += D(c-1)
+                contrib = contrib - dh(hc[t.out], c);         // src[c] -= D(c)
             }
-            const T e = A.eb[q][C][i] + contrib;
-            A.eb[q ^ 1][C][i] = e;
+            e[C] = eb[C] + contrib;
             T acc = T(0);
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
                 const Term t = term_of(C, k);
                 const int a = t.axis;
-                const T *h = slot + A.sH[t.in];
                 const T *mt = g.metric[0][a];
-                T d = h[i] - h[i - g.stride(a)];
+                T d = sc[t.in] - sm[C][k];
                 if (mt != nullptr) d = d * mt[co[a]];
                 acc = acc + (t.sign > 0 ? d : -d);
             }
-            A.S[C][i] = A.S[C][i] + e * acc;
+            s[C] = S0[C] + e[C] * acc;
+        }
+#pragma unroll
+        for (int C = 0; C < 3; ++C) {
+            A.eb[q ^ 1][C][i] = e[C];
+            A.S[C][i] = s[C];
         }
         return;
     }
@@ -339,6 +361,22 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_h(const __grid_consta
     if (ACTIVE & 4) e[2] = A.eb[q ^ 1][2][i];
     if (ACTIVE == 63 && fast && g.active == 63 && adj_interior(A, x0, y0, z, false, 1)) {
         const int co[3] = {x, y, z};
+        const long long st[3] = {1, g.pitch, g.plane};
+        T ep[3][2], ie0[3], iep[3][2], hb[3];
+#pragma unroll
+        for (int o = 0; o < 3; ++o) {
+            ie0[o] = __ldg(g.inv_eps[o] + i);
+            hb[o] = __ldg(A.hb[q][o] + i);
+        }
+#pragma unroll
+        for (int C = 0; C < 3; ++C)
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const RevTerm t = rev_of(C, k);
+                ep[C][k] = __ldg(A.eb[q ^ 1][t.out] + i + st[t.axis]);
+                iep[C][k] = __ldg(g.inv_eps[t.out] + i + st[t.axis]);
+            }
+        T out[3];
 #pragma unroll
         for (int C = 0; C < 3; ++C) {
             T contrib = T(0);
@@ -346,19 +384,19 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_h(const __grid_consta
             for (int k = 0; k < 2; ++k) {
                 const RevTerm t = rev_of(C, k);
                 const int a = t.axis, c = co[a];
-                const long long st = g.stride(a);
-                const T *ie = g.inv_eps[t.out];
                 const T *mt = g.metric[0][a];
-                auto de = [&](long long kk, int cc, T eb) -> T {
-                    const T dst = (g.cn * ie[kk]) * eb;
+                auto de = [&](T ie, int cc, T eb) -> T {
+                    const T dst = (g.cn * ie) * eb;
                     const T v = t.sign > 0 ? dst : -dst;
                     return mt != nullptr ? v * mt[cc] : v;
                 };
-                contrib = contrib + de(i, c, e[t.out]);                               // src[c] += D(c)
-                contrib = contrib - de(i + st, c + 1, A.eb[q ^ 1][t.out][i + st]);   // src[c] -= D(c+1)
+                contrib = contrib + de(ie0[t.out], c, e[t.out]);            // src[c] += D(c)
+                contrib = contrib - de(iep[C][k], c + 1, ep[C][k]);        // src[c] -= D(c+1)
             }
-            A.hb[q ^ 1][C][i] = A.hb[q][C][i] + contrib;
+            out[C] = hb[C] + contrib;
         }
+#pragma unroll
+        for (int C = 0; C < 3; ++C) A.hb[q ^ 1][C][i] = out[C];
         return;
     }
     if (ACTIVE & 8) A.hb[q ^ 1][0][i] = hbar_value<T, 0, true>(A, q, x, y, z, i, e);

@@ -2415,8 +2415,11 @@ int adjoint_step_t(tfd_adjoint *adj, const void *snapshot, const void *seeds, cu
         if (e_kernel) start = std::max(start, low_end(A.slab[1][a], a) + 1);
         return (tile - start % tile) % tile;
     };
-    const int exs = shift(0, true, kAdjX), eys = shift(1, true, kAdjY);
-    const int hxs = shift(0, false, kAdjX), hys = shift(1, false, kAdjY);
+    // TFD_ADJ_XSHIFT=0 keeps the x tiles at multiples of 32 (rows aligned to 128 bytes) for comparisons.
+    const char *xenv = getenv("TFD_ADJ_XSHIFT");
+    const bool xshift = !(xenv && std::atoi(xenv) == 0);
+    const int exs = xshift ? shift(0, true, kAdjX) : 0, eys = shift(1, true, kAdjY);
+    const int hxs = xshift ? shift(0, false, kAdjX) : 0, hys = shift(1, false, kAdjY);
     auto grid_of = [&](int xs, int ys) {
         return dim3((unsigned)((g.n[0] + xs + kAdjX - 1) / kAdjX), (unsigned)((g.n[1] + ys + kAdjY - 1) / kAdjY), (unsigned)g.n[2]);
     };

@@ -147,13 +147,22 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
         const int y = (int)(traces[t].offset / pitch);
         band_traces |= y >= r0 && y < r1;
     }
-    auto add_sources = [&](unsigned mask, int x, int y, long long n, T v) {
+    // Soft sources of a family, after its update pass: the cells of each source box in the band get the source
+    // value added, one source after the other (ascending index, the order of the strip kernels), so each cell
+    // sees the same additions in the same order as an update that adds them in place.
+    auto add_sources = [&](unsigned mask, T *field, long long n) {
         for (; mask; mask &= mask - 1) {
             const int t = __ffs(mask) - 1;
             const SourceTerm &s = g.src[t];
-            if (x >= s.lo[0] && x < s.hi[0] && y >= s.lo[1] && y < s.hi[1]) v = v + g.src_values[(long long)t * g.steps + n];
+            const int ylo = max(s.lo[1], r0), yhi = min(s.hi[1], r1), xlo = max(s.lo[0], 0), xhi = min(s.hi[0], nx);
+            const int w = xhi - xlo, cnt = (w > 0 && yhi > ylo) ? w * (yhi - ylo) : 0;
+            const T v = g.src_values[(long long)t * g.steps + n];
+            __syncthreads();
+            for (int q = tid; q < cnt; q += kCl2dThreads) {
+                const int e = (ylo - r0 + q / w) * W + xlo + q % w;
+                field[e] = field[e] + v;
+            }
         }
-        return v;
     };
     const bool pec_x = g.pec_on[0] != 0, pec_y = g.pec_on[1] != 0;
     const T pneg_x = g.pec_neg[0], pneg_y = g.pec_neg[1], cn = g.cn;
@@ -199,7 +208,6 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
                 }
                 acc = acc + (-d);
                 T ez = Ez[e] + (cn * ie[e]) * acc;
-                if (src_e) ez = add_sources(src_e, x, y, n, ez);
                 Ez[e] = ez;
             }
             yl += dq;
@@ -209,6 +217,9 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
                 ++yl;
             }
         }
+        if (src_e) add_sources(src_e, Ez, n);             // CTA-uniform
+        // A CTA enters the cluster barrier once all its warps are done.
+        __syncthreads();
         cluster.sync();
         // ---- H phase ----
         for (int yl = yl_first, xs = xs_first; yl < rows;) {
@@ -250,8 +261,6 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
                 }
                 acc = T(0) + (-d);
                 T hyn = Hy[e] - cn * acc;
-                if (src_hx) hxn = add_sources(src_hx, x, h, n, hxn);
-                if (src_hy) hyn = add_sources(src_hy, x, h, n, hyn);
                 Hx[e] = hxn;
                 Hy[e] = hyn;
             }
@@ -262,6 +271,8 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
                 ++yl;
             }
         }
+        if (src_hx) add_sources(src_hx, Hx, n);
+        if (src_hy) add_sources(src_hy, Hy, n);
         if (band_traces) {
             // Point traces of step n sampled by the rank that owns the cell (a CTA-uniform branch).
             __syncthreads();
@@ -277,6 +288,7 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
                 trace_out[n * n_traces + t] = v;
             }
         }
+        __syncthreads();
         cluster.sync();
     }
     // Write the band back at the parity of the step count reached, and the counter.
