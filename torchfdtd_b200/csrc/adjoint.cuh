@@ -239,23 +239,149 @@ __host__ __device__ __forceinline__ bool adj_meets(const int *b, int lo, int hi)
     return (lo < b[1] && b[0] <= hi) || (lo < b[3] && b[2] <= hi);
 }
 
-// An interior block: on every axis its cells lie in [1, n-2] (both neighbours inside the grid, no face or
-// periodic edge), and no CPML term applies to any D value the block's cells evaluate: the H family on
-// [lo + h_lo, hi] (h_lo = -1 for the e_bar update, which differences D(c-1) and D(c); HFAM false skips it) and
-// the E family on [lo, hi + e_hi]. There every D value is the plain transposed difference, and the general
-// path's arithmetic reduces to the operations of the fast path below, in the same order.
+// Block classes for the fast paths. On x and y every cell of the block lies in [1, n-2] (both neighbours
+// inside the grid, no face or periodic edge) and no CPML term applies to any D value the block's cells
+// evaluate: the H family on [lo - 1, hi] (HFAM: the e_bar update differences D(c-1) and D(c)) and the E family
+// on [lo, hi + e_hi]; the plane z lies in [1, nz-2]. Class 1: no CPML term on z either, so every D value is the
+// plain transposed difference; class 2: the z terms meet a z slab and go through the general D functions.
+// Class 0: the general path. In classes 1 and 2 the general path's arithmetic reduces to the fast path's
+// operations, in the same order.
 template <typename T>
-__device__ __forceinline__ bool adj_interior(const AdjArgs<T> &A, int x0, int y0, int z, bool hfam, int e_hi) {
+__device__ __forceinline__ int adj_class(const AdjArgs<T> &A, int x0, int y0, int z, bool hfam, int e_hi) {
     const Grid<T> &g = A.g;
     const int lo[3] = {max(x0, 0), max(y0, 0), z};
     const int hi[3] = {min(x0 + kAdjX, g.n[0]) - 1, min(y0 + kAdjY, g.n[1]) - 1, z};
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        if (lo[a] < 1 || hi[a] > g.n[a] - 2) return false;
-        if (hfam && adj_meets(A.slab[1][a], lo[a] - 1, hi[a])) return false;
-        if (adj_meets(A.slab[0][a], lo[a], hi[a] + e_hi)) return false;
+    for (int a = 0; a < 3; ++a)
+        if (lo[a] < 1 || hi[a] > g.n[a] - 2) return 0;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        if (hfam && adj_meets(A.slab[1][a], lo[a] - 1, hi[a])) return 0;
+        if (adj_meets(A.slab[0][a], lo[a], hi[a] + e_hi)) return 0;
     }
-    return true;
+    const bool zslab = (hfam && adj_meets(A.slab[1][2], z - 1, z)) || adj_meets(A.slab[0][2], z, z + e_hi);
+    return zslab ? 2 : 1;
+}
+
+// e_bar_new and the sensitivity of the three components of an interior cell (classes 1 and 2 above). Every
+// input of the plain terms is loaded before the first store (the stores could alias the loads for the
+// compiler, which would otherwise serialise the three components' memory round trips).
+template <typename T, bool ZGEN>
+__device__ __forceinline__ void adj_e_fast(const AdjArgs<T> &A, const T *__restrict__ slot, int q, int x, int y, int z, long long i) {
+    const Grid<T> &g = A.g;
+    const int co[3] = {x, y, z};
+    T hc[3], sc[3], hm[3][2], smv[3][2], eb[3], S0[3];
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+        hc[o] = __ldg(A.hb[q][o] + i);
+        sc[o] = __ldg(slot + A.sH[o] + i);
+        eb[o] = __ldg(A.eb[q][o] + i);
+        S0[o] = A.S[o][i];
+    }
+#pragma unroll
+    for (int C = 0; C < 3; ++C)
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const RevTerm t = rev_of(C, k);
+            if (!(ZGEN && t.axis == 2)) hm[C][k] = __ldg(A.hb[q][t.out] + i - g.stride(t.axis));
+            const Term f = term_of(C, k);
+            smv[C][k] = __ldg(slot + A.sH[f.in] + i - g.stride(f.axis));
+        }
+    T e[3], s[3];
+#pragma unroll
+    for (int C = 0; C < 3; ++C) {
+        T contrib = T(0);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const RevTerm t = rev_of(C, k);
+            const int a = t.axis, c = co[a];
+            if (ZGEN && a == 2) {
+                contrib = contrib + d_h(A, q, t, x, y, z - 1, i - g.plane, false);    // src[c] += D(c-1)
+                contrib = contrib - d_h(A, q, t, x, y, z, i, true);                  // src[c] -= D(c)
+                continue;
+            }
+            const T *mt = g.metric[1][a];
+            auto dh = [&](T h, int cc) -> T {
+                const T dst = -g.cn * h;
+                const T v = t.sign > 0 ? dst : -dst;
+                return mt != nullptr ? v * mt[cc] : v;
+            };
+            contrib = contrib + dh(hm[C][k], c - 1);      // src[c] += D(c-1)
+            contrib = contrib - dh(hc[t.out], c);         // src[c] -= D(c)
+        }
+        e[C] = eb[C] + contrib;
+        T acc = T(0);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const Term t = term_of(C, k);
+            const int a = t.axis;
+            const T *mt = g.metric[0][a];
+            T d = sc[t.in] - smv[C][k];
+            if (mt != nullptr) d = d * mt[co[a]];
+            if (ZGEN && a == 2 && A.sPsiE[2][t.j] >= 0) {
+                const int r = adj_slab_row(A.slab[0][2], z);
+                if (r >= 0) {
+                    const long long p = g.psi_index(2, x, y, z, r, g.rows[0][2]);
+                    const T mem = slot[A.sPsiE[2][t.j] + p] * g.cb[0][2][z] + g.cc[0][2][z] * d;
+                    d = d * g.ck[0][2][z] + mem;
+                }
+            }
+            acc = acc + (t.sign > 0 ? d : -d);
+        }
+        s[C] = S0[C] + e[C] * acc;
+    }
+#pragma unroll
+    for (int C = 0; C < 3; ++C) {
+        A.eb[q ^ 1][C][i] = e[C];
+        A.S[C][i] = s[C];
+    }
+}
+
+// h_bar_new of the three components of an interior cell; e_own: the cell's e_bar_new.
+template <typename T, bool ZGEN>
+__device__ __forceinline__ void adj_h_fast(const AdjArgs<T> &A, int q, int x, int y, int z, long long i, const T *e_own) {
+    const Grid<T> &g = A.g;
+    const int co[3] = {x, y, z};
+    T ep[3][2], ie0[3], iep[3][2], hb[3];
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+        ie0[o] = __ldg(g.inv_eps[o] + i);
+        hb[o] = __ldg(A.hb[q][o] + i);
+    }
+#pragma unroll
+    for (int C = 0; C < 3; ++C)
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const RevTerm t = rev_of(C, k);
+            ep[C][k] = __ldg(A.eb[q ^ 1][t.out] + i + g.stride(t.axis));
+            if (!(ZGEN && t.axis == 2)) iep[C][k] = __ldg(g.inv_eps[t.out] + i + g.stride(t.axis));
+        }
+    T out[3];
+#pragma unroll
+    for (int C = 0; C < 3; ++C) {
+        T contrib = T(0);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const RevTerm t = rev_of(C, k);
+            const int a = t.axis, c = co[a];
+            if (ZGEN && a == 2) {
+                contrib = contrib + d_e(A, q, t, x, y, z, i, e_own[t.out], true);                   // src[c] += D(c)
+                contrib = contrib - d_e(A, q, t, x, y, z + 1, i + g.plane, ep[C][k], false);       // src[c] -= D(c+1)
+                continue;
+            }
+            const T *mt = g.metric[0][a];
+            auto de = [&](T ie, int cc, T eb) -> T {
+                const T dst = (g.cn * ie) * eb;
+                const T v = t.sign > 0 ? dst : -dst;
+                return mt != nullptr ? v * mt[cc] : v;
+            };
+            contrib = contrib + de(ie0[t.out], c, e_own[t.out]);       // src[c] += D(c)
+            contrib = contrib - de(iep[C][k], c + 1, ep[C][k]);        // src[c] -= D(c+1)
+        }
+        out[C] = hb[C] + contrib;
+    }
+#pragma unroll
+    for (int C = 0; C < 3; ++C) A.hb[q ^ 1][C][i] = out[C];
 }
 
 // Part 1 of the reverse step: e_bar_new of the own cell, and S += e_bar_new * curl_b(H_n).
@@ -269,64 +395,16 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_e(const __grid_consta
     const int z = blockIdx.z;
     if (x < 0 || y < 0 || x >= g.n[0] || y >= g.n[1]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
-    if (ACTIVE == 63 && fast && g.active == 63 && adj_interior(A, x0, y0, z, true, 0)) {
-        // Every input is loaded before the first store (the stores could alias the loads for the compiler, which
-        // would otherwise serialise the three components' memory round trips).
-        const int co[3] = {x, y, z};
-        const long long st[3] = {1, g.pitch, g.plane};
-        T hc[3], sc[3], hm[3][2], sm[3][2], eb[3], S0[3];
-#pragma unroll
-        for (int o = 0; o < 3; ++o) {
-            hc[o] = __ldg(A.hb[q][o] + i);
-            sc[o] = __ldg(slot + A.sH[o] + i);
-            eb[o] = __ldg(A.eb[q][o] + i);
-            S0[o] = A.S[o][i];
+    if (ACTIVE == 63 && fast && g.active == 63) {
+        const int cls = adj_class(A, x0, y0, z, true, 0);
+        if (cls == 1) {
+            adj_e_fast<T, false>(A, slot, q, x, y, z, i);
+            return;
         }
-#pragma unroll
-        for (int C = 0; C < 3; ++C)
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const RevTerm t = rev_of(C, k);
-                hm[C][k] = __ldg(A.hb[q][t.out] + i - st[t.axis]);
-                const Term f = term_of(C, k);
-                sm[C][k] = __ldg(slot + A.sH[f.in] + i - st[f.axis]);
-            }
-        T e[3], s[3];
-#pragma unroll
-        for (int C = 0; C < 3; ++C) {
-            T contrib = T(0);
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const RevTerm t = rev_of(C, k);
-                const int a = t.axis, c = co[a];
-                const T *mt = g.metric[1][a];
-                auto dh = [&](T h, int cc) -> T {
-                    const T dst = -g.cn * h;
-                    const T v = t.sign > 0 ? dst : -dst;
-                    return mt != nullptr ? v * mt[cc] : v;
-                };
-                contrib = contrib + dh(hm[C][k], c - 1);      // src[c] += D(c-1)
-                contrib = contrib - dh(hc[t.out], c);         // src[c] -= D(c)
-            }
-            e[C] = eb[C] + contrib;
-            T acc = T(0);
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const Term t = term_of(C, k);
-                const int a = t.axis;
-                const T *mt = g.metric[0][a];
-                T d = sc[t.in] - sm[C][k];
-                if (mt != nullptr) d = d * mt[co[a]];
-                acc = acc + (t.sign > 0 ? d : -d);
-            }
-            s[C] = S0[C] + e[C] * acc;
+        if (cls == 2) {
+            adj_e_fast<T, true>(A, slot, q, x, y, z, i);
+            return;
         }
-#pragma unroll
-        for (int C = 0; C < 3; ++C) {
-            A.eb[q ^ 1][C][i] = e[C];
-            A.S[C][i] = s[C];
-        }
-        return;
     }
     if (ACTIVE & 1) {
         const T e = ebar_value<T, 0>(A, q, x, y, z, i, true);
@@ -359,45 +437,16 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_h(const __grid_consta
     if (ACTIVE & 1) e[0] = A.eb[q ^ 1][0][i];
     if (ACTIVE & 2) e[1] = A.eb[q ^ 1][1][i];
     if (ACTIVE & 4) e[2] = A.eb[q ^ 1][2][i];
-    if (ACTIVE == 63 && fast && g.active == 63 && adj_interior(A, x0, y0, z, false, 1)) {
-        const int co[3] = {x, y, z};
-        const long long st[3] = {1, g.pitch, g.plane};
-        T ep[3][2], ie0[3], iep[3][2], hb[3];
-#pragma unroll
-        for (int o = 0; o < 3; ++o) {
-            ie0[o] = __ldg(g.inv_eps[o] + i);
-            hb[o] = __ldg(A.hb[q][o] + i);
+    if (ACTIVE == 63 && fast && g.active == 63) {
+        const int cls = adj_class(A, x0, y0, z, false, 1);
+        if (cls == 1) {
+            adj_h_fast<T, false>(A, q, x, y, z, i, e);
+            return;
         }
-#pragma unroll
-        for (int C = 0; C < 3; ++C)
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const RevTerm t = rev_of(C, k);
-                ep[C][k] = __ldg(A.eb[q ^ 1][t.out] + i + st[t.axis]);
-                iep[C][k] = __ldg(g.inv_eps[t.out] + i + st[t.axis]);
-            }
-        T out[3];
-#pragma unroll
-        for (int C = 0; C < 3; ++C) {
-            T contrib = T(0);
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const RevTerm t = rev_of(C, k);
-                const int a = t.axis, c = co[a];
-                const T *mt = g.metric[0][a];
-                auto de = [&](T ie, int cc, T eb) -> T {
-                    const T dst = (g.cn * ie) * eb;
-                    const T v = t.sign > 0 ? dst : -dst;
-                    return mt != nullptr ? v * mt[cc] : v;
-                };
-                contrib = contrib + de(ie0[t.out], c, e[t.out]);            // src[c] += D(c)
-                contrib = contrib - de(iep[C][k], c + 1, ep[C][k]);        // src[c] -= D(c+1)
-            }
-            out[C] = hb[C] + contrib;
+        if (cls == 2) {
+            adj_h_fast<T, true>(A, q, x, y, z, i, e);
+            return;
         }
-#pragma unroll
-        for (int C = 0; C < 3; ++C) A.hb[q ^ 1][C][i] = out[C];
-        return;
     }
     if (ACTIVE & 8) A.hb[q ^ 1][0][i] = hbar_value<T, 0, true>(A, q, x, y, z, i, e);
     if (ACTIVE & 16) A.hb[q ^ 1][1][i] = hbar_value<T, 1, true>(A, q, x, y, z, i, e);
