@@ -1026,6 +1026,10 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
         MarchMix &mx = p->march_mix;
         mx = MarchMix{};
         mx.ix0 = ix0; mx.ix1 = ix1; mx.iy0 = iy0; mx.iy1 = iy1;
+        // x-boundary tiles of the interior y range on the pure planes take the x-tier body (non-periodic grids;
+        // TFD_MARCH_XBODY=0 gives them the general body, for comparisons).
+        const char *xenv = getenv("TFD_MARCH_XBODY");
+        mx.xband = (xenv && std::atoi(xenv) == 0) ? 0 : 1;
         mx.zb[0] = 0; mx.zb[1] = za; mx.zb[2] = zb; mx.zb[3] = nzp;
         int total = 0;
         for (int q = 0; q < 3; ++q) {

@@ -446,6 +446,108 @@ __device__ __forceinline__ void march_h_row(const Grid<T> &g, const T *ep, const
     hz = hs[2 * HS + sh] - g.cn * acc;
 }
 
+// The x tier of the x-boundary body (MODE 5): a row of a tile that meets an x slab or an x face but no y / z
+// slab or face. Only the x differences carry CPML memories (per lane: rx >= 0) and the x faces are selects;
+// the y and z differences are plain. The operations are those of march_e_row / march_h_row with the y and z
+// terms plain, in the same order. rx, q: this lane's x slab row and coefficients (fixed over the tile);
+// ix: the memory element of the lane's cell; po / pn: old / new parity offsets of the E-family x memories.
+template <typename T, int SAMPLES, int D>
+__device__ __forceinline__ void march_e_xtier(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, bool xin, int rx,
+                                              int ix, int po, int pn, bool own, const Coef<T> &q, T &ex, T &ey, T &ez) {
+    using S = MarchShape<T, SAMPLES, D>;
+    constexpr int HS = S::BOXH_STRIDE / sizeof(T);
+    constexpr int ES = S::BOXE_STRIDE / sizeof(T);
+    const T *Hx = hk, *Hy = hk + HS, *Hz = hk + 2 * HS;
+    const bool ax = rx >= 0;
+    T o0 = T(0), o1 = T(0);
+    if (ax) {
+        o0 = g.psiE[0][0][0][po + ix];
+        o1 = g.psiE[0][0][1][po + ix];
+    }
+    T d, acc, m;
+    // Ex: (y, Hz, +), (z, Hy, -)
+    d = Hz[s] - Hz[s - S::BXW];
+    acc = T(0);
+    acc = acc + d;
+    d = Hy[s] - hm[HS + s];
+    acc = acc + (-d);
+    ex = ek[se] + (g.cn * ek[3 * ES + se]) * acc;
+    // Ey: (x, Hz, -, j0), (z, Hx, +)
+    d = xin ? Hz[s] - Hz[s - 1] : T(0);
+    if (ax) {
+        m = o0 * q.b + q.c * d;
+        if (own) g.psiE[0][0][0][pn + ix] = m;
+        d = d * q.k + m;
+    }
+    acc = T(0);
+    acc = acc + (-d);
+    d = Hx[s] - hm[s];
+    acc = acc + d;
+    ey = ek[ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? 1 : 0)) * ES + se]) * acc;
+    // Ez: (x, Hy, +, j1), (y, Hx, -)
+    d = xin ? Hy[s] - Hy[s - 1] : T(0);
+    if (ax) {
+        m = o1 * q.b + q.c * d;
+        if (own) g.psiE[0][0][1][pn + ix] = m;
+        d = d * q.k + m;
+    }
+    acc = T(0);
+    acc = acc + d;
+    d = Hx[s] - Hx[s - S::BXW];
+    acc = acc + (-d);
+    ez = ek[2 * ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? 2 : 0)) * ES + se]) * acc;
+}
+
+// ep / ec: E_new of the cell's plane and of the plane above; xn: the +x neighbour exists (else the PEC ghost
+// term or 0); the H-family x memories are updated in place.
+template <typename T, int SAMPLES, int D>
+__device__ __forceinline__ void march_h_xtier(const Grid<T> &g, const T *ep, const T *ec, const T *hs, int sh, int e, bool xn, int rx,
+                                              int ix, const Coef<T> &q, T &hx, T &hy, T &hz) {
+    using S = MarchShape<T, SAMPLES, D>;
+    constexpr int HS = S::BOXH_STRIDE / sizeof(T);
+    constexpr int EB = S::EBUF;
+    const bool ax = xn && rx >= 0;
+    T o0 = T(0), o1 = T(0);
+    if (ax) {
+        o0 = g.psiH[0][0][ix];
+        o1 = g.psiH[0][1][ix];
+    }
+    const T *Ex = ep, *Ey = ep + EB, *Ez = ep + 2 * EB;
+    auto dx = [&](const T *f) -> T { return xn ? f[e + 1] - f[e] : (g.pec_on[0] ? g.pec_neg[0] * f[e] : T(0)); };
+    T d, acc, m;
+    // Hx: (y, Ez, +), (z, Ey, -)
+    d = Ez[e + kMarchLanes] - Ez[e];
+    acc = T(0);
+    acc = acc + d;
+    d = ec[EB + e] - ep[EB + e];
+    acc = acc + (-d);
+    hx = hs[sh] - g.cn * acc;
+    // Hy: (x, Ez, -, j0), (z, Ex, +)
+    d = dx(Ez);
+    if (ax) {
+        m = o0 * q.b + q.c * d;
+        g.psiH[0][0][ix] = m;
+        d = d * q.k + m;
+    }
+    acc = T(0);
+    acc = acc + (-d);
+    d = ec[e] - ep[e];
+    acc = acc + d;
+    hy = hs[HS + sh] - g.cn * acc;
+    // Hz: (x, Ey, +, j1), (y, Ex, -)
+    d = dx(Ey);
+    if (ax) {
+        m = o1 * q.b + q.c * d;
+        g.psiH[0][1][ix] = m;
+        d = d * q.k + m;
+    }
+    acc = T(0);
+    acc = acc + d;
+    d = Ex[e + kMarchLanes] - Ex[e];
+    acc = acc + (-d);
+    hz = hs[2 * HS + sh] - g.cn * acc;
+}
+
 // D planes of TMA prefetch; MINB CTAs per SM requested from the register allocator.
 // MODE 0 (general) runs any tile. MODE 1 (pure) has only the fast path (plus source injection): the host
 // launches it over tiles whose computed 32 x 16 cells lie inside the domain and outside every x/y CPML
@@ -464,6 +566,9 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     // MODE 4 (z-pure) runs interior tiles (as MODE 1) on any planes: fast rows, and z rows (a z slab, or the
     // first / last plane of a grid with z faces) in march_e_zslab / march_h_zslab.
     constexpr bool ZPURE = MODE == 4;
+    // MODE 5 (x-boundary) runs tiles outside the interior block's x range whose rows meet no y slab or face, on
+    // planes clear of the z slabs and faces (k_step_march_mixed only): every row takes the x tier.
+    constexpr bool XPURE = MODE == 5;
     constexpr bool INTERIOR = MODE == 1 || ZPURE;
     constexpr bool PXY = MODE == 2;
     // Rows that meet only a z slab get their own tier (plain x / y differences, z memories) in the periodic
@@ -472,10 +577,11 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     // cost the 512 x 512 x 256 CPML step 1.3 % (instruction cache); there the z-pure body takes them.
     constexpr bool ZTIER = (MODE == 2 || ZPURE) && !METRIC;
     static_assert(!METRIC || MODE == 0 || MODE == 2, "the metric variant is a general body");
+    static_assert(!XPURE || !METRIC, "the x-boundary body assumes a uniform mesh");
     // The general and z-pure bodies keep their row loops rolled: unrolled, the general body's three row tiers
     // exist once per row and the code outgrows the instruction cache once a pure body shares the SM
     // (measured: 75 % vs 94 % hits).
-    constexpr int kRowUnroll = MODE == 1 ? kMarchRowsPerThread : 1;
+    constexpr int kRowUnroll = (MODE == 1 || XPURE) ? kMarchRowsPerThread : 1;
     constexpr int HS = S::BOXH_STRIDE / sizeof(T);
     constexpr int ES = S::BOXE_STRIDE / sizeof(T);
     const Grid<T> &g = args.g;
@@ -586,7 +692,16 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     // meets an x or y slab; bit R + h, it has a domain face; bits 2R + h and 3R + h, the same for H.
     constexpr int R = kMarchRowsPerThread;
     unsigned rowbits = 0;
-    if (!INTERIOR) {
+    // x-boundary body: this lane's x slab rows and coefficients, fixed over the tile.
+    int rx_e = -1, rx_h = -1;
+    Coef<T> qx_e{T(0), T(0), T(1)}, qx_h{T(0), T(0), T(1)};
+    if constexpr (XPURE) {
+        rx_e = TFD_SLAB_ROW(args, 0, 0, xc);
+        qx_e = coef_at(g, 0, 0, xc, rx_e);
+        rx_h = TFD_SLAB_ROW(args, 1, 0, x);
+        qx_h = coef_at(g, 1, 0, x, rx_h);
+    }
+    if (!INTERIOR && !XPURE) {
         const bool slab_x_e = TFD_SLAB_MEETS(args, 0, 0, x0, x0 + kMarchLanes);
         const bool slab_x_h = TFD_SLAB_MEETS(args, 1, 0, x0, x0 + kMarchOwnX);
         const bool face_x_e = x0 == 0 && !px;
@@ -705,7 +820,11 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                 const bool cpml_row = ((rowbits >> h) & 1u) || rzE >= 0;
                 const bool plain_xy = !((rowbits >> h) & 1u) && !((rowbits >> (R + h)) & 1u) && zprev && !smask;
                 const bool fast = MODE == 1 || (ZPURE ? rzE < 0 && zprev : !cpml_row && plain_xy);
-                if (fast) {
+                if (XPURE) {
+                    const int pxo = args.psi_parity[0];
+                    march_e_xtier<T, SAMPLES, D>(g, hk, hm, ek, sh, se, xc > 0, rx_e, (kz * ny + yc) * g.rows[0][0] + rx_e,
+                                                 par ? pxo : 0, par ? 0 : pxo, own, qx_e, ex, ey, ez);
+                } else if (fast) {
                     ex = march_e_fast<T, SAMPLES, D, 0, METRIC>(g, hk, hm, ek, sh, se, mE);
                     ey = march_e_fast<T, SAMPLES, D, 1, METRIC>(g, hk, hm, ek, sh, se, mE);
                     ez = march_e_fast<T, SAMPLES, D, 2, METRIC>(g, hk, hm, ek, sh, se, mE);
@@ -768,7 +887,7 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                 const int e = r * kMarchLanes + lane;
                 const int i = y * g.pitch + x;
                 const bool cpml_row = ((rowbits >> (2 * R + h)) & 1u) || rzH >= 0;
-                const bool fast = MODE == 1 || (ZPURE ? rzH < 0 && znext : !cpml_row && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask);
+                const bool fast = !XPURE && (MODE == 1 || (ZPURE ? rzH < 0 && znext : !cpml_row && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask));
                 T mH[3] = {mxH, T(1), mzH};
                 if constexpr (METRIC) {
                     if (g.metric[1][1] != nullptr) mH[1] = g.metric[1][1][y];
@@ -798,7 +917,10 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                     // Interior tiles have their +x / +y neighbours.
                     const bool xn = ZPURE || x < nx - 1 || px, yn = ZPURE || y < ny - 1 || py;
                     T hv[3];
-                    if (ZPURE || (ZTIER && !((rowbits >> (2 * R + h)) & 1u) && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask)) {
+                    if (XPURE) {
+                        march_h_xtier<T, SAMPLES, D>(g, eprv, ecur, hs, sh, e, xn, rx_h, (km * ny + y) * g.rows[1][0] + rx_h, qx_h, hv[0],
+                                                     hv[1], hv[2]);
+                    } else if (ZPURE || (ZTIER && !((rowbits >> (2 * R + h)) & 1u) && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask)) {
                         // A z-slab row (rzH >= 0), or in the z-pure body also the last plane of the grid (!znext).
                         march_h_zslab<T, SAMPLES, D>(g, eprv, ecur, hs, sh, e, znext, znext && rzH >= 0, (rzH * ny + y) * g.pitch + x,
                                                      coef_at(g, 1, 2, km, rzH), hv[0], hv[1], hv[2]);
@@ -844,6 +966,7 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
 // kernel, while its CTAs interleave with the general ones as in one launch.
 struct MarchMix {
     int ix0, ix1, iy0, iy1;
+    int xband;                   // 1: x-boundary tiles of the interior y range take the x-boundary body on pure planes
     int zb[4];
     int lz[3], chunks[3];
 };
@@ -859,11 +982,14 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march_mixed(const 
     const int z0 = mx.zb[seg] + zc * mx.lz[seg];
     const int z1 = min(z0 + mx.lz[seg], mx.zb[seg + 1]);
     const int tx = blockIdx.x, ty = blockIdx.y;
-    const bool interior = tx >= mx.ix0 && tx < mx.ix1 && ty >= mx.iy0 && ty < mx.iy1;
+    const bool yband = ty >= mx.iy0 && ty < mx.iy1;
+    const bool interior = tx >= mx.ix0 && tx < mx.ix1 && yband;
     if (interior && seg == 1)
         march_body<T, SAMPLES, D, 1>(args, tx, ty, z0, z1);
     else if (interior)
         march_body<T, SAMPLES, D, 4>(args, tx, ty, z0, z1);
+    else if (GEN == 0 && mx.xband && yband && seg == 1)
+        march_body<T, SAMPLES, D, 5>(args, tx, ty, z0, z1);
     else
         march_body<T, SAMPLES, D, GEN>(args, tx, ty, z0, z1);
 }
