@@ -548,6 +548,105 @@ __device__ __forceinline__ void march_h_xtier(const Grid<T> &g, const T *ep, con
     hz = hs[2 * HS + sh] - g.cn * acc;
 }
 
+// The y tier of the y-boundary body (MODE 6): a row of a tile inside the interior x range that meets a y slab
+// or a y face but no z slab or face. Only the y differences carry CPML memories (ry >= 0, the row's slab row)
+// and the y faces are selects; the x and z differences are plain. Same operations and order as march_e_row /
+// march_h_row with the x and z terms plain. iy: the memory element of the cell.
+template <typename T, int SAMPLES, int D>
+__device__ __forceinline__ void march_e_ytier(const Grid<T> &g, const T *hk, const T *hm, const T *ek, int s, int se, bool yin, int ry,
+                                              int iy, int po, int pn, bool own, const Coef<T> &q, T &ex, T &ey, T &ez) {
+    using S = MarchShape<T, SAMPLES, D>;
+    constexpr int HS = S::BOXH_STRIDE / sizeof(T);
+    constexpr int ES = S::BOXE_STRIDE / sizeof(T);
+    const T *Hx = hk, *Hy = hk + HS, *Hz = hk + 2 * HS;
+    const bool ay = ry >= 0;
+    T o0 = T(0), o1 = T(0);
+    if (ay) {
+        o0 = g.psiE[0][1][0][po + iy];
+        o1 = g.psiE[0][1][1][po + iy];
+    }
+    T d, acc, m;
+    // Ex: (y, Hz, +, j0), (z, Hy, -)
+    d = yin ? Hz[s] - Hz[s - S::BXW] : T(0);
+    if (ay) {
+        m = o0 * q.b + q.c * d;
+        if (own) g.psiE[0][1][0][pn + iy] = m;
+        d = d * q.k + m;
+    }
+    acc = T(0);
+    acc = acc + d;
+    d = Hy[s] - hm[HS + s];
+    acc = acc + (-d);
+    ex = ek[se] + (g.cn * ek[3 * ES + se]) * acc;
+    // Ey: (x, Hz, -), (z, Hx, +)
+    d = Hz[s] - Hz[s - 1];
+    acc = T(0);
+    acc = acc + (-d);
+    d = Hx[s] - hm[s];
+    acc = acc + d;
+    ey = ek[ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? 1 : 0)) * ES + se]) * acc;
+    // Ez: (x, Hy, +), (y, Hx, -, j1)
+    d = Hy[s] - Hy[s - 1];
+    acc = T(0);
+    acc = acc + d;
+    d = yin ? Hx[s] - Hx[s - S::BXW] : T(0);
+    if (ay) {
+        m = o1 * q.b + q.c * d;
+        if (own) g.psiE[0][1][1][pn + iy] = m;
+        d = d * q.k + m;
+    }
+    acc = acc + (-d);
+    ez = ek[2 * ES + se] + (g.cn * ek[(3 + (SAMPLES == 3 ? 2 : 0)) * ES + se]) * acc;
+}
+
+template <typename T, int SAMPLES, int D>
+__device__ __forceinline__ void march_h_ytier(const Grid<T> &g, const T *ep, const T *ec, const T *hs, int sh, int e, bool yn, int ry,
+                                              int iy, const Coef<T> &q, T &hx, T &hy, T &hz) {
+    using S = MarchShape<T, SAMPLES, D>;
+    constexpr int HS = S::BOXH_STRIDE / sizeof(T);
+    constexpr int EB = S::EBUF;
+    const bool ay = yn && ry >= 0;
+    T o0 = T(0), o1 = T(0);
+    if (ay) {
+        o0 = g.psiH[1][0][iy];
+        o1 = g.psiH[1][1][iy];
+    }
+    const T *Ex = ep, *Ey = ep + EB, *Ez = ep + 2 * EB;
+    auto dy = [&](const T *f) -> T { return yn ? f[e + kMarchLanes] - f[e] : (g.pec_on[1] ? g.pec_neg[1] * f[e] : T(0)); };
+    T d, acc, m;
+    // Hx: (y, Ez, +, j0), (z, Ey, -)
+    d = dy(Ez);
+    if (ay) {
+        m = o0 * q.b + q.c * d;
+        g.psiH[1][0][iy] = m;
+        d = d * q.k + m;
+    }
+    acc = T(0);
+    acc = acc + d;
+    d = ec[EB + e] - ep[EB + e];
+    acc = acc + (-d);
+    hx = hs[sh] - g.cn * acc;
+    // Hy: (x, Ez, -), (z, Ex, +)
+    d = Ez[e + 1] - Ez[e];
+    acc = T(0);
+    acc = acc + (-d);
+    d = ec[e] - ep[e];
+    acc = acc + d;
+    hy = hs[HS + sh] - g.cn * acc;
+    // Hz: (x, Ey, +), (y, Ex, -, j1)
+    d = Ey[e + 1] - Ey[e];
+    acc = T(0);
+    acc = acc + d;
+    d = dy(Ex);
+    if (ay) {
+        m = o1 * q.b + q.c * d;
+        g.psiH[1][1][iy] = m;
+        d = d * q.k + m;
+    }
+    acc = acc + (-d);
+    hz = hs[2 * HS + sh] - g.cn * acc;
+}
+
 // D planes of TMA prefetch; MINB CTAs per SM requested from the register allocator.
 // MODE 0 (general) runs any tile. MODE 1 (pure) has only the fast path (plus source injection): the host
 // launches it over tiles whose computed 32 x 16 cells lie inside the domain and outside every x/y CPML
@@ -569,6 +668,9 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     // MODE 5 (x-boundary) runs tiles outside the interior block's x range whose rows meet no y slab or face, on
     // planes clear of the z slabs and faces (k_step_march_mixed only): every row takes the x tier.
     constexpr bool XPURE = MODE == 5;
+    // MODE 6 (y-boundary) runs tiles of the interior x range outside its y range on the same planes: fast rows,
+    // and rows with a y slab, a y face or a source in the y tier.
+    constexpr bool YPURE = MODE == 6;
     constexpr bool INTERIOR = MODE == 1 || ZPURE;
     constexpr bool PXY = MODE == 2;
     // Rows that meet only a z slab get their own tier (plain x / y differences, z memories) in the periodic
@@ -577,7 +679,7 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     // cost the 512 x 512 x 256 CPML step 1.3 % (instruction cache); there the z-pure body takes them.
     constexpr bool ZTIER = (MODE == 2 || ZPURE) && !METRIC;
     static_assert(!METRIC || MODE == 0 || MODE == 2, "the metric variant is a general body");
-    static_assert(!XPURE || !METRIC, "the x-boundary body assumes a uniform mesh");
+    static_assert(!(XPURE || YPURE) || !METRIC, "the x- and y-boundary bodies assume a uniform mesh");
     // The general and z-pure bodies keep their row loops rolled: unrolled, the general body's three row tiers
     // exist once per row and the code outgrows the instruction cache once a pure body shares the SM
     // (measured: 75 % vs 94 % hits).
@@ -701,7 +803,7 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
         rx_h = TFD_SLAB_ROW(args, 1, 0, x);
         qx_h = coef_at(g, 1, 0, x, rx_h);
     }
-    if (!INTERIOR && !XPURE) {
+    if (!INTERIOR && !XPURE && !YPURE) {
         const bool slab_x_e = TFD_SLAB_MEETS(args, 0, 0, x0, x0 + kMarchLanes);
         const bool slab_x_h = TFD_SLAB_MEETS(args, 1, 0, x0, x0 + kMarchOwnX);
         const bool face_x_e = x0 == 0 && !px;
@@ -824,6 +926,17 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                     const int pxo = args.psi_parity[0];
                     march_e_xtier<T, SAMPLES, D>(g, hk, hm, ek, sh, se, xc > 0, rx_e, (kz * ny + yc) * g.rows[0][0] + rx_e,
                                                  par ? pxo : 0, par ? 0 : pxo, own, qx_e, ex, ey, ez);
+                } else if (YPURE) {
+                    const int ry = TFD_SLAB_ROW(args, 0, 1, yc);
+                    if (ry < 0 && yc > 0 && !smask) {
+                        ex = march_e_fast<T, SAMPLES, D, 0>(g, hk, hm, ek, sh, se);
+                        ey = march_e_fast<T, SAMPLES, D, 1>(g, hk, hm, ek, sh, se);
+                        ez = march_e_fast<T, SAMPLES, D, 2>(g, hk, hm, ek, sh, se);
+                    } else {
+                        const int pyo = args.psi_parity[1];
+                        march_e_ytier<T, SAMPLES, D>(g, hk, hm, ek, sh, se, yc > 0, ry, (kz * g.rows[0][1] + ry) * g.pitch + xc,
+                                                     par ? pyo : 0, par ? 0 : pyo, own, coef_at(g, 0, 1, yc, ry), ex, ey, ez);
+                    }
                 } else if (fast) {
                     ex = march_e_fast<T, SAMPLES, D, 0, METRIC>(g, hk, hm, ek, sh, se, mE);
                     ey = march_e_fast<T, SAMPLES, D, 1, METRIC>(g, hk, hm, ek, sh, se, mE);
@@ -887,7 +1000,9 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                 const int e = r * kMarchLanes + lane;
                 const int i = y * g.pitch + x;
                 const bool cpml_row = ((rowbits >> (2 * R + h)) & 1u) || rzH >= 0;
-                const bool fast = !XPURE && (MODE == 1 || (ZPURE ? rzH < 0 && znext : !cpml_row && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask));
+                const bool fast = !XPURE && (MODE == 1 || (YPURE ? TFD_SLAB_ROW(args, 1, 1, y) < 0 && y < ny - 1 && !hmask
+                                                          : ZPURE ? rzH < 0 && znext
+                                                                  : !cpml_row && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask));
                 T mH[3] = {mxH, T(1), mzH};
                 if constexpr (METRIC) {
                     if (g.metric[1][1] != nullptr) mH[1] = g.metric[1][1][y];
@@ -920,6 +1035,10 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
                     if (XPURE) {
                         march_h_xtier<T, SAMPLES, D>(g, eprv, ecur, hs, sh, e, xn, rx_h, (km * ny + y) * g.rows[1][0] + rx_h, qx_h, hv[0],
                                                      hv[1], hv[2]);
+                    } else if (YPURE) {
+                        const int ry = TFD_SLAB_ROW(args, 1, 1, y);
+                        march_h_ytier<T, SAMPLES, D>(g, eprv, ecur, hs, sh, e, yn, ry, (km * g.rows[1][1] + ry) * g.pitch + x,
+                                                     coef_at(g, 1, 1, y, ry), hv[0], hv[1], hv[2]);
                     } else if (ZPURE || (ZTIER && !((rowbits >> (2 * R + h)) & 1u) && !((rowbits >> (3 * R + h)) & 1u) && znext && !hmask)) {
                         // A z-slab row (rzH >= 0), or in the z-pure body also the last plane of the grid (!znext).
                         march_h_zslab<T, SAMPLES, D>(g, eprv, ecur, hs, sh, e, znext, znext && rzH >= 0, (rzH * ny + y) * g.pitch + x,
@@ -966,7 +1085,8 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march(const __grid
 // kernel, while its CTAs interleave with the general ones as in one launch.
 struct MarchMix {
     int ix0, ix1, iy0, iy1;
-    int xband;                   // 1: x-boundary tiles of the interior y range take the x-boundary body on pure planes
+    int xband;                   // 1: on pure planes, x-boundary tiles of the interior y range take the x-boundary body and
+                                 // y-boundary tiles of the interior x range the y-boundary body
     int zb[4];
     int lz[3], chunks[3];
 };
@@ -990,6 +1110,8 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march_mixed(const 
         march_body<T, SAMPLES, D, 4>(args, tx, ty, z0, z1);
     else if (GEN == 0 && mx.xband && yband && seg == 1)
         march_body<T, SAMPLES, D, 5>(args, tx, ty, z0, z1);
+    else if (GEN == 0 && mx.xband && tx >= mx.ix0 && tx < mx.ix1 && seg == 1)
+        march_body<T, SAMPLES, D, 6>(args, tx, ty, z0, z1);
     else
         march_body<T, SAMPLES, D, GEN>(args, tx, ty, z0, z1);
 }
