@@ -52,7 +52,7 @@ C0 = 299792458.0
 # 512x512x256: 2.428 + 1.776 GB per k_step_march_mixed launch; batch64: 493.4 MB (k_step2d_interior) + 118.5 MB
 # (k_step2d_general) per step at the tuned launch shape.
 L2_NOTE = 'inputs larger than L2 (no flush needed)'
-MEASURED_TRAFFIC_PER_CELL = {('roofline', 'march'): 4.218e9 / 67108864, ('batch64', 'tile2d'): 611.9e6 / 20187264}
+MEASURED_TRAFFIC_PER_CELL = {('roofline', 'march'): 4.175e9 / 67108864, ('batch64', 'tile2d'): 611.9e6 / 20187264}
 
 
 def baseline_face(layers):
