@@ -229,9 +229,8 @@ __device__ __forceinline__ T forward_curl(const AdjArgs<T> &A, const T *slot, in
 // ACTIVE: bitmask of advanced components (bit c: E_c, bit 3+c: H_c). Blocks of kAdjX x kAdjY cells of one
 // z plane (blockIdx.x, blockIdx.y: x and y tile; blockIdx.z: plane), so the x and y neighbours a cell reads
 // are mostly in its block's L1 lines. The tile origins are shifted by (xs, ys) cells (tile (bx, by) starts at
-// (bx kAdjX - xs, by kAdjY - ys)) so that a tile edge falls where the interior of the grid begins; interior
-// tiles take a fast path unless `fast` is 0 (the general path alone, for comparisons). Reads parity q,
-// writes q^1.
+// (bx kAdjX - xs, by kAdjY - ys)) so that tiles start at x = 1 and y = 1; tiles clear of the grid faces take a
+// fast path unless `fast` is 0 (the general path alone, for comparisons). Reads parity q, writes q^1.
 constexpr int kAdjX = 32, kAdjY = 8;
 
 // Whether the CPML slab bounds b = {lo0, hi0, lo1, hi1} (half-open) meet the coordinates [lo, hi].
@@ -239,34 +238,31 @@ __host__ __device__ __forceinline__ bool adj_meets(const int *b, int lo, int hi)
     return (lo < b[1] && b[0] <= hi) || (lo < b[3] && b[2] <= hi);
 }
 
-// Block classes for the fast paths. On x and y every cell of the block lies in [1, n-2] (both neighbours
-// inside the grid, no face or periodic edge) and no CPML term applies to any D value the block's cells
-// evaluate: the H family on [lo - 1, hi] (HFAM: the e_bar update differences D(c-1) and D(c)) and the E family
-// on [lo, hi + e_hi]; the plane z lies in [1, nz-2]. Class 1: no CPML term on z either, so every D value is the
-// plain transposed difference; class 2: the z terms meet a z slab and go through the general D functions.
-// Class 0: the general path. In classes 1 and 2 the general path's arithmetic reduces to the fast path's
-// operations, in the same order.
+// Block classes for the fast paths. Every cell of the block lies in [1, n-2] on every axis (both neighbours
+// inside the grid: no face or periodic edge); otherwise the block takes the general path (class -1). Else the
+// class is a mask with bit a set when a CPML term may apply to a D value the block's cells evaluate on axis a:
+// the H family on [lo - 1, hi] (HFAM: the e_bar update differences D(c-1) and D(c)) and the E family on
+// [lo, hi + e_hi]. Terms on the axes of the mask go through the general D functions; the others are the plain
+// transposed differences, to which the general path's arithmetic reduces there, in the same order.
 template <typename T>
 __device__ __forceinline__ int adj_class(const AdjArgs<T> &A, int x0, int y0, int z, bool hfam, int e_hi) {
     const Grid<T> &g = A.g;
     const int lo[3] = {max(x0, 0), max(y0, 0), z};
     const int hi[3] = {min(x0 + kAdjX, g.n[0]) - 1, min(y0 + kAdjY, g.n[1]) - 1, z};
+    int mask = 0;
 #pragma unroll
-    for (int a = 0; a < 3; ++a)
-        if (lo[a] < 1 || hi[a] > g.n[a] - 2) return 0;
-#pragma unroll
-    for (int a = 0; a < 2; ++a) {
-        if (hfam && adj_meets(A.slab[1][a], lo[a] - 1, hi[a])) return 0;
-        if (adj_meets(A.slab[0][a], lo[a], hi[a] + e_hi)) return 0;
+    for (int a = 0; a < 3; ++a) {
+        if (lo[a] < 1 || hi[a] > g.n[a] - 2) return -1;
+        if ((hfam && adj_meets(A.slab[1][a], lo[a] - 1, hi[a])) || adj_meets(A.slab[0][a], lo[a], hi[a] + e_hi)) mask |= 1 << a;
     }
-    const bool zslab = (hfam && adj_meets(A.slab[1][2], z - 1, z)) || adj_meets(A.slab[0][2], z, z + e_hi);
-    return zslab ? 2 : 1;
+    return mask;
 }
 
-// e_bar_new and the sensitivity of the three components of an interior cell (classes 1 and 2 above). Every
-// input of the plain terms is loaded before the first store (the stores could alias the loads for the
-// compiler, which would otherwise serialise the three components' memory round trips).
-template <typename T, bool ZGEN>
+// e_bar_new and the sensitivity of the three components of a cell of a fast-path block; GEN: the axes whose
+// terms go through the general D functions (the mask above). Every input of the plain terms is loaded before
+// the first store (the stores could alias the loads for the compiler, which would otherwise serialise the three
+// components' memory round trips).
+template <typename T, int GEN>
 __device__ __forceinline__ void adj_e_fast(const AdjArgs<T> &A, const T *__restrict__ slot, int q, int x, int y, int z, long long i) {
     const Grid<T> &g = A.g;
     const int co[3] = {x, y, z};
@@ -283,7 +279,7 @@ __device__ __forceinline__ void adj_e_fast(const AdjArgs<T> &A, const T *__restr
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const RevTerm t = rev_of(C, k);
-            if (!(ZGEN && t.axis == 2)) hm[C][k] = __ldg(A.hb[q][t.out] + i - g.stride(t.axis));
+            if (!((GEN >> t.axis) & 1)) hm[C][k] = __ldg(A.hb[q][t.out] + i - g.stride(t.axis));
             const Term f = term_of(C, k);
             smv[C][k] = __ldg(slot + A.sH[f.in] + i - g.stride(f.axis));
         }
@@ -295,9 +291,10 @@ __device__ __forceinline__ void adj_e_fast(const AdjArgs<T> &A, const T *__restr
         for (int k = 0; k < 2; ++k) {
             const RevTerm t = rev_of(C, k);
             const int a = t.axis, c = co[a];
-            if (ZGEN && a == 2) {
-                contrib = contrib + d_h(A, q, t, x, y, z - 1, i - g.plane, false);    // src[c] += D(c-1)
-                contrib = contrib - d_h(A, q, t, x, y, z, i, true);                  // src[c] -= D(c)
+            if ((GEN >> a) & 1) {
+                const int xm = a == 0 ? x - 1 : x, ym = a == 1 ? y - 1 : y, zm = a == 2 ? z - 1 : z;
+                contrib = contrib + d_h(A, q, t, xm, ym, zm, i - g.stride(a), false);   // src[c] += D(c-1)
+                contrib = contrib - d_h(A, q, t, x, y, z, i, true);                    // src[c] -= D(c)
                 continue;
             }
             const T *mt = g.metric[1][a];
@@ -314,16 +311,16 @@ __device__ __forceinline__ void adj_e_fast(const AdjArgs<T> &A, const T *__restr
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const Term t = term_of(C, k);
-            const int a = t.axis;
+            const int a = t.axis, c = co[a];
             const T *mt = g.metric[0][a];
             T d = sc[t.in] - smv[C][k];
-            if (mt != nullptr) d = d * mt[co[a]];
-            if (ZGEN && a == 2 && A.sPsiE[2][t.j] >= 0) {
-                const int r = adj_slab_row(A.slab[0][2], z);
+            if (mt != nullptr) d = d * mt[c];
+            if (((GEN >> a) & 1) && A.sPsiE[a][t.j] >= 0) {
+                const int r = adj_slab_row(A.slab[0][a], c);
                 if (r >= 0) {
-                    const long long p = g.psi_index(2, x, y, z, r, g.rows[0][2]);
-                    const T mem = slot[A.sPsiE[2][t.j] + p] * g.cb[0][2][z] + g.cc[0][2][z] * d;
-                    d = d * g.ck[0][2][z] + mem;
+                    const long long p = g.psi_index(a, x, y, z, r, g.rows[0][a]);
+                    const T mem = slot[A.sPsiE[a][t.j] + p] * g.cb[0][a][c] + g.cc[0][a][c] * d;
+                    d = d * g.ck[0][a][c] + mem;
                 }
             }
             acc = acc + (t.sign > 0 ? d : -d);
@@ -337,8 +334,8 @@ __device__ __forceinline__ void adj_e_fast(const AdjArgs<T> &A, const T *__restr
     }
 }
 
-// h_bar_new of the three components of an interior cell; e_own: the cell's e_bar_new.
-template <typename T, bool ZGEN>
+// h_bar_new of the three components of a cell of a fast-path block; e_own: the cell's e_bar_new.
+template <typename T, int GEN>
 __device__ __forceinline__ void adj_h_fast(const AdjArgs<T> &A, int q, int x, int y, int z, long long i, const T *e_own) {
     const Grid<T> &g = A.g;
     const int co[3] = {x, y, z};
@@ -354,7 +351,7 @@ __device__ __forceinline__ void adj_h_fast(const AdjArgs<T> &A, int q, int x, in
         for (int k = 0; k < 2; ++k) {
             const RevTerm t = rev_of(C, k);
             ep[C][k] = __ldg(A.eb[q ^ 1][t.out] + i + g.stride(t.axis));
-            if (!(ZGEN && t.axis == 2)) iep[C][k] = __ldg(g.inv_eps[t.out] + i + g.stride(t.axis));
+            if (!((GEN >> t.axis) & 1)) iep[C][k] = __ldg(g.inv_eps[t.out] + i + g.stride(t.axis));
         }
     T out[3];
 #pragma unroll
@@ -364,9 +361,10 @@ __device__ __forceinline__ void adj_h_fast(const AdjArgs<T> &A, int q, int x, in
         for (int k = 0; k < 2; ++k) {
             const RevTerm t = rev_of(C, k);
             const int a = t.axis, c = co[a];
-            if (ZGEN && a == 2) {
+            if ((GEN >> a) & 1) {
+                const int xp = a == 0 ? x + 1 : x, yp = a == 1 ? y + 1 : y, zp = a == 2 ? z + 1 : z;
                 contrib = contrib + d_e(A, q, t, x, y, z, i, e_own[t.out], true);                   // src[c] += D(c)
-                contrib = contrib - d_e(A, q, t, x, y, z + 1, i + g.plane, ep[C][k], false);       // src[c] -= D(c+1)
+                contrib = contrib - d_e(A, q, t, xp, yp, zp, i + g.stride(a), ep[C][k], false);    // src[c] -= D(c+1)
                 continue;
             }
             const T *mt = g.metric[0][a];
@@ -396,14 +394,16 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_e(const __grid_consta
     if (x < 0 || y < 0 || x >= g.n[0] || y >= g.n[1]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
     if (ACTIVE == 63 && fast && g.active == 63) {
-        const int cls = adj_class(A, x0, y0, z, true, 0);
-        if (cls == 1) {
-            adj_e_fast<T, false>(A, slot, q, x, y, z, i);
-            return;
-        }
-        if (cls == 2) {
-            adj_e_fast<T, true>(A, slot, q, x, y, z, i);
-            return;
+        switch (adj_class(A, x0, y0, z, true, 0)) {
+            case 0: adj_e_fast<T, 0>(A, slot, q, x, y, z, i); return;
+            case 1: adj_e_fast<T, 1>(A, slot, q, x, y, z, i); return;
+            case 2: adj_e_fast<T, 2>(A, slot, q, x, y, z, i); return;
+            case 3: adj_e_fast<T, 3>(A, slot, q, x, y, z, i); return;
+            case 4: adj_e_fast<T, 4>(A, slot, q, x, y, z, i); return;
+            case 5: adj_e_fast<T, 5>(A, slot, q, x, y, z, i); return;
+            case 6: adj_e_fast<T, 6>(A, slot, q, x, y, z, i); return;
+            case 7: adj_e_fast<T, 7>(A, slot, q, x, y, z, i); return;
+            default: break;
         }
     }
     if (ACTIVE & 1) {
@@ -438,14 +438,16 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_h(const __grid_consta
     if (ACTIVE & 2) e[1] = A.eb[q ^ 1][1][i];
     if (ACTIVE & 4) e[2] = A.eb[q ^ 1][2][i];
     if (ACTIVE == 63 && fast && g.active == 63) {
-        const int cls = adj_class(A, x0, y0, z, false, 1);
-        if (cls == 1) {
-            adj_h_fast<T, false>(A, q, x, y, z, i, e);
-            return;
-        }
-        if (cls == 2) {
-            adj_h_fast<T, true>(A, q, x, y, z, i, e);
-            return;
+        switch (adj_class(A, x0, y0, z, false, 1)) {
+            case 0: adj_h_fast<T, 0>(A, q, x, y, z, i, e); return;
+            case 1: adj_h_fast<T, 1>(A, q, x, y, z, i, e); return;
+            case 2: adj_h_fast<T, 2>(A, q, x, y, z, i, e); return;
+            case 3: adj_h_fast<T, 3>(A, q, x, y, z, i, e); return;
+            case 4: adj_h_fast<T, 4>(A, q, x, y, z, i, e); return;
+            case 5: adj_h_fast<T, 5>(A, q, x, y, z, i, e); return;
+            case 6: adj_h_fast<T, 6>(A, q, x, y, z, i, e); return;
+            case 7: adj_h_fast<T, 7>(A, q, x, y, z, i, e); return;
+            default: break;
         }
     }
     if (ACTIVE & 8) A.hb[q ^ 1][0][i] = hbar_value<T, 0, true>(A, q, x, y, z, i, e);

@@ -2410,20 +2410,13 @@ int adjoint_step_t(tfd_adjoint *adj, const void *snapshot, const void *seeds, cu
         k_adjoint_seed<T><<<std::max(1, std::min(1184, (n_obs + 255) / 256)), 256, 0, s>>>(A, p->ptr<TraceDev>(p->L.trace_tab), n_obs,
                                                                                        (const T *)seeds, adj->q);
     const Grid<T> &g = A.g;
-    // Tile origins shifted so that a tile edge falls on the first interior cell of x and y (after the low CPML
-    // slab; the e_bar update also differences D(c-1), one cell further): the interior tiles then take the fast
-    // path of the kernels whole.
-    auto low_end = [&](const int *b, int a) { return (b[1] > b[0] && b[0] < g.n[a] / 2) ? b[1] : 0; };
-    auto shift = [&](int a, bool e_kernel, int tile) {
-        int start = std::max(1, low_end(A.slab[0][a], a));
-        if (e_kernel) start = std::max(start, low_end(A.slab[1][a], a) + 1);
-        return (tile - start % tile) % tile;
-    };
+    // Tile origins shifted by one cell less than a tile, so that tiles start at x = 1 and y = 1: a tile whose cells
+    // all lie in [1, n-2] takes the fast path of the kernels (the first tile holds the x = 0 / y = 0 face).
     // TFD_ADJ_XSHIFT=0 keeps the x tiles at multiples of 32 (rows aligned to 128 bytes) for comparisons.
     const char *xenv = getenv("TFD_ADJ_XSHIFT");
     const bool xshift = !(xenv && std::atoi(xenv) == 0);
-    const int exs = xshift ? shift(0, true, kAdjX) : 0, eys = shift(1, true, kAdjY);
-    const int hxs = xshift ? shift(0, false, kAdjX) : 0, hys = shift(1, false, kAdjY);
+    const int exs = xshift ? kAdjX - 1 : 0, eys = kAdjY - 1;
+    const int hxs = exs, hys = eys;
     auto grid_of = [&](int xs, int ys) {
         return dim3((unsigned)((g.n[0] + xs + kAdjX - 1) / kAdjX), (unsigned)((g.n[1] + ys + kAdjY - 1) / kAdjY), (unsigned)g.n[2]);
     };
