@@ -1209,11 +1209,7 @@ void launch_strips(const Grid<T> *grids, const Tile2D *table, int interior, int 
     if (all > interior)
         k_step2d_general<T><<<ctas_2d(all - interior, ctas), k2dThreads, 0, both ? side->stream : s>>>(grids, table + interior,
                                                                                                      all - interior, counter);
-    if (interior > 0) {
-        static const bool async_rows = !(getenv("TFD_2D_ASYNC") && std::atoi(getenv("TFD_2D_ASYNC")) == 0);
-        if (async_rows) k_step2d_interior<T, true><<<ctas_2d(interior, ctas), k2dThreads, 0, s>>>(grids, table, interior, counter);
-        else k_step2d_interior<T, false><<<ctas_2d(interior, ctas), k2dThreads, 0, s>>>(grids, table, interior, counter);
-    }
+    if (interior > 0) k_step2d_interior<T><<<ctas_2d(interior, ctas), k2dThreads, 0, s>>>(grids, table, interior, counter);
     if (both) {
         cudaEventRecord(side->join, side->stream);
         cudaStreamWaitEvent(s, side->join, 0);

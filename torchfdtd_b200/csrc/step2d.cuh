@@ -113,85 +113,6 @@ __device__ __forceinline__ void strip_interior(const Grid<T> &g, const Tile2D &s
     }
 }
 
-// The interior strip of the per-step kernel with its rows staged through shared memory: each lane copies its
-// row elements (Hx, Hy, Ez, 1/eps, and Hy(x-1) on lane 0) with cp.async into a ring of R row slots of its
-// warp, so that R - 1 rows are in flight without holding them in registers (the register ring of
-// strip_interior is limited to 3 rows by the 64-register budget of 4 CTAs per SM). Each lane reads back only
-// what it copied itself, so the warp needs no barrier. Same arithmetic as strip_interior.
-template <typename T>
-struct AsyncRing2D {
-    static constexpr int R = sizeof(T) == 4 ? 8 : 4;   // rows in flight (a power of two)
-    T v[R][5][32];
-};
-
-__device__ __forceinline__ void cp_async_elem(void *dst, const void *src, int bytes) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-    if (bytes == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
-    else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
-}
-
-template <typename T>
-__device__ __forceinline__ void strip_interior_async(const Grid<T> &g, const Tile2D &st, int par, int lane, AsyncRing2D<T> &ring) {
-    constexpr unsigned kAll = 0xffffffffu;
-    constexpr int R = AsyncRing2D<T>::R;
-    const int pitch = g.pitch;
-    const int base = st.y0 * pitch + st.x0 + lane;
-    const T *__restrict__ Hx = g.H[par][0] + base;
-    const T *__restrict__ Hy = g.H[par][1] + base;
-    const T *__restrict__ Ez = g.E[par][2] + base;
-    const T *__restrict__ iep = g.inv_eps[2] + base;
-    T *__restrict__ Hxn = g.H[par ^ 1][0] + base;
-    T *__restrict__ Hyn = g.H[par ^ 1][1] + base;
-    T *__restrict__ Ezn = g.E[par ^ 1][2] + base;
-    const T cn = g.cn;
-    const bool own = lane < k2dOwnX;
-    const int rows = st.y1 - st.y0;                    // owned rows; row `rows` is the halo row
-    T hx_prev = Hx[-pitch];
-    T hy_prev = T(0), ez_prev = T(0);
-    auto issue = [&](int k) {
-        if (k <= rows) {
-            const int o = k * pitch, sl = k & (R - 1);
-            cp_async_elem(&ring.v[sl][0][lane], Hx + o, sizeof(T));
-            cp_async_elem(&ring.v[sl][1][lane], Hy + o, sizeof(T));
-            cp_async_elem(&ring.v[sl][2][lane], Ez + o, sizeof(T));
-            cp_async_elem(&ring.v[sl][3][lane], iep + o, sizeof(T));
-            if (lane == 0) cp_async_elem(&ring.v[sl][4][0], Hy + o - 1, sizeof(T));
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");   // an empty group past the last row keeps the count
-    };
-    // R - 1 rows in flight: row r + R - 1 goes into the slot row r - 1 used, whose values were consumed in the
-    // previous iteration, so no copy can overwrite a slot before this lane has read it.
-#pragma unroll
-    for (int k = 0; k < R - 1; ++k) issue(k);
-    for (int r = 0; r <= rows; ++r) {
-        asm volatile("cp.async.wait_group %0;" ::"n"(R - 2) : "memory");   // row r's group has landed
-        const int sl = r & (R - 1);
-        const T c_hx = ring.v[sl][0][lane], c_hy = ring.v[sl][1][lane], c_ez = ring.v[sl][2][lane], c_ie = ring.v[sl][3][lane];
-        const T c_hyl = lane == 0 ? ring.v[sl][4][0] : T(0);
-        issue(r + R - 1);
-        T hy_left = __shfl_up_sync(kAll, c_hy, 1);
-        if (lane == 0) hy_left = c_hyl;
-        T acc = T(0) + (c_hy - hy_left);
-        acc = acc + (-(c_hx - hx_prev));
-        const T ez_new = c_ez + (cn * c_ie) * acc;
-        const int o = r * pitch;
-        if (own && r < rows) Ezn[o] = ez_new;
-        const T ez_right = __shfl_down_sync(kAll, ez_prev, 1);
-        if (r > 0) {
-            const T hxn = hx_prev - cn * (T(0) + (ez_new - ez_prev));
-            const T hyn = hy_prev - cn * (T(0) + (-(ez_right - ez_prev)));
-            if (own) {
-                Hxn[o - pitch] = hxn;
-                Hyn[o - pitch] = hyn;
-            }
-        }
-        hx_prev = c_hx;
-        hy_prev = c_hy;
-        ez_prev = ez_new;
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");   // nothing of this strip is still in flight into the ring
-}
-
 // Everything of row y the general path reads, fetched K rows ahead: the fields, Hy(x-1) for lane 0, the
 // E-family CPML memories of row y (x slab of this lane, y slab of this row) and the H-family memories of
 // row y-1, which this iteration completes, with the y-slab rows of both.
@@ -366,12 +287,10 @@ __device__ __forceinline__ void strip_general(const Grid<T> &g, const Tile2D &st
 // Two kernels walk the two parts of a strip table, interior strips first: the lean path fits 64 registers
 // (4 CTAs, 32 warps per SM), the general path gets up to 128. Both read only old-parity state and write
 // disjoint owned cells, so they need no ordering between them within a step.
-// ASYNC: rows staged through shared memory by cp.async (strip_interior_async), else the register ring.
-template <typename T, bool ASYNC>
+template <typename T>
 __global__ void __launch_bounds__(k2dThreads, 4) k_step2d_interior(const Grid<T> *__restrict__ grids,
                                                                   const Tile2D *__restrict__ strips, int nstrips,
                                                                   const long long *counter) {
-    __shared__ AsyncRing2D<T> ring[ASYNC ? k2dWarps : 1];
     const long long n = *counter;
     const int par = (int)(n & 1);
     const int lane = threadIdx.x & 31;
@@ -385,8 +304,7 @@ __global__ void __launch_bounds__(k2dThreads, 4) k_step2d_interior(const Grid<T>
             if (lane == 0) atomicExch(g.status, kStatusBadStrip);
             continue;
         }
-        if constexpr (ASYNC) strip_interior_async(g, st, par, lane, ring[threadIdx.x >> 5]);
-        else strip_interior(g, st, par, lane);
+        strip_interior(g, st, par, lane);
     }
 }
 
