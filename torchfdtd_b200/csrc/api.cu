@@ -2410,12 +2410,10 @@ int adjoint_step_t(tfd_adjoint *adj, const void *snapshot, const void *seeds, cu
         k_adjoint_seed<T><<<std::max(1, std::min(1184, (n_obs + 255) / 256)), 256, 0, s>>>(A, p->ptr<TraceDev>(p->L.trace_tab), n_obs,
                                                                                        (const T *)seeds, adj->q);
     const Grid<T> &g = A.g;
-    // Tile origins shifted by one cell less than a tile, so that tiles start at x = 1 and y = 1: a tile whose cells
-    // all lie in [1, n-2] takes the fast path of the kernels (the first tile holds the x = 0 / y = 0 face).
-    // TFD_ADJ_XSHIFT=0 keeps the x tiles at multiples of 32 (rows aligned to 128 bytes) for comparisons.
-    const char *xenv = getenv("TFD_ADJ_XSHIFT");
-    const bool xshift = !(xenv && std::atoi(xenv) == 0);
-    const int exs = xshift ? kAdjX - 1 : 0, eys = kAdjY - 1;
+    // x tiles at multiples of 32 (rows aligned to 128 bytes: measured 13 % faster for k_adjoint_e than tiles
+    // starting at x = 1, which put one more column of tiles on the fast path); y tiles shifted to start at y = 1,
+    // so the first tile row holds the y = 0 face alone. A tile whose cells all lie in [1, n-2] takes the fast path.
+    const int exs = 0, eys = kAdjY - 1;
     const int hxs = exs, hys = eys;
     auto grid_of = [&](int xs, int ys) {
         return dim3((unsigned)((g.n[0] + xs + kAdjX - 1) / kAdjX), (unsigned)((g.n[1] + ys + kAdjY - 1) / kAdjY), (unsigned)g.n[2]);
