@@ -283,20 +283,6 @@ StripGeom strip_geom(const tfd_desc *d) {
     return G;
 }
 
-// Strip table order: interior strips (kind 1), then the x- and y-tier strips (kinds 2, 3), then the general ones
-// (kind 0); the interior kernel walks the first part, the tier kernel the second, the general kernel the rest.
-inline int strip_rank(const Tile2D &a) { return a.kind == 1 ? 0 : (a.kind == 0 ? 2 : 1); }
-inline void order_strips(std::vector<Tile2D> &t) {
-    std::stable_sort(t.begin(), t.end(), [](const Tile2D &a, const Tile2D &b) { return strip_rank(a) < strip_rank(b); });
-}
-// Strips of the interior kernel (kind 1) and of both lean kernels (kinds 1-3).
-int interior_count(const std::vector<Tile2D> &t) {
-    return (int)std::count_if(t.begin(), t.end(), [](const Tile2D &a) { return a.kind == 1; });
-}
-int lean_count(const std::vector<Tile2D> &t) {
-    return (int)std::count_if(t.begin(), t.end(), [](const Tile2D &a) { return a.kind != 0; });
-}
-
 // Strips of one grid: rows split into a lower boundary band, an interior band and an upper boundary band
 // (so that whole strips avoid the y slabs), each band cut into strips of `rows` rows, columns in steps of
 // 31, x-fastest so that neighbouring strips (which share halo columns) run together. A strip is interior
@@ -329,25 +315,24 @@ std::vector<Tile2D> strips_of(const StripGeom &G, int grid_index, int rows) {
         }
         return true;
     };
-    // TFD_2D_TIERS=0 sends the x- and y-tier strips to the general kernel (for comparisons).
-    static const bool tiers = !(getenv("TFD_2D_TIERS") && std::atoi(getenv("TFD_2D_TIERS")) == 0);
     std::vector<Tile2D> t;
     for (size_t b = 0; b < bands.size(); ++b) {
         const bool inner = bands.size() == 3 && b == 1;
         for (int y0 = bands[b].first; y0 < bands[b].second; y0 += rows) {
             const int y1 = std::min(y0 + rows, bands[b].second);
             for (int x0 = 0; x0 < nx; x0 += k2dOwnX) {
-                // 1: interior; 2: interior rows, x slab or face (x tier); 3: boundary rows, interior columns (y tier);
-                // 0: the general path (corners, sources, nonuniform meshes).
-                int kind = 0;
-                if (!G.metric && bands.size() == 3 && no_source(x0, y0, y1) && (tiers || (inner && x_interior(x0))))
-                    kind = inner ? (x_interior(x0) ? 1 : 2) : (x_interior(x0) ? 3 : 0);
+                const int kind = inner && !G.metric && x_interior(x0) && no_source(x0, y0, y1) ? 1 : 0;
                 t.push_back(Tile2D{grid_index, x0, y0, y1, kind});
             }
         }
     }
-    order_strips(t);
+    // Interior strips first: the lean kernel walks [0, interior), the general kernel the rest.
+    std::stable_partition(t.begin(), t.end(), [](const Tile2D &a) { return a.kind == 1; });
     return t;
+}
+
+int interior_count(const std::vector<Tile2D> &t) {
+    return (int)std::count_if(t.begin(), t.end(), [](const Tile2D &a) { return a.kind == 1; });
 }
 
 // Upper bound of the strip count of a grid for strips of at least 8 rows (two band edges add two cuts).
@@ -511,8 +496,7 @@ struct tfd_plan {
         if (fork) cudaEventDestroy(fork);
     }
     int march_variant = 42;
-    int tile2d_interior = 0;       // interior strips (kind 1) at the head of the strip table
-    int tile2d_lean = 0;           // interior and tier strips (kinds 1-3): the general strips follow
+    int tile2d_interior = 0;
     int persist_ctas = 0;          // > 0: 2D steps run as one persistent cooperative launch of this many CTAs
     Cluster2D cluster2d{};         // ranks > 0: 2D steps run on chip in one thread-block cluster
     size_t cluster2d_smem = 0;
@@ -1190,7 +1174,6 @@ int setup_tile2d(tfd_plan *p, cudaStream_t s) {
     std::vector<Tile2D> tiles = strips_of(strip_geom<T>(p), 0, p->L.strip_rows);
     if ((int)tiles.size() != p->L.tiles2d) return fail(TFD_ERR_INVALID, "2D strip table does not match the layout");
     p->tile2d_interior = interior_count(tiles);
-    p->tile2d_lean = lean_count(tiles);
     if (p->tile2d_interior > 0 && p->tile2d_interior < p->L.tiles2d && !p->side2d) {
         p->side2d.reset(new SideStream());
         TFD_CHECK(p->side2d->create());
@@ -1212,22 +1195,20 @@ int setup_tile2d(tfd_plan *p, cudaStream_t s) {
     return setup_cluster2d<T>(p);
 }
 
-// One 2D step over a strip table ordered [interior strips | tier strips | general strips] (`interior` and `lean`
-// strips before the general ones). The tier and general strips (latency-bound: CPML memories, edges, sources)
-// start first on the side stream, one kernel after the other, and overlap the bandwidth-bound interior kernel;
-// the caller's stream waits for both (graph capture follows the fork).
+// One 2D step over a strip table whose first `interior` strips are interior strips. The general strips
+// (latency-bound: CPML memories, edges, sources) start first on the side stream and overlap the
+// bandwidth-bound interior kernel; the caller's stream waits for both (graph capture follows the fork).
 template <typename T>
-void launch_strips(const Grid<T> *grids, const Tile2D *table, int interior, int lean, int all, int ctas, const long long *counter,
+void launch_strips(const Grid<T> *grids, const Tile2D *table, int interior, int all, int ctas, const long long *counter,
                    cudaStream_t s, const SideStream *side) {
     const bool both = interior > 0 && all > interior && side != nullptr && side->stream != nullptr;
     if (both) {
         cudaEventRecord(side->fork, s);
         cudaStreamWaitEvent(side->stream, side->fork, 0);
     }
-    cudaStream_t aux = both ? side->stream : s;
-    if (lean > interior)
-        k_step2d_tier<T><<<ctas_2d(lean - interior, ctas), k2dThreads, 0, aux>>>(grids, table + interior, lean - interior, counter);
-    if (all > lean) k_step2d_general<T><<<ctas_2d(all - lean, ctas), k2dThreads, 0, aux>>>(grids, table + lean, all - lean, counter);
+    if (all > interior)
+        k_step2d_general<T><<<ctas_2d(all - interior, ctas), k2dThreads, 0, both ? side->stream : s>>>(grids, table + interior,
+                                                                                                     all - interior, counter);
     if (interior > 0) k_step2d_interior<T><<<ctas_2d(interior, ctas), k2dThreads, 0, s>>>(grids, table, interior, counter);
     if (both) {
         cudaEventRecord(side->join, side->stream);
@@ -1238,7 +1219,7 @@ void launch_strips(const Grid<T> *grids, const Tile2D *table, int interior, int 
 template <typename T>
 void launch_tile2d(tfd_plan *p, cudaStream_t s) {
     launch_strips<T>((const Grid<T> *)(p->arena + p->L.grid_tab), (const Tile2D *)(p->arena + p->L.tile_tab), p->tile2d_interior,
-                     p->tile2d_lean, p->L.tiles2d, p->desc.launch_variant, p->grid<T>().counter, s, p->side2d.get());
+                     p->L.tiles2d, p->desc.launch_variant, p->grid<T>().counter, s, p->side2d.get());
 }
 
 }  // namespace
@@ -2006,7 +1987,7 @@ int tfd_step_launches(const tfd_plan *p, int32_t nsteps, int64_t *launches) {
             *launches = nsteps > 0 ? 1 : 0;
             return TFD_OK;
         }
-        per_step = (p->tile2d_interior > 0) + (p->tile2d_lean > p->tile2d_interior) + (p->L.tiles2d > p->tile2d_lean) + 1;
+        per_step = (p->tile2d_interior > 0) + (p->L.tiles2d > p->tile2d_interior) + 1;
     } else if (p->kernel == TFD_KERNEL_MARCH) {
         per_step = (long long)p->march_launches.size() + 1;
     }
@@ -2022,7 +2003,7 @@ struct tfd_batch {
     int precision = 4;
     char *arena = nullptr;
     size_t counter = 0, done = 0, grids = 0, tiles = 0, mon = 0, total = 0;
-    int ntiles = 0, interior = 0, lean = 0, capacity = 0, rows = 8, ctas = 0, max_planes = 0, max_chunks = 1;
+    int ntiles = 0, interior = 0, capacity = 0, rows = 8, ctas = 0, max_planes = 0, max_chunks = 1;
     SideStream side;
     long long cells = 0;
     size_t bar = 0;                // persistent stepping: arrival count and generation
@@ -2072,13 +2053,12 @@ int batch_strips_t(tfd_batch *b, int rows, cudaStream_t s) {
         tiles.insert(tiles.end(), t.begin(), t.end());
     }
     if ((int)tiles.size() > b->capacity) return fail(TFD_ERR_INVALID, "strip table exceeds the batch arena");
-    // Every member's interior strips first, then their tier strips, then the general ones.
-    order_strips(tiles);
+    // Interior strips of every member first: the lean kernel walks [0, interior) of the whole table.
+    std::stable_partition(tiles.begin(), tiles.end(), [](const Tile2D &a) { return a.kind == 1; });
     TFD_CUDA(cudaMemcpyAsync(b->arena + b->tiles, tiles.data(), tiles.size() * sizeof(Tile2D), cudaMemcpyHostToDevice, s));
     TFD_CUDA(cudaStreamSynchronize(s));
     b->ntiles = (int)tiles.size();
     b->interior = interior_count(tiles);
-    b->lean = lean_count(tiles);
     b->rows = rows;
     return TFD_OK;
 }
@@ -2160,7 +2140,7 @@ int batch_step_t(tfd_batch *b, int nsteps, cudaStream_t s) {
     long long *counter = (long long *)(b->arena + b->counter);
     const dim3 mgrid((unsigned)b->max_chunks, (unsigned)std::max(1, b->max_planes), (unsigned)b->plans.size());
     for (int k = 0; k < nsteps; ++k) {
-        launch_strips<T>((const Grid<T> *)(b->arena + b->grids), (const Tile2D *)(b->arena + b->tiles), b->interior, b->lean, b->ntiles,
+        launch_strips<T>((const Grid<T> *)(b->arena + b->grids), (const Tile2D *)(b->arena + b->tiles), b->interior, b->ntiles,
                          b->ctas, counter, s, &b->side);
         k_monitor_batch<T><<<mgrid, kMonitorThreads, 0, s>>>((const MonitorArgs<T> *)(b->arena + b->mon), counter,
                                                              (unsigned *)(b->arena + b->done));

@@ -85,9 +85,9 @@ __global__ void __launch_bounds__(k2dThreads, 2) k_step2d_persistent(const Grid<
         if (k > 0) observe_step(m, mgx, mgy, n - 1);
         for (int s = w0; s < all; s += warps_total) {
             const Tile2D st = strips[s];
-            if (s < interior && st.kind == 1) {
+            if (s < interior) {
                 // The lean path reads x0-1, x0+31, y0-1 and y1 unchecked: refuse a strip that is not interior.
-                if (st.x0 < 1 || st.x0 + 31 > g.n[0] - 1 || st.y0 < 1 || st.y1 > g.n[1] - 1 || st.y1 < st.y0) {
+                if (st.kind != 1 || st.x0 < 1 || st.x0 + 31 > g.n[0] - 1 || st.y0 < 1 || st.y1 > g.n[1] - 1 || st.y1 < st.y0) {
                     if (lane == 0) atomicExch(g.status, kStatusBadStrip);
                     continue;
                 }
@@ -133,9 +133,8 @@ __global__ void __launch_bounds__(k2dThreads, 2) k_step2d_batch_persistent(const
             const Tile2D st = strips[s];
             const Grid<T> &g = grids[st.grid];
             if (n >= g.steps) continue;                // this member has finished its run (warp-uniform)
-            if (s < interior && st.kind == 1) {
-                // The lean path reads x0-1, x0+31, y0-1 and y1 unchecked: refuse a strip that is not interior.
-                if (st.x0 < 1 || st.x0 + 31 > g.n[0] - 1 || st.y0 < 1 || st.y1 > g.n[1] - 1 || st.y1 < st.y0) {
+            if (s < interior) {
+                if (st.kind != 1 || st.x0 < 1 || st.x0 + 31 > g.n[0] - 1 || st.y0 < 1 || st.y1 > g.n[1] - 1 || st.y1 < st.y0) {
                     if (lane == 0) atomicExch(g.status, kStatusBadStrip);
                     continue;
                 }

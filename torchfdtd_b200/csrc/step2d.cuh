@@ -113,226 +113,6 @@ __device__ __forceinline__ void strip_interior(const Grid<T> &g, const Tile2D &s
     }
 }
 
-// x-tier strip (kind 2): a strip of the interior row band (no y slab, no y face, rows y0-1 .. y1 inside the
-// grid) that meets an x slab or an x face, with no source. Only the x differences carry CPML memories (per lane)
-// and the x faces are selects; the y differences are plain. Same operations, in the same order, as
-// strip_general takes for such a strip.
-template <typename T>
-struct XRow2D { T hx, hy, ez, ie, hyl, pex, phx; };
-
-template <typename T>
-__device__ __forceinline__ void strip_xtier(const Grid<T> &g, const Tile2D &st, int par, int lane) {
-    constexpr unsigned kAll = 0xffffffffu;
-    constexpr int K = 2;
-    const int nx = g.n[0], pitch = g.pitch;
-    const int x = st.x0 + lane, y0 = st.y0, y1 = st.y1;
-    const bool in_x = x < nx;
-    const bool own = in_x && lane < k2dOwnX;
-    const T *__restrict__ Hx = g.H[par][0];
-    const T *__restrict__ Hy = g.H[par][1];
-    const T *__restrict__ Ez = g.E[par][2];
-    const T *__restrict__ iep = g.inv_eps[2];
-    T *__restrict__ Hxn = g.H[par ^ 1][0];
-    T *__restrict__ Hyn = g.H[par ^ 1][1];
-    T *__restrict__ Ezn = g.E[par ^ 1][2];
-    const T cn = g.cn;
-    const int *rxp_e = g.row[0][0], *rxp_h = g.row[1][0];
-    const int rxE = (rxp_e != nullptr && in_x && x > 0) ? rxp_e[x] : -1;
-    const int rxH = (rxp_h != nullptr && in_x && x < nx - 1) ? rxp_h[x] : -1;
-    T bxE = T(0), cxE = T(0), kxE = T(0), bxH = T(0), cxH = T(0), kxH = T(0);
-    if (rxE >= 0) { bxE = g.cb[0][0][x]; cxE = g.cc[0][0][x]; kxE = g.ck[0][0][x]; }
-    if (rxH >= 0) { bxH = g.cb[1][0][x]; cxH = g.cc[1][0][x]; kxH = g.ck[1][0][x]; }
-    const int RxE = g.rows[0][0], RxH = g.rows[1][0];
-    const T *psiEx = g.psiE[par][0][1];
-    T *psiExn = g.psiE[par ^ 1][0][1];
-    T *psiHx = g.psiH[0][0];
-    const bool pec_x = g.pec_on[0] != 0;
-    const T pneg_x = g.pec_neg[0];
-    auto load = [&](XRow2D<T> &r, int y) {
-        const bool row = y <= y1;
-        const bool live = row && in_x;
-        const int i = y * pitch + x;
-        r.hx = live ? Hx[i] : T(0);
-        r.hy = live ? Hy[i] : T(0);
-        r.ez = live ? Ez[i] : T(0);
-        r.ie = live ? iep[i] : T(0);
-        r.hyl = (row && lane == 0 && x > 0) ? Hy[i - 1] : T(0);
-        r.pex = (live && rxE >= 0) ? psiEx[y * RxE + rxE] : T(0);
-        r.phx = (y > y0 && row && rxH >= 0) ? psiHx[(y - 1) * RxH + rxH] : T(0);
-    };
-    T hx_prev = in_x ? Hx[(y0 - 1) * pitch + x] : T(0);
-    T hy_prev = T(0), ez_prev = T(0);
-    XRow2D<T> ring[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) load(ring[k], y0 + k);
-    for (int yb = y0; yb <= y1; yb += K) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int y = yb + k;
-            if (y > y1) break;                         // warp-uniform
-            const XRow2D<T> r = ring[k];
-            load(ring[k], y + K);
-            T hy_left = __shfl_up_sync(kAll, r.hy, 1);
-            if (lane == 0) hy_left = r.hyl;
-            T d = x > 0 ? r.hy - hy_left : T(0);
-            if (rxE >= 0) {
-                const T mem = r.pex * bxE + cxE * d;
-                if (own && y < y1) psiExn[y * RxE + rxE] = mem;
-                d = d * kxE + mem;
-            }
-            T acc = T(0) + d;
-            d = r.hx - hx_prev;
-            acc = acc + (-d);
-            const T ez_new = r.ez + (cn * r.ie) * acc;
-            if (own && y < y1) Ezn[y * pitch + x] = ez_new;
-            const T ez_right = __shfl_down_sync(kAll, ez_prev, 1);
-            if (y > y0) {
-                const int h = y - 1;
-                d = ez_new - ez_prev;
-                acc = T(0) + d;
-                const T hxn = hx_prev - cn * acc;
-                d = T(0);
-                if (x < nx - 1) {
-                    d = ez_right - ez_prev;
-                    if (rxH >= 0) {
-                        const T mem = r.phx * bxH + cxH * d;
-                        if (own) psiHx[h * RxH + rxH] = mem;
-                        d = d * kxH + mem;
-                    }
-                } else if (pec_x) {
-                    d = pneg_x * ez_prev;
-                }
-                acc = T(0) + (-d);
-                const T hyn = hy_prev - cn * acc;
-                if (own) {
-                    Hxn[h * pitch + x] = hxn;
-                    Hyn[h * pitch + x] = hyn;
-                }
-            }
-            hx_prev = r.hx;
-            hy_prev = r.hy;
-            ez_prev = ez_new;
-        }
-    }
-}
-
-// y-tier strip (kind 3): a strip of a boundary row band whose 32 columns avoid every x slab and x face, with no
-// source. Only the y differences carry CPML memories (per row) and the y faces are selects; the x differences
-// are plain. Same operations, in the same order, as strip_general takes for such a strip.
-template <typename T>
-struct YRow2D { T hx, hy, ez, ie, hyl, pey, phy; int rye, ryh; };
-
-template <typename T>
-__device__ __forceinline__ void strip_ytier(const Grid<T> &g, const Tile2D &st, int par, int lane) {
-    constexpr unsigned kAll = 0xffffffffu;
-    constexpr int K = 2;
-    const int ny = g.n[1], pitch = g.pitch;
-    const int x = st.x0 + lane, y0 = st.y0, y1 = st.y1;
-    const bool own = lane < k2dOwnX;
-    const T *__restrict__ Hx = g.H[par][0];
-    const T *__restrict__ Hy = g.H[par][1];
-    const T *__restrict__ Ez = g.E[par][2];
-    const T *__restrict__ iep = g.inv_eps[2];
-    T *__restrict__ Hxn = g.H[par ^ 1][0];
-    T *__restrict__ Hyn = g.H[par ^ 1][1];
-    T *__restrict__ Ezn = g.E[par ^ 1][2];
-    const T cn = g.cn;
-    const int *ryp_e = g.row[0][1], *ryp_h = g.row[1][1];
-    const T *psiEy = g.psiE[par][1][1];
-    T *psiEyn = g.psiE[par ^ 1][1][1];
-    T *psiHy = g.psiH[1][0];
-    const bool pec_y = g.pec_on[1] != 0;
-    const T pneg_y = g.pec_neg[1];
-    auto load = [&](YRow2D<T> &r, int y) {
-        const bool row = y <= y1 && y < ny;
-        const int i = y * pitch + x;
-        r.hx = row ? Hx[i] : T(0);
-        r.hy = row ? Hy[i] : T(0);
-        r.ez = row ? Ez[i] : T(0);
-        r.ie = row ? iep[i] : T(0);
-        r.hyl = (row && lane == 0) ? Hy[i - 1] : T(0);
-        r.rye = (row && ryp_e != nullptr && y > 0) ? ryp_e[y] : -1;
-        r.pey = r.rye >= 0 ? psiEy[r.rye * pitch + x] : T(0);
-        const int h = y - 1;
-        r.ryh = (y > y0 && y <= y1 && ryp_h != nullptr && h < ny - 1) ? ryp_h[h] : -1;
-        r.phy = r.ryh >= 0 ? psiHy[r.ryh * pitch + x] : T(0);
-    };
-    T hx_prev = y0 > 0 ? Hx[(y0 - 1) * pitch + x] : T(0);
-    T hy_prev = T(0), ez_prev = T(0);
-    YRow2D<T> ring[K];
-#pragma unroll
-    for (int k = 0; k < K; ++k) load(ring[k], y0 + k);
-    for (int yb = y0; yb <= y1; yb += K) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int y = yb + k;
-            if (y > y1) break;                         // warp-uniform
-            const YRow2D<T> r = ring[k];
-            load(ring[k], y + K);
-            T ez_new = T(0);
-            if (y < ny) {
-                T hy_left = __shfl_up_sync(kAll, r.hy, 1);
-                if (lane == 0) hy_left = r.hyl;
-                T d = r.hy - hy_left;
-                T acc = T(0) + d;
-                d = y > 0 ? r.hx - hx_prev : T(0);
-                if (r.rye >= 0) {
-                    const T mem = r.pey * g.cb[0][1][y] + g.cc[0][1][y] * d;
-                    if (own && y < y1) psiEyn[r.rye * pitch + x] = mem;
-                    d = d * g.ck[0][1][y] + mem;
-                }
-                acc = acc + (-d);
-                ez_new = r.ez + (cn * r.ie) * acc;
-                if (own && y < y1) Ezn[y * pitch + x] = ez_new;
-            }
-            const T ez_right = __shfl_down_sync(kAll, ez_prev, 1);
-            if (y > y0) {
-                const int h = y - 1;
-                T d = T(0);
-                if (h < ny - 1) {
-                    d = ez_new - ez_prev;
-                    if (r.ryh >= 0) {
-                        const T mem = r.phy * g.cb[1][1][h] + g.cc[1][1][h] * d;
-                        if (own) psiHy[r.ryh * pitch + x] = mem;
-                        d = d * g.ck[1][1][h] + mem;
-                    }
-                } else if (pec_y) {
-                    d = pneg_y * ez_prev;
-                }
-                T acc = T(0) + d;
-                const T hxn = hx_prev - cn * acc;
-                d = ez_right - ez_prev;
-                acc = T(0) + (-d);
-                const T hyn = hy_prev - cn * acc;
-                if (own) {
-                    Hxn[h * pitch + x] = hxn;
-                    Hyn[h * pitch + x] = hyn;
-                }
-            }
-            hx_prev = r.hx;
-            hy_prev = r.hy;
-            ez_prev = ez_new;
-        }
-    }
-}
-
-// A tier strip (kinds 2, 3) with the bounds its path reads unchecked; a strip that does not meet them is refused
-// with the device status word.
-template <typename T>
-__device__ __forceinline__ void strip_tier(const Grid<T> &g, const Tile2D &st, int par, int lane) {
-    const int nx = g.n[0], ny = g.n[1];
-    bool ok = st.y1 >= st.y0;
-    if (st.kind == 2) ok = ok && st.x0 >= 0 && st.x0 < nx && st.y0 >= 1 && st.y1 <= ny - 1;
-    else if (st.kind == 3) ok = ok && st.x0 >= 1 && st.x0 + 31 <= nx - 1 && st.y0 >= 0 && st.y1 <= ny;
-    else ok = false;
-    if (!ok) {
-        if (lane == 0) atomicExch(g.status, kStatusBadStrip);
-        return;
-    }
-    if (st.kind == 2) strip_xtier(g, st, par, lane);
-    else strip_ytier(g, st, par, lane);
-}
-
 // Everything of row y the general path reads, fetched K rows ahead: the fields, Hy(x-1) for lane 0, the
 // E-family CPML memories of row y (x slab of this lane, y slab of this row) and the H-family memories of
 // row y-1, which this iteration completes, with the y-slab rows of both.
@@ -525,23 +305,6 @@ __global__ void __launch_bounds__(k2dThreads, 4) k_step2d_interior(const Grid<T>
             continue;
         }
         strip_interior(g, st, par, lane);
-    }
-}
-
-// The x- and y-tier strips (kinds 2 and 3); like the general kernel it gets up to 128 registers (its two row rings
-// and ten field and memory pointers spill at 64).
-template <typename T>
-__global__ void __launch_bounds__(k2dThreads, 2) k_step2d_tier(const Grid<T> *__restrict__ grids, const Tile2D *__restrict__ strips,
-                                                              int nstrips, const long long *counter) {
-    const long long n = *counter;
-    const int par = (int)(n & 1);
-    const int lane = threadIdx.x & 31;
-    const int warps_total = gridDim.x * k2dWarps;
-    for (int s = blockIdx.x * k2dWarps + (threadIdx.x >> 5); s < nstrips; s += warps_total) {
-        const Tile2D st = strips[s];
-        const Grid<T> &g = grids[st.grid];
-        if (n >= g.steps) continue;
-        strip_tier(g, st, par, lane);
     }
 }
 
