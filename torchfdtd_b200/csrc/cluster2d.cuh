@@ -11,7 +11,9 @@
 //   H phase: Hx from Ez (row y + 1: the CTA above for the last row), Hy from Ez (x + 1), the H-family memories,
 //            the H soft sources, then the point traces of the step (the owning CTA writes them to HBM);
 //   cluster barrier.
-// Each phase reads only the other family, so the updates are in place. The arithmetic per cell is that of
+// A warp takes a 32-column segment of a group of consecutive rows and marches up through them (E pass: Hx of the
+// row below kept in a register; H pass: Ez of the row above), with the x neighbours by shuffle. Each phase
+// reads only the other family, so the updates are in place. The arithmetic per cell is that of
 // the strip kernels' general path (step2d.cuh: strip_general), so the fields are bitwise the same. The state
 // is loaded from the parity the step counter names at the start of the launch and written back, with the
 // counter, at the end. Scope: 2D TMz plans without DFT planes (the traces are the only observations).
@@ -172,103 +174,118 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
     const T *const xb_h = sm + L.tab[1][0], *const yb_h = sm + L.tab[1][1];
     const int *const xs_e = ints + L.slab[0][0], *const ys_e = ints + L.slab[0][1];
     const int *const xs_h = ints + L.slab[1][0], *const ys_h = ints + L.slab[1][1];
-    // Work units: a warp takes 32 consecutive cells of one row. Unit u is row u / XU, columns 32 (u % XU) ...;
-    // a warp's units advance by kCl2dWarps, kept as (row, segment) without a division per unit.
+    // Work units: a warp takes a 32-column segment (cg) of a group of consecutive rows (rg) and marches up
+    // through its rows, keeping the row below (E pass: Hx(y-1)) or above (H pass: Ez(y+1)) in registers and
+    // taking the x neighbours by shuffle. XU segments per row, RG row groups (as many as the warps allow), each
+    // of RPG rows; unit u = w, w + 32, ... is segment u % XU of row group u / XU.
     const int XU = (nx + 31) / 32;
-    const int dq = kCl2dWarps / XU, dr = kCl2dWarps % XU;
-    const int yl_first = warp / XU, xs_first = warp % XU;
+    const int RG = max(1, min(rows, kCl2dWarps / XU));
+    const int RPG = (rows + RG - 1) / RG;
+    const int units = XU * RG;
     cluster.sync();                                       // every band and table loaded before any neighbour reads it
 
     long long n = n0;
     for (int k = 0; k < c.count && n < g.steps; ++k, ++n) {
-        // ---- E phase ----
-        for (int yl = yl_first, xs = xs_first; yl < rows;) {
-            const int y = r0 + yl, x = xs * 32 + lane;
-            // Row-uniform terms of dy(Hx).
-            const int rye = ys_e[y];
-            const T *hxb = yl > 0 ? Hx + (yl - 1) * W : (hx_below != nullptr ? hx_below + (rows_below - 1) * W : Hx);
-            if (x < nx) {
-                const int e = yl * W + x;
-                T d = x > 0 ? Hy[e] - Hy[e - 1] : T(0);
-                if (mx_e && x > 0) d = d * xb_e[3 * nx + x];
-                const int rxE = xs_e[x];
-                if (rxE >= 0) {
-                    const T mem = pex[yl * RxE + rxE] * xb_e[x] + xb_e[nx + x] * d;
-                    pex[yl * RxE + rxE] = mem;
-                    d = d * xb_e[2 * nx + x] + mem;
+        // ---- E pass ----
+        for (int u = warp; u < units; u += kCl2dWarps) {
+            const int x = (u % XU) * 32 + lane, ylo = (u / XU) * RPG, yhi = min(ylo + RPG, rows);
+            const bool in = x < nx;
+            // This lane's x terms: CPML row and coefficients, metric factor.
+            const int rxE = in ? xs_e[x] : -1;
+            T bx = T(0), cx = T(0), kx = T(1), mxv = T(1);
+            if (rxE >= 0) { bx = xb_e[x]; cx = xb_e[nx + x]; kx = xb_e[2 * nx + x]; }
+            if (mx_e && in) mxv = xb_e[3 * nx + x];
+            // Hx of the row below the group: this band's row, the band below (DSMEM), or none at y = 0.
+            T hx_prev = T(0);
+            if (in && ylo > 0 && ylo <= rows) hx_prev = Hx[(ylo - 1) * W + x];
+            else if (in && hx_below != nullptr) hx_prev = hx_below[(rows_below - 1) * W + x];
+            for (int yl = ylo; yl < yhi; ++yl) {
+                const int y = r0 + yl, e = yl * W + x;
+                const T hy = in ? Hy[e] : T(0);
+                const T hx = in ? Hx[e] : T(0);
+                T hy_left = __shfl_up_sync(0xffffffffu, hy, 1);
+                if (lane == 0 && x > 0 && in) hy_left = Hy[e - 1];
+                if (in) {
+                    T d = x > 0 ? hy - hy_left : T(0);
+                    if (mx_e && x > 0) d = d * mxv;
+                    if (rxE >= 0) {
+                        const T mem = pex[yl * RxE + rxE] * bx + cx * d;
+                        pex[yl * RxE + rxE] = mem;
+                        d = d * kx + mem;
+                    }
+                    T acc = T(0) + d;
+                    d = y > 0 ? hx - hx_prev : T(0);
+                    if (my_e && y > 0) d = d * yb_e[3 * ny + y];
+                    const int rye = ys_e[y];
+                    if (rye >= 0) {
+                        const int pi = (rye - c.rye_lo[rank]) * W + x;
+                        const T mem = pey[pi] * yb_e[y] + yb_e[ny + y] * d;
+                        pey[pi] = mem;
+                        d = d * yb_e[2 * ny + y] + mem;
+                    }
+                    acc = acc + (-d);
+                    Ez[e] = Ez[e] + (cn * ie[e]) * acc;
                 }
-                T acc = T(0) + d;
-                d = y > 0 ? Hx[e] - hxb[x] : T(0);
-                if (my_e && y > 0) d = d * yb_e[3 * ny + y];
-                if (rye >= 0) {
-                    const int pi = (rye - c.rye_lo[rank]) * W + x;
-                    const T mem = pey[pi] * yb_e[y] + yb_e[ny + y] * d;
-                    pey[pi] = mem;
-                    d = d * yb_e[2 * ny + y] + mem;
-                }
-                acc = acc + (-d);
-                T ez = Ez[e] + (cn * ie[e]) * acc;
-                Ez[e] = ez;
-            }
-            yl += dq;
-            xs += dr;
-            if (xs >= XU) {
-                xs -= XU;
-                ++yl;
+                hx_prev = hx;
             }
         }
         if (src_e) add_sources(src_e, Ez, n);             // CTA-uniform
         // A CTA enters the cluster barrier once all its warps are done.
         __syncthreads();
         cluster.sync();
-        // ---- H phase ----
-        for (int yl = yl_first, xs = xs_first; yl < rows;) {
-            const int h = r0 + yl, x = xs * 32 + lane;
-            const int ryh = ys_h[h];
-            const T *ezu = yl + 1 < rows ? Ez + (yl + 1) * W : (ez_above != nullptr ? ez_above : Ez);
-            if (x < nx) {
-                const int e = yl * W + x;
-                const T ezc = Ez[e];
-                // Hx: dy(Ez)
-                T d = T(0);
-                if (h < ny - 1) {
-                    d = ezu[x] - ezc;
-                    if (my_h) d = d * yb_h[3 * ny + h];
-                    if (ryh >= 0) {
-                        const int pi = (ryh - c.ryh_lo[rank]) * W + x;
-                        const T mem = phy[pi] * yb_h[h] + yb_h[ny + h] * d;
-                        phy[pi] = mem;
-                        d = d * yb_h[2 * ny + h] + mem;
+        // ---- H pass ----
+        for (int u = warp; u < units; u += kCl2dWarps) {
+            const int x = (u % XU) * 32 + lane, ylo = (u / XU) * RPG, yhi = min(ylo + RPG, rows);
+            const bool in = x < nx;
+            const int rxH = in ? xs_h[x] : -1;
+            T bx = T(0), cx = T(0), kx = T(1), mxv = T(1);
+            if (rxH >= 0) { bx = xb_h[x]; cx = xb_h[nx + x]; kx = xb_h[2 * nx + x]; }
+            if (mx_h && in) mxv = xb_h[3 * nx + x];
+            T ez_cur = (in && ylo < rows) ? Ez[ylo * W + x] : T(0);
+            for (int yl = ylo; yl < yhi; ++yl) {
+                const int h = r0 + yl, e = yl * W + x;
+                // Ez of the row above: this band's row, the band above (DSMEM); none above the last grid row.
+                T ez_up = T(0);
+                if (in && yl + 1 < rows) ez_up = Ez[e + W];
+                else if (in && ez_above != nullptr) ez_up = ez_above[x];
+                T ez_right = __shfl_down_sync(0xffffffffu, ez_cur, 1);
+                if (lane == 31 && x + 1 < nx) ez_right = Ez[e + 1];
+                if (in) {
+                    // Hx: dy(Ez)
+                    T d = T(0);
+                    if (h < ny - 1) {
+                        d = ez_up - ez_cur;
+                        if (my_h) d = d * yb_h[3 * ny + h];
+                        const int ryh = ys_h[h];
+                        if (ryh >= 0) {
+                            const int pi = (ryh - c.ryh_lo[rank]) * W + x;
+                            const T mem = phy[pi] * yb_h[h] + yb_h[ny + h] * d;
+                            phy[pi] = mem;
+                            d = d * yb_h[2 * ny + h] + mem;
+                        }
+                    } else if (pec_y) {
+                        d = pneg_y * ez_cur;
                     }
-                } else if (pec_y) {
-                    d = pneg_y * ezc;
-                }
-                T acc = T(0) + d;
-                T hxn = Hx[e] - cn * acc;
-                // Hy: -dx(Ez)
-                d = T(0);
-                if (x < nx - 1) {
-                    d = Ez[e + 1] - ezc;
-                    if (mx_h) d = d * xb_h[3 * nx + x];
-                    const int rxH = xs_h[x];
-                    if (rxH >= 0) {
-                        const T mem = phx[yl * RxH + rxH] * xb_h[x] + xb_h[nx + x] * d;
-                        phx[yl * RxH + rxH] = mem;
-                        d = d * xb_h[2 * nx + x] + mem;
+                    T acc = T(0) + d;
+                    const T hxn = Hx[e] - cn * acc;
+                    // Hy: -dx(Ez)
+                    d = T(0);
+                    if (x < nx - 1) {
+                        d = ez_right - ez_cur;
+                        if (mx_h) d = d * mxv;
+                        if (rxH >= 0) {
+                            const T mem = phx[yl * RxH + rxH] * bx + cx * d;
+                            phx[yl * RxH + rxH] = mem;
+                            d = d * kx + mem;
+                        }
+                    } else if (pec_x) {
+                        d = pneg_x * ez_cur;
                     }
-                } else if (pec_x) {
-                    d = pneg_x * ezc;
+                    acc = T(0) + (-d);
+                    Hx[e] = hxn;
+                    Hy[e] = Hy[e] - cn * acc;
                 }
-                acc = T(0) + (-d);
-                T hyn = Hy[e] - cn * acc;
-                Hx[e] = hxn;
-                Hy[e] = hyn;
-            }
-            yl += dq;
-            xs += dr;
-            if (xs >= XU) {
-                xs -= XU;
-                ++yl;
+                ez_cur = ez_up;
             }
         }
         if (src_hx) add_sources(src_hx, Hx, n);
