@@ -192,6 +192,9 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
             const bool in = x < nx;
             // This lane's x terms: CPML row and coefficients, metric factor.
             const int rxE = in ? xs_e[x] : -1;
+            // A plain segment: every lane has its -x neighbour and no x memory, on a uniform mesh; its rows clear of
+            // the y slabs and the y = 0 face take the bare update (the general arithmetic reduces to it there).
+            const bool xplain = __all_sync(0xffffffffu, in && x > 0 && rxE < 0) && !mx_e && !my_e;
             T bx = T(0), cx = T(0), kx = T(1), mxv = T(1);
             if (rxE >= 0) { bx = xb_e[x]; cx = xb_e[nx + x]; kx = xb_e[2 * nx + x]; }
             if (mx_e && in) mxv = xb_e[3 * nx + x];
@@ -205,7 +208,11 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
                 const T hx = in ? Hx[e] : T(0);
                 T hy_left = __shfl_up_sync(0xffffffffu, hy, 1);
                 if (lane == 0 && x > 0 && in) hy_left = Hy[e - 1];
-                if (in) {
+                if (xplain && y > 0 && ys_e[y] < 0) {
+                    T acc = T(0) + (hy - hy_left);
+                    acc = acc + (-(hx - hx_prev));
+                    Ez[e] = Ez[e] + (cn * ie[e]) * acc;
+                } else if (in) {
                     T d = x > 0 ? hy - hy_left : T(0);
                     if (mx_e && x > 0) d = d * mxv;
                     if (rxE >= 0) {
@@ -238,6 +245,8 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
             const int x = (u % XU) * 32 + lane, ylo = (u / XU) * RPG, yhi = min(ylo + RPG, rows);
             const bool in = x < nx;
             const int rxH = in ? xs_h[x] : -1;
+            // A plain segment: every lane has its +x neighbour and no x memory, on a uniform mesh.
+            const bool xplain = __all_sync(0xffffffffu, x < nx - 1 && rxH < 0) && !mx_h && !my_h;
             T bx = T(0), cx = T(0), kx = T(1), mxv = T(1);
             if (rxH >= 0) { bx = xb_h[x]; cx = xb_h[nx + x]; kx = xb_h[2 * nx + x]; }
             if (mx_h && in) mxv = xb_h[3 * nx + x];
@@ -250,7 +259,11 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
                 else if (in && ez_above != nullptr) ez_up = ez_above[x];
                 T ez_right = __shfl_down_sync(0xffffffffu, ez_cur, 1);
                 if (lane == 31 && x + 1 < nx) ez_right = Ez[e + 1];
-                if (in) {
+                if (xplain && h < ny - 1 && ys_h[h] < 0) {
+                    const T hxn = Hx[e] - cn * (T(0) + (ez_up - ez_cur));
+                    Hy[e] = Hy[e] - cn * (T(0) + (-(ez_right - ez_cur)));
+                    Hx[e] = hxn;
+                } else if (in) {
                     // Hx: dy(Ez)
                     T d = T(0);
                     if (h < ny - 1) {
