@@ -152,14 +152,18 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
     // Soft sources of a family, after its update pass: the cells of each source box in the band get the source
     // value added, one source after the other (ascending index, the order of the strip kernels), so each cell
     // sees the same additions in the same order as an update that adds them in place.
+    // Source values of the step, loaded at its top by thread t for term t so that their latency overlaps the E
+    // pass (a source mask has 32 bits, so at most 32 terms reach here).
+    __shared__ T src_val[32];
+    const unsigned src_any = src_e | src_hx | src_hy;
     auto add_sources = [&](unsigned mask, T *field, long long n) {
         for (; mask; mask &= mask - 1) {
             const int t = __ffs(mask) - 1;
             const SourceTerm &s = g.src[t];
             const int ylo = max(s.lo[1], r0), yhi = min(s.hi[1], r1), xlo = max(s.lo[0], 0), xhi = min(s.hi[0], nx);
             const int w = xhi - xlo, cnt = (w > 0 && yhi > ylo) ? w * (yhi - ylo) : 0;
-            const T v = g.src_values[(long long)t * g.steps + n];
             __syncthreads();
+            const T v = src_val[t];                   // prefetched at the top of the step
             for (int q = tid; q < cnt; q += kCl2dThreads) {
                 const int e = (ylo - r0 + q / w) * W + xlo + q % w;
                 field[e] = field[e] + v;
@@ -184,8 +188,17 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
     const int units = XU * RG;
     cluster.sync();                                       // every band and table loaded before any neighbour reads it
 
+    // Point traces: a thread keeps the band-local index of its trace (-1: another band's cell) and the field.
+    int tr_e = -1, tr_f = 0;
+    if (tid < n_traces) {
+        const TraceDev tr = traces[tid];
+        const int y = (int)(tr.offset / pitch), x = (int)(tr.offset % pitch);
+        if (y >= r0 && y < r1) tr_e = (y - r0) * W + x;
+        tr_f = (tr.family == 0 && tr.comp == 2) ? 1 : (tr.family == 1 && tr.comp == 0) ? 2 : (tr.family == 1 && tr.comp == 1) ? 3 : 0;
+    }
     long long n = n0;
     for (int k = 0; k < c.count && n < g.steps; ++k, ++n) {
+        if (tid < 32 && ((src_any >> tid) & 1u)) src_val[tid] = g.src_values[(long long)tid * g.steps + n];
         // ---- E pass ----
         for (int u = warp; u < units; u += kCl2dWarps) {
             const int x = (u % XU) * 32 + lane, ylo = (u / XU) * RPG, yhi = min(ylo + RPG, rows);
@@ -306,7 +319,11 @@ __global__ void __launch_bounds__(kCl2dThreads, 1) k_step2d_cluster(const __grid
         if (band_traces) {
             // Point traces of step n sampled by the rank that owns the cell (a CTA-uniform branch).
             __syncthreads();
-            for (int t = tid; t < n_traces; t += kCl2dThreads) {
+            if (tid < n_traces && tr_e >= 0) {
+                const T v = tr_f == 1 ? Ez[tr_e] : tr_f == 2 ? Hx[tr_e] : tr_f == 3 ? Hy[tr_e] : T(0);
+                trace_out[n * n_traces + tid] = v;
+            }
+            for (int t = tid + kCl2dThreads; t < n_traces; t += kCl2dThreads) {
                 const TraceDev tr = traces[t];
                 const int y = (int)(tr.offset / pitch), x = (int)(tr.offset % pitch);
                 if (y < r0 || y >= r1) continue;
