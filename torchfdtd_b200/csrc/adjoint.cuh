@@ -230,33 +230,8 @@ __device__ __forceinline__ T forward_curl(const AdjArgs<T> &A, const T *slot, in
 // z plane (blockIdx.x, blockIdx.y: x and y tile; blockIdx.z: plane), so the x and y neighbours a cell reads
 // are mostly in its block's L1 lines. The tile origins are shifted by (xs, ys) cells (tile (bx, by) starts at
 // (bx kAdjX - xs, by kAdjY - ys)) so that tiles start at x = 1 and y = 1; tiles clear of the grid faces take a
-// fast path unless bit 0 of `fast` is clear (the general path alone, for comparisons); bit 1 turns on the L2
-// prefetch of the tiles a few planes ahead. Reads parity q, writes q^1.
+// fast path unless `fast` is 0 (the general path alone, for comparisons). Reads parity q, writes q^1.
 constexpr int kAdjX = 32, kAdjY = 8;
-
-// L2 prefetch: a block issues one bulk prefetch per (array, row) of its tile at plane z + kAdjPrefetch, whose
-// blocks run about a wave later; their loads then find the rows in L2 instead of waiting on DRAM (both kernels
-// are bound by load latency: one cell per thread, a long-scoreboard stall per few instructions). A prefetch
-// changes no data; rows outside the grid and addresses that are not 16-byte aligned are skipped.
-constexpr int kAdjPrefetch = 4;
-
-template <typename T, typename F>
-__device__ __forceinline__ void adj_prefetch(const Grid<T> &g, int x0, int y0, int z, int count, F array) {
-    const int zp = z + kAdjPrefetch;
-    if (zp >= g.n[2]) return;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const int r = tid % kAdjY, a = tid / kAdjY;        // row of the tile, array
-    if (a >= count) return;
-    const int y = y0 + r, xa = max(x0, 0);
-    const int cols = min(x0 + kAdjX, g.n[0]) - xa;
-    if (y < 0 || y >= g.n[1] || cols <= 0) return;
-    const T *base = array(a);
-    if (base == nullptr) return;
-    const T *p = base + (long long)zp * g.plane + (long long)y * g.pitch + xa;
-    if ((reinterpret_cast<uintptr_t>(p) & 15u) != 0) return;
-    const uint32_t bytes = ((uint32_t)(cols * (int)sizeof(T)) + 15u) & ~15u;
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
 
 // Whether the CPML slab bounds b = {lo0, hi0, lo1, hi1} (half-open) meet the coordinates [lo, hi].
 __host__ __device__ __forceinline__ bool adj_meets(const int *b, int lo, int hi) {
@@ -416,14 +391,9 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_e(const __grid_consta
     const int x = x0 + threadIdx.x;
     const int y = y0 + threadIdx.y;
     const int z = blockIdx.z;
-    // h_bar, the snapshot's H, e_bar and S of the tile a few planes ahead.
-    if (fast & 2) adj_prefetch(g, x0, y0, z, 12, [&](int a) -> const T * {
-        const int c = a % 3;
-        return a < 3 ? A.hb[q][c] : a < 6 ? (A.sH[c] >= 0 ? slot + A.sH[c] : nullptr) : a < 9 ? A.eb[q][c] : A.S[c];
-    });
     if (x < 0 || y < 0 || x >= g.n[0] || y >= g.n[1]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
-    if (ACTIVE == 63 && (fast & 1) && g.active == 63) {
+    if (ACTIVE == 63 && fast && g.active == 63) {
         switch (adj_class(A, x0, y0, z, true, 0)) {
             case 0: adj_e_fast<T, 0>(A, slot, q, x, y, z, i); return;
             case 1: adj_e_fast<T, 1>(A, slot, q, x, y, z, i); return;
@@ -461,18 +431,13 @@ __global__ void __launch_bounds__(kAdjX * kAdjY) k_adjoint_h(const __grid_consta
     const int x = x0 + threadIdx.x;
     const int y = y0 + threadIdx.y;
     const int z = blockIdx.z;
-    // e_bar_new, 1/eps and h_bar of the tile a few planes ahead.
-    if (fast & 2) adj_prefetch(g, x0, y0, z, 9, [&](int a) -> const T * {
-        const int c = a % 3;
-        return a < 3 ? A.eb[q ^ 1][c] : a < 6 ? g.inv_eps[c] : A.hb[q][c];
-    });
     if (x < 0 || y < 0 || x >= g.n[0] || y >= g.n[1]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
     T e[3] = {T(0), T(0), T(0)};
     if (ACTIVE & 1) e[0] = A.eb[q ^ 1][0][i];
     if (ACTIVE & 2) e[1] = A.eb[q ^ 1][1][i];
     if (ACTIVE & 4) e[2] = A.eb[q ^ 1][2][i];
-    if (ACTIVE == 63 && (fast & 1) && g.active == 63) {
+    if (ACTIVE == 63 && fast && g.active == 63) {
         switch (adj_class(A, x0, y0, z, false, 1)) {
             case 0: adj_h_fast<T, 0>(A, q, x, y, z, i, e); return;
             case 1: adj_h_fast<T, 1>(A, q, x, y, z, i, e); return;

@@ -2419,9 +2419,8 @@ int adjoint_step_t(tfd_adjoint *adj, const void *snapshot, const void *seeds, cu
         return dim3((unsigned)((g.n[0] + xs + kAdjX - 1) / kAdjX), (unsigned)((g.n[1] + ys + kAdjY - 1) / kAdjY), (unsigned)g.n[2]);
     };
     const dim3 ge = grid_of(exs, eys), gh = grid_of(hxs, hys);
-    // TFD_ADJ_FAST=0: the general path alone; TFD_ADJ_PREFETCH=0: no L2 prefetch (both for comparisons).
-    const char *env = getenv("TFD_ADJ_FAST"), *penv = getenv("TFD_ADJ_PREFETCH");
-    const int fast = ((env && std::atoi(env) == 0) ? 0 : 1) | ((penv && std::atoi(penv) == 0) ? 0 : 2);
+    const char *env = getenv("TFD_ADJ_FAST");
+    const int fast = (env && std::atoi(env) == 0) ? 0 : 1;
     const dim3 block(kAdjX, kAdjY);
     const T *slot = (const T *)snapshot;
     switch (p->desc.components) {
