@@ -178,6 +178,12 @@ __global__ void __launch_bounds__(128) k_step_gather_rows(const __grid_constant_
 // The step split in two launches (plans with TFSF boxes, whose E corrections must land between the E and the
 // H update, and plans with dispersive materials, whose pole states each E sample advances exactly once): the E
 // kernel writes E_new and the E-family CPML memories, the H kernel reads E_new back.
+// Whether the cell's family-f CPML row on axis a is absent (no slab there) and no metric factor applies.
+template <typename T>
+__device__ __forceinline__ bool gather_plain_axis(const Grid<T> &g, int f, int a, int coord) {
+    return g.metric[f][a] == nullptr && (g.row[f][a] == nullptr || g.row[f][a][coord] < 0);
+}
+
 template <typename T, int ACTIVE>
 __global__ void __launch_bounds__(128) k_step_gather_e(const __grid_constant__ Grid<T> g) {
     const long long n = *g.counter;
@@ -188,6 +194,47 @@ __global__ void __launch_bounds__(128) k_step_gather_e(const __grid_constant__ G
     const int z = blockIdx.x / g.n[1];
     if (x >= g.n[0]) return;
     const long long i = (long long)z * g.plane + (long long)y * g.pitch + x;
+    // Plain cells (all six components advanced; on every axis of the grid the -1 neighbour exists and no
+    // E-family CPML term or metric factor applies): the bare backward differences, every H value loaded before
+    // the stores; the general path's arithmetic reduces to exactly this there (then ADE and sources as usual).
+    if (ACTIVE == 63 && g.active == 63 && x >= 1 && gather_plain_axis(g, 0, 0, x) && (y >= 1 || g.n[1] == 1) &&
+        (g.n[1] == 1 || gather_plain_axis(g, 0, 1, y)) && (z >= 1 || g.n[2] == 1) && (g.n[2] == 1 || gather_plain_axis(g, 0, 2, z))) {
+        T hc[3], hm[3][2], eo[3], ie[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            hc[c] = g.H[par][c][i];
+            eo[c] = g.E[par][c][i];
+            ie[c] = g.inv_eps[c][i];
+        }
+#pragma unroll
+        for (int C = 0; C < 3; ++C)
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const Term t = term_of(C, k);
+                hm[C][k] = g.n[t.axis] == 1 ? T(0) : g.H[par][t.in][i - g.stride(t.axis)];
+            }
+        T e[3];
+#pragma unroll
+        for (int C = 0; C < 3; ++C) {
+            T acc = T(0);
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const Term t = term_of(C, k);
+                if (g.n[t.axis] == 1) continue;
+                const T d = hc[t.in] - hm[C][k];
+                acc = acc + (t.sign > 0 ? d : -d);
+            }
+            T v = eo[C] + (g.cn * ie[C]) * acc;
+            if (g.ade_map[C] != nullptr) {
+                const int j = g.ade_map[C][i];
+                if (j >= 0) v = ade_correct(g, j, eo[C], v, true);
+            }
+            e[C] = inject(g, 0, C, n, x, y, z, v);
+        }
+#pragma unroll
+        for (int C = 0; C < 3; ++C) g.E[par ^ 1][C][i] = e[C];
+        return;
+    }
     if (ACTIVE & 1) g.E[par ^ 1][0][i] = e_value<T, 0>(g, par, n, x, y, z, i, true);
     if (ACTIVE & 2) g.E[par ^ 1][1][i] = e_value<T, 1>(g, par, n, x, y, z, i, true);
     if (ACTIVE & 4) g.E[par ^ 1][2][i] = e_value<T, 2>(g, par, n, x, y, z, i, true);
@@ -207,6 +254,37 @@ __global__ void __launch_bounds__(128) k_step_gather_h(const __grid_constant__ G
     if (ACTIVE & 1) e[0] = g.E[par ^ 1][0][i];
     if (ACTIVE & 2) e[1] = g.E[par ^ 1][1][i];
     if (ACTIVE & 4) e[2] = g.E[par ^ 1][2][i];
+    // Plain cells: on every axis of the grid the +1 neighbour exists and no H-family CPML term or metric factor
+    // applies; the bare forward differences of the stored E_new.
+    if (ACTIVE == 63 && g.active == 63 && x < g.n[0] - 1 && gather_plain_axis(g, 1, 0, x) && (y < g.n[1] - 1 || g.n[1] == 1) &&
+        (g.n[1] == 1 || gather_plain_axis(g, 1, 1, y)) && (z < g.n[2] - 1 || g.n[2] == 1) && (g.n[2] == 1 || gather_plain_axis(g, 1, 2, z))) {
+        T ep[3][2], ho[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ho[c] = g.H[par][c][i];
+#pragma unroll
+        for (int C = 0; C < 3; ++C)
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const Term t = term_of(C, k);
+                ep[C][k] = g.n[t.axis] == 1 ? T(0) : g.E[par ^ 1][t.in][i + g.stride(t.axis)];
+            }
+        T h[3];
+#pragma unroll
+        for (int C = 0; C < 3; ++C) {
+            T acc = T(0);
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const Term t = term_of(C, k);
+                if (g.n[t.axis] == 1) continue;
+                const T d = ep[C][k] - e[t.in];
+                acc = acc + (t.sign > 0 ? d : -d);
+            }
+            h[C] = inject(g, 1, C, n, x, y, z, ho[C] - g.cn * acc);
+        }
+#pragma unroll
+        for (int C = 0; C < 3; ++C) g.H[par ^ 1][C][i] = h[C];
+        return;
+    }
     if (ACTIVE & 8) g.H[par ^ 1][0][i] = h_value<T, 0, true>(g, par, n, x, y, z, i, e);
     if (ACTIVE & 16) g.H[par ^ 1][1][i] = h_value<T, 1, true>(g, par, n, x, y, z, i, e);
     if (ACTIVE & 32) g.H[par ^ 1][2][i] = h_value<T, 2, true>(g, par, n, x, y, z, i, e);
