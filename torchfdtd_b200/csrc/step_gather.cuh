@@ -213,6 +213,9 @@ __global__ void __launch_bounds__(128) k_step_gather_e(const __grid_constant__ G
                 const Term t = term_of(C, k);
                 hm[C][k] = g.n[t.axis] == 1 ? T(0) : g.H[par][t.in][i - g.stride(t.axis)];
             }
+        int jc[3];
+#pragma unroll
+        for (int C = 0; C < 3; ++C) jc[C] = g.ade_map[C] != nullptr ? g.ade_map[C][i] : -1;
         T e[3];
 #pragma unroll
         for (int C = 0; C < 3; ++C) {
@@ -224,13 +227,45 @@ __global__ void __launch_bounds__(128) k_step_gather_e(const __grid_constant__ G
                 const T d = hc[t.in] - hm[C][k];
                 acc = acc + (t.sign > 0 ? d : -d);
             }
-            T v = eo[C] + (g.cn * ie[C]) * acc;
-            if (g.ade_map[C] != nullptr) {
-                const int j = g.ade_map[C][i];
-                if (j >= 0) v = ade_correct(g, j, eo[C], v, true);
-            }
-            e[C] = inject(g, 0, C, n, x, y, z, v);
+            e[C] = eo[C] + (g.cn * ie[C]) * acc;
         }
+        if (jc[0] >= 0 || jc[1] >= 0 || jc[2] >= 0) {
+            // Dispersive samples: the pole states of every component are loaded before any correction is computed
+            // (single-pole states; several poles take ade_correct). Same arithmetic as ade_correct.
+            int st_of[3], l_of[3];
+            T Pv[3], Qv[3];
+#pragma unroll
+            for (int C = 0; C < 3; ++C) {
+                st_of[C] = -1;
+                if (jc[C] < 0) continue;
+                int s = 0;
+                while (s + 1 < g.n_ade && jc[C] >= g.ade[s + 1].start) ++s;
+                st_of[C] = s;
+                l_of[C] = jc[C] - g.ade[s].start;
+                if (g.ade[s].poles == 1) {
+                    Pv[C] = g.ade[s].P[l_of[C]];
+                    Qv[C] = g.ade[s].Q[l_of[C]];
+                }
+            }
+#pragma unroll
+            for (int C = 0; C < 3; ++C) {
+                if (jc[C] < 0) continue;
+                const AdeDev<T> &st = g.ade[st_of[C]];
+                if (st.poles != 1) {
+                    e[C] = ade_correct(g, jc[C], eo[C], e[C], true);
+                    continue;
+                }
+                const T resp = (Qv[C] - st.a[0] * Pv[C]) / st.d[0];
+                const T total = resp;
+                const T v = (st.eps * e[C] - st.ksum * eo[C] - total) / st.denom;
+                const T delta = resp + st.k[0] * (v + eo[C]);
+                st.P[l_of[C]] = Pv[C] + delta;
+                st.Q[l_of[C]] = -Qv[C] + T(2) * delta;
+                e[C] = v;
+            }
+        }
+#pragma unroll
+        for (int C = 0; C < 3; ++C) e[C] = inject(g, 0, C, n, x, y, z, e[C]);
 #pragma unroll
         for (int C = 0; C < 3; ++C) g.E[par ^ 1][C][i] = e[C];
         return;

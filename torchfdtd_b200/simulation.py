@@ -269,6 +269,7 @@ class Observer:
         self.interval = max(r.snapshot_interval, math.ceil(r.steps / 100))
         self.frames, self.frame_steps = [], []
         self.host_fields = None                     # future of prefaulted (E, H) host arrays, large grids
+        self.ring = None                            # future of the pinned download staging ring, large grids
         self.diagnostic_seconds = 0.
 
     def decimate(self, a):
@@ -338,6 +339,8 @@ class Observer:
             e_dev, h_dev = grid.fields_device()
             t_wait = time.perf_counter()
             e_out, h_out = self.host_fields.result() if self.host_fields is not None else (None, None)
+            if self.ring is not None:
+                self.ring.result()
             t_copy = time.perf_counter()
             e, h = download(e_dev, out=e_out), download(h_dev, out=h_out)
             t_done = time.perf_counter()
@@ -494,14 +497,13 @@ class Simulation:
         shape, dtype = (*plan.shape, 3), np.dtype(plan.dtype)
         large = math.prod(shape) * dtype.itemsize > LARGE_FIELD_BYTES
         if large:
-            # Helper threads pin the download's staging ring (a CUDA host allocation: it overlaps the plan creation
-            # and the uploads and is waited for before the graph capture, which must not see it) and, once the
-            # device arena exists, map the result's host arrays (host memory only; started after the arena
-            # because the page zeroing slows a concurrent device allocation).
+            # Helper threads pin the download's staging ring and map the result's host arrays while the device
+            # steps. Both start once the graphs are captured: the ring is a CUDA host allocation, which a capture
+            # must not see, and the page zeroing of either slowed the device arena allocation and the graph
+            # instantiation when they ran beside them.
             from concurrent.futures import ThreadPoolExecutor
             from .native import host_buffer, staging_ring
             helper = ThreadPoolExecutor(max_workers=2)
-            ring = helper.submit(staging_ring, torch.float32 if dtype == np.float32 else torch.float64)
         grid, graphs = None, {}
         try:
             variant, tuning = 0, None
@@ -518,17 +520,11 @@ class Simulation:
             if tuning is not None:
                 lap('launch_tuning')
             grid = NativeGrid(plan, kernel=kernel, variant=variant, permittivity=permittivity)
-            if large:
-                host_fields = helper.submit(lambda: (host_buffer(shape, dtype), host_buffer(shape, dtype)))
             phases.update(grid.timing)
             mark[0] = time.perf_counter()
             free, _ = torch.cuda.mem_get_info()
             observer = Observer(p, plan, grid)
-            observer.host_fields = host_fields
             lap('observer')
-            if ring is not None:
-                ring.result()                           # pinned once per process, before any capture
-                lap('staging_ring')
             width = 1
             stream = torch.cuda.Stream()
             stream.wait_stream(torch.cuda.current_stream())
@@ -544,6 +540,10 @@ class Simulation:
                 torch.cuda.synchronize()
             torch.cuda.synchronize()
             lap('graph_capture')
+            if large:
+                ring = helper.submit(staging_ring, torch.float32 if dtype == np.float32 else torch.float64)
+                host_fields = helper.submit(lambda: (host_buffer(shape, dtype), host_buffer(shape, dtype)))
+                observer.host_fields, observer.ring = host_fields, ring
             setup_seconds = time.perf_counter() - started
             compute_start = time.perf_counter()
             completed, termination_reason, replays = 0, 'max_steps', 0
