@@ -131,3 +131,33 @@ def test_float32_against_float64_runs_of_the_same_kernels():
     assert out['tmz2d']['trace'] < 1e-5 and out['tmz2d']['spectrum'] < 1e-5
     assert max(out['tmz2d'][k] for k in ('Ez', 'Hx', 'Hy')) < 5e-2
     assert max(v for v in out['strip'].values()) < 1e-5
+
+
+@pytest.mark.parametrize('precision', ['float32', 'float64'])
+def test_graded_mesh_306x306x172_metric_mixed_launch_every_memory(precision):
+    """The graded-mesh workload (metric equidistribution, auto-refined box, physically graded CPML) for 10 steps
+    through the metric mixed march launch: the pure body with metric factors on the interior block, the general
+    metric body elsewhere; fields, every CPML memory and the traces bitwise against the C oracle."""
+    from torchfdtd_b200.native import NativeGrid
+    project, eps = config_project('graded', 10, precision)
+    plan = plan_grid(project)
+    if eps is not None:
+        plan.epsilon, plan.inv_eps = eps, (1 / eps).astype(plan.dtype)
+    assert plan.metrics, 'the workload must run on a nonuniform mesh'
+    grid = NativeGrid(plan)
+    assert grid.kernel == 'march'
+    grid.step(10)
+    E, H = grid.get_fields()
+    psi = grid.get_psi()
+    traces = grid.get_traces()
+    status = grid.device_status()
+    grid.close()
+    assert status == 0
+    oracle = CpuOracle(plan).run(10)
+    np.testing.assert_array_equal(E, oracle.E)
+    np.testing.assert_array_equal(H, oracle.H)
+    assert len(psi) == len(oracle.memory_states)
+    for got, want in zip(psi, oracle.memory_states):
+        np.testing.assert_array_equal(got, want)
+    np.testing.assert_array_equal(traces[:10], oracle.traces[:10])
+    assert np.abs(E).max() > 0

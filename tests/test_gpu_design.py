@@ -40,3 +40,28 @@ def test_adjoint_loop_improves_and_surrogate_loop_is_verified_by_fdtd():
     assert len(hist) >= 1 and all(np.isfinite(f) for _, f, _ in hist)
     verified = problem.fom(problem.transmission([torch.sigmoid(best_theta).cpu().numpy()]))[0]
     assert abs(verified - best) <= 1e-5 * max(1, abs(best))                         # FDTD judged the best design
+
+
+def test_surrogate_loop_reaches_the_plain_fom_in_less_time():
+    """The race on the reduced scene, from the same start (theta = 0, rho = 0.5): the plain adjoint loop runs 20
+    iterations; the surrogate-assisted loop, with a network trained on 1024 batched FDTD samples, must reach the
+    plain loop's FDTD-verified FOM within 1 % in less wall time (every design it reports is FDTD-verified).
+    Dataset generation and training are not timed: they are paid once for many designs."""
+    import torch
+    from torchfdtd_b200.design import adjoint_design, generate_dataset, surrogate_design
+    from torchfdtd_b200.surrogate import ConvNeuralOperator
+    problem = small_problem()
+    rhos, targets, _ = generate_dataset(problem, count=1024, seed=2)
+    net = ConvNeuralOperator(outputs=32, seed=0, input_shape=(40, 40))
+    rho_t, y_t = torch.tensor(rhos, device='cuda'), torch.tensor(targets, device='cuda')
+    net.fit(rho_t, y_t, epochs=20, batch=64, lr=2e-3)
+    adjoint_design(problem, iterations=2, lr=.3)                                     # loads the kernels once
+    history, _ = adjoint_design(problem, iterations=20, lr=.3)
+    plain_seconds, plain_fom = history[-1]
+    hist, best, best_theta = surrogate_design(problem, net, target_fom=0.99 * plain_fom, iterations=200, lr=.3,
+                                              verify_every=5, finetune_steps=5, data=(rho_t, y_t), max_seconds=2 * plain_seconds)
+    seconds = hist[-1][0]
+    verified = problem.fom(problem.transmission([torch.sigmoid(best_theta).cpu().numpy()]))[0]
+    assert abs(verified - best) <= 1e-5 * max(1, abs(best))
+    assert best >= 0.99 * plain_fom, (best, plain_fom)
+    assert seconds < plain_seconds, (seconds, plain_seconds)

@@ -928,6 +928,8 @@ int setup_march_s(tfd_plan *p, int split, int lz_fixed) {
                                       (int)p->march_smem));
         TFD_CUDA(cudaFuncSetAttribute(k_step_march<T, SAMPLES, D, MINB, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)p->march_smem));
+        TFD_CUDA(cudaFuncSetAttribute(k_step_march_mixed<T, SAMPLES, D, MINB, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)p->march_smem));
     }
     const int edge_mode = seams ? 2 : 0;
     int device = 0, sms = 148, per_sm = 1;
@@ -1077,12 +1079,14 @@ int setup_march(tfd_plan *p) {
                                          (sizeof(T) == 8 ? std::string("22 (FP64)") : std::string("14, 22, 23, 32")));
     const bool three = p->desc.material_samples == 3;
     const Grid<T> &g = p->grid<T>();
-    // A nonuniform mesh runs the general body with its metric factors, one launch over all tiles, at the
-    // launch shape the periodic-seam body is built for.
+    // A nonuniform mesh runs the metric bodies at the launch shape the periodic-seam body is built for: the mixed
+    // launch (pure body on the interior block) by default, the general body alone for split digits 1 and 2 and
+    // with periodic seams.
     p->march_metric = false;
     for (int f = 0; f < 2; ++f)
         for (int a = 0; a < 3; ++a) p->march_metric = p->march_metric || g.metric[f][a] != nullptr;
-    const int sp = p->march_metric ? 2 : split;
+    // Nonuniform meshes: the metric mixed launch (pure body on the interior block) unless a split is asked for.
+    const int sp = (p->march_metric && (split == 1 || split == 2 || g.periodic[0] || g.periodic[1])) ? 2 : split;
     switch ((g.periodic[0] || g.periodic[1] || p->march_metric) ? periodic_march_variant<T>() : dm) {
         case 22: return three ? setup_march_s<T, 3, 2, 2>(p, sp, lz) : setup_march_s<T, 1, 2, 2>(p, sp, lz);
         case 32: return three ? setup_march_s<T, 3, 3, 2>(p, sp, lz) : setup_march_s<T, 1, 3, 2>(p, sp, lz);
@@ -1100,7 +1104,11 @@ void launch_march(tfd_plan *p, cudaStream_t s) {
         cudaStream_t st = k == 0 ? s : p->aux[k - 1];
         if (k > 0) cudaStreamWaitEvent(st, p->fork, 0);
         if (l.mode == 3) {
-            if (p->grid<T>().periodic[0] || p->grid<T>().periodic[1]) {
+            if (p->march_metric) {
+                if constexpr (D * 10 + MINB == periodic_march_variant<T>())
+                    k_step_march_mixed<T, SAMPLES, D, MINB, 0, true><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(),
+                                                                                                                p->march_mix);
+            } else if (p->grid<T>().periodic[0] || p->grid<T>().periodic[1]) {
                 if constexpr (D * 10 + MINB == periodic_march_variant<T>())
                     k_step_march_mixed<T, SAMPLES, D, MINB, 2><<<l.grid, kMarchThreads, p->march_smem, st>>>(p->march<T>(), p->march_mix);
             } else {

@@ -678,7 +678,7 @@ __device__ __forceinline__ void march_body(const MarchArgs<T> &args, int tx, int
     // step at 512 x 512 x 128. With x / y slabs the general work is mostly x / y slab rows, and the extra tier
     // cost the 512 x 512 x 256 CPML step 1.3 % (instruction cache); there the z-pure body takes them.
     constexpr bool ZTIER = (MODE == 2 || ZPURE) && !METRIC;
-    static_assert(!METRIC || MODE == 0 || MODE == 2, "the metric variant is a general body");
+    static_assert(!METRIC || MODE == 0 || MODE == 1 || MODE == 2, "the metric variants are the general and pure bodies");
     static_assert(!(XPURE || YPURE) || !METRIC, "the x- and y-boundary bodies assume a uniform mesh");
     // The general and z-pure bodies keep their row loops rolled: unrolled, the general body's three row tiers
     // exist once per row and the code outgrows the instruction cache once a pure body shares the SM
@@ -1091,7 +1091,9 @@ struct MarchMix {
     int lz[3], chunks[3];
 };
 
-template <typename T, int SAMPLES, int D, int MINB, int GEN>
+// METRIC (a nonuniform mesh, GEN 0): the pure body with the metric factors on the interior block's pure planes,
+// the general metric body elsewhere (the z-pure and boundary bodies assume unit factors).
+template <typename T, int SAMPLES, int D, int MINB, int GEN, bool METRIC = false>
 __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march_mixed(const __grid_constant__ MarchArgs<T> args,
                                                                           const __grid_constant__ MarchMix mx) {
     int zc = blockIdx.z, seg = 0;
@@ -1104,6 +1106,11 @@ __global__ void __launch_bounds__(kMarchThreads, MINB) k_step_march_mixed(const 
     const int tx = blockIdx.x, ty = blockIdx.y;
     const bool yband = ty >= mx.iy0 && ty < mx.iy1;
     const bool interior = tx >= mx.ix0 && tx < mx.ix1 && yband;
+    if constexpr (METRIC) {
+        if (interior && seg == 1) march_body<T, SAMPLES, D, 1, true>(args, tx, ty, z0, z1);
+        else march_body<T, SAMPLES, D, 0, true>(args, tx, ty, z0, z1);
+        return;
+    }
     if (interior && seg == 1)
         march_body<T, SAMPLES, D, 1>(args, tx, ty, z0, z1);
     else if (interior)
