@@ -315,8 +315,6 @@ std::vector<Tile2D> strips_of(const StripGeom &G, int grid_index, int rows) {
         }
         return true;
     };
-    // Rows per general strip (TFD_2D_GENERAL_ROWS in the environment overrides, 0 keeps the interior strips' rows).
-    static const int general_rows = getenv("TFD_2D_GENERAL_ROWS") ? std::atoi(getenv("TFD_2D_GENERAL_ROWS")) : 8;
     std::vector<Tile2D> t;
     for (size_t b = 0; b < bands.size(); ++b) {
         const bool inner = bands.size() == 3 && b == 1;
@@ -324,13 +322,7 @@ std::vector<Tile2D> strips_of(const StripGeom &G, int grid_index, int rows) {
             const int y1 = std::min(y0 + rows, bands[b].second);
             for (int x0 = 0; x0 < nx; x0 += k2dOwnX) {
                 const int kind = inner && !G.metric && x_interior(x0) && no_source(x0, y0, y1) ? 1 : 0;
-                if (kind == 1 || general_rows <= 0) {
-                    t.push_back(Tile2D{grid_index, x0, y0, y1, kind});
-                    continue;
-                }
-                // General strips are latency-bound chains of dependent row updates: cut into shorter pieces,
-                // more of them run side by side.
-                for (int a = y0; a < y1; a += general_rows) t.push_back(Tile2D{grid_index, x0, a, std::min(a + general_rows, y1), 0});
+                t.push_back(Tile2D{grid_index, x0, y0, y1, kind});
             }
         }
     }
@@ -343,9 +335,8 @@ int interior_count(const std::vector<Tile2D> &t) {
     return (int)std::count_if(t.begin(), t.end(), [](const Tile2D &a) { return a.kind == 1; });
 }
 
-// Upper bound of the strip count of a grid for strips of at least 8 rows (each of the three row bands may end
-// in a shorter strip).
-int strip_capacity(int nx, int ny) { return ((nx + k2dOwnX - 1) / k2dOwnX) * ((ny + 7) / 8 + 3); }
+// Upper bound of the strip count of a grid for strips of at least 8 rows (two band edges add two cuts).
+int strip_capacity(int nx, int ny) { return ((nx + k2dOwnX - 1) / k2dOwnX) * ((ny + 7) / 8 + 2); }
 
 // 2D TMz grids up to this many cells step in one persistent launch (see setup_tile2d), over strips of
 // persist2d_strip_rows() rows. TFD_PERSIST2D=0/1 and TFD_PERSIST_ROWS in the environment override both,
