@@ -493,14 +493,14 @@ class Simulation:
 
         plan, permittivity = self._run_plan()
         lap('plan')
-        helper = None
+        helper, host_fields, ring = None, None, None
         shape, dtype = (*plan.shape, 3), np.dtype(plan.dtype)
         large = math.prod(shape) * dtype.itemsize > LARGE_FIELD_BYTES
         if large:
             # Helper threads pin the download's staging ring and map the result's host arrays while the device
-            # steps. Both start once the first steps are queued (prepare() below): the ring is a CUDA host
-            # allocation, which a graph capture must not see, and the page zeroing of either slowed the device
-            # arena allocation and the graph instantiation when they ran beside them.
+            # steps. Both start once the graphs are captured: the ring is a CUDA host allocation, which a capture
+            # must not see, and the page zeroing of either slowed the device arena allocation and the graph
+            # instantiation when they ran beside them.
             from concurrent.futures import ThreadPoolExecutor
             from .native import host_buffer, staging_ring
             helper = ThreadPoolExecutor(max_workers=2)
@@ -540,15 +540,10 @@ class Simulation:
                 torch.cuda.synchronize()
             torch.cuda.synchronize()
             lap('graph_capture')
-            prepared = [not large]
-
-            def prepare():
-                # Once the first steps are queued on the device: the helpers' pinning and page mapping then run
-                # while it works (the pinned allocation can hold the interpreter lock while it pins).
-                if not prepared[0]:
-                    observer.ring = helper.submit(staging_ring, torch.float32 if dtype == np.float32 else torch.float64)
-                    observer.host_fields = helper.submit(lambda: (host_buffer(shape, dtype), host_buffer(shape, dtype)))
-                    prepared[0] = True
+            if large:
+                ring = helper.submit(staging_ring, torch.float32 if dtype == np.float32 else torch.float64)
+                host_fields = helper.submit(lambda: (host_buffer(shape, dtype), host_buffer(shape, dtype)))
+                observer.host_fields, observer.ring = host_fields, ring
             setup_seconds = time.perf_counter() - started
             compute_start = time.perf_counter()
             completed, termination_reason, replays = 0, 'max_steps', 0
@@ -562,12 +557,10 @@ class Simulation:
                         replays += 1
                     else:
                         grid.step(advance, stream)
-                    prepare()
                     completed = target
                     if observer.observe(completed, progress, compute_start):
                         termination_reason = 'decayed'
                         break
-            prepare()
             torch.cuda.synchronize()
             seconds = time.perf_counter() - compute_start
             phases['stepping'] = seconds
