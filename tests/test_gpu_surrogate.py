@@ -78,3 +78,52 @@ def test_training_fits_a_smooth_map():
     net = ConvNeuralOperator(outputs=2, seed=0, input_shape=(20, 20))
     history = net.fit(rho, target, epochs=15, batch=64, lr=3e-3)
     assert history[-1] < .1 * history[0]
+
+
+@pytest.mark.parametrize('ci,stride,shape', [(16, 1, (3, 24, 20)), (64, 2, (2, 33, 17)), (64, 1, (4, 40, 40)), (16, 1, (2, 61, 57))])
+def test_backward_weight_paths_agree_and_match_float64(ci, stride, shape):
+    """tfd_sg_conv_backward_weight on the tcgen05 kernel (taps stacked in M, MN-major operands, bias from a ones
+    row) and on the mma.sync kernel, against dW[tap, co, ci] = sum_p dz[p, co] x[in(p, tap), ci] and
+    dbias[co] = sum_p dz[p, co] summed in float64 over the same BF16 operands. Shapes with more than one
+    4096-pixel chunk and a ragged last 32-pixel block are included."""
+    import ctypes
+    import torch
+    from torchfdtd_b200.surrogate import WGRAD_CHUNK, _lib, device_status, out_size, set_tensor_path
+    lib, check = _lib()
+    n, h, w = shape
+    ho, wo = out_size(h, stride), out_size(w, stride)
+    gen = torch.Generator().manual_seed(ci + stride + h)
+    x = torch.randn((n, h, w, ci), generator=gen).to(torch.bfloat16)
+    dz = torch.randn((n, ho, wo, 64), generator=gen).to(torch.bfloat16)
+    size = ctypes.c_size_t()
+    check(lib.tfd_sg_wgrad_scratch(n, h, w, ci, stride, WGRAD_CHUNK, ctypes.byref(size)))
+    scratch = torch.empty(size.value // 4 + 1, dtype=torch.float32, device='cuda')
+    xd, dzd = x.cuda(), dz.cuda()
+    results = {}
+    for path in ('tcgen05', 'mma'):
+        set_tensor_path(path)
+        try:
+            dw = torch.full((9, 64, ci), float('nan'), device='cuda')
+            db = torch.full((64,), float('nan'), device='cuda')
+            check(lib.tfd_sg_conv_backward_weight(ctypes.c_void_p(dzd.data_ptr()), ctypes.c_void_p(xd.data_ptr()),
+                                                  ctypes.c_void_p(dw.data_ptr()), ctypes.c_void_p(db.data_ptr()),
+                                                  ctypes.c_void_p(scratch.data_ptr()), size.value, n, h, w, ci, stride, WGRAD_CHUNK,
+                                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+            torch.cuda.synchronize()
+            results[path] = (dw.cpu().numpy().astype(np.float64), db.cpu().numpy().astype(np.float64))
+        finally:
+            set_tensor_path('tcgen05')
+    assert device_status() == 0
+    xs, dzs = x.double().numpy(), dz.double().numpy().reshape(-1, 64)
+    pad = np.zeros((n, h + 2, w + 2, ci))
+    pad[:, 1:-1, 1:-1] = xs
+    expected = np.empty((9, 64, ci))
+    for t in range(9):
+        ky, kx = divmod(t, 3)
+        xt = pad[:, ky:ky + stride * (ho - 1) + 1:stride, kx:kx + stride * (wo - 1) + 1:stride].reshape(-1, ci)
+        expected[t] = dzs.T @ xt
+    expected_bias = dzs.sum(axis=0)
+    for path, (dw, db) in results.items():
+        assert rel(dw, expected) <= 1e-5, path
+        assert rel(db, expected_bias) <= 1e-5, path
+    assert rel(results['tcgen05'][0], results['mma'][0]) <= 1e-5

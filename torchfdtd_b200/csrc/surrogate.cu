@@ -1,7 +1,8 @@
 // Learned surrogate: a small convolutional neural operator (8 conv layers, 64 channels) mapping a 2D design
 // density to its complex transmission spectrum, trained and evaluated by these kernels.
 //
-// Numerics: BF16 operands, FP32 accumulation (tensor-core mma.sync m16n8k16, bf16 x bf16 -> f32), FP32
+// Numerics: BF16 operands, FP32 accumulation (tcgen05 kind::f16 into tensor memory by default, or warp-level
+// mma.sync m16n8k16 as the selectable legacy path; bf16 x bf16 -> f32), FP32
 // master weights, bias, head (linear on the flattened last feature map), loss and Adam state. Activations are NHWC bf16 with C = 16 (the packed input:
 // density, x, y, 1, zeros) or C = 64, so one pixel is one or four 16-byte vectors.
 //
@@ -9,9 +10,11 @@
 //   forward          z[p, co] = bias[co] + sum_{tap, ci} x[in(p, tap), ci] w[tap, co, ci];  a = gelu(z)
 //   backward (data)  dx[q, ci] = sum_{tap, co} dz[out(q, tap), co] w[tap, co, ci]  (then * gelu'(z_prev))
 //   backward (weight) dw[tap, co, ci] = sum_p dz[p, co] x[in(p, tap), ci]; dbias[co] = sum_p dz[p, co]
-// All three are implicit GEMMs on 64 x 64 tiles: 4 warps, each 16 rows x 64 columns of m16n8k16 MMAs, with
-// the operands staged in shared memory (row-major A, column-major B, both padded to 144-byte rows so the
-// fragment loads are bank-conflict free).
+// All three are implicit GEMMs. The tcgen05 kernels (k_conv_tc for forward and backward data, k_wgrad_tc for
+// backward weight) stage cp.async gathers in shared memory for MMAs issued by one thread into tensor memory. The
+// mma.sync kernels work on 64 x 64 tiles: 4 warps, each 16 rows x 64 columns of m16n8k16 MMAs, with the operands
+// staged in shared memory (row-major A, column-major B, both padded to 144-byte rows so the fragment loads are
+// bank-conflict free).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -592,7 +595,143 @@ __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, c
     if (warp == 0) tmem_free<COLS>(tmem);
 }
 
-int g_tensor_path = 1;       // 1: tcgen05 kernels for conv forward / backward data; 0: mma.sync kernels
+// ---- tcgen05 backward weight ----------------------------------------------------------------------------
+// dW^T as one GEMM per chunk of output pixels: rows (tap, ci) -- all 9 taps stacked, 9 * CI rows, plus one row
+// of ones whose product with dz is the bias gradient -- times columns co, K = pixels. Both operands are staged
+// MN-major (no swizzle): for each 8-element chunk of rows (or of co), the stage's 32 pixels lie 16 bytes apart
+// (8-pixel core matrices 128 bytes apart = LBO, row chunks KB * 16 bytes apart = SBO), so a pixel's gathered
+// 16-byte vector lands whole. The rows are split into MT tiles of M = 128, each with its own 64-column
+// accumulator in tensor memory; the padding rows past the ones row stay zero. Three stages: the cp.async gathers
+// of block b+2 are in flight while the tensor cores work on block b. Bounded waits as in k_conv_tc.
+constexpr int kWgKB = 32;                          // pixels per stage (two K = 16 MMA steps)
+template <int CI>
+struct WgradShape {
+    static constexpr int ROWS = 9 * CI;                    // (tap, ci) rows; row ROWS is the ones row
+    static constexpr int MT = (ROWS + 1 + 127) / 128;      // M = 128 tiles
+    static constexpr int MCH = MT * 16;                    // 8-row chunks of A
+    static constexpr int A_BYTES = MCH * kWgKB * 16;
+    static constexpr int B_BYTES = 8 * kWgKB * 16;         // 64 co = 8 chunks
+    static constexpr int COLS = MT * 64 <= 32 ? 32 : MT * 64 <= 64 ? 64 : MT * 64 <= 128 ? 128 : MT * 64 <= 256 ? 256 : 512;
+    static constexpr int SMEM = kStages * (A_BYTES + B_BYTES) + 64;
+};
+
+template <int CI>
+__global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dZ, const bf16 *__restrict__ X, float *__restrict__ partial,
+                                                 float *__restrict__ partial_bias, int N, int H, int W, int Ho, int Wo, int stride,
+                                                 int chunk) {
+    using S = WgradShape<CI>;
+    constexpr int CC = CI / 8;                             // 16-byte chunks of one input pixel
+    constexpr uint32_t IDESC = umma_idesc(128, kCo) | (1u << 15) | (1u << 16);   // A and B MN-major
+    constexpr uint32_t LBO = 8 * 16, SBO = kWgKB * 16;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *As = smem, *Bs = smem + kStages * S::A_BYTES;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Bs + kStages * S::B_BYTES);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + kStages);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long P = (long long)N * Ho * Wo;
+    const long long begin = (long long)blockIdx.x * chunk;
+    const long long end = begin + chunk < P ? begin + chunk : P;
+    const int blocks = (int)((end - begin + kWgKB - 1) / kWgKB);
+    if (warp == 0) tmem_alloc<S::COLS>(slot);
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) bar_init(&bar[s]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // The rows past the gathered ones never change: the ones row (element 0 of its chunk) and zero padding.
+    for (int e = tid; e < kStages * (S::MCH - S::ROWS / 8) * kWgKB; e += 128) {
+        const int s = e / ((S::MCH - S::ROWS / 8) * kWgKB), r = e % ((S::MCH - S::ROWS / 8) * kWgKB);
+        const int mc = S::ROWS / 8 + r / kWgKB, j = r % kWgKB;
+        *reinterpret_cast<uint4 *>(As + s * S::A_BYTES + (mc * kWgKB + j) * 16) =
+            make_uint4(mc == S::ROWS / 8 ? 0x3F80u : 0u, 0u, 0u, 0u);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+
+    // Gathers of pixel block b into its stage: lane = pixel of the block, warp = a quarter of the chunks.
+    auto issue = [&](int b) {
+        const int s = b % kStages;
+        const long long p = begin + (long long)b * kWgKB + lane;
+        const bool live = p < end;
+        const int n = live ? (int)(p / ((long long)Ho * Wo)) : 0;
+        const int rem = live ? (int)(p % ((long long)Ho * Wo)) : 0;
+        const int oy = rem / Wo, ox = rem % Wo;
+        unsigned char *as = As + s * S::A_BYTES + lane * 16;
+        for (int i = warp; i < 9 * CC; i += 4) {
+            const int t = i / CC, c = i % CC;
+            const int iy = oy * stride + t / 3 - 1, ix = ox * stride + t % 3 - 1;
+            const bool in = live && iy >= 0 && iy < H && ix >= 0 && ix < W;
+            const bf16 *src = in ? X + (((long long)n * H + iy) * W + ix) * CI + c * 8 : X;
+            cp_async16(as + i * (kWgKB * 16), src, in ? 16 : 0);
+        }
+        unsigned char *bs = Bs + s * S::B_BYTES + lane * 16;
+        for (int c = warp; c < 8; c += 4) cp_async16(bs + c * (kWgKB * 16), live ? dZ + p * kCo + c * 8 : dZ, live ? 16 : 0);
+        cp_async_commit();
+    };
+
+    bool ok = true;
+    int issued = 0;
+    issue(0);
+    if (blocks > 1) issue(1);
+    else cp_async_commit();
+    for (int b = 0; b < blocks; ++b) {
+        const int s = b % kStages;
+        if (b + 2 < blocks) {
+            // Stage (b + 2) % 3 was last read by the MMAs of block b - 1.
+            if (b >= 1 && !bar_wait(&bar[(b - 1) % kStages], ((b - 1) / kStages) & 1)) ok = false;
+            if (__syncthreads_or(!ok)) break;
+            issue(b + 2);
+        } else {
+            cp_async_commit();
+        }
+        cp_async_wait<2>();
+        proxy_fence();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t as = sh_addr(As + s * S::A_BYTES), bs = sh_addr(Bs + s * S::B_BYTES);
+#pragma unroll
+            for (int kk = 0; kk < kWgKB / 16; ++kk) {
+                const uint64_t bd = umma_desc(bs + kk * 256, LBO, SBO);
+#pragma unroll
+                for (int m = 0; m < S::MT; ++m)
+                    umma_bf16(tmem + m * kCo, umma_desc(as + m * 16 * SBO + kk * 256, LBO, SBO), bd, IDESC, (b | kk) != 0);
+            }
+            umma_commit(&bar[s]);
+        }
+        issued = b + 1;
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (issued > 0 && !bar_wait(&bar[(issued - 1) % kStages], ((issued - 1) / kStages) & 1)) ok = false;
+    tc_fence_after();
+    if (__syncthreads_or(!ok) || issued < blocks) {
+        if (tid == 0) atomicExch(&g_sg_status, 1);
+    } else {
+#pragma unroll 1
+        for (int m = 0; m < S::MT; ++m) {
+            const int r = m * 128 + warp * 32 + lane;         // this lane's row: (tap, ci) or the ones row
+#pragma unroll
+            for (int c0 = 0; c0 < kCo; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + m * kCo + c0, v);
+                if (r < S::ROWS) {
+                    float *o = partial + ((long long)blockIdx.x * 9 + r / CI) * kCo * CI + r % CI;
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) o[(c0 + i) * CI] = v[i];
+                } else if (r == S::ROWS) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) partial_bias[(long long)blockIdx.x * kCo + c0 + i] = v[i];
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_free<S::COLS>(tmem);
+}
+
+int g_tensor_path = 1;       // 1: tcgen05 kernels for the convolutions; 0: mma.sync kernels
 
 int blocks_for(long long work, int threads) {
     const long long b = (work + threads - 1) / threads;
@@ -619,7 +758,7 @@ int out_size(int n, int stride) { return (n - 1) / stride + 1; }
 
 extern "C" {
 
-// 1: conv forward and backward data on the tcgen05 kernels (default); 0: on the mma.sync kernels.
+// 1: conv forward, backward data and backward weight on the tcgen05 kernels (default); 0: on the mma.sync kernels.
 int tfd_sg_set_tensor_path(int32_t mode) {
     if (mode != 0 && mode != 1) return bad("tfd_sg_set_tensor_path: mode 0 or 1");
     g_tensor_path = mode;
@@ -724,10 +863,25 @@ int tfd_sg_conv_backward_weight(const void *dz, const void *x, float *dw, float 
     const int chunks = (int)((P + chunk - 1) / chunk);
     float *partial = scratch, *partial_bias = scratch + (long long)chunks * 9 * kCo * ci;
     cudaStream_t s = (cudaStream_t)stream;
-    const dim3 grid((unsigned)chunks, 9);
-    if (ci == 16) k_conv_wgrad<16><<<grid, kThreads, 0, s>>>((const bf16 *)dz, (const bf16 *)x, partial, partial_bias, n, h, wd, ho, wo, stride, chunk);
-    else k_conv_wgrad<64><<<grid, kThreads, 0, s>>>((const bf16 *)dz, (const bf16 *)x, partial, partial_bias, n, h, wd, ho, wo, stride, chunk);
-    if ((rc = check_launch("tfd_sg_conv_backward_weight"))) return rc;
+    if (g_tensor_path) {
+        if (ci == 16) {
+            static const cudaError_t attr = cudaFuncSetAttribute(k_wgrad_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, WgradShape<16>::SMEM);
+            (void)attr;
+            k_wgrad_tc<16><<<chunks, 128, WgradShape<16>::SMEM, s>>>((const bf16 *)dz, (const bf16 *)x, partial, partial_bias, n, h, wd, ho, wo,
+                                                                    stride, chunk);
+        } else {
+            static const cudaError_t attr = cudaFuncSetAttribute(k_wgrad_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, WgradShape<64>::SMEM);
+            (void)attr;
+            k_wgrad_tc<64><<<chunks, 128, WgradShape<64>::SMEM, s>>>((const bf16 *)dz, (const bf16 *)x, partial, partial_bias, n, h, wd, ho, wo,
+                                                                    stride, chunk);
+        }
+        if ((rc = check_launch("tfd_sg_conv_backward_weight (tcgen05)"))) return rc;
+    } else {
+        const dim3 grid((unsigned)chunks, 9);
+        if (ci == 16) k_conv_wgrad<16><<<grid, kThreads, 0, s>>>((const bf16 *)dz, (const bf16 *)x, partial, partial_bias, n, h, wd, ho, wo, stride, chunk);
+        else k_conv_wgrad<64><<<grid, kThreads, 0, s>>>((const bf16 *)dz, (const bf16 *)x, partial, partial_bias, n, h, wd, ho, wo, stride, chunk);
+        if ((rc = check_launch("tfd_sg_conv_backward_weight"))) return rc;
+    }
     const long long len = 9LL * kCo * ci;
     k_reduce_partials<<<blocks_for(len, 256), 256, 0, s>>>(partial, chunks, len, dw);
     k_reduce_partials<<<1, kCo, 0, s>>>(partial_bias, chunks, kCo, dbias);

@@ -49,8 +49,8 @@ def _lib():
 
 
 def set_tensor_path(mode):
-    """'tcgen05' (default): conv forward and backward data on the 5th-generation tensor cores with tensor-memory
-    accumulators; 'mma': on warp-level mma.sync kernels (the backward-weight kernel always uses mma.sync)."""
+    """'tcgen05' (default): conv forward, backward data and backward weight on the 5th-generation tensor cores with
+    tensor-memory accumulators; 'mma': on warp-level mma.sync kernels."""
     lib, check = _lib()
     check(lib.tfd_sg_set_tensor_path({'mma': 0, 'tcgen05': 1}[mode]))
 
