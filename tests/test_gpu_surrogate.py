@@ -18,7 +18,7 @@ def rel(a, b):
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-30))
 
 
-@pytest.fixture(params=['tcgen05', 'mma'])
+@pytest.fixture(params=['tcgen05', 'tcgen05_gather', 'mma'])
 def tensor_path(request):
     from torchfdtd_b200.surrogate import set_tensor_path
     set_tensor_path(request.param)
@@ -127,3 +127,61 @@ def test_backward_weight_paths_agree_and_match_float64(ci, stride, shape):
         assert rel(dw, expected) <= 1e-5, path
         assert rel(db, expected_bias) <= 1e-5, path
     assert rel(results['tcgen05'][0], results['mma'][0]) <= 1e-5
+
+
+def _conv_reference(x, w, stride):
+    """z[p, co] = sum_{tap, ci} x[in(p, tap), ci] w[tap, co, ci] in float64 (zero padding 1)."""
+    n, h, wd, ci = x.shape
+    ho, wo = (h - 1) // stride + 1, (wd - 1) // stride + 1
+    pad = np.zeros((n, h + 2, wd + 2, ci))
+    pad[:, 1:-1, 1:-1] = x
+    z = np.zeros((n, ho, wo, w.shape[1]))
+    for t in range(9):
+        ky, kx = divmod(t, 3)
+        z += pad[:, ky:ky + stride * (ho - 1) + 1:stride, kx:kx + stride * (wo - 1) + 1:stride] @ w[t].T
+    return z
+
+
+@pytest.mark.parametrize('ci,shape', [(16, (3, 24, 20)), (64, (2, 33, 17)), (64, (64, 40, 40)), (16, (5, 100, 100)), (64, (1, 9, 500))])
+def test_shifted_window_conv_matches_the_gather_kernel_and_float64(ci, shape):
+    """Stride-1 forward and backward data on the shifted-window tcgen05 kernel against the per-tap gather kernel
+    and against float64 sums of the same BF16 operands: grids whose padded rows do not fill whole 128-row tiles,
+    more tiles than CTAs (the persistent loop), and a 500-wide row whose patch exceeds shared memory (both paths
+    then run the gather kernel)."""
+    import ctypes
+    import torch
+    from torchfdtd_b200.surrogate import _lib, device_status, set_tensor_path
+    lib, check = _lib()
+    n, h, w = shape
+    gen = torch.Generator().manual_seed(ci + h + w)
+    x = torch.randn((n, h, w, ci), generator=gen).to(torch.bfloat16)
+    wt = (torch.randn((9, 64, ci), generator=gen) / (3 * ci ** .5)).to(torch.bfloat16)
+    wt_t = wt.transpose(1, 2).contiguous()                          # [tap][ci][co] for backward data
+    bias = torch.randn(64, generator=gen) * .1
+    dz = torch.randn((n, h, w, 64), generator=gen).to(torch.bfloat16)
+    dev = {k: v.cuda() for k, v in dict(x=x, w=wt, wt=wt_t, bias=bias, dz=dz).items()}
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {}
+    for path in ('tcgen05', 'tcgen05_gather'):
+        set_tensor_path(path)
+        try:
+            z = torch.empty((n, h, w, 64), dtype=torch.bfloat16, device='cuda')
+            a = torch.empty_like(z)
+            dx = torch.full((n, h, w, ci), float('nan'), device='cuda')
+            check(lib.tfd_sg_conv_forward(ptr(dev['x']), ptr(dev['w']), ptr(dev['bias']), ptr(z), ptr(a), n, h, w, ci, 1, stream))
+            check(lib.tfd_sg_conv_backward_data(ptr(dev['dz']), ptr(dev['wt']), None, ptr(dx), n, h, w, ci, 1, stream))
+            torch.cuda.synchronize()
+            out[path] = (z.float().cpu().numpy(), a.float().cpu().numpy(), dx.cpu().numpy())
+        finally:
+            set_tensor_path('tcgen05')
+    assert device_status() == 0
+    zref = _conv_reference(x.double().numpy(), wt.double().numpy(), 1) + bias.double().numpy()
+    # backward data = the conv of dz with the taps flipped and the weights transposed
+    dxref = _conv_reference(dz.double().numpy(), wt_t.double().numpy()[::-1], 1)
+    for path, (z, a, dx) in out.items():
+        assert rel(z, zref) <= 1e-2, path
+        assert rel(dx, dxref) <= 1e-5, path
+    assert rel(out['tcgen05'][0], out['tcgen05_gather'][0]) <= 1e-3
+    assert rel(out['tcgen05'][1], out['tcgen05_gather'][1]) <= 1e-3
+    assert rel(out['tcgen05'][2], out['tcgen05_gather'][2]) <= 1e-5

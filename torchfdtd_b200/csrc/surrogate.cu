@@ -731,7 +731,212 @@ __global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dZ, c
     if (warp == 0) tmem_free<S::COLS>(tmem);
 }
 
-int g_tensor_path = 1;       // 1: tcgen05 kernels for the convolutions; 0: mma.sync kernels
+// ---- tcgen05 shifted-window conv (stride 1) -------------------------------------------------------------
+// With stride 1, a tap of the 3x3 conv is a shift of a flattened, zero-padded image: give the image a zero
+// border (width Wp = W + 2) and number its pixels g = py * Wp + px; output pixel (y, x) at f = y * Wp + x
+// reads tap (ky, kx) of the forward conv at g = f + ky * Wp + kx, and backward data (a conv of dz with the
+// taps flipped) at g = f + (2 - ky) * Wp + (2 - kx). A CTA takes M = 128 consecutive f of one image (the two
+// border columns of each row are computed and dropped) and loads the padded pixels [f0, f0 + NP) once, NP =
+// 128 + 2 Wp + 2, into shared memory in the K-major no-swizzle layout with rows 16 bytes apart ([K chunk]
+// [pixel][16 bytes], K chunks LBO apart): the A operand of every tap is then the same patch with the
+// descriptor's start moved by 16 bytes per pixel of shift. The 9 taps' weights stay in shared memory for the
+// whole persistent tile loop. A ring of NB = 2..4 patch buffers (as many as fit) with the loads issued NB - 1
+// tiles ahead, and two tensor-memory accumulators: while the tensor cores work on tile j, the CTA stores tile
+// j-1's outputs and loads tile j+NB-1's patch. Bounded waits as in k_conv_tc.
+template <int MODE, int CI>
+struct ShiftShape {
+    static constexpr int K = MODE == 0 ? CI : kCo;         // reduction channels per tap
+    static constexpr int NC = MODE == 0 ? kCo : CI;        // output columns
+    static constexpr int KC = K / 8;                        // 16-byte K chunks
+    static constexpr int W_BYTES = 9 * KC * NC * 16;       // resident weights: [tap][K chunk][column][16 bytes]
+    static constexpr int COLS = 2 * NC < 32 ? 32 : 2 * NC;  // two accumulators
+    // K chunks of a patch lie (NP + LPAD) * 16 bytes apart: with NP a multiple of 8, the 8 (or 2) chunks of a
+    // pixel that a quarter-warp stores land on distinct banks.
+    static constexpr int LPAD = KC == 8 ? 1 : 4;
+};
+constexpr int kShiftThreads = 256;                        // 8 warps: 4 lane quarters x 2 column halves
+constexpr int kShiftMaxSmem = 227 * 1024;
+constexpr int kShiftSmPerSm = 228 * 1024;                  // shared memory of an SM (1 KB of it reserved per CTA)
+__host__ __device__ constexpr int shift_np(int W) { return (128 + 2 * (W + 2) + 2 + 7) / 8 * 8; }
+
+template <int MODE, int CI>
+__global__ void __launch_bounds__(kShiftThreads) k_conv_shift(const bf16 *__restrict__ src, const bf16 *__restrict__ wsrc,
+                                                             const float *__restrict__ bias, const bf16 *__restrict__ zprev,
+                                                             bf16 *__restrict__ out0, void *__restrict__ out1, int N, int H, int W, int NB) {
+    using S = ShiftShape<MODE, CI>;
+    constexpr int K = S::K, NC = S::NC, KC = S::KC;
+    constexpr uint32_t IDESC = umma_idesc(128, NC);
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const int Wp = W + 2, np = shift_np(W);
+    const int lbo = (np + S::LPAD) * 16, pbytes = KC * lbo;
+    unsigned char *ws = smem, *ps = smem + S::W_BYTES;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(ps + NB * pbytes);     // bar[i]: MMA commit of the tiles in buffer i
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 4);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles_img = (H * Wp + 127) / 128, tiles = N * tiles_img;
+    if (warp == 0) tmem_alloc<S::COLS>(slot);
+    if (tid == 0) {
+        for (int i = 0; i < NB; ++i) bar_init(&bar[i]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *slot;
+
+    for (int e = tid; e < 9 * NC * KC; e += kShiftThreads) {
+        const int kc = e % KC, col = (e / KC) % NC, tap = e / (KC * NC);
+        cp_async16(ws + ((tap * KC + kc) * NC + col) * 16, wsrc + ((long long)tap * NC + col) * K + kc * 8, 16);
+    }
+    // Patch of local tile j (global tile blockIdx.x + j * gridDim.x) into buffer j % NB: padded pixels
+    // [f0, f0 + np) of its image, zero outside the image. One cp.async group per call, empty past the last tile.
+    auto load = [&](int j) {
+        const int tile = blockIdx.x + j * gridDim.x;
+        if (tile < tiles) {
+            unsigned char *p = ps + (j % NB) * pbytes;
+            const int n = tile / tiles_img, f0 = (tile % tiles_img) * 128;
+            for (int e = tid; e < np * KC; e += kShiftThreads) {
+                const int kc = e % KC, i = e / KC, g = f0 + i;
+                const int py = g / Wp, px = g - py * Wp;
+                const bool in = py >= 1 && py <= H && px >= 1 && px <= W;
+                const bf16 *s = in ? src + (((long long)n * H + py - 1) * W + px - 1) * K + kc * 8 : src;
+                cp_async16(p + kc * lbo + i * 16, s, in ? 16 : 0);
+            }
+        }
+        cp_async_commit();
+    };
+    // Outputs of local tile j from accumulator j & 1: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 (its
+    // rows) and the columns of half w / 4 (all of them with warps 0-3 when NC = 16).
+    auto store = [&](int j) {
+        const int tile = blockIdx.x + j * gridDim.x;
+        const int quarter = warp & 3, half = warp >> 2;
+        constexpr int HALF = NC >= 32 ? NC / 2 : NC;
+        if (NC < 32 && half) return;
+        const int n = tile / tiles_img, f = (tile % tiles_img) * 128 + quarter * 32 + lane;
+        const int oy = f / Wp, ox = f - oy * Wp;
+        const bool live = oy < H && ox < W;
+        const long long row = ((long long)n * H + oy) * W + ox;
+#pragma unroll
+        for (int c0 = half * HALF; c0 < half * HALF + HALF; c0 += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (j & 1) * NC + c0, v);
+            if (!live) continue;
+            if (MODE == 0) {
+                __align__(16) bf16 zb[16], ab[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const float z = v[i] + bias[c0 + i];
+                    zb[i] = __float2bfloat16_rn(z);
+                    ab[i] = __float2bfloat16_rn(gelu(z));
+                }
+                uint4 *zd = reinterpret_cast<uint4 *>(out0 + row * kCo + c0);
+                uint4 *adst = reinterpret_cast<uint4 *>(reinterpret_cast<bf16 *>(out1) + row * kCo + c0);
+                zd[0] = reinterpret_cast<const uint4 *>(zb)[0];
+                zd[1] = reinterpret_cast<const uint4 *>(zb)[1];
+                adst[0] = reinterpret_cast<const uint4 *>(ab)[0];
+                adst[1] = reinterpret_cast<const uint4 *>(ab)[1];
+            } else if (zprev) {
+                __align__(16) bf16 zp[16], db[16];
+                reinterpret_cast<uint4 *>(zp)[0] = reinterpret_cast<const uint4 *>(zprev + row * CI + c0)[0];
+                reinterpret_cast<uint4 *>(zp)[1] = reinterpret_cast<const uint4 *>(zprev + row * CI + c0)[1];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) db[i] = __float2bfloat16_rn(v[i] * gelu_grad(__bfloat162float(zp[i])));
+                uint4 *dd = reinterpret_cast<uint4 *>(out0 + row * CI + c0);
+                dd[0] = reinterpret_cast<const uint4 *>(db)[0];
+                dd[1] = reinterpret_cast<const uint4 *>(db)[1];
+            } else {
+                float4 *o = reinterpret_cast<float4 *>(reinterpret_cast<float *>(out1) + row * CI + c0);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            }
+        }
+    };
+
+    const int count = (int)blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;   // local tiles
+    bool ok = true;
+    int committed = 0, waited = 0;                 // local tiles whose MMAs were committed / waited for
+    for (int j = 0; j < NB - 1; ++j) load(j);      // the weights ride in the first group
+    for (int j = 0; j < count; ++j) {
+        // Groups committed so far: NB - 1 + j; tile j's is complete when at most NB - 2 are pending.
+        if (NB == 2) cp_async_wait<0>();
+        else if (NB == 3) cp_async_wait<1>();
+        else cp_async_wait<2>();
+        proxy_fence();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t pa = sh_addr(ps + (j % NB) * pbytes), wa = sh_addr(ws);
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                const int ky = t / 3, kx = t % 3;
+                const int shift = MODE == 0 ? ky * Wp + kx : (2 - ky) * Wp + (2 - kx);
+#pragma unroll
+                for (int kk = 0; kk < K / 16; ++kk) {
+                    const uint64_t ad = umma_desc(pa + shift * 16 + kk * 2 * lbo, lbo, 128);
+                    const uint64_t bd = umma_desc(wa + (t * KC + 2 * kk) * NC * 16, NC * 16, 128);
+                    umma_bf16(tmem + (j & 1) * NC, ad, bd, IDESC, (t | kk) != 0);
+                }
+            }
+            umma_commit(&bar[j % NB]);
+        }
+        committed = j + 1;
+        // Tile j-1's MMAs: once done, its buffer takes tile j+NB-1 and its accumulator is stored while the
+        // tensor cores work on tile j.
+        if (j >= 1) {
+            if (!bar_wait(&bar[(j - 1) % NB], ((j - 1) / NB) & 1)) ok = false;
+            if (__syncthreads_or(!ok)) break;
+            waited = j;
+            tc_fence_after();
+        }
+        load(j + NB - 1);
+        if (j >= 1) store(j - 1);
+        tc_fence_before();
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (committed > waited) {
+        const int last = committed - 1;
+        if (!bar_wait(&bar[last % NB], (last / NB) & 1)) ok = false;
+        tc_fence_after();
+        if (!__syncthreads_or(!ok) && waited == last) store(last);
+    }
+    if (__syncthreads_or(!ok) && tid == 0) atomicExch(&g_sg_status, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_free<S::COLS>(tmem);
+}
+
+// Launches the shifted-window kernel when at least two patch buffers fit in shared memory (image rows up to a
+// few hundred pixels); false when the caller should use the gather kernel instead.
+template <int MODE, int CI>
+bool launch_shift(const bf16 *src, const bf16 *w, const float *bias, const bf16 *zprev, bf16 *o0, void *o1, int n, int h, int wd,
+                  cudaStream_t s) {
+    using S = ShiftShape<MODE, CI>;
+    const long long pbytes = (long long)S::KC * (shift_np(wd) + S::LPAD) * 16;
+    int nb = 4;
+    while (nb >= 2 && S::W_BYTES + nb * pbytes + 64 > kShiftMaxSmem) --nb;
+    if (nb < 2) return false;
+    const int smem = (int)(S::W_BYTES + nb * pbytes + 64);
+    static const cudaError_t attr = cudaFuncSetAttribute(k_conv_shift<MODE, CI>, cudaFuncAttributeMaxDynamicSharedMemorySize, kShiftMaxSmem);
+    (void)attr;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+            sms = 148;
+    }
+    int per_sm = kShiftSmPerSm / (smem + 1024);
+    per_sm = per_sm < 512 / S::COLS ? per_sm : 512 / S::COLS;      // tensor-memory columns of an SM
+    per_sm = per_sm < 2048 / kShiftThreads ? per_sm : 2048 / kShiftThreads;
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    const long long tiles = (long long)n * ((h * (wd + 2) + 127) / 128);
+    const long long grid = tiles < (long long)sms * per_sm ? tiles : (long long)sms * per_sm;
+    k_conv_shift<MODE, CI><<<(unsigned)grid, kShiftThreads, (size_t)smem, s>>>(src, w, bias, zprev, o0, o1, n, h, wd, nb);
+    return true;
+}
+
+// 0: mma.sync kernels; 1: tcgen05 kernels, the shifted-window form for stride-1 layers where it fits (default);
+// 2: tcgen05 kernels, the per-tap gather form for every layer.
+int g_tensor_path = 1;
 
 int blocks_for(long long work, int threads) {
     const long long b = (work + threads - 1) / threads;
@@ -758,9 +963,11 @@ int out_size(int n, int stride) { return (n - 1) / stride + 1; }
 
 extern "C" {
 
-// 1: conv forward, backward data and backward weight on the tcgen05 kernels (default); 0: on the mma.sync kernels.
+// 1: conv forward, backward data and backward weight on the tcgen05 kernels, stride-1 layers in the
+// shifted-window form where it fits (default); 2: the same with the per-tap gather form for every layer;
+// 0: on the mma.sync kernels.
 int tfd_sg_set_tensor_path(int32_t mode) {
-    if (mode != 0 && mode != 1) return bad("tfd_sg_set_tensor_path: mode 0 or 1");
+    if (mode < 0 || mode > 2) return bad("tfd_sg_set_tensor_path: mode 0, 1 or 2");
     g_tensor_path = mode;
     return TFD_OK;
 }
@@ -793,6 +1000,11 @@ int tfd_sg_conv_forward(const void *x, const void *w, const float *bias, void *z
     const int ho = out_size(h, stride), wo = out_size(wd, stride);
     const long long P = (long long)n * ho * wo;
     cudaStream_t s = (cudaStream_t)stream;
+    if (g_tensor_path == 1 && stride == 1) {
+        const bool done = ci == 16 ? launch_shift<0, 16>((const bf16 *)x, (const bf16 *)w, bias, nullptr, (bf16 *)z, a, n, h, wd, s)
+                                   : launch_shift<0, 64>((const bf16 *)x, (const bf16 *)w, bias, nullptr, (bf16 *)z, a, n, h, wd, s);
+        if (done) return check_launch("tfd_sg_conv_forward (tcgen05, shifted window)");
+    }
     if (g_tensor_path) {
         const dim3 grid((unsigned)((P + 127) / 128));
         if (ci == 16) {
@@ -819,10 +1031,15 @@ int tfd_sg_conv_backward_data(const void *dz, const void *wt, const void *zprev,
     const int ho = out_size(h, stride), wo = out_size(wd, stride);
     const long long Q = (long long)n * h * wd;
     cudaStream_t s = (cudaStream_t)stream;
+    bf16 *o0 = zprev ? (bf16 *)out : nullptr;
+    void *o1 = zprev ? nullptr : out;
+    if (g_tensor_path == 1 && stride == 1) {
+        const bool done = ci == 16 ? launch_shift<1, 16>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd, s)
+                                   : launch_shift<1, 64>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd, s);
+        if (done) return check_launch("tfd_sg_conv_backward_data (tcgen05, shifted window)");
+    }
     if (g_tensor_path) {
         const dim3 grid((unsigned)((Q + 127) / 128));
-        bf16 *o0 = zprev ? (bf16 *)out : nullptr;
-        void *o1 = zprev ? nullptr : out;
         if (ci == 16) {
             static const cudaError_t attr = cudaFuncSetAttribute(k_conv_tc<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(64, 16));
             (void)attr;

@@ -50,9 +50,11 @@ def _lib():
 
 def set_tensor_path(mode):
     """'tcgen05' (default): conv forward, backward data and backward weight on the 5th-generation tensor cores with
-    tensor-memory accumulators; 'mma': on warp-level mma.sync kernels."""
+    tensor-memory accumulators, stride-1 layers as shifted windows of a patch loaded once per tile (where the patch
+    fits in shared memory); 'tcgen05_gather': the same kernels with a per-tap gather for every layer; 'mma': on
+    warp-level mma.sync kernels."""
     lib, check = _lib()
-    check(lib.tfd_sg_set_tensor_path({'mma': 0, 'tcgen05': 1}[mode]))
+    check(lib.tfd_sg_set_tensor_path({'mma': 0, 'tcgen05': 1, 'tcgen05_gather': 2}[mode]))
 
 
 def device_status():
