@@ -62,13 +62,21 @@ __device__ __forceinline__ void warp_gemm(float (&acc)[NT][4], const bf16 *A, in
     }
 }
 
+// GELU (tanh form) with the hardware tanh (tanh.approx.f32, one MUFU operation, relative error about 2^-11): the
+// activations are rounded to BF16 (2^-8) right after, and the epilogues of the conv kernels are bound by this
+// arithmetic, not by their memory traffic.
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 __device__ __forceinline__ float gelu(float z) {
     const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
-    return 0.5f * z * (1.0f + tanhf(u));
+    return 0.5f * z * (1.0f + tanh_hw(u));
 }
 __device__ __forceinline__ float gelu_grad(float z) {
     const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
-    const float th = tanhf(u);
+    const float th = tanh_hw(u);
     return 0.5f * (1.0f + th) + 0.5f * z * (1.0f - th * th) * 0.7978845608028654f * (1.0f + 3.0f * 0.044715f * z * z);
 }
 
@@ -245,12 +253,32 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad(const bf16 *__restrict_
     if (tap == 4 && threadIdx.x < kCo) partial_bias[(long long)blockIdx.x * kCo + threadIdx.x] = bias_acc;
 }
 
-__global__ void k_reduce_partials(const float *__restrict__ partial, int chunks, long long len, float *__restrict__ out) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < len; e += (long long)gridDim.x * blockDim.x) {
-        float s = 0.f;
-        for (int c = 0; c < chunks; ++c) s += partial[(long long)c * len + e];
-        out[e] = s;
+// out[e] = the sum over chunks c, in chunk order, of partial[c * len + e]; the threads past the weights reduce the
+// bias partials (len_b per chunk) the same way. Each thread has eight chunks' loads in flight at a time.
+__global__ void k_reduce_partials(const float *__restrict__ partial, int chunks, long long len, float *__restrict__ out,
+                                  const float *__restrict__ partial_b, int len_b, float *__restrict__ out_b) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const float *src;
+    long long stride;
+    float *dst;
+    if (e < len) {
+        src = partial + e, stride = len, dst = out + e;
+    } else if (e < len + len_b) {
+        src = partial_b + (e - len), stride = len_b, dst = out_b + (e - len);
+    } else {
+        return;
     }
+    float s = 0.f;
+    int c = 0;
+    for (; c + 8 <= chunks; c += 8) {
+        float v[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = src[(long long)(c + i) * stride];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) s += v[i];
+    }
+    for (; c < chunks; ++c) s += src[(long long)c * stride];
+    *dst = s;
 }
 
 // ---- input packing, head, loss, optimiser ---------------------------------------------------------------
@@ -740,9 +768,10 @@ __global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dZ, c
 // 128 + 2 Wp + 2, into shared memory in the K-major no-swizzle layout with rows 16 bytes apart ([K chunk]
 // [pixel][16 bytes], K chunks LBO apart): the A operand of every tap is then the same patch with the
 // descriptor's start moved by 16 bytes per pixel of shift. The 9 taps' weights stay in shared memory for the
-// whole persistent tile loop. A ring of NB = 2..4 patch buffers (as many as fit) with the loads issued NB - 1
-// tiles ahead, and two tensor-memory accumulators: while the tensor cores work on tile j, the CTA stores tile
-// j-1's outputs and loads tile j+NB-1's patch. Bounded waits as in k_conv_tc.
+// whole persistent tile loop. A ring of NB = 2..4 patch buffers (as many as fit) and two tensor-memory
+// accumulators, with loads, MMAs and stores in separate warps: while the tensor cores work on tile j, the
+// storing warps drain tile j-1 and the loading warps fill the buffers of the tiles after j. Every wait is bounded;
+// a role that times out sets the CTA's abort flag and the status word, and the other roles give up their waits.
 template <int MODE, int CI>
 struct ShiftShape {
     static constexpr int K = MODE == 0 ? CI : kCo;         // reduction channels per tap
@@ -754,154 +783,204 @@ struct ShiftShape {
     // pixel that a quarter-warp stores land on distinct banks.
     static constexpr int LPAD = KC == 8 ? 1 : 4;
 };
-constexpr int kShiftThreads = 256;                        // 8 warps: 4 lane quarters x 2 column halves
+constexpr int kShiftThreads = 384;                        // 12 warps: MMA issue, 3 loading, 8 storing
 constexpr int kShiftMaxSmem = 227 * 1024;
 constexpr int kShiftSmPerSm = 228 * 1024;                  // shared memory of an SM (1 KB of it reserved per CTA)
 __host__ __device__ constexpr int shift_np(int W) { return (128 + 2 * (W + 2) + 2 + 7) / 8 * 8; }
 
+// Bounded wait that also gives up once another role of the CTA has aborted (*abort set).
+__device__ __forceinline__ bool bar_wait_or_abort(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    const uint32_t addr = sh_addr(bar);
+    for (int it = 0; it < 20000; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done) : "r"(addr), "r"(parity), "r"(100000u) : "memory");
+        if (done) return true;
+        if (*abort) return false;
+    }
+    *abort = 1;
+    atomicExch(&g_sg_status, 1);
+    return false;
+}
+
+__device__ __forceinline__ void bar_init_count(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sh_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sh_addr(bar)) : "memory");
+}
+
+// Warp roles: warp 0 issues the MMAs (one elected thread), warps 1-3 load patches, warps 4-11 store outputs (warp
+// 4 + q and 8 + q read tensor-memory lanes 32q..32q+31, one half of the columns each; with 16 columns warps 4-7
+// store alone). full[i]: the 96 loaders' patch of buffer i has landed (each loader waits for its own copies,
+// fences them for the tensor cores and arrives); empty[i]: the MMAs that read buffer i are done
+// (tcgen05.commit); accf[a]: accumulator a holds a finished tile (commit); acce[a]: the storing threads have
+// read accumulator a. A loader keeps two tiles of copies in flight and runs up to NB
+// tiles ahead of the tensor cores; the tensor cores run one tile ahead of the stores.
 template <int MODE, int CI>
 __global__ void __launch_bounds__(kShiftThreads) k_conv_shift(const bf16 *__restrict__ src, const bf16 *__restrict__ wsrc,
                                                              const float *__restrict__ bias, const bf16 *__restrict__ zprev,
                                                              bf16 *__restrict__ out0, void *__restrict__ out1, int N, int H, int W, int NB) {
     using S = ShiftShape<MODE, CI>;
     constexpr int K = S::K, NC = S::NC, KC = S::KC;
+    constexpr int LOADERS = 96;
+    constexpr int STORERS = NC >= 32 ? 256 : 128;          // threads that read an accumulator
+    constexpr int SPAN = NC >= 32 ? NC / 2 : NC;           // columns per storing warp
     constexpr uint32_t IDESC = umma_idesc(128, NC);
     extern __shared__ __align__(1024) unsigned char smem[];
     const int Wp = W + 2, np = shift_np(W);
     const int lbo = (np + S::LPAD) * 16, pbytes = KC * lbo;
     unsigned char *ws = smem, *ps = smem + S::W_BYTES;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(ps + NB * pbytes);     // bar[i]: MMA commit of the tiles in buffer i
-    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 4);
+    uint64_t *full = reinterpret_cast<uint64_t *>(ps + NB * pbytes);
+    uint64_t *empty = full + 4, *accf = full + 8, *acce = full + 10;
+    uint32_t *slot = reinterpret_cast<uint32_t *>(full + 12);
+    volatile int *abort = reinterpret_cast<volatile int *>(slot + 1);
+    float *sbias = reinterpret_cast<float *>(full + 13);      // forward: the 64 biases
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_img = (H * Wp + 127) / 128, tiles = N * tiles_img;
+    const int count = (int)blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;   // local tiles
     if (warp == 0) tmem_alloc<S::COLS>(slot);
     if (tid == 0) {
-        for (int i = 0; i < NB; ++i) bar_init(&bar[i]);
+        for (int i = 0; i < NB; ++i) {
+            bar_init_count(&full[i], LOADERS);
+            bar_init_count(&empty[i], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            bar_init_count(&accf[a], 1);
+            bar_init_count(&acce[a], STORERS);
+        }
+        *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    for (int e = tid; e < 9 * NC * KC; e += kShiftThreads) {
+        const int kc = e % KC, col = (e / KC) % NC, tap = e / (KC * NC);
+        cp_async16(ws + ((tap * KC + kc) * NC + col) * 16, wsrc + ((long long)tap * NC + col) * K + kc * 8, 16);
+    }
+    if (MODE == 0 && tid < kCo) sbias[tid] = bias[tid];
+    cp_async_commit();
+    cp_async_wait<0>();
+    proxy_fence();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *slot;
 
-    for (int e = tid; e < 9 * NC * KC; e += kShiftThreads) {
-        const int kc = e % KC, col = (e / KC) % NC, tap = e / (KC * NC);
-        cp_async16(ws + ((tap * KC + kc) * NC + col) * 16, wsrc + ((long long)tap * NC + col) * K + kc * 8, 16);
-    }
-    // Patch of local tile j (global tile blockIdx.x + j * gridDim.x) into buffer j % NB: padded pixels
-    // [f0, f0 + np) of its image, zero outside the image. One cp.async group per call, empty past the last tile.
-    auto load = [&](int j) {
-        const int tile = blockIdx.x + j * gridDim.x;
-        if (tile < tiles) {
-            unsigned char *p = ps + (j % NB) * pbytes;
+    if (warp >= 1 && warp <= 3) {
+        // Loaders: patch of local tile j = padded pixels [f0, f0 + np) of its image into buffer j % NB.
+        const int lt = tid - 32;
+        for (int j = 0; j < count; ++j) {
+            const int b = j % NB;
+            if (j >= NB && !bar_wait_or_abort(&empty[b], (j / NB - 1) & 1, abort)) break;
+            const int tile = blockIdx.x + j * gridDim.x;
             const int n = tile / tiles_img, f0 = (tile % tiles_img) * 128;
-            for (int e = tid; e < np * KC; e += kShiftThreads) {
+            unsigned char *p = ps + b * pbytes;
+            for (int e = lt; e < np * KC; e += LOADERS) {
                 const int kc = e % KC, i = e / KC, g = f0 + i;
                 const int py = g / Wp, px = g - py * Wp;
                 const bool in = py >= 1 && py <= H && px >= 1 && px <= W;
                 const bf16 *s = in ? src + (((long long)n * H + py - 1) * W + px - 1) * K + kc * 8 : src;
                 cp_async16(p + kc * lbo + i * 16, s, in ? 16 : 0);
             }
-        }
-        cp_async_commit();
-    };
-    // Outputs of local tile j from accumulator j & 1: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 (its
-    // rows) and the columns of half w / 4 (all of them with warps 0-3 when NC = 16).
-    auto store = [&](int j) {
-        const int tile = blockIdx.x + j * gridDim.x;
-        const int quarter = warp & 3, half = warp >> 2;
-        constexpr int HALF = NC >= 32 ? NC / 2 : NC;
-        if (NC < 32 && half) return;
-        const int n = tile / tiles_img, f = (tile % tiles_img) * 128 + quarter * 32 + lane;
-        const int oy = f / Wp, ox = f - oy * Wp;
-        const bool live = oy < H && ox < W;
-        const long long row = ((long long)n * H + oy) * W + ox;
-#pragma unroll
-        for (int c0 = half * HALF; c0 < half * HALF + HALF; c0 += 16) {
-            float v[16];
-            tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (j & 1) * NC + c0, v);
-            if (!live) continue;
-            if (MODE == 0) {
-                __align__(16) bf16 zb[16], ab[16];
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const float z = v[i] + bias[c0 + i];
-                    zb[i] = __float2bfloat16_rn(z);
-                    ab[i] = __float2bfloat16_rn(gelu(z));
-                }
-                uint4 *zd = reinterpret_cast<uint4 *>(out0 + row * kCo + c0);
-                uint4 *adst = reinterpret_cast<uint4 *>(reinterpret_cast<bf16 *>(out1) + row * kCo + c0);
-                zd[0] = reinterpret_cast<const uint4 *>(zb)[0];
-                zd[1] = reinterpret_cast<const uint4 *>(zb)[1];
-                adst[0] = reinterpret_cast<const uint4 *>(ab)[0];
-                adst[1] = reinterpret_cast<const uint4 *>(ab)[1];
-            } else if (zprev) {
-                __align__(16) bf16 zp[16], db[16];
-                reinterpret_cast<uint4 *>(zp)[0] = reinterpret_cast<const uint4 *>(zprev + row * CI + c0)[0];
-                reinterpret_cast<uint4 *>(zp)[1] = reinterpret_cast<const uint4 *>(zprev + row * CI + c0)[1];
-#pragma unroll
-                for (int i = 0; i < 16; ++i) db[i] = __float2bfloat16_rn(v[i] * gelu_grad(__bfloat162float(zp[i])));
-                uint4 *dd = reinterpret_cast<uint4 *>(out0 + row * CI + c0);
-                dd[0] = reinterpret_cast<const uint4 *>(db)[0];
-                dd[1] = reinterpret_cast<const uint4 *>(db)[1];
-            } else {
-                float4 *o = reinterpret_cast<float4 *>(reinterpret_cast<float *>(out1) + row * CI + c0);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            cp_async_commit();
+            if (j >= 1) {                                 // tile j-1's copies have landed
+                cp_async_wait<1>();
+                proxy_fence();
+                bar_arrive(&full[(j - 1) % NB]);
             }
         }
-    };
-
-    const int count = (int)blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;   // local tiles
-    bool ok = true;
-    int committed = 0, waited = 0;                 // local tiles whose MMAs were committed / waited for
-    for (int j = 0; j < NB - 1; ++j) load(j);      // the weights ride in the first group
-    for (int j = 0; j < count; ++j) {
-        // Groups committed so far: NB - 1 + j; tile j's is complete when at most NB - 2 are pending.
-        if (NB == 2) cp_async_wait<0>();
-        else if (NB == 3) cp_async_wait<1>();
-        else cp_async_wait<2>();
+        cp_async_wait<0>();
         proxy_fence();
-        __syncthreads();
-        if (tid == 0) {
+        if (count > 0 && !*abort) bar_arrive(&full[(count - 1) % NB]);
+    } else if (warp == 0) {
+        // The MMAs of local tile j into accumulator j & 1, one elected thread.
+        int committed = 0;
+        if (lane == 0) {
+            for (int j = 0; j < count; ++j) {
+                const int b = j % NB, a = j & 1;
+                if (!bar_wait_or_abort(&full[b], (j / NB) & 1, abort)) break;
+                if (j >= 2 && !bar_wait_or_abort(&acce[a], (j / 2 - 1) & 1, abort)) break;
+                tc_fence_after();
+                const uint32_t pa = sh_addr(ps + b * pbytes), wa = sh_addr(ws);
+#pragma unroll
+                for (int t = 0; t < 9; ++t) {
+                    const int ky = t / 3, kx = t % 3;
+                    const int shift = MODE == 0 ? ky * Wp + kx : (2 - ky) * Wp + (2 - kx);
+#pragma unroll
+                    for (int kk = 0; kk < K / 16; ++kk) {
+                        const uint64_t ad = umma_desc(pa + shift * 16 + kk * 2 * lbo, lbo, 128);
+                        const uint64_t bd = umma_desc(wa + (t * KC + 2 * kk) * NC * 16, NC * 16, 128);
+                        umma_bf16(tmem + a * NC, ad, bd, IDESC, (t | kk) != 0);
+                    }
+                }
+                umma_commit(&empty[b]);
+                umma_commit(&accf[a]);
+                committed = j + 1;
+            }
+            // On an abort, wait (bounded, whatever the flag) for the MMAs already issued before tensor memory is freed.
+            if (*abort && committed > 0) {
+                const int last = committed - 1;
+                uint32_t done = 0;
+                for (int it = 0; it < 20000 && !done; ++it)
+                    asm volatile(
+                        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+                        : "=r"(done) : "r"(sh_addr(&accf[last & 1])), "r"((last / 2) & 1), "r"(100000u) : "memory");
+            }
+        }
+        __syncwarp();
+    } else if ((warp - 4) * 32 < STORERS) {
+        // Stores of local tile j from accumulator j & 1: this thread's row (tensor-memory lane), SPAN columns.
+        const int quarter = (warp - 4) & 3, cbeg = ((warp - 4) >> 2) * SPAN;
+        for (int j = 0; j < count; ++j) {
+            const int a = j & 1;
+            if (!bar_wait_or_abort(&accf[a], (j / 2) & 1, abort)) break;
             tc_fence_after();
-            const uint32_t pa = sh_addr(ps + (j % NB) * pbytes), wa = sh_addr(ws);
+            const int tile = blockIdx.x + j * gridDim.x;
+            const int n = tile / tiles_img, f = (tile % tiles_img) * 128 + quarter * 32 + lane;
+            const int oy = f / Wp, ox = f - oy * Wp;
+            const bool live = oy < H && ox < W;
+            const long long row = ((long long)n * H + oy) * W + ox;
 #pragma unroll
-            for (int t = 0; t < 9; ++t) {
-                const int ky = t / 3, kx = t % 3;
-                const int shift = MODE == 0 ? ky * Wp + kx : (2 - ky) * Wp + (2 - kx);
+            for (int c0 = cbeg; c0 < cbeg + SPAN; c0 += 16) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + a * NC + c0, v);
+                if (!live) continue;
+                if (MODE == 0) {
+                    __align__(16) bf16 zb[16], ab[16];
 #pragma unroll
-                for (int kk = 0; kk < K / 16; ++kk) {
-                    const uint64_t ad = umma_desc(pa + shift * 16 + kk * 2 * lbo, lbo, 128);
-                    const uint64_t bd = umma_desc(wa + (t * KC + 2 * kk) * NC * 16, NC * 16, 128);
-                    umma_bf16(tmem + (j & 1) * NC, ad, bd, IDESC, (t | kk) != 0);
+                    for (int i = 0; i < 16; ++i) {
+                        const float z = v[i] + sbias[c0 + i];
+                        zb[i] = __float2bfloat16_rn(z);
+                        ab[i] = __float2bfloat16_rn(gelu(z));
+                    }
+                    uint4 *zd = reinterpret_cast<uint4 *>(out0 + row * kCo + c0);
+                    uint4 *adst = reinterpret_cast<uint4 *>(reinterpret_cast<bf16 *>(out1) + row * kCo + c0);
+                    zd[0] = reinterpret_cast<const uint4 *>(zb)[0];
+                    zd[1] = reinterpret_cast<const uint4 *>(zb)[1];
+                    adst[0] = reinterpret_cast<const uint4 *>(ab)[0];
+                    adst[1] = reinterpret_cast<const uint4 *>(ab)[1];
+                } else if (zprev) {
+                    __align__(16) bf16 zp[16], db[16];
+                    reinterpret_cast<uint4 *>(zp)[0] = reinterpret_cast<const uint4 *>(zprev + row * CI + c0)[0];
+                    reinterpret_cast<uint4 *>(zp)[1] = reinterpret_cast<const uint4 *>(zprev + row * CI + c0)[1];
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) db[i] = __float2bfloat16_rn(v[i] * gelu_grad(__bfloat162float(zp[i])));
+                    uint4 *dd = reinterpret_cast<uint4 *>(out0 + row * CI + c0);
+                    dd[0] = reinterpret_cast<const uint4 *>(db)[0];
+                    dd[1] = reinterpret_cast<const uint4 *>(db)[1];
+                } else {
+                    float4 *o = reinterpret_cast<float4 *>(reinterpret_cast<float *>(out1) + row * CI + c0);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
                 }
             }
-            umma_commit(&bar[j % NB]);
+            tc_fence_before();
+            bar_arrive(&acce[a]);
         }
-        committed = j + 1;
-        // Tile j-1's MMAs: once done, its buffer takes tile j+NB-1 and its accumulator is stored while the
-        // tensor cores work on tile j.
-        if (j >= 1) {
-            if (!bar_wait(&bar[(j - 1) % NB], ((j - 1) / NB) & 1)) ok = false;
-            if (__syncthreads_or(!ok)) break;
-            waited = j;
-            tc_fence_after();
-        }
-        load(j + NB - 1);
-        if (j >= 1) store(j - 1);
-        tc_fence_before();
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    if (committed > waited) {
-        const int last = committed - 1;
-        if (!bar_wait(&bar[last % NB], (last / NB) & 1)) ok = false;
-        tc_fence_after();
-        if (!__syncthreads_or(!ok) && waited == last) store(last);
-    }
-    if (__syncthreads_or(!ok) && tid == 0) atomicExch(&g_sg_status, 1);
     tc_fence_before();
     __syncthreads();
+    tc_fence_after();
     if (warp == 0) tmem_free<S::COLS>(tmem);
 }
 
@@ -912,10 +991,10 @@ bool launch_shift(const bf16 *src, const bf16 *w, const float *bias, const bf16 
                   cudaStream_t s) {
     using S = ShiftShape<MODE, CI>;
     const long long pbytes = (long long)S::KC * (shift_np(wd) + S::LPAD) * 16;
-    int nb = 4;
-    while (nb >= 2 && S::W_BYTES + nb * pbytes + 64 > kShiftMaxSmem) --nb;
+    int nb = 4;                          // + 384 bytes: 12 mbarriers, the tensor-memory slot, the abort flag, 64 biases
+    while (nb >= 2 && S::W_BYTES + nb * pbytes + 384 > kShiftMaxSmem) --nb;
     if (nb < 2) return false;
-    const int smem = (int)(S::W_BYTES + nb * pbytes + 64);
+    const int smem = (int)(S::W_BYTES + nb * pbytes + 384);
     static const cudaError_t attr = cudaFuncSetAttribute(k_conv_shift<MODE, CI>, cudaFuncAttributeMaxDynamicSharedMemorySize, kShiftMaxSmem);
     (void)attr;
     static int sms = 0;
@@ -1059,10 +1138,19 @@ int tfd_sg_conv_backward_data(const void *dz, const void *wt, const void *zprev,
     return check_launch("tfd_sg_conv_backward_data");
 }
 
+// Output pixels per partial sum of the weight gradient: at most `chunk`, and fewer on small layers so that about
+// two CTAs per SM (296) sum side by side (a multiple of 64 pixels).
+static long long wgrad_chunk(long long P, int chunk) {
+    long long want = (P + 295) / 296;
+    want = (want + kTile - 1) / kTile * kTile;
+    return want < chunk ? want : chunk;
+}
+
 int tfd_sg_wgrad_scratch(int32_t n, int32_t h, int32_t wd, int32_t ci, int32_t stride, int32_t chunk, size_t *bytes) {
     if (!bytes || chunk < kTile || chunk % kTile) return bad("tfd_sg_wgrad_scratch: chunk must be a positive multiple of 64");
     const long long P = (long long)n * out_size(h, stride) * out_size(wd, stride);
-    const long long chunks = (P + chunk - 1) / chunk;
+    const long long c = wgrad_chunk(P, chunk);
+    const long long chunks = (P + c - 1) / c;
     *bytes = (size_t)(chunks * 9 * kCo * ci + chunks * kCo) * sizeof(float);
     return TFD_OK;
 }
@@ -1077,6 +1165,7 @@ int tfd_sg_conv_backward_weight(const void *dz, const void *x, float *dw, float 
     if (scratch_bytes < need) return bad("tfd_sg_conv_backward_weight: scratch smaller than tfd_sg_wgrad_scratch()");
     const int ho = out_size(h, stride), wo = out_size(wd, stride);
     const long long P = (long long)n * ho * wo;
+    chunk = (int32_t)wgrad_chunk(P, chunk);
     const int chunks = (int)((P + chunk - 1) / chunk);
     float *partial = scratch, *partial_bias = scratch + (long long)chunks * 9 * kCo * ci;
     cudaStream_t s = (cudaStream_t)stream;
@@ -1100,8 +1189,7 @@ int tfd_sg_conv_backward_weight(const void *dz, const void *x, float *dw, float 
         if ((rc = check_launch("tfd_sg_conv_backward_weight"))) return rc;
     }
     const long long len = 9LL * kCo * ci;
-    k_reduce_partials<<<blocks_for(len, 256), 256, 0, s>>>(partial, chunks, len, dw);
-    k_reduce_partials<<<1, kCo, 0, s>>>(partial_bias, chunks, kCo, dbias);
+    k_reduce_partials<<<(unsigned)((len + kCo + 255) / 256), 256, 0, s>>>(partial, chunks, len, dw, partial_bias, kCo, dbias);
     return check_launch("tfd_sg_conv_backward_weight reduce");
 }
 

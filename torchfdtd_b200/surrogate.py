@@ -17,7 +17,7 @@ import numpy as np
 
 LAYERS = ((16, 1), (64, 2), (64, 1), (64, 2), (64, 1), (64, 2), (64, 1), (64, 2))   # (input channels, stride)
 CO = 64
-WGRAD_CHUNK = 4096
+WGRAD_CHUNK = 4096          # the most output pixels per weight-gradient partial sum (small layers use fewer)
 
 _SIGNATURES = {
     'tfd_sg_pack_input': [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p],
