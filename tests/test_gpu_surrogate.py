@@ -185,3 +185,44 @@ def test_shifted_window_conv_matches_the_gather_kernel_and_float64(ci, shape):
     assert rel(out['tcgen05'][0], out['tcgen05_gather'][0]) <= 1e-3
     assert rel(out['tcgen05'][1], out['tcgen05_gather'][1]) <= 1e-3
     assert rel(out['tcgen05'][2], out['tcgen05_gather'][2]) <= 1e-5
+
+
+@pytest.mark.parametrize('ci,shape', [(64, (2, 33, 17)), (16, (3, 24, 20)), (64, (4, 50, 50)), (64, (1, 1, 7))])
+def test_stride2_backward_data_by_parity_class_matches_float64(ci, shape):
+    """Backward data of a stride-2 layer (the tcgen05 kernel runs each parity class of input pixels with only the
+    taps that reach it) against the mma.sync kernel and against dx[2 oy + ky - 1, 2 ox + kx - 1] += dz[oy, ox] w[tap]
+    summed in float64 over the same BF16 operands; odd sizes leave classes of different sizes, and a one-row image
+    leaves two classes empty."""
+    import ctypes
+    import torch
+    from torchfdtd_b200.surrogate import _lib, device_status, out_size, set_tensor_path
+    lib, check = _lib()
+    n, h, w = shape
+    ho, wo = out_size(h, 2), out_size(w, 2)
+    gen = torch.Generator().manual_seed(7 * ci + h)
+    wt = (torch.randn((9, 64, ci), generator=gen) / 24).to(torch.bfloat16)
+    wt_t = wt.transpose(1, 2).contiguous()
+    dz = torch.randn((n, ho, wo, 64), generator=gen).to(torch.bfloat16)
+    dzd, wtd = dz.cuda(), wt_t.cuda()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {}
+    for path in ('tcgen05', 'mma'):
+        set_tensor_path(path)
+        try:
+            dx = torch.full((n, h, w, ci), float('nan'), device='cuda')
+            check(lib.tfd_sg_conv_backward_data(ctypes.c_void_p(dzd.data_ptr()), ctypes.c_void_p(wtd.data_ptr()), None,
+                                                ctypes.c_void_p(dx.data_ptr()), n, h, w, ci, 2, stream))
+            torch.cuda.synchronize()
+            out[path] = dx.cpu().numpy()
+        finally:
+            set_tensor_path('tcgen05')
+    assert device_status() == 0
+    d, wf = dz.double().numpy(), wt.double().numpy()
+    pad = np.zeros((n, h + 2, w + 2, ci))
+    for t in range(9):
+        ky, kx = divmod(t, 3)
+        pad[:, ky:ky + 2 * (ho - 1) + 1:2, kx:kx + 2 * (wo - 1) + 1:2] += d @ wf[t]
+    expected = pad[:, 1:-1, 1:-1]
+    for path, dx in out.items():
+        assert np.isfinite(dx).all(), path
+        assert rel(dx, expected) <= 1e-5, path

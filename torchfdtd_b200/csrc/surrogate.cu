@@ -488,10 +488,15 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // MODE 1 backward data (K = 64 output channels per tap, N = CI input channels).
 // The gathers of tap t+2 (cp.async, zero-filled outside the image) are in flight while the tensor cores
 // work on tap t; a stage is refilled once the commit of the MMAs that read it has arrived.
+// Backward data with stride 2 (cls != nullptr): input pixel (y, x) takes dz only through the taps with
+// ky = y + 1 and kx = x + 1 (mod 2), one tap for (even, even), two for (even, odd) and (odd, even), four for
+// (odd, odd). The rows are grouped by that parity class (CTAs [cls[c], cls[c + 1]) take class c = 2 (y & 1) +
+// (x & 1), rows in (n, y / 2, x / 2) order) and a CTA runs only its class's taps.
 template <int MODE, int CI>
 __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, const bf16 *__restrict__ wsrc,
                                                 const float *__restrict__ bias, const bf16 *__restrict__ zprev, bf16 *__restrict__ out0,
-                                                void *__restrict__ out1, int N, int H, int W, int Ho, int Wo, int stride) {
+                                                void *__restrict__ out1, int N, int H, int W, int Ho, int Wo, int stride,
+                                                const int4 cls = make_int4(0, 0, 0, 0)) {
     constexpr int K = MODE == 0 ? CI : kCo;              // reduction channels per tap
     constexpr int NC = MODE == 0 ? kCo : CI;             // output columns
     constexpr int KC = K / 8;                            // 16-byte K chunks per tap
@@ -504,13 +509,30 @@ __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, c
     uint32_t *slot = reinterpret_cast<uint32_t *>(bar + kStages);
     const int tid = threadIdx.x, warp = tid >> 5;
     // Output rows: MODE 0 output pixels (n, oy, ox); MODE 1 input pixels (n, y, x).
-    const int RH = MODE == 0 ? Ho : H, RW = MODE == 0 ? Wo : W;
+    const bool classes = MODE == 1 && cls.w > 0;
+    int cy = 0, cx = 0, blk = blockIdx.x;
+    if (classes) {
+        const int c = (int)blockIdx.x >= cls.z ? 3 : (int)blockIdx.x >= cls.y ? 2 : (int)blockIdx.x >= cls.x ? 1 : 0;
+        blk -= c == 0 ? 0 : c == 1 ? cls.x : c == 2 ? cls.y : cls.z;
+        cy = c >> 1, cx = c & 1;
+    }
+    // Rows of this CTA's class: y = 2 u + cy, x = 2 v + cx (all pixels with one class when there are no classes).
+    const int RH = MODE == 0 ? Ho : classes ? (H - cy + 1) / 2 : H, RW = MODE == 0 ? Wo : classes ? (W - cx + 1) / 2 : W;
     const long long rows = (long long)N * RH * RW;
-    const long long row = (long long)blockIdx.x * 128 + tid;
-    const bool live = row < rows;
-    const int n = live ? (int)(row / ((long long)RH * RW)) : 0;
-    const int rem = live ? (int)(row % ((long long)RH * RW)) : 0;
-    const int ry = rem / RW, rx = rem % RW;
+    const long long crow = (long long)blk * 128 + tid;
+    const bool live = crow < rows;
+    const int n = live ? (int)(crow / ((long long)RH * RW)) : 0;
+    const int rem = live ? (int)(crow % ((long long)RH * RW)) : 0;
+    const int ry = classes ? 2 * (rem / RW) + cy : rem / RW, rx = classes ? 2 * (rem % RW) + cx : rem % RW;
+    const long long row = classes ? ((long long)n * H + ry) * W + rx : crow;     // the pixel this thread writes
+    // Taps of this CTA: all 9, or the class's 1, 2 or 4 (tap index i -> (ky, kx)).
+    const int nkx = classes ? (cx ? 2 : 1) : 3;
+    const int taps = classes ? (cy ? 2 : 1) * nkx : 9;
+    auto tap_of = [&](int i) {
+        if (!classes) return i;
+        const int ky = cy ? 2 * (i / nkx) : 1, kx = cx ? 2 * (i % nkx) : 1;
+        return ky * 3 + kx;
+    };
     if (warp == 0) tmem_alloc<COLS>(slot);
     if (tid == 0) {
         for (int s = 0; s < kStages; ++s) bar_init(&bar[s]);
@@ -523,8 +545,8 @@ __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, c
 
     // Gathers of one tap into its stage: this thread's row (K channels of the tap's neighbour, zero outside
     // the image or off the stride grid) and its share of the tap's weights ([K chunk][column][16 bytes]).
-    auto issue = [&](int tap) {
-        const int s = tap % kStages, ky = tap / 3, kx = tap % 3;
+    auto issue = [&](int i) {
+        const int s = i % kStages, tap = tap_of(i), ky = tap / 3, kx = tap % 3;
         const bf16 *a = nullptr;
         if (live) {
             if (MODE == 0) {
@@ -550,10 +572,11 @@ __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, c
     bool ok = true;
     int issued = 0;                                      // taps whose MMAs were committed
     issue(0);
-    issue(1);
-    for (int tap = 0; tap < 9; ++tap) {
+    if (taps > 1) issue(1);
+    else cp_async_commit();
+    for (int tap = 0; tap < taps; ++tap) {
         const int s = tap % kStages;
-        if (tap + 2 < 9) {
+        if (tap + 2 < taps) {
             // Stage (tap + 2) % 3 was last read by the MMAs of tap - 1.
             if (tap >= 1 && !bar_wait(&bar[(tap - 1) % kStages], ((tap - 1) / kStages) & 1)) ok = false;
             if (__syncthreads_or(!ok)) break;
@@ -581,7 +604,7 @@ __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, c
     // Wait for the last committed tap (its commit covers every earlier MMA of this thread).
     if (issued > 0 && !bar_wait(&bar[(issued - 1) % kStages], ((issued - 1) / kStages) & 1)) ok = false;
     tc_fence_after();
-    if (__syncthreads_or(!ok) || issued < 9) {
+    if (__syncthreads_or(!ok) || issued < taps) {
         if (tid == 0) atomicExch(&g_sg_status, 1);
     } else {
 #pragma unroll
@@ -1118,17 +1141,29 @@ int tfd_sg_conv_backward_data(const void *dz, const void *wt, const void *zprev,
         if (done) return check_launch("tfd_sg_conv_backward_data (tcgen05, shifted window)");
     }
     if (g_tensor_path) {
-        const dim3 grid((unsigned)((Q + 127) / 128));
+        dim3 grid((unsigned)((Q + 127) / 128));
+        int4 cls = make_int4(0, 0, 0, 0);
+        if (stride == 2) {
+            // CTAs by parity class: class c = 2 (y & 1) + (x & 1) takes blocks [end of class c-1, end of class c).
+            long long end[4], total = 0;
+            for (int c = 0; c < 4; ++c) {
+                const long long rows = (long long)n * ((h - (c >> 1) + 1) / 2) * ((wd - (c & 1) + 1) / 2);
+                total += (rows + 127) / 128;
+                end[c] = total;
+            }
+            cls = make_int4((int)end[0], (int)end[1], (int)end[2], 1);
+            grid = dim3((unsigned)total);
+        }
         if (ci == 16) {
             static const cudaError_t attr = cudaFuncSetAttribute(k_conv_tc<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(64, 16));
             (void)attr;
             k_conv_tc<1, 16><<<grid, 128, tc_smem(64, 16), s>>>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd,
-                                                               ho, wo, stride);
+                                                               ho, wo, stride, cls);
         } else {
             static const cudaError_t attr = cudaFuncSetAttribute(k_conv_tc<1, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem(64, 64));
             (void)attr;
             k_conv_tc<1, 64><<<grid, 128, tc_smem(64, 64), s>>>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd,
-                                                               ho, wo, stride);
+                                                               ho, wo, stride, cls);
         }
         return check_launch("tfd_sg_conv_backward_data (tcgen05)");
     }
