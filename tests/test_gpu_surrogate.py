@@ -189,8 +189,9 @@ def test_shifted_window_conv_matches_the_gather_kernel_and_float64(ci, shape):
 
 @pytest.mark.parametrize('ci,shape', [(64, (2, 33, 17)), (16, (3, 24, 20)), (64, (4, 50, 50)), (64, (1, 1, 7))])
 def test_stride2_backward_data_by_parity_class_matches_float64(ci, shape):
-    """Backward data of a stride-2 layer (the tcgen05 kernel runs each parity class of input pixels with only the
-    taps that reach it) against the mma.sync kernel and against dx[2 oy + ky - 1, 2 ox + kx - 1] += dz[oy, ox] w[tap]
+    """Backward data of a stride-2 layer (the tcgen05 kernels run each parity class of input pixels with only the
+    taps that reach it: as shifted windows of the dz image, and in the gather form) against the mma.sync kernel and
+    against dx[2 oy + ky - 1, 2 ox + kx - 1] += dz[oy, ox] w[tap]
     summed in float64 over the same BF16 operands; odd sizes leave classes of different sizes, and a one-row image
     leaves two classes empty."""
     import ctypes
@@ -206,7 +207,7 @@ def test_stride2_backward_data_by_parity_class_matches_float64(ci, shape):
     dzd, wtd = dz.cuda(), wt_t.cuda()
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     out = {}
-    for path in ('tcgen05', 'mma'):
+    for path in ('tcgen05', 'tcgen05_gather', 'mma'):
         set_tensor_path(path)
         try:
             dx = torch.full((n, h, w, ci), float('nan'), device='cuda')

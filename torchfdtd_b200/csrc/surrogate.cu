@@ -810,6 +810,9 @@ constexpr int kShiftThreads = 384;                        // 12 warps: MMA issue
 constexpr int kShiftMaxSmem = 227 * 1024;
 constexpr int kShiftSmPerSm = 228 * 1024;                  // shared memory of an SM (1 KB of it reserved per CTA)
 __host__ __device__ constexpr int shift_np(int W) { return (128 + 2 * (W + 2) + 2 + 7) / 8 * 8; }
+// MODE 2 (stride-2 backward data by parity class): the dz image with one zero column and row at its far edges
+// (row width Wo + 1), read at offsets 0 or 1 along each axis.
+__host__ __device__ constexpr int shift_np2(int Wo) { return (128 + (Wo + 1) + 1 + 7) / 8 * 8; }
 
 // Bounded wait that also gives up once another role of the CTA has aborted (*abort set).
 __device__ __forceinline__ bool bar_wait_or_abort(uint64_t *bar, uint32_t parity, volatile int *abort) {
@@ -852,7 +855,12 @@ __global__ void __launch_bounds__(kShiftThreads) k_conv_shift(const bf16 *__rest
     constexpr int SPAN = NC >= 32 ? NC / 2 : NC;           // columns per storing warp
     constexpr uint32_t IDESC = umma_idesc(128, NC);
     extern __shared__ __align__(1024) unsigned char smem[];
-    const int Wp = W + 2, np = shift_np(W);
+    // MODE 2: input pixels (y, x) = (2u + cy, 2v + cx) of parity class c = 2 cy + cx take dz[u + dy][v + dx] through
+    // the taps ky = y + 1, kx = x + 1 (mod 2), dy = (cy + 1 - ky) / 2 in {0, 1} (likewise dx): per class a conv of
+    // the dz image with 1, 2 or 4 taps, on rows f = u (Wo + 1) + v. MODES 0 and 1: rows f = y (W + 2) + x.
+    constexpr bool CLS = MODE == 2;
+    const int Ho = (H - 1) / 2 + 1, Wo = (W - 1) / 2 + 1;
+    const int Wp = CLS ? Wo + 1 : W + 2, np = CLS ? shift_np2(Wo) : shift_np(W);
     const int lbo = (np + S::LPAD) * 16, pbytes = KC * lbo;
     unsigned char *ws = smem, *ps = smem + S::W_BYTES;
     uint64_t *full = reinterpret_cast<uint64_t *>(ps + NB * pbytes);
@@ -861,7 +869,25 @@ __global__ void __launch_bounds__(kShiftThreads) k_conv_shift(const bf16 *__rest
     volatile int *abort = reinterpret_cast<volatile int *>(slot + 1);
     float *sbias = reinterpret_cast<float *>(full + 13);      // forward: the 64 biases
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tiles_img = (H * Wp + 127) / 128, tiles = N * tiles_img;
+    const int tiles_img = (H * Wp + 127) / 128;
+    int tend[4] = {0, 0, 0, 0}, tiles = N * tiles_img;      // MODE 2: tiles of classes 0..c
+    if (CLS) {
+        for (int c = 0, t = 0; c < 4; ++c) {
+            t += N * ((((H - (c >> 1) + 1) / 2) * Wp + 127) / 128);
+            tend[c] = t;
+        }
+        tiles = tend[3];
+    }
+    // Image n, first row f0 and parity class c of a tile.
+    auto decode = [&](int tile, int &n, int &f0, int &c) {
+        if (!CLS) {
+            n = tile / tiles_img, f0 = (tile % tiles_img) * 128, c = 0;
+            return;
+        }
+        c = tile >= tend[2] ? 3 : tile >= tend[1] ? 2 : tile >= tend[0] ? 1 : 0;
+        const int local = tile - (c ? tend[c - 1] : 0), per = ((((H - (c >> 1) + 1) / 2) * Wp + 127) / 128);
+        n = local / per, f0 = (local % per) * 128;
+    };
     const int count = (int)blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;   // local tiles
     if (warp == 0) tmem_alloc<S::COLS>(slot);
     if (tid == 0) {
@@ -895,14 +921,16 @@ __global__ void __launch_bounds__(kShiftThreads) k_conv_shift(const bf16 *__rest
         for (int j = 0; j < count; ++j) {
             const int b = j % NB;
             if (j >= NB && !bar_wait_or_abort(&empty[b], (j / NB - 1) & 1, abort)) break;
-            const int tile = blockIdx.x + j * gridDim.x;
-            const int n = tile / tiles_img, f0 = (tile % tiles_img) * 128;
+            int n, f0, c;
+            decode(blockIdx.x + j * gridDim.x, n, f0, c);
             unsigned char *p = ps + b * pbytes;
             for (int e = lt; e < np * KC; e += LOADERS) {
                 const int kc = e % KC, i = e / KC, g = f0 + i;
                 const int py = g / Wp, px = g - py * Wp;
-                const bool in = py >= 1 && py <= H && px >= 1 && px <= W;
-                const bf16 *s = in ? src + (((long long)n * H + py - 1) * W + px - 1) * K + kc * 8 : src;
+                const bool in = CLS ? py < Ho && px < Wo : py >= 1 && py <= H && px >= 1 && px <= W;
+                const bf16 *s = !in ? src
+                              : CLS ? src + (((long long)n * Ho + py) * Wo + px) * K + kc * 8
+                                    : src + (((long long)n * H + py - 1) * W + px - 1) * K + kc * 8;
                 cp_async16(p + kc * lbo + i * 16, s, in ? 16 : 0);
             }
             cp_async_commit();
@@ -925,15 +953,28 @@ __global__ void __launch_bounds__(kShiftThreads) k_conv_shift(const bf16 *__rest
                 if (j >= 2 && !bar_wait_or_abort(&acce[a], (j / 2 - 1) & 1, abort)) break;
                 tc_fence_after();
                 const uint32_t pa = sh_addr(ps + b * pbytes), wa = sh_addr(ws);
-#pragma unroll
-                for (int t = 0; t < 9; ++t) {
-                    const int ky = t / 3, kx = t % 3;
-                    const int shift = MODE == 0 ? ky * Wp + kx : (2 - ky) * Wp + (2 - kx);
+                int n, f0, c;
+                decode(blockIdx.x + j * gridDim.x, n, f0, c);
+                // Tap i of the tile: weights of tap t, patch shifted by `shift` pixels.
+                auto mma_tap = [&](int i, int t, int shift) {
 #pragma unroll
                     for (int kk = 0; kk < K / 16; ++kk) {
                         const uint64_t ad = umma_desc(pa + shift * 16 + kk * 2 * lbo, lbo, 128);
                         const uint64_t bd = umma_desc(wa + (t * KC + 2 * kk) * NC * 16, NC * 16, 128);
-                        umma_bf16(tmem + a * NC, ad, bd, IDESC, (t | kk) != 0);
+                        umma_bf16(tmem + a * NC, ad, bd, IDESC, (i | kk) != 0);
+                    }
+                };
+                if constexpr (CLS) {
+                    const int nkx = c & 1 ? 2 : 1, taps = (c >> 1 ? 2 : 1) * nkx;
+                    for (int i = 0; i < taps; ++i) {
+                        const int ky = c >> 1 ? 2 * (i / nkx) : 1, kx = c & 1 ? 2 * (i % nkx) : 1;
+                        mma_tap(i, ky * 3 + kx, (ky == 0) * Wp + (kx == 0));
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) {
+                        const int ky = i / 3, kx = i % 3;
+                        mma_tap(i, i, MODE == 0 ? ky * Wp + kx : (2 - ky) * Wp + (2 - kx));
                     }
                 }
                 umma_commit(&empty[b]);
@@ -958,11 +999,13 @@ __global__ void __launch_bounds__(kShiftThreads) k_conv_shift(const bf16 *__rest
             const int a = j & 1;
             if (!bar_wait_or_abort(&accf[a], (j / 2) & 1, abort)) break;
             tc_fence_after();
-            const int tile = blockIdx.x + j * gridDim.x;
-            const int n = tile / tiles_img, f = (tile % tiles_img) * 128 + quarter * 32 + lane;
-            const int oy = f / Wp, ox = f - oy * Wp;
-            const bool live = oy < H && ox < W;
-            const long long row = ((long long)n * H + oy) * W + ox;
+            int n, f0, c;
+            decode(blockIdx.x + j * gridDim.x, n, f0, c);
+            const int f = f0 + quarter * 32 + lane;
+            const int u = f / Wp, v = f - u * Wp;
+            const int cy = c >> 1, cx = c & 1;
+            const bool live = CLS ? u < (H - cy + 1) / 2 && v < (W - cx + 1) / 2 : u < H && v < W;
+            const long long row = CLS ? ((long long)n * H + 2 * u + cy) * W + 2 * v + cx : ((long long)n * H + u) * W + v;
 #pragma unroll
             for (int c0 = cbeg; c0 < cbeg + SPAN; c0 += 16) {
                 float v[16];
@@ -1013,7 +1056,8 @@ template <int MODE, int CI>
 bool launch_shift(const bf16 *src, const bf16 *w, const float *bias, const bf16 *zprev, bf16 *o0, void *o1, int n, int h, int wd,
                   cudaStream_t s) {
     using S = ShiftShape<MODE, CI>;
-    const long long pbytes = (long long)S::KC * (shift_np(wd) + S::LPAD) * 16;
+    const int wo = (wd - 1) / 2 + 1, wp = MODE == 2 ? wo + 1 : wd + 2;
+    const long long pbytes = (long long)S::KC * ((MODE == 2 ? shift_np2(wo) : shift_np(wd)) + S::LPAD) * 16;
     int nb = 4;                          // + 384 bytes: 12 mbarriers, the tensor-memory slot, the abort flag, 64 biases
     while (nb >= 2 && S::W_BYTES + nb * pbytes + 384 > kShiftMaxSmem) --nb;
     if (nb < 2) return false;
@@ -1030,14 +1074,18 @@ bool launch_shift(const bf16 *src, const bf16 *w, const float *bias, const bf16 
     per_sm = per_sm < 512 / S::COLS ? per_sm : 512 / S::COLS;      // tensor-memory columns of an SM
     per_sm = per_sm < 2048 / kShiftThreads ? per_sm : 2048 / kShiftThreads;
     per_sm = per_sm < 1 ? 1 : per_sm;
-    const long long tiles = (long long)n * ((h * (wd + 2) + 127) / 128);
+    long long tiles = (long long)n * ((h * wp + 127) / 128);
+    if (MODE == 2) {
+        tiles = 0;
+        for (int c = 0; c < 4; ++c) tiles += (long long)n * ((((h - (c >> 1) + 1) / 2) * wp + 127) / 128);
+    }
     const long long grid = tiles < (long long)sms * per_sm ? tiles : (long long)sms * per_sm;
     k_conv_shift<MODE, CI><<<(unsigned)grid, kShiftThreads, (size_t)smem, s>>>(src, w, bias, zprev, o0, o1, n, h, wd, nb);
     return true;
 }
 
-// 0: mma.sync kernels; 1: tcgen05 kernels, the shifted-window form for stride-1 layers where it fits (default);
-// 2: tcgen05 kernels, the per-tap gather form for every layer.
+// 0: mma.sync kernels; 1: tcgen05 kernels, the shifted-window form where it fits (default: stride-1 layers, and the
+// stride-2 input gradient by parity class); 2: tcgen05 kernels, the per-tap gather form for every layer.
 int g_tensor_path = 1;
 
 int blocks_for(long long work, int threads) {
@@ -1135,9 +1183,14 @@ int tfd_sg_conv_backward_data(const void *dz, const void *wt, const void *zprev,
     cudaStream_t s = (cudaStream_t)stream;
     bf16 *o0 = zprev ? (bf16 *)out : nullptr;
     void *o1 = zprev ? nullptr : out;
-    if (g_tensor_path == 1 && stride == 1) {
-        const bool done = ci == 16 ? launch_shift<1, 16>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd, s)
-                                   : launch_shift<1, 64>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd, s);
+    if (g_tensor_path == 1) {
+        bool done;
+        if (stride == 1)
+            done = ci == 16 ? launch_shift<1, 16>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd, s)
+                            : launch_shift<1, 64>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd, s);
+        else
+            done = ci == 16 ? launch_shift<2, 16>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd, s)
+                            : launch_shift<2, 64>((const bf16 *)dz, (const bf16 *)wt, nullptr, (const bf16 *)zprev, o0, o1, n, h, wd, s);
         if (done) return check_launch("tfd_sg_conv_backward_data (tcgen05, shifted window)");
     }
     if (g_tensor_path) {
