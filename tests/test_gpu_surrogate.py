@@ -227,3 +227,40 @@ def test_stride2_backward_data_by_parity_class_matches_float64(ci, shape):
     for path, dx in out.items():
         assert np.isfinite(dx).all(), path
         assert rel(dx, expected) <= 1e-5, path
+
+
+@pytest.mark.parametrize('shape', [(2, 33, 17), (3, 50, 50), (2, 100, 100), (1, 1, 7)])
+def test_stride2_forward_phase_windows_match_the_gather_kernel_and_float64(shape):
+    """Stride-2 forward of a 64-channel layer on the tcgen05 path (the per-tap gather kernel: the shifted-window form
+    with the four row/column phases of the padded input as windows of one patch was measured slower, 821 against
+    410 us on the 100x100 layer) against float64 sums of the same BF16 operands, on odd sizes and a one-row image."""
+    import ctypes
+    import torch
+    from torchfdtd_b200.surrogate import _lib, device_status, out_size, set_tensor_path
+    lib, check = _lib()
+    n, h, w = shape
+    ho, wo = out_size(h, 2), out_size(w, 2)
+    gen = torch.Generator().manual_seed(h * w)
+    x = torch.randn((n, h, w, 64), generator=gen).to(torch.bfloat16)
+    wt = (torch.randn((9, 64, 64), generator=gen) / 24).to(torch.bfloat16)
+    bias = torch.randn(64, generator=gen) * .1
+    xd, wd, bd = x.cuda(), wt.cuda(), bias.cuda()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {}
+    for path in ('tcgen05', 'tcgen05_gather'):
+        set_tensor_path(path)
+        try:
+            z = torch.empty((n, ho, wo, 64), dtype=torch.bfloat16, device='cuda')
+            a = torch.empty_like(z)
+            check(lib.tfd_sg_conv_forward(ctypes.c_void_p(xd.data_ptr()), ctypes.c_void_p(wd.data_ptr()), ctypes.c_void_p(bd.data_ptr()),
+                                          ctypes.c_void_p(z.data_ptr()), ctypes.c_void_p(a.data_ptr()), n, h, w, 64, 2, stream))
+            torch.cuda.synchronize()
+            out[path] = (z.float().cpu().numpy(), a.float().cpu().numpy())
+        finally:
+            set_tensor_path('tcgen05')
+    assert device_status() == 0
+    zref = _conv_reference(x.double().numpy(), wt.double().numpy(), 2) + bias.double().numpy()
+    for path, (z, a) in out.items():
+        assert rel(z, zref) <= 1e-2, path
+    assert rel(out['tcgen05'][0], out['tcgen05_gather'][0]) <= 1e-3
+    assert rel(out['tcgen05'][1], out['tcgen05_gather'][1]) <= 1e-3
