@@ -655,6 +655,7 @@ __global__ void __launch_bounds__(128) k_conv_tc(const bf16 *__restrict__ src, c
 // accumulator in tensor memory; the padding rows past the ones row stay zero. Three stages: the cp.async gathers
 // of block b+2 are in flight while the tensor cores work on block b. Bounded waits as in k_conv_tc.
 constexpr int kWgKB = 32;                          // pixels per stage (two K = 16 MMA steps)
+constexpr int kWgThreads = 256;                    // 8 warps: more gathers in flight (one CTA per SM: 512 tensor-memory columns)
 template <int CI>
 struct WgradShape {
     static constexpr int ROWS = 9 * CI;                    // (tap, ci) rows; row ROWS is the ones row
@@ -667,7 +668,7 @@ struct WgradShape {
 };
 
 template <int CI>
-__global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dZ, const bf16 *__restrict__ X, float *__restrict__ partial,
+__global__ void __launch_bounds__(kWgThreads) k_wgrad_tc(const bf16 *__restrict__ dZ, const bf16 *__restrict__ X, float *__restrict__ partial,
                                                  float *__restrict__ partial_bias, int N, int H, int W, int Ho, int Wo, int stride,
                                                  int chunk) {
     using S = WgradShape<CI>;
@@ -689,7 +690,7 @@ __global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dZ, c
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // The rows past the gathered ones never change: the ones row (element 0 of its chunk) and zero padding.
-    for (int e = tid; e < kStages * (S::MCH - S::ROWS / 8) * kWgKB; e += 128) {
+    for (int e = tid; e < kStages * (S::MCH - S::ROWS / 8) * kWgKB; e += kWgThreads) {
         const int s = e / ((S::MCH - S::ROWS / 8) * kWgKB), r = e % ((S::MCH - S::ROWS / 8) * kWgKB);
         const int mc = S::ROWS / 8 + r / kWgKB, j = r % kWgKB;
         *reinterpret_cast<uint4 *>(As + s * S::A_BYTES + (mc * kWgKB + j) * 16) =
@@ -700,7 +701,7 @@ __global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dZ, c
     tc_fence_after();
     const uint32_t tmem = *slot;
 
-    // Gathers of pixel block b into its stage: lane = pixel of the block, warp = a quarter of the chunks.
+    // Gathers of pixel block b into its stage: lane = pixel of the block, warp = an eighth of the chunks.
     auto issue = [&](int b) {
         const int s = b % kStages;
         const long long p = begin + (long long)b * kWgKB + lane;
@@ -709,7 +710,7 @@ __global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dZ, c
         const int rem = live ? (int)(p % ((long long)Ho * Wo)) : 0;
         const int oy = rem / Wo, ox = rem % Wo;
         unsigned char *as = As + s * S::A_BYTES + lane * 16;
-        for (int i = warp; i < 9 * CC; i += 4) {
+        for (int i = warp; i < 9 * CC; i += kWgThreads / 32) {
             const int t = i / CC, c = i % CC;
             const int iy = oy * stride + t / 3 - 1, ix = ox * stride + t % 3 - 1;
             const bool in = live && iy >= 0 && iy < H && ix >= 0 && ix < W;
@@ -717,7 +718,7 @@ __global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dZ, c
             cp_async16(as + i * (kWgKB * 16), src, in ? 16 : 0);
         }
         unsigned char *bs = Bs + s * S::B_BYTES + lane * 16;
-        for (int c = warp; c < 8; c += 4) cp_async16(bs + c * (kWgKB * 16), live ? dZ + p * kCo + c * 8 : dZ, live ? 16 : 0);
+        for (int c = warp; c < 8; c += kWgThreads / 32) cp_async16(bs + c * (kWgKB * 16), live ? dZ + p * kCo + c * 8 : dZ, live ? 16 : 0);
         cp_async_commit();
     };
 
@@ -759,13 +760,15 @@ __global__ void __launch_bounds__(128) k_wgrad_tc(const bf16 *__restrict__ dZ, c
     if (__syncthreads_or(!ok) || issued < blocks) {
         if (tid == 0) atomicExch(&g_sg_status, 1);
     } else {
+        // Warp w reads tensor-memory lanes 32 (w % 4) .. + 31 of the tiles m = w / 4, w / 4 + 2, ...
 #pragma unroll 1
-        for (int m = 0; m < S::MT; ++m) {
-            const int r = m * 128 + warp * 32 + lane;         // this lane's row: (tap, ci) or the ones row
+        for (int m = warp >> 2; m < S::MT; m += 2) {
+            const int q = warp & 3;
+            const int r = m * 128 + q * 32 + lane;            // this lane's row: (tap, ci) or the ones row
 #pragma unroll
             for (int c0 = 0; c0 < kCo; c0 += 16) {
                 float v[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + m * kCo + c0, v);
+                tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + m * kCo + c0, v);
                 if (r < S::ROWS) {
                     float *o = partial + ((long long)blockIdx.x * 9 + r / CI) * kCo * CI + r % CI;
 #pragma unroll
@@ -1261,12 +1264,12 @@ int tfd_sg_conv_backward_weight(const void *dz, const void *x, float *dw, float 
         if (ci == 16) {
             static const cudaError_t attr = cudaFuncSetAttribute(k_wgrad_tc<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, WgradShape<16>::SMEM);
             (void)attr;
-            k_wgrad_tc<16><<<chunks, 128, WgradShape<16>::SMEM, s>>>((const bf16 *)dz, (const bf16 *)x, partial, partial_bias, n, h, wd, ho, wo,
+            k_wgrad_tc<16><<<chunks, kWgThreads, WgradShape<16>::SMEM, s>>>((const bf16 *)dz, (const bf16 *)x, partial, partial_bias, n, h, wd, ho, wo,
                                                                     stride, chunk);
         } else {
             static const cudaError_t attr = cudaFuncSetAttribute(k_wgrad_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, WgradShape<64>::SMEM);
             (void)attr;
-            k_wgrad_tc<64><<<chunks, 128, WgradShape<64>::SMEM, s>>>((const bf16 *)dz, (const bf16 *)x, partial, partial_bias, n, h, wd, ho, wo,
+            k_wgrad_tc<64><<<chunks, kWgThreads, WgradShape<64>::SMEM, s>>>((const bf16 *)dz, (const bf16 *)x, partial, partial_bias, n, h, wd, ho, wo,
                                                                     stride, chunk);
         }
         if ((rc = check_launch("tfd_sg_conv_backward_weight (tcgen05)"))) return rc;
