@@ -469,6 +469,23 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 lanes x 32 columns in one load and one wait.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,"
+        "%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]),
+          "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+          "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -847,8 +864,9 @@ __device__ __forceinline__ void bar_arrive(uint64_t *bar) {
 // (tcgen05.commit); accf[a]: accumulator a holds a finished tile (commit); acce[a]: the storing threads have
 // read accumulator a. A loader keeps two tiles of copies in flight and runs up to NB
 // tiles ahead of the tensor cores; the tensor cores run one tile ahead of the stores.
+// Register budget: three CTAs per SM for the 16-channel input layer (its shared memory allows three), one otherwise.
 template <int MODE, int CI>
-__global__ void __launch_bounds__(kShiftThreads) k_conv_shift(const bf16 *__restrict__ src, const bf16 *__restrict__ wsrc,
+__global__ void __launch_bounds__(kShiftThreads, MODE == 0 && CI == 16 ? 3 : 1) k_conv_shift(const bf16 *__restrict__ src, const bf16 *__restrict__ wsrc,
                                                              const float *__restrict__ bias, const bf16 *__restrict__ zprev,
                                                              bf16 *__restrict__ out0, void *__restrict__ out1, int N, int H, int W, int NB) {
     using S = ShiftShape<MODE, CI>;
@@ -1009,10 +1027,19 @@ __global__ void __launch_bounds__(kShiftThreads) k_conv_shift(const bf16 *__rest
             const int cy = c >> 1, cx = c & 1;
             const bool live = CLS ? u < (H - cy + 1) / 2 && v < (W - cx + 1) / 2 : u < H && v < W;
             const long long row = CLS ? ((long long)n * H + 2 * u + cy) * W + 2 * v + cx : ((long long)n * H + u) * W + v;
+            // This warp's SPAN columns in one tensor-memory load (one wait), then 16 at a time.
+            float vs[SPAN];
+            if constexpr (SPAN == 32) {
+                tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + a * NC + cbeg, vs);
+            } else {
+                float v16[16];
+                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + a * NC + cbeg, v16);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) vs[i] = v16[i];
+            }
 #pragma unroll
             for (int c0 = cbeg; c0 < cbeg + SPAN; c0 += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + a * NC + c0, v);
+                const float *v = vs + (c0 - cbeg);
                 if (!live) continue;
                 if (MODE == 0) {
                     __align__(16) bf16 zb[16], ab[16];
@@ -1073,7 +1100,14 @@ bool launch_shift(const bf16 *src, const bf16 *w, const float *bias, const bf16 
         if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
             sms = 148;
     }
+    static int regs = 0;
+    if (!regs) {
+        cudaFuncAttributes fa;
+        regs = cudaFuncGetAttributes(&fa, k_conv_shift<MODE, CI>) == cudaSuccess && fa.numRegs > 0 ? fa.numRegs : 255;
+    }
     int per_sm = kShiftSmPerSm / (smem + 1024);
+    const int regs_cta = (regs * 32 + 255) / 256 * 256 * (kShiftThreads / 32);   // registers are allocated per warp
+    per_sm = per_sm < 65536 / regs_cta ? per_sm : 65536 / regs_cta;
     per_sm = per_sm < 512 / S::COLS ? per_sm : 512 / S::COLS;      // tensor-memory columns of an SM
     per_sm = per_sm < 2048 / kShiftThreads ? per_sm : 2048 / kShiftThreads;
     per_sm = per_sm < 1 ? 1 : per_sm;
