@@ -10,8 +10,9 @@
 //   forward          z[p, co] = bias[co] + sum_{tap, ci} x[in(p, tap), ci] w[tap, co, ci];  a = gelu(z)
 //   backward (data)  dx[q, ci] = sum_{tap, co} dz[out(q, tap), co] w[tap, co, ci]  (then * gelu'(z_prev))
 //   backward (weight) dw[tap, co, ci] = sum_p dz[p, co] x[in(p, tap), ci]; dbias[co] = sum_p dz[p, co]
-// All three are implicit GEMMs. The tcgen05 kernels (k_conv_tc for forward and backward data, k_wgrad_tc for
-// backward weight) stage cp.async gathers in shared memory for MMAs issued by one thread into tensor memory. The
+// All three are implicit GEMMs. The tcgen05 kernels (k_conv_shift for the stride-1 layers and the stride-2 input
+// gradient, k_conv_tc for the other forward and backward-data cases, k_wgrad_tc for backward weight) stage cp.async
+// loads in shared memory for MMAs issued by one thread into tensor memory. The
 // mma.sync kernels work on 64 x 64 tiles: 4 warps, each 16 rows x 64 columns of m16n8k16 MMAs, with the operands
 // staged in shared memory (row-major A, column-major B, both padded to 144-byte rows so the fragment loads are
 // bank-conflict free).
