@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kThreads) k_conv_dgrad(const bf16 *__restrict_
 
 // ---- backward, weight -----------------------------------------------------------------------------------
 // One CTA: one tap, one chunk of output pixels; rows co, columns ci, K = pixels. Writes its partial sums
-// (and, for the centre tap, the partial bias gradient); k_reduce_partials adds the chunks in order.
+// (and, for the centre tap, the partial bias gradient); k_reduce_partials adds the chunks in a fixed order.
 template <int CI>
 __global__ void __launch_bounds__(kThreads) k_conv_wgrad(const bf16 *__restrict__ dZ, const bf16 *__restrict__ X,
                                                         float *__restrict__ partial, float *__restrict__ partial_bias, int N, int H,
@@ -254,32 +254,39 @@ __global__ void __launch_bounds__(kThreads) k_conv_wgrad(const bf16 *__restrict_
     if (tap == 4 && threadIdx.x < kCo) partial_bias[(long long)blockIdx.x * kCo + threadIdx.x] = bias_acc;
 }
 
-// out[e] = the sum over chunks c, in chunk order, of partial[c * len + e]; the threads past the weights reduce the
-// bias partials (len_b per chunk) the same way. Each thread has eight chunks' loads in flight at a time.
-__global__ void k_reduce_partials(const float *__restrict__ partial, int chunks, long long len, float *__restrict__ out,
-                                  const float *__restrict__ partial_b, int len_b, float *__restrict__ out_b) {
-    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const float *src;
-    long long stride;
-    float *dst;
+// out[e] = the sum over chunks c of partial[c * len + e]; elements past the weights reduce the bias partials
+// (len_b per chunk) the same way. A block of 256 threads takes 64 elements: thread group g (64 threads) sums chunks
+// g, g + 4, g + 8, ... in order with eight loads in flight, and the four group sums are added in the order 0, 1, 2,
+// 3, so the result does not depend on scheduling.
+__global__ void __launch_bounds__(256) k_reduce_partials(const float *__restrict__ partial, int chunks, long long len,
+                                                         float *__restrict__ out, const float *__restrict__ partial_b, int len_b,
+                                                         float *__restrict__ out_b) {
+    __shared__ float part[4][64];
+    const int g = threadIdx.x >> 6, l = threadIdx.x & 63;
+    const long long e = blockIdx.x * 64LL + l;
+    const float *src = nullptr;
+    long long stride = 0;
+    float *dst = nullptr;
     if (e < len) {
         src = partial + e, stride = len, dst = out + e;
     } else if (e < len + len_b) {
         src = partial_b + (e - len), stride = len_b, dst = out_b + (e - len);
-    } else {
-        return;
     }
     float s = 0.f;
-    int c = 0;
-    for (; c + 8 <= chunks; c += 8) {
-        float v[8];
+    if (src) {
+        int c = g;
+        for (; c + 28 < chunks; c += 32) {
+            float v[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] = src[(long long)(c + i) * stride];
+            for (int i = 0; i < 8; ++i) v[i] = src[(long long)(c + 4 * i) * stride];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) s += v[i];
+            for (int i = 0; i < 8; ++i) s += v[i];
+        }
+        for (; c < chunks; c += 4) s += src[(long long)c * stride];
     }
-    for (; c < chunks; ++c) s += src[(long long)c * stride];
-    *dst = s;
+    part[g][l] = s;
+    __syncthreads();
+    if (g == 0 && dst) *dst = ((part[0][l] + part[1][l]) + part[2][l]) + part[3][l];
 }
 
 // ---- input packing, head, loss, optimiser ---------------------------------------------------------------
@@ -1315,7 +1322,7 @@ int tfd_sg_conv_backward_weight(const void *dz, const void *x, float *dw, float 
         if ((rc = check_launch("tfd_sg_conv_backward_weight"))) return rc;
     }
     const long long len = 9LL * kCo * ci;
-    k_reduce_partials<<<(unsigned)((len + kCo + 255) / 256), 256, 0, s>>>(partial, chunks, len, dw, partial_bias, kCo, dbias);
+    k_reduce_partials<<<(unsigned)((len + kCo + 63) / 64), 256, 0, s>>>(partial, chunks, len, dw, partial_bias, kCo, dbias);
     return check_launch("tfd_sg_conv_backward_weight reduce");
 }
 
